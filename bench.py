@@ -1,0 +1,273 @@
+"""Benchmark of the spectral path-tracing hot path on B200.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload box_room]
+
+One step renders the whole workload once (every pixel, every frame of its spp,
+through vs_render on the GPU).  value = paths of all ranks / max-over-ranks
+device time of the K timed steps, in Mpaths/s.  Multi-GPU runs are
+independent replicas (weak scaling); the path has no exchange step.
+--impl reference times the reference integrator's CPU restatement (the
+reference itself does not build offline) on the host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # Box room: 256 x 256, 16 spp, max depth 8, 4 hero wavelengths, 6500 K
+    # blackbody light, PCG sampler seed 0, FP32 film.
+    'box_room': dict(kind='box_room', width=256, height=256, spp=16, max_depth=8, dimension=4, sampler='pcg', seed=0),
+}
+
+
+def workload_scene(name):
+    from vision_b200 import scenes
+    w = WORKLOADS[name]
+    if w['kind'] == 'box_room':
+        return scenes.box_room(width=w['width'], height=w['height'], max_depth=w['max_depth'],
+                               dimension=w['dimension'], sampler=w['sampler'], seed=w['seed'])
+    raise ValueError(name)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get('hbm_gbs', 6650.0), 'measured'
+    return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ['clocks.sm', 'clocks.max.sm', 'power.draw', 'clocks_event_reasons.hw_slowdown',
+              'clocks_event_reasons.hw_thermal_slowdown', 'clocks_event_reasons.sw_thermal_slowdown',
+              'clocks_event_reasons.sw_power_cap']
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + ','.join(self.FIELDS),
+                                          '--format=csv,noheader,nounits', '-lms', '100'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(',')]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def cpu_baseline(scene, budget_s=12.0):
+    """The oracle (a scalar C++ port of the reference integrator) on all host
+    cores, on whole frames of the same workload until the time budget is used."""
+    import oracle
+    o = oracle.OracleScene(scene)
+    threads = os.cpu_count()
+    npix = o.width * o.height
+    frames = 0
+    t0 = time.perf_counter()
+    while frames < 16 and time.perf_counter() - t0 < budget_s:
+        o.render(frames, 1, threads=threads)
+        frames += 1
+    dt = time.perf_counter() - t0
+    return {'value': frames * npix / dt / 1e6, 'unit': 'Mpaths/s', 'cores': threads, 'kind': 'port',
+            'sample': '%d of 16 frames of the %dx%d workload (%d paths) in %.1f s' % (frames, o.width, o.height,
+                                                                                    frames * npix, dt)}
+
+
+def run_reference(args, rank):
+    """Reference arm: the CPU restatement of the reference integrator on the
+    host cores (the reference's CUDA/OptiX build cannot be built offline)."""
+    if rank != 0:
+        return
+    import vision_b200 as vb
+    import oracle
+    w = WORKLOADS[args.workload]
+    ctx = vb.Context(-1)
+    scene = vb.Scene(ctx, workload_scene(args.workload)).build_accel()
+    o = oracle.OracleScene(scene)
+    threads = os.cpu_count()
+    npix = o.width * o.height
+    for i in range(args.warmup):
+        o.render(i % w['spp'], 1, threads=threads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        o.render(i % w['spp'], 1, threads=threads)
+    dt = time.perf_counter() - t0
+    value = args.steps * npix / dt / 1e6
+    line = {'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': dt * 1e3 / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
+                       'step': 'one 1-spp frame of the workload per step'},
+            'impl': 'reference',
+            'cpu_baseline': {'value': value, 'unit': 'Mpaths/s', 'cores': threads, 'kind': 'port',
+                             'sample': '1 frame (%d paths) per step' % npix},
+            'e2e': {'value': value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='box_room', choices=sorted(WORKLOADS))
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank)
+        return
+
+    import torch
+    import vision_b200 as vb
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    w = WORKLOADS[args.workload]
+    ctx = vb.Context(local_rank)
+    scene = vb.Scene(ctx, workload_scene(args.workload))
+    t0 = time.perf_counter()
+    scene.build_accel()
+    build_s = time.perf_counter() - t0
+    info = scene.info()
+    spp = w['spp']
+    npix = w['width'] * w['height']
+    paths_per_step = npix * spp
+    stream = torch.cuda.current_stream().cuda_stream
+
+    # Algorithmic bytes per path (B_path = 32 + sum over segments of
+    # 80 N_node + 36 N_tri + 180), from an instrumented render outside the timing.
+    segs, nodes, tris = scene.render_stats(0, spp)
+    bytes_per_path = 32.0 + (80.0 * nodes + 36.0 * tris + 180.0 * segs) / paths_per_step
+
+    for i in range(args.warmup):
+        scene.render(0, spp, stream=stream)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+    clocks = ClockSampler(torch.cuda.current_device())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    scene.timing_enable(True)
+    launches0 = vb.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (inputs are smaller than L2)
+        starts[i].record()
+        scene.render(0, spp, stream=stream)
+        ends[i].record()
+    torch.cuda.synchronize()
+    launches = vb.launch_count() - launches0
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    step_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    render_ms, film_ms, render_launches = scene.timing_read()
+    scene.timing_enable(False)
+    t = torch.tensor([step_ms, render_ms], dtype=torch.float64, device='cuda')
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms, render_ms = float(t[0]), float(t[1])
+    value = world * paths_per_step * args.steps / (step_ms / 1e3) / 1e6
+
+    # End to end through the public API with host buffers: camera in, film out.
+    cam = scene.export('camera', np.float32)[:16].copy()
+    film_host = torch.empty((info['height'], info['width'], 4), dtype=torch.float32).pin_memory()
+    film_np = film_host.numpy()
+    e2e_steps = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        vb.lib.vs_camera_set(scene.handle, vb._ptr(cam), 40.0)
+        scene.render(0, spp)
+        ctx.check(vb.lib.vs_film_download(scene.handle, vb._ptr(film_np), film_np.nbytes, vb.FILM_LINEAR), 'film')
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device='cuda')
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * paths_per_step * e2e_steps / float(e2e_t[0]) / 1e6
+
+    peak, peak_src = measured_peaks()
+    kernel_s = render_ms / 1e3 / max(render_launches, 1)
+    achieved = bytes_per_path * paths_per_step / kernel_s / 1e9
+    line = {
+        'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': step_ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
+                   'prims': info['prim_count'], 'bvh_nodes': info['bvh_node_count'],
+                   'paths_per_step': paths_per_step, 'l2': 'flushed between steps (256 MiB write)',
+                   'parallelism': 'replicas%d' % world, 'scene_build_s': round(build_s, 3)},
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                     'peak_source': peak_src, 'traffic': None, 'kernel': 'k_render',
+                     'bytes_per_path': bytes_per_path,
+                     'per_path': {'segments': segs / paths_per_step, 'nodes': nodes / paths_per_step,
+                                  'tris': tris / paths_per_step},
+                     'kernel_ms_per_launch': kernel_s * 1e3, 'film_ms_per_launch': film_ms / max(render_launches, 1)},
+        'clocks': clk,
+        'e2e': {'value': e2e_value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 64,
+                'd2h_bytes_per_step': int(film_np.nbytes)},
+        'gpu_launches': int(launches),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line['cpu_baseline'] = cpu_baseline(scene)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

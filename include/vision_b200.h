@@ -1,0 +1,176 @@
+/*
+ * vision_b200 — C ABI of the B200 spectral path-tracing hot path.
+ *
+ * The reference renderer (FaithZL/Vision) reaches its path tracer through a
+ * C++ vtable ABI (src/sdk/vision.h:66-99, VisionRenderer: init_pipeline,
+ * init_scene, add_instance, build_accel, update_camera, compile, render,
+ * download_radiance) and through per-plugin DLLs built from the scene JSON
+ * (src/base/node.h:109-118).  This header is the drop-in boundary for that
+ * path: plain C, opaque handles, integer status codes, caller-owned buffers,
+ * no exceptions and no torch or CUDA types in the signatures (streams are
+ * passed as void*).
+ *
+ * Every entry point is thread-safe per handle: calls on one scene serialise
+ * on that scene's lock.
+ */
+#ifndef VISION_B200_H
+#define VISION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define VS_OK 0
+#define VS_E_INVALID 1     /* bad argument (null pointer, size mismatch) */
+#define VS_E_UNSUPPORTED 2 /* plugin type or option outside this library; message names it */
+#define VS_E_PARSE 3       /* malformed scene JSON */
+#define VS_E_CUDA 4        /* CUDA runtime error; message has the CUDA error string */
+#define VS_E_STATE 5       /* call out of order (e.g. render before build_accel) */
+#define VS_E_NO_DEVICE 6   /* the context was created without a GPU */
+#define VS_E_RANGE 7       /* size beyond a documented limit */
+
+/* Film precision for vs_render (the reference film is FP32, normal.cpp:87-101). */
+#define VS_FILM_FP32 0
+#define VS_FILM_FP64 1
+
+/* Film buffers for vs_film_download. */
+#define VS_FILM_LINEAR 0     /* FP32 running mean, float4 per pixel (rt_buffer) */
+#define VS_FILM_EXPOSED 1    /* 1 - exp(-linear * exposure), float4 per pixel */
+#define VS_FILM_SUM64 2      /* FP64 sums: double4 (r, g, b, samples) per pixel */
+
+typedef struct vs_context vs_context;
+typedef struct vs_scene vs_scene;
+
+/* Closest-hit record: reference TriangleHit{inst_id, prim_id, bary}. */
+typedef struct vs_hit {
+    uint32_t inst_id; /* 0xffffffff on a miss */
+    uint32_t prim_id; /* global primitive index in shape order */
+    float u, v;       /* barycentric weights of vertex 1 and vertex 2 */
+} vs_hit;
+
+typedef struct vs_scene_info {
+    uint32_t vertex_count;
+    uint32_t prim_count;
+    uint32_t instance_count;
+    uint32_t material_count;
+    uint32_t light_count;
+    uint32_t prim_alias_count;
+    uint32_t spd_floats;
+    uint32_t bvh_node_count;
+    uint32_t bvh_depth;
+    uint32_t width;
+    uint32_t height;
+    uint32_t spectrum_dim;
+    uint32_t max_depth;
+    uint32_t accel_built;
+} vs_scene_info;
+
+/* Library version: major * 10000 + minor * 100 + patch. */
+int vs_version(void);
+
+/* Creates a context on CUDA device `device`; device = -1 makes a host-only
+ * context that can parse, build and export scenes but not render. */
+int vs_context_create(int device, vs_context **out);
+void vs_context_destroy(vs_context *ctx);
+/* Message of the last failed call on this context (never NULL). */
+const char *vs_last_error(const vs_context *ctx);
+
+/* Scene from a vision_scene.json document (reference SceneDesc::from_json,
+ * src/core/scene_desc.cpp:55-61, plus JsonImporter, importers/json/importer.cpp:16-23).
+ * `table_cache` may name a file that caches the RGB->spectrum table (or be NULL). */
+int vs_scene_load_json(vs_context *ctx, const char *json, size_t len, const char *base_dir,
+                       const char *table_cache, vs_scene **out);
+void vs_scene_destroy(vs_scene *scene);
+
+/* Builds the compressed BVH8 and uploads the scene to the device
+ * (reference Geometry::build_accel, src/base/mgr/geometry.cpp:36-52;
+ * SDK VisionRenderer::build_accel, src/sdk/vision.h:66-80). */
+int vs_scene_build_accel(vs_scene *scene);
+
+/* Film resolution (reference RadianceCollector::update_resolution,
+ * src/base/sensor/radiance_collector.h:58-62). Resets the film. */
+int vs_set_resolution(vs_scene *scene, uint32_t width, uint32_t height);
+
+/* Camera-to-world 4x4 (column-major, 16 floats) and vertical field of view in
+ * degrees (reference VisionRenderer::update_camera, src/sdk/vision.cpp:139-160). */
+int vs_camera_set(vs_scene *scene, const float *c2w16, float fov_y_deg);
+
+int vs_scene_info_get(const vs_scene *scene, vs_scene_info *out);
+
+/* Copies one flattened scene array (VS_EXPORT_*) into dst; `bytes` must equal
+ * the array size, which vs_scene_export_size reports. */
+#define VS_EXPORT_POS 0         /* float[3] per vertex, world space */
+#define VS_EXPORT_NRM 1         /* float[3] per vertex, world space, unnormalised */
+#define VS_EXPORT_UV 2          /* float[2] per vertex */
+#define VS_EXPORT_IDX 3         /* uint32[3] per primitive */
+#define VS_EXPORT_PRIM_INST 4   /* uint32 per primitive */
+#define VS_EXPORT_INSTANCES 5   /* 16 bytes per instance: mat, light, first_prim, prim_count */
+#define VS_EXPORT_MATERIALS 6   /* 64 bytes per material */
+#define VS_EXPORT_LIGHTS 7      /* 64 bytes per area light */
+#define VS_EXPORT_PRIM_ALIAS 8  /* (float prob, uint32 alias) per entry */
+#define VS_EXPORT_PRIM_PMF 9    /* float per entry */
+#define VS_EXPORT_LIGHT_ALIAS 10
+#define VS_EXPORT_LIGHT_PMF 11
+#define VS_EXPORT_CAMERA 12     /* camera block, 112 bytes */
+#define VS_EXPORT_INTEGRATOR 13 /* integrator block, 48 bytes */
+#define VS_EXPORT_SPD 14        /* float */
+#define VS_EXPORT_MATERIAL_RGB 15 /* float[3] per material */
+#define VS_EXPORT_LIGHT_RGB 16  /* float[3] per light */
+#define VS_EXPORT_BVH_NODES 17  /* 80 bytes per node */
+#define VS_EXPORT_BVH_TRIS 18   /* float[12] per primitive in leaf order */
+int vs_scene_export_size(const vs_scene *scene, int what, size_t *bytes);
+int vs_scene_export(const vs_scene *scene, int what, void *dst, size_t bytes);
+
+/* Renders frames [frame_begin, frame_begin + frame_count), one sample per
+ * pixel per frame (reference PathTracingIntegrator::render, pt.cpp:90-99),
+ * accumulating into the FP32 running-mean film (and the FP64 sums when
+ * film_precision = VS_FILM_FP64).  frame_begin = 0 resets the film.
+ * `stream` is a cudaStream_t or NULL for the context's stream. Asynchronous. */
+int vs_render(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, int film_precision, void *stream);
+
+/* Waits for all work queued on the scene's stream. */
+int vs_synchronize(vs_scene *scene);
+
+/* Copies a film buffer (VS_FILM_*) to host memory (reference
+ * VisionRenderer::download_radiance, src/sdk/vision.cpp:132-137). */
+int vs_film_download(vs_scene *scene, void *dst, size_t bytes, int which);
+
+/* Seeded ray batches against the scene's BVH.  Rays are 8 floats each:
+ * origin xyz, unused, direction xyz, t_max; hits cover t in (0, t_max).
+ * `_device` variants take device pointers and run on `stream`; `_host`
+ * variants take host pointers and include the copies. */
+int vs_trace_closest_device(vs_scene *scene, const float *rays, uint32_t n, vs_hit *hits, float *t, void *stream);
+int vs_trace_closest_host(vs_scene *scene, const float *rays, uint32_t n, vs_hit *hits, float *t);
+int vs_trace_any_device(vs_scene *scene, const float *rays, uint32_t n, uint32_t *occluded, void *stream);
+int vs_trace_any_host(vs_scene *scene, const float *rays, uint32_t n, uint32_t *occluded);
+
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t vs_launch_count(void);
+
+/* CUDA-event timing of the kernels vs_render launches on this scene.
+ * vs_timing_enable(scene, 1) clears the record and starts timing;
+ * vs_timing_read waits for the recorded events and returns the summed
+ * megakernel and film-pass durations and the number of megakernel launches. */
+int vs_timing_enable(vs_scene *scene, int enable);
+int vs_timing_read(vs_scene *scene, double *render_ms, double *film_ms, uint32_t *render_launches);
+
+/* Instrumented render of frames [frame_begin, frame_begin + frame_count) that
+ * leaves the film untouched and returns traversal counters: out3[0] ray
+ * segments traced (closest + shadow), out3[1] BVH8 nodes visited, out3[2]
+ * triangle tests.  Synchronous; used to size the algorithmic bytes per path. */
+int vs_render_stats(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, uint64_t *out3);
+
+/* RGB -> sigmoid coefficients with the uplift table (reference
+ * RGBToSpectrumTable::decode_albedo / decode_unbound, hero.cpp:92-141).
+ * mode 0 = albedo (out[3] = luminance), 1 = unbound (out[3] = scale). */
+int vs_rgb_to_spectrum(vs_context *ctx, const char *table_cache, const float *rgb3, int mode, float *out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VISION_B200_H */

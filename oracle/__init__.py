@@ -1,0 +1,146 @@
+"""ORACLE — test infrastructure only.
+
+ctypes bridge to the CPU restatement in oracle/oracle.cpp.  Imported only by
+tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg, always
+as the checker and never as the thing measured or shipped.  The parity status
+of the oracle (what pins it, what is unpinned) is stated in oracle.cpp's
+header.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, '_build', 'liboracle.so')
+
+
+def build():
+    src = os.path.join(HERE, 'oracle.cpp')
+    if os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= os.path.getmtime(src):
+        return LIB_PATH
+    subprocess.run(['make', '-s', '-C', HERE], check=True)
+    return LIB_PATH
+
+
+class OracleSceneStruct(ctypes.Structure):
+    _fields_ = [('pos', ctypes.c_void_p), ('nrm', ctypes.c_void_p), ('uv', ctypes.c_void_p), ('idx', ctypes.c_void_p),
+                ('prim_inst', ctypes.c_void_p), ('vertex_count', ctypes.c_uint32), ('prim_count', ctypes.c_uint32),
+                ('instances', ctypes.c_void_p), ('instance_count', ctypes.c_uint32),
+                ('materials', ctypes.c_void_p), ('material_count', ctypes.c_uint32),
+                ('lights', ctypes.c_void_p), ('light_count', ctypes.c_uint32),
+                ('prim_alias', ctypes.c_void_p), ('prim_pmf', ctypes.c_void_p),
+                ('light_alias', ctypes.c_void_p), ('light_pmf', ctypes.c_void_p),
+                ('camera', ctypes.c_void_p), ('integrator', ctypes.c_void_p), ('spd', ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        U = ctypes.c_uint32
+        L.oracle_trace_closest.argtypes = [P, P, U, P, P]
+        L.oracle_trace_any.argtypes = [P, P, U, P]
+        L.oracle_paths.argtypes = [P, P, U, U, U, U, P]
+        L.oracle_render.argtypes = [P, U, U, U, P, P]
+        L.oracle_sampler_stream.argtypes = [U, U, U, U, U, U, U, P]
+        L.oracle_tea.argtypes = [U, U]
+        L.oracle_tea.restype = U
+        L.oracle_wavelengths.argtypes = [U, ctypes.c_float, P, P]
+        L.oracle_linear_srgb.argtypes = [U, P, P, P, P]
+        L.oracle_cie_y_integral.restype = ctypes.c_float
+        L.oracle_spd_eval.argtypes = [P, ctypes.c_int, ctypes.c_float]
+        L.oracle_spd_eval.restype = ctypes.c_float
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class OracleScene:
+    """The exported flat scene of a vision_b200.Scene, held alive for the oracle."""
+
+    def __init__(self, scene):
+        keys = ['pos', 'nrm', 'uv', 'idx', 'prim_inst', 'instances', 'materials', 'lights', 'prim_alias', 'prim_pmf',
+                'light_alias', 'light_pmf', 'camera', 'integrator', 'spd']
+        self.arr = {}
+        for k in keys:
+            a = scene.export(k)
+            if a.size == 0:
+                a = np.zeros(16, np.uint8)
+            self.arr[k] = np.ascontiguousarray(a)
+        info = scene.info()
+        self.width, self.height = info['width'], info['height']
+        a = self.arr
+        self.s = OracleSceneStruct(_p(a['pos']), _p(a['nrm']), _p(a['uv']), _p(a['idx']), _p(a['prim_inst']),
+                                   info['vertex_count'], info['prim_count'], _p(a['instances']), info['instance_count'],
+                                   _p(a['materials']), info['material_count'], _p(a['lights']), info['light_count'],
+                                   _p(a['prim_alias']), _p(a['prim_pmf']), _p(a['light_alias']), _p(a['light_pmf']),
+                                   _p(a['camera']), _p(a['integrator']), _p(a['spd']))
+
+    def trace_closest(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hits = np.zeros((n, 4), np.uint32)
+        t = np.zeros(n, np.float32)
+        lib().oracle_trace_closest(ctypes.byref(self.s), _p(rays), n, _p(hits), _p(t))
+        return hits, t
+
+    def trace_any(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32)
+        occ = np.zeros(rays.shape[0], np.uint32)
+        lib().oracle_trace_any(ctypes.byref(self.s), _p(rays), rays.shape[0], _p(occ))
+        return occ
+
+    def render(self, frame_begin, frame_count, threads=None, fp64=False):
+        threads = threads or os.cpu_count()
+        film = np.zeros((self.height, self.width, 4), np.float32)
+        f64 = np.zeros((self.height, self.width, 4), np.float64) if fp64 else None
+        lib().oracle_render(ctypes.byref(self.s), frame_begin, frame_count, threads, _p(film),
+                            _p(f64) if fp64 else None)
+        return (film, f64) if fp64 else film
+
+    def paths(self, pixels, frame_begin, frame_count, threads=None):
+        pixels = np.ascontiguousarray(pixels, np.uint32)
+        out = np.zeros((frame_count, pixels.size, 3), np.float32)
+        lib().oracle_paths(ctypes.byref(self.s), _p(pixels), pixels.size, frame_begin, frame_count,
+                           threads or os.cpu_count(), _p(out))
+        return out
+
+
+def sampler_stream(px, py, sample, dim, n, kind=0, seed=0):
+    out = np.zeros(n, np.float32)
+    lib().oracle_sampler_stream(px, py, sample, dim, kind, seed, n, _p(out))
+    return out
+
+
+def tea(a, b):
+    return lib().oracle_tea(a, b)
+
+
+def wavelengths(n, u):
+    lam = np.zeros(n, np.float32)
+    pdf = np.zeros(n, np.float32)
+    lib().oracle_wavelengths(n, ctypes.c_float(u), _p(lam), _p(pdf))
+    return lam, pdf
+
+
+def linear_srgb(lam, pdf, s):
+    lam = np.ascontiguousarray(lam, np.float32)
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    s = np.ascontiguousarray(s, np.float32)
+    rgb = np.zeros(3, np.float32)
+    lib().oracle_linear_srgb(lam.size, _p(lam), _p(pdf), _p(s), _p(rgb))
+    return rgb
+
+
+def cie_y_integral():
+    return lib().oracle_cie_y_integral()

@@ -1,0 +1,867 @@
+// ORACLE — test infrastructure only.  A scalar CPU restatement of the
+// reference's spectral path tracer (FaithZL/Vision), used by tests/, by
+// __graft_entry__.smoke() and by bench.py's cpu_baseline leg as the checker.
+// It is never part of the rendering product.
+//
+// Parity pinning: the reference cannot be built or run (its ocarina submodule
+// holds the DSL/OptiX backend and is empty; its host code is Windows-only), so
+// this oracle is pinned against the reference's own data tables (CIE/D65
+// spectra, metal IOR), against the golden vectors committed under
+// tests/golden/ (TEA/LCG streams, alias tables, wavelength samples derived
+// from the reference formulas) and, function by function, against the
+// reference source lines cited below.  Path-level image parity against a
+// reference binary is unpinned.
+//
+// The oracle reads the flattened scene exported by libvision_b200
+// (vs_scene_export) so that it traces exactly the same triangles, materials
+// and emitters; everything from the sampler to the film is computed here,
+// independently of the CUDA code, in FP32 like the reference, with an FP64
+// film option.  Compile with -ffp-contract=off: the watertight triangle test
+// must round exactly like the GPU's explicitly rounded version.
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../vision_b200/csrc/data/spectral_tables.inc"
+
+namespace oracle {
+
+struct V3 {
+    float x, y, z;
+};
+static inline V3 v3(float x, float y, float z) { return {x, y, z}; }
+static inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline V3 mul(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline V3 neg(V3 a) { return {-a.x, -a.y, -a.z}; }
+static inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+static inline float len(V3 a) { return std::sqrt(dot(a, a)); }
+static inline V3 normalize(V3 a) { return mul(a, 1.0f / std::sqrt(dot(a, a))); }
+static inline float at(V3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+static inline uint32_t fbits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+static inline float bitsf(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+
+// ----- exported scene layout (include/vision_b200.h, VS_EXPORT_*) -----------
+struct Material {
+    uint32_t type, flags, spd0, spd1;
+    float coef[4];
+    float p[8];
+};
+struct AreaLight {
+    uint32_t inst, first_prim, prim_count, alias_offset, two_sided, kind;
+    float scale, lum_power;
+    float coef[4];
+    float rgb_avg[4];
+};
+struct Instance {
+    uint32_t mat_id, light_id, first_prim, prim_count;
+};
+struct Alias {
+    float prob;
+    uint32_t alias;
+};
+struct Camera {
+    float c2w[4][4];
+    float tan_half_fov, screen_lo_x, screen_hi_y, screen_span_x, screen_span_y, filter_rx, filter_ry;
+    uint32_t width, height;
+    float exposure;
+    uint32_t pad0, pad1;
+};
+struct Integrator {
+    uint32_t max_depth, min_depth;
+    float rr_threshold;
+    uint32_t mis_mode, spectrum_dim, scatter_pdf_dim, sampler, seed, light_sampler, light_count, pad0, pad1;
+};
+
+}  // namespace oracle
+
+extern "C" {
+// Pointers into the exported arrays; counts in elements.
+struct oracle_scene {
+    const float *pos;
+    const float *nrm;
+    const float *uv;
+    const uint32_t *idx;
+    const uint32_t *prim_inst;
+    uint32_t vertex_count;
+    uint32_t prim_count;
+    const void *instances;
+    uint32_t instance_count;
+    const void *materials;
+    uint32_t material_count;
+    const void *lights;
+    uint32_t light_count;
+    const void *prim_alias;
+    const float *prim_pmf;
+    const void *light_alias;
+    const float *light_pmf;
+    const void *camera;
+    const void *integrator;
+    const float *spd;
+};
+}
+
+namespace oracle {
+
+constexpr uint32_t kInvalid = 0xffffffffu;
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kInvPi = 0.31830988618379067154f;
+constexpr float kOneMinusEps = 0x1.fffffep-1f;
+constexpr float kShadowEps = 0.0001f;
+
+// ----- spectral tables -------------------------------------------------------
+// SPD::create_cie_* downsample every 5th 1-nm sample: 94 entries, 360..825 nm
+// (src/base/color/spd.cpp:31-38,96-110); cie_y_integral sums 94 trapezoids of
+// 5 nm up to 830 nm (:14-23).
+struct Tables {
+    float x[94], y[94], z[94], d65[94];
+    float y_integral;
+    Tables() {
+        for (int i = 0; i < 94; ++i) {
+            x[i] = VS_CIE_X[5 * i];
+            y[i] = VS_CIE_Y[5 * i];
+            z[i] = VS_CIE_Z[5 * i];
+            d65[i] = VS_CIE_D65[5 * i];
+        }
+        float sum = 0.0f;
+        for (int i = 0; i < 94; ++i) sum += 0.5f * (VS_CIE_Y[5 * i] + VS_CIE_Y[5 * (i + 1)]);
+        y_integral = sum * 5.0f;
+    }
+};
+static const Tables &tables() {
+    static Tables t;
+    return t;
+}
+
+// SPD::eval (spd.cpp:67-76): spacing 471 / n, index clamped to n - 2.
+static float spd_eval(const float *f, int n, float lambda) {
+    float interval = 471.0f / static_cast<float>(n);
+    float t = (std::min(std::max(lambda, 360.0f), 830.0f) - 360.0f) / interval;
+    float sample_count = static_cast<float>(static_cast<uint32_t>((830.0f - 360.0f) / interval) + 1u);
+    uint32_t i = static_cast<uint32_t>(std::min(t, sample_count - 2.0f));
+    float fr = t - std::floor(t);
+    return f[i] + fr * (f[i + 1] - f[i]);
+}
+
+// RGBSigmoidPolynomial (hero.cpp:27-49).
+static float sigmoid_poly(const float *c, float l) {
+    float x = std::fma(std::fma(c[0], l, c[1]), l, c[2]);
+    if (std::isinf(x)) return x > 0.0f ? 1.0f : 0.0f;
+    return 0.5f * std::fma(x, 1.0f / std::sqrt(std::fma(x, x, 1.0f)), 1.0f);
+}
+
+static float planck(float lambda_nm, float T) {
+    const float c = 299792458.0f, h = 6.62606957e-34f, kb = 1.3806488e-23f;
+    float l = lambda_nm * 1e-9f;
+    float l2 = l * l;
+    float l5 = l2 * l2 * l;
+    return (2.0f * h * c * c) / (l5 * (std::exp((h * c) / (l * kb * T)) - 1.0f));
+}
+
+// ----- sampler (independent.cpp:24-42, util.h:13-33) --------------------------
+static uint32_t tea(uint32_t v0, uint32_t v1) {
+    uint32_t s0 = 0;
+    for (int n = 0; n < 4; ++n) {
+        s0 += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+    }
+    return v0;
+}
+
+struct Sampler {
+    uint32_t kind = 0;
+    uint32_t lcg = 0;
+    uint64_t pcg_state = 0, pcg_inc = 1;
+    void start(uint32_t px, uint32_t py, uint32_t sample, uint32_t dim, uint32_t k, uint32_t seed) {
+        kind = k;
+        uint32_t s = tea(tea(px, py), tea(sample, dim));
+        if (kind == 0) {
+            lcg = s;
+        } else {
+            // PCG32 (O'Neill): state advanced from 0, plus the hash, advanced again;
+            // 48-bit state with the seed as stream selector.
+            pcg_inc = (static_cast<uint64_t>(seed) << 1u) | 1u;
+            uint64_t st = 0u;
+            st = st * 6364136223846793005ull + pcg_inc;
+            st += s;
+            st = st * 6364136223846793005ull + pcg_inc;
+            pcg_state = st & 0xffffffffffffull;
+        }
+    }
+    float next() {
+        if (kind == 0) {
+            lcg = 1664525u * lcg + 1013904223u;
+            return static_cast<float>(lcg & 0x00ffffffu) * (1.0f / 16777216.0f);
+        }
+        uint64_t old = pcg_state;
+        pcg_state = (old * 6364136223846793005ull + pcg_inc) & 0xffffffffffffull;
+        uint32_t xs = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+        uint32_t rot = static_cast<uint32_t>(old >> 59u);
+        uint32_t r = (xs >> rot) | (xs << ((32u - rot) & 31u));
+        return static_cast<float>(r >> 8) * (1.0f / 16777216.0f);
+    }
+};
+
+// ----- wavelengths (hero.cpp:15-25,286-299) ----------------------------------
+struct Swl {
+    int n;
+    float lambda[8];
+    float pdf[8];
+};
+static Swl sample_wavelengths(int n, float u) {
+    Swl w;
+    w.n = n;
+    for (int i = 0; i < n; ++i) {
+        float offset = static_cast<float>(static_cast<uint32_t>(i) * (1.0f / n));
+        float up = u + offset;
+        up = up - std::floor(up);
+        float l = 538.0f - 138.888889f * std::atanh(0.85691062f - 1.82750197f * up);
+        w.lambda[i] = l;
+        float c = std::cosh(0.0072f * (l - 538.0f));
+        w.pdf[i] = 0.0039398042f / (c * c);
+    }
+    return w;
+}
+
+// HeroWavelengthSpectrum::cie_xyz / linear_srgb (hero.cpp:261-285; cie.h:414-421).
+static V3 linear_srgb(const float *s, const Swl &w) {
+    const Tables &T = tables();
+    double dummy = 0;
+    (void)dummy;
+    float X = 0, Y = 0, Z = 0;
+    int valid = 0;
+    for (int i = 0; i < w.n; ++i) {
+        float p = w.pdf[i];
+        valid += p > 0.0f;
+        auto sd = [&](float a) { return p == 0.0f ? 0.0f : a / p; };
+        X += sd(spd_eval(T.x, 94, w.lambda[i]) * s[i]);
+        Y += sd(spd_eval(T.y, 94, w.lambda[i]) * s[i]);
+        Z += sd(spd_eval(T.z, 94, w.lambda[i]) * s[i]);
+    }
+    float factor = 1.0f / (static_cast<float>(valid) * T.y_integral);
+    X *= factor; Y *= factor; Z *= factor;
+    return {3.240479f * X - 1.537150f * Y - 0.498535f * Z, -0.969256f * X + 1.875991f * Y + 0.041556f * Z,
+            0.055648f * X - 0.204043f * Y + 1.057311f * Z};
+}
+
+// ----- ray offset (Waechter & Binder, Ray Tracing Gems ch. 6) -----------------
+static float offset1(float p, float n) {
+    int of = static_cast<int>(256.0f * n);
+    int pi = static_cast<int>(fbits(p));
+    float pn = bitsf(static_cast<uint32_t>(pi + (p < 0.0f ? -of : of)));
+    return std::fabs(p) < 1.0f / 32.0f ? p + (1.0f / 65536.0f) * n : pn;
+}
+static V3 offset_ray_origin(V3 p, V3 n) { return {offset1(p.x, n.x), offset1(p.y, n.y), offset1(p.z, n.z)}; }
+
+// ----- geometry --------------------------------------------------------------
+struct Scene {
+    const oracle_scene *s;
+    const Instance *inst;
+    const Material *mat;
+    const AreaLight *lights;
+    const Alias *prim_alias;
+    const Alias *light_alias;
+    Camera cam;
+    Integrator ip;
+    // Binary BVH over primitives (median split), for scenes too large to brute force.
+    struct Node {
+        float lo[3], hi[3];
+        uint32_t left, right, first, count;
+    };
+    std::vector<Node> nodes;
+    std::vector<uint32_t> order;
+
+    V3 P(uint32_t v) const { return {s->pos[3 * v], s->pos[3 * v + 1], s->pos[3 * v + 2]}; }
+    V3 N(uint32_t v) const { return {s->nrm[3 * v], s->nrm[3 * v + 1], s->nrm[3 * v + 2]}; }
+
+    uint32_t build(uint32_t first, uint32_t count) {
+        uint32_t id = static_cast<uint32_t>(nodes.size());
+        nodes.push_back({});
+        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (uint32_t i = first; i < first + count; ++i) {
+            uint32_t p = order[i];
+            for (int k = 0; k < 3; ++k) {
+                V3 v = P(s->idx[3 * p + k]);
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = std::min(lo[a], at(v, a));
+                    hi[a] = std::max(hi[a], at(v, a));
+                }
+            }
+            for (int a = 0; a < 3; ++a) {
+                float c = 0.0f;
+                for (int k = 0; k < 3; ++k) c += at(P(s->idx[3 * p + k]), a);
+                clo[a] = std::min(clo[a], c);
+                chi[a] = std::max(chi[a], c);
+            }
+        }
+        std::memcpy(nodes[id].lo, lo, sizeof(lo));
+        std::memcpy(nodes[id].hi, hi, sizeof(hi));
+        if (count <= 4) {
+            nodes[id].first = first;
+            nodes[id].count = count;
+            nodes[id].left = nodes[id].right = 0;
+            return id;
+        }
+        int axis = 0;
+        for (int a = 1; a < 3; ++a)
+            if (chi[a] - clo[a] > chi[axis] - clo[axis]) axis = a;
+        uint32_t mid = first + count / 2;
+        std::nth_element(order.begin() + first, order.begin() + mid, order.begin() + first + count,
+                         [&](uint32_t a, uint32_t b) {
+                             float ca = 0.0f, cb = 0.0f;
+                             for (int k = 0; k < 3; ++k) {
+                                 ca += at(P(s->idx[3 * a + k]), axis);
+                                 cb += at(P(s->idx[3 * b + k]), axis);
+                             }
+                             return ca < cb || (ca == cb && a < b);
+                         });
+        uint32_t l = build(first, mid - first);
+        uint32_t r = build(mid, first + count - mid);
+        nodes[id].left = l;
+        nodes[id].right = r;
+        nodes[id].count = 0;
+        return id;
+    }
+
+    explicit Scene(const oracle_scene *sc) : s(sc) {
+        inst = static_cast<const Instance *>(sc->instances);
+        mat = static_cast<const Material *>(sc->materials);
+        lights = static_cast<const AreaLight *>(sc->lights);
+        prim_alias = static_cast<const Alias *>(sc->prim_alias);
+        light_alias = static_cast<const Alias *>(sc->light_alias);
+        std::memcpy(&cam, sc->camera, sizeof(Camera));
+        std::memcpy(&ip, sc->integrator, sizeof(Integrator));
+        order.resize(sc->prim_count);
+        for (uint32_t i = 0; i < sc->prim_count; ++i) order[i] = i;
+        nodes.reserve(sc->prim_count / 2 + 8);
+        build(0, sc->prim_count);
+    }
+};
+
+// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013), same operation
+// order and rounding as the GPU version.
+struct RayPre {
+    V3 o, d, inv;
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+static RayPre precompute(V3 o, V3 d) {
+    RayPre r;
+    r.o = o;
+    r.d = d;
+    const float tiny = 1e-30f;
+    auto inv1 = [&](float x) { return 1.0f / (std::fabs(x) > tiny ? x : std::copysign(tiny, x)); };
+    r.inv = {inv1(d.x), inv1(d.y), inv1(d.z)};
+    float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    if (at(d, kz) < 0.0f) std::swap(kx, ky);
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    float dz = at(d, kz);
+    r.sx = at(d, kx) / dz;
+    r.sy = at(d, ky) / dz;
+    r.sz = 1.0f / dz;
+    return r;
+}
+static bool tri_hit(const RayPre &r, V3 v0, V3 v1, V3 v2, float tmin, float tmax, float &t_out, float &u_out,
+                    float &v_out) {
+    float ax = at(v0, r.kx) - at(r.o, r.kx), ay = at(v0, r.ky) - at(r.o, r.ky), az = at(v0, r.kz) - at(r.o, r.kz);
+    float bx = at(v1, r.kx) - at(r.o, r.kx), by = at(v1, r.ky) - at(r.o, r.ky), bz = at(v1, r.kz) - at(r.o, r.kz);
+    float cx = at(v2, r.kx) - at(r.o, r.kx), cy = at(v2, r.ky) - at(r.o, r.ky), cz = at(v2, r.kz) - at(r.o, r.kz);
+    float Ax = ax - r.sx * az, Ay = ay - r.sy * az;
+    float Bx = bx - r.sx * bz, By = by - r.sy * bz;
+    float Cx = cx - r.sx * cz, Cy = cy - r.sy * cz;
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = static_cast<float>(static_cast<double>(Cx) * By - static_cast<double>(Cy) * Bx);
+        V = static_cast<float>(static_cast<double>(Ax) * Cy - static_cast<double>(Ay) * Cx);
+        W = static_cast<float>(static_cast<double>(Bx) * Ay - static_cast<double>(By) * Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = (U + V) + W;
+    if (det == 0.0f) return false;
+    float Az = r.sz * az, Bz = r.sz * bz, Cz = r.sz * cz;
+    float T = (U * Az + V * Bz) + W * Cz;
+    float t = T / det;
+    if (!(t > tmin && t < tmax)) return false;
+    t_out = t;
+    u_out = V / det;
+    v_out = W / det;
+    return true;
+}
+
+static bool box_hit(const RayPre &r, const float *lo, const float *hi, float tmax) {
+    float tn = 0.0f, tf = tmax;
+    for (int a = 0; a < 3; ++a) {
+        float t0 = (lo[a] - at(r.o, a)) * at(r.inv, a), t1 = (hi[a] - at(r.o, a)) * at(r.inv, a);
+        tn = std::max(tn, std::min(t0, t1));
+        tf = std::min(tf, std::max(t0, t1));
+    }
+    return tn <= tf * 1.000001f;
+}
+
+struct HitRec {
+    uint32_t prim = kInvalid;
+    float t = 0, u = 0, v = 0;
+};
+
+// Closest hit over t in (0, tmax); exact ties in t go to the lower primitive id.
+static HitRec closest(const Scene &sc, const RayPre &r, float tmax) {
+    HitRec best;
+    best.t = tmax;
+    uint32_t stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        const Scene::Node &n = sc.nodes[stack[--sp]];
+        if (!box_hit(r, n.lo, n.hi, best.t * 1.000001f)) continue;
+        if (n.count) {
+            for (uint32_t i = n.first; i < n.first + n.count; ++i) {
+                uint32_t p = sc.order[i];
+                float t, u, v;
+                float lim = best.prim == kInvalid ? tmax : best.t * 1.000001f;
+                if (tri_hit(r, sc.P(sc.s->idx[3 * p]), sc.P(sc.s->idx[3 * p + 1]), sc.P(sc.s->idx[3 * p + 2]), 0.0f, lim,
+                            t, u, v)) {
+                    if (t < best.t || (t == best.t && p < best.prim)) {
+                        best.prim = p; best.t = t; best.u = u; best.v = v;
+                    }
+                }
+            }
+        } else {
+            stack[sp++] = n.left;
+            stack[sp++] = n.right;
+        }
+    }
+    return best;
+}
+
+static bool any_hit(const Scene &sc, const RayPre &r, float tmax) {
+    uint32_t stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        const Scene::Node &n = sc.nodes[stack[--sp]];
+        if (!box_hit(r, n.lo, n.hi, tmax * 1.000001f)) continue;
+        if (n.count) {
+            for (uint32_t i = n.first; i < n.first + n.count; ++i) {
+                uint32_t p = sc.order[i];
+                float t, u, v;
+                if (tri_hit(r, sc.P(sc.s->idx[3 * p]), sc.P(sc.s->idx[3 * p + 1]), sc.P(sc.s->idx[3 * p + 2]), 0.0f, tmax,
+                            t, u, v))
+                    return true;
+            }
+        } else {
+            stack[sp++] = n.left;
+            stack[sp++] = n.right;
+        }
+    }
+    return false;
+}
+
+// ----- surface interaction (geometry.cpp:78-165, interaction.h:87-110) --------
+struct Frame {
+    V3 x, y, z;
+    V3 to_local(V3 v) const { return {dot(v, x), dot(v, y), dot(v, z)}; }
+    V3 to_world(V3 v) const { return add(add(mul(x, v.x), mul(y, v.y)), mul(z, v.z)); }
+};
+struct It {
+    V3 pos, ng, wo;
+    Frame sh;
+    float area;
+    uint32_t prim, mat, light;
+};
+static It interaction(const Scene &sc, uint32_t prim, float u, float v, V3 ray_dir) {
+    It it;
+    const uint32_t *ix = sc.s->idx + 3 * prim;
+    V3 p0 = sc.P(ix[0]), p1 = sc.P(ix[1]), p2 = sc.P(ix[2]);
+    float w = 1.0f - u - v;
+    it.pos = add(add(mul(p0, w), mul(p1, u)), mul(p2, v));
+    V3 dp02 = sub(p0, p2), dp12 = sub(p1, p2);
+    V3 ng_un = cross(dp02, dp12);
+    it.area = 0.5f * len(ng_un);
+    it.ng = normalize(ng_un);
+    const float *uv = sc.s->uv;
+    float u0 = uv[2 * ix[0]], v0 = uv[2 * ix[0] + 1], u1 = uv[2 * ix[1]], v1 = uv[2 * ix[1] + 1], u2 = uv[2 * ix[2]],
+          v2 = uv[2 * ix[2] + 1];
+    float du02 = u0 - u2, dv02 = v0 - v2, du12 = u1 - u2, dv12 = v1 - v2;
+    float det = du02 * dv12 - dv02 * du12;
+    V3 dp_dv = std::fabs(det) < 1e-8f ? normalize(sub(p2, p0)) : mul(sub(mul(dp12, du02), mul(dp02, du12)), 1.0f / det);
+    V3 n = add(add(mul(sc.N(ix[0]), w), mul(sc.N(ix[1]), u)), mul(sc.N(ix[2]), v));
+    V3 ns = (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) ? it.ng : normalize(n);
+    V3 x = normalize(cross(ns, dp_dv));
+    V3 y = normalize(cross(ns, x));
+    it.sh = {x, y, ns};
+    it.wo = normalize(neg(ray_dir));
+    it.prim = prim;
+    const Instance &in = sc.inst[sc.s->prim_inst[prim]];
+    it.mat = in.mat_id;
+    it.light = in.light_id;
+    return it;
+}
+
+// ----- emitters (area.cpp:91-149, light.cpp, lightsampler.cpp:159-267) --------
+static void emitter(const AreaLight &L, const Swl &w, float *out) {
+    const Tables &T = tables();
+    for (int i = 0; i < w.n; ++i) {
+        float l = w.lambda[i];
+        float e = L.kind == 0 ? sigmoid_poly(L.coef, l) * L.coef[3] * spd_eval(T.d65, 94, l) : planck(l, L.coef[0]) * L.coef[1];
+        out[i] = e * L.scale;
+    }
+}
+
+static uint32_t alias_sample(const Alias *tab, uint32_t size, float u, float *u_remap) {
+    u = u * static_cast<float>(size);
+    uint32_t idx = std::min(static_cast<uint32_t>(u), size - 1u);
+    u = std::min(u - static_cast<float>(idx), kOneMinusEps);
+    const Alias &e = tab[idx];
+    bool keep = u < e.prob;
+    if (u_remap) *u_remap = keep ? std::min(u / e.prob, kOneMinusEps) : std::min((1.0f - u) / (1.0f - e.prob), kOneMinusEps);
+    return keep ? idx : e.alias;
+}
+
+static float pdf_wi(float pdf_pos, V3 ng, V3 w) {
+    float c = std::fabs(dot(ng, normalize(w)));
+    float r = pdf_pos * dot(w, w) / c;
+    return (std::isinf(r) || std::isnan(r)) ? 0.0f : r;
+}
+
+static float light_pmf(const Scene &sc, uint32_t li) {
+    return sc.ip.light_sampler == 1 ? sc.s->light_pmf[li] : 1.0f / static_cast<float>(sc.ip.light_count);
+}
+
+struct LS {
+    float L[8];
+    float pdf;
+    V3 p;
+};
+static LS sample_light(const Scene &sc, const It &it, float ul, float ux, float uy, const Swl &w) {
+    LS ls;
+    uint32_t n = sc.ip.light_count;
+    uint32_t li;
+    float pmf_l;
+    if (sc.ip.light_sampler == 1) {
+        li = alias_sample(sc.light_alias, n, ul, nullptr);
+        pmf_l = sc.s->light_pmf[li];
+    } else {
+        li = static_cast<uint32_t>(std::min(ul * static_cast<float>(n), static_cast<float>(n) - 1.0f));
+        pmf_l = 1.0f / static_cast<float>(n);
+    }
+    const AreaLight &L = sc.lights[li];
+    float ur = ux;
+    uint32_t local = alias_sample(sc.prim_alias + L.alias_offset, L.prim_count, ux, &ur);
+    float pmf_p = sc.s->prim_pmf[L.alias_offset + local];
+    float su0 = std::sqrt(ur);
+    float bu = 1.0f - su0, bv = uy * su0;
+    uint32_t prim = L.first_prim + local;
+    const uint32_t *ix = sc.s->idx + 3 * prim;
+    V3 p0 = sc.P(ix[0]), p1 = sc.P(ix[1]), p2 = sc.P(ix[2]);
+    float bw = 1.0f - bu - bv;
+    V3 pos = add(add(mul(p0, bw), mul(p1, bu)), mul(p2, bv));
+    V3 ng_un = cross(sub(p0, p2), sub(p1, p2));
+    float area = 0.5f * len(ng_un);
+    V3 ng = normalize(ng_un);
+    float pdf_pos = (1.0f / area) * pmf_p;
+    V3 wr = sub(it.pos, pos);
+    bool front = dot(wr, ng) > 0.0f || L.two_sided;
+    if (front) emitter(L, w, ls.L);
+    else for (int i = 0; i < w.n; ++i) ls.L[i] = 0.0f;
+    ls.pdf = pdf_wi(pdf_pos, ng, wr) * pmf_l;
+    ls.p = offset_ray_origin(pos, dot(ng, wr) > 0.0f ? ng : neg(ng));
+    return ls;
+}
+
+// ----- BSDF (diffuse.cpp, bxdf.cpp:30-52, lobe.cpp:240-250, material.cpp:132-184) ---
+constexpr uint32_t kRefl = 2, kTrans = 4, kDiffRefl = 8 | 2, kUnset = 1;
+struct Eval {
+    float f[8];
+    float pdf;
+    uint32_t flags;
+};
+static Eval bsdf_eval(const Material &m, const float *kr, int n, const Frame &fr, V3 ng, V3 wo_w, V3 wi_w) {
+    Eval e;
+    V3 wo = fr.to_local(wo_w), wi = fr.to_local(wi_w);
+    if (m.type == 0) {
+        bool s = wo.z * wi.z > 0.0f;
+        float ac = std::fabs(wi.z);
+        for (int i = 0; i < n; ++i) e.f[i] = s ? kr[i] * (kInvPi * ac) : 0.0f;
+        e.pdf = s ? ac * kInvPi : 0.0f;
+        e.flags = kDiffRefl;
+    } else {
+        for (int i = 0; i < n; ++i) e.f[i] = 0.0f;
+        e.pdf = 1.0f;
+        e.flags = kUnset;
+    }
+    bool same = dot(wo_w, ng) * dot(wi_w, ng) > 0.0f;
+    bool trans = (e.flags & kTrans) != 0;
+    if (same == trans) e.pdf = 0.0f;
+    return e;
+}
+
+// ----- the path (pt.cpp:53-72; integrator.cpp:134-283) ------------------------
+static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) {
+    const Integrator &ip = sc.ip;
+    const Camera &cam = sc.cam;
+    int n = static_cast<int>(ip.spectrum_dim);
+    Sampler smp;
+    smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
+    Swl w = sample_wavelengths(n, smp.next());
+    smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
+    float fu = smp.next(), fv = smp.next();
+    float fx = -cam.filter_rx + fu * (cam.filter_rx - -cam.filter_rx);
+    float fy = -cam.filter_ry + fv * (cam.filter_ry - -cam.filter_ry);
+    smp.next(); smp.next(); smp.next();
+    float film_x = static_cast<float>(px) + 0.5f + fx, film_y = static_cast<float>(py) + 0.5f + fy;
+    float sx = cam.screen_lo_x + film_x / static_cast<float>(cam.width) * cam.screen_span_x;
+    float sy = cam.screen_hi_y - film_y / static_cast<float>(cam.height) * cam.screen_span_y;
+    V3 dc = normalize(v3(sx * cam.tan_half_fov, sy * cam.tan_half_fov, 1.0f));
+    const float(*m)[4] = cam.c2w;
+    V3 ro = {m[3][0], m[3][1], m[3][2]};
+    V3 rd = normalize(v3(m[0][0] * dc.x + m[1][0] * dc.y + m[2][0] * dc.z, m[0][1] * dc.x + m[1][1] * dc.y + m[2][1] * dc.z,
+                         m[0][2] * dc.x + m[1][2] * dc.y + m[2][2] * dc.z));
+    float scatter_pdf = 1e16f;
+    float thr[8];
+    for (int i = 0; i < n; ++i) thr[i] = 1.0f;
+    V3 ret = {0, 0, 0};
+    float eta_scale = 1.0f;
+    for (uint32_t b = 0; b < ip.max_depth; ++b) {
+        RayPre rp = precompute(ro, rd);
+        HitRec h = closest(sc, rp, FLT_MAX);
+        if (h.prim == kInvalid) break;
+        It it = interaction(sc, h.prim, h.u, h.v, rd);
+        if (it.light != kInvalid) {
+            const AreaLight &L = sc.lights[it.light];
+            float pmf_p = sc.s->prim_pmf[L.alias_offset + (it.prim - L.first_prim)];
+            float pdf_pos = (1.0f / it.area) * pmf_p;
+            V3 wv = sub(ro, it.pos);
+            bool front = dot(wv, it.ng) > 0.0f || L.two_sided;
+            float Le[8];
+            if (front) emitter(L, w, Le);
+            else for (int i = 0; i < n; ++i) Le[i] = 0.0f;
+            float lpdf = pdf_wi(pdf_pos, it.ng, wv) * light_pmf(sc, it.light);
+            float weight = scatter_pdf / (scatter_pdf + lpdf);
+            if (ip.mis_mode == 2) weight = 1.0f;
+            else if (ip.mis_mode == 1) weight = b == 0 ? weight : 0.0f;
+            float d[8];
+            for (int i = 0; i < n; ++i) d[i] = Le[i] * thr[i] * weight;
+            V3 c = linear_srgb(d, w);
+            ret = add(ret, c);
+        }
+        float ul = smp.next();
+        float ux = smp.next(), uy = smp.next();
+        LS ls = sample_light(sc, it, ul, ux, uy, w);
+        V3 dir = sub(ls.p, it.pos);
+        V3 nn = dot(it.ng, dir) > 0.0f ? it.ng : neg(it.ng);
+        bool occ = any_hit(sc, precompute(offset_ray_origin(it.pos, nn), dir), 1.0f - kShadowEps);
+        const Material &mt = sc.mat[it.mat];
+        float kr[8];
+        for (int i = 0; i < n; ++i) kr[i] = mt.type == 0 ? sigmoid_poly(mt.coef, w.lambda[i]) : 0.0f;
+        V3 wl = normalize(sub(ls.p, it.pos));
+        Eval se = bsdf_eval(mt, kr, n, it.sh, it.ng, it.wo, wl);
+        // BSDF sample (Lobe::sample, lobe.cpp:135-142).
+        Eval be;
+        V3 wi_s;
+        if (mt.type == 0) {
+            float u0 = smp.next(), u1 = smp.next();
+            float r = std::sqrt(u0), th = 2.0f * kPi * u1;
+            float dx = r * std::cos(th), dy = r * std::sin(th);
+            float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
+            V3 wo_l = it.sh.to_local(it.wo);
+            V3 wi_l = {dx, dy, wo_l.z < 0.0f ? -z : z};
+            wi_s = it.sh.to_world(wi_l);
+            be = bsdf_eval(mt, kr, n, it.sh, it.ng, it.wo, wi_s);
+        } else {
+            wi_s = it.wo;
+            for (int i = 0; i < n; ++i) be.f[i] = 0.0f;
+            be.pdf = 1.0f;
+            be.flags = kDiffRefl;
+        }
+        float wmis = ls.pdf / (ls.pdf + se.pdf);
+        if (ip.mis_mode == 1) wmis = 1.0f;
+        if (!occ && se.pdf > 0.0f && ls.pdf > 0.0f && ip.mis_mode != 2) {
+            float d[8];
+            for (int i = 0; i < n; ++i) d[i] = thr[i] * (ls.L[i] * se.f[i] * (wmis / ls.pdf));
+            ret = add(ret, linear_srgb(d, w));
+        }
+        float bs_eta = 1.0f;
+        eta_scale *= bs_eta * bs_eta;
+        float lum = thr[0];
+        for (int i = 1; i < n; ++i) lum = std::max(lum, thr[i]);
+        if (!(be.pdf > 0.0f) || lum == 0.0f) break;
+        for (int i = 0; i < n; ++i) thr[i] = thr[i] * (be.f[i] / be.pdf);
+        if (eta_scale * lum < ip.rr_threshold && b >= ip.min_depth) {
+            float q = std::min(0.95f, lum);
+            float rr = smp.next();
+            if (q < rr) break;
+            for (int i = 0; i < n; ++i) thr[i] = thr[i] * (1.0f / q);
+        }
+        bool zero = true;
+        for (int i = 0; i < n; ++i) zero = zero && thr[i] == 0.0f;
+        if (zero) break;
+        scatter_pdf = be.pdf;
+        V3 nb = dot(it.ng, wi_s) > 0.0f ? it.ng : neg(it.ng);
+        ro = offset_ray_origin(it.pos, nb);
+        rd = wi_s;
+    }
+    return ret;
+}
+
+}  // namespace oracle
+
+extern "C" {
+
+int oracle_version(void) { return 1; }
+
+// Closest hit for n rays (8 floats each: origin, unused, direction, tmax).
+// hits: 4 uint32 per ray (inst, prim, u bits, v bits); t: -1 on a miss.
+int oracle_trace_closest(const oracle_scene *s, const float *rays, uint32_t n, uint32_t *hits, float *t) {
+    oracle::Scene sc(s);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *r = rays + 8 * i;
+        oracle::RayPre rp = oracle::precompute({r[0], r[1], r[2]}, {r[4], r[5], r[6]});
+        oracle::HitRec h = oracle::closest(sc, rp, r[7]);
+        if (h.prim == oracle::kInvalid) {
+            hits[4 * i] = hits[4 * i + 1] = oracle::kInvalid;
+            hits[4 * i + 2] = hits[4 * i + 3] = 0;
+            t[i] = -1.0f;
+        } else {
+            hits[4 * i] = s->prim_inst[h.prim];
+            hits[4 * i + 1] = h.prim;
+            hits[4 * i + 2] = oracle::fbits(h.u);
+            hits[4 * i + 3] = oracle::fbits(h.v);
+            t[i] = h.t;
+        }
+    }
+    return 0;
+}
+
+int oracle_trace_any(const oracle_scene *s, const float *rays, uint32_t n, uint32_t *occ) {
+    oracle::Scene sc(s);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *r = rays + 8 * i;
+        occ[i] = oracle::any_hit(sc, oracle::precompute({r[0], r[1], r[2]}, {r[4], r[5], r[6]}), r[7]) ? 1u : 0u;
+    }
+    return 0;
+}
+
+// Per-path radiance of the listed pixels for frames [frame_begin, frame_begin+frame_count):
+// out[(f * npix_list + k) * 3 + c].
+int oracle_paths(const oracle_scene *s, const uint32_t *pixels, uint32_t npix_list, uint32_t frame_begin,
+                 uint32_t frame_count, uint32_t threads, float *out) {
+    oracle::Scene sc(s);
+    uint64_t total = static_cast<uint64_t>(npix_list) * frame_count;
+    std::atomic<uint64_t> next{0};
+    auto work = [&]() {
+        while (true) {
+            uint64_t j = next.fetch_add(64);
+            if (j >= total) break;
+            uint64_t e = std::min<uint64_t>(total, j + 64);
+            for (uint64_t q = j; q < e; ++q) {
+                uint32_t f = static_cast<uint32_t>(q / npix_list), k = static_cast<uint32_t>(q % npix_list);
+                uint32_t pix = pixels[k];
+                oracle::V3 L = oracle::trace_path(sc, pix % sc.cam.width, pix / sc.cam.width, frame_begin + f);
+                out[3 * q] = L.x;
+                out[3 * q + 1] = L.y;
+                out[3 * q + 2] = L.z;
+            }
+        }
+    };
+    if (threads <= 1) {
+        work();
+    } else {
+        std::vector<std::thread> th;
+        for (uint32_t i = 0; i < threads; ++i) th.emplace_back(work);
+        for (auto &x : th) x.join();
+    }
+    return 0;
+}
+
+// Full-frame render with the reference film semantics: FP32 running mean of
+// zero_if_nan_inf(L) (normal.cpp:87-101) into film32 (4 floats per pixel) and,
+// when film64 is non-null, FP64 sums (r, g, b, count) per pixel.
+int oracle_render(const oracle_scene *s, uint32_t frame_begin, uint32_t frame_count, uint32_t threads, float *film32,
+                  double *film64) {
+    oracle::Scene sc(s);
+    uint32_t npix = sc.cam.width * sc.cam.height;
+    std::atomic<uint32_t> next{0};
+    auto work = [&]() {
+        while (true) {
+            uint32_t p0 = next.fetch_add(16);
+            if (p0 >= npix) break;
+            for (uint32_t p = p0; p < std::min(npix, p0 + 16); ++p) {
+                float *acc = film32 + 4 * p;
+                if (frame_begin == 0) acc[0] = acc[1] = acc[2] = acc[3] = 0.0f;
+                double *a64 = film64 ? film64 + 4 * p : nullptr;
+                if (a64 && frame_begin == 0) a64[0] = a64[1] = a64[2] = a64[3] = 0.0;
+                for (uint32_t f = frame_begin; f < frame_begin + frame_count; ++f) {
+                    oracle::V3 L = oracle::trace_path(sc, p % sc.cam.width, p / sc.cam.width, f);
+                    float v[4] = {L.x, L.y, L.z, 1.0f};
+                    bool bad = false;
+                    for (int c = 0; c < 3; ++c) bad = bad || std::isnan(v[c]) || std::isinf(v[c]);
+                    if (bad) v[0] = v[1] = v[2] = v[3] = 0.0f;
+                    float a = 1.0f / static_cast<float>(f + 1u);
+                    for (int c = 0; c < 4; ++c) acc[c] = acc[c] + a * (v[c] - acc[c]);
+                    if (a64) {
+                        for (int c = 0; c < 3; ++c) a64[c] += bad ? 0.0 : v[c];
+                        a64[3] += 1.0;
+                    }
+                }
+            }
+        }
+    };
+    if (threads <= 1) {
+        work();
+    } else {
+        std::vector<std::thread> th;
+        for (uint32_t i = 0; i < threads; ++i) th.emplace_back(work);
+        for (auto &x : th) x.join();
+    }
+    return 0;
+}
+
+// TEA/LCG stream of the independent sampler, for golden-vector checks.
+void oracle_sampler_stream(uint32_t px, uint32_t py, uint32_t sample, uint32_t dim, uint32_t kind, uint32_t seed,
+                           uint32_t n, float *out) {
+    oracle::Sampler s;
+    s.start(px, py, sample, dim, kind, seed);
+    for (uint32_t i = 0; i < n; ++i) out[i] = s.next();
+}
+
+uint32_t oracle_tea(uint32_t a, uint32_t b) { return oracle::tea(a, b); }
+
+// Hero wavelengths and pdfs of one uniform sample.
+void oracle_wavelengths(uint32_t n, float u, float *lambda, float *pdf) {
+    oracle::Swl w = oracle::sample_wavelengths(static_cast<int>(n), u);
+    for (uint32_t i = 0; i < n; ++i) {
+        lambda[i] = w.lambda[i];
+        pdf[i] = w.pdf[i];
+    }
+}
+
+// Linear sRGB of a sampled spectrum.
+void oracle_linear_srgb(uint32_t n, const float *lambda, const float *pdf, const float *s, float *rgb) {
+    oracle::Swl w;
+    w.n = static_cast<int>(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        w.lambda[i] = lambda[i];
+        w.pdf[i] = pdf[i];
+    }
+    oracle::V3 c = oracle::linear_srgb(s, w);
+    rgb[0] = c.x; rgb[1] = c.y; rgb[2] = c.z;
+}
+
+float oracle_cie_y_integral(void) { return oracle::tables().y_integral; }
+
+float oracle_spd_eval(const float *f, int n, float lambda) { return oracle::spd_eval(f, n, lambda); }
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+"""Scene-layer semantics of the C-ABI host side (no GPU)."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from vision_b200 import scenes
+
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+
+
+def test_box_room_counts(vb, host_ctx):
+    s = vb.Scene(host_ctx, scenes.box_room()).build_accel()
+    i = s.info()
+    assert i['prim_count'] == 5 * 2 + 2 * 12 + 2
+    assert i['light_count'] == 1
+    assert i['spectrum_dim'] == 4 and i['max_depth'] == 8
+    assert (i['width'], i['height']) == (256, 256)
+
+
+def test_quad_matches_reference_layout(vb, host_ctx):
+    # Quad::init (quad.cpp:21-50): P = (w,0,h),(w,0,-h),(-w,0,h),(-w,0,-h); tris (0,1,2),(2,1,3).
+    sc = scenes.box_room(width=4, height=4)
+    s = vb.Scene(host_ctx, sc)
+    pos = s.export('pos', np.float32).reshape(-1, 3)
+    idx = s.export('idx', np.uint32).reshape(-1, 3)
+    np.testing.assert_array_equal(pos[:4], [[0.5, 0, 0.5], [0.5, 0, -0.5], [-0.5, 0, 0.5], [-0.5, 0, -0.5]])
+    np.testing.assert_array_equal(idx[:2], [[0, 1, 2], [2, 1, 3]])
+    # Geometric normal of the floor points up (+y), into the room.
+    p = pos[idx[0]]
+    ng = np.cross(p[0] - p[2], p[1] - p[2])
+    assert ng[1] > 0 and abs(ng[0]) < 1e-6 and abs(ng[2]) < 1e-6
+
+
+def test_walls_face_into_the_room(vb, host_ctx):
+    s = vb.Scene(host_ctx, scenes.box_room(width=4, height=4))
+    pos = s.export('pos', np.float32).reshape(-1, 3)
+    idx = s.export('idx', np.uint32).reshape(-1, 3)
+    center = np.array([0, 0.5, 0], np.float32)
+    for t in range(10):  # the five wall quads
+        p = pos[idx[t]]
+        ng = np.cross(p[0] - p[2], p[1] - p[2])
+        assert np.dot(ng, center - p.mean(0)) > 0, t
+    # The light quad faces down.
+    p = pos[idx[-1]]
+    assert np.cross(p[0] - p[2], p[1] - p[2])[1] < 0
+
+
+def test_cube_matches_reference_sizes(vb, host_ctx):
+    s = vb.Scene(host_ctx, scenes.box_room(width=4, height=4))
+    pos = s.export('pos', np.float32).reshape(-1, 3)
+    idx = s.export('idx', np.uint32).reshape(-1, 3)
+    tall = pos[np.unique(idx[10:22])]
+    assert abs(tall[:, 1].max() - 0.6) < 1e-5 and abs(tall[:, 1].min()) < 1e-5
+    # Rotated 15 degrees about y: edge length along the rotated x axis stays 0.3.
+    e = np.linalg.norm(tall[None] - tall[:, None], axis=-1)
+    assert np.any(np.isclose(e, 0.3, atol=1e-5))
+
+
+def test_camera_look_at(vb, host_ctx):
+    s = vb.Scene(host_ctx, scenes.box_room(width=4, height=4))
+    cam = s.export('camera', np.float32)
+    c2w = cam[:16].reshape(4, 4)  # column-major: c2w[c][r]
+    np.testing.assert_allclose(c2w[3, :3], [0, 0.5, 1.85], atol=1e-6)
+    fwd = c2w[2, :3]
+    np.testing.assert_allclose(fwd, [0, 0, -1], atol=1e-6)
+    assert abs(cam[16] - math.tan(math.radians(20))) < 1e-6
+
+
+def test_rgb_light_is_normalised(vb, host_ctx):
+    # Light::Light + NumberArray::normalize: [17,17,17] -> colour 1, scale 17.
+    s = vb.Scene(host_ctx, scenes.box_room(width=4, height=4, rgb_light=True))
+    L = s.export('lights', np.float32).reshape(-1, 16)
+    Lu = L.view(np.uint32)
+    assert Lu[0, 5] == 0  # RGB emitter
+    assert L[0, 6] == np.float32(17.0)
+    np.testing.assert_array_equal(s.export('light_rgb', np.float32), [1, 1, 1])
+    # decode_unbound of (1,1,1): grey -> c = 0, scale 2.
+    np.testing.assert_array_equal(L[0, 8:12], [0, 0, 0, 2])
+
+
+def test_alias_tables_match_reference_algorithm(vb, host_ctx):
+    # An emissive inline mesh with uneven triangle areas; its per-primitive
+    # alias table must equal the reference algorithm (golden restatement).
+    rng = np.random.default_rng(3)
+    n = 17
+    P, I = [], []
+    for t in range(n):
+        base = rng.random(3) * 0.5
+        a = 0.01 + 0.3 * rng.random()
+        P += list(base) + list(base + [a, 0, 0]) + list(base + [0, 0, a])
+        I += [3 * t, 3 * t + 2, 3 * t + 1]
+    sc = scenes.box_room(width=4, height=4)
+    sc['shapes'].append({'type': 'mesh', 'name': 'emitter', 'param': {
+        'positions': P, 'indices': I, 'material': 'Light',
+        'emission': {'type': 'area', 'param': {'color': [1, 1, 1], 'scale': 1.0}}}})
+    s = vb.Scene(host_ctx, sc)
+    L = s.export('lights', np.uint32).reshape(-1, 16)
+    assert L.shape[0] == 2
+    off, cnt = L[1, 3], L[1, 2]
+    tab = s.export('prim_alias', np.uint8).view([('prob', np.float32), ('alias', np.uint32)])[off:off + cnt]
+    pmf = s.export('prim_pmf', np.float32)[off:off + cnt]
+    pos = s.export('pos', np.float32).reshape(-1, 3)
+    idx = s.export('idx', np.uint32).reshape(-1, 3)[L[1, 1]:L[1, 1] + cnt]
+    areas = []
+    for t in idx:
+        p = pos[t]
+        areas.append(np.float32(0.5) * np.float32(np.linalg.norm(np.cross(p[0] - p[2], p[1] - p[2]).astype(np.float32))))
+    # Reference Vose construction (alias.h:86-122), restated.
+    w = [float(a) for a in areas]
+    ratio = len(w) / sum(np.float64(x) for x in w)
+    table = [[float(np.float32(x * ratio)), i] for i, x in enumerate(w)]
+    over = [i for i, t in enumerate(table) if t[0] > 1.0]
+    under = [i for i, t in enumerate(table) if not t[0] > 1.0]
+    while over and under:
+        o, u = over.pop(), under.pop()
+        table[o][0] = float(np.float32(np.float32(table[o][0]) - (np.float32(1.0) - np.float32(table[u][0]))))
+        table[u][1] = o
+        if table[o][0] > 1.0:
+            over.append(o)
+        elif table[o][0] < 1.0:
+            under.append(o)
+    for i in over + under:
+        table[i] = [1.0, i]
+    np.testing.assert_allclose(tab['prob'], [t[0] for t in table], rtol=1e-6, atol=1e-6)
+    np.testing.assert_array_equal(tab['alias'], [t[1] for t in table])
+    np.testing.assert_allclose(pmf, np.array(w) / np.sum(w), rtol=1e-5)
+
+
+def test_golden_alias_tables(vb, host_ctx):
+    for c in json.load(open(os.path.join(G, 'alias.json'))):
+        # Build through the library with an emissive mesh whose triangle areas
+        # are the golden weights.
+        P, I = [], []
+        for t, wgt in enumerate(c['weights']):
+            a = math.sqrt(2.0 * wgt)
+            P += [0, 0, 3 * t, a, 0, 3 * t, 0, 0, 3 * t + a]
+            I += [3 * t, 3 * t + 2, 3 * t + 1]
+        sc = scenes.box_room(width=4, height=4)
+        sc['shapes'].append({'type': 'mesh', 'name': 'e', 'param': {
+            'positions': P, 'indices': I, 'material': 'Light',
+            'emission': {'type': 'area', 'param': {'color': [1, 1, 1]}}}})
+        s = vb.Scene(host_ctx, sc)
+        L = s.export('lights', np.uint32).reshape(-1, 16)
+        off, cnt = L[1, 3], L[1, 2]
+        pmf = s.export('prim_pmf', np.float32)[off:off + cnt]
+        np.testing.assert_allclose(pmf, c['pmf'], rtol=1e-4)
+
+
+def test_unsupported_light_in_light_sampler(vb, host_ctx):
+    sc = scenes.box_room(width=4, height=4)
+    sc['light_sampler']['param']['lights'] = [{'type': 'point', 'param': {}}]
+    with pytest.raises(vb.UnsupportedError):
+        vb.Scene(host_ctx, sc)

@@ -1,0 +1,253 @@
+"""vision_b200 — B200-native spectral path-tracing hot path of FaithZL/Vision.
+
+Python mirror of the reference's render entry (the SDK's VisionRenderer,
+src/sdk/vision.h:66-99, and the fixed pipeline's prepare -> compile -> render
+loop, src/pipelines/fixed/pipeline.cpp:9-44) over the C ABI of
+libvision_b200.so (include/vision_b200.h).  There is no CPU fallback: if the
+shared library is missing the import fails.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libvision_b200.so')
+TABLE_CACHE = os.path.join(HERE, 'data', 'srgb2spec_64.bin')
+
+VS_OK = 0
+VS_E_INVALID = 1
+VS_E_UNSUPPORTED = 2
+VS_E_PARSE = 3
+VS_E_CUDA = 4
+VS_E_STATE = 5
+VS_E_NO_DEVICE = 6
+VS_E_RANGE = 7
+
+FILM_FP32 = 0
+FILM_FP64 = 1
+FILM_LINEAR = 0
+FILM_EXPOSED = 1
+FILM_SUM64 = 2
+
+EXPORT = dict(pos=0, nrm=1, uv=2, idx=3, prim_inst=4, instances=5, materials=6, lights=7, prim_alias=8,
+              prim_pmf=9, light_alias=10, light_pmf=11, camera=12, integrator=13, spd=14, material_rgb=15,
+              light_rgb=16, bvh_nodes=17, bvh_tris=18)
+
+
+class VisionError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__('%s (status %d)' % (message, code))
+        self.code = code
+
+
+class UnsupportedError(VisionError):
+    pass
+
+
+class HitStruct(ctypes.Structure):
+    _fields_ = [('inst_id', ctypes.c_uint32), ('prim_id', ctypes.c_uint32), ('u', ctypes.c_float), ('v', ctypes.c_float)]
+
+
+class SceneInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        'vertex_count', 'prim_count', 'instance_count', 'material_count', 'light_count', 'prim_alias_count',
+        'spd_floats', 'bvh_node_count', 'bvh_depth', 'width', 'height', 'spectrum_dim', 'max_depth', 'accel_built')]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError('libvision_b200.so not built: run `python vision_b200/build.py` (%s missing)' % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    U32 = ctypes.c_uint32
+    sig = {
+        'vs_version': ([], ctypes.c_int),
+        'vs_context_create': ([ctypes.c_int, ctypes.POINTER(P)], ctypes.c_int),
+        'vs_context_destroy': ([P], None),
+        'vs_last_error': ([P], ctypes.c_char_p),
+        'vs_scene_load_json': ([P, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_char_p,
+                                ctypes.POINTER(P)], ctypes.c_int),
+        'vs_scene_destroy': ([P], None),
+        'vs_scene_build_accel': ([P], ctypes.c_int),
+        'vs_set_resolution': ([P, U32, U32], ctypes.c_int),
+        'vs_camera_set': ([P, P, ctypes.c_float], ctypes.c_int),
+        'vs_scene_info_get': ([P, ctypes.POINTER(SceneInfo)], ctypes.c_int),
+        'vs_scene_export_size': ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+        'vs_scene_export': ([P, ctypes.c_int, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_render': ([P, U32, U32, ctypes.c_int, P], ctypes.c_int),
+        'vs_synchronize': ([P], ctypes.c_int),
+        'vs_film_download': ([P, P, ctypes.c_size_t, ctypes.c_int], ctypes.c_int),
+        'vs_trace_closest_device': ([P, P, U32, P, P, P], ctypes.c_int),
+        'vs_trace_closest_host': ([P, P, U32, P, P], ctypes.c_int),
+        'vs_trace_any_device': ([P, P, U32, P, P], ctypes.c_int),
+        'vs_trace_any_host': ([P, P, U32, P], ctypes.c_int),
+        'vs_rgb_to_spectrum': ([P, ctypes.c_char_p, P, ctypes.c_int, P], ctypes.c_int),
+        'vs_launch_count': ([], ctypes.c_uint64),
+        'vs_render_stats': ([P, U32, U32, P], ctypes.c_int),
+        'vs_timing_enable': ([P, ctypes.c_int], ctypes.c_int),
+        'vs_timing_read': ([P, P, P, P], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+# Symbols declared in include/vision_b200.h (checked by the CPU tests).
+ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', 'vs_last_error', 'vs_scene_load_json',
+                      'vs_scene_destroy', 'vs_scene_build_accel', 'vs_set_resolution', 'vs_camera_set',
+                      'vs_scene_info_get', 'vs_scene_export_size', 'vs_scene_export', 'vs_render', 'vs_synchronize',
+                      'vs_film_download', 'vs_trace_closest_device', 'vs_trace_closest_host', 'vs_trace_any_device',
+                      'vs_trace_any_host', 'vs_rgb_to_spectrum', 'vs_launch_count', 'vs_render_stats', 'vs_timing_enable',
+                      'vs_timing_read'])
+
+
+def launch_count():
+    """Kernels launched by libvision_b200 since it was loaded."""
+    return int(lib.vs_launch_count())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Context:
+    """CUDA device context (device=-1: host only, for parsing and export)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        rc = lib.vs_context_create(device, ctypes.byref(h))
+        if rc != VS_OK:
+            raise VisionError(rc, 'vs_context_create(%d) failed' % device)
+        self.handle = h
+        self.device = device
+
+    def check(self, rc, what):
+        if rc != VS_OK:
+            msg = '%s: %s' % (what, lib.vs_last_error(self.handle).decode())
+            raise (UnsupportedError if rc == VS_E_UNSUPPORTED else VisionError)(rc, msg)
+
+    def rgb_to_spectrum(self, rgb, mode=0):
+        out = np.zeros(4, np.float32)
+        self.check(lib.vs_rgb_to_spectrum(self.handle, TABLE_CACHE.encode(), _ptr(np.asarray(rgb, np.float32)),
+                                          mode, _ptr(out)), 'rgb_to_spectrum')
+        return out
+
+    def close(self):
+        if self.handle:
+            lib.vs_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """A loaded vision_scene.json.  Mirrors Pipeline::prepare/render and the SDK
+    calls build_accel / update_camera / render / download_radiance."""
+
+    def __init__(self, ctx, scene, base_dir='.'):
+        os.makedirs(os.path.dirname(TABLE_CACHE), exist_ok=True)
+        self.ctx = ctx
+        text = scene if isinstance(scene, str) else json.dumps(scene)
+        data = text.encode()
+        h = ctypes.c_void_p()
+        ctx.check(lib.vs_scene_load_json(ctx.handle, data, len(data), base_dir.encode(), TABLE_CACHE.encode(),
+                                         ctypes.byref(h)), 'load scene')
+        self.handle = h
+        self.frames = 0
+
+    def build_accel(self):
+        self.ctx.check(lib.vs_scene_build_accel(self.handle), 'build_accel')
+        return self
+
+    def info(self):
+        i = SceneInfo()
+        self.ctx.check(lib.vs_scene_info_get(self.handle, ctypes.byref(i)), 'scene info')
+        return {n: getattr(i, n) for n, _ in SceneInfo._fields_}
+
+    def export(self, what, dtype=np.uint8):
+        key = EXPORT[what]
+        n = ctypes.c_size_t()
+        self.ctx.check(lib.vs_scene_export_size(self.handle, key, ctypes.byref(n)), 'export size')
+        buf = np.zeros(max(n.value, 1), np.uint8)
+        self.ctx.check(lib.vs_scene_export(self.handle, key, _ptr(buf), n.value), 'export')
+        return buf[:n.value].view(dtype)
+
+    def set_resolution(self, w, h):
+        self.ctx.check(lib.vs_set_resolution(self.handle, w, h), 'set_resolution')
+        self.frames = 0
+
+    def render(self, frame_begin, frame_count, fp64=False, stream=None):
+        self.ctx.check(lib.vs_render(self.handle, frame_begin, frame_count, FILM_FP64 if fp64 else FILM_FP32,
+                                     ctypes.c_void_p(stream) if stream else None), 'render')
+        self.frames = frame_begin + frame_count
+
+    def synchronize(self):
+        self.ctx.check(lib.vs_synchronize(self.handle), 'synchronize')
+
+    def film(self, which=FILM_LINEAR):
+        i = self.info()
+        npix = i['width'] * i['height']
+        if which == FILM_SUM64:
+            out = np.zeros((i['height'], i['width'], 4), np.float64)
+        else:
+            out = np.zeros((i['height'], i['width'], 4), np.float32)
+        self.ctx.check(lib.vs_film_download(self.handle, _ptr(out), out.nbytes, which), 'film download')
+        return out
+
+    def trace_closest(self, rays):
+        """rays: (n, 8) float32 host array -> (hits (n, 4) uint32 [inst, prim, u bits, v bits], t (n,))."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hits = np.zeros((n, 4), np.uint32)
+        t = np.zeros(n, np.float32)
+        self.ctx.check(lib.vs_trace_closest_host(self.handle, _ptr(rays), n, _ptr(hits), _ptr(t)), 'trace_closest')
+        return hits, t
+
+    def trace_any(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32)
+        occ = np.zeros(rays.shape[0], np.uint32)
+        self.ctx.check(lib.vs_trace_any_host(self.handle, _ptr(rays), rays.shape[0], _ptr(occ)), 'trace_any')
+        return occ
+
+    def trace_closest_device(self, rays_ptr, n, hits_ptr, t_ptr, stream=None):
+        self.ctx.check(lib.vs_trace_closest_device(self.handle, ctypes.c_void_p(rays_ptr), n, ctypes.c_void_p(hits_ptr),
+                                                   ctypes.c_void_p(t_ptr), ctypes.c_void_p(stream) if stream else None),
+                       'trace_closest_device')
+
+    def timing_enable(self, on=True):
+        self.ctx.check(lib.vs_timing_enable(self.handle, 1 if on else 0), 'timing_enable')
+
+    def timing_read(self):
+        """(megakernel ms, film ms, megakernel launches) since timing_enable."""
+        r = ctypes.c_double()
+        f = ctypes.c_double()
+        n = ctypes.c_uint32()
+        self.ctx.check(lib.vs_timing_read(self.handle, ctypes.byref(r), ctypes.byref(f), ctypes.byref(n)), 'timing_read')
+        return r.value, f.value, n.value
+
+    def render_stats(self, frame_begin, frame_count):
+        """Traversal counters of an instrumented render: (segments, nodes, tris)."""
+        out = np.zeros(3, np.uint64)
+        self.ctx.check(lib.vs_render_stats(self.handle, frame_begin, frame_count, _ptr(out)), 'render_stats')
+        return tuple(int(x) for x in out)
+
+    def close(self):
+        if self.handle:
+            lib.vs_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,324 @@
+// Compressed 8-wide BVH builder.
+//
+// The reference hands its triangles to OptiX (Geometry::build_accel,
+// src/base/mgr/geometry.cpp:36-52); B200 has no RT-core path here, so the
+// acceleration structure is built on the host: a binned-SAH binary BVH with
+// leaves of at most three triangles is collapsed into 8-wide nodes whose child
+// boxes are quantised to 8 bits per plane against a per-node power-of-two grid
+// (80-byte nodes, after Ylitie, Karras and Laine, "Efficient Incoherent Ray
+// Traversal on GPUs Through Compressed Wide BVHs", HPG 2017).  Child slots are
+// ordered by direction so that traversal visits children roughly front to back
+// by flipping slot bits with the ray octant.
+#include "vs_host.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <thread>
+
+namespace vs {
+
+namespace {
+
+struct Box {
+    f3 lo{FLT_MAX, FLT_MAX, FLT_MAX};
+    f3 hi{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    void grow(f3 p) { lo = vmin(lo, p); hi = vmax(hi, p); }
+    void grow(const Box &b) { lo = vmin(lo, b.lo); hi = vmax(hi, b.hi); }
+    float area() const {
+        f3 d = hi - lo;
+        if (d.x < 0) return 0.0f;
+        return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
+    }
+    f3 center() const { return (lo + hi) * 0.5f; }
+};
+
+struct Node2 {
+    Box box;
+    uint32_t left = 0, right = 0;  // children (internal) or first/count (leaf)
+    uint32_t first = 0, count = 0;
+    bool leaf = false;
+};
+
+constexpr int kBins = 32;
+constexpr uint32_t kMaxLeaf = 3;
+
+struct Builder2 {
+    const std::vector<Box> &boxes;
+    const std::vector<f3> &cent;
+    std::vector<uint32_t> &order;
+    std::vector<Node2> nodes;
+
+    uint32_t build(uint32_t first, uint32_t count) {
+        uint32_t id = static_cast<uint32_t>(nodes.size());
+        nodes.emplace_back();
+        Box bb, cb;
+        for (uint32_t i = first; i < first + count; ++i) {
+            bb.grow(boxes[order[i]]);
+            cb.grow(cent[order[i]]);
+        }
+        nodes[id].box = bb;
+        if (count <= kMaxLeaf) {
+            nodes[id].leaf = true;
+            nodes[id].first = first;
+            nodes[id].count = count;
+            return id;
+        }
+        // Binned SAH over centroids.
+        int best_axis = -1, best_split = -1;
+        float best_cost = FLT_MAX;
+        for (int axis = 0; axis < 3; ++axis) {
+            float lo = comp(cb.lo, axis), hi = comp(cb.hi, axis);
+            if (!(hi > lo)) continue;
+            Box bin_box[kBins];
+            uint32_t bin_cnt[kBins] = {0};
+            float k = kBins / (hi - lo);
+            for (uint32_t i = first; i < first + count; ++i) {
+                int b = std::min(kBins - 1, static_cast<int>((comp(cent[order[i]], axis) - lo) * k));
+                bin_cnt[b]++;
+                bin_box[b].grow(boxes[order[i]]);
+            }
+            float right_area[kBins];
+            uint32_t right_cnt[kBins];
+            Box acc;
+            uint32_t c = 0;
+            for (int b = kBins - 1; b > 0; --b) {
+                acc.grow(bin_box[b]);
+                c += bin_cnt[b];
+                right_area[b] = acc.area();
+                right_cnt[b] = c;
+            }
+            Box lacc;
+            uint32_t lc = 0;
+            for (int b = 0; b < kBins - 1; ++b) {
+                lacc.grow(bin_box[b]);
+                lc += bin_cnt[b];
+                if (lc == 0 || right_cnt[b + 1] == 0) continue;
+                float cost = lacc.area() * lc + right_area[b + 1] * right_cnt[b + 1];
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = axis;
+                    best_split = b;
+                }
+            }
+        }
+        uint32_t mid;
+        if (best_axis < 0) {
+            mid = first + count / 2;  // all centroids coincide: split in the middle
+        } else {
+            float lo = comp(cb.lo, best_axis), hi = comp(cb.hi, best_axis);
+            float k = kBins / (hi - lo);
+            auto it = std::partition(order.begin() + first, order.begin() + first + count, [&](uint32_t p) {
+                int b = std::min(kBins - 1, static_cast<int>((comp(cent[p], best_axis) - lo) * k));
+                return b <= best_split;
+            });
+            mid = static_cast<uint32_t>(it - order.begin());
+            if (mid == first || mid == first + count) mid = first + count / 2;
+        }
+        uint32_t l = build(first, mid - first);
+        uint32_t r = build(mid, first + count - mid);
+        nodes[id].left = l;
+        nodes[id].right = r;
+        return id;
+    }
+};
+
+struct Collapse {
+    const std::vector<Node2> &n2;
+    const std::vector<uint32_t> &order;
+    const HostScene &scene;
+    std::vector<Bvh8Node> &out;
+    std::vector<float> &tri_v;
+    std::vector<uint32_t> subtree_count;
+    uint32_t max_depth = 0;
+
+    uint32_t count_tris(uint32_t id) {
+        const Node2 &n = n2[id];
+        uint32_t c = n.leaf ? n.count : count_tris(n.left) + count_tris(n.right);
+        subtree_count[id] = c;
+        return c;
+    }
+
+    void gather(uint32_t id, std::vector<uint32_t> &prims) const {
+        const Node2 &n = n2[id];
+        if (n.leaf) {
+            for (uint32_t i = 0; i < n.count; ++i) prims.push_back(order[n.first + i]);
+        } else {
+            gather(n.left, prims);
+            gather(n.right, prims);
+        }
+    }
+
+    bool is_leaf_child(uint32_t id) const { return n2[id].leaf || subtree_count[id] <= kMaxLeaf; }
+
+    void emit_tri(uint32_t prim) {
+        for (int k = 0; k < 3; ++k) {
+            f3 p = scene.pos[scene.idx[3 * prim + k]];
+            tri_v.push_back(p.x);
+            tri_v.push_back(p.y);
+            tri_v.push_back(p.z);
+            tri_v.push_back(k == 0 ? bits_float(prim) : 0.0f);
+        }
+    }
+
+    // Writes node `slot_index` of `out` for binary node `id` and recurses.
+    void build(uint32_t id, uint32_t out_index, uint32_t depth) {
+        max_depth = std::max(max_depth, depth);
+        std::vector<uint32_t> ch;
+        if (is_leaf_child(id)) {
+            ch.push_back(id);
+        } else {
+            ch.push_back(n2[id].left);
+            ch.push_back(n2[id].right);
+            while (ch.size() < 8) {
+                int best = -1;
+                float best_area = -1.0f;
+                for (size_t i = 0; i < ch.size(); ++i) {
+                    if (is_leaf_child(ch[i])) continue;
+                    float a = n2[ch[i]].box.area();
+                    if (a > best_area) {
+                        best_area = a;
+                        best = static_cast<int>(i);
+                    }
+                }
+                if (best < 0) break;
+                uint32_t c = ch[best];
+                ch[best] = n2[c].left;
+                ch.push_back(n2[c].right);
+            }
+        }
+        // Assign children to slots: slot s prefers children lying toward the
+        // corner whose coordinate signs are the bits of s (bit set = +).
+        Box nb;
+        for (uint32_t c : ch) nb.grow(n2[c].box);
+        f3 nc = nb.center();
+        int slot_of[8];
+        bool used_slot[8] = {false};
+        bool done[8] = {false};
+        for (size_t step = 0; step < ch.size(); ++step) {
+            float best_cost = FLT_MAX;
+            int bc = -1, bs = -1;
+            for (size_t i = 0; i < ch.size(); ++i) {
+                if (done[i]) continue;
+                f3 d = n2[ch[i]].box.center() - nc;
+                for (int sl = 0; sl < 8; ++sl) {
+                    if (used_slot[sl]) continue;
+                    f3 dir = {(sl & 1) ? 1.0f : -1.0f, (sl & 2) ? 1.0f : -1.0f, (sl & 4) ? 1.0f : -1.0f};
+                    float cost = -dot(d, dir);
+                    if (cost < best_cost) {
+                        best_cost = cost;
+                        bc = static_cast<int>(i);
+                        bs = sl;
+                    }
+                }
+            }
+            done[bc] = true;
+            used_slot[bs] = true;
+            slot_of[bc] = bs;
+        }
+        int child_at[8];
+        for (int sl = 0; sl < 8; ++sl) child_at[sl] = -1;
+        for (size_t i = 0; i < ch.size(); ++i) child_at[slot_of[i]] = static_cast<int>(i);
+
+        Bvh8Node node;
+        std::memset(&node, 0, sizeof(node));
+        node.px = nb.lo.x;
+        node.py = nb.lo.y;
+        node.pz = nb.lo.z;
+        // Per-axis grid step 2^e with 255 steps covering the node box.
+        float step[3];
+        for (int a = 0; a < 3; ++a) {
+            float ext = comp(nb.hi, a) - comp(nb.lo, a);
+            int e = -100;
+            if (ext > 0.0f) e = static_cast<int>(std::ceil(std::log2(ext / 255.0f)));
+            e = std::max(e, -120);
+            while (true) {
+                float s = std::ldexp(1.0f, e);
+                float lo = comp(nb.lo, a);
+                // The top of the grid must reach the node's upper bound.
+                if (lo + 255.0f * s >= comp(nb.hi, a)) break;
+                ++e;
+            }
+            node.e[a] = static_cast<uint8_t>(e + 127);
+            step[a] = std::ldexp(1.0f, e);
+        }
+        float p[3] = {node.px, node.py, node.pz};
+        uint32_t internal_count = 0;
+        for (int sl = 0; sl < 8; ++sl)
+            if (child_at[sl] >= 0 && !is_leaf_child(ch[child_at[sl]])) internal_count++;
+        node.base_child = static_cast<uint32_t>(out.size());
+        node.base_tri = static_cast<uint32_t>(tri_v.size() / 12);
+        out.resize(out.size() + internal_count);
+        uint32_t tri_offset = 0;
+        std::vector<std::pair<uint32_t, uint32_t>> recurse;  // (binary id, out index)
+        uint32_t next_internal = node.base_child;
+        for (int sl = 0; sl < 8; ++sl) {
+            if (child_at[sl] < 0) continue;
+            uint32_t c = ch[child_at[sl]];
+            const Box &cb = n2[c].box;
+            for (int a = 0; a < 3; ++a) {
+                float s = step[a];
+                float lo = comp(cb.lo, a), hi = comp(cb.hi, a);
+                int ql = static_cast<int>(std::floor((lo - p[a]) / s));
+                int qh = static_cast<int>(std::ceil((hi - p[a]) / s));
+                ql = std::min(std::max(ql, 0), 255);
+                qh = std::min(std::max(qh, 0), 255);
+                // Conservative with the exact float ops the traversal uses.
+                while (ql > 0 && p[a] + static_cast<float>(ql) * s > lo) --ql;
+                while (qh < 255 && p[a] + static_cast<float>(qh) * s < hi) ++qh;
+                if (p[a] + static_cast<float>(ql) * s > lo || p[a] + static_cast<float>(qh) * s < hi)
+                    throw std::runtime_error("bvh8: quantisation cannot bound a child box");
+                node.qlo[a][sl] = static_cast<uint8_t>(ql);
+                node.qhi[a][sl] = static_cast<uint8_t>(qh);
+            }
+            if (is_leaf_child(c)) {
+                std::vector<uint32_t> prims;
+                gather(c, prims);
+                if (prims.size() > kMaxLeaf || tri_offset + prims.size() > 24)
+                    throw std::runtime_error("bvh8: leaf too large");
+                node.meta[sl] = static_cast<uint8_t>((((1u << prims.size()) - 1u) << 5) | tri_offset);
+                for (uint32_t pr : prims) emit_tri(pr);
+                tri_offset += static_cast<uint32_t>(prims.size());
+            } else {
+                node.imask |= static_cast<uint8_t>(1u << sl);
+                node.meta[sl] = static_cast<uint8_t>(0x20u | (24u + sl));
+                recurse.push_back({c, next_internal++});
+            }
+        }
+        out[out_index] = node;
+        for (auto &r : recurse) build(r.first, r.second, depth + 1);
+    }
+};
+
+}  // namespace
+
+void build_bvh8(HostScene &s) {
+    uint32_t n = static_cast<uint32_t>(s.prim_inst.size());
+    std::vector<Box> boxes(n);
+    std::vector<f3> cent(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        Box b;
+        for (int k = 0; k < 3; ++k) b.grow(s.pos[s.idx[3 * i + k]]);
+        boxes[i] = b;
+        cent[i] = b.center();
+    }
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    Builder2 b2{boxes, cent, order, {}};
+    b2.nodes.reserve(2 * n);
+    b2.build(0, n);
+    s.nodes.clear();
+    s.tri_v.clear();
+    s.tri_v.reserve(static_cast<size_t>(n) * 12);
+    Collapse col{b2.nodes, order, s, s.nodes, s.tri_v, std::vector<uint32_t>(b2.nodes.size(), 0)};
+    col.count_tris(0);
+    s.nodes.resize(1);
+    col.build(0, 0, 1);
+    s.bvh_depth = col.max_depth;
+    if (s.tri_v.size() != static_cast<size_t>(n) * 12) throw std::runtime_error("bvh8: primitive count mismatch");
+    if (col.max_depth + 1 > 32) throw std::runtime_error("bvh8: tree deeper than the traversal stack");
+}
+
+}  // namespace vs

@@ -1,0 +1,585 @@
+// extern "C" boundary of libvision_b200.so (declared in include/vision_b200.h).
+#include "../../include/vision_b200.h"
+
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "vs_host.h"
+#include "vs_launch.h"
+
+using namespace vs;
+
+struct vs_context {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    mutable std::mutex mu;
+    std::string error;
+    bool consts_uploaded = false;
+};
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+    T *ptr = nullptr;
+    size_t count = 0;
+    cudaError_t upload(const std::vector<T> &v) {
+        free();
+        if (v.empty()) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&ptr, v.size() * sizeof(T));
+        if (e != cudaSuccess) { ptr = nullptr; return e; }
+        count = v.size();
+        return cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    }
+    cudaError_t alloc(size_t n) {
+        if (n <= count && ptr) return cudaSuccess;
+        free();
+        cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
+        if (e != cudaSuccess) { ptr = nullptr; return e; }
+        count = n;
+        return cudaSuccess;
+    }
+    void free() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+};
+
+}  // namespace
+
+struct vs_scene {
+    vs_context *ctx = nullptr;
+    std::mutex mu;
+    HostScene host;
+    bool built = false;
+    bool uploaded = false;
+    DevBuf<Bvh8Node> nodes;
+    DevBuf<float> tri_v;
+    DevBuf<float4> vtx;
+    DevBuf<uint4> prims;
+    DevBuf<Instance> instances;
+    DevBuf<Material> materials;
+    DevBuf<AreaLight> lights;
+    DevBuf<AliasEntry> prim_alias, light_alias;
+    DevBuf<float> prim_pmf, light_pmf, spd;
+    // Film and per-sample radiance (scratch between the megakernel and the film pass).
+    DevBuf<float4> film32, exposed;
+    DevBuf<double> film64;
+    DevBuf<float4> radiance;
+    uint32_t film_frames = 0;
+    bool film64_valid = false;
+    // Optional CUDA-event timing of the megakernel and film launches.
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_render, ev_film;  // start/stop pairs
+    cudaEvent_t ev_join = nullptr;
+
+    ~vs_scene() {
+        for (cudaEvent_t e : ev_render) cudaEventDestroy(e);
+        for (cudaEvent_t e : ev_film) cudaEventDestroy(e);
+        if (ev_join) cudaEventDestroy(ev_join);
+        nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
+        prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free();
+        film32.free(); exposed.free(); film64.free(); radiance.free();
+    }
+
+    DeviceScene device_view() const {
+        DeviceScene d{};
+        d.nodes = reinterpret_cast<const uint4 *>(nodes.ptr);
+        d.tri_v = reinterpret_cast<const float4 *>(tri_v.ptr);
+        d.vtx = vtx.ptr;
+        d.prims = prims.ptr;
+        d.instances = instances.ptr;
+        d.materials = materials.ptr;
+        d.lights = lights.ptr;
+        d.prim_alias = prim_alias.ptr;
+        d.prim_pmf = prim_pmf.ptr;
+        d.light_alias = light_alias.ptr;
+        d.light_pmf = light_pmf.ptr;
+        d.spd = spd.ptr;
+        d.cam = host.cam;
+        d.ip = host.ip;
+        d.node_count = static_cast<uint32_t>(host.nodes.size());
+        d.prim_count = static_cast<uint32_t>(host.prim_inst.size());
+        d.stats = nullptr;
+        return d;
+    }
+};
+
+namespace {
+
+// Upper bound on paths per megakernel launch; sizes the radiance scratch
+// (16 bytes per path).
+constexpr uint64_t kMaxPathsPerLaunch = 1ull << 26;
+
+int fail(const vs_context *ctx, int code, const std::string &msg) {
+    if (ctx) {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        const_cast<vs_context *>(ctx)->error = msg;
+    }
+    return code;
+}
+
+int cuda_fail(const vs_context *ctx, cudaError_t e, const char *where) {
+    return fail(ctx, VS_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define VS_CUDA(call, where)                                        \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where);    \
+    } while (0)
+
+cudaStream_t pick_stream(const vs_scene *s, void *stream) {
+    return stream ? static_cast<cudaStream_t>(stream) : s->ctx->stream;
+}
+
+int upload_scene(vs_scene *s) {
+    vs_context *ctx = s->ctx;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!ctx->consts_uploaded) {
+        const Cie5 &c = cie5();
+        VS_CUDA(upload_spectral_consts(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        ctx->consts_uploaded = true;
+    }
+    const HostScene &h = s->host;
+    std::vector<float4> vtx(h.pos.size() * 2);
+    for (size_t i = 0; i < h.pos.size(); ++i) {
+        vtx[2 * i] = make_float4(h.pos[i].x, h.pos[i].y, h.pos[i].z, h.uv[i].x);
+        vtx[2 * i + 1] = make_float4(h.nrm[i].x, h.nrm[i].y, h.nrm[i].z, h.uv[i].y);
+    }
+    std::vector<uint4> prims(h.prim_inst.size());
+    for (size_t i = 0; i < prims.size(); ++i)
+        prims[i] = make_uint4(h.idx[3 * i], h.idx[3 * i + 1], h.idx[3 * i + 2], h.prim_inst[i]);
+    VS_CUDA(s->nodes.upload(h.nodes), "upload nodes");
+    VS_CUDA(s->tri_v.upload(h.tri_v), "upload triangles");
+    VS_CUDA(s->vtx.upload(vtx), "upload vertices");
+    VS_CUDA(s->prims.upload(prims), "upload primitives");
+    VS_CUDA(s->instances.upload(h.instances), "upload instances");
+    VS_CUDA(s->materials.upload(h.materials), "upload materials");
+    VS_CUDA(s->lights.upload(h.lights), "upload lights");
+    VS_CUDA(s->prim_alias.upload(h.prim_alias), "upload alias");
+    VS_CUDA(s->prim_pmf.upload(h.prim_pmf), "upload pmf");
+    VS_CUDA(s->light_alias.upload(h.light_alias), "upload light alias");
+    VS_CUDA(s->light_pmf.upload(h.light_pmf), "upload light pmf");
+    std::vector<float> spd = h.spd;
+    if (spd.empty()) spd.push_back(0.0f);
+    VS_CUDA(s->spd.upload(spd), "upload spd");
+    s->uploaded = true;
+    return VS_OK;
+}
+
+int ensure_film(vs_scene *s) {
+    vs_context *ctx = s->ctx;
+    size_t npix = static_cast<size_t>(s->host.cam.width) * s->host.cam.height;
+    VS_CUDA(s->film32.alloc(npix), "film alloc");
+    VS_CUDA(s->exposed.alloc(npix), "film alloc");
+    return VS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vs_version(void) { return 100; }
+
+int vs_context_create(int device, vs_context **out) {
+    if (!out) return VS_E_INVALID;
+    *out = nullptr;
+    vs_context *ctx = new vs_context();
+    ctx->device = device;
+    if (device >= 0) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || device >= n) {
+            delete ctx;
+            return VS_E_NO_DEVICE;
+        }
+        if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return VS_E_CUDA;
+        }
+    }
+    *out = ctx;
+    return VS_OK;
+}
+
+void vs_context_destroy(vs_context *ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *vs_last_error(const vs_context *ctx) {
+    if (!ctx) return "null context";
+    return ctx->error.c_str();
+}
+
+int vs_scene_load_json(vs_context *ctx, const char *json, size_t len, const char *base_dir, const char *table_cache,
+                       vs_scene **out) {
+    if (!ctx || !json || !out) return fail(ctx, VS_E_INVALID, "null argument");
+    *out = nullptr;
+    vs_scene *s = new vs_scene();
+    s->ctx = ctx;
+    try {
+        load_scene_json(std::string(json, len), base_dir ? base_dir : "", table_cache ? table_cache : "", s->host);
+    } catch (const std::exception &e) {
+        std::string m = e.what();
+        delete s;
+        if (m.rfind("unsupported", 0) == 0) return fail(ctx, VS_E_UNSUPPORTED, m);
+        return fail(ctx, VS_E_PARSE, m);
+    }
+    *out = s;
+    return VS_OK;
+}
+
+void vs_scene_destroy(vs_scene *s) {
+    if (!s) return;
+    if (s->ctx && s->ctx->device >= 0) cudaSetDevice(s->ctx->device);
+    delete s;
+}
+
+int vs_scene_build_accel(vs_scene *s) {
+    if (!s) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    std::lock_guard<std::mutex> lock(s->mu);
+    try {
+        build_bvh8(s->host);
+    } catch (const std::exception &e) {
+        return fail(ctx, VS_E_RANGE, e.what());
+    }
+    s->built = true;
+    if (ctx->device >= 0) {
+        int rc = upload_scene(s);
+        if (rc != VS_OK) return rc;
+    }
+    return VS_OK;
+}
+
+int vs_set_resolution(vs_scene *s, uint32_t width, uint32_t height) {
+    if (!s || width == 0 || height == 0) return fail(s ? s->ctx : nullptr, VS_E_INVALID, "bad resolution");
+    std::lock_guard<std::mutex> lock(s->mu);
+    update_camera(s->host, width, height);
+    s->film_frames = 0;
+    s->film64_valid = false;
+    return VS_OK;
+}
+
+int vs_camera_set(vs_scene *s, const float *c2w16, float fov_y_deg) {
+    if (!s || !c2w16) return VS_E_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r) s->host.cam.c2w.m[c][r] = c2w16[4 * c + r];
+    float fov = fov_y_deg < 15.0f ? 15.0f : (fov_y_deg > 120.0f ? 120.0f : fov_y_deg);
+    s->host.cam.tan_half_fov = std::tan(fov * kPi / 180.0f * 0.5f);
+    s->film_frames = 0;
+    s->film64_valid = false;
+    return VS_OK;
+}
+
+int vs_scene_info_get(const vs_scene *s, vs_scene_info *o) {
+    if (!s || !o) return VS_E_INVALID;
+    const HostScene &h = s->host;
+    o->vertex_count = static_cast<uint32_t>(h.pos.size());
+    o->prim_count = static_cast<uint32_t>(h.prim_inst.size());
+    o->instance_count = static_cast<uint32_t>(h.instances.size());
+    o->material_count = static_cast<uint32_t>(h.materials.size());
+    o->light_count = static_cast<uint32_t>(h.lights.size());
+    o->prim_alias_count = static_cast<uint32_t>(h.prim_alias.size());
+    o->spd_floats = static_cast<uint32_t>(h.spd.size());
+    o->bvh_node_count = static_cast<uint32_t>(h.nodes.size());
+    o->bvh_depth = h.bvh_depth;
+    o->width = h.cam.width;
+    o->height = h.cam.height;
+    o->spectrum_dim = h.ip.spectrum_dim;
+    o->max_depth = h.ip.max_depth;
+    o->accel_built = s->built ? 1u : 0u;
+    return VS_OK;
+}
+
+namespace {
+struct ExportView {
+    const void *ptr;
+    size_t bytes;
+};
+ExportView export_view(const vs_scene *s, int what) {
+    const HostScene &h = s->host;
+    switch (what) {
+        case VS_EXPORT_POS: return {h.pos.data(), h.pos.size() * sizeof(f3)};
+        case VS_EXPORT_NRM: return {h.nrm.data(), h.nrm.size() * sizeof(f3)};
+        case VS_EXPORT_UV: return {h.uv.data(), h.uv.size() * sizeof(f2)};
+        case VS_EXPORT_IDX: return {h.idx.data(), h.idx.size() * 4};
+        case VS_EXPORT_PRIM_INST: return {h.prim_inst.data(), h.prim_inst.size() * 4};
+        case VS_EXPORT_INSTANCES: return {h.instances.data(), h.instances.size() * sizeof(Instance)};
+        case VS_EXPORT_MATERIALS: return {h.materials.data(), h.materials.size() * sizeof(Material)};
+        case VS_EXPORT_LIGHTS: return {h.lights.data(), h.lights.size() * sizeof(AreaLight)};
+        case VS_EXPORT_PRIM_ALIAS: return {h.prim_alias.data(), h.prim_alias.size() * sizeof(AliasEntry)};
+        case VS_EXPORT_PRIM_PMF: return {h.prim_pmf.data(), h.prim_pmf.size() * 4};
+        case VS_EXPORT_LIGHT_ALIAS: return {h.light_alias.data(), h.light_alias.size() * sizeof(AliasEntry)};
+        case VS_EXPORT_LIGHT_PMF: return {h.light_pmf.data(), h.light_pmf.size() * 4};
+        case VS_EXPORT_CAMERA: return {&h.cam, sizeof(Camera)};
+        case VS_EXPORT_INTEGRATOR: return {&h.ip, sizeof(IntegratorParams)};
+        case VS_EXPORT_SPD: return {h.spd.data(), h.spd.size() * 4};
+        case VS_EXPORT_MATERIAL_RGB: return {h.material_rgb.data(), h.material_rgb.size() * sizeof(f3)};
+        case VS_EXPORT_LIGHT_RGB: return {h.light_rgb.data(), h.light_rgb.size() * sizeof(f3)};
+        case VS_EXPORT_BVH_NODES: return {h.nodes.data(), h.nodes.size() * sizeof(Bvh8Node)};
+        case VS_EXPORT_BVH_TRIS: return {h.tri_v.data(), h.tri_v.size() * 4};
+        default: return {nullptr, static_cast<size_t>(-1)};
+    }
+}
+}  // namespace
+
+int vs_scene_export_size(const vs_scene *s, int what, size_t *bytes) {
+    if (!s || !bytes) return VS_E_INVALID;
+    ExportView v = export_view(s, what);
+    if (v.bytes == static_cast<size_t>(-1)) return fail(s->ctx, VS_E_INVALID, "unknown export id");
+    *bytes = v.bytes;
+    return VS_OK;
+}
+
+int vs_scene_export(const vs_scene *s, int what, void *dst, size_t bytes) {
+    if (!s || (!dst && bytes)) return VS_E_INVALID;
+    ExportView v = export_view(s, what);
+    if (v.bytes == static_cast<size_t>(-1)) return fail(s->ctx, VS_E_INVALID, "unknown export id");
+    if (bytes != v.bytes) return fail(s->ctx, VS_E_INVALID, "export size mismatch");
+    if (bytes) std::memcpy(dst, v.ptr, bytes);
+    return VS_OK;
+}
+
+int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_precision, void *stream) {
+    if (!s) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render");
+    if (frame_begin != 0 && frame_begin != s->film_frames)
+        return fail(ctx, VS_E_STATE, "frames must continue the film (frame_begin == frames rendered) or restart at 0");
+    if (film_precision == VS_FILM_FP64 && frame_begin != 0 && !s->film64_valid)
+        return fail(ctx, VS_E_STATE, "FP64 film must be enabled from frame 0");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    int rc = ensure_film(s);
+    if (rc != VS_OK) return rc;
+    cudaStream_t st = pick_stream(s, stream);
+    uint64_t npix = static_cast<uint64_t>(s->host.cam.width) * s->host.cam.height;
+    if (film_precision == VS_FILM_FP64) VS_CUDA(s->film64.alloc(npix * 4), "film64 alloc");
+    uint64_t frames_per_chunk = kMaxPathsPerLaunch / npix;
+    if (frames_per_chunk == 0) return fail(ctx, VS_E_RANGE, "resolution above the per-launch path limit");
+    if (frames_per_chunk > frame_count) frames_per_chunk = frame_count;
+    VS_CUDA(s->radiance.alloc(static_cast<size_t>(frames_per_chunk * npix)), "radiance alloc");
+    DeviceScene dv = s->device_view();
+    auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
+        cudaEvent_t e;
+        cudaError_t r = cudaEventCreate(&e);
+        if (r != cudaSuccess) return r;
+        v.push_back(e);
+        return cudaEventRecord(e, st);
+    };
+    for (uint32_t f = 0; f < frame_count; f += static_cast<uint32_t>(frames_per_chunk)) {
+        uint32_t fc = static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk, frame_count - f));
+        if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
+        VS_CUDA(launch_render(dv, frame_begin + f, fc, s->radiance.ptr, st), "render launch");
+        if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
+        if (s->timing) VS_CUDA(timed_event(s->ev_film), "timing event");
+        VS_CUDA(launch_film(s->radiance.ptr, static_cast<uint32_t>(npix), frame_begin + f, fc, s->film32.ptr,
+                            film_precision == VS_FILM_FP64 ? s->film64.ptr : nullptr, st),
+                "film launch");
+        if (s->timing) VS_CUDA(timed_event(s->ev_film), "timing event");
+    }
+    // Later calls on the context stream (film download) must see this work.
+    if (st != ctx->stream) {
+        if (!s->ev_join) VS_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "join event");
+        VS_CUDA(cudaEventRecord(s->ev_join, st), "join record");
+        VS_CUDA(cudaStreamWaitEvent(ctx->stream, s->ev_join, 0), "join wait");
+    }
+    s->film_frames = frame_begin + frame_count;
+    s->film64_valid = film_precision == VS_FILM_FP64 && (frame_begin == 0 || s->film64_valid);
+    return VS_OK;
+}
+
+int vs_synchronize(vs_scene *s) {
+    if (!s) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return VS_OK;
+    VS_CUDA(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return VS_OK;
+}
+
+int vs_film_download(vs_scene *s, void *dst, size_t bytes, int which) {
+    if (!s || !dst) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context has no film");
+    std::lock_guard<std::mutex> lock(s->mu);
+    size_t npix = static_cast<size_t>(s->host.cam.width) * s->host.cam.height;
+    if (s->film_frames == 0) return fail(ctx, VS_E_STATE, "nothing rendered");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    if (which == VS_FILM_LINEAR || which == VS_FILM_EXPOSED) {
+        if (bytes != npix * 16) return fail(ctx, VS_E_INVALID, "film size mismatch");
+        const float4 *src = s->film32.ptr;
+        if (which == VS_FILM_EXPOSED) {
+            VS_CUDA(launch_exposure(s->film32.ptr, static_cast<uint32_t>(npix), s->host.cam.exposure, s->exposed.ptr, st),
+                    "exposure");
+            src = s->exposed.ptr;
+        }
+        VS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), "film copy");
+    } else if (which == VS_FILM_SUM64) {
+        if (!s->film64_valid) return fail(ctx, VS_E_STATE, "FP64 film not rendered");
+        if (bytes != npix * 32) return fail(ctx, VS_E_INVALID, "film size mismatch");
+        VS_CUDA(cudaMemcpyAsync(dst, s->film64.ptr, bytes, cudaMemcpyDeviceToHost, st), "film copy");
+    } else {
+        return fail(ctx, VS_E_INVALID, "unknown film buffer");
+    }
+    VS_CUDA(cudaStreamSynchronize(st), "film sync");
+    return VS_OK;
+}
+
+int vs_trace_closest_device(vs_scene *s, const float *rays, uint32_t n, vs_hit *hits, float *t, void *stream) {
+    if (!s || (n && (!rays || !hits || !t))) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot trace");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede tracing");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    VS_CUDA(launch_trace_closest(s->device_view(), rays, n, reinterpret_cast<Hit *>(hits), t, pick_stream(s, stream)),
+            "trace launch");
+    return VS_OK;
+}
+
+int vs_trace_any_device(vs_scene *s, const float *rays, uint32_t n, uint32_t *occ, void *stream) {
+    if (!s || (n && (!rays || !occ))) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot trace");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede tracing");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    VS_CUDA(launch_trace_any(s->device_view(), rays, n, occ, pick_stream(s, stream)), "trace launch");
+    return VS_OK;
+}
+
+int vs_trace_closest_host(vs_scene *s, const float *rays, uint32_t n, vs_hit *hits, float *t) {
+    if (!s || (n && (!rays || !hits || !t))) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot trace");
+    if (n == 0) return VS_OK;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    float *d_rays = nullptr, *d_t = nullptr;
+    vs_hit *d_hits = nullptr;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaMallocAsync(&d_rays, static_cast<size_t>(n) * 32, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_hits, static_cast<size_t>(n) * sizeof(vs_hit), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_t, static_cast<size_t>(n) * 4, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rays, rays, static_cast<size_t>(n) * 32, cudaMemcpyHostToDevice, st);
+    int rc = VS_OK;
+    if (e == cudaSuccess) rc = vs_trace_closest_device(s, d_rays, n, d_hits, d_t, st);
+    if (e == cudaSuccess && rc == VS_OK) e = cudaMemcpyAsync(hits, d_hits, static_cast<size_t>(n) * sizeof(vs_hit), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && rc == VS_OK) e = cudaMemcpyAsync(t, d_t, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, st);
+    if (d_rays) cudaFreeAsync(d_rays, st);
+    if (d_hits) cudaFreeAsync(d_hits, st);
+    if (d_t) cudaFreeAsync(d_t, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "trace (host buffers)");
+    if (rc != VS_OK) return rc;
+    if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "trace sync");
+    return VS_OK;
+}
+
+int vs_trace_any_host(vs_scene *s, const float *rays, uint32_t n, uint32_t *occ) {
+    if (!s || (n && (!rays || !occ))) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot trace");
+    if (n == 0) return VS_OK;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    float *d_rays = nullptr;
+    uint32_t *d_occ = nullptr;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaMallocAsync(&d_rays, static_cast<size_t>(n) * 32, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_occ, static_cast<size_t>(n) * 4, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rays, rays, static_cast<size_t>(n) * 32, cudaMemcpyHostToDevice, st);
+    int rc = VS_OK;
+    if (e == cudaSuccess) rc = vs_trace_any_device(s, d_rays, n, d_occ, st);
+    if (e == cudaSuccess && rc == VS_OK) e = cudaMemcpyAsync(occ, d_occ, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, st);
+    if (d_rays) cudaFreeAsync(d_rays, st);
+    if (d_occ) cudaFreeAsync(d_occ, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "trace (host buffers)");
+    if (rc != VS_OK) return rc;
+    if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "trace sync");
+    return VS_OK;
+}
+
+uint64_t vs_launch_count(void) { return launch_count(); }
+
+int vs_timing_enable(vs_scene *s, int enable) {
+    if (!s) return VS_E_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (cudaEvent_t e : s->ev_render) cudaEventDestroy(e);
+    for (cudaEvent_t e : s->ev_film) cudaEventDestroy(e);
+    s->ev_render.clear();
+    s->ev_film.clear();
+    s->timing = enable != 0;
+    return VS_OK;
+}
+
+int vs_timing_read(vs_scene *s, double *render_ms, double *film_ms, uint32_t *render_launches) {
+    if (!s || !render_ms || !film_ms || !render_launches) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    std::lock_guard<std::mutex> lock(s->mu);
+    double r = 0.0, f = 0.0;
+    for (size_t i = 0; i + 1 < s->ev_render.size(); i += 2) {
+        float ms = 0.0f;
+        VS_CUDA(cudaEventSynchronize(s->ev_render[i + 1]), "timing sync");
+        VS_CUDA(cudaEventElapsedTime(&ms, s->ev_render[i], s->ev_render[i + 1]), "timing read");
+        r += ms;
+    }
+    for (size_t i = 0; i + 1 < s->ev_film.size(); i += 2) {
+        float ms = 0.0f;
+        VS_CUDA(cudaEventSynchronize(s->ev_film[i + 1]), "timing sync");
+        VS_CUDA(cudaEventElapsedTime(&ms, s->ev_film[i], s->ev_film[i + 1]), "timing read");
+        f += ms;
+    }
+    *render_ms = r;
+    *film_ms = f;
+    *render_launches = static_cast<uint32_t>(s->ev_render.size() / 2);
+    return VS_OK;
+}
+
+int vs_render_stats(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, uint64_t *out3) {
+    if (!s || !out3) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render_stats");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    uint64_t npix = static_cast<uint64_t>(s->host.cam.width) * s->host.cam.height;
+    if (npix * frame_count > kMaxPathsPerLaunch) return fail(ctx, VS_E_RANGE, "too many paths for one instrumented launch");
+    VS_CUDA(s->radiance.alloc(static_cast<size_t>(npix * frame_count)), "radiance alloc");
+    unsigned long long *d_stats = nullptr;
+    VS_CUDA(cudaMalloc(&d_stats, 3 * sizeof(unsigned long long)), "stats alloc");
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaMemsetAsync(d_stats, 0, 3 * sizeof(unsigned long long), st);
+    DeviceScene dv = s->device_view();
+    dv.stats = d_stats;
+    if (e == cudaSuccess) e = launch_render(dv, frame_begin, frame_count, s->radiance.ptr, st);
+    unsigned long long h[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_stats);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "instrumented render");
+    out3[0] = h[0];
+    out3[1] = h[1];
+    out3[2] = h[2];
+    return VS_OK;
+}
+
+int vs_rgb_to_spectrum(vs_context *ctx, const char *table_cache, const float *rgb3, int mode, float *out4) {
+    if (!rgb3 || !out4) return fail(ctx, VS_E_INVALID, "null argument");
+    const float *table = rgb2spec_table(table_cache ? table_cache : "");
+    if (mode == 0) rgb2spec_decode_albedo(table, rgb3, out4);
+    else if (mode == 1) rgb2spec_decode_unbound(table, rgb3, out4);
+    else return fail(ctx, VS_E_INVALID, "mode must be 0 or 1");
+    return VS_OK;
+}
+
+}  // extern "C"

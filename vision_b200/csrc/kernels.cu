@@ -1,0 +1,172 @@
+// sm_100a kernels of the path-tracing hot path:
+//   k_trace_closest  - seeded closest-hit batches (parity hook)
+//   k_render         - megakernel: one camera path per thread, radiance to a
+//                      per-sample buffer
+//   k_film_*         - film accumulation in the reference's frame order
+//                      (FP32 running mean) or as FP64 sums
+#include "vs_integrator.cuh"
+#include "vs_launch.h"
+
+#include <atomic>
+
+namespace vs {
+
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long launch_count() { return g_launches.load(); }
+
+__global__ void __launch_bounds__(128) k_trace_closest(DeviceScene s, const float *rays, uint32_t n, Hit *hits,
+                                                       float *t_out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 *r4 = reinterpret_cast<const float4 *>(rays) + 2u * i;
+    float4 a = r4[0], b = r4[1];
+    RayPre rp = precompute_ray(make3(a.x, a.y, a.z), make3(b.x, b.y, b.z));
+    float tmax = b.w;
+    Hit h;
+    float t;
+    if (trace_closest(s, rp, tmax, h, t)) {
+        hits[i] = h;
+        t_out[i] = t;
+    } else {
+        hits[i] = Hit{kInvalid, kInvalid, 0.0f, 0.0f};
+        t_out[i] = -1.0f;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_trace_any(DeviceScene s, const float *rays, uint32_t n, uint32_t *occ) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 *r4 = reinterpret_cast<const float4 *>(rays) + 2u * i;
+    float4 a = r4[0], b = r4[1];
+    RayPre rp = precompute_ray(make3(a.x, a.y, a.z), make3(b.x, b.y, b.z));
+    occ[i] = trace_any(s, rp, b.w) ? 1u : 0u;
+}
+
+// Paths are numbered frame-major: path p covers pixel p % (w*h) of frame
+// frame_begin + p / (w*h), so neighbouring threads trace neighbouring pixels.
+template <int N>
+__global__ void __launch_bounds__(128) k_render(DeviceScene s, uint32_t frame_begin, uint64_t path_count,
+                                                float4 *radiance) {
+    uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= path_count) return;
+    uint32_t npix = s.cam.width * s.cam.height;
+    uint32_t frame = frame_begin + static_cast<uint32_t>(p / npix);
+    uint32_t pix = static_cast<uint32_t>(p % npix);
+    uint32_t px = pix % s.cam.width, py = pix / s.cam.width;
+    f3 L = trace_path<N>(s, px, py, frame);
+    radiance[p] = make_float4(L.x, L.y, L.z, 1.0f);
+}
+
+// NormalRadianceCollector::add_sample (normal.cpp:87-101) for frame_count
+// consecutive frames: zero_if_nan_inf, then the running mean
+// lerp(1 / (frame + 1), prev, value), in frame order.
+__global__ void k_film_running_mean(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count,
+                                    float4 *film) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    float4 acc = frame_begin == 0 ? make_float4(0, 0, 0, 0) : film[i];
+    for (uint32_t f = 0; f < frame_count; ++f) {
+        float4 v = radiance[static_cast<size_t>(f) * npix + i];
+        bool bad = isnan(v.x) || isnan(v.y) || isnan(v.z) || isinf(v.x) || isinf(v.y) || isinf(v.z);
+        if (bad) v = make_float4(0, 0, 0, 0);
+        float a = 1.0f / static_cast<float>(frame_begin + f + 1u);
+        acc.x = acc.x + a * (v.x - acc.x);
+        acc.y = acc.y + a * (v.y - acc.y);
+        acc.z = acc.z + a * (v.z - acc.z);
+        acc.w = acc.w + a * (v.w - acc.w);
+    }
+    film[i] = acc;
+}
+
+// FP64 film: per-pixel sums of the sanitised samples and the sample count.
+__global__ void k_film_sum64(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count,
+                             double *sum4) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    double4 acc = frame_begin == 0 ? make_double4(0, 0, 0, 0) : reinterpret_cast<double4 *>(sum4)[i];
+    for (uint32_t f = 0; f < frame_count; ++f) {
+        float4 v = radiance[static_cast<size_t>(f) * npix + i];
+        bool bad = isnan(v.x) || isnan(v.y) || isnan(v.z) || isinf(v.x) || isinf(v.y) || isinf(v.z);
+        if (bad) v = make_float4(0, 0, 0, 1);
+        acc.x += v.x;
+        acc.y += v.y;
+        acc.z += v.z;
+        acc.w += 1.0;
+    }
+    reinterpret_cast<double4 *>(sum4)[i] = acc;
+}
+
+// Exposure + linear tone map of the linear film (RadianceCollector::apply_exposure,
+// radiance_collector.cpp:24-26).
+__global__ void k_film_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    float4 v = film[i];
+    out[i] = make_float4(1.0f - expf(-v.x * exposure), 1.0f - expf(-v.y * exposure), 1.0f - expf(-v.z * exposure), 1.0f);
+}
+
+cudaError_t upload_spectral_consts(const float *x, const float *y, const float *z, const float *d65, float y_integral) {
+    SpectralConsts c;
+    for (int i = 0; i < kSpd5Count; ++i) {
+        c.cie_x[i] = x[i];
+        c.cie_y[i] = y[i];
+        c.cie_z[i] = z[i];
+        c.d65[i] = d65[i];
+    }
+    c.inv_cie_y_integral = 1.0f / y_integral;
+    return cudaMemcpyToSymbol(c_spec, &c, sizeof(c));
+}
+
+cudaError_t launch_trace_closest(const DeviceScene &s, const float *rays, uint32_t n, Hit *hits, float *t,
+                                 cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_trace_closest<<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, hits, t);
+    g_launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace_any(const DeviceScene &s, const float *rays, uint32_t n, uint32_t *occ, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_trace_any<<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, occ);
+    g_launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_render(const DeviceScene &s, uint32_t frame_begin, uint32_t frame_count, float4 *radiance,
+                          cudaStream_t st) {
+    uint64_t paths = static_cast<uint64_t>(s.cam.width) * s.cam.height * frame_count;
+    if (paths == 0) return cudaSuccess;
+    uint64_t blocks = (paths + 127) / 128;
+    if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    switch (s.ip.spectrum_dim) {
+        case 1: k_render<1><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
+        case 2: k_render<2><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
+        case 3: k_render<3><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
+        case 4: k_render<4><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
+        default: return cudaErrorInvalidValue;
+    }
+    g_launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count, float4 *film32,
+                        double *film64, cudaStream_t st) {
+    unsigned blocks = (npix + 255) / 256;
+    if (film32) {
+        k_film_running_mean<<<blocks, 256, 0, st>>>(radiance, npix, frame_begin, frame_count, film32);
+        g_launches++;
+    }
+    if (film64) {
+        k_film_sum64<<<blocks, 256, 0, st>>>(radiance, npix, frame_begin, frame_count, film64);
+        g_launches++;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out, cudaStream_t st) {
+    k_film_exposure<<<(npix + 255) / 256, 256, 0, st>>>(film, npix, exposure, out);
+    g_launches++;
+    return cudaGetLastError();
+}
+
+}  // namespace vs

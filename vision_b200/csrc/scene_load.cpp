@@ -1,0 +1,522 @@
+// vision_scene.json -> HostScene.
+//
+// Keeps the reference's schema (src/core/scene_desc.cpp:37-53,
+// src/core/node_desc.cpp): top-level "shapes", "materials", "camera",
+// "integrator", "spectrum", "sampler", "light_sampler", "render_setting";
+// nodes are {"type", "name", "param"}; slots are a number, an array, a
+// {"channels", "node"} pair or a {"type": "number", "param": {"value"}} node;
+// emission hangs off a shape as {"emission": {"type": "area", "param"}}.
+#include "vs_host.h"
+#include "json.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <stdexcept>
+
+#include "data/spectral_tables.inc"
+
+namespace vs {
+
+const Cie5 &cie5() {
+    static Cie5 c = [] {
+        Cie5 r{};
+        for (int i = 0; i < kSpd5Count; ++i) {
+            r.x[i] = VS_CIE_X[5 * i];
+            r.y[i] = VS_CIE_Y[5 * i];
+            r.z[i] = VS_CIE_Z[5 * i];
+            r.d65[i] = VS_CIE_D65[5 * i];
+        }
+        float sum = 0.0f;
+        for (int i = 0; i < kSpd5Count; ++i) sum += 0.5f * (VS_CIE_Y[i * 5] + VS_CIE_Y[(i + 1) * 5]);
+        r.y_integral = sum * 5.0f;
+        return r;
+    }();
+    return c;
+}
+
+void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &table, std::vector<float> &pmf) {
+    size_t n = weights.size();
+    double sum = 0.0;
+    for (float w : weights) sum += w;
+    double ratio = static_cast<double>(n) / sum;
+    std::vector<uint32_t> over, under;
+    table.assign(n, AliasEntry{0.0f, 0u});
+    for (uint32_t i = 0; i < n; ++i) {
+        float p = static_cast<float>(weights[i] * ratio);
+        table[i] = {p, i};
+        (p > 1.0f ? over : under).push_back(i);
+    }
+    while (!over.empty() && !under.empty()) {
+        uint32_t o = over.back(), u = under.back();
+        over.pop_back();
+        under.pop_back();
+        table[o].prob -= 1.0f - table[u].prob;
+        table[u].alias = o;
+        if (table[o].prob > 1.0f) over.push_back(o);
+        else if (table[o].prob < 1.0f) under.push_back(o);
+    }
+    for (uint32_t i : over) table[i] = {1.0f, i};
+    for (uint32_t i : under) table[i] = {1.0f, i};
+    float integral = static_cast<float>(sum / static_cast<double>(n));
+    pmf.resize(n);
+    for (size_t i = 0; i < n; ++i)
+        pmf[i] = integral > 0.0f ? weights[i] / (integral * static_cast<float>(n)) : 0.0f;
+}
+
+namespace {
+
+std::runtime_error unsupported(const std::string &what) {
+    return std::runtime_error("unsupported: " + what);
+}
+
+m4 mat_from_columns(const Json &cols) {
+    m4 m = m4_identity();
+    if (!cols.is_array() || cols.size() != 4) throw std::runtime_error("matrix4x4 needs 4 columns");
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r) m.m[c][r] = cols[c][r].as_float();
+    return m;
+}
+
+m4 translation(f3 t) {
+    m4 m = m4_identity();
+    m.m[3][0] = t.x; m.m[3][1] = t.y; m.m[3][2] = t.z;
+    return m;
+}
+m4 scale_m(f3 s) {
+    m4 m = m4_identity();
+    m.m[0][0] = s.x; m.m[1][1] = s.y; m.m[2][2] = s.z;
+    return m;
+}
+// Right-handed rotations about the axes, angle in degrees.
+m4 rot_x(float deg) {
+    float a = deg * kPi / 180.0f, c = std::cos(a), s = std::sin(a);
+    m4 m = m4_identity();
+    m.m[1][1] = c; m.m[1][2] = s; m.m[2][1] = -s; m.m[2][2] = c;
+    return m;
+}
+m4 rot_y(float deg) {
+    float a = deg * kPi / 180.0f, c = std::cos(a), s = std::sin(a);
+    m4 m = m4_identity();
+    m.m[0][0] = c; m.m[0][2] = -s; m.m[2][0] = s; m.m[2][2] = c;
+    return m;
+}
+m4 rot_z(float deg) {
+    float a = deg * kPi / 180.0f, c = std::cos(a), s = std::sin(a);
+    m4 m = m4_identity();
+    m.m[0][0] = c; m.m[0][1] = s; m.m[1][0] = -s; m.m[1][1] = c;
+    return m;
+}
+
+f3 as_f3(const Json &j, f3 def) {
+    if (!j.is_array() || j.size() < 3) return def;
+    return {j[0].as_float(), j[1].as_float(), j[2].as_float()};
+}
+
+// Camera frame whose columns are right, up, forward, position; only used to
+// recover yaw and pitch (Sensor::update_mat, sensor.cpp:78-83).
+m4 look_at(f3 pos, f3 target, f3 up) {
+    f3 fwd = normalize(target - pos);
+    f3 right = normalize(cross(fwd, up));
+    f3 up2 = cross(right, fwd);
+    m4 m = m4_identity();
+    m.m[0][0] = right.x; m.m[0][1] = right.y; m.m[0][2] = right.z;
+    m.m[1][0] = up2.x; m.m[1][1] = up2.y; m.m[1][2] = up2.z;
+    m.m[2][0] = fwd.x; m.m[2][1] = fwd.y; m.m[2][2] = fwd.z;
+    m.m[3][0] = pos.x; m.m[3][1] = pos.y; m.m[3][2] = pos.z;
+    return m;
+}
+
+// TransformDesc::init (node_desc.cpp:26-52).
+m4 parse_transform(const Json &t) {
+    if (t.is_null()) return m4_identity();
+    std::string type = t["type"].as_string("matrix4x4");
+    const Json &p = t["param"];
+    if (type == "matrix4x4") return p.contains("matrix4x4") ? mat_from_columns(p["matrix4x4"]) : m4_identity();
+    if (type == "look_at")
+        return look_at(as_f3(p["position"], make3(0.0f)), as_f3(p["target_pos"], make3(0, 0, 1)), as_f3(p["up"], make3(0, 1, 0)));
+    if (type == "Euler") {
+        m4 yaw = rot_y(p["yaw"].as_float(0.0f));
+        m4 roll = rot_z(p["roll"].as_float(0.0f));
+        m4 pitch = rot_x(p["pitch"].as_float(0.0f));
+        return translation(as_f3(p["position"], make3(0.0f))) * pitch * roll * yaw;
+    }
+    throw unsupported("transform type '" + type + "'");
+}
+
+// Slot value as a flat float list (SlotDesc::init, node_desc.cpp:127-150).
+std::vector<float> slot_values(const Json &j) {
+    if (j.is_number() || j.is_array()) return j.as_floats();
+    if (j.is_object()) {
+        if (j.contains("channels")) return slot_values(j["node"]);
+        std::string type = j["type"].as_string("number");
+        if (type == "number" || type == "constant") {
+            const Json &p = j.contains("param") ? j["param"] : j;
+            return p["value"].as_floats();
+        }
+        throw unsupported("shader node type '" + type + "'");
+    }
+    return {};
+}
+
+bool is_blackbody_slot(const Json &j) {
+    const Json &n = j.is_object() && j.contains("channels") ? j["node"] : j;
+    return n.is_object() && n["type"].as_string() == "blackbody";
+}
+const Json &slot_node(const Json &j) { return j.is_object() && j.contains("channels") ? j["node"] : j; }
+
+f3 slot_rgb(const Json &j, f3 def) {
+    std::vector<float> v = slot_values(j);
+    if (v.empty()) return def;
+    if (v.size() == 1) return make3(v[0]);
+    return {v[0], v[1], v.size() > 2 ? v[2] : v[1]};
+}
+float slot_scalar(const Json &j, float def) {
+    std::vector<float> v = slot_values(j);
+    return v.empty() ? def : v[0];
+}
+
+struct MeshData {
+    std::vector<f3> p, n;
+    std::vector<f2> uv;
+    std::vector<uint32_t> idx;
+};
+
+// Quad::init (src/render_core/shapes/quad.cpp:21-50): unit quad in the xz plane
+// facing +y, vertex normals set to the unnormalised geometric normal.
+MeshData make_quad(float width, float height) {
+    MeshData m;
+    float w = width / 2, h = height / 2;
+    m.p = {{w, 0, h}, {w, 0, -h}, {-w, 0, h}, {-w, 0, -h}};
+    m.uv = {{1, 1}, {1, 0}, {0, 1}, {0, 0}};
+    f3 ng = cross(m.p[0] - m.p[2], m.p[1] - m.p[2]);
+    m.n.assign(4, ng);
+    m.idx = {0, 1, 2, 2, 1, 3};
+    return m;
+}
+
+// Cube::init (src/render_core/shapes/cube.cpp:20-71).
+MeshData make_cube(float x, float y, float z) {
+    y = y == 0 ? x : y;
+    z = z == 0 ? y : z;
+    x /= 2; y /= 2; z /= 2;
+    MeshData m;
+    m.p = {{-x, -y, z}, {x, -y, z}, {-x, y, z}, {x, y, z},     {-x, y, -z}, {x, y, -z}, {-x, -y, -z}, {x, -y, -z},
+           {-x, y, z},  {x, y, z},  {-x, y, -z}, {x, y, -z},   {-x, -y, z}, {x, -y, z}, {-x, -y, -z}, {x, -y, -z},
+           {x, -y, z},  {x, y, z},  {x, y, -z},  {x, -y, -z},  {-x, -y, z}, {-x, y, z}, {-x, y, -z},  {-x, -y, -z}};
+    const f3 N[6] = {{0, 0, 1}, {0, 0, -1}, {0, 1, 0}, {0, -1, 0}, {1, 0, 0}, {-1, 0, 0}};
+    for (int f = 0; f < 6; ++f)
+        for (int k = 0; k < 4; ++k) m.n.push_back(N[f]);
+    m.uv = {{0, 0}, {1, 0}, {0, 1}, {1, 1}, {0, 1}, {1, 1}, {0, 0}, {1, 0}, {0, 1}, {1, 1}, {0, 0}, {1, 0},
+            {0, 1}, {1, 1}, {0, 0}, {1, 0}, {0, 1}, {1, 1}, {1, 0}, {0, 0}, {0, 1}, {1, 1}, {1, 0}, {0, 0}};
+    m.idx = {0, 1, 3, 0, 3, 2, 6, 5, 7, 4, 5, 6, 10, 9, 11, 8, 9, 10, 13, 14, 15, 13, 12, 14, 18, 17, 19, 17, 16, 19, 21, 22, 23, 20, 21, 23};
+    return m;
+}
+
+// Inline triangle mesh: {"positions": [x0,y0,z0,...], "indices": [...],
+// optional "normals", "uvs"}.  Stand-in for the assimp "model" shape.
+MeshData make_inline_mesh(const Json &p) {
+    MeshData m;
+    std::vector<float> P = p["positions"].as_floats();
+    std::vector<float> Nn = p["normals"].as_floats();
+    std::vector<float> UV = p["uvs"].as_floats();
+    const Json &I = p["indices"];
+    for (size_t i = 0; i + 2 < P.size(); i += 3) m.p.push_back({P[i], P[i + 1], P[i + 2]});
+    for (size_t i = 0; i < m.p.size(); ++i) {
+        m.n.push_back(Nn.size() >= 3 * (i + 1) ? f3{Nn[3 * i], Nn[3 * i + 1], Nn[3 * i + 2]} : f3{0, 0, 0});
+        m.uv.push_back(UV.size() >= 2 * (i + 1) ? f2{UV[2 * i], UV[2 * i + 1]} : f2{0, 0});
+    }
+    for (size_t i = 0; i < I.size(); ++i) m.idx.push_back(I[i].as_uint());
+    return m;
+}
+
+// Normal-matrix transform (inverse transpose of the upper 3x3).
+f3 xform_normal(const m4 &m, f3 n) {
+    double a[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) a[r][c] = m.m[c][r];
+    double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                 a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    double inv[3][3];
+    inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) / det;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+    inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) / det;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+    inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) / det;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    // (inv)^T * n
+    return {static_cast<float>(inv[0][0] * n.x + inv[1][0] * n.y + inv[2][0] * n.z),
+            static_cast<float>(inv[0][1] * n.x + inv[1][1] * n.y + inv[2][1] * n.z),
+            static_cast<float>(inv[0][2] * n.x + inv[1][2] * n.y + inv[2][2] * n.z)};
+}
+
+struct Loader {
+    HostScene &s;
+    const float *table;
+    std::map<std::string, uint32_t> mat_by_name;
+
+    uint32_t add_spd(const float *v, int n) {
+        uint32_t off = static_cast<uint32_t>(s.spd.size());
+        s.spd.push_back(static_cast<float>(n));
+        s.spd.insert(s.spd.end(), v, v + n);
+        return off;
+    }
+
+    void load_material(const Json &m) {
+        std::string type = m["type"].as_string("diffuse");
+        std::string name = m["name"].as_string();
+        const Json &p = m["param"];
+        Material mat{};
+        mat.spd0 = mat.spd1 = kInvalid;
+        f3 rgb = make3(0.0f);
+        if (type == "diffuse") {
+            // DiffuseMaterial: colour slot, default 0.5 (diffuse.cpp:37-44).
+            mat.type = kMatDiffuse;
+            rgb = slot_rgb(p["color"], make3(0.5f));
+            float in[3] = {rgb.x, rgb.y, rgb.z};
+            rgb2spec_decode_albedo(table, in, mat.coef);
+        } else if (type == "black_body") {
+            mat.type = kMatBlackBody;
+        } else {
+            throw unsupported("material type '" + type + "' (" + name + ")");
+        }
+        mat_by_name[name] = static_cast<uint32_t>(s.materials.size());
+        s.materials.push_back(mat);
+        s.material_names.push_back(name);
+        s.material_rgb.push_back(rgb);
+    }
+
+    uint32_t black_body_material() {
+        auto it = mat_by_name.find("__black_body__");
+        if (it != mat_by_name.end()) return it->second;
+        Json j = Json::parse("{\"type\":\"black_body\",\"name\":\"__black_body__\",\"param\":{}}");
+        load_material(j);
+        return mat_by_name["__black_body__"];
+    }
+
+    void add_mesh(const MeshData &mesh, const m4 &o2w, uint32_t mat, const std::string &name, const Json *emission) {
+        uint32_t inst_id = static_cast<uint32_t>(s.instances.size());
+        uint32_t vbase = static_cast<uint32_t>(s.pos.size());
+        for (size_t i = 0; i < mesh.p.size(); ++i) {
+            s.pos.push_back(xform_point(o2w, mesh.p[i]));
+            s.nrm.push_back(is_zero(mesh.n[i]) ? mesh.n[i] : xform_normal(o2w, mesh.n[i]));
+            s.uv.push_back(mesh.uv[i]);
+        }
+        Instance inst{};
+        inst.mat_id = mat;
+        inst.light_id = kInvalid;
+        inst.first_prim = static_cast<uint32_t>(s.prim_inst.size());
+        inst.prim_count = static_cast<uint32_t>(mesh.idx.size() / 3);
+        for (size_t t = 0; t + 2 < mesh.idx.size(); t += 3) {
+            for (int k = 0; k < 3; ++k) {
+                uint32_t vi = mesh.idx[t + k];
+                if (vi >= mesh.p.size()) throw std::runtime_error("mesh '" + name + "': index out of range");
+                s.idx.push_back(vbase + vi);
+            }
+            s.prim_inst.push_back(inst_id);
+        }
+        if (emission) {
+            inst.light_id = static_cast<uint32_t>(s.lights.size());
+            add_area_light(*emission, inst_id, inst);
+        }
+        s.instances.push_back(inst);
+        s.instance_names.push_back(name);
+    }
+
+    // Light::Light (light.cpp:10-17) + AreaLight (area.cpp:33-177).
+    void add_area_light(const Json &em, uint32_t inst_id, const Instance &inst) {
+        std::string type = em["type"].as_string("area");
+        if (type != "area") throw unsupported("emission type '" + type + "'");
+        const Json &p = em["param"];
+        AreaLight L{};
+        L.inst = inst_id;
+        L.first_prim = inst.first_prim;
+        L.prim_count = inst.prim_count;
+        L.two_sided = p["two_sided"].as_bool(false) ? 1u : 0u;
+        float scale = p["scale"].is_number() ? p["scale"].as_float() : 1.0f;
+        f3 avg;
+        if (is_blackbody_slot(p["color"])) {
+            // New emitter: Planck spectrum normalised to a peak of one.
+            const Json &n = slot_node(p["color"]);
+            float T = n["param"]["temperature"].as_float(6500.0f);
+            L.kind = kEmitBlackbody;
+            L.coef[0] = T;
+            L.coef[1] = 1.0f / planck(planck_peak_nm(T), T);
+            // Average colour: linear sRGB of the normalised spectrum.
+            double xyz[3] = {0, 0, 0};
+            for (int i = 0; i < kCieSamples; ++i) {
+                double e = planck(360.0f + i, T) * L.coef[1];
+                xyz[0] += e * VS_CIE_X[i];
+                xyz[1] += e * VS_CIE_Y[i];
+                xyz[2] += e * VS_CIE_Z[i];
+            }
+            double yi = cie5().y_integral;
+            avg = xyz_to_linear_srgb(make3(float(xyz[0] / yi), float(xyz[1] / yi), float(xyz[2] / yi)));
+            s.light_rgb.push_back(avg);
+        } else {
+            f3 rgb = slot_rgb(p["color"], make3(1.0f));
+            // NumberArray::normalize (number.cpp:40-48): fold the max channel into the scale.
+            float mx = std::max(rgb.x, std::max(rgb.y, rgb.z));
+            if (mx >= 1.0f) {
+                rgb = rgb / mx;
+                scale *= mx;
+            }
+            L.kind = kEmitRGB;
+            float in[3] = {rgb.x, rgb.y, rgb.z};
+            rgb2spec_decode_unbound(table, in, L.coef);
+            avg = rgb;
+            s.light_rgb.push_back(rgb);
+        }
+        L.scale = scale;
+        L.rgb_avg[0] = avg.x * scale;
+        L.rgb_avg[1] = avg.y * scale;
+        L.rgb_avg[2] = avg.z * scale;
+        // Per-primitive alias table over world-space triangle areas.
+        std::vector<float> areas;
+        float total = 0.0f;
+        for (uint32_t t = 0; t < inst.prim_count; ++t) {
+            uint32_t pr = inst.first_prim + t;
+            f3 p0 = s.pos[s.idx[3 * pr]], p1 = s.pos[s.idx[3 * pr + 1]], p2 = s.pos[s.idx[3 * pr + 2]];
+            float a = 0.5f * length(cross(p0 - p2, p1 - p2));
+            areas.push_back(a);
+            total += a;
+        }
+        std::vector<AliasEntry> tab;
+        std::vector<float> pmf;
+        build_alias(areas, tab, pmf);
+        L.alias_offset = static_cast<uint32_t>(s.prim_alias.size());
+        s.prim_alias.insert(s.prim_alias.end(), tab.begin(), tab.end());
+        s.prim_pmf.insert(s.prim_pmf.end(), pmf.begin(), pmf.end());
+        // AreaLight::power (area.cpp:87-89).
+        f3 power = L.two_sided ? make3(2.0f) * make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]) * (total * kPi)
+                               : make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]) * (total * kPi);
+        L.lum_power = linear_srgb_to_y(power);
+        s.lights.push_back(L);
+    }
+
+    void load_shape(const Json &sh) {
+        std::string type = sh["type"].as_string();
+        std::string name = sh["name"].as_string();
+        const Json &p = sh["param"];
+        m4 o2w = parse_transform(p["transform"]);
+        MeshData mesh;
+        if (type == "quad") mesh = make_quad(p["width"].as_float(1.0f), p["height"].as_float(1.0f));
+        else if (type == "cube") mesh = make_cube(p["x"].as_float(1.0f), p["y"].as_float(1.0f), p["z"].as_float(1.0f));
+        else if (type == "mesh") mesh = make_inline_mesh(p);
+        else throw unsupported("shape type '" + type + "' (" + name + ")");
+        const Json *emission = p.contains("emission") ? &p["emission"] : nullptr;
+        uint32_t mat = kInvalid;
+        std::string mname = p["material"].as_string();
+        if (!mname.empty()) {
+            auto it = mat_by_name.find(mname);
+            if (it == mat_by_name.end()) throw std::runtime_error("shape '" + name + "': unknown material '" + mname + "'");
+            mat = it->second;
+        } else if (emission) {
+            mat = black_body_material();
+        }
+        if (mat == kInvalid) mat = black_body_material();
+        add_mesh(mesh, o2w, mat, name, emission);
+    }
+};
+
+}  // namespace
+
+void update_camera(HostScene &s, uint32_t width, uint32_t height) {
+    Camera &c = s.cam;
+    c.width = width;
+    c.height = height;
+    // RadianceCollector::update_screen_window (radiance_collector.cpp:33-42).
+    float ratio = static_cast<float>(width) / static_cast<float>(height);
+    float lo_x = -1.0f, hi_x = 1.0f, lo_y = -1.0f, hi_y = 1.0f;
+    if (ratio > 1.0f) {
+        lo_x = -ratio; hi_x = ratio;
+    } else {
+        lo_y = -1.0f / ratio; hi_y = 1.0f / ratio;
+    }
+    c.screen_lo_x = lo_x;
+    c.screen_hi_y = hi_y;
+    c.screen_span_x = hi_x - lo_x;
+    c.screen_span_y = hi_y - lo_y;
+}
+
+void load_scene_json(const std::string &text, const std::string &base_dir, const std::string &table_cache,
+                     HostScene &s) {
+    (void)base_dir;
+    Json root = Json::parse(text);
+    Loader ld{s, rgb2spec_table(table_cache), {}};
+    // Spectrum (SpectrumDesc, node_desc.cpp:346-350; hero.cpp:239).
+    const Json &sp = root["spectrum"];
+    s.spectrum_type = sp["type"].as_string("hero");
+    if (s.spectrum_type != "hero") throw unsupported("spectrum type '" + s.spectrum_type + "'");
+    s.ip.spectrum_dim = sp["param"]["dimension"].as_uint(3u);
+    if (s.ip.spectrum_dim < 1 || s.ip.spectrum_dim > 4) throw unsupported("hero dimension " + std::to_string(s.ip.spectrum_dim));
+    // Materials, then shapes (which reference materials by name).
+    for (const Json &m : root["materials"].elements()) ld.load_material(m);
+    for (const Json &sh : root["shapes"].elements()) ld.load_shape(sh);
+    if (s.prim_inst.empty()) throw std::runtime_error("scene has no primitives");
+    // Light sampler (LightSamplerDesc, node_desc.cpp:318-328).
+    const Json &lsj = root["light_sampler"];
+    std::string lst = lsj["type"].as_string("uniform");
+    if (lst == "uniform") s.ip.light_sampler = kLightSamplerUniform;
+    else if (lst == "power") s.ip.light_sampler = kLightSamplerPower;
+    else throw unsupported("light sampler '" + lst + "'");
+    for (const Json &l : lsj["param"]["lights"].elements())
+        throw unsupported("light type '" + l["type"].as_string() + "' in light_sampler");
+    s.ip.light_count = static_cast<uint32_t>(s.lights.size());
+    if (s.ip.light_count == 0) throw unsupported("scene without lights");
+    {
+        std::vector<float> w;
+        for (const AreaLight &L : s.lights) w.push_back(L.lum_power);
+        build_alias(w, s.light_alias, s.light_pmf);
+    }
+    // Integrator (IlluminationIntegrator ctor, integrator.cpp:60-67).
+    const Json &ij = root["integrator"];
+    std::string it = ij["type"].as_string("pt");
+    if (it != "pt") throw unsupported("integrator type '" + it + "'");
+    const Json &ip = ij["param"];
+    s.ip.max_depth = ip["max_depth"].as_uint(16u);
+    s.ip.min_depth = ip["min_depth"].as_uint(5u);
+    s.ip.rr_threshold = ip["rr_threshold"].as_float(1.0f);
+    s.ip.mis_mode = ip["mis_mode"].as_uint(0u);
+    // Sampler.
+    const Json &smp = root["sampler"];
+    std::string st = smp["type"].as_string("independent");
+    if (st == "independent") s.ip.sampler = kSamplerIndependent;
+    else if (st == "pcg") s.ip.sampler = kSamplerPCG;
+    else throw unsupported("sampler type '" + st + "'");
+    s.ip.seed = smp["param"]["seed"].as_uint(0u);
+    bool dispersive = false;
+    for (const Material &m : s.materials) dispersive = dispersive || (m.flags & kMatFlagDispersive);
+    s.ip.scatter_pdf_dim = dispersive ? s.ip.spectrum_dim : 1u;
+    // Camera (SensorDesc, node_desc.cpp:84-95; Sensor::init, sensor.cpp:20-26).
+    const Json &cj = root["camera"];
+    std::string ct = cj["type"].as_string("pinhole");
+    if (ct != "pinhole" && ct != "thin_lens") throw unsupported("camera type '" + ct + "'");
+    const Json &cp = cj["param"];
+    float fov = std::min(std::max(cp["fov_y"].as_float(20.0f), 15.0f), 120.0f);
+    m4 m = parse_transform(cp["transform"]);
+    float pitch = std::atan2(m.m[1][2], m.m[1][1]) * 180.0f / kPi;
+    float yaw = std::atan2(m.m[2][0], m.m[0][0]) * 180.0f / kPi;
+    f3 position = {m.m[3][0], m.m[3][1], m.m[3][2]};
+    // Sensor::camera_to_world (sensor.cpp:163-172): T * scale(1,1,-1) * Ry(yaw) * Rx(-pitch).
+    s.cam.c2w = translation(position) * scale_m(make3(1, 1, -1)) * rot_y(yaw) * rot_x(-pitch);
+    s.cam.tan_half_fov = std::tan(fov * kPi / 180.0f * 0.5f);
+    const Json &rc = cp["radiance_collector"]["param"];
+    std::vector<float> res = rc["resolution"].as_floats();
+    uint32_t w = res.size() >= 2 ? static_cast<uint32_t>(res[0]) : 1280u;
+    uint32_t h = res.size() >= 2 ? static_cast<uint32_t>(res[1]) : 720u;
+    s.cam.exposure = rc["exposure"].as_float(1.0f);
+    const Json &fj = cp["filter"];
+    std::string ft = fj["type"].as_string("box");
+    if (ft != "box") throw unsupported("filter type '" + ft + "'");
+    std::vector<float> rad = fj["param"]["radius"].as_floats();
+    s.cam.filter_rx = rad.size() >= 1 ? rad[0] : 0.5f;
+    s.cam.filter_ry = rad.size() >= 2 ? rad[1] : s.cam.filter_rx;
+    update_camera(s, w, h);
+}
+
+}  // namespace vs

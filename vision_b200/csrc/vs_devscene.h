@@ -1,0 +1,32 @@
+// Device view of an uploaded scene, passed by value as a kernel parameter.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "vs_scene.h"
+
+namespace vs {
+
+// Everything a render kernel reads, passed by value as a kernel parameter.
+struct DeviceScene {
+    const uint4 *nodes;          // Bvh8Node array (5 uint4 per node)
+    const float4 *tri_v;         // leaf-ordered triangles: 3 float4 each, w0 = prim id bits
+    const float4 *vtx;           // 2 float4 per vertex: (pos.xyz, u), (normal.xyz, v)
+    const uint4 *prims;          // per primitive: vertex indices i, j, k and instance id
+    const Instance *instances;
+    const Material *materials;
+    const AreaLight *lights;
+    const AliasEntry *prim_alias; // per-light alias tables over primitives
+    const float *prim_pmf;        // PMF of each entry of prim_alias
+    const AliasEntry *light_alias;// power light sampler
+    const float *light_pmf;
+    const float *spd;             // concatenated SPD sample arrays
+    Camera cam;
+    IntegratorParams ip;
+    uint32_t node_count;
+    uint32_t prim_count;
+    // Optional traversal counters (null in normal launches): [0] ray segments
+    // traced, [1] BVH8 nodes visited, [2] triangle tests.
+    unsigned long long *stats;
+};
+
+}  // namespace vs

@@ -1,0 +1,77 @@
+// Host-side scene representation and builders (C++17, no CUDA types).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "vs_math.h"
+#include "vs_scene.h"
+#include "vs_spectral.h"
+
+namespace vs {
+
+// Everything the kernels need, flattened: world-space vertices, primitives in
+// instance order, materials, emitters, sampling tables, sensor and integrator
+// settings.  Built from the scene JSON by load_scene_json().
+struct HostScene {
+    // Geometry (world space).
+    std::vector<f3> pos;
+    std::vector<f3> nrm;       // world-space vertex normals (not normalised)
+    std::vector<f2> uv;
+    std::vector<uint32_t> idx;  // 3 per primitive
+    std::vector<uint32_t> prim_inst;
+    std::vector<Instance> instances;
+    std::vector<std::string> instance_names;
+    // Materials.
+    std::vector<Material> materials;
+    std::vector<std::string> material_names;
+    std::vector<f3> material_rgb;  // colour slot value before the uplift
+    // Area lights (one per emissive instance) and their sampling tables.
+    std::vector<AreaLight> lights;
+    std::vector<f3> light_rgb;     // normalised colour slot value
+    std::vector<AliasEntry> prim_alias;
+    std::vector<float> prim_pmf;
+    std::vector<AliasEntry> light_alias;
+    std::vector<float> light_pmf;
+    // Spectral samples of named SPDs (metal eta/k, glass ior), concatenated.
+    std::vector<float> spd;
+    Camera cam{};
+    IntegratorParams ip{};
+    std::string spectrum_type = "hero";
+    // Compressed BVH8 over the primitives.
+    std::vector<Bvh8Node> nodes;
+    std::vector<float> tri_v;  // 12 floats per primitive in leaf order
+    uint32_t bvh_depth = 0;
+};
+
+// Parses a vision_scene.json document.  Throws std::runtime_error with a
+// message naming the offending key or plugin type.
+void load_scene_json(const std::string &text, const std::string &base_dir, const std::string &table_cache,
+                     HostScene &scene);
+
+// Sets resolution / camera-derived fields after load or on update.
+void update_camera(HostScene &scene, uint32_t width, uint32_t height);
+
+// Builds the compressed BVH8 (nodes, tri_v) from pos/idx.
+void build_bvh8(HostScene &scene);
+
+// Vose alias table with the reference's layout and float arithmetic
+// (src/render_core/warpers/alias.h:86-122); fills entries and the PMF of every
+// entry (func / (integral * size)).
+void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &entries, std::vector<float> &pmf);
+
+// RGB -> spectrum coefficient table (3 x 64^3 x float4) and its decoders.
+const float *rgb2spec_table(const std::string &cache_path);
+void rgb2spec_decode_albedo(const float *table, const float rgb[3], float out[4]);
+void rgb2spec_decode_unbound(const float *table, const float rgb[3], float out[4]);
+
+// CIE tables downsampled to the reference's 94-entry 5 nm SPDs and the CIE Y
+// integral (src/base/color/spd.cpp:14-38).
+struct Cie5 {
+    float x[kSpd5Count], y[kSpd5Count], z[kSpd5Count], d65[kSpd5Count];
+    float y_integral;
+};
+const Cie5 &cie5();
+
+}  // namespace vs

@@ -1,0 +1,260 @@
+// Per-path integrator of the megakernel: surface interaction, area-light
+// sampling, BSDF evaluation/sampling and the bounce loop of
+// IlluminationIntegrator::Li (src/base/integrator.cpp:134-283).
+#pragma once
+
+#include "vs_device.cuh"
+#include "vs_bsdf.cuh"
+
+namespace vs {
+
+// Geometry::compute_surface_interaction (src/base/mgr/geometry.cpp:78-165).
+// Positions and vertex normals are stored in world space, so the instance
+// transform of the reference is folded into the scene build.  The shading
+// frame follows PartialDerivative::update (interaction.h:87-110) and is kept
+// orthonormal.
+struct Interaction {
+    f3 pos;
+    f3 ng;
+    f3 wo;
+    Frame shading;
+    f2 uv;
+    float prim_area;
+    uint32_t prim;
+    uint32_t inst;
+    uint32_t mat;
+    uint32_t light;
+};
+
+__device__ __forceinline__ f3 ld3(const float4 &v) { return {v.x, v.y, v.z}; }
+
+__device__ __forceinline__ void load_triangle(const DeviceScene &s, uint32_t prim, uint4 &idx, float4 a[2],
+                                              float4 b[2], float4 c[2]) {
+    idx = __ldg(&s.prims[prim]);
+    a[0] = __ldg(&s.vtx[2u * idx.x]); a[1] = __ldg(&s.vtx[2u * idx.x + 1u]);
+    b[0] = __ldg(&s.vtx[2u * idx.y]); b[1] = __ldg(&s.vtx[2u * idx.y + 1u]);
+    c[0] = __ldg(&s.vtx[2u * idx.z]); c[1] = __ldg(&s.vtx[2u * idx.z + 1u]);
+}
+
+__device__ __forceinline__ Interaction surface_interaction(const DeviceScene &s, const Hit &hit, f3 ray_dir,
+                                                           bool complete) {
+    Interaction it;
+    uint4 idx;
+    float4 A[2], B[2], C[2];
+    load_triangle(s, hit.prim_id, idx, A, B, C);
+    f3 p0 = ld3(A[0]), p1 = ld3(B[0]), p2 = ld3(C[0]);
+    float w = 1.0f - hit.u - hit.v;
+    it.pos = p0 * w + p1 * hit.u + p2 * hit.v;
+    f3 dp02 = p0 - p2, dp12 = p1 - p2;
+    f3 ng_un = cross(dp02, dp12);
+    it.prim_area = 0.5f * length(ng_un);
+    it.ng = normalize(ng_un);
+    f2 uv0 = {A[0].w, A[1].w}, uv1 = {B[0].w, B[1].w}, uv2 = {C[0].w, C[1].w};
+    it.uv = {uv0.x * w + uv1.x * hit.u + uv2.x * hit.v, uv0.y * w + uv1.y * hit.u + uv2.y * hit.v};
+    it.prim = hit.prim_id;
+    it.inst = idx.w;
+    Instance inst = s.instances[idx.w];
+    it.mat = inst.mat_id;
+    it.light = inst.light_id;
+    it.wo = normalize(-ray_dir);
+    if (complete) {
+        f2 duv02 = uv0 - uv2, duv12 = uv1 - uv2;
+        float det = duv02.x * duv12.y - duv02.y * duv12.x;
+        f3 dp_dv;
+        if (fabsf(det) < 1e-8f) {
+            dp_dv = normalize(p2 - p0);
+        } else {
+            float inv_det = 1.0f / det;
+            dp_dv = (dp12 * duv02.x - dp02 * duv12.x) * inv_det;
+        }
+        f3 n = ld3(A[1]) * w + ld3(B[1]) * hit.u + ld3(C[1]) * hit.v;
+        f3 ns = is_zero(n) ? it.ng : normalize(n);
+        f3 x = normalize(cross(ns, dp_dv));
+        f3 y = normalize(cross(ns, x));
+        it.shading = {x, y, ns};
+    }
+    return it;
+}
+
+// Light sample (LightSampler::sample_wi, lightsampler.cpp:210-216 and
+// AreaLight::sample_wi, area.cpp:120-149).
+template <int N>
+struct LightSample {
+    Spec<N> L;
+    float pdf;
+    f3 p_light;
+};
+
+__device__ __forceinline__ uint32_t alias_sample(const AliasEntry *table, uint32_t size, float u,
+                                                 float *u_remapped) {
+    u = u * static_cast<float>(size);
+    uint32_t idx = min(static_cast<uint32_t>(u), size - 1u);
+    u = fminf(u - static_cast<float>(idx), kOneMinusEpsilon);
+    AliasEntry e = table[idx];
+    bool keep = u < e.prob;
+    if (u_remapped)
+        *u_remapped = keep ? fminf(u / e.prob, kOneMinusEpsilon) : fminf((1.0f - u) / (1.0f - e.prob), kOneMinusEpsilon);
+    return keep ? idx : e.alias;
+}
+
+// PDF_wi (src/math/warp.h:88-94) with the inf/nan guard of AreaLight::PDF_wi.
+__device__ __forceinline__ float pdf_wi_from_area(float pdf_pos, f3 ng, f3 w_un) {
+    float cos_t = fabsf(dot(ng, normalize(w_un)));
+    float r = pdf_pos * length_sq(w_un) / cos_t;
+    return (isinf(r) || isnan(r)) ? 0.0f : r;
+}
+
+template <int N>
+__device__ __forceinline__ float light_pmf(const DeviceScene &s, uint32_t light) {
+    if (s.ip.light_sampler == kLightSamplerPower) return s.light_pmf[light];
+    return 1.0f / static_cast<float>(s.ip.light_count);
+}
+
+template <int N>
+__device__ __forceinline__ LightSample<N> sample_light(const DeviceScene &s, const Interaction &it, float u_light,
+                                                       f2 u, const Wavelengths<N> &wl) {
+    LightSample<N> ls;
+    uint32_t n = s.ip.light_count;
+    uint32_t li;
+    float pmf_light;
+    if (s.ip.light_sampler == kLightSamplerPower) {
+        li = alias_sample(s.light_alias, n, u_light, nullptr);
+        pmf_light = s.light_pmf[li];
+    } else {
+        li = static_cast<uint32_t>(fminf(u_light * static_cast<float>(n), static_cast<float>(n) - 1.0f));
+        pmf_light = 1.0f / static_cast<float>(n);
+    }
+    AreaLight L = s.lights[li];
+    float ux = u.x;
+    uint32_t local = alias_sample(s.prim_alias + L.alias_offset, L.prim_count, u.x, &ux);
+    float pmf_prim = s.prim_pmf[L.alias_offset + local];
+    float su0 = sqrtf(ux);
+    Hit h;
+    h.prim_id = L.first_prim + local;
+    h.u = 1.0f - su0;
+    h.v = u.y * su0;
+    // LightEvalContext: position, geometric normal and area of the sampled point.
+    uint4 idx;
+    float4 A[2], B[2], C[2];
+    load_triangle(s, h.prim_id, idx, A, B, C);
+    f3 p0 = ld3(A[0]), p1 = ld3(B[0]), p2 = ld3(C[0]);
+    float w = 1.0f - h.u - h.v;
+    f3 pos = p0 * w + p1 * h.u + p2 * h.v;
+    f3 ng_un = cross(p0 - p2, p1 - p2);
+    float area = 0.5f * length(ng_un);
+    f3 ng = normalize(ng_un);
+    float pdf_pos = (1.0f / area) * pmf_prim;
+    f3 w_ref = it.pos - pos;
+    bool front = dot(w_ref, ng) > 0.0f || L.two_sided;
+    ls.L = front ? emitter_spectrum<N>(L, wl) : Spec<N>::fill(0.0f);
+    ls.pdf = pdf_wi_from_area(pdf_pos, ng, w_ref) * pmf_light;
+    f3 n_off = dot(ng, w_ref) > 0.0f ? ng : -ng;
+    ls.p_light = offset_ray_origin(pos, n_off);
+    return ls;
+}
+
+// LightSampler::evaluate_hit_wi (lightsampler.cpp:252-267) for a path that hit
+// an emissive primitive; p_ref is the ray origin.
+template <int N>
+__device__ __forceinline__ void eval_hit_light(const DeviceScene &s, const Interaction &it, f3 p_ref,
+                                               const Wavelengths<N> &wl, Spec<N> &L, float &pdf) {
+    AreaLight light = s.lights[it.light];
+    float pmf_prim = s.prim_pmf[light.alias_offset + (it.prim - light.first_prim)];
+    float pdf_pos = (1.0f / it.prim_area) * pmf_prim;
+    f3 w = p_ref - it.pos;
+    bool front = dot(w, it.ng) > 0.0f || light.two_sided;
+    L = front ? emitter_spectrum<N>(light, wl) : Spec<N>::fill(0.0f);
+    pdf = pdf_wi_from_area(pdf_pos, it.ng, w) * light_pmf<N>(s, it.light);
+}
+
+// One camera path (PathTracingIntegrator kernel body, pt.cpp:53-72, and
+// IlluminationIntegrator::Li, integrator.cpp:134-283).  Returns linear sRGB
+// radiance times the filter weight.
+template <int N>
+__device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_t frame) {
+    const IntegratorParams &ip = s.ip;
+    const Camera &cam = s.cam;
+    Sampler smp;
+    // Wavelengths come from a separate stream (RenderEnv::initial, integrator.cpp:49-58).
+    smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
+    Wavelengths<N> wl = sample_wavelengths<N>(smp.next());
+    smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
+    // Sampler::sensor_sample (sampler.h:65-73) with the box filter (box.cpp:16-20).
+    f2 uf = smp.next2();
+    float fx = lerpf(uf.x, -cam.filter_rx, cam.filter_rx);
+    float fy = lerpf(uf.y, -cam.filter_ry, cam.filter_ry);
+    (void)smp.next2();  // lens sample (unused by the pinhole)
+    (void)smp.next();   // time sample
+    float film_x = static_cast<float>(px) + 0.5f + fx;
+    float film_y = static_cast<float>(py) + 0.5f + fy;
+    // raster -> screen -> camera (Sensor::generate_ray, sensor.cpp:44-56,63-76).
+    float sx = cam.screen_lo_x + film_x / static_cast<float>(cam.width) * cam.screen_span_x;
+    float sy = cam.screen_hi_y - film_y / static_cast<float>(cam.height) * cam.screen_span_y;
+    f3 dir_cam = normalize(make3(sx * cam.tan_half_fov, sy * cam.tan_half_fov, 1.0f));
+    f3 ro = xform_point(cam.c2w, make3(0.0f));
+    f3 rd = normalize(xform_vector(cam.c2w, dir_cam));
+
+    float scatter_pdf = 1e16f;
+    Spec<N> throughput = Spec<N>::fill(1.0f);
+    f3 ret = make3(0.0f);
+    f3 prev_ng = rd;
+    float eta_scale = 1.0f;
+    const bool dispersive_pdf = ip.scatter_pdf_dim > 1;
+
+    for (uint32_t bounce = 0; bounce < ip.max_depth; ++bounce) {
+        RayPre rp = precompute_ray(ro, rd);
+        Hit hit;
+        float t_hit;
+        if (!trace_closest(s, rp, 3.402823466e+38f, hit, t_hit)) break;  // no environment light
+        Interaction it = surface_interaction(s, hit, rd, true);
+        if (it.light != kInvalid) {
+            Spec<N> Le;
+            float lpdf;
+            eval_hit_light<N>(s, it, ro, wl, Le, lpdf);
+            float weight = scatter_pdf / (scatter_pdf + lpdf);
+            if (ip.mis_mode == 2u) weight = 1.0f;
+            else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
+            ret += linear_srgb<N>(Le * throughput * weight, wl);
+        }
+        prev_ng = it.ng;
+        // Light sample: 1 draw for the light, 2 for the surface point.
+        float u_light = smp.next();
+        f2 u_surf = smp.next2();
+        LightSample<N> ls = sample_light<N>(s, it, u_light, u_surf, wl);
+        Ray sh = spawn_ray_to(it.pos, it.ng, ls.p_light);
+        bool occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
+        // Material evaluation + BSDF sample (direct_lighting, integrator.cpp:20-44).
+        Material mat = s.materials[it.mat];
+        Bsdf<N> bsdf = make_bsdf<N>(s, mat, it.shading, it.ng, it.wo, wl);
+        if (bsdf.dispersive) invalidate_secondary<N>(wl);
+        f3 wi_light = normalize(ls.p_light - it.pos);
+        BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, wl);
+        BsdfSample<N> bs = bsdf.sample(it.wo, smp, wl);
+        Spec<N> Ld = Spec<N>::fill(0.0f);
+        float w_mis = ls.pdf / (ls.pdf + se.pdf[0]);
+        if (ip.mis_mode == 1u) w_mis = 1.0f;
+        if (!occluded && se.valid(dispersive_pdf) && ls.pdf > 0.0f) {
+            Ld = ls.L * se.f * (w_mis / ls.pdf);
+        }
+        if (ip.mis_mode != 2u) ret += linear_srgb<N>(throughput * Ld, wl);
+        eta_scale *= sqr(bs.eta);
+        float lum = throughput.max();
+        if (!bs.eval.valid(dispersive_pdf) || lum == 0.0f) break;
+        throughput = throughput * bs.eval.throughput(dispersive_pdf);
+        if (eta_scale * lum < ip.rr_threshold && bounce >= ip.min_depth) {
+            float q = fminf(0.95f, lum);
+            float rr = smp.next();
+            if (q < rr) break;
+            throughput = throughput * (1.0f / q);
+        }
+        // A path whose throughput is exactly zero adds nothing from here on.
+        if (throughput.all_zero()) break;
+        scatter_pdf = bs.eval.pdf[0];
+        Ray nr = spawn_ray(it.pos, it.ng, bs.wi);
+        ro = nr.o;
+        rd = nr.d;
+    }
+    return ret;
+}
+
+}  // namespace vs

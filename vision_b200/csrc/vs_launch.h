@@ -1,0 +1,20 @@
+// Host-callable launch wrappers of the kernels in kernels.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "vs_devscene.h"
+
+namespace vs {
+
+cudaError_t upload_spectral_consts(const float *x, const float *y, const float *z, const float *d65, float y_integral);
+cudaError_t launch_trace_closest(const DeviceScene &s, const float *rays, uint32_t n, Hit *hits, float *t,
+                                 cudaStream_t st);
+cudaError_t launch_trace_any(const DeviceScene &s, const float *rays, uint32_t n, uint32_t *occ, cudaStream_t st);
+cudaError_t launch_render(const DeviceScene &s, uint32_t frame_begin, uint32_t frame_count, float4 *radiance,
+                          cudaStream_t st);
+cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count, float4 *film32,
+                        double *film64, cudaStream_t st);
+unsigned long long launch_count();
+cudaError_t launch_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out, cudaStream_t st);
+
+}  // namespace vs

@@ -1,0 +1,82 @@
+"""Procedural scenes in the reference's vision_scene.json schema.
+
+box_room(): the plain-tracer workload — a unit box room of 10 triangles
+(floor, ceiling, back, left, right walls as quads), a 0.3 x 0.6 x 0.3 box
+rotated +15 degrees and a 0.3 x 0.3 x 0.3 box rotated -18 degrees about y
+(12 triangles each, the `cube` shape), a 0.25 x 0.25 ceiling quad light, a
+pinhole camera with fov_y 40, 256 x 256, 16 spp, max depth 8 and 4 hero
+wavelengths.  The light is a 6500 K blackbody scaled to radiance 17, or its
+RGB twin [17, 17, 17] (the reference's own illumination slot) when
+rgb_light=True.
+"""
+import math
+
+LEFT_RGB = [0.63, 0.065, 0.05]
+RIGHT_RGB = [0.14, 0.45, 0.091]
+GREY_RGB = [0.725, 0.725, 0.725]
+
+
+def _cols(c0, c1, c2, t):
+    """matrix4x4 in the schema's column order (fourth column = translation)."""
+    return {"type": "matrix4x4", "param": {"matrix4x4": [list(c0) + [0.0], list(c1) + [0.0], list(c2) + [0.0],
+                                                         list(t) + [1.0]]}}
+
+
+def _ry(deg, t):
+    a = math.radians(deg)
+    c, s = math.cos(a), math.sin(a)
+    return _cols((c, 0.0, -s), (0.0, 1.0, 0.0), (s, 0.0, c), t)
+
+
+def box_room(width=256, height=256, max_depth=8, min_depth=5, rr_threshold=1.0, dimension=4,
+             sampler="independent", seed=0, rgb_light=False, light_scale=17.0):
+    quad = lambda name, mat, xf, w=1.0, h=1.0: {"type": "quad", "name": name,
+                                                 "param": {"width": w, "height": h, "material": mat, "transform": xf}}
+    shapes = [
+        quad("floor", "Floor", _cols((1, 0, 0), (0, 1, 0), (0, 0, 1), (0, 0, 0))),
+        quad("ceiling", "Ceiling", _cols((1, 0, 0), (0, -1, 0), (0, 0, -1), (0, 1, 0))),
+        quad("back", "BackWall", _cols((1, 0, 0), (0, 0, 1), (0, -1, 0), (0, 0.5, -0.5))),
+        quad("left", "LeftWall", _cols((0, -1, 0), (1, 0, 0), (0, 0, 1), (-0.5, 0.5, 0))),
+        quad("right", "RightWall", _cols((0, 1, 0), (-1, 0, 0), (0, 0, 1), (0.5, 0.5, 0))),
+        {"type": "cube", "name": "tall_box",
+         "param": {"x": 0.3, "y": 0.6, "z": 0.3, "material": "TallBox", "transform": _ry(15.0, (-0.17, 0.3, -0.13))}},
+        {"type": "cube", "name": "short_box",
+         "param": {"x": 0.3, "y": 0.3, "z": 0.3, "material": "ShortBox", "transform": _ry(-18.0, (0.17, 0.15, 0.12))}},
+    ]
+    if rgb_light:
+        color = {"channels": "xyz", "node": [light_scale] * 3}
+        scale = 1.0
+    else:
+        color = {"channels": "xyz", "node": {"type": "blackbody", "param": {"temperature": 6500.0}}}
+        scale = light_scale
+    shapes.append({"type": "quad", "name": "light",
+                   "param": {"width": 0.25, "height": 0.25, "material": "Light",
+                             "transform": _cols((1, 0, 0), (0, -1, 0), (0, 0, -1), (0, 0.999, 0)),
+                             "emission": {"type": "area", "param": {"color": color, "scale": scale,
+                                                                    "two_sided": False}}}})
+    materials = [
+        {"type": "diffuse", "name": "Floor", "param": {"color": GREY_RGB}},
+        {"type": "diffuse", "name": "Ceiling", "param": {"color": GREY_RGB}},
+        {"type": "diffuse", "name": "BackWall", "param": {"color": GREY_RGB}},
+        {"type": "diffuse", "name": "LeftWall", "param": {"color": LEFT_RGB}},
+        {"type": "diffuse", "name": "RightWall", "param": {"color": RIGHT_RGB}},
+        {"type": "diffuse", "name": "TallBox", "param": {"color": GREY_RGB}},
+        {"type": "diffuse", "name": "ShortBox", "param": {"color": GREY_RGB}},
+        {"type": "black_body", "name": "Light", "param": {}},
+    ]
+    return {
+        "shapes": shapes,
+        "materials": materials,
+        "camera": {"type": "pinhole", "param": {
+            "fov_y": 40.0,
+            "transform": {"type": "look_at", "param": {"position": [0.0, 0.5, 1.85], "target_pos": [0.0, 0.5, 0.0],
+                                                       "up": [0.0, 1.0, 0.0]}},
+            "radiance_collector": {"type": "normal", "param": {"resolution": [width, height], "exposure": 1.0}},
+            "filter": {"type": "box", "param": {"radius": [0.5, 0.5]}}}},
+        "integrator": {"type": "pt", "param": {"max_depth": max_depth, "min_depth": min_depth,
+                                               "rr_threshold": rr_threshold}},
+        "spectrum": {"type": "hero", "param": {"dimension": dimension}},
+        "sampler": {"type": sampler, "param": {"seed": seed}},
+        "light_sampler": {"type": "uniform", "param": {"lights": []}},
+        "render_setting": {"polymorphic_mode": 1},
+    }
