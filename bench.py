@@ -151,7 +151,7 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--steps', type=int, default=100)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='box_room', choices=sorted(WORKLOADS))
@@ -182,7 +182,11 @@ def main():
     spp = w['spp']
     npix = w['width'] * w['height']
     paths_per_step = npix * spp
-    stream = torch.cuda.current_stream().cuda_stream
+    # A dedicated stream: the library and the CUDA events must share it (the
+    # legacy default stream does not order against the library's own stream).
+    torch_stream = torch.cuda.Stream()
+    torch.cuda.set_stream(torch_stream)
+    stream = torch_stream.cuda_stream
 
     # Algorithmic bytes per path (B_path = 32 + sum over segments of
     # 80 N_node + 36 N_tri + 180), from an instrumented render outside the timing.

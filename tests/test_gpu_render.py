@@ -40,7 +40,10 @@ def test_independent_seeds_agree_statistically(vb, gpu_ctx):
     s, o = _pair(vb, gpu_ctx, width=32, height=32)
     s.render(0, 64, fp64=True)
     g = s.film(vb.FILM_SUM64)[..., :3] / 64.0
-    c = o.render(64, 64)[..., :3]
+    # The FP32 film is a running mean over the frame index (frames 64.. would
+    # be averaged with 64 empty frames), so compare the FP64 sums.
+    _, c64 = o.render(64, 64, fp64=True)
+    c = c64[..., :3] / 64.0
     gb = g.reshape(4, 8, 4, 8, 3).mean((1, 3))
     cb = c.reshape(4, 8, 4, 8, 3).mean((1, 3))
     rel = np.abs(gb - cb) / (0.5 * (gb + cb) + 1e-3)
