@@ -164,6 +164,20 @@ int vs_timing_read(vs_scene *scene, double *render_ms, double *film_ms, uint32_t
  * triangle tests.  Synchronous; used to size the algorithmic bytes per path. */
 int vs_render_stats(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, uint64_t *out3);
 
+/* Allocation-free render for callers that cannot call cudaMalloc at render
+ * time (a frame loop inside a fixed memory budget, an embedding application
+ * whose allocator owns device memory).  No counterpart in the reference: it
+ * is vs_render with the film in `film` (caller-owned device memory, float4
+ * per pixel, holding the running mean of frames [0, frame_begin) when
+ * frame_begin > 0) and the per-path radiance in a fixed 16 MiB array inside
+ * the library, so it calls no cudaMalloc, cudaFree or allocating library
+ * routine.  The first call on a device looks up that array's device address;
+ * make it before any stream capture.  Resolutions above 1048576 pixels return
+ * VS_E_RANGE.  All calls share the one array: calls that overlap on the GPU
+ * (other streams, other threads) race and must be serialised by the caller.
+ * The scene must have been built with vs_scene_build_accel. */
+int vs_render_noalloc(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, float *film, void *stream);
+
 /* RGB -> sigmoid coefficients with the uplift table (reference
  * RGBToSpectrumTable::decode_albedo / decode_unbound, hero.cpp:92-141).
  * mode 0 = albedo (out[3] = luminance), 1 = unbound (out[3] = scale). */

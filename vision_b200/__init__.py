@@ -88,6 +88,7 @@ def _load():
         'vs_render_stats': ([P, U32, U32, P], ctypes.c_int),
         'vs_timing_enable': ([P, ctypes.c_int], ctypes.c_int),
         'vs_timing_read': ([P, P, P, P], ctypes.c_int),
+        'vs_render_noalloc': ([P, U32, U32, P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -104,7 +105,7 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_scene_info_get', 'vs_scene_export_size', 'vs_scene_export', 'vs_render', 'vs_synchronize',
                       'vs_film_download', 'vs_trace_closest_device', 'vs_trace_closest_host', 'vs_trace_any_device',
                       'vs_trace_any_host', 'vs_rgb_to_spectrum', 'vs_launch_count', 'vs_render_stats', 'vs_timing_enable',
-                      'vs_timing_read'])
+                      'vs_timing_read', 'vs_render_noalloc'])
 
 
 def launch_count():

@@ -182,6 +182,24 @@ int ensure_film(vs_scene *s) {
 
 }  // namespace
 
+namespace vs {
+
+int noalloc_prepare(vs_scene *s, void *stream, DeviceScene *view, cudaStream_t *st, int *device) {
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render_noalloc");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    *view = s->device_view();
+    *st = pick_stream(s, stream);
+    *device = ctx->device;
+    return VS_OK;
+}
+
+int noalloc_fail(vs_scene *s, int code, const char *msg) { return fail(s->ctx, code, msg); }
+
+}  // namespace vs
+
 extern "C" {
 
 int vs_version(void) { return 100; }
