@@ -122,6 +122,7 @@ int vs_scene_info_get(const vs_scene *scene, vs_scene_info *out);
 #define VS_EXPORT_LIGHT_RGB 16  /* float[3] per light */
 #define VS_EXPORT_BVH_NODES 17  /* 80 bytes per node */
 #define VS_EXPORT_BVH_TRIS 18   /* float[12] per primitive in leaf order */
+#define VS_EXPORT_LUTS 19       /* float albedo tables of the compensated lobes (empty if unused) */
 int vs_scene_export_size(const vs_scene *scene, int what, size_t *bytes);
 int vs_scene_export(const vs_scene *scene, int what, void *dst, size_t bytes);
 
@@ -177,6 +178,13 @@ int vs_render_stats(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count,
  * (other streams, other threads) race and must be serialised by the caller.
  * The scene must have been built with vs_scene_build_accel. */
 int vs_render_noalloc(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, float *film, void *stream);
+
+/* Albedo tables of the energy-compensated lobes (164864 floats: PureReflection
+ * 32^2, Dielectric and DielectricInv 32^3 x 2, Specular 32^3).  which = 0: the
+ * values the renderer uses (the reference's precomputed_table.h); which = 1:
+ * the same tables regenerated from the lobe definitions (apps/precompute's
+ * job), cached in cache_path.  No device work. */
+int vs_albedo_luts(int which, const char *cache_path, float *out, size_t count);
 
 /* RGB -> sigmoid coefficients with the uplift table (reference
  * RGBToSpectrumTable::decode_albedo / decode_unbound, hero.cpp:92-141).

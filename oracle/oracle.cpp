@@ -581,31 +581,462 @@ static LS sample_light(const Scene &sc, const It &it, float ul, float ux, float 
     return ls;
 }
 
-// ----- BSDF (diffuse.cpp, bxdf.cpp:30-52, lobe.cpp:240-250, material.cpp:132-184) ---
-constexpr uint32_t kRefl = 2, kTrans = 4, kDiffRefl = 8 | 2, kUnset = 1;
+// ----- BSDFs ------------------------------------------------------------------
+// Materials: diffuse (diffuse.cpp), black_body (black_body.cpp), metal
+// (metal.cpp + ConductorLobe/PureReflectionLobe, lobe.cpp:716-735), glass
+// (glass.cpp + DielectricLobe, lobe.cpp:253-450), principled_bsdf
+// (principled_bsdf.cpp:352-461, with zero sheen/coat/transmission weights).
+// Everything is evaluated in world space through per-lobe local frames the way
+// MaterialEvaluator::evaluate/sample do with individual shading normals
+// (material.cpp:132-184).
+constexpr uint32_t kRefl = 2, kTrans = 4, kDiffRefl = 8 | 2, kGlossyRefl = 16 | 2, kGlossyTrans = 16 | 4, kUnset = 1;
+
+namespace mf {
+// microfacet.cpp / microfacet.h, GGX with visible-normal sampling.
+static float D(V3 h, float ax, float ay) {
+    float x = h.x / ax, y = h.y / ay, z = h.z;
+    float l2 = x * x + y * y + z * z;
+    return kInvPi / (ax * ay * (l2 * l2));
+}
+static float lambda(V3 w, float ax, float ay) {
+    if (w.z == 0.0f) return 0.0f;
+    float t = ((ax * w.x) * (ax * w.x) + (ay * w.y) * (ay * w.y)) / (w.z * w.z);
+    return 0.5f * (std::sqrt(1.0f + t) - 1.0f);
+}
+static float G1(V3 w, float ax, float ay) { return 1.0f / (1.0f + lambda(w, ax, ay)); }
+static float G(V3 a, V3 b, float ax, float ay) { return 1.0f / (1.0f + lambda(a, ax, ay) + lambda(b, ax, ay)); }
+static V3 sample_wh(V3 wo, float u0, float u1, float ax, float ay) {
+    bool flip = wo.z < 0.0f;
+    V3 ve = flip ? neg(wo) : wo;
+    V3 vh = normalize(v3(ax * ve.x, ay * ve.y, ve.z));
+    float ls = vh.x * vh.x + vh.y * vh.y;
+    V3 t1 = ls > 1e-7f ? mul(v3(-vh.y, vh.x, 0.0f), 1.0f / std::sqrt(ls)) : v3(1, 0, 0);
+    V3 t2 = ls > 1e-7f ? cross(vh, t1) : v3(0, 1, 0);
+    float r = std::sqrt(u0), th = 2.0f * kPi * u1;
+    float tx = r * std::cos(th), ty = r * std::sin(th);
+    float sw = 0.5f * (1.0f + vh.z);
+    float a = std::sqrt(std::max(0.0f, 1.0f - tx * tx));
+    ty = a + sw * (ty - a);
+    V3 nh = add(add(mul(t1, tx), mul(t2, ty)), mul(vh, std::sqrt(std::max(0.0f, 1.0f - (tx * tx + ty * ty)))));
+    V3 ne = normalize(v3(ax * nh.x, ay * nh.y, std::max(0.0f, nh.z)));
+    return flip ? neg(ne) : ne;
+}
+static float pdf_wh(V3 wo, V3 h, float ax, float ay) {
+    return D(h, ax, ay) * G1(wo, ax, ay) * std::fabs(dot(wo, h)) / std::fabs(wo.z);
+}
+static float pdf_refl(V3 wo, V3 h, float ax, float ay) { return pdf_wh(wo, h, ax, ay) / (4.0f * std::fabs(dot(wo, h))); }
+static float pdf_trans(V3 wo, V3 h, V3 wi, float eta, float ax, float ay) {
+    float d = dot(wi, h) * eta + dot(wo, h);
+    return pdf_wh(wo, h, ax, ay) * (std::fabs(dot(wi, h)) / (d * d));
+}
+static float brdf(V3 wo, V3 h, V3 wi, float ax, float ay) {
+    return D(h, ax, ay) * G(wo, wi, ax, ay) / std::fabs(4.0f * wo.z * wi.z);
+}
+static float btdf(V3 wo, V3 h, V3 wi, float eta, float ax, float ay) {
+    float num = D(h, ax, ay) * G(wo, wi, ax, ay) * std::fabs(dot(wi, h) * dot(wo, h));
+    float d = dot(wi, h) * eta + dot(wo, h);
+    float den = d * d * std::fabs(wi.z * wo.z);
+    float ft = den == 0.0f ? 0.0f : num / den;
+    return ft * (1.0f / (eta * eta));  // radiance transport
+}
+static V3 reflect(V3 wo, V3 n) { return add(neg(wo), mul(n, 2.0f * dot(wo, n))); }
+static bool refract(V3 wi, V3 n, float eta, V3 &wt) {
+    float ci = dot(n, wi);
+    float s2i = std::max(0.0f, 1.0f - ci * ci);
+    float s2t = s2i / (eta * eta);
+    float ct = std::sqrt(std::max(0.0f, 1.0f - s2t));
+    wt = add(mul(wi, -1.0f / eta), mul(n, ci / eta - ct));
+    return s2t < 1.0f;
+}
+static float fr_dielectric(float c, float eta) {
+    float s2i = 1.0f - c * c;
+    float s2t = s2i / (eta * eta);
+    float ct = std::sqrt(std::max(0.0f, 1.0f - s2t));
+    float rp = (eta * c - ct) / (eta * c + ct);
+    float rs = (c - eta * ct) / (c + eta * ct);
+    return s2t >= 1.0f ? 1.0f : (rp * rp + rs * rs) * 0.5f;
+}
+// fresnel_complex with Complex<> of src/math/complex.h.
+static float fr_conductor(float c, float eta, float k) {
+    auto mulc = [](float ar, float ai, float br, float bi, float &r, float &i) { r = ar * br - ai * bi; i = ar * bi + ai * br; };
+    auto divc = [](float ar, float ai, float br, float bi, float &r, float &i) {
+        float s = 1.0f / (br * br + bi * bi);
+        r = s * (ar * br + ai * bi);
+        i = s * (ai * br - ar * bi);
+    };
+    float e2r, e2i;
+    mulc(eta, k, eta, k, e2r, e2i);
+    float s2r, s2i;
+    divc(1.0f - c * c, 0.0f, e2r, e2i, s2r, s2i);
+    float zr = 1.0f - s2r, zi = -s2i;
+    float n = std::sqrt(zr * zr + zi * zi);
+    float t1 = std::sqrt(0.5f * (n + std::fabs(zr)));
+    float t2 = 0.5f * zi / t1;
+    float ctr = n == 0.0f ? 0.0f : (zr >= 0.0f ? t1 : std::fabs(t2));
+    float cti = n == 0.0f ? 0.0f : (zr >= 0.0f ? t2 : std::copysign(t1, zi));
+    float ecr = eta * c, eci = k * c;
+    float pr, pi;
+    divc(ecr - ctr, eci - cti, ecr + ctr, eci + cti, pr, pi);
+    float ectr, ecti;
+    mulc(eta, k, ctr, cti, ectr, ecti);
+    float sr, si;
+    divc(c - ectr, -ecti, c + ectr, ecti, sr, si);
+    return ((pr * pr + pi * pi) + (sr * sr + si * si)) * 0.5f;
+}
+}  // namespace mf
+
+#include "../vision_b200/csrc/data/albedo_luts.inc"
+
+// MaterialLut::sample: normalised coordinates, linear filter, clamp to edge.
+static float lut_axis(float u, int &i0, int &i1) {
+    float x = u * 32.0f - 0.5f;
+    float fl = std::floor(x);
+    int i = static_cast<int>(fl);
+    i0 = std::min(std::max(i, 0), 31);
+    i1 = std::min(std::max(i + 1, 0), 31);
+    return x - fl;
+}
+static float lut2(const float *t, float u, float v) {
+    int x0, x1, y0, y1;
+    float fx = lut_axis(u, x0, x1), fy = lut_axis(v, y0, y1);
+    float a = t[y0 * 32 + x0] + fx * (t[y0 * 32 + x1] - t[y0 * 32 + x0]);
+    float b = t[y1 * 32 + x0] + fx * (t[y1 * 32 + x1] - t[y1 * 32 + x0]);
+    return a + fy * (b - a);
+}
+static float lut3(const float *t, int ch, float u, float v, float w) {
+    int x0, x1, y0, y1, z0, z1;
+    float fx = lut_axis(u, x0, x1), fy = lut_axis(v, y0, y1), fz = lut_axis(w, z0, z1);
+    auto at = [&](int x, int y, int z) { return t[((z * 32 + y) * 32 + x) * ch]; };
+    float c00 = at(x0, y0, z0) + fx * (at(x1, y0, z0) - at(x0, y0, z0));
+    float c10 = at(x0, y1, z0) + fx * (at(x1, y1, z0) - at(x0, y1, z0));
+    float c01 = at(x0, y0, z1) + fx * (at(x1, y0, z1) - at(x0, y0, z1));
+    float c11 = at(x0, y1, z1) + fx * (at(x1, y1, z1) - at(x0, y1, z1));
+    float c0 = c00 + fy * (c10 - c00), c1 = c01 + fy * (c11 - c01);
+    return c0 + fz * (c1 - c0);
+}
+static const float *kLutPure = VS_ALBEDO_LUTS;
+static const float *kLutDiel = VS_ALBEDO_LUTS + 1024;
+static const float *kLutDielInv = VS_ALBEDO_LUTS + 1024 + 65536;
+static const float *kLutSpec = VS_ALBEDO_LUTS + 1024 + 131072;
+
 struct Eval {
     float f[8];
     float pdf;
     uint32_t flags;
 };
-static Eval bsdf_eval(const Material &m, const float *kr, int n, const Frame &fr, V3 ng, V3 wo_w, V3 wi_w) {
-    Eval e;
-    V3 wo = fr.to_local(wo_w), wi = fr.to_local(wi_w);
-    if (m.type == 0) {
-        bool s = wo.z * wi.z > 0.0f;
-        float ac = std::fabs(wi.z);
-        for (int i = 0; i < n; ++i) e.f[i] = s ? kr[i] * (kInvPi * ac) : 0.0f;
-        e.pdf = s ? ac * kInvPi : 0.0f;
-        e.flags = kDiffRefl;
-    } else {
-        for (int i = 0; i < n; ++i) e.f[i] = 0.0f;
-        e.pdf = 1.0f;
-        e.flags = kUnset;
+
+// A lobe of the material's lobe set.
+struct Lobe {
+    enum Kind { Lambert, MicrofacetRefl, Dielectric, NoScatter } kind;
+    enum Fr { Conductor, Schlick, F82, One } fresnel = One;
+    float ax = 1, ay = 1;
+    bool compensate = false;
+    float kr[8], fa[8], fb[8];
+    float eta0 = 1.0f;
+    float eta[8];
+    float sample_weight = 1.0f;
+};
+
+struct Bsdf {
+    int n = 1;
+    Frame fr;
+    V3 ng;
+    Lobe lobes[3];
+    int count = 0;
+    bool lobe_set = false;  // LobeSet: world-space hemisphere factors and a 1D lobe choice
+    bool dispersive = false;
+};
+
+static void fresnel_eval(const Lobe &l, int n, float c, float *F) {
+    for (int i = 0; i < n; ++i) {
+        if (l.fresnel == Lobe::Conductor) F[i] = mf::fr_conductor(c, l.fa[i], l.fb[i]);
+        else if (l.fresnel == Lobe::Schlick) {
+            float fr = mf::fr_dielectric(c, l.eta0);
+            float f0 = ((l.eta0 - 1.0f) / (l.eta0 + 1.0f)) * ((l.eta0 - 1.0f) / (l.eta0 + 1.0f));
+            float t = std::min(std::max((fr - f0) / (1.0f - f0), 0.0f), 1.0f);
+            F[i] = l.fa[i] + t * (1.0f - l.fa[i]);
+        } else if (l.fresnel == Lobe::F82) {
+            float mu = std::min(std::max(1.0f - c, 0.0f), 1.0f);
+            float mu5 = mu * mu * mu * mu * mu;
+            float fs = l.fa[i] + mu5 * (1.0f - l.fa[i]);
+            F[i] = std::min(std::max(fs - l.fb[i] * c * mu5 * mu, 0.0f), 1.0f);
+        } else {
+            F[i] = 1.0f;
+        }
     }
-    bool same = dot(wo_w, ng) * dot(wi_w, ng) > 0.0f;
-    bool trans = (e.flags & kTrans) != 0;
-    if (same == trans) e.pdf = 0.0f;
+}
+
+// Local evaluation of one lobe: f (without the cosine), pdf, flags.
+static void lobe_eval(const Lobe &l, int n, V3 wo, V3 wi, float *f, float &pdf, uint32_t &flags, float &eta_out) {
+    eta_out = 1.0f;
+    if (l.kind == Lobe::Lambert) {
+        bool s = wo.z * wi.z > 0.0f;
+        for (int i = 0; i < n; ++i) f[i] = s ? l.kr[i] * kInvPi : 0.0f;
+        pdf = s ? std::fabs(wi.z) * kInvPi : 0.0f;
+        flags = kDiffRefl;
+    } else if (l.kind == Lobe::MicrofacetRefl) {
+        flags = kGlossyRefl;
+        if (!(wo.z * wi.z > 0.0f)) {
+            for (int i = 0; i < n; ++i) f[i] = 0.0f;
+            pdf = 0.0f;
+            return;
+        }
+        V3 h = normalize(add(wo, wi));
+        V3 hf = h.z < 0.0f ? neg(h) : h;
+        float F[8];
+        fresnel_eval(l, n, std::fabs(dot(wo, hf)), F);
+        float b = mf::brdf(wo, hf, wi, l.ax, l.ay);
+        float comp = l.compensate ? 1.0f / lut2(kLutPure, std::sqrt(l.ax * l.ay), wo.z) : 1.0f;
+        for (int i = 0; i < n; ++i) f[i] = b * F[i] * l.kr[i] * comp;
+        pdf = mf::pdf_refl(wo, h, l.ax, l.ay);
+    } else if (l.kind == Lobe::Dielectric) {
+        bool refl = wo.z * wi.z > 0.0f;
+        float e0 = l.eta[0];
+        float ep = refl ? 1.0f : e0;
+        eta_out = ep;
+        V3 h = normalize(add(wo, mul(wi, ep)));
+        if (dot(h, wo) < 0.0f) h = neg(h);
+        float F[8], T[8];
+        for (int i = 0; i < n; ++i) F[i] = mf::fr_dielectric(std::fabs(dot(h, wo)), l.eta[i]);
+        float sf = 0, st = 0;
+        for (int i = 0; i < n; ++i) {
+            sf += F[i];
+            st += (1.0f - F[i]) * l.kr[i] + F[i];
+        }
+        float pr = (sf / n) / (st / n);
+        float e = e0 > 1.0f ? e0 : 1.0f / e0;
+        float comp = 1.0f / lut3(e0 > 1.0f ? kLutDiel : kLutDielInv, 2, std::sqrt(std::sqrt(l.ax * l.ay)),
+                                 std::fabs(wo.z), (e - 1.003f) / (5.0f - 1.003f));
+        if (refl) {
+            float b = mf::brdf(wo, h, wi, l.ax, l.ay);
+            for (int i = 0; i < n; ++i) f[i] = F[i] * b * comp;
+            pdf = mf::pdf_refl(wo, h, l.ax, l.ay) * pr;
+            flags = kGlossyRefl;
+        } else {
+            V3 h2 = normalize(add(wo, mul(wi, e0)));
+            float bt = mf::btdf(wo, h2, wi, e0, l.ax, l.ay);
+            for (int i = 0; i < n; ++i) {
+                T[i] = (1.0f - F[i]) * l.kr[i];
+                f[i] = T[i] * bt * comp;
+            }
+            pdf = mf::pdf_trans(wo, h, wi, e0, l.ax, l.ay) * (1.0f - pr);
+            flags = kGlossyTrans;
+        }
+    } else {
+        for (int i = 0; i < n; ++i) f[i] = 0.0f;
+        pdf = 1.0f;
+        flags = kUnset;
+    }
+}
+
+// MaterialEvaluator::evaluate with individual shading normals.
+static Eval bsdf_eval(const Bsdf &b, V3 wo_w, V3 wi_w, float *eta_out) {
+    Eval e;
+    V3 wo = b.fr.to_local(wo_w), wi = b.fr.to_local(wi_w);
+    float ac = std::fabs(wi.z);
+    float eta = 1.0f;
+    if (!b.lobe_set) {
+        lobe_eval(b.lobes[0], b.n, wo, wi, e.f, e.pdf, e.flags, eta);
+        for (int i = 0; i < b.n; ++i) e.f[i] *= ac;
+    } else {
+        for (int i = 0; i < b.n; ++i) e.f[i] = 0.0f;
+        e.pdf = 0.0f;
+        e.flags = 0;
+        bool same = wo.z * wi.z > 0.0f;
+        for (int k = 0; k < b.count; ++k) {
+            const Lobe &l = b.lobes[k];
+            float f[8], p;
+            uint32_t fl;
+            float et;
+            lobe_eval(l, b.n, wo, wi, f, p, fl, et);
+            float factor = (l.kind == Lobe::Dielectric || same) ? 1.0f : 0.0f;
+            for (int i = 0; i < b.n; ++i) e.f[i] += f[i] * ac * factor;
+            e.pdf += p * l.sample_weight * factor;
+            e.flags |= fl;
+            if (l.kind == Lobe::Dielectric) eta = et;
+        }
+    }
+    if (eta_out) *eta_out = eta;
+    bool same_g = dot(wo_w, b.ng) * dot(wi_w, b.ng) > 0.0f;
+    if (same_g == ((e.flags & kTrans) != 0)) e.pdf = 0.0f;
     return e;
+}
+
+static V3 lobe_sample(const Lobe &l, int n, V3 wo, Sampler &smp, bool &valid) {
+    valid = true;
+    if (l.kind == Lobe::Lambert) {
+        float u0 = smp.next(), u1 = smp.next();
+        float r = std::sqrt(u0), th = 2.0f * kPi * u1;
+        float dx = r * std::cos(th), dy = r * std::sin(th);
+        float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
+        return {dx, dy, wo.z < 0.0f ? -z : z};
+    }
+    if (l.kind == Lobe::MicrofacetRefl) {
+        float u0 = smp.next(), u1 = smp.next();
+        V3 h = mf::sample_wh(wo, u0, u1, l.ax, l.ay);
+        V3 wi = mf::reflect(wo, h);
+        valid = wo.z * wi.z > 0.0f;
+        return wi;
+    }
+    // Dielectric: microfacet normal (2D), then reflect/refract choice (1D).
+    float u0 = smp.next(), u1 = smp.next();
+    V3 h = mf::sample_wh(wo, u0, u1, l.ax, l.ay);
+    float F[8], sf = 0, st = 0;
+    for (int i = 0; i < n; ++i) {
+        F[i] = mf::fr_dielectric(std::fabs(dot(wo, h)), l.eta[i]);
+        sf += F[i];
+        st += (1.0f - F[i]) * l.kr[i] + F[i];
+    }
+    float uc = smp.next();
+    V3 wi;
+    if (uc < (sf / n) / (st / n)) {
+        wi = mf::reflect(wo, h);
+        valid = wo.z * wi.z > 0.0f;
+    } else {
+        bool ok = mf::refract(wo, h, l.eta[0], wi);
+        valid = ok && !(wo.z * wi.z > 0.0f);
+    }
+    return wi;
+}
+
+// Lobe::sample / LobeSet::sample_wi_impl + MaterialEvaluator::sample.
+static Eval bsdf_sample(const Bsdf &b, V3 wo_w, Sampler &smp, V3 &wi_w, float &eta, bool no_scatter) {
+    Eval e;
+    if (no_scatter) {
+        wi_w = wo_w;
+        for (int i = 0; i < b.n; ++i) e.f[i] = 0.0f;
+        e.pdf = 1.0f;
+        e.flags = kDiffRefl;
+        eta = 1.0f;
+        return e;
+    }
+    V3 wo = b.fr.to_local(wo_w);
+    bool valid;
+    V3 wi;
+    if (!b.lobe_set) {
+        wi = lobe_sample(b.lobes[0], b.n, wo, smp, valid);
+    } else {
+        float uc = smp.next();
+        smp.next();
+        smp.next();
+        int strategy = 0;
+        float sum = 0.0f;
+        for (int k = 0; k < b.count; ++k) {
+            if (uc > sum) strategy = k;
+            sum += b.lobes[k].sample_weight;
+        }
+        wi = lobe_sample(b.lobes[strategy], b.n, wo, smp, valid);
+    }
+    wi_w = b.fr.to_world(wi);
+    e = bsdf_eval(b, wo_w, wi_w, &eta);
+    if (!valid) e.pdf = 0.0f;
+    return e;
+}
+
+static float spd_of(const float *spd, uint32_t off, float lambda) {
+    return spd_eval(spd + off + 1, static_cast<int>(spd[off]), lambda);
+}
+
+// Material::create_evaluator for the supported plugins.
+static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Swl &w) {
+    Bsdf b;
+    b.n = w.n;
+    b.fr = it.sh;
+    b.ng = it.ng;
+    b.dispersive = (m.flags & 1u) != 0;
+    Lobe &l0 = b.lobes[0];
+    b.count = 1;
+    if (m.type == 0) {
+        l0.kind = Lobe::Lambert;
+        for (int i = 0; i < w.n; ++i) l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
+    } else if (m.type == 2) {  // metal: ConductorLobe
+        l0.kind = Lobe::MicrofacetRefl;
+        l0.fresnel = Lobe::Conductor;
+        l0.compensate = true;
+        l0.ax = m.p[0];
+        l0.ay = m.p[1];
+        for (int i = 0; i < w.n; ++i) {
+            l0.kr[i] = 1.0f;
+            l0.fa[i] = spd_of(sc.s->spd, m.spd0, w.lambda[i]);
+            l0.fb[i] = spd_of(sc.s->spd, m.spd1, w.lambda[i]);
+        }
+    } else if (m.type == 3) {  // glass: DielectricLobe
+        l0.kind = Lobe::Dielectric;
+        l0.ax = m.p[0];
+        l0.ay = m.p[1];
+        bool front = dot(it.wo, it.ng) > 0.0f;  // Interaction::correct_eta
+        for (int i = 0; i < w.n; ++i) {
+            l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
+            float ior = m.spd0 != kInvalid ? spd_of(sc.s->spd, m.spd0, w.lambda[i]) : m.p[2];
+            l0.eta[i] = front ? ior : 1.0f / ior;
+        }
+    } else if (m.type == 4) {  // principled_bsdf: metallic, specular, diffuse
+        b.lobe_set = true;
+        int n = w.n;
+        float ax = m.p[0], ay = m.p[1], metallic = m.p[2], ior = m.p[3];
+        float color[8], tint[8], weight[8];
+        const float tc[3] = {m.p[4], m.p[5], m.p[6]};
+        for (int i = 0; i < n; ++i) {
+            color[i] = sigmoid_poly(m.coef, w.lambda[i]);
+            tint[i] = sigmoid_poly(tc, w.lambda[i]);
+            weight[i] = 1.0f;
+        }
+        float cos_theta = dot(it.wo, it.ng);
+        float front = cos_theta > 0.0f ? 1.0f : 0.0f;
+        auto mean = [&](const float *v) {
+            float a = 0;
+            for (int i = 0; i < n; ++i) a += v[i];
+            return a * (1.0f / n);
+        };
+        Lobe met;
+        met.kind = Lobe::MicrofacetRefl;
+        met.fresnel = Lobe::F82;
+        met.compensate = true;
+        met.ax = ax;
+        met.ay = ay;
+        float mm = metallic * front;
+        const float f = 6.0f / 7.0f, f5 = f * f * f * f * f;
+        for (int i = 0; i < n; ++i) {
+            met.kr[i] = weight[i] * mm;
+            met.fa[i] = color[i];
+            float fs = color[i] + f5 * (1.0f - color[i]);
+            met.fb[i] = fs * (7.0f / (f5 * f)) * (1.0f - tint[i]);
+        }
+        met.sample_weight = mm * mean(weight);
+        for (int i = 0; i < n; ++i) weight[i] *= (1.0f - mm);
+        Lobe spec;
+        spec.kind = Lobe::MicrofacetRefl;
+        spec.fresnel = Lobe::Schlick;
+        spec.ax = ax;
+        spec.ay = ay;
+        spec.eta0 = ior;
+        float f0 = ((ior - 1.0f) / (ior + 1.0f)) * ((ior - 1.0f) / (ior + 1.0f));
+        float sl = lut3(kLutSpec, 1, std::sqrt(std::sqrt(ax * ay)), cos_theta, std::sqrt(std::fabs((ior - 1.0f) / (ior + 1.0f))));
+        float alb[8];
+        float mx = -FLT_MAX;
+        for (int i = 0; i < n; ++i) {
+            spec.kr[i] = weight[i];
+            spec.fa[i] = f0 * tint[i];
+            alb[i] = (spec.fa[i] + sl * (1.0f - spec.fa[i])) * weight[i];
+            mx = std::max(mx, weight[i] == 0.0f ? 0.0f : alb[i] / weight[i]);
+        }
+        spec.sample_weight = mean(alb);
+        float lw = std::min(std::max(1.0f - mx, 0.0f), 1.0f);
+        Lobe dif;
+        dif.kind = Lobe::Lambert;
+        for (int i = 0; i < n; ++i) dif.kr[i] = color[i] * (weight[i] * lw) * front;
+        dif.sample_weight = mean(dif.kr);
+        float sum = met.sample_weight + spec.sample_weight + dif.sample_weight;
+        b.count = 0;
+        for (Lobe *l : {&met, &spec, &dif}) {
+            if (!(l->sample_weight > 0.0f)) continue;
+            l->sample_weight /= sum;
+            b.lobes[b.count++] = *l;
+        }
+    } else {
+        l0.kind = Lobe::NoScatter;
+    }
+    return b;
 }
 
 // ----- the path (pt.cpp:53-72; integrator.cpp:134-283) ------------------------
@@ -664,28 +1095,18 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
         V3 nn = dot(it.ng, dir) > 0.0f ? it.ng : neg(it.ng);
         bool occ = any_hit(sc, precompute(offset_ray_origin(it.pos, nn), dir), 1.0f - kShadowEps);
         const Material &mt = sc.mat[it.mat];
-        float kr[8];
-        for (int i = 0; i < n; ++i) kr[i] = mt.type == 0 ? sigmoid_poly(mt.coef, w.lambda[i]) : 0.0f;
-        V3 wl = normalize(sub(ls.p, it.pos));
-        Eval se = bsdf_eval(mt, kr, n, it.sh, it.ng, it.wo, wl);
-        // BSDF sample (Lobe::sample, lobe.cpp:135-142).
-        Eval be;
-        V3 wi_s;
-        if (mt.type == 0) {
-            float u0 = smp.next(), u1 = smp.next();
-            float r = std::sqrt(u0), th = 2.0f * kPi * u1;
-            float dx = r * std::cos(th), dy = r * std::sin(th);
-            float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
-            V3 wo_l = it.sh.to_local(it.wo);
-            V3 wi_l = {dx, dy, wo_l.z < 0.0f ? -z : z};
-            wi_s = it.sh.to_world(wi_l);
-            be = bsdf_eval(mt, kr, n, it.sh, it.ng, it.wo, wi_s);
-        } else {
-            wi_s = it.wo;
-            for (int i = 0; i < n; ++i) be.f[i] = 0.0f;
-            be.pdf = 1.0f;
-            be.flags = kDiffRefl;
+        Bsdf bsdf = make_bsdf(sc, mt, it, w);
+        if (bsdf.dispersive && w.n > 1) {  // SampledWavelengths::check_dispersive
+            bool all = true;
+            for (int i = 1; i < w.n; ++i) all = all && w.pdf[i] != 0.0f;
+            if (all)
+                for (int i = 1; i < w.n; ++i) w.pdf[i] = 0.0f;
         }
+        V3 wl = normalize(sub(ls.p, it.pos));
+        Eval se = bsdf_eval(bsdf, it.wo, wl, nullptr);
+        V3 wi_s;
+        float bs_eta = 1.0f;
+        Eval be = bsdf_sample(bsdf, it.wo, smp, wi_s, bs_eta, mt.type == 1);
         float wmis = ls.pdf / (ls.pdf + se.pdf);
         if (ip.mis_mode == 1) wmis = 1.0f;
         if (!occ && se.pdf > 0.0f && ls.pdf > 0.0f && ip.mis_mode != 2) {
@@ -693,7 +1114,6 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
             for (int i = 0; i < n; ++i) d[i] = thr[i] * (ls.L[i] * se.f[i] * (wmis / ls.pdf));
             ret = add(ret, linear_srgb(d, w));
         }
-        float bs_eta = 1.0f;
         eta_scale *= bs_eta * bs_eta;
         float lum = thr[0];
         for (int i = 1; i < n; ++i) lum = std::max(lum, thr[i]);

@@ -18,6 +18,10 @@ reference lines, independently of both the CUDA library and the C++ oracle:
                       (src/render_core/warpers/alias.h:86-122,148-169)
   spd_eval.json       SPD::eval lookups with the reference's 471/n spacing
                       (src/base/color/spd.cpp:67-76)
+  albedo_luts.json    the reference's precomputed lobe albedo tables
+                      (src/base/scattering/precomputed_table.h): the full
+                      32x32 PureReflectionLobe table and the Dielectric,
+                      DielectricInv and Specular 32^3 tables on a 7^3 subgrid
 
 usage: python tests/golden/make_golden.py <reference-root>
 """
@@ -134,6 +138,39 @@ def main():
             fr = float(t) - np.floor(float(t))
             ev.append({'table': name, 'lambda': lam, 'value': float(f[i] + np.float32(fr) * (f[i + 1] - f[i]))})
     json.dump(ev, open(os.path.join(OUT, 'spd_eval.json'), 'w'))
+    write_luts(ref)
+
+
+def read_luts(ref):
+    text = open(os.path.join(ref, 'src/base/scattering/precomputed_table.h')).read()
+    out = {}
+    for name in ('DielectricLobe', 'DielectricInvLobe', 'SpecularLobe', 'PureReflectionLobe'):
+        m = re.search(r'const\s+(float2|float)\s+%s_Table\[(\d+)\]\s*=\s*\{(.*?)\};' % name, text, re.S)
+        body = m.group(3)
+        if m.group(1) == 'float2':
+            pairs = re.findall(r'float2\(\s*([-+0-9.eE]+)f?\s*,\s*([-+0-9.eE]+)f?\s*\)', body)
+            vals = np.array([[float(a), float(b)] for a, b in pairs], np.float32)
+        else:
+            vals = np.array([float(x.rstrip('f')) for x in re.findall(r'[-+]?\d*\.\d+(?:[eE][-+]?\d+)?f?', body)],
+                            np.float32)
+        assert vals.shape[0] == int(m.group(2)), (name, vals.shape)
+        out[name] = vals
+    return out
+
+
+def write_luts(ref):
+    t = read_luts(ref)
+    sub = [0, 5, 10, 15, 20, 25, 31]
+    res = {'subgrid': sub, 'PureReflectionLobe': t['PureReflectionLobe'].tolist()}
+    for name in ('DielectricLobe', 'DielectricInvLobe', 'SpecularLobe'):
+        cells = []
+        for z in sub:
+            for y in sub:
+                for x in sub:
+                    v = t[name][(z * 32 + y) * 32 + x]
+                    cells.append([x, y, z] + np.atleast_1d(v).astype(float).tolist())
+        res[name] = cells
+    json.dump(res, open(os.path.join(OUT, 'albedo_luts.json'), 'w'))
 
 
 if __name__ == '__main__':

@@ -68,3 +68,17 @@ def test_blackbody_and_rgb_light(vb, gpu_ctx):
         c = o.render(0, 4)
         close = np.abs(g - c) <= 1e-3 * (1.0 + np.abs(c))
         assert close.all(-1).mean() >= 0.97
+
+
+def test_matched_seed_parity_materials(vb, gpu_ctx):
+    # Gold conductor, dispersive glass and principled surfaces.
+    s = vb.Scene(gpu_ctx, scenes.material_room(64, 64)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g = s.film()
+    c = o.render(0, 16)
+    assert np.all(np.isfinite(g))
+    close = np.abs(g[..., :3] - c[..., :3]) <= 2e-3 * (1.0 + np.abs(c[..., :3]))
+    frac = close.all(-1).mean()
+    assert frac >= 0.95, frac
+    assert abs(g[..., :3].mean() - c[..., :3].mean()) < 5e-3 * c[..., :3].mean()

@@ -1,0 +1,89 @@
+"""Material layer on the host: plugin parameters, SPD slots and the albedo
+tables of the compensated lobes (no GPU)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from vision_b200 import scenes
+
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+
+
+def test_shipped_albedo_tables_equal_reference(vb):
+    g = json.load(open(os.path.join(G, 'albedo_luts.json')))
+    t = vb.albedo_luts()
+    np.testing.assert_allclose(t[:1024], g['PureReflectionLobe'], rtol=0, atol=1e-6)
+    for name, off, ch in (('DielectricLobe', 1024, 2), ('DielectricInvLobe', 1024 + 65536, 2),
+                          ('SpecularLobe', 1024 + 131072, 1)):
+        for c in g[name]:
+            x, y, z = (int(v) for v in c[:3])
+            i = off + ((z * 32 + y) * 32 + x) * ch
+            np.testing.assert_allclose(t[i:i + ch], c[3:3 + ch], rtol=0, atol=1e-6)
+
+
+def test_regenerated_albedo_tables_close_to_reference(vb):
+    # apps/precompute's job, redone from the lobe definitions.  The shipped
+    # values carry the reference's own sampling error (24-bit LCG sample pairs),
+    # so agreement is to a few percent, not to float precision.
+    g = json.load(open(os.path.join(G, 'albedo_luts.json')))
+    t = vb.albedo_luts(regenerated=True)
+    d = np.abs(t[:1024] - np.array(g['PureReflectionLobe']))
+    assert d.max() < 0.05 and d.mean() < 0.01
+    for name, off, ch in (('DielectricLobe', 1024, 2), ('DielectricInvLobe', 1024 + 65536, 2),
+                          ('SpecularLobe', 1024 + 131072, 1)):
+        diffs = []
+        for c in g[name]:
+            x, y, z = (int(v) for v in c[:3])
+            i = off + ((z * 32 + y) * 32 + x) * ch
+            diffs.append(np.abs(t[i:i + ch] - c[3:3 + ch]))
+        diffs = np.array(diffs)
+        assert diffs.max() < 0.06, name
+        assert diffs.mean() < 0.012, name
+
+
+def test_metal_glass_principled_records(vb, host_ctx):
+    s = vb.Scene(host_ctx, scenes.material_room(8, 8))
+    names = None
+    mats = s.export('materials', np.uint32).reshape(-1, 16)
+    matf = mats.view(np.float32)
+    types = list(mats[:, 0])
+    assert types.count(2) == 1 and types.count(3) == 1 and types.count(4) == 1
+    metal = matf[types.index(2)]
+    # roughness 0.3 remapped to alpha = 0.09 (metal.cpp:143).
+    assert abs(metal[8] - 0.09) < 1e-7 and abs(metal[9] - 0.09) < 1e-7
+    glass = mats[types.index(3)]
+    assert glass[1] & 1  # dispersive: ior is an spd slot
+    spd = s.export('spd', np.float32)
+    off = glass[2]
+    n = int(spd[off])
+    assert n == 94
+    lam = 360.0 + 5.0 * np.arange(94)
+    np.testing.assert_allclose(spd[off + 1:off + 1 + n], 1.5 + 0.0042 / (lam / 1000.0) ** 2, rtol=1e-6)
+    info = s.info()
+    integ = s.export('integrator', np.uint32)
+    assert integ[5] == info['spectrum_dim']  # scatter_pdf_dim = dimension with a dispersive material
+    pr = matf[types.index(4)]
+    assert abs(pr[8] - 0.35 ** 2) < 1e-6 and abs(pr[10] - 0.4) < 1e-7 and abs(pr[11] - 1.5) < 1e-7
+
+
+def test_principled_nonzero_coat_is_unsupported(vb, host_ctx):
+    sc = scenes.material_room(8, 8)
+    for m in sc['materials']:
+        if m['type'] == 'principled_bsdf':
+            m['param']['coat_weight'] = 0.5
+    with pytest.raises(vb.UnsupportedError) as e:
+        vb.Scene(host_ctx, sc)
+    assert 'coat_weight' in str(e.value)
+
+
+def test_metal_names(vb, host_ctx):
+    for name, ok in (('Au', True), ('Cu', True), ('Al', True), ('Ag', True), ('Unobtainium', True), ('Ti', False)):
+        sc = scenes.box_room(width=4, height=4)
+        sc['materials'][0] = {'type': 'metal', 'name': 'Floor', 'param': {'material_name': name}}
+        if ok:
+            vb.Scene(host_ctx, sc)
+        else:
+            with pytest.raises(vb.UnsupportedError):
+                vb.Scene(host_ctx, sc)

@@ -33,7 +33,7 @@ FILM_SUM64 = 2
 
 EXPORT = dict(pos=0, nrm=1, uv=2, idx=3, prim_inst=4, instances=5, materials=6, lights=7, prim_alias=8,
               prim_pmf=9, light_alias=10, light_pmf=11, camera=12, integrator=13, spd=14, material_rgb=15,
-              light_rgb=16, bvh_nodes=17, bvh_tris=18)
+              light_rgb=16, bvh_nodes=17, bvh_tris=18, luts=19)
 
 
 class VisionError(RuntimeError):
@@ -89,6 +89,7 @@ def _load():
         'vs_timing_enable': ([P, ctypes.c_int], ctypes.c_int),
         'vs_timing_read': ([P, P, P, P], ctypes.c_int),
         'vs_render_noalloc': ([P, U32, U32, P, P], ctypes.c_int),
+        'vs_albedo_luts': ([ctypes.c_int, ctypes.c_char_p, P, ctypes.c_size_t], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -105,12 +106,25 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_scene_info_get', 'vs_scene_export_size', 'vs_scene_export', 'vs_render', 'vs_synchronize',
                       'vs_film_download', 'vs_trace_closest_device', 'vs_trace_closest_host', 'vs_trace_any_device',
                       'vs_trace_any_host', 'vs_rgb_to_spectrum', 'vs_launch_count', 'vs_render_stats', 'vs_timing_enable',
-                      'vs_timing_read', 'vs_render_noalloc'])
+                      'vs_timing_read', 'vs_render_noalloc', 'vs_albedo_luts'])
 
 
 def launch_count():
     """Kernels launched by libvision_b200 since it was loaded."""
     return int(lib.vs_launch_count())
+
+
+LUT_FLOATS = 164864
+
+
+def albedo_luts(regenerated=False):
+    """Albedo tables of the compensated lobes: shipped (reference) or regenerated."""
+    out = np.zeros(LUT_FLOATS, np.float32)
+    rc = lib.vs_albedo_luts(1 if regenerated else 0, os.path.join(HERE, 'data', 'albedo_luts_regen.bin').encode(),
+                            out.ctypes.data_as(ctypes.c_void_p), out.size)
+    if rc != VS_OK:
+        raise VisionError(rc, 'vs_albedo_luts failed')
+    return out
 
 
 def _ptr(a):

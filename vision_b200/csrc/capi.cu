@@ -9,6 +9,7 @@
 
 #include "vs_host.h"
 #include "vs_launch.h"
+#include "vs_microfacet.h"
 
 using namespace vs;
 
@@ -65,7 +66,7 @@ struct vs_scene {
     DevBuf<Material> materials;
     DevBuf<AreaLight> lights;
     DevBuf<AliasEntry> prim_alias, light_alias;
-    DevBuf<float> prim_pmf, light_pmf, spd;
+    DevBuf<float> prim_pmf, light_pmf, spd, luts;
     // Film and per-sample radiance (scratch between the megakernel and the film pass).
     DevBuf<float4> film32, exposed;
     DevBuf<double> film64;
@@ -82,7 +83,7 @@ struct vs_scene {
         for (cudaEvent_t e : ev_film) cudaEventDestroy(e);
         if (ev_join) cudaEventDestroy(ev_join);
         nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
-        prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free();
+        prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
         film32.free(); exposed.free(); film64.free(); radiance.free();
     }
 
@@ -100,6 +101,7 @@ struct vs_scene {
         d.light_alias = light_alias.ptr;
         d.light_pmf = light_pmf.ptr;
         d.spd = spd.ptr;
+        d.luts = luts.ptr;
         d.cam = host.cam;
         d.ip = host.ip;
         d.node_count = static_cast<uint32_t>(host.nodes.size());
@@ -168,6 +170,12 @@ int upload_scene(vs_scene *s) {
     std::vector<float> spd = h.spd;
     if (spd.empty()) spd.push_back(0.0f);
     VS_CUDA(s->spd.upload(spd), "upload spd");
+    std::vector<float> luts(1, 0.0f);
+    if (h.needs_luts) {
+        const float *t = microfacet_luts();
+        luts.assign(t, t + kLutFloats);
+    }
+    VS_CUDA(s->luts.upload(luts), "upload luts");
     s->uploaded = true;
     return VS_OK;
 }
@@ -344,6 +352,10 @@ ExportView export_view(const vs_scene *s, int what) {
         case VS_EXPORT_LIGHT_RGB: return {h.light_rgb.data(), h.light_rgb.size() * sizeof(f3)};
         case VS_EXPORT_BVH_NODES: return {h.nodes.data(), h.nodes.size() * sizeof(Bvh8Node)};
         case VS_EXPORT_BVH_TRIS: return {h.tri_v.data(), h.tri_v.size() * 4};
+        case VS_EXPORT_LUTS: {
+            if (!h.needs_luts) return {nullptr, 0};
+            return {microfacet_luts(), static_cast<size_t>(kLutFloats) * 4};
+        }
         default: return {nullptr, static_cast<size_t>(-1)};
     }
 }
@@ -588,6 +600,13 @@ int vs_render_stats(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, uin
     out3[0] = h[0];
     out3[1] = h[1];
     out3[2] = h[2];
+    return VS_OK;
+}
+
+int vs_albedo_luts(int which, const char *cache_path, float *out, size_t count) {
+    if (!out || count != static_cast<size_t>(kLutFloats)) return VS_E_INVALID;
+    const float *t = which == 0 ? microfacet_luts() : regenerate_microfacet_luts(cache_path ? cache_path : "");
+    std::memcpy(out, t, count * sizeof(float));
     return VS_OK;
 }
 

@@ -254,6 +254,54 @@ f3 xform_normal(const m4 &m, f3 n) {
             static_cast<float>(inv[0][2] * n.x + inv[1][2] * n.y + inv[2][2] * n.z)};
 }
 
+bool is_known_metal(const std::string &m) {
+    for (const char *n : {"Ag", "Al", "Au", "Cu", "CuZn", "Fe", "Li", "Ti", "V", "VN"})
+        if (m == n) return true;
+    return false;
+}
+
+// calculate_alpha (src/base/scattering/microfacet.h:43-58).
+void alpha_aniso(float a, float aniso, float &ax, float &ay) {
+    if (std::fabs(aniso) <= 1e-4f) {
+        ax = ay = a;
+        return;
+    }
+    ax = aniso < 0.0f ? a / (1.0f + aniso) : a * (1.0f - aniso);
+    ay = aniso < 0.0f ? a * (1.0f + aniso) : a / (1.0f - aniso);
+}
+
+// SPD::to_list (src/base/color/spd.h:41-47): samples every 5 nm from 360 nm
+// while below 830 nm (94 samples).
+template <typename F>
+std::vector<float> to_list(F &&f) {
+    std::vector<float> v;
+    for (float l = kLambdaMin; l < kLambdaMax; l += 5.0f) v.push_back(f(l));
+    return v;
+}
+
+// Named glasses (Sellmeier fits of glass.cpp:104-134; Schott catalogue data).
+std::vector<float> sellmeier_curve(const std::string &name) {
+    struct Coef { float b1, b2, b3, c1, c2, c3; };
+    Coef c;
+    if (name == "LASF9") c = {2.00029547f, 0.298926886f, 1.80691843f, 0.0121426017f, 0.0538736236f, 156.530829f};
+    else c = {1.03961212f, 0.231792344f, 1.01046945f, 0.00600069867f, 0.0200179144f, 103.560653f};  // BK7 and unknown
+    return to_list([&](float lambda) {
+        float l = lambda / 1000.0f;
+        float l2 = l * l;
+        float f = c.b1 * l2 / (l2 - c.c1) + c.b2 * l2 / (l2 - c.c2) + c.b3 * l2 / (l2 - c.c3);
+        return std::sqrt(f + 1.0f);
+    });
+}
+
+// Cauchy dispersion n(lambda) = A + B / lambda^2, lambda in micrometres.  The
+// reference has no Cauchy curve; it is expressed as an spd ior slot.
+std::vector<float> cauchy_curve(float A, float B) {
+    return to_list([&](float lambda) {
+        float l = lambda / 1000.0f;
+        return A + B / (l * l);
+    });
+}
+
 struct Loader {
     HostScene &s;
     const float *table;
@@ -281,6 +329,79 @@ struct Loader {
             rgb2spec_decode_albedo(table, in, mat.coef);
         } else if (type == "black_body") {
             mat.type = kMatBlackBody;
+        } else if (type == "metal") {
+            // MetalMaterial (metal.cpp:40-156): complex IOR of a named metal as
+            // SPDs, GGX roughness remapped to alpha = r^2, anisotropy.
+            mat.type = kMatMetal;
+            std::string metal = p["material_name"].as_string();
+            const float *eta = nullptr, *k = nullptr;
+            if (metal == "Au") { eta = VS_METAL_AU_ETA; k = VS_METAL_AU_K; }
+            else if (metal == "Al") { eta = VS_METAL_AL_ETA; k = VS_METAL_AL_K; }
+            else if (metal == "Cu") { eta = VS_METAL_CU_ETA; k = VS_METAL_CU_K; }
+            else if (metal == "Ag" || metal.empty() || !is_known_metal(metal)) { eta = VS_METAL_AG_ETA; k = VS_METAL_AG_K; }
+            else throw unsupported("metal '" + metal + "' (" + name + ")");
+            mat.spd0 = add_spd(eta, 95);
+            mat.spd1 = add_spd(k, 95);
+            float r = clampf(slot_scalar(p["roughness"], 0.01f), 0.0001f, 1.0f);
+            float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
+            bool remap = p["remapping_roughness"].as_bool(true);
+            float a = remap ? r * r : r;
+            alpha_aniso(a, aniso, mat.p[0], mat.p[1]);
+            s.needs_luts = true;
+        } else if (type == "glass") {
+            // GlassMaterial (glass.cpp:169-257): colour, ior (number, spd node,
+            // named Sellmeier glass, or a Cauchy curve), roughness, anisotropy.
+            mat.type = kMatGlass;
+            rgb = slot_rgb(p["color"], make3(1.0f));
+            float in[3] = {rgb.x, rgb.y, rgb.z};
+            rgb2spec_decode_albedo(table, in, mat.coef);
+            std::string glass = p["material_name"].as_string();
+            const Json &ior = p["ior"];
+            const Json &ion = slot_node(ior);
+            std::vector<float> curve;
+            if (!glass.empty()) {
+                curve = sellmeier_curve(glass);
+            } else if (ion.is_object() && ion["type"].as_string() == "spd") {
+                curve = (ion.contains("param") ? ion["param"]["value"] : ion["value"]).as_floats();
+            } else if (ion.is_object() && ion["type"].as_string() == "cauchy") {
+                const Json &cp = ion["param"];
+                curve = cauchy_curve(cp["A"].as_float(1.5f), cp["B"].as_float(0.0f));
+            }
+            if (!curve.empty()) {
+                if (curve.size() < 2) throw std::runtime_error("glass '" + name + "': ior spd needs >= 2 samples");
+                mat.spd0 = add_spd(curve.data(), static_cast<int>(curve.size()));
+                mat.flags |= kMatFlagDispersive;
+            } else {
+                mat.p[2] = slot_scalar(ior, 1.5f);
+            }
+            float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.01f, 1.0f);
+            float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
+            bool remap = p["remapping_roughness"].as_bool(true);
+            float a = remap ? r * r : r;
+            alpha_aniso(a, aniso, mat.p[0], mat.p[1]);
+            s.needs_luts = true;
+        } else if (type == "principled_bsdf") {
+            // PrincipledBSDF (principled_bsdf.cpp:263-461).
+            mat.type = kMatPrincipled;
+            rgb = slot_rgb(p["color"], make3(1.0f));
+            float in[3] = {rgb.x, rgb.y, rgb.z};
+            rgb2spec_decode_albedo(table, in, mat.coef);
+            float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.0001f, 1.0f);
+            float aniso = slot_scalar(p["anisotropic"], 0.0f);
+            float aspect = std::sqrt(1.0f - aniso * 0.9f);
+            mat.p[0] = std::max(0.001f, r * r / aspect);
+            mat.p[1] = std::max(0.001f, r * r * aspect);
+            mat.p[2] = slot_scalar(p["metallic"], 0.0f);
+            mat.p[3] = slot_scalar(p["ior"], 1.5f);
+            f3 tint = slot_rgb(p["spec_tint"], make3(1.0f));
+            float tin[3] = {tint.x, tint.y, tint.z}, tc[4];
+            rgb2spec_decode_albedo(table, tin, tc);
+            mat.p[4] = tc[0]; mat.p[5] = tc[1]; mat.p[6] = tc[2];
+            for (const char *key : {"sheen_weight", "coat_weight", "transmission_weight"}) {
+                if (slot_scalar(p[key], 0.0f) != 0.0f)
+                    throw unsupported(std::string("principled_bsdf ") + key + " > 0 (" + name + ")");
+            }
+            s.needs_luts = true;
         } else {
             throw unsupported("material type '" + type + "' (" + name + ")");
         }
@@ -447,6 +568,10 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
                      HostScene &s) {
     (void)base_dir;
     Json root = Json::parse(text);
+    if (!table_cache.empty()) {
+        size_t slash = table_cache.find_last_of('/');
+        s.lut_cache = (slash == std::string::npos ? std::string() : table_cache.substr(0, slash + 1)) + "microfacet_luts.bin";
+    }
     Loader ld{s, rgb2spec_table(table_cache), {}};
     // Spectrum (SpectrumDesc, node_desc.cpp:346-350; hero.cpp:239).
     const Json &sp = root["spectrum"];

@@ -1,12 +1,20 @@
 // BSDFs of the in-scope material plugins, evaluated and sampled in world space
 // the way MaterialEvaluator does with individual shading normals
 // (src/base/scattering/material.cpp:132-184): each lobe works in its local
-// frame, multiplies f by |cos theta_i|, and the evaluator zeroes the pdf when
-// wi and wo lie on sides of the geometric normal that contradict the lobe's
-// reflection/transmission flag.
+// frame and multiplies f by |cos theta_i|; the evaluator zeroes the pdf when
+// wi and wo lie on sides of the geometric normal that contradict the lobes'
+// reflection/transmission flags.
+//
+// Materials: diffuse (diffuse.cpp), black_body (black_body.cpp), metal
+// (metal.cpp: GGX conductor with complex Fresnel and albedo compensation),
+// glass (glass.cpp: rough dielectric, optionally dispersive, compensated) and
+// principled_bsdf (principled_bsdf.cpp: metallic F82 + Schlick specular +
+// diffuse; the scene loader rejects non-zero sheen, coat and transmission
+// weights, whose lobes are otherwise inert).
 #pragma once
 
 #include "vs_device.cuh"
+#include "vs_microfacet.h"
 
 namespace vs {
 
@@ -18,29 +26,16 @@ constexpr uint32_t kFlagDiffuse = 1u << 3;
 constexpr uint32_t kFlagGlossy = 1u << 4;
 constexpr uint32_t kFlagSpecular = 1u << 5;
 constexpr uint32_t kFlagDiffRefl = kFlagDiffuse | kFlagReflection;
+constexpr uint32_t kFlagGlossyRefl = kFlagGlossy | kFlagReflection;
+constexpr uint32_t kFlagGlossyTrans = kFlagGlossy | kFlagTransmission;
 
 template <int N>
 struct BsdfEval {
     Spec<N> f;
-    float pdf[N];  // scatter pdf per wavelength; only pdf[0] is used unless dispersive
+    float pdf;  // the reference keeps one scatter pdf broadcast to all channels
     uint32_t flags;
-    __device__ __forceinline__ bool valid(bool per_lambda) const {
-        if (!per_lambda) return pdf[0] > 0.0f;
-        bool ok = true;
-#pragma unroll
-        for (int i = 0; i < N; ++i) ok = ok && (pdf[i] > 0.0f);
-        return ok;
-    }
-    __device__ __forceinline__ Spec<N> throughput(bool per_lambda) const {
-        Spec<N> r;
-#pragma unroll
-        for (int i = 0; i < N; ++i) r.v[i] = f.v[i] / (per_lambda ? pdf[i] : pdf[0]);
-        return r;
-    }
-    __device__ __forceinline__ void set_pdf(float p) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) pdf[i] = p;
-    }
+    __device__ __forceinline__ bool valid() const { return pdf > 0.0f; }
+    __device__ __forceinline__ Spec<N> throughput() const { return f * (1.0f / pdf); }
 };
 
 template <int N>
@@ -64,81 +59,418 @@ __device__ __forceinline__ void invalidate_secondary(Wavelengths<N> &w) {
 
 // square_to_cosine_hemisphere (src/math/warp.h:24-47).
 __device__ __forceinline__ f3 cosine_hemisphere(f2 u) {
-    float r = sqrtf(u.x);
-    float theta = k2Pi * u.y;
-    float dx = r * cosf(theta), dy = r * sinf(theta);
-    float z = sqrtf(fmaxf(0.0f, 1.0f - dx * dx - dy * dy));
-    return {dx, dy, z};
+    f2 d = square_to_disk(u);
+    float z = sqrtf(fmaxf(0.0f, 1.0f - d.x * d.x - d.y * d.y));
+    return {d.x, d.y, z};
 }
 
-__device__ __forceinline__ bool same_hemisphere_world(f3 a, f3 b, f3 n) { return dot(a, n) * dot(b, n) > 0.0f; }
+template <int N>
+__device__ __forceinline__ float avg(const Spec<N> &s) {
+    float a = 0.0f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) a += s.v[i];
+    return a * (1.0f / N);
+}
+
+// Fresnel variants of the microfacet lobes (src/base/scattering/fresnel.h).
+enum FresnelKind : uint32_t { kFresnelConductor = 0, kFresnelSchlick = 1, kFresnelF82 = 2, kFresnelConstant = 3 };
+
+// One microfacet reflection lobe: MicrofacetReflection + Fresnel, with the
+// PureReflectionLobe albedo compensation when `compensate` is set.
+template <int N>
+struct MfLobe {
+    float ax, ay;
+    uint32_t fresnel;
+    bool compensate;
+    Spec<N> kr;
+    Spec<N> fa, fb;  // conductor: eta, k;  Schlick: F0, -;  F82: F0, B
+    float eta0;      // Schlick: eta[0]
+
+    __device__ __forceinline__ Spec<N> F(float c) const {
+        Spec<N> r;
+        if (fresnel == kFresnelConductor) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) r.v[i] = fresnel_complex(c, fa.v[i], fb.v[i]);
+        } else if (fresnel == kFresnelSchlick) {
+            // FresnelSchlick::evaluate (fresnel.h:60-67).
+            float f_real = fresnel_dielectric(c, eta0);
+            float f0_real = schlick_F0_from_ior(eta0);
+            float t = clampf((f_real - f0_real) / (1.0f - f0_real), 0.0f, 1.0f);
+#pragma unroll
+            for (int i = 0; i < N; ++i) r.v[i] = fa.v[i] + t * (1.0f - fa.v[i]);
+        } else if (fresnel == kFresnelF82) {
+            // FresnelF82Tint::evaluate (fresnel.h:117-124).
+            float mu = clampf(1.0f - c, 0.0f, 1.0f);
+            float mu2 = mu * mu;
+            float mu5 = mu2 * mu2 * mu;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                float fs = fa.v[i] + mu5 * (1.0f - fa.v[i]);
+                r.v[i] = clampf(fs - fb.v[i] * c * mu5 * mu, 0.0f, 1.0f);
+            }
+        } else {
+            r = Spec<N>::fill(1.0f);
+        }
+        return r;
+    }
+
+    // MicrofacetLobe::evaluate_local_impl -> BxDF::safe_evaluate (bxdf.cpp:30-43),
+    // MicrofacetReflection::f / PDF (bxdf.cpp:56-70), compensation (lobe.cpp:716-735).
+    __device__ __forceinline__ void eval_local(f3 wo, f3 wi, const float *luts, Spec<N> &f, float &pdf) const {
+        bool s = wo.z * wi.z > 0.0f;
+        if (!s) {
+            f = Spec<N>::fill(0.0f);
+            pdf = 0.0f;
+            return;
+        }
+        f3 wh = normalize(wo + wi);
+        f3 whf = wh.z < 0.0f ? -wh : wh;
+        float brdf = ggx_brdf(wo, whf, wi, ax, ay);
+        Spec<N> Fr = F(fabsf(dot(wo, whf)));
+        float comp = 1.0f;
+        if (compensate) comp = 1.0f / lut_sample2(luts + kLutPureReflection, sqrtf(ax * ay), wo.z);
+        f = Fr * kr * (brdf * comp);
+        pdf = ggx_pdf_reflection(wo, wh, ax, ay);
+    }
+    // MicrofacetReflection::sample_wi (bxdf.cpp:72-77).
+    __device__ __forceinline__ f3 sample_local(f3 wo, f2 u, bool &valid) const {
+        f3 wh = ggx_sample_vndf(wo, u, ax, ay);
+        f3 wi = reflect_dir(wo, wh);
+        valid = wo.z * wi.z > 0.0f;
+        return wi;
+    }
+};
+
+// DielectricLobe (src/base/scattering/lobe.cpp:253-450).
+template <int N>
+struct DielLobe {
+    float ax, ay;
+    Spec<N> eta;  // per wavelength, already corrected for the side (Interaction::correct_eta)
+    Spec<N> kt;
+    bool compensate;
+
+    __device__ __forceinline__ Spec<N> F(float c) const {
+        Spec<N> r;
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.v[i] = fresnel_dielectric(c, eta.v[i]);
+        return r;
+    }
+    __device__ __forceinline__ float refl_prob(const Spec<N> &Fr) const {
+        Spec<N> total;
+#pragma unroll
+        for (int i = 0; i < N; ++i) total.v[i] = (1.0f - Fr.v[i]) * kt.v[i] + Fr.v[i];
+        return avg(Fr) / avg(total);
+    }
+    __device__ __forceinline__ float comp(f3 wo, const float *luts) const {
+        if (!compensate) return 1.0f;
+        float e = eta.v[0];
+        const float *t = luts + (e > 1.0f ? kLutDielectric : kLutDielectricInv);
+        float z = ((e > 1.0f ? e : 1.0f / e) - kIorLower) / (kIorUpper - kIorLower);
+        float x = sqrtf(sqrtf(ax * ay));
+        return 1.0f / lut_sample3(t, 2, 0, x, fabsf(wo.z), z);
+    }
+    __device__ __forceinline__ void eval_local(f3 wo, f3 wi, const float *luts, Spec<N> &f, float &pdf,
+                                               uint32_t &flags, float &eta_out) const {
+        bool reflect = wo.z * wi.z > 0.0f;
+        float e0 = eta.v[0];
+        float eta_p = reflect ? 1.0f : e0;
+        eta_out = eta_p;
+        f3 wh = normalize(wo + wi * eta_p);
+        if (dot(wh, wo) < 0.0f) wh = -wh;
+        Spec<N> Fr = F(fabsf(dot(wh, wo)));
+        float c = comp(wo, luts);
+        if (reflect) {
+            f = Fr * (ggx_brdf(wo, wh, wi, ax, ay) * c);
+            pdf = ggx_pdf_reflection(wo, wh, ax, ay) * refl_prob(Fr);
+            flags = kFlagGlossyRefl;
+        } else {
+            f3 wh2 = normalize(wo + wi * e0);
+            float bt = ggx_btdf(wo, wh2, wi, e0, ax, ay, true);
+            Spec<N> T;
+#pragma unroll
+            for (int i = 0; i < N; ++i) T.v[i] = (1.0f - Fr.v[i]) * kt.v[i];
+            f = T * (bt * c);
+            pdf = ggx_pdf_transmission(wo, wh, wi, e0, ax, ay) * (1.0f - refl_prob(Fr));
+            flags = kFlagGlossyTrans;
+        }
+    }
+    // DielectricLobe::sample_wi_local_impl (lobe.cpp:431-449): 2D for the
+    // microfacet normal, then 1D to choose reflection or refraction.
+    __device__ __forceinline__ f3 sample_local(f3 wo, Sampler &smp, bool &valid) const {
+        f3 wh = ggx_sample_vndf(wo, smp.next2(), ax, ay);
+        float d = dot(wo, wh);
+        Spec<N> Fr = F(fabsf(d));
+        float uc = smp.next();
+        f3 wi;
+        if (uc < refl_prob(Fr)) {
+            wi = reflect_dir(wo, wh);
+            valid = wo.z * wi.z > 0.0f;
+        } else {
+            bool ok = refract_dir(wo, wh, eta.v[0], wi);
+            valid = ok && !(wo.z * wi.z > 0.0f);
+        }
+        return wi;
+    }
+};
 
 template <int N>
 struct Bsdf {
     uint32_t type;
     Frame frame;
     f3 ng;
-    Spec<N> kr;
+    const float *luts;
     bool dispersive;
+    // Diffuse colour (diffuse, principled diffuse lobe).
+    Spec<N> kd;
+    // Microfacet lobes: metal uses mf[0]; principled uses mf[0] = metallic,
+    // mf[1] = specular.
+    MfLobe<N> mf[2];
+    DielLobe<N> dl;
+    // Principled lobe-set sample weights (normalised): metallic, transmission,
+    // specular, diffuse; and whether the transmission lobe is present.
+    float w_metal, w_trans, w_spec, w_diff;
+    float trans_scale;
+    bool has_trans;
 
-    // Zero the pdf of a sample whose geometric side contradicts its flag
+    // Zero the pdf of a direction whose geometric side contradicts the flags
     // (MaterialEvaluator::evaluate, material.cpp:137-147).
     __device__ __forceinline__ void discard_check(f3 wo, f3 wi, BsdfEval<N> &e) const {
-        bool same = same_hemisphere_world(wo, wi, ng);
+        bool same = dot(wo, ng) * dot(wi, ng) > 0.0f;
         bool trans = (e.flags & kFlagTransmission) != 0u;
-        if (same == trans) e.set_pdf(0.0f);
+        if (same == trans) e.pdf = 0.0f;
     }
 
-    __device__ __forceinline__ BsdfEval<N> evaluate(f3 wo_w, f3 wi_w, const Wavelengths<N> &) const {
+    __device__ BsdfEval<N> evaluate(f3 wo_w, f3 wi_w, float *eta_out) const {
         BsdfEval<N> e;
         f3 wo = frame.to_local(wo_w), wi = frame.to_local(wi_w);
+        float eta = 1.0f;
+        float acos_i = fabsf(wi.z);
         if (type == kMatDiffuse) {
-            // DiffuseLobe -> LambertReflection::safe_evaluate (bxdf.cpp:30-43).
             bool s = wo.z * wi.z > 0.0f;
-            float acos_i = fabsf(wi.z);
-            e.f = s ? kr * (kInvPi * acos_i) : Spec<N>::fill(0.0f);
-            e.set_pdf(s ? acos_i * kInvPi : 0.0f);
+            e.f = s ? kd * (kInvPi * acos_i) : Spec<N>::fill(0.0f);
+            e.pdf = s ? acos_i * kInvPi : 0.0f;
             e.flags = kFlagDiffRefl;
+        } else if (type == kMatMetal) {
+            mf[0].eval_local(wo, wi, luts, e.f, e.pdf);
+            e.f = e.f * acos_i;
+            e.flags = kFlagGlossyRefl;
+        } else if (type == kMatGlass) {
+            dl.eval_local(wo, wi, luts, e.f, e.pdf, e.flags, eta);
+            e.f = e.f * acos_i;
+        } else if (type == kMatPrincipled) {
+            // LobeSet::evaluate_impl (lobe.cpp:665-681): sum of the lobes, each
+            // masked by its own hemisphere test, pdfs weighted by the
+            // normalised sample weights.
+            e.f = Spec<N>::fill(0.0f);
+            e.pdf = 0.0f;
+            e.flags = 0u;
+            bool same = wo.z * wi.z > 0.0f;
+            Spec<N> f;
+            float p;
+            if (w_metal > 0.0f) {
+                mf[0].eval_local(wo, wi, luts, f, p);
+                if (same) {
+                    e.f = e.f + f * acos_i;
+                    e.pdf += p * w_metal;
+                }
+                e.flags |= kFlagGlossyRefl;
+            }
+            if (has_trans) {
+                uint32_t fl;
+                dl.eval_local(wo, wi, luts, f, p, fl, eta);
+                e.f = e.f + f * (acos_i * trans_scale);
+                e.pdf += p * w_trans;
+                e.flags |= fl;
+            }
+            if (w_spec > 0.0f) {
+                mf[1].eval_local(wo, wi, luts, f, p);
+                if (same) {
+                    e.f = e.f + f * acos_i;
+                    e.pdf += p * w_spec;
+                }
+                e.flags |= kFlagGlossyRefl;
+            }
+            if (w_diff > 0.0f) {
+                if (same) {
+                    e.f = e.f + kd * (kInvPi * acos_i);
+                    e.pdf += acos_i * kInvPi * w_diff;
+                }
+                e.flags |= kFlagDiffRefl;
+            }
         } else {
             // BlackBodyLobe (black_body.cpp:32-39): no scattering.
             e.f = Spec<N>::fill(0.0f);
-            e.set_pdf(1.0f);
+            e.pdf = 1.0f;
             e.flags = kFlagUnset;
         }
+        if (eta_out) *eta_out = eta;
         discard_check(wo_w, wi_w, e);
         return e;
     }
 
-    __device__ __forceinline__ BsdfSample<N> sample(f3 wo_w, Sampler &smp, const Wavelengths<N> &wl) const {
+    __device__ BsdfSample<N> sample(f3 wo_w, Sampler &smp) const {
         BsdfSample<N> bs;
         bs.eta = 1.0f;
+        f3 wo = frame.to_local(wo_w);
+        bool valid = true;
+        f3 wi;
         if (type == kMatDiffuse) {
-            f2 u = smp.next2();
-            f3 wo = frame.to_local(wo_w);
-            f3 wi = cosine_hemisphere(u);
+            wi = cosine_hemisphere(smp.next2());
             wi.z = wo.z < 0.0f ? -wi.z : wi.z;
-            bs.wi = frame.to_world(wi);
-            bs.eval = evaluate(wo_w, bs.wi, wl);
+        } else if (type == kMatMetal) {
+            wi = mf[0].sample_local(wo, smp.next2(), valid);
+        } else if (type == kMatGlass) {
+            wi = dl.sample_local(wo, smp, valid);
+        } else if (type == kMatPrincipled) {
+            // LobeSet::sample_wi_impl (lobe.cpp:598-627): 1D lobe choice, an
+            // unused 2D draw, then the chosen lobe's own draws.
+            float uc = smp.next();
+            (void)smp.next2();
+            int strategy = 0;
+            float sum = 0.0f;
+            const float ws[4] = {w_metal, w_trans, w_spec, w_diff};
+            const bool present[4] = {w_metal > 0.0f, has_trans, w_spec > 0.0f, w_diff > 0.0f};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (!present[i]) continue;
+                strategy = uc > sum ? i : strategy;
+                sum += ws[i];
+            }
+            if (strategy == 0) wi = mf[0].sample_local(wo, smp.next2(), valid);
+            else if (strategy == 1) wi = dl.sample_local(wo, smp, valid);
+            else if (strategy == 2) wi = mf[1].sample_local(wo, smp.next2(), valid);
+            else {
+                wi = cosine_hemisphere(smp.next2());
+                wi.z = wo.z < 0.0f ? -wi.z : wi.z;
+            }
         } else {
             bs.wi = wo_w;
             bs.eval.f = Spec<N>::fill(0.0f);
-            bs.eval.set_pdf(1.0f);
+            bs.eval.pdf = 1.0f;
             bs.eval.flags = kFlagDiffRefl;
+            return bs;
         }
+        bs.wi = frame.to_world(wi);
+        bs.eval = evaluate(wo_w, bs.wi, &bs.eta);
+        if (!valid) bs.eval.pdf = 0.0f;
         return bs;
     }
 };
 
+// Material::create_evaluator for the in-scope plugins.  The lobe parameters
+// come from the 64-byte material record written by the scene loader.
 template <int N>
-__device__ __forceinline__ Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng,
-                                             f3 wo, const Wavelengths<N> &wl) {
+__device__ Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng, f3 wo,
+                             const Wavelengths<N> &wl) {
     Bsdf<N> b;
     b.type = m.type;
     b.frame = frame;
     b.ng = ng;
+    b.luts = s.luts;
     b.dispersive = (m.flags & kMatFlagDispersive) != 0u;
-    if (m.type == kMatDiffuse) b.kr = albedo_spectrum<N>(m.coef, wl);
-    else b.kr = Spec<N>::fill(0.0f);
+    b.w_metal = b.w_trans = b.w_spec = b.w_diff = 0.0f;
+    b.has_trans = false;
+    b.trans_scale = 0.0f;
+    if (m.type == kMatDiffuse) {
+        b.kd = albedo_spectrum<N>(m.coef, wl);
+    } else if (m.type == kMatMetal) {
+        // MetalMaterial::create_lobe_set (metal.cpp:137-156).
+        MfLobe<N> &l = b.mf[0];
+        l.ax = m.p[0];
+        l.ay = m.p[1];
+        l.fresnel = kFresnelConductor;
+        l.compensate = true;
+        l.kr = Spec<N>::fill(1.0f);
+        const float *eta = s.spd + m.spd0;
+        const float *k = s.spd + m.spd1;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            l.fa.v[i] = spd_eval(eta + 1, static_cast<int>(eta[0]), wl.lambda[i]);
+            l.fb.v[i] = spd_eval(k + 1, static_cast<int>(k[0]), wl.lambda[i]);
+        }
+        l.eta0 = 1.0f;
+    } else if (m.type == kMatGlass) {
+        // GlassMaterial::create_lobe_set (glass.cpp:240-257).
+        DielLobe<N> &d = b.dl;
+        d.ax = m.p[0];
+        d.ay = m.p[1];
+        d.kt = albedo_spectrum<N>(m.coef, wl);
+        d.compensate = true;
+        bool front = dot(wo, ng) > 0.0f;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            float ior = m.spd0 != kInvalid ? spd_eval(s.spd + m.spd0 + 1, static_cast<int>(s.spd[m.spd0]), wl.lambda[i])
+                                           : m.p[2];
+            d.eta.v[i] = front ? ior : 1.0f / ior;
+        }
+    } else if (m.type == kMatPrincipled) {
+        // PrincipledBSDF::create_lobe_set (principled_bsdf.cpp:352-461) with
+        // sheen and coat at weight 0 (their lobes then contribute nothing).
+        float ax = m.p[0], ay = m.p[1];
+        float metallic_param = m.p[2];
+        float ior = m.p[3];
+        Spec<N> color = albedo_spectrum<N>(m.coef, wl);
+        const float tint_coef[3] = {m.p[4], m.p[5], m.p[6]};
+        Spec<N> tint = albedo_spectrum<N>(tint_coef, wl);
+        float cos_theta = dot(wo, ng);
+        float front = cos_theta > 0.0f ? 1.0f : 0.0f;
+        Spec<N> weight = Spec<N>::fill(1.0f);
+        float sw_metal = 0.0f, sw_trans = 0.0f, sw_spec = 0.0f, sw_diff = 0.0f;
+        // Metallic: F82 tint (F0 = colour, F82 = specular tint).
+        float metallic = metallic_param * front;
+        {
+            MfLobe<N> &l = b.mf[0];
+            l.ax = ax;
+            l.ay = ay;
+            l.fresnel = kFresnelF82;
+            l.compensate = true;
+            l.kr = weight * metallic;
+            const float f = 6.0f / 7.0f;
+            const float f5 = f * f * f * f * f;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                l.fa.v[i] = color.v[i];
+                float fs = color.v[i] + f5 * (1.0f - color.v[i]);
+                l.fb.v[i] = fs * (7.0f / (f5 * f)) * (1.0f - tint.v[i]);
+            }
+            l.eta0 = 1.0f;
+            sw_metal = metallic * avg(weight);
+            weight = weight * (1.0f - metallic);
+        }
+        // Specular: Schlick with F0 = schlick(ior) * tint; albedo from its table.
+        {
+            MfLobe<N> &l = b.mf[1];
+            l.ax = ax;
+            l.ay = ay;
+            l.fresnel = kFresnelSchlick;
+            l.compensate = false;
+            l.kr = weight;
+            float f0 = schlick_F0_from_ior(ior);
+            l.fa = tint * f0;
+            l.eta0 = ior;
+            float x = sqrtf(sqrtf(ax * ay));
+            float z = sqrtf(fabsf((ior - 1.0f) / (ior + 1.0f)));
+            float sl = lut_sample3(s.luts + kLutSpecular, 1, 0, x, cos_theta, z);
+            Spec<N> alb;
+#pragma unroll
+            for (int i = 0; i < N; ++i) alb.v[i] = (l.fa.v[i] + sl * (1.0f - l.fa.v[i])) * weight.v[i];
+            sw_spec = avg(alb);
+            // layering_weight (principled_bsdf.cpp:209-214).
+            float mx = -3.402823466e+38f;
+#pragma unroll
+            for (int i = 0; i < N; ++i) mx = fmaxf(mx, safe_div(alb.v[i], weight.v[i]));
+            weight = weight * clampf(1.0f - mx, 0.0f, 1.0f);
+        }
+        // Diffuse.
+        b.kd = color * weight * front;
+        sw_diff = avg(b.kd);
+        // LobeSet::normalize_sampled_weight (lobe.cpp:483-492).
+        float sum = sw_metal + sw_trans + sw_spec + sw_diff;
+        b.w_metal = sw_metal / sum;
+        b.w_trans = b.has_trans ? sw_trans / sum : 0.0f;
+        b.w_spec = sw_spec / sum;
+        b.w_diff = sw_diff / sum;
+    }
     return b;
 }
 

@@ -118,6 +118,13 @@ __device__ __forceinline__ Spec<N> operator*(const Spec<N> &a, const Spec<N> &b)
     return r;
 }
 template <int N>
+__device__ __forceinline__ Spec<N> operator+(const Spec<N> &a, const Spec<N> &b) {
+    Spec<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.v[i] = a.v[i] + b.v[i];
+    return r;
+}
+template <int N>
 __device__ __forceinline__ Spec<N> operator*(const Spec<N> &a, float s) {
     Spec<N> r;
 #pragma unroll

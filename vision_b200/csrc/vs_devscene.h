@@ -19,7 +19,8 @@ struct DeviceScene {
     const float *prim_pmf;        // PMF of each entry of prim_alias
     const AliasEntry *light_alias;// power light sampler
     const float *light_pmf;
-    const float *spd;             // concatenated SPD sample arrays
+    const float *spd;             // concatenated SPD sample arrays ([n, v0..v(n-1)] each)
+    const float *luts;            // albedo tables of the compensated lobes (vs_microfacet.h offsets)
     Camera cam;
     IntegratorParams ip;
     uint32_t node_count;

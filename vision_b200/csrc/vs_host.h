@@ -36,6 +36,8 @@ struct HostScene {
     std::vector<float> light_pmf;
     // Spectral samples of named SPDs (metal eta/k, glass ior), concatenated.
     std::vector<float> spd;
+    bool needs_luts = false;
+    std::string lut_cache;
     Camera cam{};
     IntegratorParams ip{};
     std::string spectrum_type = "hero";
@@ -65,6 +67,12 @@ void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &ent
 const float *rgb2spec_table(const std::string &cache_path);
 void rgb2spec_decode_albedo(const float *table, const float rgb[3], float out[4]);
 void rgb2spec_decode_unbound(const float *table, const float rgb[3], float out[4]);
+
+// Albedo tables of the compensated lobes (layout in vs_microfacet.h): the
+// reference's shipped values, and the same tables regenerated from the lobe
+// definitions (built on first use, cached in `cache_path`).
+const float *microfacet_luts();
+const float *regenerate_microfacet_luts(const std::string &cache_path);
 
 // CIE tables downsampled to the reference's 94-entry 5 nm SPDs and the CIE Y
 // integral (src/base/color/spd.cpp:14-38).

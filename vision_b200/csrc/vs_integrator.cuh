@@ -199,7 +199,6 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
     f3 ret = make3(0.0f);
     f3 prev_ng = rd;
     float eta_scale = 1.0f;
-    const bool dispersive_pdf = ip.scatter_pdf_dim > 1;
 
     for (uint32_t bounce = 0; bounce < ip.max_depth; ++bounce) {
         RayPre rp = precompute_ray(ro, rd);
@@ -228,19 +227,19 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
         Bsdf<N> bsdf = make_bsdf<N>(s, mat, it.shading, it.ng, it.wo, wl);
         if (bsdf.dispersive) invalidate_secondary<N>(wl);
         f3 wi_light = normalize(ls.p_light - it.pos);
-        BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, wl);
-        BsdfSample<N> bs = bsdf.sample(it.wo, smp, wl);
+        BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, nullptr);
+        BsdfSample<N> bs = bsdf.sample(it.wo, smp);
         Spec<N> Ld = Spec<N>::fill(0.0f);
-        float w_mis = ls.pdf / (ls.pdf + se.pdf[0]);
+        float w_mis = ls.pdf / (ls.pdf + se.pdf);
         if (ip.mis_mode == 1u) w_mis = 1.0f;
-        if (!occluded && se.valid(dispersive_pdf) && ls.pdf > 0.0f) {
+        if (!occluded && se.valid() && ls.pdf > 0.0f) {
             Ld = ls.L * se.f * (w_mis / ls.pdf);
         }
         if (ip.mis_mode != 2u) ret += linear_srgb<N>(throughput * Ld, wl);
         eta_scale *= sqr(bs.eta);
         float lum = throughput.max();
-        if (!bs.eval.valid(dispersive_pdf) || lum == 0.0f) break;
-        throughput = throughput * bs.eval.throughput(dispersive_pdf);
+        if (!bs.eval.valid() || lum == 0.0f) break;
+        throughput = throughput * bs.eval.throughput();
         if (eta_scale * lum < ip.rr_threshold && bounce >= ip.min_depth) {
             float q = fminf(0.95f, lum);
             float rr = smp.next();
@@ -249,7 +248,7 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
         }
         // A path whose throughput is exactly zero adds nothing from here on.
         if (throughput.all_zero()) break;
-        scatter_pdf = bs.eval.pdf[0];
+        scatter_pdf = bs.eval.pdf;
         Ray nr = spawn_ray(it.pos, it.ng, bs.wi);
         ro = nr.o;
         rd = nr.d;

@@ -80,3 +80,18 @@ def box_room(width=256, height=256, max_depth=8, min_depth=5, rr_threshold=1.0, 
         "light_sampler": {"type": "uniform", "param": {"lights": []}},
         "render_setting": {"polymorphic_mode": 1},
     }
+
+
+def material_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
+    """The box room with the microfacet materials on its objects: a gold
+    conductor tall box, a dispersive glass short box (Cauchy A = 1.5,
+    B = 0.0042) and a principled floor."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    mats = {m["name"]: m for m in sc["materials"]}
+    mats["TallBox"].update({"type": "metal", "param": {"material_name": "Au", "roughness": 0.3}})
+    mats["ShortBox"].update({"type": "glass", "param": {
+        "color": [1.0, 1.0, 1.0], "roughness": 0.2,
+        "ior": {"type": "cauchy", "param": {"A": 1.5, "B": 0.0042}}}})
+    mats["Floor"].update({"type": "principled_bsdf", "param": {
+        "color": [0.8, 0.5, 0.3], "metallic": 0.4, "roughness": 0.35}})
+    return sc
