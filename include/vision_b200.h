@@ -123,6 +123,13 @@ int vs_scene_info_get(const vs_scene *scene, vs_scene_info *out);
 #define VS_EXPORT_BVH_NODES 17  /* 80 bytes per node */
 #define VS_EXPORT_BVH_TRIS 18   /* float[12] per primitive in leaf order */
 #define VS_EXPORT_LUTS 19       /* float albedo tables of the compensated lobes (empty if unused) */
+#define VS_EXPORT_ENV 20        /* environment light block, 160 bytes (empty without one) */
+#define VS_EXPORT_ENV_TEX 21    /* float[4] per texel of the environment map */
+#define VS_EXPORT_ENV_MARGINAL 22       /* alias entries over rows */
+#define VS_EXPORT_ENV_MARGINAL_FUNC 23  /* float row integrals */
+#define VS_EXPORT_ENV_COND 24           /* alias entries per texel (row-major) */
+#define VS_EXPORT_ENV_COND_FUNC 25      /* float weight per texel */
+#define VS_EXPORT_RGB2SPEC 26   /* float[4] x 3 x 64^3 RGB -> spectrum coefficient table */
 int vs_scene_export_size(const vs_scene *scene, int what, size_t *bytes);
 int vs_scene_export(const vs_scene *scene, int what, void *dst, size_t bytes);
 

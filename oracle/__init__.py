@@ -32,7 +32,10 @@ class OracleSceneStruct(ctypes.Structure):
                 ('lights', ctypes.c_void_p), ('light_count', ctypes.c_uint32),
                 ('prim_alias', ctypes.c_void_p), ('prim_pmf', ctypes.c_void_p),
                 ('light_alias', ctypes.c_void_p), ('light_pmf', ctypes.c_void_p),
-                ('camera', ctypes.c_void_p), ('integrator', ctypes.c_void_p), ('spd', ctypes.c_void_p)]
+                ('camera', ctypes.c_void_p), ('integrator', ctypes.c_void_p), ('spd', ctypes.c_void_p),
+                ('env', ctypes.c_void_p), ('env_tex', ctypes.c_void_p), ('env_marginal', ctypes.c_void_p),
+                ('env_marginal_func', ctypes.c_void_p), ('env_cond', ctypes.c_void_p),
+                ('env_cond_func', ctypes.c_void_p), ('rgb2spec', ctypes.c_void_p)]
 
 
 _lib = None
@@ -71,6 +74,9 @@ class OracleScene:
     def __init__(self, scene):
         keys = ['pos', 'nrm', 'uv', 'idx', 'prim_inst', 'instances', 'materials', 'lights', 'prim_alias', 'prim_pmf',
                 'light_alias', 'light_pmf', 'camera', 'integrator', 'spd']
+        env = scene.export('env')
+        if env.size:
+            keys += ['env', 'env_tex', 'env_marginal', 'env_marginal_func', 'env_cond', 'env_cond_func', 'rgb2spec']
         self.arr = {}
         for k in keys:
             a = scene.export(k)
@@ -84,7 +90,10 @@ class OracleScene:
                                    info['vertex_count'], info['prim_count'], _p(a['instances']), info['instance_count'],
                                    _p(a['materials']), info['material_count'], _p(a['lights']), info['light_count'],
                                    _p(a['prim_alias']), _p(a['prim_pmf']), _p(a['light_alias']), _p(a['light_pmf']),
-                                   _p(a['camera']), _p(a['integrator']), _p(a['spd']))
+                                   _p(a['camera']), _p(a['integrator']), _p(a['spd']),
+                                   *([_p(a[k]) for k in ('env', 'env_tex', 'env_marginal', 'env_marginal_func',
+                                                         'env_cond', 'env_cond_func', 'rgb2spec')]
+                                     if env.size else [None] * 7))
 
     def trace_closest(self, rays):
         rays = np.ascontiguousarray(rays, np.float32)

@@ -73,6 +73,13 @@ struct Camera {
     float exposure;
     uint32_t pad0, pad1;
 };
+struct EnvLight {
+    float w2o[4][4];
+    float o2w[4][4];
+    uint32_t width, height;
+    float scale, integral, world_diameter, lum_power;
+    uint32_t pad0, pad1;
+};
 struct Integrator {
     uint32_t max_depth, min_depth;
     float rr_threshold;
@@ -104,6 +111,14 @@ struct oracle_scene {
     const void *camera;
     const void *integrator;
     const float *spd;
+    // Environment light (env == nullptr: none).
+    const void *env;
+    const float *env_tex;
+    const void *env_marginal;
+    const float *env_marginal_func;
+    const void *env_cond;
+    const float *env_cond_func;
+    const float *rgb2spec;
 };
 }
 
@@ -270,6 +285,8 @@ struct Scene {
     const Alias *light_alias;
     Camera cam;
     Integrator ip;
+    EnvLight env;
+    bool has_env = false;
     // Binary BVH over primitives (median split), for scenes too large to brute force.
     struct Node {
         float lo[3], hi[3];
@@ -339,6 +356,10 @@ struct Scene {
         light_alias = static_cast<const Alias *>(sc->light_alias);
         std::memcpy(&cam, sc->camera, sizeof(Camera));
         std::memcpy(&ip, sc->integrator, sizeof(Integrator));
+        if (sc->env) {
+            std::memcpy(&env, sc->env, sizeof(EnvLight));
+            has_env = true;
+        }
         order.resize(sc->prim_count);
         for (uint32_t i = 0; i < sc->prim_count; ++i) order[i] = i;
         nodes.reserve(sc->prim_count / 2 + 8);
@@ -540,6 +561,99 @@ static float light_pmf(const Scene &sc, uint32_t li) {
     return sc.ip.light_sampler == 1 ? sc.s->light_pmf[li] : 1.0f / static_cast<float>(sc.ip.light_count);
 }
 
+// ----- spherical environment (spherical.cpp, alias2d.cpp, hero.cpp:92-141) ----
+static V3 mat_vec(const float (*m)[4], V3 v) {
+    return {m[0][0] * v.x + m[1][0] * v.y + m[2][0] * v.z, m[0][1] * v.x + m[1][1] * v.y + m[2][1] * v.z,
+            m[0][2] * v.x + m[1][2] * v.y + m[2][2] * v.z};
+}
+
+// RGBToSpectrumTable::decode_unbound with the table's trilinear lookup.
+static void decode_unbound(const float *table, float r, float g, float b, float c[4]) {
+    float rgb[3] = {std::max(r, 0.0f), std::max(g, 0.0f), std::max(b, 0.0f)};
+    float m = std::max(rgb[0], std::max(rgb[1], rgb[2]));
+    float sc = 2.0f * m;
+    float q[3];
+    for (int k = 0; k < 3; ++k) q[k] = std::min(std::max(sc == 0.0f ? 0.0f : rgb[k] / sc, 0.0f), 1.0f);
+    c[3] = sc;
+    if (q[0] == q[1] && q[1] == q[2]) {
+        c[0] = c[1] = 0.0f;
+        c[2] = (q[0] - 0.5f) / std::sqrt(q[0] * (1.0f - q[0]));
+        return;
+    }
+    const uint32_t res = 64;
+    uint32_t mc = (q[0] > q[1]) ? ((q[0] > q[2]) ? 0u : 2u) : ((q[1] > q[2]) ? 1u : 2u);
+    float z = q[mc];
+    float x = q[(mc + 1) % 3] * (res - 1u) / z;
+    float y = q[(mc + 2) % 3] * (res - 1u) / z;
+    auto iss = [](float v) { return 0.5f - std::sin(std::asin(1.0f - 2.0f * v) * (1.0f / 3.0f)); };
+    float zz = iss(iss(z)) * (res - 1u);
+    uint32_t xi = std::min(static_cast<uint32_t>(x), res - 2), yi = std::min(static_cast<uint32_t>(y), res - 2),
+             zi = std::min(static_cast<uint32_t>(zz), res - 2);
+    float dx = x - xi, dy = y - yi, dz = zz - zi;
+    auto L = [](float t, float a, float bb) { return a + t * (bb - a); };
+    for (int i = 0; i < 3; ++i) {
+        auto co = [&](int ox, int oy, int oz) {
+            return table[((((size_t)mc * res + (zi + oz)) * res + (yi + oy)) * res + (xi + ox)) * 4 + i];
+        };
+        c[i] = L(dz, L(dy, L(dx, co(0, 0, 0), co(1, 0, 0)), L(dx, co(0, 1, 0), co(1, 1, 0))),
+                 L(dy, L(dx, co(0, 0, 1), co(1, 0, 1)), L(dx, co(0, 1, 1), co(1, 1, 1))));
+    }
+}
+
+static void env_L(const Scene &sc, float u, float v, const Swl &w, float *out) {
+    const int W = static_cast<int>(sc.env.width), H = static_cast<int>(sc.env.height);
+    float x = u * W - 0.5f, y = v * H - 0.5f;
+    float fx = std::floor(x), fy = std::floor(y);
+    float tx = x - fx, ty = y - fy;
+    int x0 = static_cast<int>(fx), y0 = static_cast<int>(fy);
+    int x1 = ((x0 + 1) % W + W) % W;
+    x0 = (x0 % W + W) % W;
+    int y1 = std::min(std::max(y0 + 1, 0), H - 1);
+    y0 = std::min(std::max(y0, 0), H - 1);
+    const float *t = sc.s->env_tex;
+    float rgb[3];
+    for (int c = 0; c < 3; ++c) {
+        float a = t[(y0 * W + x0) * 4 + c], b = t[(y0 * W + x1) * 4 + c];
+        float cc = t[(y1 * W + x0) * 4 + c], d = t[(y1 * W + x1) * 4 + c];
+        float top = a + tx * (b - a), bot = cc + tx * (d - cc);
+        rgb[c] = top + ty * (bot - top);
+    }
+    float co[4];
+    decode_unbound(sc.s->rgb2spec, rgb[0], rgb[1], rgb[2], co);
+    for (int i = 0; i < w.n; ++i)
+        out[i] = sigmoid_poly(co, w.lambda[i]) * co[3] * spd_eval(tables().d65, 94, w.lambda[i]) * sc.env.scale;
+}
+
+static float env_pdf_map(const Scene &sc, float u, float v) {
+    uint32_t W = sc.env.width, H = sc.env.height;
+    uint32_t iu = std::min(static_cast<uint32_t>(std::max(u * W, 0.0f)), W - 1);
+    uint32_t iv = std::min(static_cast<uint32_t>(std::max(v * H, 0.0f)), H - 1);
+    return sc.env.integral > 0.0f ? sc.s->env_cond_func[iv * W + iu] / sc.env.integral : 0.0f;
+}
+
+// SphericalMap::evaluate_wi for an escaped ray direction.
+static void env_eval(const Scene &sc, V3 dir, const Swl &w, float *L, float &pdf) {
+    V3 local = mat_vec(sc.env.w2o, dir);
+    float theta = std::acos(std::min(std::max(local.z, -1.0f), 1.0f));
+    float phi = std::atan2(local.y, local.x);
+    if (phi < 0.0f) phi += 2.0f * kPi;
+    float u = phi * (1.0f / (2.0f * kPi)), v = theta * kInvPi;
+    float st = std::sin(theta);
+    env_L(sc, u, v, w, L);
+    float p = env_pdf_map(sc, u, v) / (2.0f * kPi * kPi * st);
+    pdf = st == 0.0f ? 0.0f : p;
+}
+
+static float alias_cont(const Alias *tab, uint32_t size, float u, uint32_t &ofs) {
+    u = u * static_cast<float>(size);
+    uint32_t idx = std::min(static_cast<uint32_t>(u), size - 1u);
+    u = std::min(u - static_cast<float>(idx), kOneMinusEps);
+    bool keep = u < tab[idx].prob;
+    float ur = keep ? std::min(u / tab[idx].prob, kOneMinusEps) : std::min((1.0f - u) / (1.0f - tab[idx].prob), kOneMinusEps);
+    ofs = keep ? idx : tab[idx].alias;
+    return (static_cast<float>(ofs) + ur) / static_cast<float>(size);
+}
+
 struct LS {
     float L[8];
     float pdf;
@@ -556,6 +670,27 @@ static LS sample_light(const Scene &sc, const It &it, float ul, float ux, float 
     } else {
         li = static_cast<uint32_t>(std::min(ul * static_cast<float>(n), static_cast<float>(n) - 1.0f));
         pmf_l = 1.0f / static_cast<float>(n);
+    }
+    if (sc.has_env && li == sc.ip.light_count - 1) {
+        // SphericalMap::sample_wi + AliasTable2D::sample_continuous.
+        uint32_t W = sc.env.width, H = sc.env.height;
+        const Alias *marg = static_cast<const Alias *>(sc.s->env_marginal);
+        const Alias *cond = static_cast<const Alias *>(sc.s->env_cond);
+        uint32_t iv, iu;
+        float fv = alias_cont(marg, H, uy, iv);
+        float pdf_v = sc.env.integral > 0.0f ? sc.s->env_marginal_func[iv] / sc.env.integral : 0.0f;
+        float fu = alias_cont(cond + (size_t)iv * W, W, ux, iu);
+        float iu_int = sc.s->env_marginal_func[iv];
+        float pdf_u = iu_int > 0.0f ? sc.s->env_cond_func[(size_t)iv * W + iu] / iu_int : 0.0f;
+        float theta = fv * kPi, phi = fu * 2.0f * kPi;
+        float st = std::sin(theta), ct = std::cos(theta);
+        V3 local = {st * std::cos(phi), st * std::sin(phi), ct};
+        V3 wd = normalize(mat_vec(sc.env.o2w, local));
+        float p = pdf_u * pdf_v / (2.0f * kPi * kPi * st);
+        ls.pdf = (std::isinf(p) ? 0.0f : p) * pmf_l;
+        env_L(sc, fu, fv, w, ls.L);
+        ls.p = add(it.pos, mul(wd, sc.env.world_diameter));
+        return ls;
     }
     const AreaLight &L = sc.lights[li];
     float ur = ux;
@@ -1068,7 +1203,21 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
     for (uint32_t b = 0; b < ip.max_depth; ++b) {
         RayPre rp = precompute(ro, rd);
         HitRec h = closest(sc, rp, FLT_MAX);
-        if (h.prim == kInvalid) break;
+        if (h.prim == kInvalid) {
+            // IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132).
+            if (sc.has_env) {
+                float Le[8], lpdf;
+                env_eval(sc, normalize(sub(add(ro, rd), ro)), w, Le, lpdf);
+                lpdf *= light_pmf(sc, sc.ip.light_count - 1);
+                float weight = scatter_pdf / (scatter_pdf + lpdf);
+                if (ip.mis_mode == 2) weight = 1.0f;
+                else if (ip.mis_mode == 1) weight = b == 0 ? weight : 0.0f;
+                float d[8];
+                for (int i = 0; i < n; ++i) d[i] = Le[i] * thr[i] * weight;
+                ret = add(ret, linear_srgb(d, w));
+            }
+            break;
+        }
         It it = interaction(sc, h.prim, h.u, h.v, rd);
         if (it.light != kInvalid) {
             const AreaLight &L = sc.lights[it.light];

@@ -154,3 +154,35 @@ def test_unsupported_light_in_light_sampler(vb, host_ctx):
     sc['light_sampler']['param']['lights'] = [{'type': 'point', 'param': {}}]
     with pytest.raises(vb.UnsupportedError):
         vb.Scene(host_ctx, sc)
+
+
+def test_environment_warper_matches_reference_construction(vb, host_ctx):
+    # AliasTable2D::build (alias2d.cpp:30-66) from the weights of
+    # SphericalMap::calculate_weights (spherical.cpp:187-213), restated here.
+    sc = scenes.large_scene(width=8, height=8, subdivisions=1, grid=4, tiles=2, sky_width=64, sky_height=32)
+    s = vb.Scene(host_ctx, sc)
+    env = s.export('env', np.float32)
+    W, H = env[32:34].view(np.uint32)
+    tex = s.export('env_tex', np.float32).reshape(H, W, 4)
+    idx = np.arange(W * H)
+    theta = ((idx // H).astype(np.float32) + np.float32(0.5)) / np.float32(W)
+    lum = (np.float32(0.212671) * tex[..., 0] + np.float32(0.715160) * tex[..., 1] +
+           np.float32(0.072169) * tex[..., 2]).reshape(-1)
+    w = (lum * np.sin(np.float32(np.pi) * theta).astype(np.float32)).astype(np.float32)
+    cf = s.export('env_cond_func', np.float32)
+    np.testing.assert_allclose(cf, w, rtol=2e-6, atol=1e-30)
+    mf = s.export('env_marginal_func', np.float32)
+    np.testing.assert_allclose(mf, w.reshape(H, W).astype(np.float64).sum(1) / W, rtol=1e-6)
+    assert abs(env[35] - np.float32(mf.astype(np.float64).sum() / H)) <= 1e-6 * env[35]
+    # The sky's sun lobe peaks near 5e4.
+    assert 1.0e4 < tex[..., :3].max() <= 5.0e4 + 10
+
+
+def test_large_scene_counts(vb, host_ctx):
+    s = vb.Scene(host_ctx, scenes.large_scene(width=8, height=8, subdivisions=7, grid=1000, tiles=10,
+                                              sky_width=64, sky_height=32))
+    i = s.info()
+    assert i['prim_count'] == 20 * 4 ** 7 + 2 * 1000 * 1000
+    assert i['instance_count'] == 101
+    types = s.export('materials', np.uint32).reshape(-1, 16)[:, 0]
+    assert set(types.tolist()) == {2, 3, 4}

@@ -67,6 +67,8 @@ struct vs_scene {
     DevBuf<AreaLight> lights;
     DevBuf<AliasEntry> prim_alias, light_alias;
     DevBuf<float> prim_pmf, light_pmf, spd, luts;
+    DevBuf<float> env_tex, env_marginal_func, env_cond_func, rgb2spec;
+    DevBuf<AliasEntry> env_marginal, env_cond;
     // Film and per-sample radiance (scratch between the megakernel and the film pass).
     DevBuf<float4> film32, exposed;
     DevBuf<double> film64;
@@ -84,6 +86,7 @@ struct vs_scene {
         if (ev_join) cudaEventDestroy(ev_join);
         nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
         prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
+        env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
         film32.free(); exposed.free(); film64.free(); radiance.free();
     }
 
@@ -102,6 +105,15 @@ struct vs_scene {
         d.light_pmf = light_pmf.ptr;
         d.spd = spd.ptr;
         d.luts = luts.ptr;
+        d.has_env = host.has_env ? 1u : 0u;
+        d.env = host.env;
+        d.env_index = host.ip.light_count - 1u;
+        d.env_tex = reinterpret_cast<const float4 *>(env_tex.ptr);
+        d.env_marginal = env_marginal.ptr;
+        d.env_marginal_func = env_marginal_func.ptr;
+        d.env_cond = env_cond.ptr;
+        d.env_cond_func = env_cond_func.ptr;
+        d.rgb2spec = reinterpret_cast<const float4 *>(rgb2spec.ptr);
         d.cam = host.cam;
         d.ip = host.ip;
         d.node_count = static_cast<uint32_t>(host.nodes.size());
@@ -176,6 +188,16 @@ int upload_scene(vs_scene *s) {
         luts.assign(t, t + kLutFloats);
     }
     VS_CUDA(s->luts.upload(luts), "upload luts");
+    if (h.has_env) {
+        VS_CUDA(s->env_tex.upload(h.env_tex), "upload env");
+        VS_CUDA(s->env_marginal.upload(h.env_marginal), "upload env");
+        VS_CUDA(s->env_marginal_func.upload(h.env_marginal_func), "upload env");
+        VS_CUDA(s->env_cond.upload(h.env_cond), "upload env");
+        VS_CUDA(s->env_cond_func.upload(h.env_cond_func), "upload env");
+        const float *t = rgb2spec_table("");
+        std::vector<float> tab(t, t + static_cast<size_t>(3) * 64 * 64 * 64 * 4);
+        VS_CUDA(s->rgb2spec.upload(tab), "upload rgb2spec");
+    }
     s->uploaded = true;
     return VS_OK;
 }
@@ -352,6 +374,13 @@ ExportView export_view(const vs_scene *s, int what) {
         case VS_EXPORT_LIGHT_RGB: return {h.light_rgb.data(), h.light_rgb.size() * sizeof(f3)};
         case VS_EXPORT_BVH_NODES: return {h.nodes.data(), h.nodes.size() * sizeof(Bvh8Node)};
         case VS_EXPORT_BVH_TRIS: return {h.tri_v.data(), h.tri_v.size() * 4};
+        case VS_EXPORT_ENV: return h.has_env ? ExportView{&h.env, sizeof(EnvLight)} : ExportView{nullptr, 0};
+        case VS_EXPORT_ENV_TEX: return {h.env_tex.data(), h.env_tex.size() * 4};
+        case VS_EXPORT_ENV_MARGINAL: return {h.env_marginal.data(), h.env_marginal.size() * sizeof(AliasEntry)};
+        case VS_EXPORT_ENV_MARGINAL_FUNC: return {h.env_marginal_func.data(), h.env_marginal_func.size() * 4};
+        case VS_EXPORT_ENV_COND: return {h.env_cond.data(), h.env_cond.size() * sizeof(AliasEntry)};
+        case VS_EXPORT_ENV_COND_FUNC: return {h.env_cond_func.data(), h.env_cond_func.size() * 4};
+        case VS_EXPORT_RGB2SPEC: return {rgb2spec_table(""), static_cast<size_t>(3) * 64 * 64 * 64 * 16};
         case VS_EXPORT_LUTS: {
             if (!h.needs_luts) return {nullptr, 0};
             return {microfacet_luts(), static_cast<size_t>(kLutFloats) * 4};

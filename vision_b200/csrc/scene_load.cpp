@@ -36,7 +36,8 @@ const Cie5 &cie5() {
     return c;
 }
 
-void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &table, std::vector<float> &pmf) {
+void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &table, std::vector<float> &pmf,
+                 float *integral_out) {
     size_t n = weights.size();
     double sum = 0.0;
     for (float w : weights) sum += w;
@@ -60,6 +61,7 @@ void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &tab
     for (uint32_t i : over) table[i] = {1.0f, i};
     for (uint32_t i : under) table[i] = {1.0f, i};
     float integral = static_cast<float>(sum / static_cast<double>(n));
+    if (integral_out) *integral_out = integral;
     pmf.resize(n);
     for (size_t i = 0; i < n; ++i)
         pmf[i] = integral > 0.0f ? weights[i] / (integral * static_cast<float>(n)) : 0.0f;
@@ -107,6 +109,34 @@ m4 rot_z(float deg) {
     m4 m = m4_identity();
     m.m[0][0] = c; m.m[0][1] = s; m.m[1][0] = -s; m.m[1][1] = c;
     return m;
+}
+
+// Inverse of an affine 4x4 (rotation/scale + translation).
+m4 invert_affine(const m4 &m) {
+    double a[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) a[r][c] = m.m[c][r];
+    double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                 a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    double inv[3][3];
+    inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) / det;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+    inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) / det;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+    inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) / det;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    m4 r = m4_identity();
+    for (int row = 0; row < 3; ++row)
+        for (int c = 0; c < 3; ++c) r.m[c][row] = static_cast<float>(inv[row][c]);
+    for (int row = 0; row < 3; ++row) {
+        double t = 0.0;
+        for (int c = 0; c < 3; ++c) t -= inv[row][c] * m.m[3][c];
+        r.m[3][row] = static_cast<float>(t);
+    }
+    return r;
 }
 
 f3 as_f3(const Json &j, f3 def) {
@@ -231,6 +261,109 @@ MeshData make_inline_mesh(const Json &p) {
     return m;
 }
 
+// Lattice value noise in [-1, 1] with smoothstep-weighted trilinear
+// interpolation of hashed corner values.
+float value_noise(f3 p, uint32_t seed) {
+    auto hash = [&](int x, int y, int z) {
+        uint32_t h = static_cast<uint32_t>(x) * 0x8da6b343u ^ static_cast<uint32_t>(y) * 0xd8163841u ^
+                     static_cast<uint32_t>(z) * 0xcb1ab31fu ^ seed * 0x165667b1u;
+        h ^= h >> 13;
+        h *= 0x5bd1e995u;
+        h ^= h >> 15;
+        return static_cast<float>(h & 0xffffffu) * (2.0f / 16777215.0f) - 1.0f;
+    };
+    float fx = std::floor(p.x), fy = std::floor(p.y), fz = std::floor(p.z);
+    int x = static_cast<int>(fx), y = static_cast<int>(fy), z = static_cast<int>(fz);
+    float tx = p.x - fx, ty = p.y - fy, tz = p.z - fz;
+    auto ss = [](float t) { return t * t * (3.0f - 2.0f * t); };
+    tx = ss(tx); ty = ss(ty); tz = ss(tz);
+    auto l = [](float t, float a, float b) { return a + t * (b - a); };
+    float c00 = l(tx, hash(x, y, z), hash(x + 1, y, z)), c10 = l(tx, hash(x, y + 1, z), hash(x + 1, y + 1, z));
+    float c01 = l(tx, hash(x, y, z + 1), hash(x + 1, y, z + 1)), c11 = l(tx, hash(x, y + 1, z + 1), hash(x + 1, y + 1, z + 1));
+    return l(tz, l(ty, c00, c10), l(ty, c01, c11));
+}
+
+// Subdivided icosahedron on the unit sphere scaled to `radius`, displaced
+// along the radius by `amplitude * radius * value_noise(frequency * p)`, with
+// area-weighted smooth vertex normals and spherical uv.
+MeshData make_icosphere(const Json &p) {
+    uint32_t sub = p["subdivisions"].as_uint(4u);
+    if (sub > 9) throw unsupported("icosphere subdivisions > 9");
+    float radius = p["radius"].as_float(1.0f);
+    const Json &dj = p["displacement"];
+    float amp = dj["amplitude"].as_float(0.0f);
+    float freq = dj["frequency"].as_float(4.0f);
+    uint32_t seed = dj["seed"].as_uint(1u);
+    const float t = (1.0f + std::sqrt(5.0f)) / 2.0f;
+    std::vector<f3> v = {{-1, t, 0}, {1, t, 0}, {-1, -t, 0}, {1, -t, 0}, {0, -1, t}, {0, 1, t},
+                         {0, -1, -t}, {0, 1, -t}, {t, 0, -1}, {t, 0, 1}, {-t, 0, -1}, {-t, 0, 1}};
+    for (f3 &q : v) q = normalize(q);
+    std::vector<uint32_t> f = {0, 11, 5, 0, 5, 1, 0, 1, 7, 0, 7, 10, 0, 10, 11, 1, 5, 9, 5, 11, 4, 11, 10, 2, 10, 7, 6, 7, 1, 8,
+                               3, 9, 4, 3, 4, 2, 3, 2, 6, 3, 6, 8, 3, 8, 9, 4, 9, 5, 2, 4, 11, 6, 2, 10, 8, 6, 7, 9, 8, 1};
+    for (uint32_t level = 0; level < sub; ++level) {
+        std::map<uint64_t, uint32_t> mid;
+        auto midpoint = [&](uint32_t a, uint32_t b) {
+            uint64_t key = a < b ? (static_cast<uint64_t>(a) << 32 | b) : (static_cast<uint64_t>(b) << 32 | a);
+            auto it = mid.find(key);
+            if (it != mid.end()) return it->second;
+            uint32_t i = static_cast<uint32_t>(v.size());
+            v.push_back(normalize((v[a] + v[b]) * 0.5f));
+            mid[key] = i;
+            return i;
+        };
+        std::vector<uint32_t> nf;
+        nf.reserve(f.size() * 4);
+        for (size_t k = 0; k + 2 < f.size(); k += 3) {
+            uint32_t a = f[k], b = f[k + 1], c = f[k + 2];
+            uint32_t ab = midpoint(a, b), bc = midpoint(b, c), ca = midpoint(c, a);
+            uint32_t tris[12] = {a, ab, ca, b, bc, ab, c, ca, bc, ab, bc, ca};
+            nf.insert(nf.end(), tris, tris + 12);
+        }
+        f.swap(nf);
+    }
+    MeshData m;
+    m.p.resize(v.size());
+    m.uv.resize(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+        float r = radius * (1.0f + amp * value_noise(v[i] * freq, seed));
+        m.p[i] = v[i] * r;
+        float theta = std::acos(clampf(v[i].y, -1.0f, 1.0f));
+        float phi = std::atan2(v[i].z, v[i].x);
+        m.uv[i] = {phi * kInv2Pi + 0.5f, theta * kInvPi};
+    }
+    // Faces wind counter-clockwise seen from outside: cross(p0 - p2, p1 - p2)
+    // points outward.
+    m.idx = f;
+    m.n.assign(v.size(), make3(0.0f));
+    for (size_t k = 0; k + 2 < f.size(); k += 3) {
+        f3 n = cross(m.p[f[k]] - m.p[f[k + 2]], m.p[f[k + 1]] - m.p[f[k + 2]]);
+        for (int j = 0; j < 3; ++j) m.n[f[k + j]] += n;
+    }
+    return m;
+}
+
+// Regular grid in the xz plane, facing +y: nx x nz quads over size_x x size_z.
+MeshData make_grid(const Json &p) {
+    uint32_t nx = p["nx"].as_uint(1u), nz = p["nz"].as_uint(1u);
+    if (nx == 0 || nz == 0 || static_cast<uint64_t>(nx) * nz > (1ull << 26)) throw unsupported("grid resolution");
+    float sx = p["size_x"].as_float(1.0f), sz = p["size_z"].as_float(1.0f);
+    MeshData m;
+    for (uint32_t j = 0; j <= nz; ++j)
+        for (uint32_t i = 0; i <= nx; ++i) {
+            float u = static_cast<float>(i) / nx, w = static_cast<float>(j) / nz;
+            m.p.push_back({(u - 0.5f) * sx, 0.0f, (w - 0.5f) * sz});
+            m.n.push_back({0.0f, 1.0f, 0.0f});
+            m.uv.push_back({u, w});
+        }
+    for (uint32_t j = 0; j < nz; ++j)
+        for (uint32_t i = 0; i < nx; ++i) {
+            uint32_t a = j * (nx + 1) + i, b = a + 1, c = a + nx + 1, d = c + 1;
+            uint32_t q[6] = {c, b, a, c, d, b};
+            m.idx.insert(m.idx.end(), q, q + 6);
+        }
+    return m;
+}
+
 // Normal-matrix transform (inverse transpose of the upper 3x3).
 f3 xform_normal(const m4 &m, f3 n) {
     double a[3][3];
@@ -300,6 +433,43 @@ std::vector<float> cauchy_curve(float A, float B) {
         float l = lambda / 1000.0f;
         return A + B / (l * l);
     });
+}
+
+// Procedural HDR sky in lat-long layout (row 0 at the zenith): a
+// horizon-to-zenith gradient above the horizon, a dim ground below, and a sun
+// lobe of `sun_radius` degrees whose radiance peaks at `sun_peak`.
+std::vector<float> make_sky(const Json &p, uint32_t &W, uint32_t &H) {
+    W = p["width"].as_uint(2048u);
+    H = p["height"].as_uint(1024u);
+    f3 zenith = as_f3(p["zenith"], make3(0.25f, 0.45f, 1.0f));
+    f3 horizon = as_f3(p["horizon"], make3(1.0f, 0.95f, 0.85f));
+    f3 ground = as_f3(p["ground"], make3(0.3f, 0.28f, 0.25f));
+    float elev = p["sun_elevation"].as_float(35.0f) * kPi / 180.0f;
+    float azim = p["sun_azimuth"].as_float(40.0f) * kPi / 180.0f;
+    float radius = p["sun_radius"].as_float(5.0f) * kPi / 180.0f;
+    float peak = p["sun_peak"].as_float(5e4f);
+    f3 sun = {std::cos(elev) * std::cos(azim), std::cos(elev) * std::sin(azim), std::sin(elev)};
+    std::vector<float> tex(static_cast<size_t>(W) * H * 4, 0.0f);
+    for (uint32_t y = 0; y < H; ++y) {
+        float theta = (y + 0.5f) / H * kPi;
+        float e = 0.5f * kPi - theta;
+        for (uint32_t x = 0; x < W; ++x) {
+            float phi = (x + 0.5f) / W * k2Pi;
+            f3 d = {std::sin(theta) * std::cos(phi), std::sin(theta) * std::sin(phi), std::cos(theta)};
+            f3 c;
+            if (e >= 0.0f) {
+                float t = std::sqrt(e / (0.5f * kPi));
+                c = horizon + (zenith - horizon) * t;
+            } else {
+                c = ground;
+            }
+            float ang = std::acos(clampf(dot(d, sun), -1.0f, 1.0f));
+            if (ang < radius) c += make3(peak * 0.5f * (1.0f + std::cos(kPi * ang / radius)));
+            float *t4 = &tex[(static_cast<size_t>(y) * W + x) * 4];
+            t4[0] = c.x; t4[1] = c.y; t4[2] = c.z; t4[3] = 0.0f;
+        }
+    }
+    return tex;
 }
 
 struct Loader {
@@ -528,6 +698,8 @@ struct Loader {
         if (type == "quad") mesh = make_quad(p["width"].as_float(1.0f), p["height"].as_float(1.0f));
         else if (type == "cube") mesh = make_cube(p["x"].as_float(1.0f), p["y"].as_float(1.0f), p["z"].as_float(1.0f));
         else if (type == "mesh") mesh = make_inline_mesh(p);
+        else if (type == "icosphere") mesh = make_icosphere(p);
+        else if (type == "grid") mesh = make_grid(p);
         else throw unsupported("shape type '" + type + "' (" + name + ")");
         const Json *emission = p.contains("emission") ? &p["emission"] : nullptr;
         uint32_t mat = kInvalid;
@@ -564,6 +736,68 @@ void update_camera(HostScene &s, uint32_t width, uint32_t height) {
     c.screen_span_y = hi_y - lo_y;
 }
 
+// SphericalMap (spherical.cpp:26-215) with a procedural sky image and its
+// AliasTable2D (alias2d.cpp:30-66) built from luminance * sin(theta) weights
+// (calculate_weights, spherical.cpp:187-213).
+static void load_spherical(const Json &p, const Json &root, HostScene &s) {
+    const Json &cn = slot_node(p["color"]);
+    if (!cn.is_object() || cn["type"].as_string() != "sky")
+        throw unsupported("spherical light colour other than a procedural 'sky' node");
+    uint32_t W, H;
+    s.env_tex = make_sky(cn["param"], W, H);
+    EnvLight &e = s.env;
+    e.width = W;
+    e.height = H;
+    e.scale = p["scale"].is_number() ? p["scale"].as_float() : 1.0f;
+    // o2w_ = o2w * rotation_x(-90) * scale(1, -1, 1) (flip_u false); w2o = inverse.
+    m4 o2w = parse_transform(p["o2w"]);
+    bool flip_u = p["flip_u"].as_bool(false);
+    m4 rx = rot_x(-90.0f) * scale_m(make3(1.0f, flip_u ? 1.0f : -1.0f, 1.0f));
+    e.o2w = o2w * rx;
+    e.w2o = invert_affine(e.o2w);
+    // Warper weights.
+    std::vector<float> weights(static_cast<size_t>(W) * H);
+    double avg[3] = {0, 0, 0};
+    for (size_t idx = 0; idx < weights.size(); ++idx) {
+        const float *t = &s.env_tex[idx * 4];
+        float v = static_cast<float>(idx / H) + 0.5f;
+        float theta = v / W;
+        float sin_theta = std::sin(kPi * theta);
+        weights[idx] = linear_srgb_to_y(make3(t[0], t[1], t[2])) * sin_theta;
+        for (int c = 0; c < 3; ++c) avg[c] += t[c];
+    }
+    std::vector<float> marginal_func(H);
+    s.env_cond.clear();
+    s.env_cond_func.clear();
+    for (uint32_t v = 0; v < H; ++v) {
+        std::vector<float> row(weights.begin() + static_cast<size_t>(v) * W, weights.begin() + static_cast<size_t>(v + 1) * W);
+        std::vector<AliasEntry> tab;
+        std::vector<float> pmf;
+        float integral = 0.0f;
+        build_alias(row, tab, pmf, &integral);
+        marginal_func[v] = integral;
+        s.env_cond.insert(s.env_cond.end(), tab.begin(), tab.end());
+        s.env_cond_func.insert(s.env_cond_func.end(), row.begin(), row.end());
+    }
+    std::vector<float> mpmf;
+    build_alias(marginal_func, s.env_marginal, mpmf, &e.integral);
+    s.env_marginal_func = marginal_func;
+    // World bounds (Scene::world_radius: max(aabb radius, min_world_radius)).
+    f3 lo = make3(3.4e38f), hi = make3(-3.4e38f);
+    for (const f3 &q : s.pos) {
+        lo = vmin(lo, q);
+        hi = vmax(hi, q);
+    }
+    float min_radius = root["render_setting"]["min_world_radius"].as_float(10.0f);
+    float radius = std::max(0.5f * length(hi - lo), min_radius);
+    e.world_diameter = 2.0f * radius;
+    // SphericalMap::power (spherical.cpp:58-61).
+    double n = static_cast<double>(W) * H;
+    f3 a = make3(float(avg[0] / n), float(avg[1] / n), float(avg[2] / n)) * e.scale;
+    e.lum_power = linear_srgb_to_y(a * (kPi * radius * radius));
+    s.has_env = true;
+}
+
 void load_scene_json(const std::string &text, const std::string &base_dir, const std::string &table_cache,
                      HostScene &s) {
     (void)base_dir;
@@ -589,13 +823,18 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     if (lst == "uniform") s.ip.light_sampler = kLightSamplerUniform;
     else if (lst == "power") s.ip.light_sampler = kLightSamplerPower;
     else throw unsupported("light sampler '" + lst + "'");
-    for (const Json &l : lsj["param"]["lights"].elements())
-        throw unsupported("light type '" + l["type"].as_string() + "' in light_sampler");
-    s.ip.light_count = static_cast<uint32_t>(s.lights.size());
+    for (const Json &l : lsj["param"]["lights"].elements()) {
+        std::string lt = l["type"].as_string("area");
+        if (lt != "spherical") throw unsupported("light type '" + lt + "' in light_sampler");
+        if (s.has_env) throw unsupported("more than one environment light");
+        load_spherical(l["param"], root, s);
+    }
+    s.ip.light_count = static_cast<uint32_t>(s.lights.size()) + (s.has_env ? 1u : 0u);
     if (s.ip.light_count == 0) throw unsupported("scene without lights");
     {
         std::vector<float> w;
         for (const AreaLight &L : s.lights) w.push_back(L.lum_power);
+        if (s.has_env) w.push_back(s.env.lum_power);
         build_alias(w, s.light_alias, s.light_pmf);
     }
     // Integrator (IlluminationIntegrator ctor, integrator.cpp:60-67).

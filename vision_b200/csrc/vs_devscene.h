@@ -21,6 +21,17 @@ struct DeviceScene {
     const float *light_pmf;
     const float *spd;             // concatenated SPD sample arrays ([n, v0..v(n-1)] each)
     const float *luts;            // albedo tables of the compensated lobes (vs_microfacet.h offsets)
+    // Environment light (only when has_env): texels as float4 RGB, the warper's
+    // marginal / conditional alias tables and weights, the RGB->spectrum table.
+    EnvLight env;
+    uint32_t has_env;
+    uint32_t env_index;           // light index of the environment (last)
+    const float4 *env_tex;
+    const AliasEntry *env_marginal;
+    const float *env_marginal_func;
+    const AliasEntry *env_cond;
+    const float *env_cond_func;
+    const float4 *rgb2spec;       // 3 x 64^3 coefficient table
     Camera cam;
     IntegratorParams ip;
     uint32_t node_count;

@@ -1,0 +1,152 @@
+// Spherical environment light on the device: lookup, evaluation for escaped
+// rays and importance sampling through the 2D alias warper.
+// Restates src/render_core/lights/environments/spherical.cpp,
+// src/render_core/warpers/alias2d.cpp and alias.h, and the RGB -> spectrum
+// decode of RGBToSpectrumTable::decode_unbound (hero.cpp:92-141).
+#pragma once
+
+#include "vs_device.cuh"
+
+namespace vs {
+
+// decode_albedo / decode_unbound on the device with the exact trilinear
+// interpolation of the host path (hero.cpp:92-141).
+__device__ __forceinline__ void rgb2spec_unbound(const float4 *table, f3 rgb_in, float c[4]) {
+    f3 rgb = vmax(rgb_in, make3(0.0f));
+    float m = max3(rgb);
+    float scale = 2.0f * m;
+    f3 q = scale == 0.0f ? make3(0.0f) : rgb / scale;
+    q = {clampf(q.x, 0.0f, 1.0f), clampf(q.y, 0.0f, 1.0f), clampf(q.z, 0.0f, 1.0f)};
+    c[3] = scale;
+    if (q.x == q.y && q.y == q.z) {
+        c[0] = 0.0f;
+        c[1] = 0.0f;
+        c[2] = (q.x - 0.5f) / sqrtf(q.x * (1.0f - q.x));
+        return;
+    }
+    const int res = 64;
+    uint32_t maxc = (q.x > q.y) ? ((q.x > q.z) ? 0u : 2u) : ((q.y > q.z) ? 1u : 2u);
+    float z = comp(q, maxc);
+    float x = comp(q, (maxc + 1u) % 3u) * (res - 1u) / z;
+    float y = comp(q, (maxc + 2u) % 3u) * (res - 1u) / z;
+    auto inv_ss = [](float v) { return 0.5f - sinf(asinf(1.0f - 2.0f * v) * (1.0f / 3.0f)); };
+    float zz = inv_ss(inv_ss(z)) * (res - 1u);
+    uint32_t xi = min(static_cast<uint32_t>(x), static_cast<uint32_t>(res - 2));
+    uint32_t yi = min(static_cast<uint32_t>(y), static_cast<uint32_t>(res - 2));
+    uint32_t zi = min(static_cast<uint32_t>(zz), static_cast<uint32_t>(res - 2));
+    float dx = x - xi, dy = y - yi, dz = zz - zi;
+    auto co = [&](int ox, int oy, int oz) {
+        return __ldg(&table[(((static_cast<size_t>(maxc) * res + (zi + oz)) * res + (yi + oy)) * res + (xi + ox))]);
+    };
+    float4 c000 = co(0, 0, 0), c100 = co(1, 0, 0), c010 = co(0, 1, 0), c110 = co(1, 1, 0);
+    float4 c001 = co(0, 0, 1), c101 = co(1, 0, 1), c011 = co(0, 1, 1), c111 = co(1, 1, 1);
+    auto tri = [&](float a000, float a100, float a010, float a110, float a001, float a101, float a011, float a111) {
+        float x00 = lerpf(dx, a000, a100), x10 = lerpf(dx, a010, a110);
+        float x01 = lerpf(dx, a001, a101), x11 = lerpf(dx, a011, a111);
+        return lerpf(dz, lerpf(dy, x00, x10), lerpf(dy, x01, x11));
+    };
+    c[0] = tri(c000.x, c100.x, c010.x, c110.x, c001.x, c101.x, c011.x, c111.x);
+    c[1] = tri(c000.y, c100.y, c010.y, c110.y, c001.y, c101.y, c011.y, c111.y);
+    c[2] = tri(c000.z, c100.z, c010.z, c110.z, c001.z, c101.z, c011.z, c111.z);
+}
+
+// Bilinear lookup of the map (texel centres at (i + 0.5) / size, u wraps,
+// v clamps).
+__device__ __forceinline__ f3 env_texel(const DeviceScene &s, float u, float v) {
+    const int W = static_cast<int>(s.env.width), H = static_cast<int>(s.env.height);
+    float x = u * W - 0.5f, y = v * H - 0.5f;
+    float fx = floorf(x), fy = floorf(y);
+    float tx = x - fx, ty = y - fy;
+    int x0 = static_cast<int>(fx), y0 = static_cast<int>(fy);
+    int x1 = x0 + 1, y1 = y0 + 1;
+    x0 = ((x0 % W) + W) % W;
+    x1 = ((x1 % W) + W) % W;
+    y0 = y0 < 0 ? 0 : (y0 > H - 1 ? H - 1 : y0);
+    y1 = y1 < 0 ? 0 : (y1 > H - 1 ? H - 1 : y1);
+    float4 a = __ldg(&s.env_tex[y0 * W + x0]), b = __ldg(&s.env_tex[y0 * W + x1]);
+    float4 c = __ldg(&s.env_tex[y1 * W + x0]), d = __ldg(&s.env_tex[y1 * W + x1]);
+    auto bl = [&](float p, float q, float r, float t) { return lerpf(ty, lerpf(tx, p, q), lerpf(tx, r, t)); };
+    return {bl(a.x, b.x, c.x, d.x), bl(a.y, b.y, c.y, d.y), bl(a.z, b.z, c.z, d.z)};
+}
+
+// SphericalMap::L: the map's RGB decoded as an illumination spectrum.
+template <int N>
+__device__ __forceinline__ Spec<N> env_L(const DeviceScene &s, float u, float v, const Wavelengths<N> &wl) {
+    f3 rgb = env_texel(s, u, v);
+    float c[4];
+    rgb2spec_unbound(s.rgb2spec, rgb, c);
+    Spec<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        r.v[i] = sigmoid_poly(c[0], c[1], c[2], wl.lambda[i]) * c[3] * cie_spd(c_spec.d65, wl.lambda[i]) * s.env.scale;
+    return r;
+}
+
+// AliasTable2D::PDF (alias2d.cpp:94-98).
+__device__ __forceinline__ float env_map_pdf(const DeviceScene &s, float u, float v) {
+    uint32_t W = s.env.width, H = s.env.height;
+    uint32_t iu = min(static_cast<uint32_t>(fmaxf(u * W, 0.0f)), W - 1u);
+    uint32_t iv = min(static_cast<uint32_t>(fmaxf(v * H, 0.0f)), H - 1u);
+    return s.env.integral > 0.0f ? __ldg(&s.env_cond_func[iv * W + iu]) / s.env.integral : 0.0f;
+}
+
+// spherical_theta / spherical_phi of a map-space direction.
+__device__ __forceinline__ void env_uv(f3 local, float &u, float &v, float &sin_theta) {
+    float theta = acosf(clampf(local.z, -1.0f, 1.0f));
+    float phi = atan2f(local.y, local.x);
+    if (phi < 0.0f) phi += k2Pi;
+    u = phi * kInv2Pi;
+    v = theta * kInvPi;
+    sin_theta = sinf(theta);
+}
+
+// SphericalMap::evaluate_wi for a world direction (escaped rays).
+template <int N>
+__device__ __forceinline__ void env_eval(const DeviceScene &s, f3 world_dir, const Wavelengths<N> &wl, Spec<N> &L,
+                                         float &pdf) {
+    f3 local = xform_vector(s.env.w2o, world_dir);
+    float u, v, st;
+    env_uv(local, u, v, st);
+    L = env_L<N>(s, u, v, wl);
+    float p = env_map_pdf(s, u, v) / (k2Pi * kPi * st);
+    pdf = st == 0.0f ? 0.0f : p;
+}
+
+// AliasTable::sample_continuous (alias.h:148-181) over one alias table.
+__device__ __forceinline__ float alias_continuous(const AliasEntry *table, uint32_t size, float u, uint32_t &ofs) {
+    u = u * static_cast<float>(size);
+    uint32_t idx = min(static_cast<uint32_t>(u), size - 1u);
+    u = fminf(u - static_cast<float>(idx), kOneMinusEpsilon);
+    AliasEntry e = table[idx];
+    bool keep = u < e.prob;
+    float ur = keep ? fminf(u / e.prob, kOneMinusEpsilon) : fminf((1.0f - u) / (1.0f - e.prob), kOneMinusEpsilon);
+    ofs = keep ? idx : e.alias;
+    return (static_cast<float>(ofs) + ur) / static_cast<float>(size);
+}
+
+// SphericalMap::sample_wi -> AliasTable2D::sample_continuous (alias2d.cpp:100-120)
+// and SphericalMap::evaluate (spherical.cpp:117-138).
+template <int N>
+__device__ __forceinline__ void env_sample(const DeviceScene &s, f3 p_ref, f2 u, const Wavelengths<N> &wl, Spec<N> &L,
+                                           float &pdf, f3 &p_light) {
+    uint32_t W = s.env.width, H = s.env.height;
+    uint32_t iv;
+    float fv = alias_continuous(s.env_marginal, H, u.y, iv);
+    float pdf_v = s.env.integral > 0.0f ? __ldg(&s.env_marginal_func[iv]) / s.env.integral : 0.0f;
+    uint32_t iu;
+    float fu = alias_continuous(s.env_cond + static_cast<size_t>(iv) * W, W, u.x, iu);
+    float integral_u = __ldg(&s.env_marginal_func[iv]);
+    float func_u = __ldg(&s.env_cond_func[static_cast<size_t>(iv) * W + iu]);
+    float pdf_u = integral_u > 0.0f ? func_u / integral_u : 0.0f;
+    float pdf_map = pdf_u * pdf_v;
+    float theta = fv * kPi, phi = fu * k2Pi;
+    float st = sinf(theta), ct = cosf(theta);
+    f3 local = {st * cosf(phi), st * sinf(phi), ct};
+    f3 world_dir = normalize(xform_vector(s.env.o2w, local));
+    float p = pdf_map / (k2Pi * kPi * st);
+    pdf = isinf(p) ? 0.0f : p;
+    L = env_L<N>(s, fu, fv, wl);
+    p_light = p_ref + world_dir * s.env.world_diameter;
+}
+
+}  // namespace vs

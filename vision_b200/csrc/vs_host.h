@@ -36,6 +36,12 @@ struct HostScene {
     std::vector<float> light_pmf;
     // Spectral samples of named SPDs (metal eta/k, glass ior), concatenated.
     std::vector<float> spd;
+    // Spherical environment light (at most one) and its 2D alias warper.
+    bool has_env = false;
+    EnvLight env{};
+    std::vector<float> env_tex;  // 4 floats (RGB, 0) per texel, row-major from the zenith
+    std::vector<AliasEntry> env_marginal, env_cond;
+    std::vector<float> env_marginal_func, env_cond_func;
     bool needs_luts = false;
     std::string lut_cache;
     Camera cam{};
@@ -61,7 +67,8 @@ void build_bvh8(HostScene &scene);
 // Vose alias table with the reference's layout and float arithmetic
 // (src/render_core/warpers/alias.h:86-122); fills entries and the PMF of every
 // entry (func / (integral * size)).
-void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &entries, std::vector<float> &pmf);
+void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &entries, std::vector<float> &pmf,
+                 float *integral = nullptr);
 
 // RGB -> spectrum coefficient table (3 x 64^3 x float4) and its decoders.
 const float *rgb2spec_table(const std::string &cache_path);

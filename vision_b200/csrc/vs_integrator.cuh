@@ -5,6 +5,7 @@
 
 #include "vs_device.cuh"
 #include "vs_bsdf.cuh"
+#include "vs_env.cuh"
 
 namespace vs {
 
@@ -124,6 +125,12 @@ __device__ __forceinline__ LightSample<N> sample_light(const DeviceScene &s, con
         li = static_cast<uint32_t>(fminf(u_light * static_cast<float>(n), static_cast<float>(n) - 1.0f));
         pmf_light = 1.0f / static_cast<float>(n);
     }
+    if (s.has_env && li == s.env_index) {
+        // SphericalMap::sample_wi (spherical.cpp:180-186).
+        env_sample<N>(s, it.pos, u, wl, ls.L, ls.pdf, ls.p_light);
+        ls.pdf *= pmf_light;
+        return ls;
+    }
     AreaLight L = s.lights[li];
     float ux = u.x;
     uint32_t local = alias_sample(s.prim_alias + L.alias_offset, L.prim_count, u.x, &ux);
@@ -204,7 +211,20 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
         RayPre rp = precompute_ray(ro, rd);
         Hit hit;
         float t_hit;
-        if (!trace_closest(s, rp, 3.402823466e+38f, hit, t_hit)) break;  // no environment light
+        if (!trace_closest(s, rp, 3.402823466e+38f, hit, t_hit)) {
+            // IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132).
+            if (s.has_env) {
+                Spec<N> Le;
+                float lpdf;
+                env_eval<N>(s, normalize((ro + rd) - ro), wl, Le, lpdf);
+                lpdf *= light_pmf<N>(s, s.env_index);
+                float weight = scatter_pdf / (scatter_pdf + lpdf);
+                if (ip.mis_mode == 2u) weight = 1.0f;
+                else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
+                ret += linear_srgb<N>(Le * throughput * weight, wl);
+            }
+            break;
+        }
         Interaction it = surface_interaction(s, hit, rd, true);
         if (it.light != kInvalid) {
             Spec<N> Le;

@@ -61,6 +61,19 @@ struct alignas(16) Instance {
     uint32_t prim_count;
 };
 
+// Spherical environment map (src/render_core/lights/environments/spherical.cpp)
+// with its 2D alias warper (src/render_core/warpers/alias2d.cpp).
+struct alignas(16) EnvLight {
+    m4 w2o;               // world -> map space (includes the map's x-rotation)
+    m4 o2w;
+    uint32_t width, height;
+    float scale;
+    float integral;       // marginal integral of the 2D warper
+    float world_diameter; // distance of sampled light points
+    float lum_power;      // luminance of pi r^2 * average colour (power light sampler)
+    uint32_t pad0, pad1;
+};
+
 // Alias-table entry (reference src/render_core/warpers/alias.h AliasEntry).
 struct AliasEntry {
     float prob;

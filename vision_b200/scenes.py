@@ -95,3 +95,71 @@ def material_room(width=64, height=64, dimension=4, sampler="independent", max_d
     mats["Floor"].update({"type": "principled_bsdf", "param": {
         "color": [0.8, 0.5, 0.3], "metallic": 0.4, "roughness": 0.35}})
     return sc
+
+
+def _draw_material(rng, name):
+    """One of the three material families, drawn uniformly, with the
+    parameter distributions of the large-scene workload."""
+    kind = rng.integers(0, 3)
+    if kind == 0:
+        return {"type": "metal", "name": name,
+                "param": {"material_name": "Au", "roughness": float(rng.uniform(0.05, 0.5))}}
+    if kind == 1:
+        return {"type": "glass", "name": name,
+                "param": {"color": [1.0, 1.0, 1.0], "roughness": 0.01,
+                          "ior": {"type": "cauchy", "param": {"A": 1.5, "B": 0.0042}}}}
+    return {"type": "principled_bsdf", "name": name,
+            "param": {"color": [float(x) for x in rng.uniform(0.0, 1.0, 3)],
+                      "metallic": float(rng.uniform(0.0, 1.0)),
+                      "roughness": float(rng.uniform(0.1, 0.9))}}
+
+
+def large_scene(width=1024, height=1024, max_depth=16, dimension=4, sampler="pcg", seed=1,
+                subdivisions=7, grid=1000, tiles=10, sky_width=2048, sky_height=1024):
+    """Seeded large scene: a displaced subdivided icosphere (value-noise
+    displacement of amplitude 0.05, seed 1) on a grid x grid ground split into
+    tiles x tiles objects; per-object materials drawn uniformly from a GGX gold
+    conductor (roughness U[0.05, 0.5]), a dispersive glass (Cauchy A = 1.5,
+    B = 0.0042) and a principled BSDF (baseColor U[0,1]^3, metallic U[0,1],
+    roughness U[0.1, 0.9]); lit by a procedural 2048 x 1024 HDR sky
+    (gradient plus a 5-degree sun lobe peaking at 5e4)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    materials = [_draw_material(rng, "sphere_mat")]
+    shapes = [{"type": "icosphere", "name": "sphere",
+               "param": {"subdivisions": subdivisions, "radius": 1.0, "material": "sphere_mat",
+                         "displacement": {"amplitude": 0.05, "frequency": 4.0, "seed": seed},
+                         "transform": _cols((1, 0, 0), (0, 1, 0), (0, 0, 1), (0, 1.0, 0))}}]
+    extent = 40.0
+    per = grid // tiles
+    tsize = extent / tiles
+    for j in range(tiles):
+        for i in range(tiles):
+            name = "ground_%d_%d" % (i, j)
+            materials.append(_draw_material(rng, name + "_mat"))
+            cx = -extent / 2 + (i + 0.5) * tsize
+            cz = -extent / 2 + (j + 0.5) * tsize
+            shapes.append({"type": "grid", "name": name,
+                           "param": {"nx": per, "nz": per, "size_x": tsize, "size_z": tsize,
+                                     "material": name + "_mat",
+                                     "transform": _cols((1, 0, 0), (0, 1, 0), (0, 0, 1), (cx, 0.0, cz))}})
+    sky = {"type": "spherical", "param": {
+        "color": {"channels": "xyz", "node": {"type": "sky", "param": {
+            "width": sky_width, "height": sky_height, "sun_elevation": 35.0, "sun_azimuth": 40.0,
+            "sun_radius": 5.0, "sun_peak": 5e4}}},
+        "scale": 1.0}}
+    return {
+        "shapes": shapes,
+        "materials": materials,
+        "camera": {"type": "pinhole", "param": {
+            "fov_y": 40.0,
+            "transform": {"type": "look_at", "param": {"position": [0.0, 2.2, 5.0], "target_pos": [0.0, 0.9, 0.0],
+                                                       "up": [0.0, 1.0, 0.0]}},
+            "radiance_collector": {"type": "normal", "param": {"resolution": [width, height], "exposure": 1.0}},
+            "filter": {"type": "box", "param": {"radius": [0.5, 0.5]}}}},
+        "integrator": {"type": "pt", "param": {"max_depth": max_depth, "min_depth": 5, "rr_threshold": 1.0}},
+        "spectrum": {"type": "hero", "param": {"dimension": dimension}},
+        "sampler": {"type": sampler, "param": {"seed": 0}},
+        "light_sampler": {"type": "uniform", "param": {"lights": [sky]}},
+        "render_setting": {"polymorphic_mode": 1},
+    }
