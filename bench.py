@@ -1,9 +1,13 @@
 """Benchmark of the spectral path-tracing hot path on B200.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload box_room]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload large_scene|box_room]
 
-One step renders the whole workload once (every pixel, every frame of its spp,
-through vs_render on the GPU).  value = paths of all ranks / max-over-ranks
+Workloads: `large_scene` (default) — the 2.3 M-triangle seeded scene
+(displaced icosphere on a 1000 x 1000 ground of 100 material tiles, GGX gold /
+dispersive glass / principled materials, procedural HDR sky), 1024 x 1024,
+64 spp, max depth 16; `box_room` — the 36-triangle box room, 256 x 256, 16 spp,
+max depth 8.  One step renders the whole workload once (every pixel, every
+frame of its spp, through vs_render on the GPU).  value = paths of all ranks / max-over-ranks
 device time of the K timed steps, in Mpaths/s.  Multi-GPU runs are
 independent replicas (weak scaling); the path has no exchange step.
 --impl reference times the reference integrator's CPU restatement (the
@@ -26,7 +30,13 @@ WORKLOADS = {
     # Box room: 256 x 256, 16 spp, max depth 8, 4 hero wavelengths, 6500 K
     # blackbody light, PCG sampler seed 0, FP32 film.
     'box_room': dict(kind='box_room', width=256, height=256, spp=16, max_depth=8, dimension=4, sampler='pcg', seed=0),
+    # Large seeded scene: 1024 x 1024, 64 spp, max depth 16, 4 hero
+    # wavelengths, PCG sampler, scene seed 1, FP32 film.
+    'large_scene': dict(kind='large_scene', width=1024, height=1024, spp=64, max_depth=16, dimension=4, sampler='pcg',
+                        seed=1),
 }
+DEFAULT_WORKLOAD = 'large_scene'
+DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5}
 
 
 def workload_scene(name):
@@ -35,7 +45,15 @@ def workload_scene(name):
     if w['kind'] == 'box_room':
         return scenes.box_room(width=w['width'], height=w['height'], max_depth=w['max_depth'],
                                dimension=w['dimension'], sampler=w['sampler'], seed=w['seed'])
+    if w['kind'] == 'large_scene':
+        return scenes.large_scene(width=w['width'], height=w['height'], max_depth=w['max_depth'],
+                                  dimension=w['dimension'], sampler=w['sampler'], seed=w['seed'])
     raise ValueError(name)
+
+
+def sample_pixels(width, height, count, seed=5):
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(width * height, size=min(count, width * height), replace=False)).astype(np.uint32)
 
 
 def measured_peaks():
@@ -98,22 +116,25 @@ class ClockSampler:
                 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_baseline(scene, budget_s=12.0):
+def cpu_baseline(scene, spp, budget_s=12.0):
     """The oracle (a scalar C++ port of the reference integrator) on all host
-    cores, on whole frames of the same workload until the time budget is used."""
+    cores, on a fixed seeded subset of the workload's pixels, frame after frame
+    until the time budget is used."""
     import oracle
     o = oracle.OracleScene(scene)
     threads = os.cpu_count()
-    npix = o.width * o.height
+    pixels = sample_pixels(o.width, o.height, 16384)
+    o.paths(pixels[:256], 0, 1, threads=threads)  # warm-up
     frames = 0
     t0 = time.perf_counter()
-    while frames < 16 and time.perf_counter() - t0 < budget_s:
-        o.render(frames, 1, threads=threads)
+    while frames < spp and time.perf_counter() - t0 < budget_s:
+        o.paths(pixels, frames, 1, threads=threads)
         frames += 1
     dt = time.perf_counter() - t0
-    return {'value': frames * npix / dt / 1e6, 'unit': 'Mpaths/s', 'cores': threads, 'kind': 'port',
-            'sample': '%d of 16 frames of the %dx%d workload (%d paths) in %.1f s' % (frames, o.width, o.height,
-                                                                                    frames * npix, dt)}
+    paths = frames * pixels.size
+    return {'value': paths / dt / 1e6, 'unit': 'Mpaths/s', 'cores': threads, 'kind': 'port',
+            'sample': '%d seeded pixels x %d frames of the %dx%d workload (%d paths) in %.1f s' % (
+                pixels.size, frames, o.width, o.height, paths, dt)}
 
 
 def run_reference(args, rank):
@@ -128,22 +149,23 @@ def run_reference(args, rank):
     scene = vb.Scene(ctx, workload_scene(args.workload)).build_accel()
     o = oracle.OracleScene(scene)
     threads = os.cpu_count()
-    npix = o.width * o.height
+    pixels = sample_pixels(o.width, o.height, 16384)
+    npix = pixels.size
     for i in range(args.warmup):
-        o.render(i % w['spp'], 1, threads=threads)
+        o.paths(pixels, i % w['spp'], 1, threads=threads)
     t0 = time.perf_counter()
     for i in range(args.steps):
-        o.render(i % w['spp'], 1, threads=threads)
+        o.paths(pixels, i % w['spp'], 1, threads=threads)
     dt = time.perf_counter() - t0
     value = args.steps * npix / dt / 1e6
     line = {'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': args.gpus, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': dt * 1e3 / args.steps, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
             'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
-                       'step': 'one 1-spp frame of the workload per step'},
+                       'step': '1 spp of 16384 seeded pixels of the workload per step'},
             'impl': 'reference',
             'cpu_baseline': {'value': value, 'unit': 'Mpaths/s', 'cores': threads, 'kind': 'port',
-                             'sample': '1 frame (%d paths) per step' % npix},
+                             'sample': '16384 seeded pixels x 1 frame (%d paths) per step' % npix},
             'e2e': {'value': value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line))
 
@@ -151,12 +173,14 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=100)
+    ap.add_argument('--steps', type=int, default=None)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='box_room', choices=sorted(WORKLOADS))
+    ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.impl == 'reference' else DEFAULT_STEPS[args.workload]
     rank = int(os.environ.get('RANK', '0'))
     world = int(os.environ.get('WORLD_SIZE', '1'))
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))
@@ -266,7 +290,7 @@ def main():
         'gpu_launches': int(launches),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line['cpu_baseline'] = cpu_baseline(scene)
+        line['cpu_baseline'] = cpu_baseline(scene, spp)
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -48,6 +48,9 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         P = ctypes.c_void_p
         U = ctypes.c_uint32
+        L.oracle_open.argtypes = [P]
+        L.oracle_open.restype = P
+        L.oracle_close.argtypes = [P]
         L.oracle_trace_closest.argtypes = [P, P, U, P, P]
         L.oracle_trace_any.argtypes = [P, P, U, P]
         L.oracle_paths.argtypes = [P, P, U, U, U, U, P]
@@ -94,33 +97,42 @@ class OracleScene:
                                    *([_p(a[k]) for k in ('env', 'env_tex', 'env_marginal', 'env_marginal_func',
                                                          'env_cond', 'env_cond_func', 'rgb2spec')]
                                      if env.size else [None] * 7))
+        self.h = ctypes.c_void_p(lib().oracle_open(ctypes.byref(self.s)))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().oracle_close(self.h)
+                self.h = None
+        except Exception:
+            pass
 
     def trace_closest(self, rays):
         rays = np.ascontiguousarray(rays, np.float32)
         n = rays.shape[0]
         hits = np.zeros((n, 4), np.uint32)
         t = np.zeros(n, np.float32)
-        lib().oracle_trace_closest(ctypes.byref(self.s), _p(rays), n, _p(hits), _p(t))
+        lib().oracle_trace_closest(self.h, _p(rays), n, _p(hits), _p(t))
         return hits, t
 
     def trace_any(self, rays):
         rays = np.ascontiguousarray(rays, np.float32)
         occ = np.zeros(rays.shape[0], np.uint32)
-        lib().oracle_trace_any(ctypes.byref(self.s), _p(rays), rays.shape[0], _p(occ))
+        lib().oracle_trace_any(self.h, _p(rays), rays.shape[0], _p(occ))
         return occ
 
     def render(self, frame_begin, frame_count, threads=None, fp64=False):
         threads = threads or os.cpu_count()
         film = np.zeros((self.height, self.width, 4), np.float32)
         f64 = np.zeros((self.height, self.width, 4), np.float64) if fp64 else None
-        lib().oracle_render(ctypes.byref(self.s), frame_begin, frame_count, threads, _p(film),
+        lib().oracle_render(self.h, frame_begin, frame_count, threads, _p(film),
                             _p(f64) if fp64 else None)
         return (film, f64) if fp64 else film
 
     def paths(self, pixels, frame_begin, frame_count, threads=None):
         pixels = np.ascontiguousarray(pixels, np.uint32)
         out = np.zeros((frame_count, pixels.size, 3), np.float32)
-        lib().oracle_paths(ctypes.byref(self.s), _p(pixels), pixels.size, frame_begin, frame_count,
+        lib().oracle_paths(self.h, _p(pixels), pixels.size, frame_begin, frame_count,
                            threads or os.cpu_count(), _p(out))
         return out
 

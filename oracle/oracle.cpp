@@ -1289,12 +1289,17 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
 
 extern "C" {
 
-int oracle_version(void) { return 1; }
+int oracle_version(void) { return 2; }
+
+// A prepared scene (the oracle's BVH is built once per handle).
+void *oracle_open(const oracle_scene *s) { return new oracle::Scene(s); }
+void oracle_close(void *h) { delete static_cast<oracle::Scene *>(h); }
 
 // Closest hit for n rays (8 floats each: origin, unused, direction, tmax).
 // hits: 4 uint32 per ray (inst, prim, u bits, v bits); t: -1 on a miss.
-int oracle_trace_closest(const oracle_scene *s, const float *rays, uint32_t n, uint32_t *hits, float *t) {
-    oracle::Scene sc(s);
+int oracle_trace_closest(void *handle, const float *rays, uint32_t n, uint32_t *hits, float *t) {
+    const oracle::Scene &sc = *static_cast<oracle::Scene *>(handle);
+    const oracle_scene *s = sc.s;
     for (uint32_t i = 0; i < n; ++i) {
         const float *r = rays + 8 * i;
         oracle::RayPre rp = oracle::precompute({r[0], r[1], r[2]}, {r[4], r[5], r[6]});
@@ -1314,8 +1319,8 @@ int oracle_trace_closest(const oracle_scene *s, const float *rays, uint32_t n, u
     return 0;
 }
 
-int oracle_trace_any(const oracle_scene *s, const float *rays, uint32_t n, uint32_t *occ) {
-    oracle::Scene sc(s);
+int oracle_trace_any(void *handle, const float *rays, uint32_t n, uint32_t *occ) {
+    const oracle::Scene &sc = *static_cast<oracle::Scene *>(handle);
     for (uint32_t i = 0; i < n; ++i) {
         const float *r = rays + 8 * i;
         occ[i] = oracle::any_hit(sc, oracle::precompute({r[0], r[1], r[2]}, {r[4], r[5], r[6]}), r[7]) ? 1u : 0u;
@@ -1325,9 +1330,9 @@ int oracle_trace_any(const oracle_scene *s, const float *rays, uint32_t n, uint3
 
 // Per-path radiance of the listed pixels for frames [frame_begin, frame_begin+frame_count):
 // out[(f * npix_list + k) * 3 + c].
-int oracle_paths(const oracle_scene *s, const uint32_t *pixels, uint32_t npix_list, uint32_t frame_begin,
+int oracle_paths(void *handle, const uint32_t *pixels, uint32_t npix_list, uint32_t frame_begin,
                  uint32_t frame_count, uint32_t threads, float *out) {
-    oracle::Scene sc(s);
+    const oracle::Scene &sc = *static_cast<oracle::Scene *>(handle);
     uint64_t total = static_cast<uint64_t>(npix_list) * frame_count;
     std::atomic<uint64_t> next{0};
     auto work = [&]() {
@@ -1358,9 +1363,9 @@ int oracle_paths(const oracle_scene *s, const uint32_t *pixels, uint32_t npix_li
 // Full-frame render with the reference film semantics: FP32 running mean of
 // zero_if_nan_inf(L) (normal.cpp:87-101) into film32 (4 floats per pixel) and,
 // when film64 is non-null, FP64 sums (r, g, b, count) per pixel.
-int oracle_render(const oracle_scene *s, uint32_t frame_begin, uint32_t frame_count, uint32_t threads, float *film32,
+int oracle_render(void *handle, uint32_t frame_begin, uint32_t frame_count, uint32_t threads, float *film32,
                   double *film64) {
-    oracle::Scene sc(s);
+    const oracle::Scene &sc = *static_cast<oracle::Scene *>(handle);
     uint32_t npix = sc.cam.width * sc.cam.height;
     std::atomic<uint32_t> next{0};
     auto work = [&]() {
