@@ -178,6 +178,8 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--spp', type=int, default=None,
+                    help='override the workload spp (profiling runs on a smaller launch; reported in config)')
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if args.impl == 'reference' else DEFAULT_STEPS[args.workload]
@@ -196,7 +198,9 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.spp:
+        w['spp'] = args.spp
     ctx = vb.Context(local_rank)
     scene = vb.Scene(ctx, workload_scene(args.workload))
     t0 = time.perf_counter()

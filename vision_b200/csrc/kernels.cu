@@ -45,7 +45,10 @@ __global__ void __launch_bounds__(128) k_trace_any(DeviceScene s, const float *r
 // Paths are numbered frame-major: path p covers pixel p % (w*h) of frame
 // frame_begin + p / (w*h), so neighbouring threads trace neighbouring pixels.
 template <int N>
-__global__ void __launch_bounds__(128) k_render(DeviceScene s, uint32_t frame_begin, uint64_t path_count,
+#ifndef VS_RENDER_MIN_BLOCKS
+#define VS_RENDER_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(128, VS_RENDER_MIN_BLOCKS) k_render(DeviceScene s, uint32_t frame_begin, uint64_t path_count,
                                                 float4 *radiance) {
     uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= path_count) return;

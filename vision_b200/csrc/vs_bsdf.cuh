@@ -240,7 +240,7 @@ struct Bsdf {
         if (same == trans) e.pdf = 0.0f;
     }
 
-    __device__ BsdfEval<N> evaluate(f3 wo_w, f3 wi_w, float *eta_out) const {
+    __device__ VS_OUTLINE BsdfEval<N> evaluate(f3 wo_w, f3 wi_w, float *eta_out) const {
         BsdfEval<N> e;
         f3 wo = frame.to_local(wo_w), wi = frame.to_local(wi_w);
         float eta = 1.0f;
@@ -308,7 +308,7 @@ struct Bsdf {
         return e;
     }
 
-    __device__ BsdfSample<N> sample(f3 wo_w, Sampler &smp) const {
+    __device__ VS_OUTLINE BsdfSample<N> sample(f3 wo_w, Sampler &smp) const {
         BsdfSample<N> bs;
         bs.eta = 1.0f;
         f3 wo = frame.to_local(wo_w);
@@ -360,7 +360,7 @@ struct Bsdf {
 // Material::create_evaluator for the in-scope plugins.  The lobe parameters
 // come from the 64-byte material record written by the scene loader.
 template <int N>
-__device__ Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng, f3 wo,
+__device__ VS_OUTLINE Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng, f3 wo,
                              const Wavelengths<N> &wl) {
     Bsdf<N> b;
     b.type = m.type;

@@ -11,6 +11,13 @@
 #include "vs_devscene.h"
 #include <cuda_runtime.h>
 
+// Large device functions called from several places in the megakernel are
+// kept out of line so that one copy of their code serves every call site
+// (the megakernel is front-end bound on instruction fetch otherwise).
+#ifndef VS_OUTLINE
+#define VS_OUTLINE __noinline__
+#endif
+
 namespace vs {
 
 // ---------------------------------------------------------------------------
@@ -160,7 +167,7 @@ __device__ __forceinline__ Wavelengths<N> sample_wavelengths(float u) {
 
 // HeroWavelengthSpectrum::cie_xyz + xyz_to_linear_srgb (hero.cpp:261-285).
 template <int N>
-__device__ __forceinline__ f3 linear_srgb(const Spec<N> &s, const Wavelengths<N> &w) {
+__device__ VS_OUTLINE f3 linear_srgb(const Spec<N> &s, const Wavelengths<N> &w) {
     f3 sum = make3(0.0f);
     int valid = 0;
 #pragma unroll

@@ -102,7 +102,7 @@ __device__ __forceinline__ void env_uv(f3 local, float &u, float &v, float &sin_
 
 // SphericalMap::evaluate_wi for a world direction (escaped rays).
 template <int N>
-__device__ __forceinline__ void env_eval(const DeviceScene &s, f3 world_dir, const Wavelengths<N> &wl, Spec<N> &L,
+__device__ VS_OUTLINE void env_eval(const DeviceScene &s, f3 world_dir, const Wavelengths<N> &wl, Spec<N> &L,
                                          float &pdf) {
     f3 local = xform_vector(s.env.w2o, world_dir);
     float u, v, st;
@@ -127,7 +127,7 @@ __device__ __forceinline__ float alias_continuous(const AliasEntry *table, uint3
 // SphericalMap::sample_wi -> AliasTable2D::sample_continuous (alias2d.cpp:100-120)
 // and SphericalMap::evaluate (spherical.cpp:117-138).
 template <int N>
-__device__ __forceinline__ void env_sample(const DeviceScene &s, f3 p_ref, f2 u, const Wavelengths<N> &wl, Spec<N> &L,
+__device__ VS_OUTLINE void env_sample(const DeviceScene &s, f3 p_ref, f2 u, const Wavelengths<N> &wl, Spec<N> &L,
                                            float &pdf, f3 &p_light) {
     uint32_t W = s.env.width, H = s.env.height;
     uint32_t iv;

@@ -112,7 +112,7 @@ __device__ __forceinline__ float light_pmf(const DeviceScene &s, uint32_t light)
 }
 
 template <int N>
-__device__ __forceinline__ LightSample<N> sample_light(const DeviceScene &s, const Interaction &it, float u_light,
+__device__ VS_OUTLINE LightSample<N> sample_light(const DeviceScene &s, const Interaction &it, float u_light,
                                                        f2 u, const Wavelengths<N> &wl) {
     LightSample<N> ls;
     uint32_t n = s.ip.light_count;
@@ -163,7 +163,7 @@ __device__ __forceinline__ LightSample<N> sample_light(const DeviceScene &s, con
 // LightSampler::evaluate_hit_wi (lightsampler.cpp:252-267) for a path that hit
 // an emissive primitive; p_ref is the ray origin.
 template <int N>
-__device__ __forceinline__ void eval_hit_light(const DeviceScene &s, const Interaction &it, f3 p_ref,
+__device__ VS_OUTLINE void eval_hit_light(const DeviceScene &s, const Interaction &it, f3 p_ref,
                                                const Wavelengths<N> &wl, Spec<N> &L, float &pdf) {
     AreaLight light = s.lights[it.light];
     float pmf_prim = s.prim_pmf[light.alias_offset + (it.prim - light.first_prim)];
