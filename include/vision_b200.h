@@ -186,6 +186,39 @@ int vs_render_stats(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count,
  * The scene must have been built with vs_scene_build_accel. */
 int vs_render_noalloc(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, float *film, void *stream);
 
+/* Real-time ReSTIR frame for a scene loaded with integrator type "rt"
+ * (reference RealTimeIntegrator::render, src/render_core/integrators/rt.cpp:144-160):
+ * direct pass (ReSTIRDI shader0/shader1, ReSTIR/direct.cpp:519-557,638-674),
+ * indirect pass (ReSTIRGI initial/temporal/spatial, ReSTIR/indirect.cpp:354-362)
+ * and the combine kernel (rt.cpp:118-126), which adds direct + indirect into
+ * the FP32 film as sample `film_index` of its running mean (0 restarts it).
+ * `frame_index` selects the sampler streams and the reservoir/surface buffer
+ * parity.  The camera of the previous vs_restir_frame call provides the
+ * motion vectors (Sensor::store_prev_data, sensor.cpp:99-103); the first
+ * frame after a reset uses the current camera.  Asynchronous on `stream`. */
+int vs_restir_frame(vs_scene *scene, uint32_t frame_index, uint32_t film_index, void *stream);
+
+/* Clears the ReSTIR history (surfaces, reservoirs, previous camera)
+ * (ReSTIRDI/ReSTIRGI::prepare, direct.cpp:676-686, indirect.cpp:377-391). */
+int vs_restir_reset(vs_scene *scene);
+
+/* Parameter block that vs_restir_frame(scene, frame_index, ...) would use now
+ * (resampling settings, camera transforms, previous camera):
+ * VS_RESTIR_PARAMS_BYTES bytes.  Works on host-only contexts. */
+#define VS_RESTIR_PARAMS_BYTES 432
+int vs_restir_params(const vs_scene *scene, uint32_t frame_index, void *dst, size_t bytes);
+
+/* Copies a per-pixel ReSTIR buffer of the last frame to host memory. */
+#define VS_RESTIR_DI_RADIANCE 0  /* float4: direct radiance (linear sRGB) */
+#define VS_RESTIR_GI_RADIANCE 1  /* float4: indirect radiance */
+#define VS_RESTIR_MOTION 2       /* float2: motion vector in pixels */
+#define VS_RESTIR_SURFACES 3     /* 64 bytes: SurfaceData of the frame */
+#define VS_RESTIR_DI_RESERVOIRS 4 /* 64 bytes: direct reservoirs after spatial reuse */
+#define VS_RESTIR_GI_RESERVOIRS 5 /* 64 bytes: indirect reservoirs after spatial reuse */
+#define VS_RESTIR_HIT_BSDF 6     /* 32 bytes: BSDF sample of the direct pass */
+#define VS_RESTIR_GI_SAMPLES 7   /* 64 bytes: initial indirect samples */
+int vs_restir_download(vs_scene *scene, int which, void *dst, size_t bytes);
+
 /* Albedo tables of the energy-compensated lobes (164864 floats: PureReflection
  * 32^2, Dielectric and DielectricInv 32^3 x 2, Specular 32^3).  which = 0: the
  * values the renderer uses (the reference's precomputed_table.h); which = 1:

@@ -17,8 +17,8 @@ LIB_PATH = os.path.join(HERE, '_build', 'liboracle.so')
 
 
 def build():
-    src = os.path.join(HERE, 'oracle.cpp')
-    if os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ('oracle.cpp', 'restir.inc')]
+    if os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(s) for s in srcs):
         return LIB_PATH
     subprocess.run(['make', '-s', '-C', HERE], check=True)
     return LIB_PATH
@@ -63,6 +63,11 @@ def lib():
         L.oracle_cie_y_integral.restype = ctypes.c_float
         L.oracle_spd_eval.argtypes = [P, ctypes.c_int, ctypes.c_float]
         L.oracle_spd_eval.restype = ctypes.c_float
+        L.oracle_rt_open.argtypes = [P, U, U]
+        L.oracle_rt_open.restype = P
+        L.oracle_rt_close.argtypes = [P]
+        L.oracle_rt_frame.argtypes = [P, P, P, U, U]
+        L.oracle_rt_buffer.argtypes = [P, ctypes.c_int, P, ctypes.c_size_t]
         _lib = L
     return _lib
 
@@ -135,6 +140,41 @@ class OracleScene:
         lib().oracle_paths(self.h, _p(pixels), pixels.size, frame_begin, frame_count,
                            threads or os.cpu_count(), _p(out))
         return out
+
+
+class OracleRestir:
+    """CPU restatement of the real-time ReSTIR frame over an OracleScene."""
+
+    BUFFERS = dict(di_radiance=0, gi_radiance=1, motion=2, surfaces=3, di_reservoirs=4, gi_reservoirs=5,
+                   hit_bsdf=6, gi_samples=7, film=8)
+
+    def __init__(self, oscene, width, height):
+        self.oscene = oscene
+        self.width, self.height = width, height
+        self.h = ctypes.c_void_p(lib().oracle_rt_open(oscene.h, width, height))
+
+    def frame(self, camera, params, film_index, threads=None):
+        camera = np.ascontiguousarray(camera).view(np.uint8)
+        params = np.ascontiguousarray(params).view(np.uint8)
+        assert camera.nbytes == 112 and params.nbytes == 432
+        rc = lib().oracle_rt_frame(self.h, _p(camera), _p(params), film_index, threads or os.cpu_count())
+        if rc != 0:
+            raise ValueError('oracle_rt_frame rejected the parameters')
+
+    def buffer(self, which, dtype):
+        out = np.zeros(self.width * self.height, dtype)
+        rc = lib().oracle_rt_buffer(self.h, self.BUFFERS[which], _p(out), out.nbytes)
+        if rc != 0:
+            raise ValueError('oracle_rt_buffer(%s) failed: %d' % (which, rc))
+        return out.reshape((self.height, self.width) + out.shape[1:])
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().oracle_rt_close(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 def sampler_stream(px, py, sample, dim, n, kind=0, seed=0):

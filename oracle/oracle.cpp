@@ -1175,32 +1175,44 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
 }
 
 // ----- the path (pt.cpp:53-72; integrator.cpp:134-283) ------------------------
-static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) {
-    const Integrator &ip = sc.ip;
-    const Camera &cam = sc.cam;
-    int n = static_cast<int>(ip.spectrum_dim);
-    Sampler smp;
-    smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
-    Swl w = sample_wavelengths(n, smp.next());
-    smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
+static void check_dispersive(const Bsdf &bsdf, Swl &w) {
+    if (bsdf.dispersive && w.n > 1) {  // SampledWavelengths::check_dispersive
+        bool all = true;
+        for (int i = 1; i < w.n; ++i) all = all && w.pdf[i] != 0.0f;
+        if (all)
+            for (int i = 1; i < w.n; ++i) w.pdf[i] = 0.0f;
+    }
+}
+
+// Sampler::sensor_sample + box filter + Sensor::generate_ray (5 draws).
+static void camera_ray(const Camera &cam, Sampler &smp, uint32_t px, uint32_t py, float &film_x, float &film_y, V3 &ro,
+                       V3 &rd) {
     float fu = smp.next(), fv = smp.next();
     float fx = -cam.filter_rx + fu * (cam.filter_rx - -cam.filter_rx);
     float fy = -cam.filter_ry + fv * (cam.filter_ry - -cam.filter_ry);
     smp.next(); smp.next(); smp.next();
-    float film_x = static_cast<float>(px) + 0.5f + fx, film_y = static_cast<float>(py) + 0.5f + fy;
+    film_x = static_cast<float>(px) + 0.5f + fx;
+    film_y = static_cast<float>(py) + 0.5f + fy;
     float sx = cam.screen_lo_x + film_x / static_cast<float>(cam.width) * cam.screen_span_x;
     float sy = cam.screen_hi_y - film_y / static_cast<float>(cam.height) * cam.screen_span_y;
     V3 dc = normalize(v3(sx * cam.tan_half_fov, sy * cam.tan_half_fov, 1.0f));
     const float(*m)[4] = cam.c2w;
-    V3 ro = {m[3][0], m[3][1], m[3][2]};
-    V3 rd = normalize(v3(m[0][0] * dc.x + m[1][0] * dc.y + m[2][0] * dc.z, m[0][1] * dc.x + m[1][1] * dc.y + m[2][1] * dc.z,
-                         m[0][2] * dc.x + m[1][2] * dc.y + m[2][2] * dc.z));
-    float scatter_pdf = 1e16f;
+    ro = {m[3][0], m[3][1], m[3][2]};
+    rd = normalize(v3(m[0][0] * dc.x + m[1][0] * dc.y + m[2][0] * dc.z, m[0][1] * dc.x + m[1][1] * dc.y + m[2][1] * dc.z,
+                      m[0][2] * dc.x + m[1][2] * dc.y + m[2][2] * dc.z));
+}
+
+// IlluminationIntegrator::Li from ray (ro, rd) with a starting scatter pdf and
+// throughput; `first` receives the first surface hit (HitContext).
+static V3 path_li(const Scene &sc, Sampler &smp, Swl &w, V3 ro, V3 rd, float scatter_pdf, const float *thr0,
+                  uint32_t max_depth, It *first, bool *first_hit) {
+    const Integrator &ip = sc.ip;
+    int n = w.n;
     float thr[8];
-    for (int i = 0; i < n; ++i) thr[i] = 1.0f;
+    for (int i = 0; i < n; ++i) thr[i] = thr0[i];
     V3 ret = {0, 0, 0};
     float eta_scale = 1.0f;
-    for (uint32_t b = 0; b < ip.max_depth; ++b) {
+    for (uint32_t b = 0; b < max_depth; ++b) {
         RayPre rp = precompute(ro, rd);
         HitRec h = closest(sc, rp, FLT_MAX);
         if (h.prim == kInvalid) {
@@ -1219,6 +1231,10 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
             break;
         }
         It it = interaction(sc, h.prim, h.u, h.v, rd);
+        if (first && b == 0) {
+            *first = it;
+            if (first_hit) *first_hit = true;
+        }
         if (it.light != kInvalid) {
             const AreaLight &L = sc.lights[it.light];
             float pmf_p = sc.s->prim_pmf[L.alias_offset + (it.prim - L.first_prim)];
@@ -1245,12 +1261,7 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
         bool occ = any_hit(sc, precompute(offset_ray_origin(it.pos, nn), dir), 1.0f - kShadowEps);
         const Material &mt = sc.mat[it.mat];
         Bsdf bsdf = make_bsdf(sc, mt, it, w);
-        if (bsdf.dispersive && w.n > 1) {  // SampledWavelengths::check_dispersive
-            bool all = true;
-            for (int i = 1; i < w.n; ++i) all = all && w.pdf[i] != 0.0f;
-            if (all)
-                for (int i = 1; i < w.n; ++i) w.pdf[i] = 0.0f;
-        }
+        check_dispersive(bsdf, w);
         V3 wl = normalize(sub(ls.p, it.pos));
         Eval se = bsdf_eval(bsdf, it.wo, wl, nullptr);
         V3 wi_s;
@@ -1284,6 +1295,23 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
     }
     return ret;
 }
+
+static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) {
+    const Integrator &ip = sc.ip;
+    int n = static_cast<int>(ip.spectrum_dim);
+    Sampler smp;
+    smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
+    Swl w = sample_wavelengths(n, smp.next());
+    smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
+    float film_x, film_y;
+    V3 ro, rd;
+    camera_ray(sc.cam, smp, px, py, film_x, film_y, ro, rd);
+    float thr[8];
+    for (int i = 0; i < n; ++i) thr[i] = 1.0f;
+    return path_li(sc, smp, w, ro, rd, 1e16f, thr, ip.max_depth, nullptr, nullptr);
+}
+
+#include "restir.inc"
 
 }  // namespace oracle
 
@@ -1437,5 +1465,51 @@ void oracle_linear_srgb(uint32_t n, const float *lambda, const float *pdf, const
 float oracle_cie_y_integral(void) { return oracle::tables().y_integral; }
 
 float oracle_spd_eval(const float *f, int n, float lambda) { return oracle::spd_eval(f, n, lambda); }
+
+// Real-time ReSTIR state over an opened scene (restir.inc).
+void *oracle_rt_open(void *handle, uint32_t width, uint32_t height) {
+    return new oracle::rt::Frame(*static_cast<oracle::Scene *>(handle), width, height);
+}
+void oracle_rt_close(void *rt) { delete static_cast<oracle::rt::Frame *>(rt); }
+
+// One frame with the given camera block (112 bytes) and parameter block
+// (432 bytes, as vs_restir_params returns it).
+int oracle_rt_frame(void *rt, const void *camera, const void *params, uint32_t film_index, uint32_t threads) {
+    auto *f = static_cast<oracle::rt::Frame *>(rt);
+    oracle::Camera cam;
+    oracle::rt::Params p;
+    std::memcpy(&cam, camera, sizeof(cam));
+    std::memcpy(&p, params, sizeof(p));
+    if (p.width * p.height != f->npix || p.di.s_count > oracle::rt::kMaxNeighbours ||
+        p.gi.s_count > oracle::rt::kMaxNeighbours)
+        return 1;
+    f->run(cam, p, film_index, threads);
+    return 0;
+}
+
+// Per-pixel buffers of the last frame: 0 direct radiance, 1 indirect
+// radiance, 2 motion, 3 surfaces, 4 direct reservoirs, 5 indirect
+// reservoirs, 6 BSDF samples, 7 initial indirect samples, 8 film.
+int oracle_rt_buffer(void *rt, int which, void *dst, size_t bytes) {
+    auto *f = static_cast<oracle::rt::Frame *>(rt);
+    uint32_t c = f->cur();
+    const void *src = nullptr;
+    size_t n = 0;
+    switch (which) {
+        case 0: src = f->di_rad.data(); n = f->di_rad.size() * 4; break;
+        case 1: src = f->gi_rad.data(); n = f->gi_rad.size() * 4; break;
+        case 2: src = f->motion.data(); n = f->motion.size() * 4; break;
+        case 3: src = f->surf[c].data(); n = f->surf[c].size() * sizeof(oracle::rt::Surface); break;
+        case 4: src = f->di[c].data(); n = f->di[c].size() * sizeof(oracle::rt::DiRes); break;
+        case 5: src = f->gi[c].data(); n = f->gi[c].size() * sizeof(oracle::rt::GiRes); break;
+        case 6: src = f->hit_bsdf.data(); n = f->hit_bsdf.size() * sizeof(oracle::rt::HitBsdf); break;
+        case 7: src = f->gi_init.data(); n = f->gi_init.size() * sizeof(oracle::rt::GiRes); break;
+        case 8: src = f->film.data(); n = f->film.size() * 4; break;
+        default: return 1;
+    }
+    if (n != bytes) return 2;
+    std::memcpy(dst, src, n);
+    return 0;
+}
 
 }  // extern "C"

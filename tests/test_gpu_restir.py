@@ -1,0 +1,90 @@
+"""Real-time ReSTIR frame on the GPU against the oracle's restatement, frame by
+frame along a moving camera: same sampler streams and the same reservoir
+arithmetic on both sides (FP64 weight sums), so every buffer agrees per pixel
+up to FP32 rounding, which can flip a rare resampling decision; those flips
+then spread to the pixels that reuse the reservoir, so the bar is a per-pixel
+agreement fraction per frame plus agreement of the frame means."""
+import numpy as np
+import pytest
+
+import oracle
+from vision_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+F4 = np.dtype(('<f4', 4))
+
+
+def _close(a, b, rtol=2e-3, atol=1e-4):
+    return (np.abs(a - b) <= atol + rtol * np.abs(b))
+
+
+def _run(vb, ctx, sc, cams, w, h):
+    s = vb.Scene(ctx, sc).build_accel()
+    o = oracle.OracleScene(s)
+    ort = oracle.OracleRestir(o, w, h)
+    for f, c2w in enumerate(cams):
+        s.set_camera(c2w, 40.0)
+        params = s.restir_params(f)
+        cam = s.export('camera').copy()
+        s.restir_frame(f, 0)
+        ort.frame(cam, params, 0)
+        yield f, s, ort
+
+
+def test_restir_frames_match_oracle(vb, gpu_ctx):
+    w, h = 96, 64
+    sc = scenes.many_lights(w, h, emitters=300, seed=5, M_light=8, history_limit=20, spatial_neighbours=5,
+                            spatial_radius=12.0, max_depth=4)
+    cams = scenes.camera_spline(6, seed=3)
+    for f, s, ort in _run(vb, gpu_ctx, sc, cams, w, h):
+        gs, cs = s.restir_buffer('surfaces'), ort.buffer('surfaces', vb.RT_SURFACE_DTYPE)
+        hit_eq = (gs['hit']['inst_id'] == cs['hit']['inst_id']) & (gs['hit']['prim_id'] == cs['hit']['prim_id'])
+        assert hit_eq.mean() >= 0.999, (f, hit_eq.mean())
+        hit = cs['hit']['inst_id'] != 0xffffffff
+        assert hit.mean() > 0.5
+        mv_ok = _close(s.restir_buffer('motion'), ort.buffer('motion', np.dtype(('<f4', 2))), 1e-3, 1e-3).all(-1)
+        assert mv_ok.mean() >= 0.995, (f, mv_ok.mean())
+        gd, cd = s.restir_buffer('di_radiance')[..., :3], ort.buffer('di_radiance', F4)[..., :3]
+        gg, cg = s.restir_buffer('gi_radiance')[..., :3], ort.buffer('gi_radiance', F4)[..., :3]
+        assert np.all(np.isfinite(gd)) and np.all(np.isfinite(gg))
+        di_ok = _close(gd, cd).all(-1).mean()
+        gi_ok = _close(gg, cg).all(-1).mean()
+        thr = 0.97 if f == 0 else 0.90
+        assert di_ok >= thr, (f, di_ok)
+        assert gi_ok >= thr - 0.05, (f, gi_ok)
+        assert abs(gd.mean() - cd.mean()) <= 0.02 * cd.mean() + 1e-4, (f, gd.mean(), cd.mean())
+        assert abs(gg.mean() - cg.mean()) <= 0.05 * cg.mean() + 1e-4, (f, gg.mean(), cg.mean())
+        film = s.film()
+        np.testing.assert_allclose(film[..., :3], np.nan_to_num(gd + gg, posinf=0, neginf=0), rtol=1e-5, atol=1e-6)
+        gr = s.restir_buffer('di_reservoirs')
+        cr = ort.buffer('di_reservoirs', vb.DI_RESERVOIR_DTYPE)
+        same_light = (gr['light_index'] == cr['light_index'])[hit].mean()
+        assert same_light >= thr, (f, same_light)
+
+
+def test_restir_reset_restarts_history(vb, gpu_ctx):
+    w, h = 48, 32
+    sc = scenes.many_lights(w, h, emitters=50, seed=9, M_light=4, max_depth=3)
+    s = vb.Scene(gpu_ctx, sc).build_accel()
+    c2w = scenes.camera_c2w((0.0, 0.5, 1.85), (0.0, 0.5, 0.0))
+    s.set_camera(c2w, 40.0)
+    s.restir_frame(0, 0)
+    first = s.restir_buffer('di_radiance').copy()
+    s.restir_frame(1, 0)
+    s.restir_reset()
+    s.restir_frame(0, 0)
+    again = s.restir_buffer('di_radiance')
+    assert np.array_equal(first, again)
+
+
+def test_restir_film_accumulates(vb, gpu_ctx):
+    w, h = 32, 24
+    sc = scenes.many_lights(w, h, emitters=40, seed=1, M_light=4, max_depth=3)
+    s = vb.Scene(gpu_ctx, sc).build_accel()
+    frames = []
+    for f in range(3):
+        s.restir_frame(f)
+        frames.append(s.restir_buffer('di_radiance')[..., :3] + s.restir_buffer('gi_radiance')[..., :3])
+    film = s.film()[..., :3]
+    np.testing.assert_allclose(film, np.mean(frames, 0), rtol=1e-5, atol=1e-6)

@@ -91,6 +91,10 @@ def _load():
         'vs_timing_read': ([P, P, P, P], ctypes.c_int),
         'vs_render_noalloc': ([P, U32, U32, P, P], ctypes.c_int),
         'vs_albedo_luts': ([ctypes.c_int, ctypes.c_char_p, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_restir_frame': ([P, U32, U32, P], ctypes.c_int),
+        'vs_restir_reset': ([P], ctypes.c_int),
+        'vs_restir_params': ([P, U32, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_restir_download': ([P, ctypes.c_int, P, ctypes.c_size_t], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -107,7 +111,24 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_scene_info_get', 'vs_scene_export_size', 'vs_scene_export', 'vs_render', 'vs_synchronize',
                       'vs_film_download', 'vs_trace_closest_device', 'vs_trace_closest_host', 'vs_trace_any_device',
                       'vs_trace_any_host', 'vs_rgb_to_spectrum', 'vs_launch_count', 'vs_render_stats', 'vs_timing_enable',
-                      'vs_timing_read', 'vs_render_noalloc', 'vs_albedo_luts'])
+                      'vs_timing_read', 'vs_render_noalloc', 'vs_albedo_luts', 'vs_restir_frame',
+                      'vs_restir_reset', 'vs_restir_params', 'vs_restir_download'])
+
+# Per-pixel ReSTIR records (vision_b200/csrc/vs_restir.h) as numpy dtypes.
+HIT_DTYPE = np.dtype([('inst_id', '<u4'), ('prim_id', '<u4'), ('u', '<f4'), ('v', '<f4')])
+RT_SURFACE_DTYPE = np.dtype([('hit', HIT_DTYPE), ('normal', '<f4', 3), ('depth', '<f4'), ('pos', '<f4', 3),
+                             ('diffuse', '<f4'), ('is_replaced', '<u4'), ('flag', '<u4'), ('pad', '<u4', 2)])
+DI_RESERVOIR_DTYPE = np.dtype([('weight_sum', '<f8'), ('C', '<f4'), ('W', '<f4'), ('light_index', '<u4'),
+                               ('prim_id', '<u4'), ('bary', '<f4', 2), ('age', '<u4'), ('p_hat', '<f4'),
+                               ('pos', '<f4', 3), ('pad', '<u4', 3)])
+GI_RESERVOIR_DTYPE = np.dtype([('weight_sum', '<f8'), ('C', '<f4'), ('W', '<f4'), ('sp_pos', '<f4', 3),
+                               ('sp_ng', '<f4', 3), ('Lo', '<f4', 3), ('age', '<f4'), ('pad', '<u4', 2)])
+HIT_BSDF_DTYPE = np.dtype([('wi', '<f4', 3), ('f', '<f4', 3), ('pdf', '<f4'), ('pad', '<u4')])
+RESTIR_PARAMS_BYTES = 432
+RESTIR = dict(di_radiance=(0, np.dtype(('<f4', 4))), gi_radiance=(1, np.dtype(('<f4', 4))),
+              motion=(2, np.dtype(('<f4', 2))), surfaces=(3, RT_SURFACE_DTYPE), di_reservoirs=(4, DI_RESERVOIR_DTYPE),
+              gi_reservoirs=(5, GI_RESERVOIR_DTYPE), hit_bsdf=(6, HIT_BSDF_DTYPE), gi_samples=(7, GI_RESERVOIR_DTYPE))
+assert RT_SURFACE_DTYPE.itemsize == 64 and DI_RESERVOIR_DTYPE.itemsize == 64 and GI_RESERVOIR_DTYPE.itemsize == 64
 
 
 def launch_count():
@@ -250,6 +271,36 @@ class Scene:
         n = ctypes.c_uint32()
         self.ctx.check(lib.vs_timing_read(self.handle, ctypes.byref(r), ctypes.byref(f), ctypes.byref(n)), 'timing_read')
         return r.value, f.value, n.value
+
+    def set_camera(self, c2w, fov_y_deg):
+        """Camera-to-world 4x4 (row-major numpy matrix; passed column-major) and fov."""
+        m = np.ascontiguousarray(np.asarray(c2w, np.float32).T)
+        self.ctx.check(lib.vs_camera_set(self.handle, _ptr(m), float(fov_y_deg)), 'camera_set')
+        self.frames = 0
+
+    def restir_frame(self, frame_index, film_index=None, stream=None):
+        """One real-time ReSTIR frame (scene integrator "rt"); the film gets the
+        frame as sample `film_index` of its running mean (default: next)."""
+        fi = self.frames if film_index is None else film_index
+        self.ctx.check(lib.vs_restir_frame(self.handle, frame_index, fi, ctypes.c_void_p(stream) if stream else None),
+                       'restir_frame')
+        self.frames = fi + 1
+
+    def restir_reset(self):
+        self.ctx.check(lib.vs_restir_reset(self.handle), 'restir_reset')
+
+    def restir_params(self, frame_index):
+        """Parameter block (bytes) of a vs_restir_frame call made now with this frame index."""
+        out = np.zeros(RESTIR_PARAMS_BYTES, np.uint8)
+        self.ctx.check(lib.vs_restir_params(self.handle, frame_index, _ptr(out), out.nbytes), 'restir_params')
+        return out
+
+    def restir_buffer(self, which):
+        key, dt = RESTIR[which]
+        i = self.info()
+        out = np.zeros(i['width'] * i['height'], dt)
+        self.ctx.check(lib.vs_restir_download(self.handle, key, _ptr(out), out.nbytes), 'restir_download')
+        return out.reshape((i['height'], i['width']) + out.shape[1:])
 
     def render_stats(self, frame_begin, frame_count):
         """Traversal counters of an instrumented render: (segments, nodes, tris)."""

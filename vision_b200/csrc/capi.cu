@@ -79,6 +79,48 @@ struct vs_scene {
     bool timing = false;
     std::vector<cudaEvent_t> ev_render, ev_film;  // start/stop pairs
     cudaEvent_t ev_join = nullptr;
+    // Real-time ReSTIR state: per-pixel buffers at the current resolution and
+    // the previous frame's camera.
+    struct Rt {
+        DevBuf<RtSurface> surf[2];
+        DevBuf<RtSurfaceExt> ext[2];
+        DevBuf<RtHitBsdf> hit_bsdf;
+        DevBuf<float2> motion;
+        DevBuf<DiReservoir> di[2], di_pass;
+        DevBuf<GiReservoir> gi[2], gi_pass, gi_init;
+        DevBuf<float4> di_radiance, gi_radiance;
+        uint32_t width = 0, height = 0;
+        bool have_prev = false;
+        Camera prev_cam{};
+        m4 prev_w2c{};
+        f3 prev_pos{};
+        RtParams last{};
+        bool rendered = false;
+        void free() {
+            for (int k = 0; k < 2; ++k) {
+                surf[k].free(); ext[k].free(); di[k].free(); gi[k].free();
+            }
+            hit_bsdf.free(); motion.free(); di_pass.free(); gi_pass.free(); gi_init.free();
+            di_radiance.free(); gi_radiance.free();
+        }
+        RtBuffers view() const {
+            RtBuffers b{};
+            for (int k = 0; k < 2; ++k) {
+                b.surf[k] = surf[k].ptr;
+                b.ext[k] = ext[k].ptr;
+                b.di[k] = di[k].ptr;
+                b.gi[k] = gi[k].ptr;
+            }
+            b.hit_bsdf = hit_bsdf.ptr;
+            b.motion = motion.ptr;
+            b.di_pass = di_pass.ptr;
+            b.gi_pass = gi_pass.ptr;
+            b.gi_init = gi_init.ptr;
+            b.di_radiance = di_radiance.ptr;
+            b.gi_radiance = gi_radiance.ptr;
+            return b;
+        }
+    } rt;
 
     ~vs_scene() {
         for (cudaEvent_t e : ev_render) cudaEventDestroy(e);
@@ -88,6 +130,7 @@ struct vs_scene {
         prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
         env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
         film32.free(); exposed.free(); film64.free(); radiance.free();
+        rt.free();
     }
 
     DeviceScene device_view() const {
@@ -157,6 +200,7 @@ int upload_scene(vs_scene *s) {
     if (!ctx->consts_uploaded) {
         const Cie5 &c = cie5();
         VS_CUDA(upload_spectral_consts(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        VS_CUDA(upload_spectral_consts_rt(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         ctx->consts_uploaded = true;
     }
     const HostScene &h = s->host;
@@ -629,6 +673,194 @@ int vs_render_stats(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, uin
     out3[0] = h[0];
     out3[1] = h[1];
     out3[2] = h[2];
+    return VS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+static_assert(sizeof(RtParams) == VS_RESTIR_PARAMS_BYTES, "RtParams layout changed");
+
+// General 4x4 inverse in double (Sensor::device_w2c = inverse(c2w), sensor.cpp:194-201).
+m4 inverse4(const m4 &a) {
+    double m[16], inv[16];
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r) m[4 * c + r] = a.m[c][r];
+    inv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] + m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
+    inv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] - m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
+    inv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] + m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
+    inv[12] = -m[4] * m[9] * m[14] + m[4] * m[10] * m[13] + m[8] * m[5] * m[14] - m[8] * m[6] * m[13] - m[12] * m[5] * m[10] + m[12] * m[6] * m[9];
+    inv[1] = -m[1] * m[10] * m[15] + m[1] * m[11] * m[14] + m[9] * m[2] * m[15] - m[9] * m[3] * m[14] - m[13] * m[2] * m[11] + m[13] * m[3] * m[10];
+    inv[5] = m[0] * m[10] * m[15] - m[0] * m[11] * m[14] - m[8] * m[2] * m[15] + m[8] * m[3] * m[14] + m[12] * m[2] * m[11] - m[12] * m[3] * m[10];
+    inv[9] = -m[0] * m[9] * m[15] + m[0] * m[11] * m[13] + m[8] * m[1] * m[15] - m[8] * m[3] * m[13] - m[12] * m[1] * m[11] + m[12] * m[3] * m[9];
+    inv[13] = m[0] * m[9] * m[14] - m[0] * m[10] * m[13] - m[8] * m[1] * m[14] + m[8] * m[2] * m[13] + m[12] * m[1] * m[10] - m[12] * m[2] * m[9];
+    inv[2] = m[1] * m[6] * m[15] - m[1] * m[7] * m[14] - m[5] * m[2] * m[15] + m[5] * m[3] * m[14] + m[13] * m[2] * m[7] - m[13] * m[3] * m[6];
+    inv[6] = -m[0] * m[6] * m[15] + m[0] * m[7] * m[14] + m[4] * m[2] * m[15] - m[4] * m[3] * m[14] - m[12] * m[2] * m[7] + m[12] * m[3] * m[6];
+    inv[10] = m[0] * m[5] * m[15] - m[0] * m[7] * m[13] - m[4] * m[1] * m[15] + m[4] * m[3] * m[13] + m[12] * m[1] * m[7] - m[12] * m[3] * m[5];
+    inv[14] = -m[0] * m[5] * m[14] + m[0] * m[6] * m[13] + m[4] * m[1] * m[14] - m[4] * m[2] * m[13] - m[12] * m[1] * m[6] + m[12] * m[2] * m[5];
+    inv[3] = -m[1] * m[6] * m[11] + m[1] * m[7] * m[10] + m[5] * m[2] * m[11] - m[5] * m[3] * m[10] - m[9] * m[2] * m[7] + m[9] * m[3] * m[6];
+    inv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] + m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
+    inv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] - m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
+    inv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] + m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
+    double det = m[0] * inv[0] + m[1] * inv[4] + m[2] * inv[8] + m[3] * inv[12];
+    m4 r{};
+    for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < 4; ++k) r.m[c][k] = static_cast<float>(inv[4 * c + k] / det);
+    return r;
+}
+
+// The parameter block of the next ReSTIR frame.
+RtParams rt_params(const vs_scene *s, uint32_t frame) {
+    const HostScene &h = s->host;
+    RtParams p{};
+    p.di = h.rt_di;
+    p.gi = h.rt_gi;
+    p.M_light = h.rt_M_light;
+    p.M_bsdf = h.rt_M_bsdf;
+    p.max_recursion = h.rt_max_recursion;
+    p.pairwise = h.rt_pairwise;
+    p.gi_max_depth = h.ip.max_depth;
+    p.frame = frame;
+    p.width = h.cam.width;
+    p.height = h.cam.height;
+    p.w2c = inverse4(h.cam.c2w);
+    p.view_pos = make3(h.cam.c2w.m[3][0], h.cam.c2w.m[3][1], h.cam.c2w.m[3][2]);
+    bool prev = s->rt.have_prev && s->rt.width == h.cam.width && s->rt.height == h.cam.height;
+    p.prev_cam = prev ? s->rt.prev_cam : h.cam;
+    p.prev_w2c = prev ? s->rt.prev_w2c : p.w2c;
+    p.prev_view_pos = prev ? s->rt.prev_pos : p.view_pos;
+    p.di_factor = h.rt_di.open ? 1.0f : 0.0f;
+    p.gi_factor = h.rt_gi.open ? 1.0f : 0.0f;
+    return p;
+}
+
+int rt_ensure(vs_scene *s, cudaStream_t st) {
+    vs_context *ctx = s->ctx;
+    vs_scene::Rt &r = s->rt;
+    uint32_t w = s->host.cam.width, hgt = s->host.cam.height;
+    if (r.width == w && r.height == hgt && r.surf[0].ptr) return VS_OK;
+    size_t n = static_cast<size_t>(w) * hgt;
+    r.free();
+    for (int k = 0; k < 2; ++k) {
+        VS_CUDA(r.surf[k].alloc(n), "restir alloc");
+        VS_CUDA(r.ext[k].alloc(n), "restir alloc");
+        VS_CUDA(r.di[k].alloc(n), "restir alloc");
+        VS_CUDA(r.gi[k].alloc(n), "restir alloc");
+    }
+    VS_CUDA(r.hit_bsdf.alloc(n), "restir alloc");
+    VS_CUDA(r.motion.alloc(n), "restir alloc");
+    VS_CUDA(r.di_pass.alloc(n), "restir alloc");
+    VS_CUDA(r.gi_pass.alloc(n), "restir alloc");
+    VS_CUDA(r.gi_init.alloc(n), "restir alloc");
+    VS_CUDA(r.di_radiance.alloc(n), "restir alloc");
+    VS_CUDA(r.gi_radiance.alloc(n), "restir alloc");
+    r.width = w;
+    r.height = hgt;
+    r.have_prev = false;
+    r.rendered = false;
+    VS_CUDA(launch_rt_reset(static_cast<uint32_t>(n), r.view(), st), "restir reset");
+    add_launches(1);
+    return VS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void *stream) {
+    if (!s) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_restir_frame");
+    if (!s->host.rt) return fail(ctx, VS_E_STATE, "scene integrator is not \"rt\"");
+    if (film_index != 0 && film_index != s->film_frames)
+        return fail(ctx, VS_E_STATE, "film_index must continue the film or restart at 0");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = pick_stream(s, stream);
+    int rc = ensure_film(s);
+    if (rc != VS_OK) return rc;
+    rc = rt_ensure(s, st);
+    if (rc != VS_OK) return rc;
+    RtParams p = rt_params(s, frame_index);
+    auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
+        cudaEvent_t e;
+        cudaError_t r = cudaEventCreate(&e);
+        if (r != cudaSuccess) return r;
+        v.push_back(e);
+        return cudaEventRecord(e, st);
+    };
+    if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
+    unsigned n = 0;
+    VS_CUDA(launch_rt_frame(s->device_view(), p, s->rt.view(), film_index, s->film32.ptr, st, &n), "restir launch");
+    add_launches(n);
+    if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
+    if (st != ctx->stream) {
+        if (!s->ev_join) VS_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "join event");
+        VS_CUDA(cudaEventRecord(s->ev_join, st), "join record");
+        VS_CUDA(cudaStreamWaitEvent(ctx->stream, s->ev_join, 0), "join wait");
+    }
+    // Sensor::after_render -> store_prev_data (sensor.cpp:95-103).
+    s->rt.prev_cam = s->host.cam;
+    s->rt.prev_w2c = p.w2c;
+    s->rt.prev_pos = p.view_pos;
+    s->rt.have_prev = true;
+    s->rt.last = p;
+    s->rt.rendered = true;
+    s->film_frames = film_index + 1u;
+    s->film64_valid = false;
+    return VS_OK;
+}
+
+int vs_restir_reset(vs_scene *s) {
+    if (!s) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->rt.have_prev = false;
+    s->rt.rendered = false;
+    if (ctx->device < 0 || !s->rt.surf[0].ptr) return VS_OK;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    size_t n = static_cast<size_t>(s->rt.width) * s->rt.height;
+    VS_CUDA(launch_rt_reset(static_cast<uint32_t>(n), s->rt.view(), ctx->stream), "restir reset");
+    add_launches(1);
+    return VS_OK;
+}
+
+int vs_restir_params(const vs_scene *s, uint32_t frame_index, void *dst, size_t bytes) {
+    if (!s || !dst) return VS_E_INVALID;
+    if (bytes != sizeof(RtParams)) return fail(s->ctx, VS_E_INVALID, "params size mismatch");
+    if (!s->host.rt) return fail(s->ctx, VS_E_STATE, "scene integrator is not \"rt\"");
+    RtParams p = rt_params(s, frame_index);
+    std::memcpy(dst, &p, sizeof(p));
+    return VS_OK;
+}
+
+int vs_restir_download(vs_scene *s, int which, void *dst, size_t bytes) {
+    if (!s || !dst) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context has no ReSTIR buffers");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->rt.rendered) return fail(ctx, VS_E_STATE, "no ReSTIR frame rendered");
+    size_t n = static_cast<size_t>(s->rt.width) * s->rt.height;
+    uint32_t cur = (s->rt.last.frame + 1u) & 1u;
+    const void *src = nullptr;
+    size_t elem = 0;
+    switch (which) {
+        case VS_RESTIR_DI_RADIANCE: src = s->rt.di_radiance.ptr; elem = 16; break;
+        case VS_RESTIR_GI_RADIANCE: src = s->rt.gi_radiance.ptr; elem = 16; break;
+        case VS_RESTIR_MOTION: src = s->rt.motion.ptr; elem = 8; break;
+        case VS_RESTIR_SURFACES: src = s->rt.surf[cur].ptr; elem = sizeof(RtSurface); break;
+        case VS_RESTIR_DI_RESERVOIRS: src = s->rt.di[cur].ptr; elem = sizeof(DiReservoir); break;
+        case VS_RESTIR_GI_RESERVOIRS: src = s->rt.gi[cur].ptr; elem = sizeof(GiReservoir); break;
+        case VS_RESTIR_HIT_BSDF: src = s->rt.hit_bsdf.ptr; elem = sizeof(RtHitBsdf); break;
+        case VS_RESTIR_GI_SAMPLES: src = s->rt.gi_init.ptr; elem = sizeof(GiReservoir); break;
+        default: return fail(ctx, VS_E_INVALID, "unknown ReSTIR buffer");
+    }
+    if (bytes != n * elem) return fail(ctx, VS_E_INVALID, "ReSTIR buffer size mismatch");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    VS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream), "restir copy");
+    VS_CUDA(cudaStreamSynchronize(ctx->stream), "restir sync");
     return VS_OK;
 }
 

@@ -13,6 +13,7 @@ namespace vs {
 
 static std::atomic<unsigned long long> g_launches{0};
 unsigned long long launch_count() { return g_launches.load(); }
+void add_launches(unsigned n) { g_launches += n; }
 
 __global__ void __launch_bounds__(128) k_trace_closest(DeviceScene s, const float *rays, uint32_t n, Hit *hits,
                                                        float *t_out) {
@@ -109,15 +110,7 @@ __global__ void k_film_exposure(const float4 *film, uint32_t npix, float exposur
 }
 
 cudaError_t upload_spectral_consts(const float *x, const float *y, const float *z, const float *d65, float y_integral) {
-    SpectralConsts c;
-    for (int i = 0; i < kSpd5Count; ++i) {
-        c.cie_x[i] = x[i];
-        c.cie_y[i] = y[i];
-        c.cie_z[i] = z[i];
-        c.d65[i] = d65[i];
-    }
-    c.inv_cie_y_integral = 1.0f / y_integral;
-    return cudaMemcpyToSymbol(c_spec, &c, sizeof(c));
+    return upload_spectral_consts_tu(x, y, z, d65, y_integral);
 }
 
 cudaError_t launch_trace_closest(const DeviceScene &s, const float *rays, uint32_t n, Hit *hits, float *t,

@@ -798,6 +798,56 @@ static void load_spherical(const Json &p, const Json &root, HostScene &s) {
     s.has_env = true;
 }
 
+namespace {
+
+// ReSTIR::ReSTIR with SpatialResamplingParam / TemporalResamplingParam
+// (ReSTIR/common.h:19-67,91-98); thresholds as cos(radians(theta)).
+RtStage load_rt_stage(const Json &d) {
+    RtStage st{};
+    st.open = d["open"].as_bool(true) ? 1u : 0u;
+    st.diff_factor = d["diffuse_factor"].as_float(0.3f);
+    st.max_age = d["max_age"].as_uint(30u);
+    const Json &sp = d["spatial"];
+    bool s_open = sp["open"].as_bool(true);
+    st.spatial = s_open ? 1u : 0u;
+    st.s_count = s_open ? sp["sample_num"].as_uint(1u) : 1u;
+    if (st.s_count > kMaxSpatialNeighbours)
+        throw unsupported("spatial sample_num above " + std::to_string(kMaxSpatialNeighbours));
+    st.s_dot = std::cos(sp["theta"].as_float(35.0f) * (kPi / 180.0f));
+    st.s_depth = sp["depth"].as_float(0.3f);
+    st.s_radius = sp["radius"].as_float(30.0f);
+    const Json &tp = d["temporal"];
+    st.temporal = tp["open"].as_bool(true) ? 1u : 0u;
+    st.history_limit = tp["history_limit"].as_uint(5u);
+    st.t_count = tp["N"].as_uint(9u);
+    st.t_mis = tp["mis"].as_bool(false) ? 1u : 0u;
+    st.t_dot = std::cos(tp["theta"].as_float(35.0f) * (kPi / 180.0f));
+    st.t_depth = tp["depth"].as_float(0.3f);
+    st.t_radius = tp["radius"].as_float(8.0f);
+    return st;
+}
+
+// RealTimeIntegrator (rt.cpp:24-31) with ReSTIRDI (direct.cpp:9-15) and
+// ReSTIRGI (indirect.cpp:9-12).  The integrator keeps max_depth - 1 for the
+// paths of the indirect samples.
+void load_rt(const Json &ip, HostScene &s) {
+    if (s.ip.spectrum_dim != 3) throw unsupported("rt integrator with a hero dimension other than 3");
+    if (s.has_env) throw unsupported("environment light with the rt integrator");
+    if (s.ip.max_depth < 3) throw unsupported("rt integrator with max_depth below 3");
+    s.rt = true;
+    s.ip.max_depth -= 1u;
+    const Json &dj = ip["direct"];
+    s.rt_di = load_rt_stage(dj);
+    s.rt_gi = load_rt_stage(ip["indirect"]);
+    s.rt_gi.t_mis = 0u;
+    s.rt_M_light = dj["M_light"].as_uint(10u);
+    s.rt_M_bsdf = dj["M_bsdf"].as_uint(1u);
+    s.rt_max_recursion = dj["max_recursion"].as_uint(5u);
+    s.rt_pairwise = dj["pairwise"].as_bool(false) ? 1u : 0u;
+}
+
+}  // namespace
+
 void load_scene_json(const std::string &text, const std::string &base_dir, const std::string &table_cache,
                      HostScene &s) {
     (void)base_dir;
@@ -840,12 +890,13 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     // Integrator (IlluminationIntegrator ctor, integrator.cpp:60-67).
     const Json &ij = root["integrator"];
     std::string it = ij["type"].as_string("pt");
-    if (it != "pt") throw unsupported("integrator type '" + it + "'");
+    if (it != "pt" && it != "rt") throw unsupported("integrator type '" + it + "'");
     const Json &ip = ij["param"];
     s.ip.max_depth = ip["max_depth"].as_uint(16u);
     s.ip.min_depth = ip["min_depth"].as_uint(5u);
     s.ip.rr_threshold = ip["rr_threshold"].as_float(1.0f);
     s.ip.mis_mode = ip["mis_mode"].as_uint(0u);
+    if (it == "rt") load_rt(ip, s);
     // Sampler.
     const Json &smp = root["sampler"];
     std::string st = smp["type"].as_string("independent");

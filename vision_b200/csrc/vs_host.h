@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "vs_math.h"
+#include "vs_restir.h"
 #include "vs_scene.h"
 #include "vs_spectral.h"
 
@@ -46,6 +47,11 @@ struct HostScene {
     std::string lut_cache;
     Camera cam{};
     IntegratorParams ip{};
+    // Real-time ReSTIR integrator (integrator type "rt", rt.cpp:24-31): the
+    // settings of its direct and indirect stages.
+    bool rt = false;
+    RtStage rt_di{}, rt_gi{};
+    uint32_t rt_M_light = 10, rt_M_bsdf = 1, rt_max_recursion = 5, rt_pairwise = 0;
     std::string spectrum_type = "hero";
     // Compressed BVH8 over the primitives.
     std::vector<Bvh8Node> nodes;

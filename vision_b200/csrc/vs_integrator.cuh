@@ -174,40 +174,40 @@ __device__ VS_OUTLINE void eval_hit_light(const DeviceScene &s, const Interactio
     pdf = pdf_wi_from_area(pdf_pos, it.ng, w) * light_pmf<N>(s, it.light);
 }
 
-// One camera path (PathTracingIntegrator kernel body, pt.cpp:53-72, and
-// IlluminationIntegrator::Li, integrator.cpp:134-283).  Returns linear sRGB
-// radiance times the filter weight.
-template <int N>
-__device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_t frame) {
-    const IntegratorParams &ip = s.ip;
-    const Camera &cam = s.cam;
-    Sampler smp;
-    // Wavelengths come from a separate stream (RenderEnv::initial, integrator.cpp:49-58).
-    smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
-    Wavelengths<N> wl = sample_wavelengths<N>(smp.next());
-    smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
-    // Sampler::sensor_sample (sampler.h:65-73) with the box filter (box.cpp:16-20).
+// Sampler::sensor_sample (sampler.h:65-73) with the box filter (box.cpp:16-20)
+// and Sensor::generate_ray (sensor.cpp:44-56,63-76): raster -> screen ->
+// camera -> world.  Draws 2 (filter) + 2 (lens, unused by the pinhole) + 1
+// (time) numbers.
+__device__ __forceinline__ void camera_ray(const Camera &cam, Sampler &smp, uint32_t px, uint32_t py, f2 &p_film,
+                                           f3 &ro, f3 &rd) {
     f2 uf = smp.next2();
     float fx = lerpf(uf.x, -cam.filter_rx, cam.filter_rx);
     float fy = lerpf(uf.y, -cam.filter_ry, cam.filter_ry);
-    (void)smp.next2();  // lens sample (unused by the pinhole)
-    (void)smp.next();   // time sample
+    (void)smp.next2();
+    (void)smp.next();
     float film_x = static_cast<float>(px) + 0.5f + fx;
     float film_y = static_cast<float>(py) + 0.5f + fy;
-    // raster -> screen -> camera (Sensor::generate_ray, sensor.cpp:44-56,63-76).
+    p_film = {film_x, film_y};
     float sx = cam.screen_lo_x + film_x / static_cast<float>(cam.width) * cam.screen_span_x;
     float sy = cam.screen_hi_y - film_y / static_cast<float>(cam.height) * cam.screen_span_y;
     f3 dir_cam = normalize(make3(sx * cam.tan_half_fov, sy * cam.tan_half_fov, 1.0f));
-    f3 ro = xform_point(cam.c2w, make3(0.0f));
-    f3 rd = normalize(xform_vector(cam.c2w, dir_cam));
+    ro = xform_point(cam.c2w, make3(0.0f));
+    rd = normalize(xform_vector(cam.c2w, dir_cam));
+}
 
-    float scatter_pdf = 1e16f;
-    Spec<N> throughput = Spec<N>::fill(1.0f);
+// The bounce loop of IlluminationIntegrator::Li (integrator.cpp:134-283) from
+// ray (ro, rd) with the given scatter pdf and throughput.  Returns linear sRGB
+// radiance.  `first`, when non-null, receives the interaction of the first
+// surface hit (the HitContext of the reference).
+template <int N>
+__device__ __forceinline__ f3 path_li(const DeviceScene &s, Sampler &smp, Wavelengths<N> &wl, f3 ro, f3 rd,
+                                      float scatter_pdf, Spec<N> throughput, uint32_t max_depth,
+                                      Interaction *first) {
+    const IntegratorParams &ip = s.ip;
     f3 ret = make3(0.0f);
-    f3 prev_ng = rd;
     float eta_scale = 1.0f;
 
-    for (uint32_t bounce = 0; bounce < ip.max_depth; ++bounce) {
+    for (uint32_t bounce = 0; bounce < max_depth; ++bounce) {
         RayPre rp = precompute_ray(ro, rd);
         Hit hit;
         float t_hit;
@@ -226,6 +226,7 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
             break;
         }
         Interaction it = surface_interaction(s, hit, rd, true);
+        if (first && bounce == 0) *first = it;
         if (it.light != kInvalid) {
             Spec<N> Le;
             float lpdf;
@@ -235,7 +236,6 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
             else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
             ret += linear_srgb<N>(Le * throughput * weight, wl);
         }
-        prev_ng = it.ng;
         // Light sample: 1 draw for the light, 2 for the surface point.
         float u_light = smp.next();
         f2 u_surf = smp.next2();
@@ -274,6 +274,22 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
         rd = nr.d;
     }
     return ret;
+}
+
+// One camera path (PathTracingIntegrator kernel body, pt.cpp:53-72).
+// Returns linear sRGB radiance times the filter weight.
+template <int N>
+__device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_t frame) {
+    const IntegratorParams &ip = s.ip;
+    Sampler smp;
+    // Wavelengths come from a separate stream (RenderEnv::initial, integrator.cpp:49-58).
+    smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
+    Wavelengths<N> wl = sample_wavelengths<N>(smp.next());
+    smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
+    f2 p_film;
+    f3 ro, rd;
+    camera_ray(s.cam, smp, px, py, p_film, ro, rd);
+    return path_li<N>(s, smp, wl, ro, rd, 1e16f, Spec<N>::fill(1.0f), ip.max_depth, nullptr);
 }
 
 }  // namespace vs

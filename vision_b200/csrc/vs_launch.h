@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include "vs_devscene.h"
+#include "vs_restir.h"
 
 namespace vs {
 
@@ -15,6 +16,12 @@ cudaError_t launch_render(const DeviceScene &s, uint32_t frame_begin, uint32_t f
 cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count, float4 *film32,
                         double *film64, cudaStream_t st);
 unsigned long long launch_count();
+void add_launches(unsigned n);
+// restir.cu
+cudaError_t upload_spectral_consts_rt(const float *x, const float *y, const float *z, const float *d65, float y_integral);
+cudaError_t launch_rt_reset(uint32_t npix, const RtBuffers &b, cudaStream_t st);
+cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuffers &b, uint32_t film_index,
+                            float4 *film, cudaStream_t st, unsigned *launches);
 cudaError_t launch_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out, cudaStream_t st);
 
 }  // namespace vs

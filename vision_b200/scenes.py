@@ -163,3 +163,102 @@ def large_scene(width=1024, height=1024, max_depth=16, dimension=4, sampler="pcg
         "light_sampler": {"type": "uniform", "param": {"lights": [sky]}},
         "render_setting": {"polymorphic_mode": 1},
     }
+
+
+def _rot_m(axis, deg):
+    a = math.radians(deg)
+    c, s = math.cos(a), math.sin(a)
+    import numpy as np
+    m = np.eye(4)
+    if axis == 'x':
+        m[1, 1], m[1, 2], m[2, 1], m[2, 2] = c, -s, s, c
+    else:
+        m[0, 0], m[0, 2], m[2, 0], m[2, 2] = c, s, -s, c
+    return m
+
+
+def camera_c2w(position, target, up=(0.0, 1.0, 0.0)):
+    """Camera-to-world matrix (row-major 4x4) that the scene loader builds from
+    a look_at transform: the sensor keeps yaw and pitch of the look-at frame and
+    composes T(position) * scale(1, 1, -1) * Ry(yaw) * Rx(-pitch)."""
+    import numpy as np
+    pos, tgt, up = (np.asarray(v, np.float64) for v in (position, target, up))
+    fwd = tgt - pos
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, up)
+    right /= np.linalg.norm(right)
+    up2 = np.cross(right, fwd)
+    # look_at columns: right, up, forward; pitch/yaw as Sensor::update_mat reads them.
+    pitch = math.degrees(math.atan2(up2[2], up2[1]))
+    yaw = math.degrees(math.atan2(fwd[0], right[0]))
+    t = np.eye(4)
+    t[:3, 3] = pos
+    sc = np.diag([1.0, 1.0, -1.0, 1.0])
+    return (t @ sc @ _rot_m('y', yaw) @ _rot_m('x', -pitch)).astype(np.float32)
+
+
+def camera_spline(frames=64, seed=3, target=(0.0, 0.45, 0.0)):
+    """Seeded camera path for the many-light workload: a Catmull-Rom spline
+    through 6 control points in front of the box room's open side
+    (x in [-0.15, 0.15], y in [0.35, 0.65], z in [1.45, 1.95]), looking at the
+    room centre.  Returns `frames` camera-to-world matrices."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ctrl = np.stack([rng.uniform(-0.15, 0.15, 6), rng.uniform(0.35, 0.65, 6), rng.uniform(1.45, 1.95, 6)], 1)
+    out = []
+    for f in range(frames):
+        t = f / max(frames - 1, 1) * (len(ctrl) - 3)
+        i = min(int(t), len(ctrl) - 4)
+        u = t - i
+        p0, p1, p2, p3 = ctrl[i:i + 4]
+        pos = 0.5 * ((2 * p1) + (-p0 + p2) * u + (2 * p0 - 5 * p1 + 4 * p2 - p3) * u * u +
+                     (-p0 + 3 * p1 - 3 * p2 + p3) * u ** 3)
+        out.append(camera_c2w(pos, target))
+    return out
+
+
+def many_lights(width=1920, height=1080, emitters=10000, seed=7, M_light=32, M_bsdf=1, history_limit=20,
+                spatial_neighbours=5, spatial_radius=30.0, max_depth=8, sampler="pcg", gi=True):
+    """Many-light ReSTIR workload: the box room plus `emitters` one-sided
+    emissive triangles (equilateral, edge U[0.01, 0.05], centres uniform in the
+    room, random orientation, 2000-9000 K blackbody spectra, scale log-uniform
+    over [1, 100]) with power-distribution light selection, rendered by the
+    real-time ReSTIR integrator on 3 hero wavelengths: 32 initial light
+    candidates, temporal reuse capped at M = 20, one spatial pass of 5
+    neighbours within 30 pixels."""
+    import numpy as np
+    sc = box_room(width=width, height=height, max_depth=max_depth, dimension=3, sampler=sampler, seed=0)
+    rng = np.random.default_rng(seed)
+    shapes = sc["shapes"]
+    for i in range(emitters):
+        edge = rng.uniform(0.01, 0.05)
+        c = rng.uniform([-0.5, 0.0, -0.5], [0.5, 1.0, 0.5])
+        # Random orthonormal frame: normal uniform on the sphere, in-plane angle uniform.
+        n = rng.normal(size=3)
+        n /= np.linalg.norm(n)
+        a = np.cross(n, [1.0, 0.0, 0.0] if abs(n[0]) < 0.9 else [0.0, 1.0, 0.0])
+        a /= np.linalg.norm(a)
+        b = np.cross(n, a)
+        th = rng.uniform(0.0, 2.0 * math.pi)
+        r = edge / math.sqrt(3.0)
+        verts = [c + r * (math.cos(th + k * 2.0 * math.pi / 3.0) * a + math.sin(th + k * 2.0 * math.pi / 3.0) * b)
+                 for k in range(3)]
+        temp = float(rng.uniform(2000.0, 9000.0))
+        scale = float(math.exp(rng.uniform(math.log(1.0), math.log(100.0))))
+        shapes.append({"type": "mesh", "name": "emitter_%d" % i,
+                       "param": {"positions": [float(x) for v in verts for x in v], "indices": [0, 1, 2],
+                                 "material": "Light",
+                                 "emission": {"type": "area", "param": {
+                                     "color": {"channels": "xyz",
+                                               "node": {"type": "blackbody", "param": {"temperature": temp}}},
+                                     "scale": scale, "two_sided": False}}}})
+    sc["light_sampler"] = {"type": "power", "param": {"lights": []}}
+    sc["integrator"] = {"type": "rt", "param": {
+        "max_depth": max_depth, "min_depth": 5, "rr_threshold": 1.0,
+        "direct": {"M_light": M_light, "M_bsdf": M_bsdf,
+                   "spatial": {"sample_num": spatial_neighbours, "radius": spatial_radius},
+                   "temporal": {"history_limit": history_limit}},
+        "indirect": {"open": bool(gi),
+                     "spatial": {"sample_num": spatial_neighbours, "radius": spatial_radius},
+                     "temporal": {"history_limit": history_limit}}}}
+    return sc
