@@ -35,8 +35,35 @@ WORKLOADS = {
     'large_scene': dict(kind='large_scene', width=1024, height=1024, spp=64, max_depth=16, dimension=4, sampler='pcg',
                         seed=1),
 }
+# Real-time ReSTIR on the many-light box room: 1920 x 1080, 1 spp per frame,
+# 10,000 blackbody emitters, power light sampler, 32 light candidates,
+# temporal M-cap 20, one spatial pass of 5 neighbours within 30 px, camera on
+# a seeded 64-frame spline; one step = one frame (direct + indirect + combine).
+WORKLOADS['many_lights'] = dict(kind='many_lights', width=1920, height=1080, spp=1, frames=64, emitters=10000,
+                                M_light=32, history_limit=20, spatial_neighbours=5, spatial_radius=30.0,
+                                max_depth=8, dimension=3, sampler='pcg', seed=7)
 DEFAULT_WORKLOAD = 'large_scene'
-DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5}
+DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64}
+
+# DRAM bytes per path of k_render measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch divided by its paths; profiles/).
+NCU_TRAFFIC_PER_PATH = {'large_scene': 1029.3e6 / 2097152, 'box_room': 18.42e6 / 1048576}
+
+# Algorithmic bytes per pixel-frame of the ReSTIR frame, from the record sizes
+# (64 B surfaces and reservoirs, 32 B extensions and BSDF samples, 16 B
+# radiance, 8 B motion vectors, 16 B light-candidate fetch of 8 B alias +
+# 36 B triangle + 64 B light record) for M light candidates and S spatial
+# neighbours:
+#   direct shader0: surface write 64 + motion 8 + BSDF sample 32 + previous
+#     reservoir and surface 128 + passthrough write 64 + M x 108
+#   direct shader1: own surface + passthrough 128 + S x 128 + radiance 16 + reservoir 64
+#   indirect initial: surface 64 + BSDF sample 32 + sample 64 + radiance 16
+#   indirect temporal: surface 64 + sample 64 + BSDF sample 32 + motion 8 + previous 128 + write 64
+#   indirect spatial: surface 64 + passthrough 64 + S x 128 + radiance 16 + reservoir 64
+#   combine: 2 x 16 radiance + film read/write 32
+def restir_bytes_per_pixel(M, S):
+    return ((64 + 8 + 32 + 128 + 64 + M * 108) + (128 + S * 128 + 16 + 64) + (64 + 32 + 64 + 16) +
+            (64 + 64 + 32 + 8 + 128 + 64) + (64 + 64 + S * 128 + 16 + 64) + (32 + 32))
 
 
 def workload_scene(name):
@@ -48,6 +75,11 @@ def workload_scene(name):
     if w['kind'] == 'large_scene':
         return scenes.large_scene(width=w['width'], height=w['height'], max_depth=w['max_depth'],
                                   dimension=w['dimension'], sampler=w['sampler'], seed=w['seed'])
+    if w['kind'] == 'many_lights':
+        return scenes.many_lights(width=w['width'], height=w['height'], emitters=w['emitters'], seed=w['seed'],
+                                  M_light=w['M_light'], history_limit=w['history_limit'],
+                                  spatial_neighbours=w['spatial_neighbours'], spatial_radius=w['spatial_radius'],
+                                  max_depth=w['max_depth'], sampler=w['sampler'])
     raise ValueError(name)
 
 
@@ -137,6 +169,26 @@ def cpu_baseline(scene, spp, budget_s=12.0):
                 pixels.size, frames, o.width, o.height, paths, dt)}
 
 
+def restir_cpu_frames(scene, w, frames, budget_s=None):
+    """The oracle's ReSTIR frames (CPU restatement) on all host cores along the
+    workload's camera spline; returns (frames done, seconds)."""
+    import oracle
+    from vision_b200 import scenes
+    o = oracle.OracleScene(scene)
+    ort = oracle.OracleRestir(o, w['width'], w['height'])
+    cams = scenes.camera_spline(w['frames'], seed=3)
+    threads = os.cpu_count()
+    done = 0
+    t0 = time.perf_counter()
+    for f in range(frames):
+        scene.set_camera(cams[f % len(cams)], 40.0)
+        ort.frame(scene.export('camera'), scene.restir_params(f), 0, threads)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
+    return done, time.perf_counter() - t0, threads
+
+
 def run_reference(args, rank):
     """Reference arm: the CPU restatement of the reference integrator on the
     host cores (the reference's CUDA/OptiX build cannot be built offline)."""
@@ -145,6 +197,24 @@ def run_reference(args, rank):
     import vision_b200 as vb
     import oracle
     w = WORKLOADS[args.workload]
+    if w['kind'] == 'many_lights':
+        ctx = vb.Context(-1)
+        scene = vb.Scene(ctx, workload_scene(args.workload)).build_accel()
+        restir_cpu_frames(scene, w, args.warmup)
+        frames, dt, threads = restir_cpu_frames(scene, w, args.steps)
+        npix = w['width'] * w['height']
+        value = frames * npix / dt / 1e6
+        line = {'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': args.gpus, 'steps': frames,
+                'warmup': args.warmup, 'ms_per_step': dt * 1e3 / frames, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+                'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
+                           'step': 'one full ReSTIR frame (every pixel) per step'},
+                'impl': 'reference',
+                'cpu_baseline': {'value': value, 'unit': 'Mpaths/s', 'cores': threads, 'kind': 'port',
+                                 'sample': '%d full frames of %dx%d' % (frames, w['width'], w['height'])},
+                'e2e': {'value': value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+        print(json.dumps(line))
+        return
     ctx = vb.Context(-1)
     scene = vb.Scene(ctx, workload_scene(args.workload)).build_accel()
     o = oracle.OracleScene(scene)
@@ -201,6 +271,9 @@ def main():
     w = dict(WORKLOADS[args.workload])
     if args.spp:
         w['spp'] = args.spp
+    if w['kind'] == 'many_lights':
+        run_restir(args, w, rank, world, local_rank, dist)
+        return
     ctx = vb.Context(local_rank)
     scene = vb.Scene(ctx, workload_scene(args.workload))
     t0 = time.perf_counter()
@@ -283,7 +356,11 @@ def main():
                    'paths_per_step': paths_per_step, 'l2': 'flushed between steps (256 MiB write)',
                    'parallelism': 'replicas%d' % world, 'scene_build_s': round(build_s, 3)},
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
-                     'peak_source': peak_src, 'traffic': None, 'kernel': 'k_render',
+                     'peak_source': peak_src,
+                     'traffic': (NCU_TRAFFIC_PER_PATH[args.workload] * paths_per_step * args.steps /
+                                 max(render_launches, 1) if args.workload in NCU_TRAFFIC_PER_PATH else None),
+                     'traffic_source': 'ncu dram bytes per path of the committed profile x paths per launch',
+                     'kernel': 'k_render',
                      'bytes_per_path': bytes_per_path,
                      'per_path': {'segments': segs / paths_per_step, 'nodes': nodes / paths_per_step,
                                   'tris': tris / paths_per_step},
@@ -295,6 +372,114 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline(scene, spp)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_restir(args, w, rank, world, local_rank, dist):
+    """The many-light ReSTIR workload: one step = one real-time frame along
+    the camera spline (frame index = step), film restarted each frame."""
+    import torch
+    import vision_b200 as vb
+    from vision_b200 import scenes
+    ctx = vb.Context(local_rank)
+    scene = vb.Scene(ctx, workload_scene(args.workload))
+    t0 = time.perf_counter()
+    scene.build_accel()
+    build_s = time.perf_counter() - t0
+    info = scene.info()
+    npix = w['width'] * w['height']
+    cams = scenes.camera_spline(w['frames'], seed=3)
+    torch_stream = torch.cuda.Stream()
+    torch.cuda.set_stream(torch_stream)
+    stream = torch_stream.cuda_stream
+    frame = 0
+
+    def step(stream_ptr):
+        nonlocal frame
+        scene.set_camera(cams[frame % len(cams)], 40.0)
+        scene.restir_frame(frame, 0, stream=stream_ptr)
+        frame += 1
+
+    for _ in range(args.warmup):
+        step(stream)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+    clocks = ClockSampler(torch.cuda.current_device())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    scene.timing_enable(True)
+    launches0 = vb.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record()
+        step(stream)
+        ends[i].record()
+    torch.cuda.synchronize()
+    launches = vb.launch_count() - launches0
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    step_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    frame_ms, _, frame_launches = scene.timing_read()
+    scene.timing_enable(False)
+    t = torch.tensor([step_ms, frame_ms], dtype=torch.float64, device='cuda')
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms, frame_ms = float(t[0]), float(t[1])
+    value = world * npix * args.steps / (step_ms / 1e3) / 1e6
+
+    # End to end through the public API with host buffers: camera in, film out.
+    film_host = torch.empty((info['height'], info['width'], 4), dtype=torch.float32).pin_memory()
+    film_np = film_host.numpy()
+    e2e_steps = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        c2w = np.ascontiguousarray(cams[frame % len(cams)].T)
+        ctx.check(vb.lib.vs_camera_set(scene.handle, vb._ptr(c2w), 40.0), 'camera')
+        ctx.check(vb.lib.vs_restir_frame(scene.handle, frame, 0, None), 'restir_frame')
+        frame += 1
+        ctx.check(vb.lib.vs_film_download(scene.handle, vb._ptr(film_np), film_np.nbytes, vb.FILM_LINEAR), 'film')
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device='cuda')
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * npix * e2e_steps / float(e2e_t[0]) / 1e6
+
+    peak, peak_src = measured_peaks()
+    bpp = restir_bytes_per_pixel(w['M_light'], w['spatial_neighbours'])
+    frame_s = frame_ms / 1e3 / max(frame_launches, 1)
+    achieved = bpp * npix / frame_s / 1e9
+    line = {
+        'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': step_ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
+                   'path': 'one pixel of one ReSTIR frame (camera path, direct and indirect resampling)',
+                   'prims': info['prim_count'], 'lights': info['light_count'],
+                   'l2': 'flushed between steps (256 MiB write)',
+                   'parallelism': 'replicas%d' % world, 'scene_build_s': round(build_s, 3)},
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                     'peak_source': peak_src, 'traffic': None, 'kernel': 'restir frame (6 kernels)',
+                     'bytes_per_pixel_frame': bpp, 'frame_ms': frame_s * 1e3},
+        'clocks': clk,
+        'e2e': {'value': e2e_value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 64 + 4,
+                'd2h_bytes_per_step': int(film_np.nbytes)},
+        'gpu_launches': int(launches),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        frames, dt, threads = restir_cpu_frames(scene, w, 2, budget_s=20.0)
+        line['cpu_baseline'] = {'value': frames * npix / dt / 1e6, 'unit': 'Mpaths/s', 'cores': threads,
+                                'kind': 'port', 'sample': '%d full %dx%d frames of the oracle ReSTIR' % (
+                                    frames, w['width'], w['height'])}
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -50,17 +50,21 @@ def test_restir_frames_match_oracle(vb, gpu_ctx):
         assert np.all(np.isfinite(gd)) and np.all(np.isfinite(gg))
         di_ok = _close(gd, cd).all(-1).mean()
         gi_ok = _close(gg, cg).all(-1).mean()
-        thr = 0.97 if f == 0 else 0.90
-        assert di_ok >= thr, (f, di_ok)
-        assert gi_ok >= thr - 0.05, (f, gi_ok)
-        assert abs(gd.mean() - cd.mean()) <= 0.02 * cd.mean() + 1e-4, (f, gd.mean(), cd.mean())
-        assert abs(gg.mean() - cg.mean()) <= 0.05 * cg.mean() + 1e-4, (f, gg.mean(), cg.mean())
+        # Measured on B200: every buffer agrees on every pixel for all six
+        # frames; the bar leaves room for a rare flipped decision.
+        assert di_ok >= 0.99, (f, di_ok)
+        assert gi_ok >= 0.98, (f, gi_ok)
+        assert abs(gd.mean() - cd.mean()) <= 0.005 * cd.mean() + 1e-5, (f, gd.mean(), cd.mean())
+        assert abs(gg.mean() - cg.mean()) <= 0.01 * cg.mean() + 1e-5, (f, gg.mean(), cg.mean())
         film = s.film()
         np.testing.assert_allclose(film[..., :3], np.nan_to_num(gd + gg, posinf=0, neginf=0), rtol=1e-5, atol=1e-6)
         gr = s.restir_buffer('di_reservoirs')
         cr = ort.buffer('di_reservoirs', vb.DI_RESERVOIR_DTYPE)
         same_light = (gr['light_index'] == cr['light_index'])[hit].mean()
-        assert same_light >= thr, (f, same_light)
+        assert same_light >= 0.99, (f, same_light)
+        gw = s.restir_buffer('gi_reservoirs')['W']
+        cw = ort.buffer('gi_reservoirs', vb.GI_RESERVOIR_DTYPE)['W']
+        assert _close(gw, cw, 2e-3, 1e-6)[hit].mean() >= 0.98, f
 
 
 def test_restir_reset_restarts_history(vb, gpu_ctx):
