@@ -42,8 +42,18 @@ WORKLOADS = {
 WORKLOADS['many_lights'] = dict(kind='many_lights', width=1920, height=1080, spp=1, frames=64, emitters=10000,
                                 M_light=32, history_limit=20, spatial_neighbours=5, spatial_radius=30.0,
                                 max_depth=8, dimension=3, sampler='pcg', seed=7)
+# Serving: Poisson arrivals (lambda = 50 jobs/s, seeded) of render jobs with
+# resolution uniform over {256^2, 512^2, 1024^2, 1920x1080}, spp uniform over
+# {1, 4, 16, 64}, each on one of 4 resident scenes (box room, large scene,
+# many-light box room geometry with the plain tracer, 10 M-triangle instanced
+# scene), HBM admission budget 150 GB; one step = one job.  The full
+# configuration is 10,000 jobs; --steps sets how many are submitted.
+WORKLOADS['serving'] = dict(kind='serving', rate=50.0, jobs=10000, hbm_budget_gb=150, max_jobs=64,
+                            paths_per_batch=1 << 24, seed=21,
+                            resolutions=[[256, 256], [512, 512], [1024, 1024], [1920, 1080]],
+                            spp=[1, 4, 16, 64], scenes=['box_room', 'large_scene', 'many_lights_pt', 'instanced'])
 DEFAULT_WORKLOAD = 'large_scene'
-DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64}
+DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64, 'serving': 200}
 
 # DRAM bytes per path of k_render measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch divided by its paths; profiles/).
@@ -274,6 +284,9 @@ def main():
     if w['kind'] == 'many_lights':
         run_restir(args, w, rank, world, local_rank, dist)
         return
+    if w['kind'] == 'serving':
+        run_serving(args, w, rank, world, local_rank, dist)
+        return
     ctx = vb.Context(local_rank)
     scene = vb.Scene(ctx, workload_scene(args.workload))
     t0 = time.perf_counter()
@@ -484,6 +497,117 @@ def run_restir(args, w, rank, world, local_rank, dist):
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def serving_scenes():
+    from vision_b200 import scenes
+    return {'box_room': scenes.box_room(256, 256, max_depth=8, dimension=4, sampler='pcg'),
+            'large_scene': scenes.large_scene(),
+            'many_lights_pt': scenes.many_lights(256, 256, integrator='pt', dimension=4, max_depth=8),
+            'instanced': scenes.instanced_scene()}
+
+
+def serving_jobs(w, count):
+    rng = np.random.default_rng(w['seed'])
+    t = np.cumsum(rng.exponential(1.0 / w['rate'], count))
+    res = rng.integers(0, len(w['resolutions']), count)
+    spp = rng.integers(0, len(w['spp']), count)
+    scn = rng.integers(0, len(w['scenes']), count)
+    fb = rng.integers(0, 1 << 16, count)
+    return [(float(t[i]), int(scn[i]), w['resolutions'][res[i]][0], w['resolutions'][res[i]][1],
+             w['spp'][spp[i]], int(fb[i])) for i in range(count)]
+
+
+def run_serving(args, w, rank, world, local_rank, dist):
+    """The serving workload: jobs arrive on a seeded Poisson clock, go through
+    the C-ABI server (host descriptor in, host film out) and are timed from
+    submission to the film on the host."""
+    import torch
+    import vision_b200 as vb
+    ctx = vb.Context(local_rank)
+    t0 = time.perf_counter()
+    built = {}
+    for name, sc in serving_scenes().items():
+        built[name] = vb.Scene(ctx, sc).build_accel()
+    build_s = time.perf_counter() - t0
+    # Algorithmic bytes per path of each scene (1 frame at its own resolution).
+    bpp = {}
+    for name, s in built.items():
+        info = s.info()
+        segs, nodes, tris = s.render_stats(0, 1)
+        bpp[name] = 32.0 + (80.0 * nodes + 36.0 * tris + 180.0 * segs) / (info['width'] * info['height'])
+    def make_server():
+        srv = vb.Server(ctx, hbm_budget=int(w['hbm_budget_gb']) << 30, max_jobs=w['max_jobs'],
+                        paths_per_batch=w['paths_per_batch'])
+        return srv, {name: srv.add_scene(s) for name, s in built.items()}
+
+    # Warm-up jobs on a separate server instance (not timed).
+    warm, wids = make_server()
+    for i in range(args.warmup):
+        warm.result(warm.submit(wids[w['scenes'][i % 4]], 256, 256, 1, frame_begin=i), timeout=600)
+    warm.close()
+    srv, ids = make_server()
+    jobs = serving_jobs(w, args.steps)
+    results = []
+    done_bytes = [0]
+    import queue
+    pending = queue.Queue()
+
+    def collect():
+        while True:
+            jid = pending.get()
+            if jid is None:
+                return
+            out = srv.result(jid, timeout=-1.0)
+            done_bytes[0] += out.nbytes
+    collector = threading.Thread(target=collect)
+    collector.start()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    launches0 = vb.launch_count()
+    start = time.perf_counter()
+    for k, (t_arr, sidx, wd, h, spp, fb) in enumerate(jobs):
+        delay = start + t_arr - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        jid = srv.submit(ids[w['scenes'][sidx]], wd, h, spp, frame_begin=fb)
+        pending.put(jid)
+        results.append((sidx, wd * h * spp))
+    pending.put(None)
+    collector.join()
+    wall = time.perf_counter() - start
+    launches = vb.launch_count() - launches0
+    clk = clocks.stop()
+    st = srv.stats()
+    paths = float(sum(p for _, p in results))
+    value = paths / wall / 1e6
+    mean_bpp = sum(bpp[w['scenes'][s]] * p for s, p in results) / paths
+    peak, peak_src = measured_peaks()
+    gpu_s = st['gpu_busy_s']
+    achieved = mean_bpp * paths / gpu_s / 1e9 if gpu_s > 0 else None
+    line = {
+        'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': world, 'steps': len(jobs),
+        'warmup': args.warmup, 'ms_per_step': wall * 1e3 / len(jobs), 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
+                   'jobs_submitted': len(jobs), 'step': 'one job (submit -> film on the host)',
+                   'parallelism': 'replicas%d' % world, 'scene_build_s': round(build_s, 1)},
+        'latency_ms': {'p50': st['p50_ms'], 'p95': st['p95_ms'], 'p99': st['p99_ms'], 'mean': st['mean_ms'],
+                       'max': st['max_ms']},
+        'server': {k: st[k] for k in ('completed', 'batches', 'graph_launches', 'gpu_busy_s', 'peak_jobs',
+                                      'peak_bytes')},
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                     'frac': achieved / peak if achieved else None, 'peak_source': peak_src, 'traffic': None,
+                     'kernel': 'k_serve (persistent path kernel)', 'bytes_per_path': mean_bpp,
+                     'gpu_busy_s': gpu_s},
+        'clocks': clk,
+        'e2e': {'value': value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 96,
+                'd2h_bytes_per_step': int(done_bytes[0] / max(len(jobs), 1))},
+        'gpu_launches': int(launches),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    srv.close()
 
 
 if __name__ == '__main__':

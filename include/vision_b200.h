@@ -219,6 +219,51 @@ int vs_restir_params(const vs_scene *scene, uint32_t frame_index, void *dst, siz
 #define VS_RESTIR_GI_SAMPLES 7   /* 64 bytes: initial indirect samples */
 int vs_restir_download(vs_scene *scene, int which, void *dst, size_t bytes);
 
+/* Render-job server: continuous batching of vs_render-equivalent jobs of mixed
+ * resolution and spp over resident scenes.  No reference counterpart (the
+ * reference renders one scene interactively); it serves the path above.
+ * A native scheduler thread admits jobs while job slots and `hbm_budget`
+ * bytes allow (each job holds a float4 film; two batch buffers of
+ * `paths_per_batch` float4 paths are reserved at creation), then keeps the GPU
+ * busy with batches of whole frames from all admitted jobs, each batch one
+ * CUDA-graph launch (work-table upload, persistent path kernel, film pass).
+ * A job's film equals vs_render of the same scene, camera, resolution and
+ * frames [frame_begin, frame_begin + spp).  Scenes must stay alive while the
+ * server uses them and must use 4 hero wavelengths.  vs_server_destroy waits
+ * for submitted jobs. */
+typedef struct vs_server vs_server;
+typedef struct vs_job_desc {
+    uint32_t scene;         /* id from vs_server_add_scene */
+    uint32_t width, height;
+    uint32_t spp;           /* frames rendered; one path per pixel per frame */
+    uint32_t frame_begin;   /* first frame index (sampler streams) */
+    float fov_y_deg;        /* <= 0: the scene's camera field of view */
+    int use_c2w;            /* 0: the scene's camera transform */
+    float c2w[16];          /* camera-to-world, column-major */
+} vs_job_desc;
+typedef struct vs_server_stats {
+    uint64_t submitted, completed, batches, graph_launches, kernel_launches;
+    double paths;           /* paths of completed jobs */
+    double wall_s;          /* first submission to last completion */
+    double gpu_busy_s;      /* summed batch durations on the GPU */
+    double p50_ms, p95_ms, p99_ms, mean_ms, max_ms; /* submission -> film on the host */
+    uint64_t peak_bytes;    /* largest admitted job memory */
+    uint32_t peak_jobs;     /* most jobs in flight at once */
+} vs_server_stats;
+int vs_server_create(vs_context *ctx, uint64_t hbm_budget, uint32_t max_jobs, uint64_t paths_per_batch,
+                     vs_server **out);
+void vs_server_destroy(vs_server *server);
+int vs_server_add_scene(vs_server *server, vs_scene *scene, uint32_t *scene_id);
+/* Non-blocking; thread-safe. */
+int vs_server_submit(vs_server *server, const vs_job_desc *job, uint64_t *job_id);
+int vs_server_poll(vs_server *server, uint64_t job_id, int *done);
+/* Waits up to timeout_s (< 0: no limit), copies the film (float4 per pixel)
+ * and releases the job. */
+int vs_server_result(vs_server *server, uint64_t job_id, float *dst, size_t bytes, double timeout_s);
+int vs_server_stats_get(vs_server *server, vs_server_stats *out);
+/* Message of the server's last failed call. */
+const char *vs_server_last_error(const vs_server *server);
+
 /* Albedo tables of the energy-compensated lobes (164864 floats: PureReflection
  * 32^2, Dielectric and DielectricInv 32^3 x 2, Specular 32^3).  which = 0: the
  * values the renderer uses (the reference's precomputed_table.h); which = 1:

@@ -76,3 +76,8 @@ def test_comments_and_trailing_commas(vb, host_ctx):
     text = text[:-1].rstrip() + ',\n}'
     s = vb.Scene(host_ctx, text)
     assert s.info()['prim_count'] == 36
+
+
+def test_server_needs_device(vb, host_ctx):
+    with pytest.raises(vb.VisionError):
+        vb.Server(host_ctx)

@@ -1,0 +1,85 @@
+"""Render-job server: a job's film equals vs_render of the same scene, camera,
+resolution and frames; the same job gives the same film alone and inside a
+mix of concurrent jobs of other scenes, resolutions and spp; admission keeps
+the job-slot limit; latency statistics are ordered."""
+import numpy as np
+import pytest
+
+from vision_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def served(vb, gpu_ctx):
+    box = vb.Scene(gpu_ctx, scenes.box_room(64, 48, sampler='pcg')).build_accel()
+    big = vb.Scene(gpu_ctx, scenes.large_scene(48, 40, subdivisions=3, grid=60, tiles=3, sky_width=256,
+                                               sky_height=128, max_depth=6)).build_accel()
+    return box, big
+
+
+def test_server_job_equals_render(vb, gpu_ctx, served):
+    box, big = served
+    srv = vb.Server(gpu_ctx, hbm_budget=4 << 30, max_jobs=8, paths_per_batch=1 << 16)
+    ids = [srv.add_scene(box), srv.add_scene(big)]
+    for sid, scene in zip(ids, (box, big)):
+        info = scene.info()
+        j = srv.submit(sid, info['width'], info['height'], 6, frame_begin=0)
+        got = srv.result(j, timeout=120)
+        scene.render(0, 6)
+        ref = scene.film()
+        close = np.abs(got - ref) <= 1e-5 + 1e-5 * np.abs(ref)
+        assert close.all(-1).mean() >= 0.999, close.all(-1).mean()
+    srv.close()
+
+
+def test_server_same_alone_and_in_mix(vb, gpu_ctx, served):
+    box, big = served
+    srv = vb.Server(gpu_ctx, hbm_budget=4 << 30, max_jobs=16, paths_per_batch=1 << 15)
+    b, g = srv.add_scene(box), srv.add_scene(big)
+    cam = scenes.camera_c2w((0.05, 0.45, 1.8), (0.0, 0.5, 0.0))
+    alone = srv.result(srv.submit(b, 40, 30, 9, frame_begin=3, c2w=cam, fov_y=40.0), timeout=120)
+    rng = np.random.default_rng(0)
+    mix = []
+    for k in range(10):
+        sid = (b, g)[k % 2]
+        w, h = [(32, 32), (48, 40), (64, 48), (24, 16)][rng.integers(0, 4)]
+        mix.append(srv.submit(sid, w, h, int(rng.choice([1, 4, 16])), frame_begin=int(rng.integers(0, 50))))
+        if k == 4:
+            target = srv.submit(b, 40, 30, 9, frame_begin=3, c2w=cam, fov_y=40.0)
+    in_mix = srv.result(target, timeout=120)
+    for j in mix:
+        srv.result(j, timeout=120)
+    assert np.array_equal(alone, in_mix)
+    st = srv.stats()
+    assert st['completed'] == st['submitted'] == 12
+    assert st['batches'] > 1 and st['graph_launches'] == st['batches']
+    assert st['p50_ms'] <= st['p95_ms'] <= st['p99_ms'] <= st['max_ms']
+    srv.close()
+
+
+def test_server_admission_limit(vb, gpu_ctx, served):
+    box, _ = served
+    srv = vb.Server(gpu_ctx, hbm_budget=4 << 30, max_jobs=2, paths_per_batch=1 << 14)
+    b = srv.add_scene(box)
+    jobs = [srv.submit(b, 32, 32, 8, frame_begin=i) for i in range(6)]
+    for j in jobs:
+        srv.result(j, timeout=120)
+    st = srv.stats()
+    assert st['peak_jobs'] <= 2 and st['completed'] == 6
+    assert st['peak_bytes'] <= 2 * 32 * 32 * 16
+    srv.close()
+
+
+def test_server_rejects(vb, gpu_ctx, served):
+    box, _ = served
+    srv = vb.Server(gpu_ctx, hbm_budget=1 << 30, max_jobs=2, paths_per_batch=1 << 12)
+    b = srv.add_scene(box)
+    with pytest.raises(vb.VisionError):
+        srv.submit(b, 128, 128, 1)      # one frame larger than a batch
+    with pytest.raises(vb.VisionError):
+        srv.submit(7, 16, 16, 1)        # unknown scene
+    rt = vb.Scene(gpu_ctx, scenes.box_room(16, 16, dimension=3)).build_accel()
+    with pytest.raises(vb.UnsupportedError):
+        srv.add_scene(rt)
+    srv.close()

@@ -57,6 +57,20 @@ class SceneInfo(ctypes.Structure):
         'spd_floats', 'bvh_node_count', 'bvh_depth', 'width', 'height', 'spectrum_dim', 'max_depth', 'accel_built')]
 
 
+class JobDesc(ctypes.Structure):
+    _fields_ = [('scene', ctypes.c_uint32), ('width', ctypes.c_uint32), ('height', ctypes.c_uint32),
+                ('spp', ctypes.c_uint32), ('frame_begin', ctypes.c_uint32), ('fov_y_deg', ctypes.c_float),
+                ('use_c2w', ctypes.c_int), ('c2w', ctypes.c_float * 16)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ('submitted', 'completed', 'batches', 'graph_launches',
+                                               'kernel_launches')] + \
+               [(n, ctypes.c_double) for n in ('paths', 'wall_s', 'gpu_busy_s', 'p50_ms', 'p95_ms', 'p99_ms',
+                                               'mean_ms', 'max_ms')] + \
+               [('peak_bytes', ctypes.c_uint64), ('peak_jobs', ctypes.c_uint32)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError('libvision_b200.so not built: run `python vision_b200/build.py` (%s missing)' % LIB_PATH)
@@ -95,6 +109,14 @@ def _load():
         'vs_restir_reset': ([P], ctypes.c_int),
         'vs_restir_params': ([P, U32, P, ctypes.c_size_t], ctypes.c_int),
         'vs_restir_download': ([P, ctypes.c_int, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_server_create': ([P, ctypes.c_uint64, U32, ctypes.c_uint64, ctypes.POINTER(P)], ctypes.c_int),
+        'vs_server_destroy': ([P], None),
+        'vs_server_add_scene': ([P, P, ctypes.POINTER(U32)], ctypes.c_int),
+        'vs_server_submit': ([P, ctypes.POINTER(JobDesc), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        'vs_server_poll': ([P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        'vs_server_result': ([P, ctypes.c_uint64, P, ctypes.c_size_t, ctypes.c_double], ctypes.c_int),
+        'vs_server_stats_get': ([P, ctypes.POINTER(ServerStats)], ctypes.c_int),
+        'vs_server_last_error': ([P], ctypes.c_char_p),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -112,7 +134,9 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_film_download', 'vs_trace_closest_device', 'vs_trace_closest_host', 'vs_trace_any_device',
                       'vs_trace_any_host', 'vs_rgb_to_spectrum', 'vs_launch_count', 'vs_render_stats', 'vs_timing_enable',
                       'vs_timing_read', 'vs_render_noalloc', 'vs_albedo_luts', 'vs_restir_frame',
-                      'vs_restir_reset', 'vs_restir_params', 'vs_restir_download'])
+                      'vs_restir_reset', 'vs_restir_params', 'vs_restir_download', 'vs_server_create',
+                      'vs_server_destroy', 'vs_server_add_scene', 'vs_server_submit', 'vs_server_poll',
+                      'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error'])
 
 # Per-pixel ReSTIR records (vision_b200/csrc/vs_restir.h) as numpy dtypes.
 HIT_DTYPE = np.dtype([('inst_id', '<u4'), ('prim_id', '<u4'), ('u', '<f4'), ('v', '<f4')])
@@ -311,6 +335,72 @@ class Scene:
     def close(self):
         if self.handle:
             lib.vs_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Render-job server (vs_server_*): continuous batching of path-tracing
+    jobs over resident scenes."""
+
+    def __init__(self, ctx, hbm_budget=150 << 30, max_jobs=64, paths_per_batch=1 << 23):
+        h = ctypes.c_void_p()
+        ctx.check(lib.vs_server_create(ctx.handle, hbm_budget, max_jobs, paths_per_batch, ctypes.byref(h)),
+                  'server_create')
+        self.ctx = ctx
+        self.handle = h
+        self.scenes = []
+        self.sizes = {}
+
+    def check(self, rc, what):
+        if rc != VS_OK:
+            msg = '%s: %s' % (what, lib.vs_server_last_error(self.handle).decode())
+            raise (UnsupportedError if rc == VS_E_UNSUPPORTED else VisionError)(rc, msg)
+
+    def add_scene(self, scene):
+        sid = ctypes.c_uint32()
+        self.check(lib.vs_server_add_scene(self.handle, scene.handle, ctypes.byref(sid)), 'add_scene')
+        self.scenes.append(scene)  # the scene must outlive its use by the server
+        return sid.value
+
+    def submit(self, scene_id, width, height, spp, frame_begin=0, c2w=None, fov_y=0.0):
+        d = JobDesc()
+        d.scene, d.width, d.height, d.spp, d.frame_begin = scene_id, width, height, spp, frame_begin
+        d.fov_y_deg = fov_y
+        if c2w is not None:
+            d.use_c2w = 1
+            m = np.asarray(c2w, np.float32).T.reshape(-1)
+            for i in range(16):
+                d.c2w[i] = float(m[i])
+        jid = ctypes.c_uint64()
+        self.check(lib.vs_server_submit(self.handle, ctypes.byref(d), ctypes.byref(jid)), 'submit')
+        self.sizes[jid.value] = (height, width)
+        return jid.value
+
+    def poll(self, job):
+        done = ctypes.c_int()
+        self.check(lib.vs_server_poll(self.handle, job, ctypes.byref(done)), 'poll')
+        return bool(done.value)
+
+    def result(self, job, timeout=-1.0):
+        h, w = self.sizes.pop(job)
+        out = np.zeros((h, w, 4), np.float32)
+        self.check(lib.vs_server_result(self.handle, job, _ptr(out), out.nbytes, timeout), 'result')
+        return out
+
+    def stats(self):
+        s = ServerStats()
+        self.check(lib.vs_server_stats_get(self.handle, ctypes.byref(s)), 'stats')
+        return {n: getattr(s, n) for n, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib.vs_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

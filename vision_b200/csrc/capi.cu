@@ -10,6 +10,7 @@
 #include "vs_host.h"
 #include "vs_launch.h"
 #include "vs_microfacet.h"
+#include "vs_server.h"
 
 using namespace vs;
 
@@ -201,6 +202,7 @@ int upload_scene(vs_scene *s) {
         const Cie5 &c = cie5();
         VS_CUDA(upload_spectral_consts(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_rt(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        VS_CUDA(upload_spectral_consts_serve(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         ctx->consts_uploaded = true;
     }
     const HostScene &h = s->host;
@@ -862,6 +864,124 @@ int vs_restir_download(vs_scene *s, int which, void *dst, size_t bytes) {
     VS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream), "restir copy");
     VS_CUDA(cudaStreamSynchronize(ctx->stream), "restir sync");
     return VS_OK;
+}
+
+}  // extern "C"
+
+struct vs_server {
+    vs_context *ctx = nullptr;
+    Server *impl = nullptr;
+    std::mutex mu;
+    std::string error;
+    int fail(int code, const std::string &msg) {
+        std::lock_guard<std::mutex> lk(mu);
+        error = msg;
+        return code;
+    }
+};
+
+extern "C" {
+
+int vs_server_create(vs_context *ctx, uint64_t hbm_budget, uint32_t max_jobs, uint64_t paths_per_batch,
+                     vs_server **out) {
+    if (!ctx || !out) return VS_E_INVALID;
+    *out = nullptr;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot serve");
+    std::string err;
+    Server *impl = nullptr;
+    int rc = server_create(ctx->device, hbm_budget, max_jobs, paths_per_batch, &impl, err);
+    if (rc != VS_OK) return fail(ctx, rc, err);
+    vs_server *s = new vs_server();
+    s->ctx = ctx;
+    s->impl = impl;
+    *out = s;
+    return VS_OK;
+}
+
+void vs_server_destroy(vs_server *s) {
+    if (!s) return;
+    server_destroy(s->impl);
+    delete s;
+}
+
+int vs_server_add_scene(vs_server *s, vs_scene *scene, uint32_t *scene_id) {
+    if (!s || !scene || !scene_id) return VS_E_INVALID;
+    DeviceScene dv;
+    {
+        std::lock_guard<std::mutex> lock(scene->mu);
+        if (!scene->uploaded) return s->fail(VS_E_STATE, "vs_scene_build_accel must precede vs_server_add_scene");
+        dv = scene->device_view();
+    }
+    std::string err;
+    int rc = server_add_scene(s->impl, dv, scene_id, err);
+    return rc == VS_OK ? VS_OK : s->fail(rc, err);
+}
+
+int vs_server_submit(vs_server *s, const vs_job_desc *job, uint64_t *job_id) {
+    if (!s || !job || !job_id) return VS_E_INVALID;
+    if (job->width == 0 || job->height == 0 || job->spp == 0) return s->fail(VS_E_INVALID, "empty job");
+    ServeJob j{};
+    j.scene = job->scene;
+    j.frame_begin = job->frame_begin;
+    j.spp = job->spp;
+    std::string err;
+    // The job's sensor: the scene's camera at the job's resolution, with the
+    // job's transform and field of view when given.
+    const Camera *base = nullptr;
+    int rc = server_scene_camera(s->impl, job->scene, &base, err);
+    if (rc != VS_OK) return s->fail(rc, err);
+    Camera cam = camera_at_resolution(*base, job->width, job->height);
+    if (job->use_c2w)
+        for (int c = 0; c < 4; ++c)
+            for (int r = 0; r < 4; ++r) cam.c2w.m[c][r] = job->c2w[4 * c + r];
+    if (job->fov_y_deg > 0.0f) {
+        float fov = std::min(std::max(job->fov_y_deg, 15.0f), 120.0f);
+        cam.tan_half_fov = std::tan(fov * kPi / 180.0f * 0.5f);
+    }
+    j.cam = cam;
+    rc = server_submit(s->impl, j, job_id, err);
+    return rc == VS_OK ? VS_OK : s->fail(rc, err);
+}
+
+int vs_server_poll(vs_server *s, uint64_t job_id, int *done) {
+    if (!s || !done) return VS_E_INVALID;
+    std::string err;
+    int rc = server_poll(s->impl, job_id, done, err);
+    return rc == VS_OK ? VS_OK : s->fail(rc, err);
+}
+
+int vs_server_result(vs_server *s, uint64_t job_id, float *dst, size_t bytes, double timeout_s) {
+    if (!s || !dst) return VS_E_INVALID;
+    std::string err;
+    int rc = server_result(s->impl, job_id, dst, bytes, timeout_s, err);
+    return rc == VS_OK ? VS_OK : s->fail(rc, err);
+}
+
+int vs_server_stats_get(vs_server *s, vs_server_stats *out) {
+    if (!s || !out) return VS_E_INVALID;
+    ServeStats st;
+    server_stats(s->impl, &st);
+    out->submitted = st.submitted;
+    out->completed = st.completed;
+    out->batches = st.batches;
+    out->graph_launches = st.graph_launches;
+    out->kernel_launches = st.kernel_launches;
+    out->paths = st.paths;
+    out->wall_s = st.wall_s;
+    out->gpu_busy_s = st.gpu_busy_s;
+    out->p50_ms = st.p50_ms;
+    out->p95_ms = st.p95_ms;
+    out->p99_ms = st.p99_ms;
+    out->mean_ms = st.mean_ms;
+    out->max_ms = st.max_ms;
+    out->peak_bytes = st.peak_bytes;
+    out->peak_jobs = st.peak_jobs;
+    return VS_OK;
+}
+
+const char *vs_server_last_error(const vs_server *s) {
+    if (!s) return "null server";
+    return s->error.c_str();
 }
 
 int vs_albedo_luts(int which, const char *cache_path, float *out, size_t count) {

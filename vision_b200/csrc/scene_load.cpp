@@ -718,8 +718,10 @@ struct Loader {
 
 }  // namespace
 
-void update_camera(HostScene &s, uint32_t width, uint32_t height) {
-    Camera &c = s.cam;
+void update_camera(HostScene &s, uint32_t width, uint32_t height) { s.cam = camera_at_resolution(s.cam, width, height); }
+
+Camera camera_at_resolution(const Camera &base, uint32_t width, uint32_t height) {
+    Camera c = base;
     c.width = width;
     c.height = height;
     // RadianceCollector::update_screen_window (radiance_collector.cpp:33-42).
@@ -734,6 +736,7 @@ void update_camera(HostScene &s, uint32_t width, uint32_t height) {
     c.screen_hi_y = hi_y;
     c.screen_span_x = hi_x - lo_x;
     c.screen_span_y = hi_y - lo_y;
+    return c;
 }
 
 // SphericalMap (spherical.cpp:26-215) with a procedural sky image and its

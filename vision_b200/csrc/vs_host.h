@@ -66,6 +66,9 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
 
 // Sets resolution / camera-derived fields after load or on update.
 void update_camera(HostScene &scene, uint32_t width, uint32_t height);
+// A sensor at another resolution: same transform, filter and field of view,
+// screen window of the new aspect ratio (radiance_collector.cpp:33-42).
+Camera camera_at_resolution(const Camera &base, uint32_t width, uint32_t height);
 
 // Builds the compressed BVH8 (nodes, tri_v) from pos/idx.
 void build_bvh8(HostScene &scene);

@@ -276,10 +276,11 @@ __device__ __forceinline__ f3 path_li(const DeviceScene &s, Sampler &smp, Wavele
     return ret;
 }
 
-// One camera path (PathTracingIntegrator kernel body, pt.cpp:53-72).
-// Returns linear sRGB radiance times the filter weight.
+// One camera path (PathTracingIntegrator kernel body, pt.cpp:53-72) through
+// sensor `cam`.  Returns linear sRGB radiance times the filter weight.
 template <int N>
-__device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_t frame) {
+__device__ __forceinline__ f3 trace_path_cam(const DeviceScene &s, const Camera &cam, uint32_t px, uint32_t py,
+                                             uint32_t frame) {
     const IntegratorParams &ip = s.ip;
     Sampler smp;
     // Wavelengths come from a separate stream (RenderEnv::initial, integrator.cpp:49-58).
@@ -288,8 +289,13 @@ __device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_
     smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
     f2 p_film;
     f3 ro, rd;
-    camera_ray(s.cam, smp, px, py, p_film, ro, rd);
+    camera_ray(cam, smp, px, py, p_film, ro, rd);
     return path_li<N>(s, smp, wl, ro, rd, 1e16f, Spec<N>::fill(1.0f), ip.max_depth, nullptr);
+}
+
+template <int N>
+__device__ f3 trace_path(const DeviceScene &s, uint32_t px, uint32_t py, uint32_t frame) {
+    return trace_path_cam<N>(s, s.cam, px, py, frame);
 }
 
 }  // namespace vs

@@ -17,6 +17,9 @@ cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_be
                         double *film64, cudaStream_t st);
 unsigned long long launch_count();
 void add_launches(unsigned n);
+// server.cu
+cudaError_t upload_spectral_consts_serve(const float *x, const float *y, const float *z, const float *d65,
+                                         float y_integral);
 // restir.cu
 cudaError_t upload_spectral_consts_rt(const float *x, const float *y, const float *z, const float *d65, float y_integral);
 cudaError_t launch_rt_reset(uint32_t npix, const RtBuffers &b, cudaStream_t st);

@@ -1,0 +1,51 @@
+// Render-job server: continuous batching of path-tracing jobs of mixed
+// resolution and spp over scenes resident on one device (server.cu).
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "vs_devscene.h"
+
+namespace vs {
+
+// Resident scenes per server and work items per batch.
+constexpr uint32_t kMaxServeScenes = 8;
+constexpr uint32_t kMaxServeItems = 256;
+
+struct ServeJob {
+    uint32_t scene;       // id from Server::add_scene
+    Camera cam;           // sensor of the job (resolution, transform)
+    uint32_t frame_begin; // first frame (sampler stream); frames frame_begin .. frame_begin + spp - 1
+    uint32_t spp;
+};
+
+struct ServeStats {
+    uint64_t submitted, completed, rejected;
+    uint64_t batches, graph_launches, kernel_launches;
+    double paths;            // paths of completed jobs
+    double wall_s;           // first submission to last completion
+    double gpu_busy_s;       // summed batch durations (CUDA events)
+    double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;  // submit -> film on the host
+    uint64_t peak_bytes;     // largest admitted job memory
+    uint32_t peak_jobs;      // largest number of jobs in flight
+};
+
+class Server;
+
+// Status codes follow include/vision_b200.h (0 = OK); `err` gets the message.
+int server_create(int device, uint64_t hbm_budget, uint32_t max_jobs, uint64_t paths_per_batch, Server **out,
+                  std::string &err);
+void server_destroy(Server *s);
+int server_add_scene(Server *s, const DeviceScene &scene, uint32_t *id, std::string &err);
+// The sensor of a resident scene (its camera when it was added).
+int server_scene_camera(Server *s, uint32_t id, const Camera **cam, std::string &err);
+int server_submit(Server *s, const ServeJob &job, uint64_t *id, std::string &err);
+// done = 1 when the job's film is on the host.
+int server_poll(Server *s, uint64_t id, int *done, std::string &err);
+// Waits (timeout_s < 0: forever) and copies the film (float4 per pixel,
+// running mean over the job's frames) to dst; releases the job.
+int server_result(Server *s, uint64_t id, float *dst, size_t bytes, double timeout_s, std::string &err);
+void server_stats(Server *s, ServeStats *out);
+
+}  // namespace vs

@@ -218,16 +218,18 @@ def camera_spline(frames=64, seed=3, target=(0.0, 0.45, 0.0)):
 
 
 def many_lights(width=1920, height=1080, emitters=10000, seed=7, M_light=32, M_bsdf=1, history_limit=20,
-                spatial_neighbours=5, spatial_radius=30.0, max_depth=8, sampler="pcg", gi=True):
+                spatial_neighbours=5, spatial_radius=30.0, max_depth=8, sampler="pcg", gi=True, integrator="rt",
+                dimension=3):
     """Many-light ReSTIR workload: the box room plus `emitters` one-sided
     emissive triangles (equilateral, edge U[0.01, 0.05], centres uniform in the
     room, random orientation, 2000-9000 K blackbody spectra, scale log-uniform
     over [1, 100]) with power-distribution light selection, rendered by the
     real-time ReSTIR integrator on 3 hero wavelengths: 32 initial light
     candidates, temporal reuse capped at M = 20, one spatial pass of 5
-    neighbours within 30 pixels."""
+    neighbours within 30 pixels.  integrator="pt" keeps the plain path tracer
+    (the geometry and emitters of the workload for other uses)."""
     import numpy as np
-    sc = box_room(width=width, height=height, max_depth=max_depth, dimension=3, sampler=sampler, seed=0)
+    sc = box_room(width=width, height=height, max_depth=max_depth, dimension=dimension, sampler=sampler, seed=0)
     rng = np.random.default_rng(seed)
     shapes = sc["shapes"]
     for i in range(emitters):
@@ -253,6 +255,8 @@ def many_lights(width=1920, height=1080, emitters=10000, seed=7, M_light=32, M_b
                                                "node": {"type": "blackbody", "param": {"temperature": temp}}},
                                      "scale": scale, "two_sided": False}}}})
     sc["light_sampler"] = {"type": "power", "param": {"lights": []}}
+    if integrator == "pt":
+        return sc
     sc["integrator"] = {"type": "rt", "param": {
         "max_depth": max_depth, "min_depth": 5, "rr_threshold": 1.0,
         "direct": {"M_light": M_light, "M_bsdf": M_bsdf,
@@ -261,4 +265,44 @@ def many_lights(width=1920, height=1080, emitters=10000, seed=7, M_light=32, M_b
         "indirect": {"open": bool(gi),
                      "spatial": {"sample_num": spatial_neighbours, "radius": spatial_radius},
                      "temporal": {"history_limit": history_limit}}}}
+    return sc
+
+
+def instanced_scene(width=1024, height=1024, copies=64, seed=11, subdivisions=6, patch=200, max_depth=16,
+                    dimension=4, sampler="pcg"):
+    """Serving scene of ~10 M triangles: `copies` seeded copies of one mesh
+    group modelled on the large scene's geometry (a displaced icosphere with
+    `subdivisions` levels, 81,920 triangles at 6, on a `patch` x `patch` grid
+    tile, 80,000 triangles at 200), each with a random position on an 8 x 8
+    layout, y rotation and scale, and a material drawn like the large scene's;
+    lit by the same procedural sky.  64 copies give 10,362,880 triangles."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    shapes, materials = [], []
+    side = int(math.ceil(math.sqrt(copies)))
+    spacing = 4.0
+    for c in range(copies):
+        gx, gz = c % side, c // side
+        cx = (gx - (side - 1) / 2.0) * spacing + rng.uniform(-0.5, 0.5)
+        cz = (gz - (side - 1) / 2.0) * spacing + rng.uniform(-0.5, 0.5)
+        s = float(rng.uniform(0.5, 1.5))
+        ang = float(rng.uniform(0.0, 360.0))
+        a = math.radians(ang)
+        ca, sa = math.cos(a), math.sin(a)
+        mat = _draw_material(rng, "copy_%d_mat" % c)
+        materials.append(mat)
+        rot = ((ca * s, 0.0, -sa * s), (0.0, s, 0.0), (sa * s, 0.0, ca * s))
+        shapes.append({"type": "icosphere", "name": "copy_%d_sphere" % c,
+                       "param": {"subdivisions": subdivisions, "radius": 1.0, "material": mat["name"],
+                                 "displacement": {"amplitude": 0.05, "frequency": 4.0, "seed": seed + c},
+                                 "transform": _cols(rot[0], rot[1], rot[2], (cx, s, cz))}})
+        shapes.append({"type": "grid", "name": "copy_%d_ground" % c,
+                       "param": {"nx": patch, "nz": patch, "size_x": spacing * 0.9, "size_z": spacing * 0.9,
+                                 "material": mat["name"],
+                                 "transform": _cols((1, 0, 0), (0, 1, 0), (0, 0, 1), (cx, 0.0, cz))}})
+    sc = large_scene(width=width, height=height, max_depth=max_depth, dimension=dimension, sampler=sampler)
+    sc["shapes"] = shapes
+    sc["materials"] = materials
+    sc["camera"]["param"]["transform"] = {"type": "look_at", "param": {
+        "position": [0.0, 12.0, 30.0], "target_pos": [0.0, 0.0, 0.0], "up": [0.0, 1.0, 0.0]}}
     return sc
