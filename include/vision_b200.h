@@ -264,6 +264,31 @@ int vs_server_stats_get(vs_server *server, vs_server_stats *out);
 /* Message of the server's last failed call. */
 const char *vs_server_last_error(const vs_server *server);
 
+/* Radiance-cache MLP (no reference counterpart): 64 BF16 inputs, 4 hidden
+ * layers of 64 with ReLU, 3 outputs, no biases; BF16 weights and activations
+ * with FP32 accumulation on the tcgen05 tensor cores; FP32 master weights
+ * trained with Adam on the mean relative L2 loss
+ * sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) / (3 n).  Feature rows are 64 BF16
+ * values (128 bytes, 16-byte aligned); outputs and targets are float4 per row
+ * (r, g, b, unused).  Pointers passed to _infer and _train are device
+ * pointers; both run asynchronously on `stream`. */
+#define VS_CACHE_PARAMS 16576
+typedef struct vs_cache vs_cache;
+/* Weights initialised uniformly in +-sqrt(6 / fan_in) from `seed`. */
+int vs_cache_create(vs_context *ctx, uint64_t seed, vs_cache **out);
+void vs_cache_destroy(vs_cache *cache);
+/* Master weights W[l][in][out], layers 0..4 (4 x 64 x 64, then 64 x 3). */
+int vs_cache_get_weights(vs_cache *cache, float *w, size_t count);
+int vs_cache_set_weights(vs_cache *cache, const float *w, size_t count);
+int vs_cache_set_optimizer(vs_cache *cache, float lr, float beta1, float beta2, float eps);
+int vs_cache_infer(vs_cache *cache, const uint16_t *features, uint32_t n, float *out4, void *stream);
+/* One training step on n samples; update = 0 computes the gradient and loss
+ * without changing the weights. */
+int vs_cache_train(vs_cache *cache, const uint16_t *features, const float *targets4, uint32_t n, int update,
+                   void *stream);
+/* Gradient (same layout as the weights) and loss of the last vs_cache_train. */
+int vs_cache_gradient(vs_cache *cache, float *grad, size_t count, double *loss);
+
 /* Albedo tables of the energy-compensated lobes (164864 floats: PureReflection
  * 32^2, Dielectric and DielectricInv 32^3 x 2, Specular 32^3).  which = 0: the
  * values the renderer uses (the reference's precomputed_table.h); which = 1:

@@ -117,6 +117,14 @@ def _load():
         'vs_server_result': ([P, ctypes.c_uint64, P, ctypes.c_size_t, ctypes.c_double], ctypes.c_int),
         'vs_server_stats_get': ([P, ctypes.POINTER(ServerStats)], ctypes.c_int),
         'vs_server_last_error': ([P], ctypes.c_char_p),
+        'vs_cache_create': ([P, ctypes.c_uint64, ctypes.POINTER(P)], ctypes.c_int),
+        'vs_cache_destroy': ([P], None),
+        'vs_cache_get_weights': ([P, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_cache_set_weights': ([P, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_cache_set_optimizer': ([P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+        'vs_cache_infer': ([P, P, U32, P, P], ctypes.c_int),
+        'vs_cache_train': ([P, P, P, U32, ctypes.c_int, P], ctypes.c_int),
+        'vs_cache_gradient': ([P, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -136,7 +144,10 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_timing_read', 'vs_render_noalloc', 'vs_albedo_luts', 'vs_restir_frame',
                       'vs_restir_reset', 'vs_restir_params', 'vs_restir_download', 'vs_server_create',
                       'vs_server_destroy', 'vs_server_add_scene', 'vs_server_submit', 'vs_server_poll',
-                      'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error'])
+                      'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error', 'vs_cache_create',
+                      'vs_cache_destroy', 'vs_cache_get_weights', 'vs_cache_set_weights', 'vs_cache_set_optimizer',
+                      'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient'])
+CACHE_PARAMS = 16576
 
 # Per-pixel ReSTIR records (vision_b200/csrc/vs_restir.h) as numpy dtypes.
 HIT_DTYPE = np.dtype([('inst_id', '<u4'), ('prim_id', '<u4'), ('u', '<f4'), ('v', '<f4')])
@@ -401,6 +412,55 @@ class Server:
     def close(self):
         if self.handle:
             lib.vs_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RadianceCache:
+    """Radiance-cache MLP on the tensor cores (vs_cache_*).  Feature and
+    output buffers are device pointers (e.g. torch tensors' data_ptr())."""
+
+    def __init__(self, ctx, seed=1):
+        h = ctypes.c_void_p()
+        ctx.check(lib.vs_cache_create(ctx.handle, seed, ctypes.byref(h)), 'cache_create')
+        self.ctx = ctx
+        self.handle = h
+
+    def weights(self):
+        w = np.zeros(CACHE_PARAMS, np.float32)
+        self.ctx.check(lib.vs_cache_get_weights(self.handle, _ptr(w), w.size), 'cache weights')
+        return w
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        self.ctx.check(lib.vs_cache_set_weights(self.handle, _ptr(w), w.size), 'cache set weights')
+
+    def set_optimizer(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.ctx.check(lib.vs_cache_set_optimizer(self.handle, lr, beta1, beta2, eps), 'cache optimizer')
+
+    def infer(self, feat_ptr, n, out_ptr, stream=None):
+        self.ctx.check(lib.vs_cache_infer(self.handle, ctypes.c_void_p(feat_ptr), n, ctypes.c_void_p(out_ptr),
+                                          ctypes.c_void_p(stream) if stream else None), 'cache infer')
+
+    def train(self, feat_ptr, target_ptr, n, update=True, stream=None):
+        self.ctx.check(lib.vs_cache_train(self.handle, ctypes.c_void_p(feat_ptr), ctypes.c_void_p(target_ptr), n,
+                                          1 if update else 0, ctypes.c_void_p(stream) if stream else None),
+                       'cache train')
+
+    def gradient(self):
+        g = np.zeros(CACHE_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        self.ctx.check(lib.vs_cache_gradient(self.handle, _ptr(g), g.size, ctypes.byref(loss)), 'cache gradient')
+        return g, loss.value
+
+    def close(self):
+        if self.handle:
+            lib.vs_cache_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,6 +1,7 @@
 // extern "C" boundary of libvision_b200.so (declared in include/vision_b200.h).
 #include "../../include/vision_b200.h"
 
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
@@ -10,6 +11,7 @@
 #include "vs_host.h"
 #include "vs_launch.h"
 #include "vs_microfacet.h"
+#include "vs_mlp.h"
 #include "vs_server.h"
 
 using namespace vs;
@@ -982,6 +984,160 @@ int vs_server_stats_get(vs_server *s, vs_server_stats *out) {
 const char *vs_server_last_error(const vs_server *s) {
     if (!s) return "null server";
     return s->error.c_str();
+}
+
+}  // extern "C"
+
+struct vs_cache {
+    vs_context *ctx = nullptr;
+    MlpState st{};
+    MlpAdam adam{1e-3f, 0.9f, 0.999f, 1e-8f, 1u, 0.0f};
+    ~vs_cache() {
+        if (ctx && ctx->device >= 0) cudaSetDevice(ctx->device);
+        cudaFree(st.w);
+        cudaFree(st.pack);
+        cudaFree(st.m);
+        cudaFree(st.v);
+        cudaFree(st.grad);
+        cudaFree(st.loss);
+        cudaFree(st.err);
+    }
+};
+
+namespace {
+int cache_check_err(vs_cache *c) {
+    vs_context *ctx = c->ctx;
+    int h = 0;
+    VS_CUDA(cudaMemcpy(&h, c->st.err, sizeof(int), cudaMemcpyDeviceToHost), "cache error flag");
+    if (h) return fail(ctx, VS_E_CUDA, "tensor-core wait timed out in the radiance-cache kernels");
+    return VS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int vs_cache_create(vs_context *ctx, uint64_t seed, vs_cache **out) {
+    if (!ctx || !out) return VS_E_INVALID;
+    *out = nullptr;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context has no radiance cache");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    vs_cache *c = new vs_cache();
+    c->ctx = ctx;
+    MlpState &s = c->st;
+    cudaError_t e = cudaMalloc(&s.w, sizeof(float) * kMlpParams);
+    if (e == cudaSuccess) e = cudaMalloc(&s.pack, sizeof(uint16_t) * kMlpPackElems);
+    if (e == cudaSuccess) e = cudaMalloc(&s.m, sizeof(float) * kMlpParams);
+    if (e == cudaSuccess) e = cudaMalloc(&s.v, sizeof(float) * kMlpParams);
+    if (e == cudaSuccess) e = cudaMalloc(&s.grad, sizeof(float) * kMlpParams);
+    if (e == cudaSuccess) e = cudaMalloc(&s.loss, sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&s.err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s.pack, 0, sizeof(uint16_t) * kMlpPackElems);
+    if (e == cudaSuccess) e = cudaMemset(s.m, 0, sizeof(float) * kMlpParams);
+    if (e == cudaSuccess) e = cudaMemset(s.v, 0, sizeof(float) * kMlpParams);
+    if (e == cudaSuccess) e = cudaMemset(s.grad, 0, sizeof(float) * kMlpParams);
+    if (e == cudaSuccess) e = cudaMemset(s.loss, 0, sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(s.err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(ctx, e, "cache alloc");
+    }
+    // Uniform +-sqrt(6 / fan_in) from a splitmix64 stream.
+    std::vector<float> w(kMlpParams);
+    uint64_t x = seed;
+    for (int i = 0; i < kMlpParams; ++i) {
+        x += 0x9e3779b97f4a7c15ull;
+        uint64_t z = x;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        float u = static_cast<float>(z >> 40) * (1.0f / 16777216.0f);
+        w[i] = (2.0f * u - 1.0f) * std::sqrt(6.0f / 64.0f);
+    }
+    e = cudaMemcpy(s.w, w.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = mlp_pack(s, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(ctx, e, "cache init");
+    }
+    add_launches(1);
+    *out = c;
+    return VS_OK;
+}
+
+void vs_cache_destroy(vs_cache *c) { delete c; }
+
+int vs_cache_get_weights(vs_cache *c, float *w, size_t count) {
+    if (!c || !w || count != static_cast<size_t>(kMlpParams)) return VS_E_INVALID;
+    vs_context *ctx = c->ctx;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    VS_CUDA(cudaDeviceSynchronize(), "cache sync");
+    VS_CUDA(cudaMemcpy(w, c->st.w, sizeof(float) * count, cudaMemcpyDeviceToHost), "cache weights");
+    return VS_OK;
+}
+
+int vs_cache_set_weights(vs_cache *c, const float *w, size_t count) {
+    if (!c || !w || count != static_cast<size_t>(kMlpParams)) return VS_E_INVALID;
+    vs_context *ctx = c->ctx;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    VS_CUDA(cudaDeviceSynchronize(), "cache sync");
+    VS_CUDA(cudaMemcpy(c->st.w, w, sizeof(float) * count, cudaMemcpyHostToDevice), "cache weights");
+    VS_CUDA(cudaMemset(c->st.m, 0, sizeof(float) * count), "cache moments");
+    VS_CUDA(cudaMemset(c->st.v, 0, sizeof(float) * count), "cache moments");
+    VS_CUDA(mlp_pack(c->st, nullptr), "cache pack");
+    VS_CUDA(cudaDeviceSynchronize(), "cache sync");
+    add_launches(1);
+    c->adam.step = 1;
+    return VS_OK;
+}
+
+int vs_cache_set_optimizer(vs_cache *c, float lr, float beta1, float beta2, float eps) {
+    if (!c) return VS_E_INVALID;
+    c->adam.lr = lr;
+    c->adam.beta1 = beta1;
+    c->adam.beta2 = beta2;
+    c->adam.eps = eps;
+    return VS_OK;
+}
+
+int vs_cache_infer(vs_cache *c, const uint16_t *features, uint32_t n, float *out4, void *stream) {
+    if (!c || (n && (!features || !out4))) return VS_E_INVALID;
+    vs_context *ctx = c->ctx;
+    if ((reinterpret_cast<uintptr_t>(features) & 15u) || (reinterpret_cast<uintptr_t>(out4) & 15u))
+        return fail(ctx, VS_E_INVALID, "cache buffers must be 16-byte aligned");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    VS_CUDA(mlp_infer(c->st, features, n, reinterpret_cast<float4 *>(out4), st), "cache infer");
+    if (n) add_launches(1);
+    return VS_OK;
+}
+
+int vs_cache_train(vs_cache *c, const uint16_t *features, const float *targets4, uint32_t n, int update,
+                   void *stream) {
+    if (!c || (n && (!features || !targets4))) return VS_E_INVALID;
+    vs_context *ctx = c->ctx;
+    if ((reinterpret_cast<uintptr_t>(features) & 15u) || (reinterpret_cast<uintptr_t>(targets4) & 15u))
+        return fail(ctx, VS_E_INVALID, "cache buffers must be 16-byte aligned");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    c->adam.loss_scale = n ? 1.0f / (3.0f * static_cast<float>(n)) : 0.0f;
+    VS_CUDA(mlp_train_step(c->st, features, reinterpret_cast<const float4 *>(targets4), n, c->adam, update != 0, st),
+            "cache train");
+    add_launches((n ? 1u : 0u) + (update ? 1u : 0u));
+    if (update) c->adam.step += 1;
+    return VS_OK;
+}
+
+int vs_cache_gradient(vs_cache *c, float *grad, size_t count, double *loss) {
+    if (!c || !grad || !loss || count != static_cast<size_t>(kMlpParams)) return VS_E_INVALID;
+    vs_context *ctx = c->ctx;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    VS_CUDA(cudaDeviceSynchronize(), "cache sync");
+    int rc = cache_check_err(c);
+    if (rc != VS_OK) return rc;
+    VS_CUDA(cudaMemcpy(grad, c->st.grad, sizeof(float) * count, cudaMemcpyDeviceToHost), "cache gradient");
+    VS_CUDA(cudaMemcpy(loss, c->st.loss, sizeof(double), cudaMemcpyDeviceToHost), "cache loss");
+    return VS_OK;
 }
 
 int vs_albedo_luts(int which, const char *cache_path, float *out, size_t count) {
