@@ -288,6 +288,15 @@ int vs_cache_train(vs_cache *cache, const uint16_t *features, const float *targe
                    void *stream);
 /* Gradient (same layout as the weights) and loss of the last vs_cache_train. */
 int vs_cache_gradient(vs_cache *cache, float *grad, size_t count, double *loss);
+/* vs_render with paths that stop after two bounces into the radiance cache:
+ * each pixel's path adds its emission and next-event estimates for two
+ * bounces, then the cache's prediction at the third vertex times the path
+ * throughput.  With train_samples > 0, that many paths per frame (a strided
+ * pixel subset moving every frame) continue two bounces further and the
+ * cache takes one Adam step per frame on their suffix radiance plus the
+ * cache at the suffix end.  Scenes must use 4 hero wavelengths. */
+int vs_render_cached(vs_scene *scene, vs_cache *cache, uint32_t frame_begin, uint32_t frame_count,
+                     uint32_t train_samples, int film_precision, void *stream);
 
 /* Albedo tables of the energy-compensated lobes (164864 floats: PureReflection
  * 32^2, Dielectric and DielectricInv 32^3 x 2, Specular 32^3).  which = 0: the

@@ -125,6 +125,7 @@ def _load():
         'vs_cache_infer': ([P, P, U32, P, P], ctypes.c_int),
         'vs_cache_train': ([P, P, P, U32, ctypes.c_int, P], ctypes.c_int),
         'vs_cache_gradient': ([P, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        'vs_render_cached': ([P, P, U32, U32, U32, ctypes.c_int, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -146,7 +147,7 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_server_destroy', 'vs_server_add_scene', 'vs_server_submit', 'vs_server_poll',
                       'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error', 'vs_cache_create',
                       'vs_cache_destroy', 'vs_cache_get_weights', 'vs_cache_set_weights', 'vs_cache_set_optimizer',
-                      'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient'])
+                      'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient', 'vs_render_cached'])
 CACHE_PARAMS = 16576
 
 # Per-pixel ReSTIR records (vision_b200/csrc/vs_restir.h) as numpy dtypes.
@@ -336,6 +337,13 @@ class Scene:
         out = np.zeros(i['width'] * i['height'], dt)
         self.ctx.check(lib.vs_restir_download(self.handle, key, _ptr(out), out.nbytes), 'restir_download')
         return out.reshape((i['height'], i['width']) + out.shape[1:])
+
+    def render_cached(self, cache, frame_begin, frame_count, train_samples=65536, fp64=False, stream=None):
+        """Cache-terminated frames; the cache trains on train_samples paths per frame."""
+        self.ctx.check(lib.vs_render_cached(self.handle, cache.handle, frame_begin, frame_count, train_samples,
+                                            FILM_FP64 if fp64 else FILM_FP32,
+                                            ctypes.c_void_p(stream) if stream else None), 'render_cached')
+        self.frames = frame_begin + frame_count
 
     def render_stats(self, frame_begin, frame_count):
         """Traversal counters of an instrumented render: (segments, nodes, tris)."""

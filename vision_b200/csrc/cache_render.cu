@@ -1,0 +1,352 @@
+// Cache-terminated path tracing with the radiance-cache MLP (mlp.cu).
+//
+// Per frame:
+//   k_cache_paths    one camera path per pixel through `query_depth` bounces
+//                    (emission with MIS and next-event estimation as in
+//                    IlluminationIntegrator::Li, integrator.cpp:134-283); at
+//                    the next surface it writes the vertex's encoded features
+//                    and its path state instead of continuing.  Every
+//                    `train_stride`-th pixel (offset per frame) is a training
+//                    path: it goes on for `suffix_depth` more bounces,
+//                    gathering the suffix radiance with the throughput
+//                    restarted at the query vertex, and writes the features of
+//                    the suffix end.
+//   mlp_infer        the cache at every query vertex and every suffix end
+//   k_cache_resolve  pixel radiance = gathered radiance + throughput times the
+//                    cache's radiance (RGB decoded as an illumination
+//                    spectrum at the path's wavelengths) into the film;
+//                    training target = suffix radiance + suffix throughput
+//                    times the cache at the suffix end (self-training).
+// The cache predicts the radiance leaving a vertex toward the previous one,
+// without the vertex's own emission (which the path adds with its MIS weight).
+// Features (64): position in the scene bounds, sin/cos(2^k pi p) for k = 0..7
+// on each axis (48); outgoing direction (3); shading normal (3); roughness (1);
+// albedo (3); sin/cos(pi w) of the outgoing direction (6).
+#include "vs_cache_render.h"
+#include "vs_integrator.cuh"
+#include "vs_launch.h"
+
+#include <cuda_bf16.h>
+
+namespace vs {
+
+namespace {
+
+constexpr int CN = 4;  // hero wavelengths of cache-rendered scenes
+using CSpec = Spec<CN>;
+using CWl = Wavelengths<CN>;
+
+__device__ __forceinline__ uint32_t bf2(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+__device__ void encode(const CacheFrameParams &p, const Interaction &it, uint16_t *out) {
+    float f[64];
+    const float pos[3] = {clampf((it.pos.x - p.bmin.x) * p.binv.x, 0.0f, 1.0f),
+                          clampf((it.pos.y - p.bmin.y) * p.binv.y, 0.0f, 1.0f),
+                          clampf((it.pos.z - p.bmin.z) * p.binv.z, 0.0f, 1.0f)};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float scale = 1.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            float sn, cs;
+            sincospif(scale * pos[a], &sn, &cs);
+            f[16 * a + 2 * k] = sn;
+            f[16 * a + 2 * k + 1] = cs;
+            scale *= 2.0f;
+        }
+    }
+    const float4 m = __ldg(&p.mat[it.mat]);
+    const f3 n = it.shading.z;
+    const float wo[3] = {it.wo.x, it.wo.y, it.wo.z};
+    f[48] = wo[0];
+    f[49] = wo[1];
+    f[50] = wo[2];
+    f[51] = n.x;
+    f[52] = n.y;
+    f[53] = n.z;
+    f[54] = m.w;
+    f[55] = m.x;
+    f[56] = m.y;
+    f[57] = m.z;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) sincospif(wo[a], &f[58 + 2 * a], &f[59 + 2 * a]);
+    uint4 *dst = reinterpret_cast<uint4 *>(out);
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+        dst[c] = make_uint4(bf2(f[8 * c], f[8 * c + 1]), bf2(f[8 * c + 2], f[8 * c + 3]),
+                            bf2(f[8 * c + 4], f[8 * c + 5]), bf2(f[8 * c + 6], f[8 * c + 7]));
+}
+
+__device__ __forceinline__ float4 spec4(const CSpec &s) { return make_float4(s.v[0], s.v[1], s.v[2], s.v[3]); }
+__device__ __forceinline__ CSpec spec_of(float4 v) {
+    CSpec s;
+    s.v[0] = v.x;
+    s.v[1] = v.y;
+    s.v[2] = v.z;
+    s.v[3] = v.w;
+    return s;
+}
+
+// Radiance of an RGB cache output at the path's wavelengths: the RGB decoded
+// as an illumination spectrum (sigmoid polynomial x scale x D65), as the
+// reference decodes RGB emission (hero.cpp:204-219).
+__device__ __forceinline__ CSpec cache_spectrum(const DeviceScene &s, float4 rgb, const CWl &wl) {
+    float c[4];
+    rgb2spec_unbound(s.rgb2spec, make3(fmaxf(rgb.x, 0.0f), fmaxf(rgb.y, 0.0f), fmaxf(rgb.z, 0.0f)), c);
+    CSpec r;
+#pragma unroll
+    for (int i = 0; i < CN; ++i) r.v[i] = sigmoid_poly(c[0], c[1], c[2], wl.lambda[i]) * c[3] * cie_spd(c_spec.d65, wl.lambda[i]);
+    return r;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFrameParams p) {
+    const uint32_t npix = s.cam.width * s.cam.height;
+    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= npix) return;
+    const uint32_t px = pix % s.cam.width, py = pix / s.cam.width;
+    const IntegratorParams &ip = s.ip;
+    // Training path?  Samples j = 0 .. n_train-1 sit at pixels offset + j * stride.
+    bool train = false;
+    uint32_t tj = 0;
+    if (p.n_train && pix >= p.train_offset && (pix - p.train_offset) % p.train_stride == 0) {
+        tj = (pix - p.train_offset) / p.train_stride;
+        train = tj < p.n_train;
+    }
+    Sampler smp;
+    smp.start(px, py, p.frame, 0xffffffffu, ip.sampler, ip.seed);
+    CWl wl = sample_wavelengths<CN>(smp.next());
+    smp.start(px, py, p.frame, 0u, ip.sampler, ip.seed);
+    f2 p_film;
+    f3 ro, rd;
+    camera_ray(s.cam, smp, px, py, p_film, ro, rd);
+
+    CSpec throughput = CSpec::fill(1.0f);
+    f3 ret = make3(0.0f);      // radiance before the query vertex
+    f3 suffix = make3(0.0f);   // training suffix radiance, throughput restarted at the query vertex
+    bool in_suffix = false;
+    float scatter_pdf = 1e16f;
+    float eta_scale = 1.0f;
+    CacheQueryRec rec;
+    rec.l_valid = make_float4(0, 0, 0, 0);
+    bool wrote_query = false;
+    const uint32_t end_depth = p.query_depth + p.suffix_depth;
+    for (uint32_t bounce = 0; bounce <= end_depth; ++bounce) {
+        RayPre rp = precompute_ray(ro, rd);
+        Hit hit;
+        float t_hit;
+        const bool hit_any = trace_closest(s, rp, 3.402823466e+38f, hit, t_hit);
+        f3 add = make3(0.0f);
+        if (!hit_any) {
+            if (s.has_env) {
+                CSpec Le;
+                float lpdf;
+                env_eval<CN>(s, normalize((ro + rd) - ro), wl, Le, lpdf);
+                lpdf *= light_pmf<CN>(s, s.env_index);
+                float weight = scatter_pdf / (scatter_pdf + lpdf);
+                if (ip.mis_mode == 2u) weight = 1.0f;
+                else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
+                add = linear_srgb<CN>(Le * throughput * weight, wl);
+            }
+            if (in_suffix) suffix += add;
+            else ret += add;
+            break;
+        }
+        Interaction it = surface_interaction(s, hit, rd, true);
+        if (it.light != kInvalid) {
+            CSpec Le;
+            float lpdf;
+            eval_hit_light<CN>(s, it, ro, wl, Le, lpdf);
+            float weight = scatter_pdf / (scatter_pdf + lpdf);
+            if (ip.mis_mode == 2u) weight = 1.0f;
+            else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
+            add = linear_srgb<CN>(Le * throughput * weight, wl);
+            if (in_suffix) suffix += add;
+            else ret += add;
+        }
+        if (bounce == p.query_depth) {
+            encode(p, it, p.q_feat + static_cast<size_t>(pix) * 64u);
+            rec.t = spec4(throughput);
+            rec.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
+            rec.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+            rec.l_valid = make_float4(ret.x, ret.y, ret.z, 1.0f);
+            wrote_query = true;
+            if (!train) break;
+            encode(p, it, p.t_feat + static_cast<size_t>(tj) * 64u);
+            in_suffix = true;
+            throughput = CSpec::fill(1.0f);
+        }
+        if (bounce == end_depth) {
+            // Suffix end: the cache continues from here.
+            encode(p, it, p.b_feat + static_cast<size_t>(tj) * 64u);
+            CacheTrainRec tr;
+            tr.suffix_valid = make_float4(suffix.x, suffix.y, suffix.z, 1.0f);
+            tr.t = spec4(throughput);
+            tr.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
+            tr.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+            p.t_rec[tj] = tr;
+            in_suffix = false;
+            break;
+        }
+        float u_light = smp.next();
+        f2 u_surf = smp.next2();
+        LightSample<CN> ls = sample_light<CN>(s, it, u_light, u_surf, wl);
+        Ray sh = spawn_ray_to(it.pos, it.ng, ls.p_light);
+        bool occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
+        Material mat = s.materials[it.mat];
+        Bsdf<CN> bsdf = make_bsdf<CN>(s, mat, it.shading, it.ng, it.wo, wl);
+        if (bsdf.dispersive) invalidate_secondary<CN>(wl);
+        f3 wi_light = normalize(ls.p_light - it.pos);
+        BsdfEval<CN> se = bsdf.evaluate(it.wo, wi_light, nullptr);
+        BsdfSample<CN> bs = bsdf.sample(it.wo, smp);
+        CSpec Ld = CSpec::fill(0.0f);
+        float w_mis = ls.pdf / (ls.pdf + se.pdf);
+        if (ip.mis_mode == 1u) w_mis = 1.0f;
+        if (!occluded && se.valid() && ls.pdf > 0.0f) Ld = ls.L * se.f * (w_mis / ls.pdf);
+        if (ip.mis_mode != 2u) {
+            add = linear_srgb<CN>(throughput * Ld, wl);
+            if (in_suffix) suffix += add;
+            else ret += add;
+        }
+        eta_scale *= sqr(bs.eta);
+        float lum = throughput.max();
+        if (!bs.eval.valid() || lum == 0.0f) break;
+        throughput = throughput * bs.eval.throughput();
+        if (eta_scale * lum < ip.rr_threshold && bounce >= ip.min_depth) {
+            float q = fminf(0.95f, lum);
+            float rr = smp.next();
+            if (q < rr) break;
+            throughput = throughput * (1.0f / q);
+        }
+        if (throughput.all_zero()) break;
+        scatter_pdf = bs.eval.pdf;
+        Ray nr = spawn_ray(it.pos, it.ng, bs.wi);
+        ro = nr.o;
+        rd = nr.d;
+    }
+    if (!wrote_query) rec.l_valid = make_float4(ret.x, ret.y, ret.z, 0.0f);
+    p.q_rec[pix] = rec;
+    if (train && in_suffix) {
+        // The suffix ended before its last vertex: no bootstrap term.
+        CacheTrainRec tr;
+        tr.suffix_valid = make_float4(suffix.x, suffix.y, suffix.z, 0.0f);
+        tr.t = make_float4(0, 0, 0, 0);
+        tr.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
+        tr.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+        p.t_rec[tj] = tr;
+        uint4 *dst = reinterpret_cast<uint4 *>(p.b_feat + static_cast<size_t>(tj) * 64u);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) dst[c] = make_uint4(0, 0, 0, 0);
+    } else if (train && !wrote_query) {
+        // The path ended before the query vertex: an empty training sample.
+        CacheTrainRec tr;
+        tr.suffix_valid = make_float4(0, 0, 0, 0);
+        tr.t = make_float4(0, 0, 0, 0);
+        tr.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
+        tr.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+        p.t_rec[tj] = tr;
+        uint4 *a = reinterpret_cast<uint4 *>(p.t_feat + static_cast<size_t>(tj) * 64u);
+        uint4 *b = reinterpret_cast<uint4 *>(p.b_feat + static_cast<size_t>(tj) * 64u);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a[c] = b[c] = make_uint4(0, 0, 0, 0);
+    }
+}
+
+namespace {
+
+__device__ __forceinline__ CWl wl_of(float4 lambda, float4 pdf) {
+    CWl w;
+    w.lambda[0] = lambda.x;
+    w.lambda[1] = lambda.y;
+    w.lambda[2] = lambda.z;
+    w.lambda[3] = lambda.w;
+    w.pdf[0] = pdf.x;
+    w.pdf[1] = pdf.y;
+    w.pdf[2] = pdf.z;
+    w.pdf[3] = pdf.w;
+    return w;
+}
+
+__device__ __forceinline__ bool bad3(f3 v) {
+    return isnan(v.x) || isnan(v.y) || isnan(v.z) || isinf(v.x) || isinf(v.y) || isinf(v.z);
+}
+
+}  // namespace
+
+// Pixel radiance into the film (running mean of frame film_index, optional
+// FP64 sums) and the training targets.
+__global__ void k_cache_resolve(DeviceScene s, CacheFrameParams p, float4 *film32, double *film64,
+                                uint32_t film_index) {
+    const uint32_t npix = s.cam.width * s.cam.height;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < npix) {
+        CacheQueryRec r = p.q_rec[i];
+        f3 L = make3(r.l_valid.x, r.l_valid.y, r.l_valid.z);
+        if (r.l_valid.w != 0.0f) {
+            CWl wl = wl_of(r.lambda, r.pdf);
+            CSpec c = cache_spectrum(s, p.q_out[i], wl);
+            L += linear_srgb<CN>(spec_of(r.t) * c, wl);
+        }
+        if (bad3(L)) L = make3(0.0f);
+        float4 acc = film_index == 0 ? make_float4(0, 0, 0, 0) : film32[i];
+        float a = 1.0f / static_cast<float>(film_index + 1u);
+        acc.x = acc.x + a * (L.x - acc.x);
+        acc.y = acc.y + a * (L.y - acc.y);
+        acc.z = acc.z + a * (L.z - acc.z);
+        acc.w = acc.w + a * (1.0f - acc.w);
+        film32[i] = acc;
+        if (film64) {
+            double4 d = film_index == 0 ? make_double4(0, 0, 0, 0) : reinterpret_cast<double4 *>(film64)[i];
+            d.x += L.x;
+            d.y += L.y;
+            d.z += L.z;
+            d.w += 1.0;
+            reinterpret_cast<double4 *>(film64)[i] = d;
+        }
+    }
+    if (i < p.n_train) {
+        CacheTrainRec r = p.t_rec[i];
+        f3 T = make3(r.suffix_valid.x, r.suffix_valid.y, r.suffix_valid.z);
+        if (r.suffix_valid.w != 0.0f) {
+            CWl wl = wl_of(r.lambda, r.pdf);
+            CSpec c = cache_spectrum(s, p.b_out[i], wl);
+            T += linear_srgb<CN>(spec_of(r.t) * c, wl);
+        }
+        if (bad3(T)) T = make3(0.0f);
+        p.targets[i] = make_float4(T.x, T.y, T.z, 0.0f);
+    }
+}
+
+cudaError_t upload_spectral_consts_cache(const float *x, const float *y, const float *z, const float *d65,
+                                         float y_integral) {
+    return upload_spectral_consts_tu(x, y, z, d65, y_integral);
+}
+
+cudaError_t launch_cache_frame(const DeviceScene &s, const CacheFrameParams &p, const MlpState &mlp, float4 *film32,
+                               double *film64, uint32_t film_index, cudaStream_t st, unsigned *launches) {
+    const uint32_t npix = s.cam.width * s.cam.height;
+    unsigned n = 0;
+    k_cache_paths<<<(npix + 127) / 128, 128, 0, st>>>(s, p);
+    ++n;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = mlp_infer(mlp, p.q_feat, npix, p.q_out, st);
+    ++n;
+    if (e == cudaSuccess && p.n_train) {
+        e = mlp_infer(mlp, p.b_feat, p.n_train, p.b_out, st);
+        ++n;
+    }
+    if (e == cudaSuccess) {
+        uint32_t m = npix > p.n_train ? npix : p.n_train;
+        k_cache_resolve<<<(m + 255) / 256, 256, 0, st>>>(s, p, film32, film64, film_index);
+        ++n;
+        e = cudaGetLastError();
+    }
+    if (launches) *launches = n;
+    return e;
+}
+
+}  // namespace vs

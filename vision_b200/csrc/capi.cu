@@ -11,6 +11,7 @@
 #include "vs_host.h"
 #include "vs_launch.h"
 #include "vs_microfacet.h"
+#include "vs_cache_render.h"
 #include "vs_mlp.h"
 #include "vs_server.h"
 
@@ -76,6 +77,18 @@ struct vs_scene {
     DevBuf<float4> film32, exposed;
     DevBuf<double> film64;
     DevBuf<float4> radiance;
+    // Cache-terminated rendering: per-pixel queries, training samples, the
+    // material albedo/roughness table of the feature encoding.
+    struct CacheBufs {
+        DevBuf<uint16_t> q_feat, t_feat, b_feat;
+        DevBuf<CacheQueryRec> q_rec;
+        DevBuf<CacheTrainRec> t_rec;
+        DevBuf<float4> q_out, b_out, targets, mat;
+        void free() {
+            q_feat.free(); t_feat.free(); b_feat.free(); q_rec.free(); t_rec.free();
+            q_out.free(); b_out.free(); targets.free(); mat.free();
+        }
+    } cachebuf;
     uint32_t film_frames = 0;
     bool film64_valid = false;
     // Optional CUDA-event timing of the megakernel and film launches.
@@ -134,6 +147,7 @@ struct vs_scene {
         env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
         film32.free(); exposed.free(); film64.free(); radiance.free();
         rt.free();
+        cachebuf.free();
     }
 
     DeviceScene device_view() const {
@@ -205,6 +219,7 @@ int upload_scene(vs_scene *s) {
         VS_CUDA(upload_spectral_consts(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_rt(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_serve(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        VS_CUDA(upload_spectral_consts_cache(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         ctx->consts_uploaded = true;
     }
     const HostScene &h = s->host;
@@ -1137,6 +1152,117 @@ int vs_cache_gradient(vs_cache *c, float *grad, size_t count, double *loss) {
     if (rc != VS_OK) return rc;
     VS_CUDA(cudaMemcpy(grad, c->st.grad, sizeof(float) * count, cudaMemcpyDeviceToHost), "cache gradient");
     VS_CUDA(cudaMemcpy(loss, c->st.loss, sizeof(double), cudaMemcpyDeviceToHost), "cache loss");
+    return VS_OK;
+}
+
+int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t frame_count, uint32_t train_samples,
+                     int film_precision, void *stream) {
+    if (!s || !c) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render_cached");
+    const HostScene &h = s->host;
+    if (h.ip.spectrum_dim != 4) return fail(ctx, VS_E_UNSUPPORTED, "cache rendering needs 4 hero wavelengths");
+    if (frame_begin != 0 && frame_begin != s->film_frames)
+        return fail(ctx, VS_E_STATE, "frames must continue the film (frame_begin == frames rendered) or restart at 0");
+    if (film_precision == VS_FILM_FP64 && frame_begin != 0 && !s->film64_valid)
+        return fail(ctx, VS_E_STATE, "FP64 film must be enabled from frame 0");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = pick_stream(s, stream);
+    int rc = ensure_film(s);
+    if (rc != VS_OK) return rc;
+    const uint32_t npix = h.cam.width * h.cam.height;
+    if (train_samples > npix) train_samples = npix;
+    if (film_precision == VS_FILM_FP64) VS_CUDA(s->film64.alloc(static_cast<size_t>(npix) * 4), "film64 alloc");
+    vs_scene::CacheBufs &b = s->cachebuf;
+    const size_t nt = train_samples ? train_samples : 1;
+    VS_CUDA(b.q_feat.alloc(static_cast<size_t>(npix) * 64), "cache alloc");
+    VS_CUDA(b.q_rec.alloc(npix), "cache alloc");
+    VS_CUDA(b.q_out.alloc(npix), "cache alloc");
+    VS_CUDA(b.t_feat.alloc(nt * 64), "cache alloc");
+    VS_CUDA(b.b_feat.alloc(nt * 64), "cache alloc");
+    VS_CUDA(b.t_rec.alloc(nt), "cache alloc");
+    VS_CUDA(b.b_out.alloc(nt), "cache alloc");
+    VS_CUDA(b.targets.alloc(nt), "cache alloc");
+    if (!b.mat.ptr) {
+        // Albedo (the colour slot's RGB) and roughness (alpha; 1 for diffuse
+        // and emitters) of every material, for the feature encoding.
+        std::vector<float4> m(h.materials.size());
+        for (size_t i = 0; i < m.size(); ++i) {
+            const Material &mt = h.materials[i];
+            f3 rgb = i < h.material_rgb.size() ? h.material_rgb[i] : make3(0.0f);
+            float rough = (mt.type == kMatDiffuse || mt.type == kMatBlackBody) ? 1.0f : mt.p[0];
+            m[i] = make_float4(rgb.x, rgb.y, rgb.z, rough);
+        }
+        VS_CUDA(b.mat.upload(m), "cache materials");
+    }
+    if (!s->rgb2spec.ptr) {
+        const float *tab = rgb2spec_table("");
+        std::vector<float> v(tab, tab + static_cast<size_t>(3) * 64 * 64 * 64 * 4);
+        VS_CUDA(s->rgb2spec.upload(v), "upload rgb2spec");
+    }
+    f3 lo = make3(3.0e38f), hi = make3(-3.0e38f);
+    for (const f3 &q : h.pos) {
+        lo = vmin(lo, q);
+        hi = vmax(hi, q);
+    }
+    CacheFrameParams p{};
+    p.bmin = lo;
+    f3 ext = hi - lo;
+    p.binv = make3(ext.x > 0 ? 1.0f / ext.x : 0.0f, ext.y > 0 ? 1.0f / ext.y : 0.0f, ext.z > 0 ? 1.0f / ext.z : 0.0f);
+    p.mat = b.mat.ptr;
+    p.q_feat = b.q_feat.ptr;
+    p.q_rec = b.q_rec.ptr;
+    p.q_out = b.q_out.ptr;
+    p.n_train = train_samples;
+    p.train_stride = train_samples ? std::max<uint32_t>(1u, npix / train_samples) : 1u;
+    p.t_feat = b.t_feat.ptr;
+    p.b_feat = b.b_feat.ptr;
+    p.t_rec = b.t_rec.ptr;
+    p.b_out = b.b_out.ptr;
+    p.targets = b.targets.ptr;
+    p.query_depth = 2;
+    p.suffix_depth = 2;
+    DeviceScene dv = s->device_view();
+    dv.rgb2spec = reinterpret_cast<const float4 *>(s->rgb2spec.ptr);
+    auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
+        cudaEvent_t e;
+        cudaError_t r = cudaEventCreate(&e);
+        if (r != cudaSuccess) return r;
+        v.push_back(e);
+        return cudaEventRecord(e, st);
+    };
+    for (uint32_t f = 0; f < frame_count; ++f) {
+        const uint32_t frame = frame_begin + f;
+        p.frame = frame;
+        // Training pixels move every frame: offset from a hash of the frame index.
+        uint32_t hsh = frame * 0x9e3779b9u;
+        hsh ^= hsh >> 16;
+        hsh *= 0x85ebca6bu;
+        hsh ^= hsh >> 13;
+        p.train_offset = train_samples ? hsh % p.train_stride : 0u;
+        if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
+        unsigned n = 0;
+        VS_CUDA(launch_cache_frame(dv, p, c->st, s->film32.ptr, film_precision == VS_FILM_FP64 ? s->film64.ptr : nullptr,
+                                   frame, st, &n),
+                "cache frame");
+        add_launches(n);
+        if (train_samples) {
+            c->adam.loss_scale = 1.0f / (3.0f * static_cast<float>(train_samples));
+            VS_CUDA(mlp_train_step(c->st, p.t_feat, p.targets, train_samples, c->adam, true, st), "cache train");
+            c->adam.step += 1;
+            add_launches(2);
+        }
+        if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
+    }
+    if (st != ctx->stream) {
+        if (!s->ev_join) VS_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "join event");
+        VS_CUDA(cudaEventRecord(s->ev_join, st), "join record");
+        VS_CUDA(cudaStreamWaitEvent(ctx->stream, s->ev_join, 0), "join wait");
+    }
+    s->film_frames = frame_begin + frame_count;
+    s->film64_valid = film_precision == VS_FILM_FP64 && (frame_begin == 0 || s->film64_valid);
     return VS_OK;
 }
 
