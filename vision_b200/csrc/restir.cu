@@ -14,7 +14,6 @@
 // wavelengths: the reference's ReSTIR code moves spectra through float3
 // (SampledSpectrum::vec3, SampledSpectrum(Float3)), which is only defined for
 // three channels.
-#define VS_OUTLINE __noinline__
 #include "vs_integrator.cuh"
 #include "vs_launch.h"
 #include "vs_restir.h"
