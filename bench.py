@@ -52,8 +52,17 @@ WORKLOADS['serving'] = dict(kind='serving', rate=50.0, jobs=10000, hbm_budget_gb
                             paths_per_batch=1 << 24, seed=21,
                             resolutions=[[256, 256], [512, 512], [1024, 1024], [1920, 1080]],
                             spp=[1, 4, 16, 64], scenes=['box_room', 'large_scene', 'many_lights_pt', 'instanced'])
+# Learned radiance cache on the box room at 1920 x 1080 (4 hero wavelengths):
+# paths end in the cache after two bounces, 65,536 training samples per frame
+# (two-bounce-longer suffixes), Adam lr 1e-3.  One step = one cached frame
+# (with its training step).  Quality: relMSE against a plain FP64-accumulated
+# render of `reference_spp` frames, and the time each method needs to reach
+# relMSE 1e-2.
+WORKLOADS['radiance_cache'] = dict(kind='radiance_cache', width=1920, height=1080, max_depth=8, dimension=4,
+                                   sampler='pcg', seed=0, train_samples=65536, lr=1e-3, warmup_frames=256,
+                                   reference_spp=1024, target_relmse=1e-2)
 DEFAULT_WORKLOAD = 'large_scene'
-DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64, 'serving': 200}
+DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64, 'serving': 200, 'radiance_cache': 64}
 
 # DRAM bytes per path of k_render measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch divided by its paths; profiles/).
@@ -287,6 +296,9 @@ def main():
     if w['kind'] == 'serving':
         run_serving(args, w, rank, world, local_rank, dist)
         return
+    if w['kind'] == 'radiance_cache':
+        run_cache(args, w, rank, world, local_rank, dist)
+        return
     ctx = vb.Context(local_rank)
     scene = vb.Scene(ctx, workload_scene(args.workload))
     t0 = time.perf_counter()
@@ -497,6 +509,137 @@ def run_restir(args, w, rank, world, local_rank, dist):
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def relmse(img, ref, eps=1e-2):
+    """Mean over pixels and channels of (img - ref)^2 / (ref^2 + eps)."""
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + eps)))
+
+
+def run_cache(args, w, rank, world, local_rank, dist):
+    """Cache-terminated rendering: throughput of the cached frames (with their
+    training steps) and time to relMSE 1e-2 against an FP64 plain reference,
+    next to the plain tracer's."""
+    import torch
+    import vision_b200 as vb
+    from vision_b200 import scenes
+    ctx = vb.Context(local_rank)
+    sc = scenes.box_room(w['width'], w['height'], max_depth=w['max_depth'], dimension=w['dimension'],
+                         sampler=w['sampler'], seed=w['seed'])
+    # The reference uses another PCG stream seed, so its samples are
+    # independent of the timed renders' (frames 0, 1, ... of seed `seed`).
+    ref_sc = scenes.box_room(w['width'], w['height'], max_depth=w['max_depth'], dimension=w['dimension'],
+                             sampler=w['sampler'], seed=w['seed'] + 7919)
+    ref_scene = vb.Scene(ctx, ref_sc).build_accel()
+    plain = vb.Scene(ctx, sc).build_accel()
+    cached = vb.Scene(ctx, sc).build_accel()
+    npix = w['width'] * w['height']
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    t0 = time.perf_counter()
+    ref_scene.render(0, w['reference_spp'], fp64=True, stream=sp)
+    ref_scene.synchronize()
+    ref_s = time.perf_counter() - t0
+    ref = ref_scene.film(vb.FILM_SUM64)[..., :3] / w['reference_spp']
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t
+
+    # Plain tracer: time and relMSE per spp.
+    plain_curve = []
+    for spp in (1, 2, 4, 8, 16, 32):
+        dt = timed(lambda: plain.render(0, spp, stream=sp))
+        plain_curve.append((spp, dt, relmse(plain.film()[..., :3], ref)))
+    # Cached: warm-up training, then timed frames (training continues).
+    cache = vb.RadianceCache(ctx, seed=1)
+    cache.set_optimizer(lr=w['lr'])
+    train_s = timed(lambda: cached.render_cached(cache, 0, w['warmup_frames'], train_samples=w['train_samples'],
+                                                 stream=sp))
+    cached_curve = []
+    for spp in (1, 2, 4, 8, 16, 32):
+        dt = timed(lambda: cached.render_cached(cache, 0, spp, train_samples=w['train_samples'], stream=sp))
+        cached_curve.append((spp, dt, relmse(cached.film()[..., :3], ref)))
+    # Throughput of the timed cached frames (CUDA events, L2 flushed between steps).
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+    for _ in range(args.warmup):
+        cached.render_cached(cache, 0, 1, train_samples=w['train_samples'], stream=sp)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    cached.timing_enable(True)
+    launches0 = vb.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record()
+        cached.render_cached(cache, i, 1, train_samples=w['train_samples'], stream=sp)
+        ends[i].record()
+    torch.cuda.synchronize()
+    launches = vb.launch_count() - launches0
+    clk = clocks.stop()
+    step_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    frame_ms, _, _ = cached.timing_read()
+    cached.timing_enable(False)
+    value = npix * args.steps / (step_ms / 1e3) / 1e6
+    # End to end through the C ABI with a host film read per step.
+    film_host = torch.empty((w['height'], w['width'], 4), dtype=torch.float32).pin_memory()
+    film_np = film_host.numpy()
+    e2e_steps = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        ctx.check(vb.lib.vs_render_cached(cached.handle, cache.handle, 0, 1, w['train_samples'], vb.FILM_FP32, None),
+                  'render_cached')
+        ctx.check(vb.lib.vs_film_download(cached.handle, vb._ptr(film_np), film_np.nbytes, vb.FILM_LINEAR), 'film')
+    e2e_value = npix * e2e_steps / (time.perf_counter() - t0) / 1e6
+
+    def time_to(curve, extra=0.0):
+        for spp, dt, r in curve:
+            if r <= w['target_relmse']:
+                return extra + dt, spp
+        return None, None
+    tp, sp_p = time_to(plain_curve)
+    tc, sp_c = time_to(cached_curve, train_s)
+    # Algorithmic flops of the network per frame: inference on every pixel's
+    # query and every suffix end, training forward + backward on the samples.
+    nt = w['train_samples']
+    flops = 33152.0 * (npix + nt) + 99456.0 * nt
+    peak_tf = 1389.6
+    try:
+        peak_tf = json.load(open(os.path.join(ROOT, 'MEASURED_PEAKS.json'))).get('bf16_tflops_sustained', peak_tf)
+    except OSError:
+        pass
+    achieved_tf = flops / (frame_ms / 1e3 / args.steps) / 1e12
+    line = {
+        'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': step_ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32 path / bf16 network', 'data': 'synthetic',
+        'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
+                   'path': 'one cache-terminated camera path per pixel per frame, training step included',
+                   'l2': 'flushed between steps (256 MiB write)', 'parallelism': 'replicas%d' % world},
+        'quality': {'reference_s': ref_s, 'target_relmse': w['target_relmse'],
+                    'plain': [{'spp': a, 's': b, 'relmse': c} for a, b, c in plain_curve],
+                    'cached': [{'spp': a, 's': b, 'relmse': c} for a, b, c in cached_curve],
+                    'cache_training_s': train_s,
+                    'time_to_target_s': {'plain': tp, 'cached': tc},
+                    'speedup': (tp / tc) if (tp and tc) else None},
+        'roofline': {'bound': 'tensor', 'achieved': achieved_tf, 'peak': peak_tf, 'unit': 'TFLOP/s',
+                     'frac': achieved_tf / peak_tf, 'peak_source': 'measured', 'traffic': None,
+                     'kernel': 'radiance-cache frame (network share of the frame time)',
+                     'flops_per_frame': flops, 'frame_ms': frame_ms / args.steps},
+        'clocks': clk,
+        'e2e': {'value': e2e_value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 0,
+                'd2h_bytes_per_step': int(film_np.nbytes)},
+        'gpu_launches': int(launches),
+    }
+    if rank == 0:
+        print(json.dumps(line))
 
 
 def serving_scenes():

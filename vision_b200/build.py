@@ -3,9 +3,12 @@
 usage: python vision_b200/build.py [--force] [-v]
 
 Objects go to vision_b200/_build/; the shared library lands next to this file
-so that it travels with the package.  Rebuilds only when a source or header is
-newer than the library.
+so that it travels with the package.  Each object and the library carry a
+digest of their sources, headers and flags (`.stamp` files); only objects
+whose digest changed are recompiled, in parallel.
 """
+import concurrent.futures
+import hashlib
 import os
 import subprocess
 import sys
@@ -29,36 +32,71 @@ def nvcc():
     return 'nvcc'
 
 
-def _newest_input():
-    t = 0.0
+def _digest(paths, extra):
+    h = hashlib.sha256()
+    for p in paths:
+        h.update(p.encode())
+        with open(p, 'rb') as f:
+            h.update(f.read())
+    h.update(' '.join(extra).encode())
+    return h.hexdigest()
+
+
+def _headers():
+    hs = [os.path.join(INCLUDE, 'vision_b200.h')]
     for root, _, files in os.walk(CSRC):
-        for f in files:
-            t = max(t, os.path.getmtime(os.path.join(root, f)))
-    t = max(t, os.path.getmtime(os.path.join(INCLUDE, 'vision_b200.h')))
-    return t
+        for f in sorted(files):
+            if not f.endswith(('.cu', '.cpp')):
+                hs.append(os.path.join(root, f))
+    return sorted(hs)
+
+
+def _source_digest(src):
+    return _digest([os.path.join(CSRC, src)] + _headers(), ARCH + COMMON)
+
+
+def _library_digest():
+    return _digest([os.path.join(CSRC, s) for s in SOURCES] + _headers(), ARCH + COMMON + SOURCES)
+
+
+def _stamp_ok(path, digest):
+    stamp = path + '.stamp'
+    return os.path.exists(path) and os.path.exists(stamp) and open(stamp).read().strip() == digest
 
 
 def up_to_date():
-    return os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest_input()
+    """True when the library was built from exactly the current sources and
+    flags (content digest, so copies with fresh file times stay valid)."""
+    return _stamp_ok(LIB, _library_digest())
 
 
 def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
-    for src in SOURCES:
+
+    def compile_one(src):
         obj = os.path.join(BUILD, os.path.splitext(src)[0] + '.o')
+        digest = _source_digest(src)
+        if not force and _stamp_ok(obj, digest):
+            return obj
         cmd = [nvcc()] + ARCH + COMMON + ['-c', os.path.join(CSRC, src), '-o', obj]
-        if src.endswith('.cu'):
-            cmd += ['-Xptxas', '-v'] if verbose else []
+        if src.endswith('.cu') and verbose:
+            cmd += ['-Xptxas', '-v']
         if verbose:
             print(' '.join(cmd))
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+        with open(obj + '.stamp', 'w') as f:
+            f.write(digest)
+        return obj
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
     tmp = LIB + '.tmp'
     subprocess.run([nvcc()] + ARCH + ['-shared', '-o', tmp] + objs + ['-lcudart', '-lpthread'], check=True)
     os.replace(tmp, LIB)
+    with open(LIB + '.stamp', 'w') as f:
+        f.write(_library_digest())
     return LIB
 
 
