@@ -52,13 +52,14 @@ WORKLOADS['serving'] = dict(kind='serving', rate=50.0, jobs=10000, hbm_budget_gb
                             paths_per_batch=1 << 24, seed=21,
                             resolutions=[[256, 256], [512, 512], [1024, 1024], [1920, 1080]],
                             spp=[1, 4, 16, 64], scenes=['box_room', 'large_scene', 'many_lights_pt', 'instanced'])
-# Learned radiance cache on the box room at 1920 x 1080 (4 hero wavelengths):
-# paths end in the cache after two bounces, 65,536 training samples per frame
+# Learned radiance cache on the box room at 1920 x 1080 (3 hero wavelengths,
+# the cache's 3 spectral outputs): paths end in the cache after two bounces,
+# 65,536 training samples per frame
 # (two-bounce-longer suffixes), Adam lr 1e-3.  One step = one cached frame
 # (with its training step).  Quality: relMSE against a plain FP64-accumulated
 # render of `reference_spp` frames, and the time each method needs to reach
 # relMSE 1e-2.
-WORKLOADS['radiance_cache'] = dict(kind='radiance_cache', width=1920, height=1080, max_depth=8, dimension=4,
+WORKLOADS['radiance_cache'] = dict(kind='radiance_cache', width=1920, height=1080, max_depth=8, dimension=3,
                                    sampler='pcg', seed=0, train_samples=65536, lr=1e-3, warmup_frames=256,
                                    reference_spp=1024, target_relmse=1e-2)
 DEFAULT_WORKLOAD = 'large_scene'

@@ -291,10 +291,12 @@ int vs_cache_gradient(vs_cache *cache, float *grad, size_t count, double *loss);
 /* vs_render with paths that stop after two bounces into the radiance cache:
  * each pixel's path adds its emission and next-event estimates for two
  * bounces, then the cache's prediction at the third vertex times the path
- * throughput.  With train_samples > 0, that many paths per frame (a strided
- * pixel subset moving every frame) continue two bounces further and the
- * cache takes one Adam step per frame on their suffix radiance plus the
- * cache at the suffix end.  Scenes must use 4 hero wavelengths. */
+ * throughput.  The cache's three outputs are the spectral radiance at the
+ * path's three hero wavelengths (the hero wavelength is one of its inputs),
+ * so scenes must use 3 hero wavelengths.  With train_samples > 0, that many
+ * paths per frame (a strided pixel subset moving every frame) continue two
+ * bounces further and the cache takes one Adam step per frame on their
+ * suffix radiance plus the cache at the suffix end. */
 int vs_render_cached(vs_scene *scene, vs_cache *cache, uint32_t frame_begin, uint32_t frame_count,
                      uint32_t train_samples, int film_precision, void *stream);
 

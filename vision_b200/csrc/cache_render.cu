@@ -13,15 +13,19 @@
 //                    the suffix end.
 //   mlp_infer        the cache at every query vertex and every suffix end
 //   k_cache_resolve  pixel radiance = gathered radiance + throughput times the
-//                    cache's radiance (RGB decoded as an illumination
-//                    spectrum at the path's wavelengths) into the film;
-//                    training target = suffix radiance + suffix throughput
-//                    times the cache at the suffix end (self-training).
-// The cache predicts the radiance leaving a vertex toward the previous one,
-// without the vertex's own emission (which the path adds with its MIS weight).
+//                    cache's radiance at the path's three hero wavelengths
+//                    into the film; training target = suffix radiance +
+//                    suffix throughput times the cache at the suffix end
+//                    (self-training), per wavelength.
+// The cache predicts spectral radiance at the path's three hero wavelengths
+// (its three outputs), leaving a vertex toward the previous one, without the
+// vertex's own emission (which the path adds with its MIS weight): the path
+// multiplies it by its own spectral throughput, so no RGB round trip enters
+// the estimate.
 // Features (64): position in the scene bounds, sin/cos(2^k pi p) for k = 0..7
 // on each axis (48); outgoing direction (3); shading normal (3); roughness (1);
-// albedo (3); sin/cos(pi w) of the outgoing direction (6).
+// albedo (3); sin/cos(2^k pi u) of the hero wavelength u = (lambda_0 - 360) /
+// 470 for k = 0..2 (6).
 #include "vs_cache_render.h"
 #include "vs_integrator.cuh"
 #include "vs_launch.h"
@@ -32,7 +36,7 @@ namespace vs {
 
 namespace {
 
-constexpr int CN = 4;  // hero wavelengths of cache-rendered scenes
+constexpr int CN = 3;  // hero wavelengths of cache-rendered scenes = cache outputs
 using CSpec = Spec<CN>;
 using CWl = Wavelengths<CN>;
 
@@ -41,7 +45,7 @@ __device__ __forceinline__ uint32_t bf2(float a, float b) {
     return *reinterpret_cast<uint32_t *>(&h);
 }
 
-__device__ void encode(const CacheFrameParams &p, const Interaction &it, uint16_t *out) {
+__device__ void encode(const CacheFrameParams &p, const Interaction &it, float lambda0, uint16_t *out) {
     float f[64];
     const float pos[3] = {clampf((it.pos.x - p.bmin.x) * p.binv.x, 0.0f, 1.0f),
                           clampf((it.pos.y - p.bmin.y) * p.binv.y, 0.0f, 1.0f),
@@ -71,8 +75,10 @@ __device__ void encode(const CacheFrameParams &p, const Interaction &it, uint16_
     f[55] = m.x;
     f[56] = m.y;
     f[57] = m.z;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) sincospif(wo[a], &f[58 + 2 * a], &f[59 + 2 * a]);
+    const float u = (lambda0 - 360.0f) * (1.0f / 470.0f);
+    sincospif(u, &f[58], &f[59]);
+    sincospif(2.0f * u, &f[60], &f[61]);
+    sincospif(4.0f * u, &f[62], &f[63]);
     uint4 *dst = reinterpret_cast<uint4 *>(out);
 #pragma unroll
     for (int c = 0; c < 8; ++c)
@@ -80,26 +86,25 @@ __device__ void encode(const CacheFrameParams &p, const Interaction &it, uint16_
                             bf2(f[8 * c + 4], f[8 * c + 5]), bf2(f[8 * c + 6], f[8 * c + 7]));
 }
 
-__device__ __forceinline__ float4 spec4(const CSpec &s) { return make_float4(s.v[0], s.v[1], s.v[2], s.v[3]); }
+__device__ __forceinline__ float4 spec4(const CSpec &s, float w) { return make_float4(s.v[0], s.v[1], s.v[2], w); }
 __device__ __forceinline__ CSpec spec_of(float4 v) {
     CSpec s;
     s.v[0] = v.x;
     s.v[1] = v.y;
     s.v[2] = v.z;
-    s.v[3] = v.w;
     return s;
 }
-
-// Radiance of an RGB cache output at the path's wavelengths: the RGB decoded
-// as an illumination spectrum (sigmoid polynomial x scale x D65), as the
-// reference decodes RGB emission (hero.cpp:204-219).
-__device__ __forceinline__ CSpec cache_spectrum(const DeviceScene &s, float4 rgb, const CWl &wl) {
-    float c[4];
-    rgb2spec_unbound(s.rgb2spec, make3(fmaxf(rgb.x, 0.0f), fmaxf(rgb.y, 0.0f), fmaxf(rgb.z, 0.0f)), c);
-    CSpec r;
-#pragma unroll
-    for (int i = 0; i < CN; ++i) r.v[i] = sigmoid_poly(c[0], c[1], c[2], wl.lambda[i]) * c[3] * cie_spd(c_spec.d65, wl.lambda[i]);
-    return r;
+// Cache output: spectral radiance at the three hero wavelengths (negative
+// predictions clamped to zero).
+__device__ __forceinline__ CSpec cache_radiance(float4 o) {
+    CSpec s;
+    s.v[0] = fmaxf(o.x, 0.0f);
+    s.v[1] = fmaxf(o.y, 0.0f);
+    s.v[2] = fmaxf(o.z, 0.0f);
+    return s;
+}
+__device__ __forceinline__ float4 wl4(const CWl &w, bool pdf) {
+    return pdf ? make_float4(w.pdf[0], w.pdf[1], w.pdf[2], 0.0f) : make_float4(w.lambda[0], w.lambda[1], w.lambda[2], 0.0f);
 }
 
 }  // namespace
@@ -126,8 +131,9 @@ __global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFramePa
     camera_ray(s.cam, smp, px, py, p_film, ro, rd);
 
     CSpec throughput = CSpec::fill(1.0f);
-    f3 ret = make3(0.0f);      // radiance before the query vertex
-    f3 suffix = make3(0.0f);   // training suffix radiance, throughput restarted at the query vertex
+    f3 ret = make3(0.0f);               // radiance before the query vertex (linear sRGB)
+    CSpec suffix = CSpec::fill(0.0f);   // training suffix radiance at the hero wavelengths,
+                                        // throughput restarted at the query vertex
     bool in_suffix = false;
     float scatter_pdf = 1e16f;
     float eta_scale = 1.0f;
@@ -135,12 +141,17 @@ __global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFramePa
     rec.l_valid = make_float4(0, 0, 0, 0);
     bool wrote_query = false;
     const uint32_t end_depth = p.query_depth + p.suffix_depth;
+    // Adds a spectral contribution (already weighted by the throughput) to the
+    // pixel radiance or, inside a training suffix, to the suffix radiance.
+    auto gather = [&](const CSpec &c) {
+        if (in_suffix) suffix = suffix + c;
+        else ret += linear_srgb<CN>(c, wl);
+    };
     for (uint32_t bounce = 0; bounce <= end_depth; ++bounce) {
         RayPre rp = precompute_ray(ro, rd);
         Hit hit;
         float t_hit;
         const bool hit_any = trace_closest(s, rp, 3.402823466e+38f, hit, t_hit);
-        f3 add = make3(0.0f);
         if (!hit_any) {
             if (s.has_env) {
                 CSpec Le;
@@ -150,10 +161,8 @@ __global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFramePa
                 float weight = scatter_pdf / (scatter_pdf + lpdf);
                 if (ip.mis_mode == 2u) weight = 1.0f;
                 else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
-                add = linear_srgb<CN>(Le * throughput * weight, wl);
+                gather(Le * throughput * weight);
             }
-            if (in_suffix) suffix += add;
-            else ret += add;
             break;
         }
         Interaction it = surface_interaction(s, hit, rd, true);
@@ -164,30 +173,28 @@ __global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFramePa
             float weight = scatter_pdf / (scatter_pdf + lpdf);
             if (ip.mis_mode == 2u) weight = 1.0f;
             else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
-            add = linear_srgb<CN>(Le * throughput * weight, wl);
-            if (in_suffix) suffix += add;
-            else ret += add;
+            gather(Le * throughput * weight);
         }
         if (bounce == p.query_depth) {
-            encode(p, it, p.q_feat + static_cast<size_t>(pix) * 64u);
-            rec.t = spec4(throughput);
-            rec.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
-            rec.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+            encode(p, it, wl.lambda[0], p.q_feat + static_cast<size_t>(pix) * 64u);
+            rec.t = spec4(throughput, 0.0f);
+            rec.lambda = wl4(wl, false);
+            rec.pdf = wl4(wl, true);
             rec.l_valid = make_float4(ret.x, ret.y, ret.z, 1.0f);
             wrote_query = true;
             if (!train) break;
-            encode(p, it, p.t_feat + static_cast<size_t>(tj) * 64u);
+            encode(p, it, wl.lambda[0], p.t_feat + static_cast<size_t>(tj) * 64u);
             in_suffix = true;
             throughput = CSpec::fill(1.0f);
         }
         if (bounce == end_depth) {
             // Suffix end: the cache continues from here.
-            encode(p, it, p.b_feat + static_cast<size_t>(tj) * 64u);
+            encode(p, it, wl.lambda[0], p.b_feat + static_cast<size_t>(tj) * 64u);
             CacheTrainRec tr;
-            tr.suffix_valid = make_float4(suffix.x, suffix.y, suffix.z, 1.0f);
-            tr.t = spec4(throughput);
-            tr.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
-            tr.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+            tr.suffix_valid = spec4(suffix, 1.0f);
+            tr.t = spec4(throughput, 0.0f);
+            tr.lambda = wl4(wl, false);
+            tr.pdf = wl4(wl, true);
             p.t_rec[tj] = tr;
             in_suffix = false;
             break;
@@ -207,11 +214,7 @@ __global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFramePa
         float w_mis = ls.pdf / (ls.pdf + se.pdf);
         if (ip.mis_mode == 1u) w_mis = 1.0f;
         if (!occluded && se.valid() && ls.pdf > 0.0f) Ld = ls.L * se.f * (w_mis / ls.pdf);
-        if (ip.mis_mode != 2u) {
-            add = linear_srgb<CN>(throughput * Ld, wl);
-            if (in_suffix) suffix += add;
-            else ret += add;
-        }
+        if (ip.mis_mode != 2u) gather(throughput * Ld);
         eta_scale *= sqr(bs.eta);
         float lum = throughput.max();
         if (!bs.eval.valid() || lum == 0.0f) break;
@@ -230,29 +233,22 @@ __global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFramePa
     }
     if (!wrote_query) rec.l_valid = make_float4(ret.x, ret.y, ret.z, 0.0f);
     p.q_rec[pix] = rec;
-    if (train && in_suffix) {
-        // The suffix ended before its last vertex: no bootstrap term.
+    if (train && (in_suffix || !wrote_query)) {
+        // The suffix ended before its last vertex (no bootstrap term), or the
+        // path before the query vertex (an empty sample with zero features).
         CacheTrainRec tr;
-        tr.suffix_valid = make_float4(suffix.x, suffix.y, suffix.z, 0.0f);
+        tr.suffix_valid = spec4(suffix, 0.0f);
         tr.t = make_float4(0, 0, 0, 0);
-        tr.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
-        tr.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+        tr.lambda = wl4(wl, false);
+        tr.pdf = wl4(wl, true);
         p.t_rec[tj] = tr;
-        uint4 *dst = reinterpret_cast<uint4 *>(p.b_feat + static_cast<size_t>(tj) * 64u);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) dst[c] = make_uint4(0, 0, 0, 0);
-    } else if (train && !wrote_query) {
-        // The path ended before the query vertex: an empty training sample.
-        CacheTrainRec tr;
-        tr.suffix_valid = make_float4(0, 0, 0, 0);
-        tr.t = make_float4(0, 0, 0, 0);
-        tr.lambda = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
-        tr.pdf = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
-        p.t_rec[tj] = tr;
-        uint4 *a = reinterpret_cast<uint4 *>(p.t_feat + static_cast<size_t>(tj) * 64u);
         uint4 *b = reinterpret_cast<uint4 *>(p.b_feat + static_cast<size_t>(tj) * 64u);
+        uint4 *a = reinterpret_cast<uint4 *>(p.t_feat + static_cast<size_t>(tj) * 64u);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) a[c] = b[c] = make_uint4(0, 0, 0, 0);
+        for (int c = 0; c < 8; ++c) {
+            b[c] = make_uint4(0, 0, 0, 0);
+            if (!wrote_query) a[c] = make_uint4(0, 0, 0, 0);
+        }
     }
 }
 
@@ -263,11 +259,9 @@ __device__ __forceinline__ CWl wl_of(float4 lambda, float4 pdf) {
     w.lambda[0] = lambda.x;
     w.lambda[1] = lambda.y;
     w.lambda[2] = lambda.z;
-    w.lambda[3] = lambda.w;
     w.pdf[0] = pdf.x;
     w.pdf[1] = pdf.y;
     w.pdf[2] = pdf.z;
-    w.pdf[3] = pdf.w;
     return w;
 }
 
@@ -288,8 +282,7 @@ __global__ void k_cache_resolve(DeviceScene s, CacheFrameParams p, float4 *film3
         f3 L = make3(r.l_valid.x, r.l_valid.y, r.l_valid.z);
         if (r.l_valid.w != 0.0f) {
             CWl wl = wl_of(r.lambda, r.pdf);
-            CSpec c = cache_spectrum(s, p.q_out[i], wl);
-            L += linear_srgb<CN>(spec_of(r.t) * c, wl);
+            L += linear_srgb<CN>(spec_of(r.t) * cache_radiance(p.q_out[i]), wl);
         }
         if (bad3(L)) L = make3(0.0f);
         float4 acc = film_index == 0 ? make_float4(0, 0, 0, 0) : film32[i];
@@ -310,14 +303,11 @@ __global__ void k_cache_resolve(DeviceScene s, CacheFrameParams p, float4 *film3
     }
     if (i < p.n_train) {
         CacheTrainRec r = p.t_rec[i];
-        f3 T = make3(r.suffix_valid.x, r.suffix_valid.y, r.suffix_valid.z);
-        if (r.suffix_valid.w != 0.0f) {
-            CWl wl = wl_of(r.lambda, r.pdf);
-            CSpec c = cache_spectrum(s, p.b_out[i], wl);
-            T += linear_srgb<CN>(spec_of(r.t) * c, wl);
-        }
-        if (bad3(T)) T = make3(0.0f);
-        p.targets[i] = make_float4(T.x, T.y, T.z, 0.0f);
+        CSpec T = spec_of(r.suffix_valid);
+        if (r.suffix_valid.w != 0.0f) T = T + spec_of(r.t) * cache_radiance(p.b_out[i]);
+        f3 v = make3(T.v[0], T.v[1], T.v[2]);
+        if (bad3(v)) v = make3(0.0f);
+        p.targets[i] = make_float4(v.x, v.y, v.z, 0.0f);
     }
 }
 

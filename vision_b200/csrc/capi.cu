@@ -1163,7 +1163,8 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     std::lock_guard<std::mutex> lock(s->mu);
     if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render_cached");
     const HostScene &h = s->host;
-    if (h.ip.spectrum_dim != 4) return fail(ctx, VS_E_UNSUPPORTED, "cache rendering needs 4 hero wavelengths");
+    if (h.ip.spectrum_dim != 3)
+        return fail(ctx, VS_E_UNSUPPORTED, "cache rendering needs 3 hero wavelengths (the cache's 3 outputs)");
     if (frame_begin != 0 && frame_begin != s->film_frames)
         return fail(ctx, VS_E_STATE, "frames must continue the film (frame_begin == frames rendered) or restart at 0");
     if (film_precision == VS_FILM_FP64 && frame_begin != 0 && !s->film64_valid)
@@ -1197,11 +1198,6 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
         }
         VS_CUDA(b.mat.upload(m), "cache materials");
     }
-    if (!s->rgb2spec.ptr) {
-        const float *tab = rgb2spec_table("");
-        std::vector<float> v(tab, tab + static_cast<size_t>(3) * 64 * 64 * 64 * 4);
-        VS_CUDA(s->rgb2spec.upload(v), "upload rgb2spec");
-    }
     f3 lo = make3(3.0e38f), hi = make3(-3.0e38f);
     for (const f3 &q : h.pos) {
         lo = vmin(lo, q);
@@ -1225,7 +1221,6 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     p.query_depth = 2;
     p.suffix_depth = 2;
     DeviceScene dv = s->device_view();
-    dv.rgb2spec = reinterpret_cast<const float4 *>(s->rgb2spec.ptr);
     auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
         cudaEvent_t e;
         cudaError_t r = cudaEventCreate(&e);

@@ -12,15 +12,16 @@
 
 namespace vs {
 
-// Per-pixel path state at the query vertex: throughput (4), wavelengths (4),
-// wavelength pdfs (4), radiance gathered before the query (3) and a validity
-// flag (w of the last float4).
+// Per-pixel path state at the query vertex: throughput (3 hero wavelengths),
+// wavelengths, wavelength pdfs, radiance gathered before the query (rgb) and
+// a validity flag (w of the last float4).
 struct CacheQueryRec {
     float4 t, lambda, pdf, l_valid;
 };
 
-// Per training sample: suffix radiance (rgb) and bootstrap flag, throughput
-// from the query vertex to the suffix end (4), wavelengths and pdfs.
+// Per training sample: suffix radiance at the 3 hero wavelengths and the
+// bootstrap flag, throughput from the query vertex to the suffix end,
+// wavelengths and pdfs.
 struct CacheTrainRec {
     float4 suffix_valid, t, lambda, pdf;
 };
