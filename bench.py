@@ -268,6 +268,8 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--schedule', default='persistent', choices=['persistent', 'grid'],
+                    help='path scheduling of the megakernel (both give the same film)')
     ap.add_argument('--spp', type=int, default=None,
                     help='override the workload spp (profiling runs on a smaller launch; reported in config)')
     args = ap.parse_args()
@@ -305,6 +307,7 @@ def main():
     t0 = time.perf_counter()
     scene.build_accel()
     build_s = time.perf_counter() - t0
+    scene.set_schedule(args.schedule)
     info = scene.info()
     spp = w['spp']
     npix = w['width'] * w['height']
@@ -380,13 +383,14 @@ def main():
         'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
                    'prims': info['prim_count'], 'bvh_nodes': info['bvh_node_count'],
                    'paths_per_step': paths_per_step, 'l2': 'flushed between steps (256 MiB write)',
-                   'parallelism': 'replicas%d' % world, 'scene_build_s': round(build_s, 3)},
+                   'parallelism': 'replicas%d' % world, 'scene_build_s': round(build_s, 3),
+                   'schedule': args.schedule},
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                      'peak_source': peak_src,
                      'traffic': (NCU_TRAFFIC_PER_PATH[args.workload] * paths_per_step * args.steps /
                                  max(render_launches, 1) if args.workload in NCU_TRAFFIC_PER_PATH else None),
                      'traffic_source': 'ncu dram bytes per path of the committed profile x paths per launch',
-                     'kernel': 'k_render',
+                     'kernel': 'k_render_regen' if args.schedule == 'persistent' else 'k_render',
                      'bytes_per_path': bytes_per_path,
                      'per_path': {'segments': segs / paths_per_step, 'nodes': nodes / paths_per_step,
                                   'tris': tris / paths_per_step},

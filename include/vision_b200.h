@@ -140,6 +140,15 @@ int vs_scene_export(const vs_scene *scene, int what, void *dst, size_t bytes);
  * `stream` is a cudaStream_t or NULL for the context's stream. Asynchronous. */
 int vs_render(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, int film_precision, void *stream);
 
+/* How vs_render schedules camera paths on the GPU.  Both give the same film
+ * bit for bit.  VS_SCHEDULE_GRID: one path per thread over a grid that covers
+ * all paths of a launch.  VS_SCHEDULE_PERSISTENT (the default): one resident
+ * wave of warps that keep 32 paths in flight each and refill the lanes of
+ * finished paths after every bounce (path regeneration). */
+#define VS_SCHEDULE_GRID 0
+#define VS_SCHEDULE_PERSISTENT 1
+int vs_render_schedule_set(vs_scene *scene, int schedule);
+
 /* Waits for all work queued on the scene's stream. */
 int vs_synchronize(vs_scene *scene);
 
@@ -299,6 +308,19 @@ int vs_cache_gradient(vs_cache *cache, float *grad, size_t count, double *loss);
  * suffix radiance plus the cache at the suffix end. */
 int vs_render_cached(vs_scene *scene, vs_cache *cache, uint32_t frame_begin, uint32_t frame_count,
                      uint32_t train_samples, int film_precision, void *stream);
+
+/* Copies a buffer of the last vs_render_cached frame to host memory: the
+ * per-pixel query vertices and the training samples of that frame. */
+#define VS_CACHE_QUERY_FEATURES 0   /* npix x 64 BF16: features of the query vertices */
+#define VS_CACHE_QUERY_RECORDS 1    /* npix x 64 bytes: throughput, wavelengths, pdfs, gathered rgb + valid */
+#define VS_CACHE_QUERY_OUTPUT 2     /* npix float4: cache output at the query vertices */
+#define VS_CACHE_TRAIN_FEATURES 3   /* n_train x 64 BF16: features of the training vertices */
+#define VS_CACHE_TRAIN_RECORDS 4    /* n_train x 64 bytes: suffix radiance + bootstrap flag, suffix throughput,
+                                       wavelengths, pdfs */
+#define VS_CACHE_SUFFIX_FEATURES 5  /* n_train x 64 BF16: features of the suffix ends */
+#define VS_CACHE_SUFFIX_OUTPUT 6    /* n_train float4: cache output at the suffix ends */
+#define VS_CACHE_TARGETS 7          /* n_train float4: training targets */
+int vs_cache_download(vs_scene *scene, int which, void *dst, size_t bytes);
 
 /* Albedo tables of the energy-compensated lobes (164864 floats: PureReflection
  * 32^2, Dielectric and DielectricInv 32^3 x 2, Specular 32^3).  which = 0: the

@@ -200,14 +200,14 @@ struct Sampler {
         if (kind == 0) {
             lcg = s;
         } else {
-            // PCG32 (O'Neill): state advanced from 0, plus the hash, advanced again;
-            // 48-bit state with the seed as stream selector.
+            // PCG32 (O'Neill 2014) seeding as pcg32_srandom_r: state 0, one
+            // step, add the TEA hash, one more step; stream = seed.
             pcg_inc = (static_cast<uint64_t>(seed) << 1u) | 1u;
             uint64_t st = 0u;
             st = st * 6364136223846793005ull + pcg_inc;
             st += s;
             st = st * 6364136223846793005ull + pcg_inc;
-            pcg_state = st & 0xffffffffffffull;
+            pcg_state = st;
         }
     }
     float next() {
@@ -215,8 +215,9 @@ struct Sampler {
             lcg = 1664525u * lcg + 1013904223u;
             return static_cast<float>(lcg & 0x00ffffffu) * (1.0f / 16777216.0f);
         }
+        // 64-bit LCG step, XSH-RR output (pcg32_random_r), top 24 bits.
         uint64_t old = pcg_state;
-        pcg_state = (old * 6364136223846793005ull + pcg_inc) & 0xffffffffffffull;
+        pcg_state = old * 6364136223846793005ull + pcg_inc;
         uint32_t xs = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
         uint32_t rot = static_cast<uint32_t>(old >> 59u);
         uint32_t r = (xs >> rot) | (xs << ((32u - rot) & 31u));

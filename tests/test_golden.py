@@ -22,6 +22,46 @@ def test_tea_and_lcg_streams():
         assert np.array_equal(s, np.array(c['stream'], np.float32))
 
 
+_PCG_MULT = 6364136223846793005
+_U64 = (1 << 64) - 1
+
+
+def _pcg32_seed(initstate, initseq):
+    inc = ((initseq << 1) | 1) & _U64
+    state = (inc + initstate) & _U64
+    return (state * _PCG_MULT + inc) & _U64, inc
+
+
+def _pcg32_next(state, inc):
+    xorshifted = (((state >> 18) ^ state) >> 27) & 0xffffffff
+    rot = state >> 59
+    out = ((xorshifted >> rot) | (xorshifted << ((-rot) & 31))) & 0xffffffff
+    return (state * _PCG_MULT + inc) & _U64, out
+
+
+def test_pcg32_known_answer_and_oracle_stream():
+    # PCG32 (O'Neill 2014, pcg32_srandom_r / pcg32_random_r): the published
+    # demo sequence for initstate 42, initseq 54 pins the restatement above.
+    state, inc = _pcg32_seed(42, 54)
+    outs = []
+    for _ in range(6):
+        state, r = _pcg32_next(state, inc)
+        outs.append(r)
+    assert outs == [0xa15c02b7, 0x7b47f409, 0xba1d3330, 0x83d2f293, 0xbfa4784b, 0xcbed606e]
+    # The sampler's PCG option: initstate = the TEA seed of (pixel, sample,
+    # dim), initseq = the scene seed, float = top 24 output bits / 2^24.  The
+    # draws must cover [0, 1) (a truncated state would confine them).
+    for px, py, sample, dim, seed in [(0, 0, 0, 0, 0), (17, 3, 5, 0, 1), (1023, 767, 63, 0xffffffff, 7)]:
+        got = oracle.sampler_stream(px, py, sample, dim, 4096, kind=1, seed=seed)
+        state, inc = _pcg32_seed(oracle.tea(oracle.tea(px, py), oracle.tea(sample, dim)), seed)
+        want = []
+        for _ in range(4096):
+            state, r = _pcg32_next(state, inc)
+            want.append((r >> 8) / 16777216.0)
+        assert np.array_equal(got, np.array(want, np.float32))
+        assert got.min() < 0.01 and got.max() > 0.99 and abs(got.mean() - 0.5) < 0.02
+
+
 def test_cie_y_integral():
     g = load('cie_5nm.json')
     assert oracle.cie_y_integral() == np.float32(g['y_integral'])

@@ -127,3 +127,34 @@ def test_large_scene_closest_hit_bit_exact(vb, gpu_ctx):
     h_cpu, t_cpu = o.trace_closest(rays)
     assert np.array_equal(h_gpu, h_cpu)
     assert np.array_equal(t_gpu.view(np.uint32), t_cpu.view(np.uint32))
+
+
+@pytest.mark.parametrize('case', ['box_room', 'materials', 'environment', 'dimension1'])
+def test_persistent_schedule_equals_grid(vb, gpu_ctx, case):
+    # Path regeneration only changes which thread traces which path: each path
+    # keeps its own sampler stream and output slot, so the films are identical.
+    if case == 'box_room':
+        sc = scenes.box_room(width=67, height=45)
+    elif case == 'materials':
+        sc = scenes.material_room(40, 36)
+    elif case == 'environment':
+        sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
+    else:
+        sc = scenes.box_room(width=33, height=31, dimension=1)
+    films = {}
+    for schedule in ('grid', 'persistent'):
+        s = vb.Scene(gpu_ctx, sc).build_accel()
+        s.set_schedule(schedule)
+        s.render(0, 5, fp64=True)
+        s.render(5, 4, fp64=True)
+        films[schedule] = (s.film(), s.film(vb.FILM_SUM64))
+    assert np.array_equal(films['grid'][0], films['persistent'][0])
+    assert np.array_equal(films['grid'][1], films['persistent'][1])
+    assert np.all(films['persistent'][1][..., 3] == 9.0)
+
+
+def test_schedule_rejects_unknown(vb, gpu_ctx):
+    s = vb.Scene(gpu_ctx, scenes.box_room(width=8, height=8)).build_accel()
+    assert vb.lib.vs_render_schedule_set(s.handle, 7) == vb.VS_E_INVALID
+    with pytest.raises(KeyError):
+        s.set_schedule('wavefront')

@@ -104,6 +104,8 @@ def _load():
         'vs_timing_enable': ([P, ctypes.c_int], ctypes.c_int),
         'vs_timing_read': ([P, P, P, P], ctypes.c_int),
         'vs_render_noalloc': ([P, U32, U32, P, P], ctypes.c_int),
+        'vs_render_schedule_set': ([P, ctypes.c_int], ctypes.c_int),
+        'vs_cache_download': ([P, ctypes.c_int, P, ctypes.c_size_t], ctypes.c_int),
         'vs_albedo_luts': ([ctypes.c_int, ctypes.c_char_p, P, ctypes.c_size_t], ctypes.c_int),
         'vs_restir_frame': ([P, U32, U32, P], ctypes.c_int),
         'vs_restir_reset': ([P], ctypes.c_int),
@@ -147,8 +149,18 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_server_destroy', 'vs_server_add_scene', 'vs_server_submit', 'vs_server_poll',
                       'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error', 'vs_cache_create',
                       'vs_cache_destroy', 'vs_cache_get_weights', 'vs_cache_set_weights', 'vs_cache_set_optimizer',
-                      'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient', 'vs_render_cached'])
+                      'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient', 'vs_render_cached',
+                      'vs_render_schedule_set', 'vs_cache_download'])
 CACHE_PARAMS = 16576
+SCHEDULE_GRID = 0
+# Buffers of the last cache-terminated frame (include/vision_b200.h VS_CACHE_*).
+CACHE_QUERY_DTYPE = np.dtype([('t', '<f4', 4), ('lambda', '<f4', 4), ('pdf', '<f4', 4), ('l_valid', '<f4', 4)])
+CACHE_TRAIN_DTYPE = np.dtype([('suffix_valid', '<f4', 4), ('t', '<f4', 4), ('lambda', '<f4', 4), ('pdf', '<f4', 4)])
+CACHE_BUFFERS = dict(query_features=(0, np.dtype(('<u2', 64)), True), query_records=(1, CACHE_QUERY_DTYPE, True),
+                     query_output=(2, np.dtype(('<f4', 4)), True), train_features=(3, np.dtype(('<u2', 64)), False),
+                     train_records=(4, CACHE_TRAIN_DTYPE, False), suffix_features=(5, np.dtype(('<u2', 64)), False),
+                     suffix_output=(6, np.dtype(('<f4', 4)), False), targets=(7, np.dtype(('<f4', 4)), False))
+SCHEDULE_PERSISTENT = 1
 
 # Per-pixel ReSTIR records (vision_b200/csrc/vs_restir.h) as numpy dtypes.
 HIT_DTYPE = np.dtype([('inst_id', '<u4'), ('prim_id', '<u4'), ('u', '<f4'), ('v', '<f4')])
@@ -297,6 +309,12 @@ class Scene:
                                                    ctypes.c_void_p(t_ptr), ctypes.c_void_p(stream) if stream else None),
                        'trace_closest_device')
 
+    def set_schedule(self, schedule):
+        """Path scheduling of render(): 'persistent' (regenerating resident
+        wave, the default) or 'grid' (one path per thread)."""
+        code = {'grid': SCHEDULE_GRID, 'persistent': SCHEDULE_PERSISTENT}[schedule]
+        self.ctx.check(lib.vs_render_schedule_set(self.handle, code), 'render_schedule_set')
+
     def timing_enable(self, on=True):
         self.ctx.check(lib.vs_timing_enable(self.handle, 1 if on else 0), 'timing_enable')
 
@@ -344,6 +362,19 @@ class Scene:
                                             FILM_FP64 if fp64 else FILM_FP32,
                                             ctypes.c_void_p(stream) if stream else None), 'render_cached')
         self.frames = frame_begin + frame_count
+        if frame_count:
+            i = self.info()
+            self._cache_train = min(train_samples, i['width'] * i['height'])
+
+    def cache_buffer(self, which):
+        """A buffer of the last cache-terminated frame (CACHE_BUFFERS key):
+        per-pixel arrays (height, width, ...) or per training sample (n, ...)."""
+        key, dt, per_pixel = CACHE_BUFFERS[which]
+        i = self.info()
+        n = i['width'] * i['height'] if per_pixel else getattr(self, '_cache_train', 0)
+        out = np.zeros(n, dt)
+        self.ctx.check(lib.vs_cache_download(self.handle, key, _ptr(out), out.nbytes), 'cache_download')
+        return out.reshape((i['height'], i['width']) + out.shape[1:]) if per_pixel else out
 
     def render_stats(self, frame_begin, frame_count):
         """Traversal counters of an instrumented render: (segments, nodes, tris)."""

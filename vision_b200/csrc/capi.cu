@@ -77,6 +77,9 @@ struct vs_scene {
     DevBuf<float4> film32, exposed;
     DevBuf<double> film64;
     DevBuf<float4> radiance;
+    // Path counter of the persistent (regenerating) megakernel.
+    DevBuf<unsigned long long> path_counter;
+    int schedule = VS_SCHEDULE_PERSISTENT;
     // Cache-terminated rendering: per-pixel queries, training samples, the
     // material albedo/roughness table of the feature encoding.
     struct CacheBufs {
@@ -84,9 +87,11 @@ struct vs_scene {
         DevBuf<CacheQueryRec> q_rec;
         DevBuf<CacheTrainRec> t_rec;
         DevBuf<float4> q_out, b_out, targets, mat;
+        uint32_t npix = 0, n_train = 0;  // sizes of the last frame (0: none rendered)
         void free() {
             q_feat.free(); t_feat.free(); b_feat.free(); q_rec.free(); t_rec.free();
             q_out.free(); b_out.free(); targets.free(); mat.free();
+            npix = n_train = 0;
         }
     } cachebuf;
     uint32_t film_frames = 0;
@@ -145,7 +150,7 @@ struct vs_scene {
         nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
         prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
         env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
-        film32.free(); exposed.free(); film64.free(); radiance.free();
+        film32.free(); exposed.free(); film64.free(); radiance.free(); path_counter.free();
         rt.free();
         cachebuf.free();
     }
@@ -490,6 +495,7 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     if (frames_per_chunk == 0) return fail(ctx, VS_E_RANGE, "resolution above the per-launch path limit");
     if (frames_per_chunk > frame_count) frames_per_chunk = frame_count;
     VS_CUDA(s->radiance.alloc(static_cast<size_t>(frames_per_chunk * npix)), "radiance alloc");
+    if (s->schedule == VS_SCHEDULE_PERSISTENT) VS_CUDA(s->path_counter.alloc(1), "path counter alloc");
     DeviceScene dv = s->device_view();
     auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
         cudaEvent_t e;
@@ -501,7 +507,9 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     for (uint32_t f = 0; f < frame_count; f += static_cast<uint32_t>(frames_per_chunk)) {
         uint32_t fc = static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk, frame_count - f));
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
-        VS_CUDA(launch_render(dv, frame_begin + f, fc, s->radiance.ptr, st), "render launch");
+        VS_CUDA(launch_render(dv, frame_begin + f, fc, s->radiance.ptr, st,
+                              s->schedule == VS_SCHEDULE_PERSISTENT ? s->path_counter.ptr : nullptr),
+                "render launch");
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
         if (s->timing) VS_CUDA(timed_event(s->ev_film), "timing event");
         VS_CUDA(launch_film(s->radiance.ptr, static_cast<uint32_t>(npix), frame_begin + f, fc, s->film32.ptr,
@@ -517,6 +525,15 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     }
     s->film_frames = frame_begin + frame_count;
     s->film64_valid = film_precision == VS_FILM_FP64 && (frame_begin == 0 || s->film64_valid);
+    return VS_OK;
+}
+
+int vs_render_schedule_set(vs_scene *s, int schedule) {
+    if (!s) return VS_E_INVALID;
+    if (schedule != VS_SCHEDULE_GRID && schedule != VS_SCHEDULE_PERSISTENT)
+        return fail(s->ctx, VS_E_INVALID, "schedule must be VS_SCHEDULE_GRID or VS_SCHEDULE_PERSISTENT");
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->schedule = schedule;
     return VS_OK;
 }
 
@@ -1258,6 +1275,38 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     }
     s->film_frames = frame_begin + frame_count;
     s->film64_valid = film_precision == VS_FILM_FP64 && (frame_begin == 0 || s->film64_valid);
+    if (frame_count) {
+        b.npix = npix;
+        b.n_train = train_samples;
+    }
+    return VS_OK;
+}
+
+int vs_cache_download(vs_scene *s, int which, void *dst, size_t bytes) {
+    if (!s || !dst) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context has no cache buffers");
+    std::lock_guard<std::mutex> lock(s->mu);
+    const vs_scene::CacheBufs &b = s->cachebuf;
+    if (b.npix == 0) return fail(ctx, VS_E_STATE, "no cache-terminated frame rendered");
+    const void *src = nullptr;
+    size_t n = 0, elem = 0;
+    switch (which) {
+        case VS_CACHE_QUERY_FEATURES: src = b.q_feat.ptr; n = b.npix; elem = 128; break;
+        case VS_CACHE_QUERY_RECORDS: src = b.q_rec.ptr; n = b.npix; elem = sizeof(CacheQueryRec); break;
+        case VS_CACHE_QUERY_OUTPUT: src = b.q_out.ptr; n = b.npix; elem = 16; break;
+        case VS_CACHE_TRAIN_FEATURES: src = b.t_feat.ptr; n = b.n_train; elem = 128; break;
+        case VS_CACHE_TRAIN_RECORDS: src = b.t_rec.ptr; n = b.n_train; elem = sizeof(CacheTrainRec); break;
+        case VS_CACHE_SUFFIX_FEATURES: src = b.b_feat.ptr; n = b.n_train; elem = 128; break;
+        case VS_CACHE_SUFFIX_OUTPUT: src = b.b_out.ptr; n = b.n_train; elem = 16; break;
+        case VS_CACHE_TARGETS: src = b.targets.ptr; n = b.n_train; elem = 16; break;
+        default: return fail(ctx, VS_E_INVALID, "unknown cache buffer");
+    }
+    if (bytes != n * elem) return fail(ctx, VS_E_INVALID, "cache buffer size mismatch");
+    if (n == 0) return VS_OK;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    VS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream), "cache copy");
+    VS_CUDA(cudaStreamSynchronize(ctx->stream), "cache sync");
     return VS_OK;
 }
 

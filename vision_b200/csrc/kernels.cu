@@ -2,11 +2,14 @@
 //   k_trace_closest  - seeded closest-hit batches (parity hook)
 //   k_render         - megakernel: one camera path per thread, radiance to a
 //                      per-sample buffer
+//   k_render_regen   - the same paths in a persistent grid that refills
+//                      finished lanes (path regeneration)
 //   k_film_*         - film accumulation in the reference's frame order
 //                      (FP32 running mean) or as FP64 sums
 #include "vs_integrator.cuh"
 #include "vs_launch.h"
 
+#include <algorithm>
 #include <atomic>
 
 namespace vs {
@@ -59,6 +62,60 @@ __global__ void __launch_bounds__(128, VS_RENDER_MIN_BLOCKS) k_render(DeviceScen
     uint32_t px = pix % s.cam.width, py = pix / s.cam.width;
     f3 L = trace_path<N>(s, px, py, frame);
     radiance[p] = make_float4(L.x, L.y, L.z, 1.0f);
+}
+
+// Persistent form of k_render with path regeneration.  A camera path ends
+// after a data-dependent number of bounces (Russian roulette, misses), so a
+// warp that traces one path per lane idles its finished lanes until the
+// longest path ends.  Here each warp keeps 32 paths in flight: after every
+// bounce the lanes whose path ended write its radiance and claim the next
+// unclaimed path indices with one atomicAdd per warp on `next_path` (zero at
+// launch).  Each path is still traced from its own sampler stream and written
+// to radiance[p], so the output equals k_render's bit for bit.  Needs
+// max_depth >= 1.
+template <int N>
+__global__ void __launch_bounds__(128, VS_RENDER_MIN_BLOCKS)
+    k_render_regen(DeviceScene s, uint32_t frame_begin, uint64_t path_count, float4 *radiance,
+                   unsigned long long *next_path) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t npix = s.cam.width * s.cam.height;
+    const uint32_t max_depth = s.ip.max_depth;
+    PathState<N> ps;
+    uint64_t p = 0;
+    bool active = false;
+    bool drained = false;  // warp-uniform: every path index has been claimed
+    for (;;) {
+        if (!drained) {
+            const unsigned need = __ballot_sync(0xffffffffu, !active);
+            if (need) {
+                const int leader = __ffs(need) - 1;
+                const unsigned count = static_cast<unsigned>(__popc(need));
+                unsigned long long base = 0;
+                if (static_cast<int>(lane) == leader) base = atomicAdd(next_path, static_cast<unsigned long long>(count));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + count >= path_count) drained = true;
+                if (!active) {
+                    const uint64_t q = base + static_cast<unsigned>(__popc(need & ((1u << lane) - 1u)));
+                    if (q < path_count) {
+                        p = q;
+                        const uint32_t frame = frame_begin + static_cast<uint32_t>(q / npix);
+                        const uint32_t pix = static_cast<uint32_t>(q % npix);
+                        path_start<N>(s, s.cam, pix % s.cam.width, pix / s.cam.width, frame, ps);
+                        active = true;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active) {
+            bool more = path_bounce<N>(s, ps, nullptr);
+            if (more) more = ++ps.bounce < max_depth;
+            if (!more) {
+                radiance[p] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);
+                active = false;
+            }
+        }
+    }
 }
 
 // NormalRadianceCollector::add_sample (normal.cpp:87-101) for frame_count
@@ -129,17 +186,52 @@ cudaError_t launch_trace_any(const DeviceScene &s, const float *rays, uint32_t n
 }
 
 cudaError_t launch_render(const DeviceScene &s, uint32_t frame_begin, uint32_t frame_count, float4 *radiance,
-                          cudaStream_t st) {
+                          cudaStream_t st, unsigned long long *path_counter) {
     uint64_t paths = static_cast<uint64_t>(s.cam.width) * s.cam.height * frame_count;
     if (paths == 0) return cudaSuccess;
     uint64_t blocks = (paths + 127) / 128;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    if (s.ip.spectrum_dim < 1 || s.ip.spectrum_dim > 4) return cudaErrorInvalidValue;
+    if (path_counter && s.ip.max_depth > 0) {
+        // One resident wave: SMs x blocks per SM, capped by the work.
+        static std::atomic<int> resident[64][5];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+        const int n = static_cast<int>(s.ip.spectrum_dim);
+        int wave = resident[dev][n].load();
+        if (wave == 0) {
+            int sms = 0, per_sm = 0;
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return e;
+            switch (n) {
+                case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_regen<1>, 128, 0); break;
+                case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_regen<2>, 128, 0); break;
+                case 3: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_regen<3>, 128, 0); break;
+                default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_regen<4>, 128, 0); break;
+            }
+            if (e != cudaSuccess) return e;
+            wave = sms * (per_sm > 0 ? per_sm : 1);
+            resident[dev][n].store(wave);
+        }
+        unsigned grid = static_cast<unsigned>(std::min<uint64_t>(blocks, static_cast<uint64_t>(wave)));
+        e = cudaMemsetAsync(path_counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+        switch (n) {
+            case 1: k_render_regen<1><<<grid, 128, 0, st>>>(s, frame_begin, paths, radiance, path_counter); break;
+            case 2: k_render_regen<2><<<grid, 128, 0, st>>>(s, frame_begin, paths, radiance, path_counter); break;
+            case 3: k_render_regen<3><<<grid, 128, 0, st>>>(s, frame_begin, paths, radiance, path_counter); break;
+            default: k_render_regen<4><<<grid, 128, 0, st>>>(s, frame_begin, paths, radiance, path_counter); break;
+        }
+        g_launches++;
+        return cudaGetLastError();
+    }
     switch (s.ip.spectrum_dim) {
         case 1: k_render<1><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
         case 2: k_render<2><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
         case 3: k_render<3><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
-        case 4: k_render<4><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
-        default: return cudaErrorInvalidValue;
+        default: k_render<4><<<static_cast<unsigned>(blocks), 128, 0, st>>>(s, frame_begin, paths, radiance); break;
     }
     g_launches++;
     return cudaGetLastError();

@@ -68,21 +68,22 @@ VS_HD uint32_t tea4(uint32_t v0, uint32_t v1) {
 }
 
 struct Sampler {
-    uint64_t state;
+    uint64_t state;  // LCG state (low 32 bits) or the 64-bit PCG32 state
     uint32_t kind;
-    VS_HD void start(uint32_t px, uint32_t py, uint32_t sample, uint32_t dim, uint32_t k, uint32_t seed) {
+    uint32_t seed;   // PCG32 stream selector: increment (seed << 1) | 1
+    VS_HD void start(uint32_t px, uint32_t py, uint32_t sample, uint32_t dim, uint32_t k, uint32_t sd) {
         kind = k;
+        seed = sd;
         uint32_t s = tea4(tea4(px, py), tea4(sample, dim));
         if (kind == kSamplerIndependent) {
             state = s;
         } else {
-            // PCG32 initialisation with stream selector derived from the seed.
-            uint64_t inc = (static_cast<uint64_t>(seed) << 1u) | 1u;
-            state = 0u;
-            state = state * 6364136223846793005ull + inc;
+            // PCG32 seeding (pcg32_srandom_r): state 0, one step, add the
+            // initial state (the TEA hash), one more step.
+            const uint64_t inc = (static_cast<uint64_t>(seed) << 1u) | 1u;
+            state = inc;
             state += s;
             state = state * 6364136223846793005ull + inc;
-            state = (state & 0xffffffffffffull) | (static_cast<uint64_t>(seed) << 48);
         }
     }
     VS_HD float next() {
@@ -92,13 +93,12 @@ struct Sampler {
             state = s;
             return static_cast<float>(s & 0x00ffffffu) * (1.0f / 16777216.0f);
         }
-        uint64_t inc = ((state >> 48) << 1u) | 1u;
-        uint64_t old = state & 0xffffffffffffull;
-        uint64_t nxt = (old * 6364136223846793005ull + inc) & 0xffffffffffffull;
-        state = nxt | ((state >> 48) << 48);
-        uint32_t xorshifted = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
-        uint32_t rot = static_cast<uint32_t>(old >> 59u);
-        uint32_t r = (xorshifted >> rot) | (xorshifted << ((32u - rot) & 31u));
+        // PCG32 step and XSH-RR output; the top 24 bits make the float.
+        const uint64_t old = state;
+        state = old * 6364136223846793005ull + ((static_cast<uint64_t>(seed) << 1u) | 1u);
+        const uint32_t xorshifted = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+        const uint32_t rot = static_cast<uint32_t>(old >> 59u);
+        const uint32_t r = (xorshifted >> rot) | (xorshifted << ((32u - rot) & 31u));
         return static_cast<float>(r >> 8) * (1.0f / 16777216.0f);
     }
     VS_HD f2 next2() {

@@ -195,102 +195,154 @@ __device__ __forceinline__ void camera_ray(const Camera &cam, Sampler &smp, uint
     rd = normalize(xform_vector(cam.c2w, dir_cam));
 }
 
+// Mutable state of one camera path between bounces: the sampler, the hero
+// wavelengths, the next ray with the pdf of the direction it was sampled
+// with, the throughput, the radiance gathered so far, the accumulated
+// relative-IOR factor of Russian roulette and the bounce index.
+template <int N>
+struct PathState {
+    Sampler smp;
+    Wavelengths<N> wl;
+    f3 ro, rd;
+    Spec<N> throughput;
+    f3 L;
+    float scatter_pdf;
+    float eta_scale;
+    uint32_t bounce;
+};
+
+// One iteration of the bounce loop of IlluminationIntegrator::Li
+// (integrator.cpp:134-283): trace ps.ro/ps.rd, add emission and the
+// MIS-weighted light sample to ps.L, sample the BSDF and set the next ray.
+// Returns false where the reference's loop breaks (miss, invalid BSDF sample,
+// Russian roulette, zero throughput).  `first`, when non-null, receives the
+// interaction of the first surface hit (the HitContext of the reference).
+template <int N>
+__device__ __forceinline__ bool path_bounce(const DeviceScene &s, PathState<N> &ps, Interaction *first) {
+    const IntegratorParams &ip = s.ip;
+    const uint32_t bounce = ps.bounce;
+    RayPre rp = precompute_ray(ps.ro, ps.rd);
+    Hit hit;
+    float t_hit;
+    if (!trace_closest(s, rp, 3.402823466e+38f, hit, t_hit)) {
+        // IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132).
+        if (s.has_env) {
+            Spec<N> Le;
+            float lpdf;
+            env_eval<N>(s, normalize((ps.ro + ps.rd) - ps.ro), ps.wl, Le, lpdf);
+            lpdf *= light_pmf<N>(s, s.env_index);
+            float weight = ps.scatter_pdf / (ps.scatter_pdf + lpdf);
+            if (ip.mis_mode == 2u) weight = 1.0f;
+            else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
+            ps.L += linear_srgb<N>(Le * ps.throughput * weight, ps.wl);
+        }
+        return false;
+    }
+    Interaction it = surface_interaction(s, hit, ps.rd, true);
+    if (first && bounce == 0) *first = it;
+    if (it.light != kInvalid) {
+        Spec<N> Le;
+        float lpdf;
+        eval_hit_light<N>(s, it, ps.ro, ps.wl, Le, lpdf);
+        float weight = ps.scatter_pdf / (ps.scatter_pdf + lpdf);
+        if (ip.mis_mode == 2u) weight = 1.0f;
+        else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
+        ps.L += linear_srgb<N>(Le * ps.throughput * weight, ps.wl);
+    }
+    // Light sample: 1 draw for the light, 2 for the surface point.
+    float u_light = ps.smp.next();
+    f2 u_surf = ps.smp.next2();
+    LightSample<N> ls = sample_light<N>(s, it, u_light, u_surf, ps.wl);
+    Ray sh = spawn_ray_to(it.pos, it.ng, ls.p_light);
+    bool occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
+    // Material evaluation + BSDF sample (direct_lighting, integrator.cpp:20-44).
+    Material mat = s.materials[it.mat];
+    Bsdf<N> bsdf = make_bsdf<N>(s, mat, it.shading, it.ng, it.wo, ps.wl);
+    if (bsdf.dispersive) invalidate_secondary<N>(ps.wl);
+    f3 wi_light = normalize(ls.p_light - it.pos);
+    BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, nullptr);
+    BsdfSample<N> bs = bsdf.sample(it.wo, ps.smp);
+    Spec<N> Ld = Spec<N>::fill(0.0f);
+    float w_mis = ls.pdf / (ls.pdf + se.pdf);
+    if (ip.mis_mode == 1u) w_mis = 1.0f;
+    if (!occluded && se.valid() && ls.pdf > 0.0f) {
+        Ld = ls.L * se.f * (w_mis / ls.pdf);
+    }
+    if (ip.mis_mode != 2u) ps.L += linear_srgb<N>(ps.throughput * Ld, ps.wl);
+    ps.eta_scale *= sqr(bs.eta);
+    float lum = ps.throughput.max();
+    if (!bs.eval.valid() || lum == 0.0f) return false;
+    ps.throughput = ps.throughput * bs.eval.throughput();
+    if (ps.eta_scale * lum < ip.rr_threshold && bounce >= ip.min_depth) {
+        float q = fminf(0.95f, lum);
+        float rr = ps.smp.next();
+        if (q < rr) return false;
+        ps.throughput = ps.throughput * (1.0f / q);
+    }
+    // A path whose throughput is exactly zero adds nothing from here on.
+    if (ps.throughput.all_zero()) return false;
+    ps.scatter_pdf = bs.eval.pdf;
+    Ray nr = spawn_ray(it.pos, it.ng, bs.wi);
+    ps.ro = nr.o;
+    ps.rd = nr.d;
+    return true;
+}
+
 // The bounce loop of IlluminationIntegrator::Li (integrator.cpp:134-283) from
 // ray (ro, rd) with the given scatter pdf and throughput.  Returns linear sRGB
-// radiance.  `first`, when non-null, receives the interaction of the first
-// surface hit (the HitContext of the reference).
+// radiance; smp and wl carry the sampler position and the (possibly
+// invalidated) wavelengths back to the caller.
 template <int N>
 __device__ __forceinline__ f3 path_li(const DeviceScene &s, Sampler &smp, Wavelengths<N> &wl, f3 ro, f3 rd,
                                       float scatter_pdf, Spec<N> throughput, uint32_t max_depth,
                                       Interaction *first) {
-    const IntegratorParams &ip = s.ip;
-    f3 ret = make3(0.0f);
-    float eta_scale = 1.0f;
-
-    for (uint32_t bounce = 0; bounce < max_depth; ++bounce) {
-        RayPre rp = precompute_ray(ro, rd);
-        Hit hit;
-        float t_hit;
-        if (!trace_closest(s, rp, 3.402823466e+38f, hit, t_hit)) {
-            // IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132).
-            if (s.has_env) {
-                Spec<N> Le;
-                float lpdf;
-                env_eval<N>(s, normalize((ro + rd) - ro), wl, Le, lpdf);
-                lpdf *= light_pmf<N>(s, s.env_index);
-                float weight = scatter_pdf / (scatter_pdf + lpdf);
-                if (ip.mis_mode == 2u) weight = 1.0f;
-                else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
-                ret += linear_srgb<N>(Le * throughput * weight, wl);
-            }
-            break;
-        }
-        Interaction it = surface_interaction(s, hit, rd, true);
-        if (first && bounce == 0) *first = it;
-        if (it.light != kInvalid) {
-            Spec<N> Le;
-            float lpdf;
-            eval_hit_light<N>(s, it, ro, wl, Le, lpdf);
-            float weight = scatter_pdf / (scatter_pdf + lpdf);
-            if (ip.mis_mode == 2u) weight = 1.0f;
-            else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
-            ret += linear_srgb<N>(Le * throughput * weight, wl);
-        }
-        // Light sample: 1 draw for the light, 2 for the surface point.
-        float u_light = smp.next();
-        f2 u_surf = smp.next2();
-        LightSample<N> ls = sample_light<N>(s, it, u_light, u_surf, wl);
-        Ray sh = spawn_ray_to(it.pos, it.ng, ls.p_light);
-        bool occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
-        // Material evaluation + BSDF sample (direct_lighting, integrator.cpp:20-44).
-        Material mat = s.materials[it.mat];
-        Bsdf<N> bsdf = make_bsdf<N>(s, mat, it.shading, it.ng, it.wo, wl);
-        if (bsdf.dispersive) invalidate_secondary<N>(wl);
-        f3 wi_light = normalize(ls.p_light - it.pos);
-        BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, nullptr);
-        BsdfSample<N> bs = bsdf.sample(it.wo, smp);
-        Spec<N> Ld = Spec<N>::fill(0.0f);
-        float w_mis = ls.pdf / (ls.pdf + se.pdf);
-        if (ip.mis_mode == 1u) w_mis = 1.0f;
-        if (!occluded && se.valid() && ls.pdf > 0.0f) {
-            Ld = ls.L * se.f * (w_mis / ls.pdf);
-        }
-        if (ip.mis_mode != 2u) ret += linear_srgb<N>(throughput * Ld, wl);
-        eta_scale *= sqr(bs.eta);
-        float lum = throughput.max();
-        if (!bs.eval.valid() || lum == 0.0f) break;
-        throughput = throughput * bs.eval.throughput();
-        if (eta_scale * lum < ip.rr_threshold && bounce >= ip.min_depth) {
-            float q = fminf(0.95f, lum);
-            float rr = smp.next();
-            if (q < rr) break;
-            throughput = throughput * (1.0f / q);
-        }
-        // A path whose throughput is exactly zero adds nothing from here on.
-        if (throughput.all_zero()) break;
-        scatter_pdf = bs.eval.pdf;
-        Ray nr = spawn_ray(it.pos, it.ng, bs.wi);
-        ro = nr.o;
-        rd = nr.d;
-    }
-    return ret;
+    PathState<N> ps;
+    ps.smp = smp;
+    ps.wl = wl;
+    ps.ro = ro;
+    ps.rd = rd;
+    ps.throughput = throughput;
+    ps.L = make3(0.0f);
+    ps.scatter_pdf = scatter_pdf;
+    ps.eta_scale = 1.0f;
+    for (ps.bounce = 0; ps.bounce < max_depth; ++ps.bounce)
+        if (!path_bounce<N>(s, ps, first)) break;
+    smp = ps.smp;
+    wl = ps.wl;
+    return ps.L;
 }
 
-// One camera path (PathTracingIntegrator kernel body, pt.cpp:53-72) through
-// sensor `cam`.  Returns linear sRGB radiance times the filter weight.
+// Start of one camera path (PathTracingIntegrator kernel body, pt.cpp:53-72)
+// through sensor `cam`: wavelengths from their own sampler stream
+// (RenderEnv::initial, integrator.cpp:49-58), then the camera ray from the
+// pixel's stream.
+template <int N>
+__device__ __forceinline__ void path_start(const DeviceScene &s, const Camera &cam, uint32_t px, uint32_t py,
+                                           uint32_t frame, PathState<N> &ps) {
+    const IntegratorParams &ip = s.ip;
+    ps.smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
+    ps.wl = sample_wavelengths<N>(ps.smp.next());
+    ps.smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
+    f2 p_film;
+    camera_ray(cam, ps.smp, px, py, p_film, ps.ro, ps.rd);
+    ps.throughput = Spec<N>::fill(1.0f);
+    ps.L = make3(0.0f);
+    ps.scatter_pdf = 1e16f;
+    ps.eta_scale = 1.0f;
+    ps.bounce = 0;
+}
+
+// One camera path through sensor `cam`.  Returns linear sRGB radiance times
+// the filter weight.
 template <int N>
 __device__ __forceinline__ f3 trace_path_cam(const DeviceScene &s, const Camera &cam, uint32_t px, uint32_t py,
                                              uint32_t frame) {
-    const IntegratorParams &ip = s.ip;
-    Sampler smp;
-    // Wavelengths come from a separate stream (RenderEnv::initial, integrator.cpp:49-58).
-    smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
-    Wavelengths<N> wl = sample_wavelengths<N>(smp.next());
-    smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
-    f2 p_film;
-    f3 ro, rd;
-    camera_ray(cam, smp, px, py, p_film, ro, rd);
-    return path_li<N>(s, smp, wl, ro, rd, 1e16f, Spec<N>::fill(1.0f), ip.max_depth, nullptr);
+    PathState<N> ps;
+    path_start<N>(s, cam, px, py, frame, ps);
+    const uint32_t max_depth = s.ip.max_depth;
+    for (; ps.bounce < max_depth; ++ps.bounce)
+        if (!path_bounce<N>(s, ps, nullptr)) break;
+    return ps.L;
 }
 
 template <int N>
