@@ -521,6 +521,10 @@ def relmse(img, ref, eps=1e-2):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + eps)))
 
 
+# spp of the equal-time quality curves (plain and cached).
+QUALITY_SPP = (1, 2, 4, 8, 16, 32, 64)
+
+
 def run_cache(args, w, rank, world, local_rank, dist):
     """Cache-terminated rendering: throughput of the cached frames (with their
     training steps) and time to relMSE 1e-2 against an FP64 plain reference,
@@ -557,7 +561,7 @@ def run_cache(args, w, rank, world, local_rank, dist):
 
     # Plain tracer: time and relMSE per spp.
     plain_curve = []
-    for spp in (1, 2, 4, 8, 16, 32):
+    for spp in QUALITY_SPP:
         dt = timed(lambda: plain.render(0, spp, stream=sp))
         plain_curve.append((spp, dt, relmse(plain.film()[..., :3], ref)))
     # Cached: warm-up training, then timed frames (training continues).
@@ -566,7 +570,7 @@ def run_cache(args, w, rank, world, local_rank, dist):
     train_s = timed(lambda: cached.render_cached(cache, 0, w['warmup_frames'], train_samples=w['train_samples'],
                                                  stream=sp))
     cached_curve = []
-    for spp in (1, 2, 4, 8, 16, 32):
+    for spp in QUALITY_SPP:
         dt = timed(lambda: cached.render_cached(cache, 0, spp, train_samples=w['train_samples'], stream=sp))
         cached_curve.append((spp, dt, relmse(cached.film()[..., :3], ref)))
     # Throughput of the timed cached frames (CUDA events, L2 flushed between steps).
@@ -609,8 +613,11 @@ def run_cache(args, w, rank, world, local_rank, dist):
             if r <= w['target_relmse']:
                 return extra + dt, spp
         return None, None
+    # Warm: the cache trained beforehand (an interactive session whose cache
+    # keeps training frame after frame); cold: the warm-up training counted.
     tp, sp_p = time_to(plain_curve)
-    tc, sp_c = time_to(cached_curve, train_s)
+    tc, sp_c = time_to(cached_curve)
+    tc_cold, _ = time_to(cached_curve, train_s)
     # Algorithmic flops of the network per frame: inference on every pixel's
     # query and every suffix end, training forward + backward on the samples.
     nt = w['train_samples']
@@ -632,8 +639,10 @@ def run_cache(args, w, rank, world, local_rank, dist):
                     'plain': [{'spp': a, 's': b, 'relmse': c} for a, b, c in plain_curve],
                     'cached': [{'spp': a, 's': b, 'relmse': c} for a, b, c in cached_curve],
                     'cache_training_s': train_s,
-                    'time_to_target_s': {'plain': tp, 'cached': tc},
-                    'speedup': (tp / tc) if (tp and tc) else None},
+                    'time_to_target_s': {'plain': tp, 'cached_warm': tc, 'cached_cold': tc_cold},
+                    'spp_to_target': {'plain': sp_p, 'cached': sp_c},
+                    'speedup_warm': (tp / tc) if (tp and tc) else None,
+                    'speedup_cold': (tp / tc_cold) if (tp and tc_cold) else None},
         'roofline': {'bound': 'tensor', 'achieved': achieved_tf, 'peak': peak_tf, 'unit': 'TFLOP/s',
                      'frac': achieved_tf / peak_tf, 'peak_source': 'measured', 'traffic': None,
                      'kernel': 'radiance-cache frame (network share of the frame time)',
