@@ -67,7 +67,8 @@ DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64, 'serving'
 
 # DRAM bytes per path of k_render measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch divided by its paths; profiles/).
-NCU_TRAFFIC_PER_PATH = {'large_scene': 1029.3e6 / 2097152, 'box_room': 18.42e6 / 1048576}
+NCU_TRAFFIC_PER_PATH = {('large_scene', 'persistent'): 383.6e6 / 2097152,
+                        ('box_room', 'persistent'): 7.42e6 / 1048576}
 
 # Algorithmic bytes per pixel-frame of the ReSTIR frame, from the record sizes
 # (64 B surfaces and reservoirs, 32 B extensions and BSDF samples, 16 B
@@ -170,16 +171,17 @@ class ClockSampler:
 
 def cpu_baseline(scene, spp, budget_s=12.0):
     """The oracle (a scalar C++ port of the reference integrator) on all host
-    cores, on a fixed seeded subset of the workload's pixels, frame after frame
-    until the time budget is used."""
+    cores, on a fixed seeded subset of the workload's pixels (at most 262,144),
+    frame after frame (frame indices continue past the workload's spp) until
+    the time budget is used."""
     import oracle
     o = oracle.OracleScene(scene)
     threads = os.cpu_count()
-    pixels = sample_pixels(o.width, o.height, 16384)
+    pixels = sample_pixels(o.width, o.height, min(o.width * o.height, 262144))
     o.paths(pixels[:256], 0, 1, threads=threads)  # warm-up
     frames = 0
     t0 = time.perf_counter()
-    while frames < spp and time.perf_counter() - t0 < budget_s:
+    while time.perf_counter() - t0 < budget_s:
         o.paths(pixels, frames, 1, threads=threads)
         frames += 1
     dt = time.perf_counter() - t0
@@ -239,7 +241,7 @@ def run_reference(args, rank):
     scene = vb.Scene(ctx, workload_scene(args.workload)).build_accel()
     o = oracle.OracleScene(scene)
     threads = os.cpu_count()
-    pixels = sample_pixels(o.width, o.height, 16384)
+    pixels = sample_pixels(o.width, o.height, min(o.width * o.height, 262144))
     npix = pixels.size
     for i in range(args.warmup):
         o.paths(pixels, i % w['spp'], 1, threads=threads)
@@ -252,10 +254,10 @@ def run_reference(args, rank):
             'warmup': args.warmup, 'ms_per_step': dt * 1e3 / args.steps, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
             'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
-                       'step': '1 spp of 16384 seeded pixels of the workload per step'},
+                       'step': '1 spp of %d seeded pixels of the workload per step' % npix},
             'impl': 'reference',
             'cpu_baseline': {'value': value, 'unit': 'Mpaths/s', 'cores': threads, 'kind': 'port',
-                             'sample': '16384 seeded pixels x 1 frame (%d paths) per step' % npix},
+                             'sample': '%d seeded pixels x 1 frame (%d paths) per step' % (npix, npix)},
             'e2e': {'value': value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line))
 
@@ -268,7 +270,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--schedule', default='persistent', choices=['persistent', 'grid'],
+    ap.add_argument('--schedule', default='wavefront', choices=['wavefront', 'persistent', 'grid'],
                     help='path scheduling of the megakernel (both give the same film)')
     ap.add_argument('--spp', type=int, default=None,
                     help='override the workload spp (profiling runs on a smaller launch; reported in config)')
@@ -387,10 +389,12 @@ def main():
                    'schedule': args.schedule},
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                      'peak_source': peak_src,
-                     'traffic': (NCU_TRAFFIC_PER_PATH[args.workload] * paths_per_step * args.steps /
-                                 max(render_launches, 1) if args.workload in NCU_TRAFFIC_PER_PATH else None),
+                     'traffic': (NCU_TRAFFIC_PER_PATH[(args.workload, args.schedule)] * paths_per_step * args.steps /
+                                 max(render_launches, 1)
+                                 if (args.workload, args.schedule) in NCU_TRAFFIC_PER_PATH else None),
                      'traffic_source': 'ncu dram bytes per path of the committed profile x paths per launch',
-                     'kernel': 'k_render_regen' if args.schedule == 'persistent' else 'k_render',
+                     'kernel': {'persistent': 'k_render_regen', 'grid': 'k_render',
+                                'wavefront': 'wavefront (k_wf_extend, k_wf_shade, k_wf_shadow)'}[args.schedule],
                      'bytes_per_path': bytes_per_path,
                      'per_path': {'segments': segs / paths_per_step, 'nodes': nodes / paths_per_step,
                                   'tris': tris / paths_per_step},
@@ -618,6 +622,15 @@ def run_cache(args, w, rank, world, local_rank, dist):
     tp, sp_p = time_to(plain_curve)
     tc, sp_c = time_to(cached_curve)
     tc_cold, _ = time_to(cached_curve, train_s)
+
+    def time_model(curve):
+        # relMSE of an unbiased estimate falls as 1/spp and the time grows as
+        # spp: from the last point, the spp and time at the target.
+        spp, dt, r = curve[-1]
+        need = spp * r / w['target_relmse']
+        return need * dt / spp, need
+    tp_m, spp_p_m = time_model(plain_curve)
+    tc_m, spp_c_m = time_model(cached_curve)
     # Algorithmic flops of the network per frame: inference on every pixel's
     # query and every suffix end, training forward + backward on the samples.
     nt = w['train_samples']
@@ -642,7 +655,9 @@ def run_cache(args, w, rank, world, local_rank, dist):
                     'time_to_target_s': {'plain': tp, 'cached_warm': tc, 'cached_cold': tc_cold},
                     'spp_to_target': {'plain': sp_p, 'cached': sp_c},
                     'speedup_warm': (tp / tc) if (tp and tc) else None,
-                    'speedup_cold': (tp / tc_cold) if (tp and tc_cold) else None},
+                    'speedup_cold': (tp / tc_cold) if (tp and tc_cold) else None,
+                    'at_target_1_over_spp': {'plain_s': tp_m, 'plain_spp': spp_p_m, 'cached_s': tc_m,
+                                             'cached_spp': spp_c_m, 'speedup_warm': tp_m / tc_m}},
         'roofline': {'bound': 'tensor', 'achieved': achieved_tf, 'peak': peak_tf, 'unit': 'TFLOP/s',
                      'frac': achieved_tf / peak_tf, 'peak_source': 'measured', 'traffic': None,
                      'kernel': 'radiance-cache frame (network share of the frame time)',

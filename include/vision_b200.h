@@ -140,13 +140,17 @@ int vs_scene_export(const vs_scene *scene, int what, void *dst, size_t bytes);
  * `stream` is a cudaStream_t or NULL for the context's stream. Asynchronous. */
 int vs_render(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, int film_precision, void *stream);
 
-/* How vs_render schedules camera paths on the GPU.  Both give the same film
- * bit for bit.  VS_SCHEDULE_GRID: one path per thread over a grid that covers
- * all paths of a launch.  VS_SCHEDULE_PERSISTENT (the default): one resident
- * wave of warps that keep 32 paths in flight each and refill the lanes of
- * finished paths after every bounce (path regeneration). */
+/* How vs_render schedules camera paths on the GPU.  All give the same film.
+ * VS_SCHEDULE_GRID: one path per thread over a grid that covers all paths of
+ * a launch.  VS_SCHEDULE_PERSISTENT: one resident wave of warps that keep 32
+ * paths in flight each and refill the lanes of finished paths after every
+ * bounce (path regeneration).  VS_SCHEDULE_WAVEFRONT (the default): waves of
+ * up to 4,194,304 paths whose bounces run as separate kernels (closest hit,
+ * shading, shadow rays) over path state in device memory (184 bytes per path
+ * slot, allocated on first use). */
 #define VS_SCHEDULE_GRID 0
 #define VS_SCHEDULE_PERSISTENT 1
+#define VS_SCHEDULE_WAVEFRONT 2
 int vs_render_schedule_set(vs_scene *scene, int schedule);
 
 /* Waits for all work queued on the scene's stream. */

@@ -129,32 +129,38 @@ def test_large_scene_closest_hit_bit_exact(vb, gpu_ctx):
     assert np.array_equal(t_gpu.view(np.uint32), t_cpu.view(np.uint32))
 
 
-@pytest.mark.parametrize('case', ['box_room', 'materials', 'environment', 'dimension1'])
-def test_persistent_schedule_equals_grid(vb, gpu_ctx, case):
-    # Path regeneration only changes which thread traces which path: each path
-    # keeps its own sampler stream and output slot, so the films are identical.
+@pytest.mark.parametrize('case', ['box_room', 'materials', 'environment', 'dimension1', 'two_waves'])
+def test_schedules_give_the_same_film(vb, gpu_ctx, case):
+    # Path regeneration only changes which thread traces which path, and the
+    # wavefront form only where a path's state lives between bounces: each
+    # path keeps its own sampler stream, draw order, summation order and
+    # output slot, so the films are identical.
     if case == 'box_room':
         sc = scenes.box_room(width=67, height=45)
     elif case == 'materials':
         sc = scenes.material_room(40, 36)
     elif case == 'environment':
         sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
-    else:
+    elif case == 'dimension1':
         sc = scenes.box_room(width=33, height=31, dimension=1)
+    else:
+        # 5 frames of 1024 x 1024 exceed one wavefront wave (2^22 paths).
+        sc = scenes.box_room(width=1024, height=1024, max_depth=4, sampler='pcg')
     films = {}
-    for schedule in ('grid', 'persistent'):
+    for schedule in ('grid', 'persistent', 'wavefront'):
         s = vb.Scene(gpu_ctx, sc).build_accel()
         s.set_schedule(schedule)
         s.render(0, 5, fp64=True)
         s.render(5, 4, fp64=True)
         films[schedule] = (s.film(), s.film(vb.FILM_SUM64))
-    assert np.array_equal(films['grid'][0], films['persistent'][0])
-    assert np.array_equal(films['grid'][1], films['persistent'][1])
-    assert np.all(films['persistent'][1][..., 3] == 9.0)
+    for schedule in ('persistent', 'wavefront'):
+        assert np.array_equal(films['grid'][0], films[schedule][0]), schedule
+        assert np.array_equal(films['grid'][1], films[schedule][1]), schedule
+        assert np.all(films[schedule][1][..., 3] == 9.0)
 
 
 def test_schedule_rejects_unknown(vb, gpu_ctx):
     s = vb.Scene(gpu_ctx, scenes.box_room(width=8, height=8)).build_accel()
     assert vb.lib.vs_render_schedule_set(s.handle, 7) == vb.VS_E_INVALID
     with pytest.raises(KeyError):
-        s.set_schedule('wavefront')
+        s.set_schedule('bogus')

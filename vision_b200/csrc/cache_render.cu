@@ -109,7 +109,7 @@ __device__ __forceinline__ float4 wl4(const CWl &w, bool pdf) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_cache_paths(DeviceScene s, CacheFrameParams p) {
+__global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ DeviceScene s, const __grid_constant__ CacheFrameParams p) {
     const uint32_t npix = s.cam.width * s.cam.height;
     const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= npix) return;
@@ -273,7 +273,7 @@ __device__ __forceinline__ bool bad3(f3 v) {
 
 // Pixel radiance into the film (running mean of frame film_index, optional
 // FP64 sums) and the training targets.
-__global__ void k_cache_resolve(DeviceScene s, CacheFrameParams p, float4 *film32, double *film64,
+__global__ void k_cache_resolve(const __grid_constant__ DeviceScene s, const __grid_constant__ CacheFrameParams p, float4 *film32, double *film64,
                                 uint32_t film_index) {
     const uint32_t npix = s.cam.width * s.cam.height;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -14,6 +14,7 @@
 #include "vs_cache_render.h"
 #include "vs_mlp.h"
 #include "vs_server.h"
+#include "vs_wavefront.h"
 
 using namespace vs;
 
@@ -79,7 +80,46 @@ struct vs_scene {
     DevBuf<float4> radiance;
     // Path counter of the persistent (regenerating) megakernel.
     DevBuf<unsigned long long> path_counter;
-    int schedule = VS_SCHEDULE_PERSISTENT;
+    int schedule = VS_SCHEDULE_WAVEFRONT;
+    // Path slots of the wavefront schedule.
+    struct WfBufs {
+        DevBuf<float4> o, d, tp, lam, pdf, L, sh_o, sh_d, sh_c;
+        DevBuf<uint4> st;
+        DevBuf<Hit> hit;
+        DevBuf<uint32_t> q0, q1, count;
+        uint32_t capacity = 0;
+        void free() {
+            o.free(); d.free(); tp.free(); lam.free(); pdf.free(); L.free(); sh_o.free(); sh_d.free(); sh_c.free();
+            st.free(); hit.free(); q0.free(); q1.free(); count.free();
+            capacity = 0;
+        }
+        cudaError_t ensure(uint32_t n) {
+            if (n <= capacity) return cudaSuccess;
+            free();
+            cudaError_t e = cudaSuccess;
+            for (DevBuf<float4> *b : {&o, &d, &tp, &lam, &pdf, &L, &sh_o, &sh_d, &sh_c})
+                if (e == cudaSuccess) e = b->alloc(n);
+            if (e == cudaSuccess) e = st.alloc(n);
+            if (e == cudaSuccess) e = hit.alloc(n);
+            if (e == cudaSuccess) e = q0.alloc(n);
+            if (e == cudaSuccess) e = q1.alloc(n);
+            if (e == cudaSuccess) e = count.alloc(4);
+            if (e != cudaSuccess) {
+                free();
+                return e;
+            }
+            capacity = n;
+            return cudaSuccess;
+        }
+        WfBuffers view() const {
+            WfBuffers b{};
+            b.capacity = capacity;
+            b.o = o.ptr; b.d = d.ptr; b.tp = tp.ptr; b.lam = lam.ptr; b.pdf = pdf.ptr; b.L = L.ptr;
+            b.st = st.ptr; b.hit = hit.ptr; b.queue[0] = q0.ptr; b.queue[1] = q1.ptr;
+            b.sh_o = sh_o.ptr; b.sh_d = sh_d.ptr; b.sh_c = sh_c.ptr; b.count = count.ptr;
+            return b;
+        }
+    } wf;
     // Cache-terminated rendering: per-pixel queries, training samples, the
     // material albedo/roughness table of the feature encoding.
     struct CacheBufs {
@@ -150,7 +190,7 @@ struct vs_scene {
         nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
         prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
         env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
-        film32.free(); exposed.free(); film64.free(); radiance.free(); path_counter.free();
+        film32.free(); exposed.free(); film64.free(); radiance.free(); path_counter.free(); wf.free();
         rt.free();
         cachebuf.free();
     }
@@ -193,6 +233,8 @@ namespace {
 // Upper bound on paths per megakernel launch; sizes the radiance scratch
 // (16 bytes per path).
 constexpr uint64_t kMaxPathsPerLaunch = 1ull << 26;
+// Path slots of one wavefront wave (184 B each: 736 MiB).
+constexpr uint64_t kWfWaveSlots = 1ull << 22;
 
 int fail(const vs_context *ctx, int code, const std::string &msg) {
     if (ctx) {
@@ -225,6 +267,7 @@ int upload_scene(vs_scene *s) {
         VS_CUDA(upload_spectral_consts_rt(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_serve(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_cache(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        VS_CUDA(upload_spectral_consts_wf(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         ctx->consts_uploaded = true;
     }
     const HostScene &h = s->host;
@@ -496,6 +539,9 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     if (frames_per_chunk > frame_count) frames_per_chunk = frame_count;
     VS_CUDA(s->radiance.alloc(static_cast<size_t>(frames_per_chunk * npix)), "radiance alloc");
     if (s->schedule == VS_SCHEDULE_PERSISTENT) VS_CUDA(s->path_counter.alloc(1), "path counter alloc");
+    if (s->schedule == VS_SCHEDULE_WAVEFRONT)
+        VS_CUDA(s->wf.ensure(static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk * npix, kWfWaveSlots))),
+                "wavefront slots alloc");
     DeviceScene dv = s->device_view();
     auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
         cudaEvent_t e;
@@ -507,9 +553,16 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     for (uint32_t f = 0; f < frame_count; f += static_cast<uint32_t>(frames_per_chunk)) {
         uint32_t fc = static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk, frame_count - f));
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
-        VS_CUDA(launch_render(dv, frame_begin + f, fc, s->radiance.ptr, st,
-                              s->schedule == VS_SCHEDULE_PERSISTENT ? s->path_counter.ptr : nullptr),
-                "render launch");
+        if (s->schedule == VS_SCHEDULE_WAVEFRONT) {
+            unsigned n = 0;
+            VS_CUDA(launch_render_wavefront(dv, frame_begin + f, fc, s->radiance.ptr, s->wf.view(), st, &n),
+                    "wavefront render");
+            add_launches(n);
+        } else {
+            VS_CUDA(launch_render(dv, frame_begin + f, fc, s->radiance.ptr, st,
+                                  s->schedule == VS_SCHEDULE_PERSISTENT ? s->path_counter.ptr : nullptr),
+                    "render launch");
+        }
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
         if (s->timing) VS_CUDA(timed_event(s->ev_film), "timing event");
         VS_CUDA(launch_film(s->radiance.ptr, static_cast<uint32_t>(npix), frame_begin + f, fc, s->film32.ptr,
@@ -530,8 +583,8 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
 
 int vs_render_schedule_set(vs_scene *s, int schedule) {
     if (!s) return VS_E_INVALID;
-    if (schedule != VS_SCHEDULE_GRID && schedule != VS_SCHEDULE_PERSISTENT)
-        return fail(s->ctx, VS_E_INVALID, "schedule must be VS_SCHEDULE_GRID or VS_SCHEDULE_PERSISTENT");
+    if (schedule != VS_SCHEDULE_GRID && schedule != VS_SCHEDULE_PERSISTENT && schedule != VS_SCHEDULE_WAVEFRONT)
+        return fail(s->ctx, VS_E_INVALID, "schedule must be VS_SCHEDULE_GRID, _PERSISTENT or _WAVEFRONT");
     std::lock_guard<std::mutex> lock(s->mu);
     s->schedule = schedule;
     return VS_OK;

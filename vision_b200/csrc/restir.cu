@@ -568,7 +568,7 @@ __device__ __forceinline__ RWl pixel_wavelengths(const DeviceScene &s, uint32_t 
 
 }  // namespace
 
-__global__ void k_rt_reset(uint32_t npix, RtBuffers b) {
+__global__ void k_rt_reset(uint32_t npix, const __grid_constant__ RtBuffers b) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npix) return;
     RtSurface sf{};
@@ -596,7 +596,7 @@ __global__ void k_rt_reset(uint32_t npix, RtBuffers b) {
 }
 
 // ReSTIRDI shader0 (direct.cpp:519-557).
-__global__ void __launch_bounds__(128) k_di_candidates(DeviceScene s, RtParams p, RtBuffers b) {
+__global__ void __launch_bounds__(128) k_di_candidates(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -717,7 +717,7 @@ __device__ VS_OUTLINE f3 di_shading(const DeviceScene &s, const RtParams &p, con
 }  // namespace
 
 // ReSTIRDI shader1 (direct.cpp:638-674).
-__global__ void __launch_bounds__(128) k_di_spatial(DeviceScene s, RtParams p, RtBuffers b) {
+__global__ void __launch_bounds__(128) k_di_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -805,7 +805,7 @@ __device__ VS_OUTLINE GiReservoir gi_combine_temporal(const DeviceScene &s, cons
 }  // namespace
 
 // ReSTIRGI initial samples (indirect.cpp:43-111).
-__global__ void __launch_bounds__(128) k_gi_initial(DeviceScene s, RtParams p, RtBuffers b) {
+__global__ void __launch_bounds__(128) k_gi_initial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -843,7 +843,7 @@ __global__ void __launch_bounds__(128) k_gi_initial(DeviceScene s, RtParams p, R
 }
 
 // ReSTIRGI temporal pass (indirect.cpp:155-236).
-__global__ void __launch_bounds__(128) k_gi_temporal(DeviceScene s, RtParams p, RtBuffers b) {
+__global__ void __launch_bounds__(128) k_gi_temporal(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -909,7 +909,7 @@ __global__ void __launch_bounds__(128) k_gi_temporal(DeviceScene s, RtParams p, 
 }
 
 // ReSTIRGI spatial reuse and shading (indirect.cpp:238-332).
-__global__ void __launch_bounds__(128) k_gi_spatial(DeviceScene s, RtParams p, RtBuffers b) {
+__global__ void __launch_bounds__(128) k_gi_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -963,7 +963,7 @@ __global__ void __launch_bounds__(128) k_gi_spatial(DeviceScene s, RtParams p, R
 
 // RealTimeIntegrator combine kernel (rt.cpp:118-126) with
 // NormalRadianceCollector::add_sample (normal.cpp:87-101).
-__global__ void k_rt_combine(uint32_t npix, RtBuffers b, float di, float ii, uint32_t film_index, float4 *film) {
+__global__ void k_rt_combine(uint32_t npix, const __grid_constant__ RtBuffers b, float di, float ii, uint32_t film_index, float4 *film) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npix) return;
     float4 d = b.di_radiance[i], g = b.gi_radiance[i];

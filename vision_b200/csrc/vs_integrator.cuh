@@ -211,20 +211,36 @@ struct PathState {
     uint32_t bounce;
 };
 
+// Shadow ray of one bounce and the radiance it adds when unoccluded (linear
+// sRGB, already weighted by the throughput and the MIS weight).
+struct ShadowQuery {
+    f3 o, d;
+    float tmax;
+    f3 c;
+    bool valid;  // false: no contribution possible, no ray to trace
+};
+
 // One iteration of the bounce loop of IlluminationIntegrator::Li
-// (integrator.cpp:134-283): trace ps.ro/ps.rd, add emission and the
-// MIS-weighted light sample to ps.L, sample the BSDF and set the next ray.
-// Returns false where the reference's loop breaks (miss, invalid BSDF sample,
-// Russian roulette, zero throughput).  `first`, when non-null, receives the
-// interaction of the first surface hit (the HitContext of the reference).
-template <int N>
-__device__ __forceinline__ bool path_bounce(const DeviceScene &s, PathState<N> &ps, Interaction *first) {
+// (integrator.cpp:134-283) after the closest-hit query: add the emission of
+// the hit (or the environment on a miss) to ps.L, prepare the next-event
+// estimate as a shadow query, sample the BSDF and set the next ray.  The caller
+// traces `sq` and adds sq.c when it is unoccluded; a query whose contribution
+// would be zero (no valid BSDF value or light pdf, or mis_mode 2) is not
+// issued, which leaves the sum unchanged.  Returns false where the
+// reference's loop breaks (miss, invalid BSDF sample, Russian roulette, zero
+// throughput).  `first`, when non-null, receives the interaction of the first
+// surface hit (the HitContext of the reference).
+//
+// kTraceShadow: trace the shadow ray in place, right after the light sample
+// (the megakernel: nothing of the query stays live across the BSDF code), and
+// add its contribution to ps.L; sq then stays invalid.
+template <int N, bool kTraceShadow>
+__device__ __forceinline__ bool path_shade(const DeviceScene &s, PathState<N> &ps, bool hit_any, const Hit &hit,
+                                           Interaction *first, ShadowQuery &sq) {
     const IntegratorParams &ip = s.ip;
     const uint32_t bounce = ps.bounce;
-    RayPre rp = precompute_ray(ps.ro, ps.rd);
-    Hit hit;
-    float t_hit;
-    if (!trace_closest(s, rp, 3.402823466e+38f, hit, t_hit)) {
+    sq.valid = false;
+    if (!hit_any) {
         // IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132).
         if (s.has_env) {
             Spec<N> Le;
@@ -254,7 +270,8 @@ __device__ __forceinline__ bool path_bounce(const DeviceScene &s, PathState<N> &
     f2 u_surf = ps.smp.next2();
     LightSample<N> ls = sample_light<N>(s, it, u_light, u_surf, ps.wl);
     Ray sh = spawn_ray_to(it.pos, it.ng, ls.p_light);
-    bool occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
+    bool occluded = false;
+    if (kTraceShadow) occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
     // Material evaluation + BSDF sample (direct_lighting, integrator.cpp:20-44).
     Material mat = s.materials[it.mat];
     Bsdf<N> bsdf = make_bsdf<N>(s, mat, it.shading, it.ng, it.wo, ps.wl);
@@ -262,13 +279,20 @@ __device__ __forceinline__ bool path_bounce(const DeviceScene &s, PathState<N> &
     f3 wi_light = normalize(ls.p_light - it.pos);
     BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, nullptr);
     BsdfSample<N> bs = bsdf.sample(it.wo, ps.smp);
-    Spec<N> Ld = Spec<N>::fill(0.0f);
     float w_mis = ls.pdf / (ls.pdf + se.pdf);
     if (ip.mis_mode == 1u) w_mis = 1.0f;
-    if (!occluded && se.valid() && ls.pdf > 0.0f) {
-        Ld = ls.L * se.f * (w_mis / ls.pdf);
+    if (kTraceShadow) {
+        Spec<N> Ld = Spec<N>::fill(0.0f);
+        if (!occluded && se.valid() && ls.pdf > 0.0f) Ld = ls.L * se.f * (w_mis / ls.pdf);
+        if (ip.mis_mode != 2u) ps.L += linear_srgb<N>(ps.throughput * Ld, ps.wl);
+    } else if (ip.mis_mode != 2u && se.valid() && ls.pdf > 0.0f) {
+        Spec<N> Ld = ls.L * se.f * (w_mis / ls.pdf);
+        sq.o = sh.o;
+        sq.d = sh.d;
+        sq.tmax = sh.tmax;
+        sq.c = linear_srgb<N>(ps.throughput * Ld, ps.wl);
+        sq.valid = true;
     }
-    if (ip.mis_mode != 2u) ps.L += linear_srgb<N>(ps.throughput * Ld, ps.wl);
     ps.eta_scale *= sqr(bs.eta);
     float lum = ps.throughput.max();
     if (!bs.eval.valid() || lum == 0.0f) return false;
@@ -286,6 +310,17 @@ __device__ __forceinline__ bool path_bounce(const DeviceScene &s, PathState<N> &
     ps.ro = nr.o;
     ps.rd = nr.d;
     return true;
+}
+
+// One iteration of the bounce loop: closest hit, shading, shadow ray.
+template <int N>
+__device__ __forceinline__ bool path_bounce(const DeviceScene &s, PathState<N> &ps, Interaction *first) {
+    RayPre rp = precompute_ray(ps.ro, ps.rd);
+    Hit hit;
+    float t_hit;
+    const bool hit_any = trace_closest(s, rp, 3.402823466e+38f, hit, t_hit);
+    ShadowQuery sq;
+    return path_shade<N, true>(s, ps, hit_any, hit, first, sq);
 }
 
 // The bounce loop of IlluminationIntegrator::Li (integrator.cpp:134-283) from

@@ -19,6 +19,8 @@ cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_be
                         double *film64, cudaStream_t st);
 unsigned long long launch_count();
 void add_launches(unsigned n);
+// wavefront.cu
+cudaError_t upload_spectral_consts_wf(const float *x, const float *y, const float *z, const float *d65, float y_integral);
 // server.cu
 cudaError_t upload_spectral_consts_serve(const float *x, const float *y, const float *z, const float *d65,
                                          float y_integral);
