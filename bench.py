@@ -770,7 +770,7 @@ def run_serving(args, w, rank, world, local_rank, dist):
                                       'peak_bytes')},
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved / peak if achieved else None, 'peak_source': peak_src, 'traffic': None,
-                     'kernel': 'k_serve (persistent path kernel)', 'bytes_per_path': mean_bpp,
+                     'kernel': 'serving batches (wavefront kernels k_sv_*)', 'bytes_per_path': mean_bpp,
                      'gpu_busy_s': gpu_s},
         'clocks': clk,
         'e2e': {'value': value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 96,

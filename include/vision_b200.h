@@ -146,8 +146,8 @@ int vs_render(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, int f
  * paths in flight each and refill the lanes of finished paths after every
  * bounce (path regeneration).  VS_SCHEDULE_WAVEFRONT (the default): waves of
  * up to 4,194,304 paths whose bounces run as separate kernels (closest hit,
- * shading, shadow rays) over path state in device memory (184 bytes per path
- * slot, allocated on first use). */
+ * shading sorted by material, shadow rays) over path state in device memory
+ * (208 bytes per path slot, allocated on first use). */
 #define VS_SCHEDULE_GRID 0
 #define VS_SCHEDULE_PERSISTENT 1
 #define VS_SCHEDULE_WAVEFRONT 2

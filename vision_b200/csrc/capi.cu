@@ -86,11 +86,11 @@ struct vs_scene {
         DevBuf<float4> o, d, tp, lam, pdf, L, sh_o, sh_d, sh_c;
         DevBuf<uint4> st;
         DevBuf<Hit> hit;
-        DevBuf<uint32_t> q0, q1, count;
+        DevBuf<uint32_t> q0, q1, tq, count;
         uint32_t capacity = 0;
         void free() {
             o.free(); d.free(); tp.free(); lam.free(); pdf.free(); L.free(); sh_o.free(); sh_d.free(); sh_c.free();
-            st.free(); hit.free(); q0.free(); q1.free(); count.free();
+            st.free(); hit.free(); q0.free(); q1.free(); tq.free(); count.free();
             capacity = 0;
         }
         cudaError_t ensure(uint32_t n) {
@@ -103,7 +103,8 @@ struct vs_scene {
             if (e == cudaSuccess) e = hit.alloc(n);
             if (e == cudaSuccess) e = q0.alloc(n);
             if (e == cudaSuccess) e = q1.alloc(n);
-            if (e == cudaSuccess) e = count.alloc(4);
+            if (e == cudaSuccess) e = tq.alloc(static_cast<size_t>(n) * kWfClasses);
+            if (e == cudaSuccess) e = count.alloc(kWfCounters);
             if (e != cudaSuccess) {
                 free();
                 return e;
@@ -116,7 +117,7 @@ struct vs_scene {
             b.capacity = capacity;
             b.o = o.ptr; b.d = d.ptr; b.tp = tp.ptr; b.lam = lam.ptr; b.pdf = pdf.ptr; b.L = L.ptr;
             b.st = st.ptr; b.hit = hit.ptr; b.queue[0] = q0.ptr; b.queue[1] = q1.ptr;
-            b.sh_o = sh_o.ptr; b.sh_d = sh_d.ptr; b.sh_c = sh_c.ptr; b.count = count.ptr;
+            b.sh_o = sh_o.ptr; b.sh_d = sh_d.ptr; b.sh_c = sh_c.ptr; b.tq = tq.ptr; b.count = count.ptr;
             return b;
         }
     } wf;
@@ -233,7 +234,7 @@ namespace {
 // Upper bound on paths per megakernel launch; sizes the radiance scratch
 // (16 bytes per path).
 constexpr uint64_t kMaxPathsPerLaunch = 1ull << 26;
-// Path slots of one wavefront wave (184 B each: 736 MiB).
+// Path slots of one wavefront wave (208 B each: 832 MiB).
 constexpr uint64_t kWfWaveSlots = 1ull << 22;
 
 int fail(const vs_context *ctx, int code, const std::string &msg) {
@@ -256,6 +257,14 @@ int cuda_fail(const vs_context *ctx, cudaError_t e, const char *where) {
 
 cudaStream_t pick_stream(const vs_scene *s, void *stream) {
     return stream ? static_cast<cudaStream_t>(stream) : s->ctx->stream;
+}
+
+// Shading classes of the wavefront that a scene can produce: misses and one
+// class per material type present.
+uint32_t shading_classes(const HostScene &h) {
+    uint32_t m = 1u;
+    for (const Material &mt : h.materials) m |= 1u << (1u + mt.type);
+    return m;
 }
 
 int upload_scene(vs_scene *s) {
@@ -555,7 +564,8 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
         if (s->schedule == VS_SCHEDULE_WAVEFRONT) {
             unsigned n = 0;
-            VS_CUDA(launch_render_wavefront(dv, frame_begin + f, fc, s->radiance.ptr, s->wf.view(), st, &n),
+            VS_CUDA(launch_render_wavefront(dv, frame_begin + f, fc, s->radiance.ptr, s->wf.view(),
+                                            shading_classes(s->host), st, &n),
                     "wavefront render");
             add_launches(n);
         } else {

@@ -6,19 +6,20 @@
 // GPU busy with batches: every batch takes whole frames from all admitted jobs
 // (a fair share each, then the leftover capacity in admission order), so jobs
 // that arrive while others render start at the next batch and their work
-// overlaps.  A batch is one CUDA-graph launch of three nodes: the work table
-// upload (pinned host -> device), the persistent path kernel k_serve (one CTA
-// per resident slot of every SM, pulling 128-path chunks from a global
-// counter, each path mapped to its job, pixel and frame) and the film pass
+// overlaps.  A batch is one CUDA-graph launch: the work table upload (pinned
+// host -> device), then the batch's paths as wavefront waves (k_sv_generate
+// maps each slot to its job, scene, pixel and frame; per bounce k_sv_extend,
+// k_sv_shade<C> for every shading class C and k_sv_shadow run the shared
+// wavefront bodies with each slot's own scene), then the film pass
 // k_serve_film (each job's running mean in frame order).  Two graph instances
-// with their own tables and radiance buffers alternate, so the host prepares
-// batch i + 1 while batch i runs.  Results are copied to pinned host memory in
-// stream order after the job's last batch; latency is submission to that copy.
+// with their own tables, path slots and radiance buffers alternate, so the
+// host prepares batch i + 1 while batch i runs.  Results are copied to pinned host memory in stream order after the
+// job's last batch; latency is submission to that copy.
 //
 // A job's film equals vs_render of the same scene, camera, resolution and
 // frames: every path uses the same sampler streams and the film the same
 // running mean in the same frame order, whatever the batch composition.
-#include "vs_integrator.cuh"
+#include "vs_wavefront.cuh"
 #include "vs_launch.h"
 #include "vs_server.h"
 #include "../../include/vision_b200.h"
@@ -73,41 +74,78 @@ __device__ __forceinline__ uint32_t find_item(const unsigned long long *begin, u
     return lo;
 }
 
-// Persistent path kernel: CTAs pull chunks of blockDim.x consecutive paths.
-__global__ void __launch_bounds__(128) k_serve(const DeviceScene *scenes, ServeTable *tab, float4 *radiance) {
+// Path slots of one wavefront wave of a batch.
+constexpr uint64_t kServeWaveSlots = 1ull << 22;
+
+// The resident scenes, copied into shared memory by each CTA.
+struct SharedScenes {
+    const DeviceScene *s;
+    __device__ __forceinline__ const DeviceScene &operator()(uint32_t id) const { return s[id]; }
+};
+
+__device__ __forceinline__ void load_scenes(const DeviceScene *scenes, DeviceScene *dst) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(scenes);
+    uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+    const uint32_t words = static_cast<uint32_t>(sizeof(DeviceScene) * kMaxServeScenes / 4);
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) d[i] = src[i];
+    __syncthreads();
+}
+
+// Camera paths of the wave that starts at batch path `base`: slot i holds
+// batch path base + i, mapped to its item (job), pixel and frame.
+__global__ void __launch_bounds__(128) k_sv_generate(const DeviceScene *scenes, const ServeTable *tab,
+                                                     const __grid_constant__ WfBuffers b, uint64_t base,
+                                                     float4 *radiance) {
     __shared__ DeviceScene s_scene[kMaxServeScenes];
     __shared__ unsigned long long s_begin[kMaxServeItems];
-    __shared__ unsigned long long s_chunk;
-    {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(scenes);
-        uint32_t *dst = reinterpret_cast<uint32_t *>(s_scene);
-        const uint32_t words = static_cast<uint32_t>(sizeof(s_scene) / 4);
-        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
-    }
     const uint32_t count = tab->count;
     const uint64_t total = tab->total_paths;
     for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) s_begin[i] = tab->items[i].path_begin;
-    __syncthreads();
-    if (count == 0) return;
-    for (;;) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(&tab->next, static_cast<unsigned long long>(blockDim.x));
-        __syncthreads();
-        const uint64_t base = s_chunk;
-        __syncthreads();
-        if (base >= total) break;
-        const uint64_t p = base + threadIdx.x;
-        if (p < total) {
-            const uint32_t k = find_item(s_begin, count, p);
-            const ServeItem &it = tab->items[k];
-            const uint64_t local = p - s_begin[k];
-            const uint32_t npix = it.npix;
-            const uint32_t f = static_cast<uint32_t>(local / npix);
-            const uint32_t pix = static_cast<uint32_t>(local - static_cast<uint64_t>(f) * npix);
-            const uint32_t w = it.cam.width;
-            f3 L = trace_path_cam<SN>(s_scene[it.scene], it.cam, pix % w, pix / w, it.frame_begin + f);
-            radiance[p] = make_float4(L.x, L.y, L.z, 1.0f);
+    load_scenes(scenes, s_scene);
+    const uint32_t n = base < total ? static_cast<uint32_t>(min(static_cast<uint64_t>(b.capacity), total - base)) : 0u;
+    if (blockIdx.x == 0 && threadIdx.x < kWfCounters) b.count[threadIdx.x] = threadIdx.x == 0 ? n : 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t p = base + i;
+        const uint32_t k = find_item(s_begin, count, p);
+        const ServeItem &it = tab->items[k];
+        const uint64_t local = p - s_begin[k];
+        const uint32_t npix = it.npix;
+        const uint32_t f = static_cast<uint32_t>(local / npix);
+        const uint32_t pix = static_cast<uint32_t>(local - static_cast<uint64_t>(f) * npix);
+        const uint32_t w = it.cam.width;
+        const DeviceScene &s = s_scene[it.scene];
+        PathState<SN> ps;
+        path_start<SN>(s, it.cam, pix % w, pix / w, it.frame_begin + f, ps);
+        if (s.ip.max_depth == 0u) {
+            radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            continue;
         }
+        wf::store<SN>(b, i, ps, it.scene);
+        b.queue[0][i] = i;
     }
+}
+
+__global__ void __launch_bounds__(128) k_sv_extend(const DeviceScene *scenes, const __grid_constant__ WfBuffers b,
+                                                   uint32_t cur) {
+    __shared__ DeviceScene s_scene[kMaxServeScenes];
+    load_scenes(scenes, s_scene);
+    wf::extend(SharedScenes{s_scene}, b, cur);
+}
+
+// Shading of class C (0: misses, 1 + MaterialType: hits of that material).
+template <uint32_t C>
+__global__ void __launch_bounds__(128) k_sv_shade(const DeviceScene *scenes, const __grid_constant__ WfBuffers b,
+                                                  uint32_t cur, uint64_t base, float4 *radiance) {
+    __shared__ DeviceScene s_scene[kMaxServeScenes];
+    load_scenes(scenes, s_scene);
+    wf::shade<SN, C>(SharedScenes{s_scene}, b, cur, base, radiance);
+}
+
+__global__ void __launch_bounds__(128) k_sv_shadow(const DeviceScene *scenes, const __grid_constant__ WfBuffers b,
+                                                   uint64_t base, float4 *radiance) {
+    __shared__ DeviceScene s_scene[kMaxServeScenes];
+    load_scenes(scenes, s_scene);
+    wf::shadow(SharedScenes{s_scene}, b, base, radiance);
 }
 
 // NormalRadianceCollector::add_sample (normal.cpp:87-101) per job pixel over
@@ -174,7 +212,12 @@ public:
     ServeTable *h_tab[2] = {nullptr, nullptr};
     ServeTable *d_tab[2] = {nullptr, nullptr};
     float4 *d_rad[2] = {nullptr, nullptr};
+    WfBuffers wfb[2] = {};
+    void *wf_mem[2] = {nullptr, nullptr};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint32_t graph_depth = 0;   // bounce iterations captured in the graphs
+    uint32_t need_depth = 0;    // largest max_depth of the resident scenes
+    unsigned graph_kernels = 0; // kernel nodes per graph
     cudaEvent_t ev_start[2] = {nullptr, nullptr}, ev_end[2] = {nullptr, nullptr};
 
     std::mutex mu;
@@ -214,6 +257,7 @@ public:
             if (h_tab[k]) cudaFreeHost(h_tab[k]);
             if (d_tab[k]) cudaFree(d_tab[k]);
             if (d_rad[k]) cudaFree(d_rad[k]);
+            if (wf_mem[k]) cudaFree(wf_mem[k]);
             if (ev_start[k]) cudaEventDestroy(ev_start[k]);
             if (ev_end[k]) cudaEventDestroy(ev_end[k]);
         }
@@ -234,24 +278,104 @@ public:
             if (e == cudaSuccess) e = cudaEventCreate(&ev_start[k]);
             if (e == cudaSuccess) e = cudaEventCreate(&ev_end[k]);
         }
-        int sms = 0, per_sm = 0;
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve, 128, 0);
-        unsigned grid = static_cast<unsigned>(std::max(1, sms * std::max(per_sm, 1)));
-        unsigned film_grid = static_cast<unsigned>(std::max(1, sms * 4));
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = alloc_slots(k);
+        if (e == cudaSuccess) e = capture(1);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess) worker = std::thread([this] { run(); });
+        return e;
+    }
+
+    static uint32_t wave_slots(uint64_t batch_paths) {
+        return static_cast<uint32_t>(std::min<uint64_t>(batch_paths, kServeWaveSlots));
+    }
+
+    // Path slots of graph instance k (one wave), one allocation.
+    cudaError_t alloc_slots(int k) {
+        const uint32_t n = wave_slots(batch_paths);
+        const size_t bytes = static_cast<size_t>(n) * kWfBytesPerSlot + 16 * 16 + 4 * kWfCounters + 256;
+        cudaError_t e = cudaMalloc(&wf_mem[k], bytes);
+        if (e != cudaSuccess) return e;
+        char *p = static_cast<char *>(wf_mem[k]);
+        auto take = [&](size_t sz) {
+            char *r = p;
+            p += (sz + 15) & ~size_t(15);
+            return r;
+        };
+        WfBuffers &b = wfb[k];
+        b.capacity = n;
+        b.o = reinterpret_cast<float4 *>(take(16ull * n));
+        b.d = reinterpret_cast<float4 *>(take(16ull * n));
+        b.tp = reinterpret_cast<float4 *>(take(16ull * n));
+        b.lam = reinterpret_cast<float4 *>(take(16ull * n));
+        b.pdf = reinterpret_cast<float4 *>(take(16ull * n));
+        b.L = reinterpret_cast<float4 *>(take(16ull * n));
+        b.st = reinterpret_cast<uint4 *>(take(16ull * n));
+        b.hit = reinterpret_cast<Hit *>(take(16ull * n));
+        b.queue[0] = reinterpret_cast<uint32_t *>(take(4ull * n));
+        b.queue[1] = reinterpret_cast<uint32_t *>(take(4ull * n));
+        b.sh_o = reinterpret_cast<float4 *>(take(16ull * n));
+        b.sh_d = reinterpret_cast<float4 *>(take(16ull * n));
+        b.sh_c = reinterpret_cast<float4 *>(take(16ull * n));
+        b.tq = reinterpret_cast<uint32_t *>(take(4ull * n * kWfClasses));
+        b.count = reinterpret_cast<uint32_t *>(take(4 * kWfCounters));
+        return cudaSuccess;
+    }
+
+    // (Re)captures both batch graphs with `depth` bounce iterations per wave.
+    // No batch may be in flight.
+    cudaError_t capture(uint32_t depth) {
+        int sms = 0, per_ext = 0, per_shadow = 0, per_gen = 0, per_shade[kWfClasses] = {};
+        cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_gen, k_sv_generate, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_ext, k_sv_extend, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[0], k_sv_shade<0>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[1], k_sv_shade<1>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[2], k_sv_shade<2>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[3], k_sv_shade<3>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[4], k_sv_shade<4>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[5], k_sv_shade<5>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shadow, k_sv_shadow, 128, 0);
+        if (e != cudaSuccess) return e;
+        auto grid_of = [&](int per) { return static_cast<unsigned>(std::max(1, sms * std::max(per, 1))); };
+        const unsigned g_gen = grid_of(per_gen), g_ext = grid_of(per_ext), g_shadow = grid_of(per_shadow);
+        unsigned g_shade[kWfClasses];
+        for (uint32_t c = 0; c < kWfClasses; ++c) g_shade[c] = grid_of(per_shade[c]);
+        const unsigned film_grid = static_cast<unsigned>(std::max(1, sms * 4));
+        const uint32_t slots = wave_slots(batch_paths);
+        const uint64_t waves = (batch_paths + slots - 1) / slots;
         for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+            if (graph[k]) {
+                cudaGraphExecDestroy(graph[k]);
+                graph[k] = nullptr;
+            }
             cudaGraph_t g = nullptr;
             e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
             if (e != cudaSuccess) break;
             cudaMemcpyAsync(d_tab[k], h_tab[k], sizeof(ServeTable), cudaMemcpyHostToDevice, stream);
-            k_serve<<<grid, 128, 0, stream>>>(d_scenes, d_tab[k], d_rad[k]);
+            for (uint64_t w = 0; w < waves; ++w) {
+                const uint64_t base = w * slots;
+                k_sv_generate<<<g_gen, 128, 0, stream>>>(d_scenes, d_tab[k], wfb[k], base, d_rad[k]);
+                for (uint32_t bounce = 0; bounce < depth; ++bounce) {
+                    const uint32_t cur = bounce & 1u;
+                    k_sv_extend<<<g_ext, 128, 0, stream>>>(d_scenes, wfb[k], cur);
+                    k_sv_shade<0><<<g_shade[0], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shade<1><<<g_shade[1], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shade<2><<<g_shade[2], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shade<3><<<g_shade[3], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shade<4><<<g_shade[4], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shade<5><<<g_shade[5], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shadow<<<g_shadow, 128, 0, stream>>>(d_scenes, wfb[k], base, d_rad[k]);
+                }
+            }
             k_serve_film<<<film_grid, 256, 0, stream>>>(d_tab[k], d_rad[k]);
             e = cudaStreamEndCapture(stream, &g);
             if (e == cudaSuccess) e = cudaGraphInstantiate(&graph[k], g, 0);
             if (g) cudaGraphDestroy(g);
         }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e == cudaSuccess) worker = std::thread([this] { run(); });
+        if (e == cudaSuccess) {
+            graph_depth = depth;
+            graph_kernels = static_cast<unsigned>(waves * (1 + (2ull + kWfClasses) * depth) + 1);
+        }
         return e;
     }
 
@@ -332,6 +456,20 @@ public:
                 continue;
             }
             if (inflight.size() >= 2) complete_oldest();
+            uint32_t depth;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                depth = need_depth;
+            }
+            if (depth > graph_depth) {
+                while (!inflight.empty()) complete_oldest();
+                cudaError_t e = capture(depth);
+                if (e != cudaSuccess) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    fail_locked(std::string("server graph capture: ") + cudaGetErrorString(e));
+                    continue;
+                }
+            }
             launch_batch(work);
         }
     }
@@ -407,8 +545,8 @@ public:
         }
         st.batches += 1;
         st.graph_launches += 1;
-        st.kernel_launches += 2;
-        add_launches(2);
+        st.kernel_launches += graph_kernels;
+        add_launches(graph_kernels);
         ++batch_no;
         inflight.push_back(std::move(b));
     }
@@ -426,7 +564,8 @@ int server_create(int device, uint64_t hbm_budget, uint32_t max_jobs, uint64_t p
     s->budget = hbm_budget;
     s->max_jobs = max_jobs;
     s->batch_paths = paths_per_batch;
-    s->scratch = 2ull * paths_per_batch * sizeof(float4) + 2ull * sizeof(ServeTable);
+    s->scratch = 2ull * paths_per_batch * sizeof(float4) + 2ull * sizeof(ServeTable) +
+                 2ull * Server::wave_slots(paths_per_batch) * kWfBytesPerSlot;
     if (s->scratch >= hbm_budget) {
         err = "HBM budget below the batch scratch buffers";
         return VS_E_RANGE;
@@ -452,14 +591,16 @@ int server_add_scene(Server *s, const DeviceScene &scene, uint32_t *id, std::str
         err = "served scenes must use 4 hero wavelengths";
         return VS_E_UNSUPPORTED;
     }
-    cudaError_t e = cudaMemcpyAsync(s->d_scenes + s->nscenes, &scene, sizeof(DeviceScene), cudaMemcpyHostToDevice,
-                                    s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    // A synchronous copy, not on the server's stream: the scheduler thread may
+    // be capturing that stream into a graph.
+    cudaSetDevice(s->device);
+    cudaError_t e = cudaMemcpy(s->d_scenes + s->nscenes, &scene, sizeof(DeviceScene), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         err = std::string("server scene upload: ") + cudaGetErrorString(e);
         return VS_E_CUDA;
     }
     s->scene_cam[s->nscenes] = scene.cam;
+    s->need_depth = std::max(s->need_depth, scene.ip.max_depth);
     *id = s->nscenes++;
     return VS_OK;
 }

@@ -213,7 +213,15 @@ struct DielLobe {
     }
 };
 
-template <int N>
+// Material types compiled into a Bsdf: bit t set for MaterialType t.  Kernels
+// that shade one material class at a time instantiate only its code.
+constexpr uint32_t kAllMaterials = 0x1fu;
+template <uint32_t M>
+__device__ __forceinline__ constexpr bool has_mat(uint32_t t) {
+    return ((M >> t) & 1u) != 0u;
+}
+
+template <int N, uint32_t M = kAllMaterials>
 struct Bsdf {
     uint32_t type;
     Frame frame;
@@ -245,19 +253,19 @@ struct Bsdf {
         f3 wo = frame.to_local(wo_w), wi = frame.to_local(wi_w);
         float eta = 1.0f;
         float acos_i = fabsf(wi.z);
-        if (type == kMatDiffuse) {
+        if (has_mat<M>(kMatDiffuse) && type == kMatDiffuse) {
             bool s = wo.z * wi.z > 0.0f;
             e.f = s ? kd * (kInvPi * acos_i) : Spec<N>::fill(0.0f);
             e.pdf = s ? acos_i * kInvPi : 0.0f;
             e.flags = kFlagDiffRefl;
-        } else if (type == kMatMetal) {
+        } else if (has_mat<M>(kMatMetal) && type == kMatMetal) {
             mf[0].eval_local(wo, wi, luts, e.f, e.pdf);
             e.f = e.f * acos_i;
             e.flags = kFlagGlossyRefl;
-        } else if (type == kMatGlass) {
+        } else if (has_mat<M>(kMatGlass) && type == kMatGlass) {
             dl.eval_local(wo, wi, luts, e.f, e.pdf, e.flags, eta);
             e.f = e.f * acos_i;
-        } else if (type == kMatPrincipled) {
+        } else if (has_mat<M>(kMatPrincipled) && type == kMatPrincipled) {
             // LobeSet::evaluate_impl (lobe.cpp:665-681): sum of the lobes, each
             // masked by its own hemisphere test, pdfs weighted by the
             // normalised sample weights.
@@ -314,14 +322,14 @@ struct Bsdf {
         f3 wo = frame.to_local(wo_w);
         bool valid = true;
         f3 wi;
-        if (type == kMatDiffuse) {
+        if (has_mat<M>(kMatDiffuse) && type == kMatDiffuse) {
             wi = cosine_hemisphere(smp.next2());
             wi.z = wo.z < 0.0f ? -wi.z : wi.z;
-        } else if (type == kMatMetal) {
+        } else if (has_mat<M>(kMatMetal) && type == kMatMetal) {
             wi = mf[0].sample_local(wo, smp.next2(), valid);
-        } else if (type == kMatGlass) {
+        } else if (has_mat<M>(kMatGlass) && type == kMatGlass) {
             wi = dl.sample_local(wo, smp, valid);
-        } else if (type == kMatPrincipled) {
+        } else if (has_mat<M>(kMatPrincipled) && type == kMatPrincipled) {
             // LobeSet::sample_wi_impl (lobe.cpp:598-627): 1D lobe choice, an
             // unused 2D draw, then the chosen lobe's own draws.
             float uc = smp.next();
@@ -359,10 +367,10 @@ struct Bsdf {
 
 // Material::create_evaluator for the in-scope plugins.  The lobe parameters
 // come from the 64-byte material record written by the scene loader.
-template <int N>
-__device__ VS_OUTLINE Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng, f3 wo,
-                             const Wavelengths<N> &wl) {
-    Bsdf<N> b;
+template <int N, uint32_t M = kAllMaterials>
+__device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng, f3 wo,
+                                const Wavelengths<N> &wl) {
+    Bsdf<N, M> b;
     b.type = m.type;
     b.frame = frame;
     b.ng = ng;
@@ -371,9 +379,9 @@ __device__ VS_OUTLINE Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m,
     b.w_metal = b.w_trans = b.w_spec = b.w_diff = 0.0f;
     b.has_trans = false;
     b.trans_scale = 0.0f;
-    if (m.type == kMatDiffuse) {
+    if (has_mat<M>(kMatDiffuse) && m.type == kMatDiffuse) {
         b.kd = albedo_spectrum<N>(m.coef, wl);
-    } else if (m.type == kMatMetal) {
+    } else if (has_mat<M>(kMatMetal) && m.type == kMatMetal) {
         // MetalMaterial::create_lobe_set (metal.cpp:137-156).
         MfLobe<N> &l = b.mf[0];
         l.ax = m.p[0];
@@ -389,7 +397,7 @@ __device__ VS_OUTLINE Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m,
             l.fb.v[i] = spd_eval(k + 1, static_cast<int>(k[0]), wl.lambda[i]);
         }
         l.eta0 = 1.0f;
-    } else if (m.type == kMatGlass) {
+    } else if (has_mat<M>(kMatGlass) && m.type == kMatGlass) {
         // GlassMaterial::create_lobe_set (glass.cpp:240-257).
         DielLobe<N> &d = b.dl;
         d.ax = m.p[0];
@@ -403,7 +411,7 @@ __device__ VS_OUTLINE Bsdf<N> make_bsdf(const DeviceScene &s, const Material &m,
                                            : m.p[2];
             d.eta.v[i] = front ? ior : 1.0f / ior;
         }
-    } else if (m.type == kMatPrincipled) {
+    } else if (has_mat<M>(kMatPrincipled) && m.type == kMatPrincipled) {
         // PrincipledBSDF::create_lobe_set (principled_bsdf.cpp:352-461) with
         // sheen and coat at weight 0 (their lobes then contribute nothing).
         float ax = m.p[0], ay = m.p[1];

@@ -233,14 +233,16 @@ struct ShadowQuery {
 //
 // kTraceShadow: trace the shadow ray in place, right after the light sample
 // (the megakernel: nothing of the query stays live across the BSDF code), and
-// add its contribution to ps.L; sq then stays invalid.
-template <int N, bool kTraceShadow>
+// add its contribution to ps.L; sq then stays invalid.  M: the material types
+// compiled in (kAllMaterials, or one class for the material-sorted wavefront
+// kernels, whose hits all have that type); M = 0 compiles the miss only.
+template <int N, bool kTraceShadow, uint32_t M = kAllMaterials>
 __device__ __forceinline__ bool path_shade(const DeviceScene &s, PathState<N> &ps, bool hit_any, const Hit &hit,
                                            Interaction *first, ShadowQuery &sq) {
     const IntegratorParams &ip = s.ip;
     const uint32_t bounce = ps.bounce;
     sq.valid = false;
-    if (!hit_any) {
+    if (!hit_any || M == 0u) {
         // IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132).
         if (s.has_env) {
             Spec<N> Le;
@@ -274,7 +276,7 @@ __device__ __forceinline__ bool path_shade(const DeviceScene &s, PathState<N> &p
     if (kTraceShadow) occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
     // Material evaluation + BSDF sample (direct_lighting, integrator.cpp:20-44).
     Material mat = s.materials[it.mat];
-    Bsdf<N> bsdf = make_bsdf<N>(s, mat, it.shading, it.ng, it.wo, ps.wl);
+    Bsdf<N, M> bsdf = make_bsdf<N, M>(s, mat, it.shading, it.ng, it.wo, ps.wl);
     if (bsdf.dispersive) invalidate_secondary<N>(ps.wl);
     f3 wi_light = normalize(ls.p_light - it.pos);
     BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, nullptr);

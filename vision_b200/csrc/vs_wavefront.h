@@ -26,17 +26,27 @@ struct WfBuffers {
     uint32_t *queue[2];  // slots whose ray is traced next (double-buffered by bounce)
     float4 *sh_o;    // shadow queue: origin + t_max
     float4 *sh_d;    // direction + slot (bits 0..30) and a last-bounce flag (bit 31)
-    float4 *sh_c;    // contribution when unoccluded (linear sRGB)
-    uint32_t *count; // [0], [1]: path queue lengths; [2]: shadow queue length
+    float4 *sh_c;    // contribution when unoccluded (linear sRGB), w: scene id
+    uint32_t *tq;    // hits sorted by shading class: class c at tq[c * capacity]
+    uint32_t *count; // [0], [1]: path queue lengths; [2]: shadow queue length;
+                     // [3 + c]: length of shading class c
 };
 
+// Shading classes of a hit: 0 = miss, 1 + MaterialType otherwise.  Each class
+// is shaded by its own kernel, compiled with that material's code only.
+constexpr uint32_t kWfClasses = 6;
+constexpr uint32_t kWfCounters = 3 + kWfClasses;
+
 // Bytes of device memory per slot of WfBuffers.
-constexpr size_t kWfBytesPerSlot = 6 * 16 + 16 + 16 + 2 * 4 + 3 * 16;
+constexpr size_t kWfBytesPerSlot = 6 * 16 + 16 + 16 + 2 * 4 + 3 * 16 + kWfClasses * 4;
 
 // Renders the paths of frames [frame_begin, frame_begin + frame_count) into
 // radiance[] (one float4 per path, frame-major, as launch_render) in waves of
 // at most b.capacity paths.  `launches` gets the number of kernels launched.
+// class_mask: bit c set when shading class c can occur (bit 0, misses, is
+// always launched); classes without a bit are not launched.
 cudaError_t launch_render_wavefront(const DeviceScene &s, uint32_t frame_begin, uint32_t frame_count,
-                                    float4 *radiance, const WfBuffers &b, cudaStream_t st, unsigned *launches);
+                                    float4 *radiance, const WfBuffers &b, uint32_t class_mask, cudaStream_t st,
+                                    unsigned *launches);
 
 }  // namespace vs

@@ -15,8 +15,7 @@
 // (emission of a bounce, then its next-event estimate), so every path gives
 // the megakernel's radiance.  Queue counters live on the device; kernels loop
 // over `count` with a grid stride, so no host synchronisation is needed.
-#include "vs_wavefront.h"
-#include "vs_integrator.cuh"
+#include "vs_wavefront.cuh"
 #include "vs_launch.h"
 
 #include <algorithm>
@@ -26,73 +25,21 @@ namespace vs {
 
 namespace {
 
-__device__ __forceinline__ float comp(const float4 &v, int i) {
-    return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
-}
-
-template <int N>
-__device__ __forceinline__ float4 pack4(const float *a) {
-    return make_float4(a[0], N > 1 ? a[1] : 0.0f, N > 2 ? a[2] : 0.0f, N > 3 ? a[3] : 0.0f);
-}
-
-template <int N>
-__device__ __forceinline__ void wf_store(const WfBuffers &b, uint32_t slot, const PathState<N> &ps) {
-    b.o[slot] = make_float4(ps.ro.x, ps.ro.y, ps.ro.z, ps.scatter_pdf);
-    b.d[slot] = make_float4(ps.rd.x, ps.rd.y, ps.rd.z, ps.eta_scale);
-    b.tp[slot] = pack4<N>(ps.throughput.v);
-    b.lam[slot] = pack4<N>(ps.wl.lambda);
-    b.pdf[slot] = pack4<N>(ps.wl.pdf);
-    b.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
-    b.st[slot] = make_uint4(static_cast<uint32_t>(ps.smp.state), static_cast<uint32_t>(ps.smp.state >> 32),
-                            ps.bounce, 0u);
-}
-
-template <int N>
-__device__ __forceinline__ void wf_load(const DeviceScene &s, const WfBuffers &b, uint32_t slot, PathState<N> &ps) {
-    const float4 o = b.o[slot], d = b.d[slot], tp = b.tp[slot], lam = b.lam[slot], pdf = b.pdf[slot],
-                 L = b.L[slot];
-    const uint4 st = b.st[slot];
-    ps.ro = make3(o.x, o.y, o.z);
-    ps.scatter_pdf = o.w;
-    ps.rd = make3(d.x, d.y, d.z);
-    ps.eta_scale = d.w;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-        ps.throughput.v[i] = comp(tp, i);
-        ps.wl.lambda[i] = comp(lam, i);
-        ps.wl.pdf[i] = comp(pdf, i);
-    }
-    ps.L = make3(L.x, L.y, L.z);
-    ps.smp.state = static_cast<uint64_t>(st.x) | (static_cast<uint64_t>(st.y) << 32);
-    ps.smp.kind = s.ip.sampler;
-    ps.smp.seed = s.ip.seed;
-    ps.bounce = st.z;
-}
-
-// Appends one entry per calling lane to a device queue: one atomicAdd per
-// converged group of lanes, positions in lane order.
-__device__ __forceinline__ uint32_t queue_push(uint32_t *counter) {
-    const unsigned mask = __activemask();
-    const int lane = static_cast<int>(threadIdx.x & 31u);
-    const int leader = __ffs(mask) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
-    base = __shfl_sync(mask, base, leader);
-    return base + static_cast<uint32_t>(__popc(mask & ((1u << lane) - 1u)));
-}
+// The one scene of a vs_render call (the kernel's grid-constant parameter).
+struct OneScene {
+    const DeviceScene *s;
+    __device__ __forceinline__ const DeviceScene &operator()(uint32_t) const { return *s; }
+};
 
 }  // namespace
 
 // Slot i of the wave holds path base + i.
 template <int N>
-__global__ void __launch_bounds__(128) k_wf_generate(const __grid_constant__ DeviceScene s, const __grid_constant__ WfBuffers b, uint32_t frame_begin, uint64_t base,
-                                                     uint32_t n, float4 *radiance) {
+__global__ void __launch_bounds__(128) k_wf_generate(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ WfBuffers b, uint32_t frame_begin,
+                                                     uint64_t base, uint32_t n, float4 *radiance) {
     const uint32_t npix = s.cam.width * s.cam.height;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        b.count[0] = n;
-        b.count[1] = 0u;
-        b.count[2] = 0u;
-    }
+    if (blockIdx.x == 0 && threadIdx.x < kWfCounters) b.count[threadIdx.x] = threadIdx.x == 0 ? n : 0u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t p = base + i;
         const uint32_t frame = frame_begin + static_cast<uint32_t>(p / npix);
@@ -103,83 +50,28 @@ __global__ void __launch_bounds__(128) k_wf_generate(const __grid_constant__ Dev
             radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             continue;
         }
-        wf_store<N>(b, i, ps);
+        wf::store<N>(b, i, ps, 0u);
         b.queue[0][i] = i;
     }
 }
 
-// Closest hits of queue `cur`.  Also clears the other queue and the shadow
-// queue for the shading pass that follows (their previous users have
-// finished: kernels of one stream run in order).
-__global__ void __launch_bounds__(128) k_wf_extend(const __grid_constant__ DeviceScene s, const __grid_constant__ WfBuffers b, uint32_t cur) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        b.count[cur ^ 1u] = 0u;
-        b.count[2] = 0u;
-    }
-    const uint32_t n = b.count[cur];
-    const uint32_t *q = b.queue[cur];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = q[i];
-        const float4 o = b.o[slot], d = b.d[slot];
-        RayPre rp = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
-        Hit h;
-        float t;
-        if (!trace_closest(s, rp, 3.402823466e+38f, h, t)) h = Hit{kInvalid, kInvalid, 0.0f, 0.0f};
-        b.hit[slot] = h;
-    }
+__global__ void __launch_bounds__(128) k_wf_extend(const __grid_constant__ DeviceScene s,
+                                                   const __grid_constant__ WfBuffers b, uint32_t cur) {
+    wf::extend(OneScene{&s}, b, cur);
 }
 
-// One bounce of every queued path after its closest hit.
-template <int N>
-__global__ void __launch_bounds__(128) k_wf_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ WfBuffers b, uint32_t cur, uint64_t base,
+// Shading of class C (0: misses, 1 + MaterialType: hits of that material).
+template <int N, uint32_t C>
+__global__ void __launch_bounds__(128) k_wf_shade(const __grid_constant__ DeviceScene s,
+                                                  const __grid_constant__ WfBuffers b, uint32_t cur, uint64_t base,
                                                   float4 *radiance) {
-    const uint32_t n = b.count[cur];
-    const uint32_t *q = b.queue[cur];
-    const uint32_t max_depth = s.ip.max_depth;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = q[i];
-        PathState<N> ps;
-        wf_load<N>(s, b, slot, ps);
-        const Hit h = b.hit[slot];
-        ShadowQuery sq;
-        bool more = path_shade<N, false>(s, ps, h.inst_id != kInvalid, h, nullptr, sq);
-        if (more) more = ++ps.bounce < max_depth;
-        if (more) {
-            wf_store<N>(b, slot, ps);
-            b.queue[cur ^ 1u][queue_push(&b.count[cur ^ 1u])] = slot;
-        } else {
-            b.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
-        }
-        if (sq.valid) {
-            const uint32_t k = queue_push(&b.count[2]);
-            b.sh_o[k] = make_float4(sq.o.x, sq.o.y, sq.o.z, sq.tmax);
-            b.sh_d[k] = make_float4(sq.d.x, sq.d.y, sq.d.z, __uint_as_float(slot | (more ? 0u : 0x80000000u)));
-            b.sh_c[k] = make_float4(sq.c.x, sq.c.y, sq.c.z, 0.0f);
-        } else if (!more) {
-            radiance[base + slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);
-        }
-    }
+    wf::shade<N, C>(OneScene{&s}, b, cur, base, radiance);
 }
 
-// Shadow queries of the bounce: add the contribution when unoccluded; write
-// the radiance of paths that ended at this bounce.
-__global__ void __launch_bounds__(128) k_wf_shadow(const __grid_constant__ DeviceScene s, const __grid_constant__ WfBuffers b, uint64_t base, float4 *radiance) {
-    const uint32_t n = b.count[2];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = b.sh_o[i], d = b.sh_d[i];
-        const uint32_t tag = __float_as_uint(d.w);
-        const uint32_t slot = tag & 0x7fffffffu;
-        const bool occluded = trace_any(s, precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z)), o.w);
-        float4 L = b.L[slot];
-        if (!occluded) {
-            const float4 c = b.sh_c[i];
-            f3 l = make3(L.x, L.y, L.z);
-            l += make3(c.x, c.y, c.z);
-            L = make_float4(l.x, l.y, l.z, 0.0f);
-            b.L[slot] = L;
-        }
-        if (tag & 0x80000000u) radiance[base + slot] = make_float4(L.x, L.y, L.z, 1.0f);
-    }
+__global__ void __launch_bounds__(128) k_wf_shadow(const __grid_constant__ DeviceScene s,
+                                                   const __grid_constant__ WfBuffers b, uint64_t base,
+                                                   float4 *radiance) {
+    wf::shadow(OneScene{&s}, b, base, radiance);
 }
 
 namespace {
@@ -201,19 +93,44 @@ cudaError_t resident_grid(K kernel, int dev, std::atomic<int> &cache, unsigned *
     return cudaSuccess;
 }
 
+struct ShadeGrids {
+    unsigned g[kWfClasses];
+};
+
+template <int N, uint32_t C>
+cudaError_t shade_grid(int dev, ShadeGrids &sg) {
+    static std::atomic<int> cache[64];
+    return resident_grid(k_wf_shade<N, C>, dev, cache[dev], &sg.g[C]);
+}
+
+template <int N, uint32_t C>
+void launch_shade(const ShadeGrids &sg, uint32_t mask, const DeviceScene &s, const WfBuffers &b, uint32_t cur,
+                  uint64_t base, float4 *radiance, cudaStream_t st, unsigned &n_launch) {
+    if (!((mask >> C) & 1u)) return;
+    k_wf_shade<N, C><<<sg.g[C], 128, 0, st>>>(s, b, cur, base, radiance);
+    ++n_launch;
+}
+
 template <int N>
 cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths, float4 *radiance,
-                      const WfBuffers &b, cudaStream_t st, unsigned *launches) {
-    static std::atomic<int> g_gen[64], g_ext[64], g_shade[64], g_shadow[64];
+                      const WfBuffers &b, uint32_t class_mask, cudaStream_t st, unsigned *launches) {
+    static std::atomic<int> g_gen[64], g_ext[64], g_shadow[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    unsigned grid_gen, grid_ext, grid_shade, grid_shadow;
+    unsigned grid_gen, grid_ext, grid_shadow;
+    ShadeGrids sg{};
     if ((e = resident_grid(k_wf_generate<N>, dev, g_gen[dev], &grid_gen)) != cudaSuccess) return e;
     if ((e = resident_grid(k_wf_extend, dev, g_ext[dev], &grid_ext)) != cudaSuccess) return e;
-    if ((e = resident_grid(k_wf_shade<N>, dev, g_shade[dev], &grid_shade)) != cudaSuccess) return e;
     if ((e = resident_grid(k_wf_shadow, dev, g_shadow[dev], &grid_shadow)) != cudaSuccess) return e;
+    if ((e = shade_grid<N, 0>(dev, sg)) != cudaSuccess) return e;
+    if ((e = shade_grid<N, 1>(dev, sg)) != cudaSuccess) return e;
+    if ((e = shade_grid<N, 2>(dev, sg)) != cudaSuccess) return e;
+    if ((e = shade_grid<N, 3>(dev, sg)) != cudaSuccess) return e;
+    if ((e = shade_grid<N, 4>(dev, sg)) != cudaSuccess) return e;
+    if ((e = shade_grid<N, 5>(dev, sg)) != cudaSuccess) return e;
+    const uint32_t mask = class_mask | 1u;
     unsigned n_launch = 0;
     for (uint64_t base = 0; base < paths; base += b.capacity) {
         const uint32_t n = static_cast<uint32_t>(std::min<uint64_t>(b.capacity, paths - base));
@@ -223,9 +140,14 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
         for (uint32_t bounce = 0; bounce < s.ip.max_depth; ++bounce) {
             const uint32_t cur = bounce & 1u;
             k_wf_extend<<<grid_ext, 128, 0, st>>>(s, b, cur);
-            k_wf_shade<N><<<grid_shade, 128, 0, st>>>(s, b, cur, base, radiance);
+            launch_shade<N, 0>(sg, mask, s, b, cur, base, radiance, st, n_launch);
+            launch_shade<N, 1>(sg, mask, s, b, cur, base, radiance, st, n_launch);
+            launch_shade<N, 2>(sg, mask, s, b, cur, base, radiance, st, n_launch);
+            launch_shade<N, 3>(sg, mask, s, b, cur, base, radiance, st, n_launch);
+            launch_shade<N, 4>(sg, mask, s, b, cur, base, radiance, st, n_launch);
+            launch_shade<N, 5>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             k_wf_shadow<<<grid_shadow, 128, 0, st>>>(s, b, base, radiance);
-            n_launch += 3;
+            n_launch += 2;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
@@ -236,16 +158,17 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
 }  // namespace
 
 cudaError_t launch_render_wavefront(const DeviceScene &s, uint32_t frame_begin, uint32_t frame_count,
-                                    float4 *radiance, const WfBuffers &b, cudaStream_t st, unsigned *launches) {
+                                    float4 *radiance, const WfBuffers &b, uint32_t class_mask, cudaStream_t st,
+                                    unsigned *launches) {
     if (launches) *launches = 0;
     const uint64_t paths = static_cast<uint64_t>(s.cam.width) * s.cam.height * frame_count;
     if (paths == 0) return cudaSuccess;
     if (b.capacity == 0 || b.capacity > 0x7fffffffu) return cudaErrorInvalidValue;
     switch (s.ip.spectrum_dim) {
-        case 1: return wave_loop<1>(s, frame_begin, paths, radiance, b, st, launches);
-        case 2: return wave_loop<2>(s, frame_begin, paths, radiance, b, st, launches);
-        case 3: return wave_loop<3>(s, frame_begin, paths, radiance, b, st, launches);
-        case 4: return wave_loop<4>(s, frame_begin, paths, radiance, b, st, launches);
+        case 1: return wave_loop<1>(s, frame_begin, paths, radiance, b, class_mask, st, launches);
+        case 2: return wave_loop<2>(s, frame_begin, paths, radiance, b, class_mask, st, launches);
+        case 3: return wave_loop<3>(s, frame_begin, paths, radiance, b, class_mask, st, launches);
+        case 4: return wave_loop<4>(s, frame_begin, paths, radiance, b, class_mask, st, launches);
         default: return cudaErrorInvalidValue;
     }
 }
