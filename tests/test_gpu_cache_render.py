@@ -56,3 +56,33 @@ def test_cached_render_needs_three_wavelengths(vb, gpu_ctx):
     cache = vb.RadianceCache(gpu_ctx, seed=1)
     with pytest.raises(vb.UnsupportedError):
         s.render_cached(cache, 0, 1)
+
+
+@pytest.mark.parametrize('room', ['box', 'materials'])
+def test_wavefront_cache_frame_equals_megakernel(vb, gpu_ctx, room):
+    # The wavefront frame (prefix passes, query kernel, compacted training
+    # suffixes) makes the same draws and sums as the one-kernel frame: the
+    # features, records, targets and film of a frame are identical.  One frame
+    # with the seeded initial weights (training happens after the frame).
+    if room == 'box':
+        sc = scenes.box_room(80, 60, max_depth=8, dimension=3, sampler='pcg')
+    else:
+        sc = scenes.material_room(64, 48, dimension=3, sampler='pcg')
+    out = {}
+    for schedule in ('grid', 'wavefront'):
+        s = vb.Scene(gpu_ctx, sc).build_accel()
+        s.set_schedule(schedule)
+        cache = vb.RadianceCache(gpu_ctx, seed=1)
+        s.render_cached(cache, 0, 1, train_samples=700)
+        bufs = {k: s.cache_buffer(k) for k in ('query_features', 'query_output', 'train_features', 'suffix_features',
+                                               'suffix_output', 'targets')}
+        q = s.cache_buffer('query_records')
+        bufs['valid'] = q['l_valid'][..., 3]
+        bufs['query_t'] = np.where(bufs['valid'][..., None] != 0, q['t'], 0)
+        bufs['film'] = s.film()
+        t = s.cache_buffer('train_records')
+        bufs['suffix'] = t['suffix_valid']
+        out[schedule] = bufs
+    for k in out['grid']:
+        assert np.array_equal(out['grid'][k], out['wavefront'][k]), k
+    assert out['grid']['valid'].mean() > 0.3

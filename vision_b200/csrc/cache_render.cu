@@ -27,10 +27,12 @@
 // albedo (3); sin/cos(2^k pi u) of the hero wavelength u = (lambda_0 - 360) /
 // 470 for k = 0..2 (6).
 #include "vs_cache_render.h"
-#include "vs_integrator.cuh"
+#include "vs_wavefront.cuh"
 #include "vs_launch.h"
 
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 namespace vs {
 
@@ -273,13 +275,16 @@ __device__ __forceinline__ bool bad3(f3 v) {
 
 // Pixel radiance into the film (running mean of frame film_index, optional
 // FP64 sums) and the training targets.
-__global__ void k_cache_resolve(const __grid_constant__ DeviceScene s, const __grid_constant__ CacheFrameParams p, float4 *film32, double *film64,
-                                uint32_t film_index) {
+// `ended` (wavefront frames): radiance of the paths that ended before their
+// query vertex, whose query records stay zero; null when the records carry it.
+__global__ void k_cache_resolve(const __grid_constant__ DeviceScene s, const __grid_constant__ CacheFrameParams p,
+                                float4 *film32, double *film64, uint32_t film_index, const float4 *ended) {
     const uint32_t npix = s.cam.width * s.cam.height;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < npix) {
         CacheQueryRec r = p.q_rec[i];
         f3 L = make3(r.l_valid.x, r.l_valid.y, r.l_valid.z);
+        if (ended && r.l_valid.w == 0.0f) L = make3(ended[i].x, ended[i].y, ended[i].z);
         if (r.l_valid.w != 0.0f) {
             CWl wl = wl_of(r.lambda, r.pdf);
             L += linear_srgb<CN>(spec_of(r.t) * cache_radiance(p.q_out[i]), wl);
@@ -331,7 +336,227 @@ cudaError_t launch_cache_frame(const DeviceScene &s, const CacheFrameParams &p, 
     }
     if (e == cudaSuccess) {
         uint32_t m = npix > p.n_train ? npix : p.n_train;
-        k_cache_resolve<<<(m + 255) / 256, 256, 0, st>>>(s, p, film32, film64, film_index);
+        k_cache_resolve<<<(m + 255) / 256, 256, 0, st>>>(s, p, film32, film64, film_index, nullptr);
+        ++n;
+        e = cudaGetLastError();
+    }
+    if (launches) *launches = n;
+    return e;
+}
+
+// ---------------------------------------------------------------------------
+// Wavefront form of the cache-terminated frame.  The two bounces before the
+// query vertex run as wavefront passes (closest hit, material-sorted
+// shading, shadow rays); k_cache_query adds the query vertex's emission,
+// encodes it and writes its record; k_cache_suffix traces the training
+// suffixes of the (compacted) training paths, so a warp no longer carries one
+// training lane through two extra bounces.  Every path makes the same sampler
+// draws and sums in the same order as k_cache_paths, so the records, features
+// and targets are those of k_cache_paths.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct CacheScene {
+    const DeviceScene *s;
+    __device__ __forceinline__ const DeviceScene &operator()(uint32_t) const { return *s; }
+};
+
+// Training sample of pixel `pix`, or n_train when it is not a training pixel.
+__device__ __forceinline__ uint32_t train_index(const CacheFrameParams &p, uint32_t pix) {
+    if (!p.n_train || pix < p.train_offset || (pix - p.train_offset) % p.train_stride != 0) return p.n_train;
+    const uint32_t tj = (pix - p.train_offset) / p.train_stride;
+    return tj < p.n_train ? tj : p.n_train;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_cw_generate(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ WfBuffers b, uint32_t frame, uint32_t n,
+                                                     float4 *ended) {
+    wf::generate<CN>(s, s.cam, b, frame, 0, n, ended);
+}
+
+__global__ void __launch_bounds__(128) k_cw_extend(const __grid_constant__ DeviceScene s,
+                                                   const __grid_constant__ WfBuffers b, uint32_t cur) {
+    wf::extend(CacheScene{&s}, b, cur);
+}
+
+template <uint32_t C>
+__global__ void __launch_bounds__(128) k_cw_shade(const __grid_constant__ DeviceScene s,
+                                                  const __grid_constant__ WfBuffers b, uint32_t cur, float4 *ended) {
+    wf::shade<CN, C>(CacheScene{&s}, b, cur, 0, ended);
+}
+
+__global__ void __launch_bounds__(128) k_cw_shadow(const __grid_constant__ DeviceScene s,
+                                                   const __grid_constant__ WfBuffers b, float4 *ended) {
+    wf::shadow(CacheScene{&s}, b, 0, ended);
+}
+
+// Query vertices (the hits of the bounce-`query_depth` rays of queue `cur`).
+__global__ void __launch_bounds__(128) k_cache_query(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ CacheFrameParams p,
+                                                     const __grid_constant__ WfBuffers b, uint32_t cur, float4 *ended,
+                                                     uint32_t *suffix_list, uint32_t *suffix_count) {
+    const uint32_t n = b.count[cur];
+    const uint32_t *q = b.queue[cur];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = q[i];
+        PathState<CN> ps;
+        wf::load<CN>(CacheScene{&s}, b, slot, ps);
+        const Hit h = b.hit[slot];
+        if (h.inst_id == kInvalid) {
+            miss_emission<CN>(s, ps, RgbAcc<CN>{});
+            ended[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);
+            continue;
+        }
+        const Interaction it = surface_interaction(s, h, ps.rd, true);
+        hit_emission<CN>(s, ps, it, RgbAcc<CN>{});
+        encode(p, it, ps.wl.lambda[0], p.q_feat + static_cast<size_t>(slot) * 64u);
+        CacheQueryRec rec;
+        rec.t = spec4(ps.throughput, 0.0f);
+        rec.lambda = wl4(ps.wl, false);
+        rec.pdf = wl4(ps.wl, true);
+        rec.l_valid = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);
+        p.q_rec[slot] = rec;
+        const uint32_t tj = train_index(p, slot);
+        if (tj < p.n_train) {
+            encode(p, it, ps.wl.lambda[0], p.t_feat + static_cast<size_t>(tj) * 64u);
+            suffix_list[wf::queue_push(suffix_count)] = slot;
+        }
+    }
+}
+
+// Training suffixes: `suffix_depth` more bounces from the query vertex with the
+// throughput restarted there, gathered per hero wavelength, then the
+// features of the suffix end (bootstrap vertex).
+__global__ void __launch_bounds__(128) k_cache_suffix(const __grid_constant__ DeviceScene s,
+                                                      const __grid_constant__ CacheFrameParams p,
+                                                      const __grid_constant__ WfBuffers b,
+                                                      const uint32_t *suffix_list, const uint32_t *suffix_count) {
+    const uint32_t n = *suffix_count;
+    const uint32_t end_depth = p.query_depth + p.suffix_depth;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t slot = suffix_list[k];
+        const uint32_t tj = train_index(p, slot);
+        PathState<CN> ps;
+        wf::load<CN>(CacheScene{&s}, b, slot, ps);
+        CSpec suffix = CSpec::fill(0.0f);
+        const SpecAcc<CN> acc{&suffix};
+        ps.throughput = CSpec::fill(1.0f);
+        ShadowQuery sq;
+        bool more = path_shade_acc<CN, true, kAllMaterials>(s, ps, true, b.hit[slot], nullptr, sq, acc, false);
+        bool complete = false;
+        while (more) {
+            ++ps.bounce;
+            Hit h;
+            float t_hit;
+            const bool hit_any = trace_closest(s, precompute_ray(ps.ro, ps.rd), 3.402823466e+38f, h, t_hit);
+            if (ps.bounce == end_depth) {
+                if (!hit_any) {
+                    miss_emission<CN>(s, ps, acc);
+                    break;
+                }
+                const Interaction it = surface_interaction(s, h, ps.rd, true);
+                hit_emission<CN>(s, ps, it, acc);
+                encode(p, it, ps.wl.lambda[0], p.b_feat + static_cast<size_t>(tj) * 64u);
+                complete = true;
+                break;
+            }
+            more = path_shade_acc<CN, true, kAllMaterials>(s, ps, hit_any, h, nullptr, sq, acc, true);
+        }
+        CacheTrainRec tr;
+        tr.suffix_valid = spec4(suffix, complete ? 1.0f : 0.0f);
+        tr.t = complete ? spec4(ps.throughput, 0.0f) : make_float4(0, 0, 0, 0);
+        tr.lambda = wl4(ps.wl, false);
+        tr.pdf = wl4(ps.wl, true);
+        p.t_rec[tj] = tr;
+    }
+}
+
+namespace {
+
+template <typename K>
+unsigned wave_grid(K kernel) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
+    return static_cast<unsigned>(std::max(1, sms * std::max(per_sm, 1)));
+}
+
+template <uint32_t C>
+void cw_shade(uint32_t mask, const DeviceScene &s, const WfBuffers &b, uint32_t cur, float4 *ended, cudaStream_t st,
+              unsigned &n) {
+    static unsigned grid = 0;
+    if (!((mask >> C) & 1u)) return;
+    if (!grid) grid = wave_grid(k_cw_shade<C>);
+    k_cw_shade<C><<<grid, 128, 0, st>>>(s, b, cur, ended);
+    ++n;
+}
+
+}  // namespace
+
+cudaError_t launch_cache_frame_wavefront(const DeviceScene &s, const CacheFrameParams &p, const MlpState &mlp,
+                                         float4 *film32, double *film64, uint32_t film_index, const WfBuffers &b,
+                                         uint32_t class_mask, float4 *ended, uint32_t *suffix_list,
+                                         uint32_t *suffix_count, cudaStream_t st, unsigned *launches) {
+    const uint32_t npix = s.cam.width * s.cam.height;
+    if (npix > b.capacity) return cudaErrorInvalidValue;
+    static unsigned g_gen = 0, g_ext = 0, g_shadow = 0, g_query = 0, g_suffix = 0;
+    if (!g_gen) {
+        g_gen = wave_grid(k_cw_generate);
+        g_ext = wave_grid(k_cw_extend);
+        g_shadow = wave_grid(k_cw_shadow);
+        g_query = wave_grid(k_cache_query);
+        g_suffix = wave_grid(k_cache_suffix);
+    }
+    // The prefix ends at the query vertex, not at the scene's depth limit
+    // (k_cache_paths does not apply it either).
+    DeviceScene sv = s;
+    sv.ip.max_depth = 0xffffffffu;
+    cudaError_t e = cudaMemsetAsync(p.q_rec, 0, sizeof(CacheQueryRec) * npix, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(suffix_count, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess && p.n_train) {
+        e = cudaMemsetAsync(p.t_rec, 0, sizeof(CacheTrainRec) * p.n_train, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(p.t_feat, 0, 128ull * p.n_train, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(p.b_feat, 0, 128ull * p.n_train, st);
+    }
+    if (e != cudaSuccess) return e;
+    unsigned n = 0;
+    const uint32_t mask = class_mask | 1u;
+    k_cw_generate<<<std::min<unsigned>(g_gen, (npix + 127) / 128), 128, 0, st>>>(sv, b, p.frame, npix, ended);
+    ++n;
+    for (uint32_t bounce = 0; bounce < p.query_depth; ++bounce) {
+        const uint32_t cur = bounce & 1u;
+        k_cw_extend<<<g_ext, 128, 0, st>>>(sv, b, cur);
+        cw_shade<0>(mask, sv, b, cur, ended, st, n);
+        cw_shade<1>(mask, sv, b, cur, ended, st, n);
+        cw_shade<2>(mask, sv, b, cur, ended, st, n);
+        cw_shade<3>(mask, sv, b, cur, ended, st, n);
+        cw_shade<4>(mask, sv, b, cur, ended, st, n);
+        cw_shade<5>(mask, sv, b, cur, ended, st, n);
+        k_cw_shadow<<<g_shadow, 128, 0, st>>>(sv, b, ended);
+        n += 2;
+    }
+    const uint32_t cur = p.query_depth & 1u;
+    k_cw_extend<<<g_ext, 128, 0, st>>>(sv, b, cur);
+    k_cache_query<<<g_query, 128, 0, st>>>(sv, p, b, cur, ended, suffix_list, suffix_count);
+    n += 2;
+    if (p.n_train) {
+        k_cache_suffix<<<std::min<unsigned>(g_suffix, (p.n_train + 127) / 128), 128, 0, st>>>(sv, p, b, suffix_list,
+                                                                                           suffix_count);
+        ++n;
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = mlp_infer(mlp, p.q_feat, npix, p.q_out, st);
+    ++n;
+    if (e == cudaSuccess && p.n_train) {
+        e = mlp_infer(mlp, p.b_feat, p.n_train, p.b_out, st);
+        ++n;
+    }
+    if (e == cudaSuccess) {
+        const uint32_t m = npix > p.n_train ? npix : p.n_train;
+        k_cache_resolve<<<(m + 255) / 256, 256, 0, st>>>(s, p, film32, film64, film_index, ended);
         ++n;
         e = cudaGetLastError();
     }

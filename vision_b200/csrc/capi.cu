@@ -128,10 +128,11 @@ struct vs_scene {
         DevBuf<CacheQueryRec> q_rec;
         DevBuf<CacheTrainRec> t_rec;
         DevBuf<float4> q_out, b_out, targets, mat;
+        DevBuf<uint32_t> suffix_list, suffix_count;  // training paths of a wavefront frame
         uint32_t npix = 0, n_train = 0;  // sizes of the last frame (0: none rendered)
         void free() {
             q_feat.free(); t_feat.free(); b_feat.free(); q_rec.free(); t_rec.free();
-            q_out.free(); b_out.free(); targets.free(); mat.free();
+            q_out.free(); b_out.free(); targets.free(); mat.free(); suffix_list.free(); suffix_count.free();
             npix = n_train = 0;
         }
     } cachebuf;
@@ -1300,6 +1301,14 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     p.targets = b.targets.ptr;
     p.query_depth = 2;
     p.suffix_depth = 2;
+    // Wavefront frames need one path slot per pixel.
+    const bool wavefront = s->schedule == VS_SCHEDULE_WAVEFRONT && npix <= kWfWaveSlots;
+    if (wavefront) {
+        VS_CUDA(s->wf.ensure(npix), "wavefront slots alloc");
+        VS_CUDA(s->radiance.alloc(npix), "radiance alloc");
+        VS_CUDA(b.suffix_list.alloc(nt), "cache alloc");
+        VS_CUDA(b.suffix_count.alloc(1), "cache alloc");
+    }
     DeviceScene dv = s->device_view();
     auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
         cudaEvent_t e;
@@ -1319,9 +1328,15 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
         p.train_offset = train_samples ? hsh % p.train_stride : 0u;
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
         unsigned n = 0;
-        VS_CUDA(launch_cache_frame(dv, p, c->st, s->film32.ptr, film_precision == VS_FILM_FP64 ? s->film64.ptr : nullptr,
-                                   frame, st, &n),
-                "cache frame");
+        double *f64 = film_precision == VS_FILM_FP64 ? s->film64.ptr : nullptr;
+        if (wavefront) {
+            VS_CUDA(launch_cache_frame_wavefront(dv, p, c->st, s->film32.ptr, f64, frame, s->wf.view(),
+                                                 shading_classes(h), s->radiance.ptr, b.suffix_list.ptr,
+                                                 b.suffix_count.ptr, st, &n),
+                    "cache frame");
+        } else {
+            VS_CUDA(launch_cache_frame(dv, p, c->st, s->film32.ptr, f64, frame, st, &n), "cache frame");
+        }
         add_launches(n);
         if (train_samples) {
             c->adam.loss_scale = 1.0f / (3.0f * static_cast<float>(train_samples));

@@ -9,6 +9,7 @@
 
 #include "vs_devscene.h"
 #include "vs_mlp.h"
+#include "vs_wavefront.h"
 
 namespace vs {
 
@@ -50,5 +51,13 @@ cudaError_t upload_spectral_consts_cache(const float *x, const float *y, const f
 // resolve (film + training targets).  The caller then trains the cache.
 cudaError_t launch_cache_frame(const DeviceScene &s, const CacheFrameParams &p, const MlpState &mlp, float4 *film32,
                                double *film64, uint32_t film_index, cudaStream_t st, unsigned *launches);
+// The same frame with the paths as wavefront passes over the slots of `b`
+// (capacity >= the frame's pixels): `ended` (one float4 per pixel) receives
+// the radiance of paths that end before their query vertex, `suffix_list`
+// (n_train entries) and `suffix_count` hold the training paths.
+cudaError_t launch_cache_frame_wavefront(const DeviceScene &s, const CacheFrameParams &p, const MlpState &mlp,
+                                         float4 *film32, double *film64, uint32_t film_index, const WfBuffers &b,
+                                         uint32_t class_mask, float4 *ended, uint32_t *suffix_list,
+                                         uint32_t *suffix_count, cudaStream_t st, unsigned *launches);
 
 }  // namespace vs

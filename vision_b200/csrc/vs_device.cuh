@@ -521,4 +521,105 @@ static __device__ __noinline__ bool trace_any(const DeviceScene &s, const RayPre
     return false;
 }
 
+// Resumable traversal: the node and triangle visits of trace_closest /
+// trace_any, one node (with the triangles it hit) per step, so that a warp can
+// give a lane whose ray has finished a new ray while the others continue (ray
+// replacement).  A ray visits the same nodes and triangles in the same order,
+// so it gets the same result.
+struct TravState {
+    uint2 ng, tg;
+    int sp;
+    float tmax;
+    float best_t;
+    uint32_t best_prim;
+    float best_u, best_v;
+};
+
+__device__ __forceinline__ void trav_init(TravState &t, const RayPre &r, float tmax) {
+    t.ng = make_uint2(0u, (1u << (24u + (0u ^ r.oct))) | 1u);
+    t.tg = make_uint2(0u, 0u);
+    t.sp = 0;
+    t.tmax = tmax;
+    t.best_t = tmax;
+    t.best_prim = kInvalid;
+    t.best_u = 0.0f;
+    t.best_v = 0.0f;
+}
+
+// One step of the closest-hit traversal; true when the traversal has ended
+// (the result is in t.best_*).
+__device__ __forceinline__ bool closest_step(const DeviceScene &s, const RayPre &r, TravState &t, uint2 *stack) {
+    {
+        uint32_t bit = __ffs(t.ng.y & 0xff000000u) - 1u;
+        t.ng.y &= ~(1u << bit);
+        uint32_t slot = (bit - 24u) ^ r.oct;
+        uint32_t child = t.ng.x + __popc(t.ng.y & 0xffu & ((1u << slot) - 1u));
+        if ((t.ng.y & 0xff000000u) != 0u && t.sp < kStackSize) stack[t.sp++] = t.ng;
+        intersect_children(s.nodes, child, r, t.best_t * kBoxSlack, t.ng, t.tg);
+    }
+    while (t.tg.y & 0x00ffffffu) {
+        uint32_t bit = __ffs(t.tg.y & 0x00ffffffu) - 1u;
+        t.tg.y &= ~(1u << bit);
+        uint32_t ti = t.tg.x + bit;
+        const float4 *tp = s.tri_v + static_cast<size_t>(ti) * 3u;
+        float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float th, u, v;
+        float tri_tmax = t.best_prim == kInvalid ? t.tmax : t.best_t * kBoxSlack;
+        if (intersect_triangle(r, a, b, c, 0.0f, tri_tmax, th, u, v)) {
+            uint32_t prim = __float_as_uint(a.w);
+            if (th < t.best_t || (th == t.best_t && prim < t.best_prim)) {
+                t.best_t = th;
+                t.best_prim = prim;
+                t.best_u = u;
+                t.best_v = v;
+            }
+        }
+    }
+    if (t.ng.y <= 0x00ffffffu) {
+        if (t.sp == 0) return true;
+        t.ng = stack[--t.sp];
+    }
+    return false;
+}
+
+// The hit of a finished closest-hit traversal (inst_id kInvalid: miss).
+__device__ __forceinline__ Hit trav_hit(const DeviceScene &s, const TravState &t) {
+    if (t.best_prim == kInvalid) return Hit{kInvalid, kInvalid, 0.0f, 0.0f};
+    return Hit{__ldg(&s.prims[t.best_prim].w), t.best_prim, t.best_u, t.best_v};
+}
+
+// One step of the any-hit traversal; true when it has ended, with `hit` set
+// when an intersection was found.
+__device__ __forceinline__ bool any_step(const DeviceScene &s, const RayPre &r, TravState &t, uint2 *stack,
+                                         bool &hit) {
+    {
+        uint32_t bit = __ffs(t.ng.y & 0xff000000u) - 1u;
+        t.ng.y &= ~(1u << bit);
+        uint32_t slot = (bit - 24u) ^ r.oct;
+        uint32_t child = t.ng.x + __popc(t.ng.y & 0xffu & ((1u << slot) - 1u));
+        if ((t.ng.y & 0xff000000u) != 0u && t.sp < kStackSize) stack[t.sp++] = t.ng;
+        intersect_children(s.nodes, child, r, t.tmax * kBoxSlack, t.ng, t.tg);
+    }
+    while (t.tg.y & 0x00ffffffu) {
+        uint32_t bit = __ffs(t.tg.y & 0x00ffffffu) - 1u;
+        t.tg.y &= ~(1u << bit);
+        uint32_t ti = t.tg.x + bit;
+        const float4 *tp = s.tri_v + static_cast<size_t>(ti) * 3u;
+        float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float th, u, v;
+        if (intersect_triangle(r, a, b, c, 0.0f, t.tmax, th, u, v)) {
+            hit = true;
+            return true;
+        }
+    }
+    if (t.ng.y <= 0x00ffffffu) {
+        if (t.sp == 0) {
+            hit = false;
+            return true;
+        }
+        t.ng = stack[--t.sp];
+    }
+    return false;
+}
+
 }  // namespace vs

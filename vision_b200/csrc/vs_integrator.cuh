@@ -236,37 +236,70 @@ struct ShadowQuery {
 // add its contribution to ps.L; sq then stays invalid.  M: the material types
 // compiled in (kAllMaterials, or one class for the material-sorted wavefront
 // kernels, whose hits all have that type); M = 0 compiles the miss only.
-template <int N, bool kTraceShadow, uint32_t M = kAllMaterials>
-__device__ __forceinline__ bool path_shade(const DeviceScene &s, PathState<N> &ps, bool hit_any, const Hit &hit,
-                                           Interaction *first, ShadowQuery &sq) {
+//
+// path_shade_acc generalises the gathering: every contribution (spectral,
+// already weighted) goes through acc(ps, c) — RgbAcc adds its linear sRGB to
+// ps.L, SpecAcc sums the spectrum — and emit = false skips the emission of
+// the hit (a path suffix that starts at a vertex whose emission belongs to
+// the prefix).  Deferred shadow queries carry linear sRGB, so a spectral
+// accumulator needs kTraceShadow.
+template <int N>
+struct RgbAcc {
+    __device__ __forceinline__ void operator()(PathState<N> &ps, const Spec<N> &c) const {
+        ps.L += linear_srgb<N>(c, ps.wl);
+    }
+};
+template <int N>
+struct SpecAcc {
+    Spec<N> *sum;
+    __device__ __forceinline__ void operator()(PathState<N> &, const Spec<N> &c) const { *sum = *sum + c; }
+};
+
+// IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132): the
+// environment seen by a ray that left the scene, MIS-weighted against the
+// pdf of the direction it was sampled with.
+template <int N, class Acc>
+__device__ __forceinline__ void miss_emission(const DeviceScene &s, PathState<N> &ps, const Acc &acc) {
+    if (!s.has_env) return;
+    const IntegratorParams &ip = s.ip;
+    Spec<N> Le;
+    float lpdf;
+    env_eval<N>(s, normalize((ps.ro + ps.rd) - ps.ro), ps.wl, Le, lpdf);
+    lpdf *= light_pmf<N>(s, s.env_index);
+    float weight = ps.scatter_pdf / (ps.scatter_pdf + lpdf);
+    if (ip.mis_mode == 2u) weight = 1.0f;
+    else if (ip.mis_mode == 1u) weight = ps.bounce == 0 ? weight : 0.0f;
+    acc(ps, Le * ps.throughput * weight);
+}
+
+// Emission of the surface a ray hit (integrator.cpp:192-203), MIS-weighted.
+template <int N, class Acc>
+__device__ __forceinline__ void hit_emission(const DeviceScene &s, PathState<N> &ps, const Interaction &it,
+                                             const Acc &acc) {
+    if (it.light == kInvalid) return;
+    const IntegratorParams &ip = s.ip;
+    Spec<N> Le;
+    float lpdf;
+    eval_hit_light<N>(s, it, ps.ro, ps.wl, Le, lpdf);
+    float weight = ps.scatter_pdf / (ps.scatter_pdf + lpdf);
+    if (ip.mis_mode == 2u) weight = 1.0f;
+    else if (ip.mis_mode == 1u) weight = ps.bounce == 0 ? weight : 0.0f;
+    acc(ps, Le * ps.throughput * weight);
+}
+
+template <int N, bool kTraceShadow, uint32_t M, class Acc>
+__device__ __forceinline__ bool path_shade_acc(const DeviceScene &s, PathState<N> &ps, bool hit_any, const Hit &hit,
+                                               Interaction *first, ShadowQuery &sq, const Acc &acc, bool emit) {
     const IntegratorParams &ip = s.ip;
     const uint32_t bounce = ps.bounce;
     sq.valid = false;
     if (!hit_any || M == 0u) {
-        // IlluminationIntegrator::evaluate_miss (integrator.cpp:111-132).
-        if (s.has_env) {
-            Spec<N> Le;
-            float lpdf;
-            env_eval<N>(s, normalize((ps.ro + ps.rd) - ps.ro), ps.wl, Le, lpdf);
-            lpdf *= light_pmf<N>(s, s.env_index);
-            float weight = ps.scatter_pdf / (ps.scatter_pdf + lpdf);
-            if (ip.mis_mode == 2u) weight = 1.0f;
-            else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
-            ps.L += linear_srgb<N>(Le * ps.throughput * weight, ps.wl);
-        }
+        miss_emission<N>(s, ps, acc);
         return false;
     }
     Interaction it = surface_interaction(s, hit, ps.rd, true);
     if (first && bounce == 0) *first = it;
-    if (it.light != kInvalid) {
-        Spec<N> Le;
-        float lpdf;
-        eval_hit_light<N>(s, it, ps.ro, ps.wl, Le, lpdf);
-        float weight = ps.scatter_pdf / (ps.scatter_pdf + lpdf);
-        if (ip.mis_mode == 2u) weight = 1.0f;
-        else if (ip.mis_mode == 1u) weight = bounce == 0 ? weight : 0.0f;
-        ps.L += linear_srgb<N>(Le * ps.throughput * weight, ps.wl);
-    }
+    if (emit) hit_emission<N>(s, ps, it, acc);
     // Light sample: 1 draw for the light, 2 for the surface point.
     float u_light = ps.smp.next();
     f2 u_surf = ps.smp.next2();
@@ -286,7 +319,7 @@ __device__ __forceinline__ bool path_shade(const DeviceScene &s, PathState<N> &p
     if (kTraceShadow) {
         Spec<N> Ld = Spec<N>::fill(0.0f);
         if (!occluded && se.valid() && ls.pdf > 0.0f) Ld = ls.L * se.f * (w_mis / ls.pdf);
-        if (ip.mis_mode != 2u) ps.L += linear_srgb<N>(ps.throughput * Ld, ps.wl);
+        if (ip.mis_mode != 2u) acc(ps, ps.throughput * Ld);
     } else if (ip.mis_mode != 2u && se.valid() && ls.pdf > 0.0f) {
         Spec<N> Ld = ls.L * se.f * (w_mis / ls.pdf);
         sq.o = sh.o;
@@ -312,6 +345,12 @@ __device__ __forceinline__ bool path_shade(const DeviceScene &s, PathState<N> &p
     ps.ro = nr.o;
     ps.rd = nr.d;
     return true;
+}
+
+template <int N, bool kTraceShadow, uint32_t M = kAllMaterials>
+__device__ __forceinline__ bool path_shade(const DeviceScene &s, PathState<N> &ps, bool hit_any, const Hit &hit,
+                                           Interaction *first, ShadowQuery &sq) {
+    return path_shade_acc<N, kTraceShadow, M>(s, ps, hit_any, hit, first, sq, RgbAcc<N>{}, true);
 }
 
 // One iteration of the bounce loop: closest hit, shading, shadow ray.

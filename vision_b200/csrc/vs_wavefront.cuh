@@ -58,6 +58,30 @@ __device__ __forceinline__ uint32_t load(const Scenes &scenes, const WfBuffers &
     return st.w;
 }
 
+// Camera paths of a wave: slot i holds path base + i of `cam` (frame-major
+// over frames frame_begin, ...), queued for the first bounce; clears every
+// counter of the wave.  A scene of max_depth 0 writes each path's (zero)
+// radiance directly.
+template <int N>
+__device__ __forceinline__ void generate(const DeviceScene &s, const Camera &cam, const WfBuffers &b,
+                                         uint32_t frame_begin, uint64_t base, uint32_t n, float4 *radiance) {
+    const uint32_t npix = cam.width * cam.height;
+    if (blockIdx.x == 0 && threadIdx.x < kWfCounters) b.count[threadIdx.x] = threadIdx.x == 0 ? n : 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t p = base + i;
+        const uint32_t frame = frame_begin + static_cast<uint32_t>(p / npix);
+        const uint32_t pix = static_cast<uint32_t>(p % npix);
+        PathState<N> ps;
+        path_start<N>(s, cam, pix % cam.width, pix / cam.width, frame, ps);
+        if (s.ip.max_depth == 0u) {
+            radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            continue;
+        }
+        store<N>(b, i, ps, 0u);
+        b.queue[0][i] = i;
+    }
+}
+
 // Appends one entry per calling lane to a device queue: one atomicAdd per
 // converged group of lanes, positions in lane order.
 __device__ __forceinline__ uint32_t queue_push(uint32_t *counter) {
@@ -83,34 +107,72 @@ __device__ __forceinline__ uint32_t class_push(uint32_t *counts, uint32_t cls) {
     return base + static_cast<uint32_t>(__popc(group & ((1u << lane) - 1u)));
 }
 
-// Closest hits of queue `cur`, sorted into the shading-class queues.  Also
-// clears the other path queue and the shadow queue for the shading pass that
-// follows (their previous users have finished: kernels of one stream run in
-// order; the class counters were cleared by the previous shadow pass or by
-// the wave's generate kernel).
+// Lanes of a warp that must be idle before the warp takes new rays.
+#ifndef VS_REFILL_LANES
+#define VS_REFILL_LANES 8
+#endif
+
+// Ray replacement for the traversal kernels: the idle lanes of a warp (at
+// least VS_REFILL_LANES of them, or all) claim the next rays of a queue of `n`
+// with one atomicAdd on `fetch`; returns the claimed index of the calling
+// lane (>= n: none) and sets `drained` once the queue is exhausted.  Called by
+// all 32 lanes.
+__device__ __forceinline__ uint32_t refill(uint32_t *fetch, uint32_t n, bool active, bool &drained) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    const uint32_t k = static_cast<uint32_t>(__popc(idle));
+    if (k < VS_REFILL_LANES && k != 32u) return n;
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int leader = __ffs(idle) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(fetch, k);
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (base + k >= n) drained = true;
+    if (active) return n;
+    return base + static_cast<uint32_t>(__popc(idle & ((1u << lane) - 1u)));
+}
+
+// Closest hits of queue `cur`, sorted into the shading-class queues.  Each
+// warp keeps 32 rays in flight and refills finished lanes from the queue.
+// Also clears the other path queue, the shadow queue and the shadow fetch
+// counter for the passes that follow (their previous users have finished:
+// kernels of one stream run in order; the class counters and this kernel's
+// fetch counter were cleared by the previous shadow pass or by the wave's
+// generate kernel).
 template <class Scenes>
 __device__ __forceinline__ void extend(const Scenes &scenes, const WfBuffers &b, uint32_t cur) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         b.count[cur ^ 1u] = 0u;
         b.count[2] = 0u;
+        b.count[kWfFetchShadow] = 0u;
     }
     const uint32_t n = b.count[cur];
     const uint32_t *q = b.queue[cur];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = q[i];
-        const float4 o = b.o[slot], d = b.d[slot];
-        const DeviceScene &s = scenes(b.st[slot].w);
-        RayPre rp = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
-        Hit h;
-        float t;
-        uint32_t cls = 0u;
-        if (trace_closest(s, rp, 3.402823466e+38f, h, t)) {
-            cls = 1u + s.materials[s.instances[h.inst_id].mat_id].type;
-        } else {
-            h = Hit{kInvalid, kInvalid, 0.0f, 0.0f};
+    uint2 stack[kStackSize];
+    bool active = false, drained = false;
+    uint32_t slot = 0;
+    const DeviceScene *s = nullptr;
+    RayPre r;
+    TravState t;
+    for (;;) {
+        if (!drained) {
+            const uint32_t i = refill(b.count + kWfFetchExtend, n, active, drained);
+            if (i < n) {
+                slot = q[i];
+                const float4 o = b.o[slot], d = b.d[slot];
+                s = &scenes(b.st[slot].w);
+                r = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
+                trav_init(t, r, 3.402823466e+38f);
+                active = true;
+            }
         }
-        b.hit[slot] = h;
-        b.tq[static_cast<size_t>(cls) * b.capacity + class_push(b.count + 3, cls)] = slot;
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active && closest_step(*s, r, t, stack)) {
+            const Hit h = trav_hit(*s, t);
+            const uint32_t cls = h.inst_id == kInvalid ? 0u : 1u + s->materials[s->instances[h.inst_id].mat_id].type;
+            b.hit[slot] = h;
+            b.tq[static_cast<size_t>(cls) * b.capacity + class_push(b.count + 3, cls)] = slot;
+            active = false;
+        }
     }
 }
 
@@ -155,27 +217,49 @@ __device__ __forceinline__ void shade(const Scenes &scenes, const WfBuffers &b, 
     }
 }
 
-// Shadow queries of the bounce: add the contribution when unoccluded; write
-// the radiance of paths that ended at this bounce.  Clears the class
-// counters for the next bounce (every shading pass of this one has finished).
+// Shadow queries of the bounce (with ray replacement, as extend): add the
+// contribution when unoccluded; write the radiance of paths that ended at
+// this bounce.  Clears the class counters and the extend fetch counter for
+// the next bounce (every shading pass of this one has finished).
 template <class Scenes>
 __device__ __forceinline__ void shadow(const Scenes &scenes, const WfBuffers &b, uint64_t base, float4 *radiance) {
     if (blockIdx.x == 0 && threadIdx.x < kWfClasses) b.count[3 + threadIdx.x] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 32) b.count[kWfFetchExtend] = 0u;
     const uint32_t n = b.count[2];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = b.sh_o[i], d = b.sh_d[i], c = b.sh_c[i];
-        const uint32_t tag = __float_as_uint(d.w);
-        const uint32_t slot = tag & 0x7fffffffu;
-        const DeviceScene &s = scenes(__float_as_uint(c.w));
-        const bool occluded = trace_any(s, precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z)), o.w);
-        float4 L = b.L[slot];
-        if (!occluded) {
-            f3 l = make3(L.x, L.y, L.z);
-            l += make3(c.x, c.y, c.z);
-            L = make_float4(l.x, l.y, l.z, 0.0f);
-            b.L[slot] = L;
+    uint2 stack[kStackSize];
+    bool active = false, drained = false;
+    uint32_t i = 0;
+    const DeviceScene *s = nullptr;
+    RayPre r;
+    TravState t;
+    for (;;) {
+        if (!drained) {
+            const uint32_t k = refill(b.count + kWfFetchShadow, n, active, drained);
+            if (k < n) {
+                i = k;
+                const float4 o = b.sh_o[i], d = b.sh_d[i];
+                s = &scenes(__float_as_uint(b.sh_c[i].w));
+                r = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
+                trav_init(t, r, o.w);
+                active = true;
+            }
         }
-        if (tag & 0x80000000u) radiance[base + slot] = make_float4(L.x, L.y, L.z, 1.0f);
+        if (!__any_sync(0xffffffffu, active)) break;
+        bool occluded = false;
+        if (active && any_step(*s, r, t, stack, occluded)) {
+            const uint32_t tag = __float_as_uint(b.sh_d[i].w);
+            const uint32_t slot = tag & 0x7fffffffu;
+            float4 L = b.L[slot];
+            if (!occluded) {
+                const float4 c = b.sh_c[i];
+                f3 l = make3(L.x, L.y, L.z);
+                l += make3(c.x, c.y, c.z);
+                L = make_float4(l.x, l.y, l.z, 0.0f);
+                b.L[slot] = L;
+            }
+            if (tag & 0x80000000u) radiance[base + slot] = make_float4(L.x, L.y, L.z, 1.0f);
+            active = false;
+        }
     }
 }
 

@@ -29,13 +29,16 @@ struct WfBuffers {
     float4 *sh_c;    // contribution when unoccluded (linear sRGB), w: scene id
     uint32_t *tq;    // hits sorted by shading class: class c at tq[c * capacity]
     uint32_t *count; // [0], [1]: path queue lengths; [2]: shadow queue length;
-                     // [3 + c]: length of shading class c
+                     // [3 + c]: length of shading class c; [kWfFetchExtend],
+                     // [kWfFetchShadow]: rays handed out by the traversal kernels
 };
 
 // Shading classes of a hit: 0 = miss, 1 + MaterialType otherwise.  Each class
 // is shaded by its own kernel, compiled with that material's code only.
 constexpr uint32_t kWfClasses = 6;
-constexpr uint32_t kWfCounters = 3 + kWfClasses;
+constexpr uint32_t kWfFetchExtend = 3 + kWfClasses;
+constexpr uint32_t kWfFetchShadow = kWfFetchExtend + 1;
+constexpr uint32_t kWfCounters = kWfFetchShadow + 1;
 
 // Bytes of device memory per slot of WfBuffers.
 constexpr size_t kWfBytesPerSlot = 6 * 16 + 16 + 16 + 2 * 4 + 3 * 16 + kWfClasses * 4;

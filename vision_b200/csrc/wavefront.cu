@@ -38,21 +38,7 @@ template <int N>
 __global__ void __launch_bounds__(128) k_wf_generate(const __grid_constant__ DeviceScene s,
                                                      const __grid_constant__ WfBuffers b, uint32_t frame_begin,
                                                      uint64_t base, uint32_t n, float4 *radiance) {
-    const uint32_t npix = s.cam.width * s.cam.height;
-    if (blockIdx.x == 0 && threadIdx.x < kWfCounters) b.count[threadIdx.x] = threadIdx.x == 0 ? n : 0u;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint64_t p = base + i;
-        const uint32_t frame = frame_begin + static_cast<uint32_t>(p / npix);
-        const uint32_t pix = static_cast<uint32_t>(p % npix);
-        PathState<N> ps;
-        path_start<N>(s, s.cam, pix % s.cam.width, pix / s.cam.width, frame, ps);
-        if (s.ip.max_depth == 0u) {
-            radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-            continue;
-        }
-        wf::store<N>(b, i, ps, 0u);
-        b.queue[0][i] = i;
-    }
+    wf::generate<N>(s, s.cam, b, frame_begin, base, n, radiance);
 }
 
 __global__ void __launch_bounds__(128) k_wf_extend(const __grid_constant__ DeviceScene s,
