@@ -893,7 +893,17 @@ int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void
     };
     if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
     unsigned n = 0;
-    VS_CUDA(launch_rt_frame(s->device_view(), p, s->rt.view(), film_index, s->film32.ptr, st, &n), "restir launch");
+    const uint64_t rt_npix = static_cast<uint64_t>(p.width) * p.height;
+    const bool wavefront = s->schedule == VS_SCHEDULE_WAVEFRONT && rt_npix <= kWfWaveSlots;
+    WfBuffers wfv{};
+    if (wavefront) {
+        VS_CUDA(s->wf.ensure(static_cast<uint32_t>(rt_npix)), "wavefront slots alloc");
+        VS_CUDA(s->radiance.alloc(rt_npix), "radiance alloc");
+        wfv = s->wf.view();
+    }
+    VS_CUDA(launch_rt_frame(s->device_view(), p, s->rt.view(), film_index, s->film32.ptr, wavefront ? &wfv : nullptr,
+                            wavefront ? s->radiance.ptr : nullptr, shading_classes(s->host), st, &n),
+            "restir launch");
     add_launches(n);
     if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
     if (st != ctx->stream) {

@@ -14,9 +14,11 @@
 // wavelengths: the reference's ReSTIR code moves spectra through float3
 // (SampledSpectrum::vec3, SampledSpectrum(Float3)), which is only defined for
 // three channels.
-#include "vs_integrator.cuh"
+#include "vs_wavefront.cuh"
 #include "vs_launch.h"
 #include "vs_restir.h"
+
+#include <algorithm>
 
 namespace vs {
 
@@ -595,8 +597,16 @@ __global__ void k_rt_reset(uint32_t npix, const __grid_constant__ RtBuffers b) {
     b.gi_radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
+// Minimum resident blocks per SM of the candidate and spatial kernels
+// (register budget; 1 leaves the compiler free).
+#ifndef VS_RT_MIN_BLOCKS
+#define VS_RT_MIN_BLOCKS 1
+#endif
+
 // ReSTIRDI shader0 (direct.cpp:519-557).
-__global__ void __launch_bounds__(128) k_di_candidates(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_di_candidates(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                    const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -717,7 +727,9 @@ __device__ VS_OUTLINE f3 di_shading(const DeviceScene &s, const RtParams &p, con
 }  // namespace
 
 // ReSTIRDI shader1 (direct.cpp:638-674).
-__global__ void __launch_bounds__(128) k_di_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_di_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                 const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -842,6 +854,134 @@ __global__ void __launch_bounds__(128) k_gi_initial(const __grid_constant__ Devi
     b.gi_init[idx] = g;
 }
 
+// ---------------------------------------------------------------------------
+// The initial indirect samples in wavefront form: k_gi_initial's path suffix
+// (path_li from the DI pass's BSDF sample) as wavefront passes over one slot
+// per pixel (slot = pixel index; the queue counters are cleared before the
+// start kernel).  k_gi_wf_start builds each path and writes the pixel's sample
+// with zero radiance; k_gi_wf_first records the first
+// vertex of the suffix after the bounce-0 closest hits; the bounce passes
+// leave each path's radiance in `radiance`; k_gi_wf_finish divides by the
+// BSDF weight as k_gi_initial does.  Same draws and sums as path_li, so the
+// samples are k_gi_initial's.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct RtScene {
+    const DeviceScene *s;
+    __device__ __forceinline__ const DeviceScene &operator()(uint32_t) const { return *s; }
+};
+
+// The pixel's surface, view position and near-specular chain throughput;
+// false when the camera ray left the scene.
+__device__ __forceinline__ bool gi_surface(const DeviceScene &s, const RtParams &p, const RtBuffers &b,
+                                           uint32_t idx, Interaction &it, f3 &tp_chain) {
+    const uint32_t cur = (p.frame + 1u) & 1u;
+    RtSurface cs = b.surf[cur][idx];
+    if (cs.hit.inst_id == kInvalid) return false;
+    f3 view_pos = p.view_pos;
+    tp_chain = make3(1.0f);
+    if (cs.is_replaced) {
+        RtSurfaceExt e = b.ext[cur][idx];
+        view_pos = make3(e.vx, e.vy, e.vz);
+        tp_chain = make3(e.tx, e.ty, e.tz);
+    }
+    it = it_at(s, cs.hit, view_pos);
+    return true;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_gi_wf_start(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ RtParams p,
+                                                     const __grid_constant__ RtBuffers b,
+                                                     const __grid_constant__ WfBuffers w) {
+    const uint32_t npix = p.width * p.height;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npix; idx += gridDim.x * blockDim.x) {
+        const uint32_t x = idx % p.width, y = idx / p.width;
+        Interaction it;
+        f3 tp_chain;
+        if (!gi_surface(s, p, b, idx, it, tp_chain)) {
+            b.gi_radiance[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
+        const RtHitBsdf hb = b.hit_bsdf[idx];
+        PathState<RN> ps;
+        ps.smp.start(x, y, p.frame, 3u, s.ip.sampler, s.ip.seed);
+        ps.wl = pixel_wavelengths(s, x, y, p.frame);
+        const Ray ray = spawn_ray(it.pos, it.ng, make3(hb.wx, hb.wy, hb.wz));
+        const f3 tp = zero_if_nan_inf(make3(hb.fx, hb.fy, hb.fz) / hb.pdf);
+        ps.ro = ray.o;
+        ps.rd = ray.d;
+        ps.scatter_pdf = hb.pdf;
+        ps.throughput = spec3(tp);
+        ps.L = make3(0.0f);
+        ps.eta_scale = 1.0f;
+        ps.bounce = 0;
+        GiReservoir g{};
+        b.gi_init[idx] = g;
+        if (p.gi_max_depth == 0u) continue;
+        wf::store<RN>(w, idx, ps, 0u);
+        w.queue[0][wf::queue_push(&w.count[0])] = idx;
+    }
+}
+
+// The first vertex of each suffix (the HitContext of path_li) after the
+// bounce-0 closest hits.
+__global__ void __launch_bounds__(128) k_gi_wf_first(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ RtBuffers b,
+                                                     const __grid_constant__ WfBuffers w) {
+    const uint32_t n = w.count[0];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = w.queue[0][i];
+        const Hit h = w.hit[slot];
+        if (h.inst_id == kInvalid) continue;
+        const float4 d = w.d[slot];
+        const Interaction it = surface_interaction(s, h, make3(d.x, d.y, d.z), true);
+        GiReservoir g{};
+        st3(g.sp_pos, it.pos);
+        st3(g.sp_ng, it.ng);
+        b.gi_init[slot] = g;
+    }
+}
+
+template <uint32_t C>
+__global__ void __launch_bounds__(128) k_gi_wf_shade(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ WfBuffers w, uint32_t cur,
+                                                     float4 *radiance) {
+    wf::shade<RN, C>(RtScene{&s}, w, cur, 0, radiance);
+}
+
+__global__ void __launch_bounds__(128) k_gi_wf_extend(const __grid_constant__ DeviceScene s,
+                                                      const __grid_constant__ WfBuffers w, uint32_t cur) {
+    wf::extend(RtScene{&s}, w, cur);
+}
+
+__global__ void __launch_bounds__(128) k_gi_wf_shadow(const __grid_constant__ DeviceScene s,
+                                                      const __grid_constant__ WfBuffers w, float4 *radiance) {
+    wf::shadow(RtScene{&s}, w, 0, radiance);
+}
+
+// Radiance of each suffix over the BSDF weight, times the chain throughput.
+__global__ void __launch_bounds__(128) k_gi_wf_finish(const __grid_constant__ DeviceScene s,
+                                                      const __grid_constant__ RtParams p,
+                                                      const __grid_constant__ RtBuffers b, const float4 *radiance) {
+    const uint32_t npix = p.width * p.height;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npix; idx += gridDim.x * blockDim.x) {
+        Interaction it;
+        f3 tp_chain;
+        if (!gi_surface(s, p, b, idx, it, tp_chain)) continue;
+        const RtHitBsdf hb = b.hit_bsdf[idx];
+        const f3 tp = zero_if_nan_inf(make3(hb.fx, hb.fy, hb.fz) / hb.pdf);
+        f3 L = make3(0.0f);
+        if (p.gi_max_depth != 0u) L = make3(radiance[idx].x, radiance[idx].y, radiance[idx].z);
+        L = zero_if_nan_inf(make3(L.x / tp.x, L.y / tp.y, L.z / tp.z));
+        GiReservoir g = b.gi_init[idx];
+        st3(g.Lo, L * tp_chain);
+        b.gi_init[idx] = g;
+    }
+}
+
 // ReSTIRGI temporal pass (indirect.cpp:155-236).
 __global__ void __launch_bounds__(128) k_gi_temporal(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
@@ -909,7 +1049,9 @@ __global__ void __launch_bounds__(128) k_gi_temporal(const __grid_constant__ Dev
 }
 
 // ReSTIRGI spatial reuse and shading (indirect.cpp:238-332).
-__global__ void __launch_bounds__(128) k_gi_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_gi_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                 const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -988,8 +1130,22 @@ cudaError_t launch_rt_reset(uint32_t npix, const RtBuffers &b, cudaStream_t st) 
     return cudaGetLastError();
 }
 
+namespace {
+
+template <typename K>
+unsigned rt_wave_grid(K kernel) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
+    return static_cast<unsigned>(std::max(1, sms * std::max(per_sm, 1)));
+}
+
+}  // namespace
+
 cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuffers &b, uint32_t film_index,
-                            float4 *film, cudaStream_t st, unsigned *launches) {
+                            float4 *film, const WfBuffers *wf, float4 *radiance, uint32_t class_mask, cudaStream_t st,
+                            unsigned *launches) {
     dim3 block(16, 8);
     dim3 grid((p.width + 15) / 16, (p.height + 7) / 8);
     unsigned n = 0;
@@ -999,10 +1155,51 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
         k_di_spatial<<<grid, block, 0, st>>>(s, p, b);
         ++n;
     }
-    k_gi_initial<<<grid, block, 0, st>>>(s, p, b);
+    if (wf && radiance) {
+        static unsigned g_ext = 0, g_shadow = 0, g_shade[kWfClasses] = {};
+        if (!g_ext) {
+            g_ext = rt_wave_grid(k_gi_wf_extend);
+            g_shadow = rt_wave_grid(k_gi_wf_shadow);
+            g_shade[0] = rt_wave_grid(k_gi_wf_shade<0>);
+            g_shade[1] = rt_wave_grid(k_gi_wf_shade<1>);
+            g_shade[2] = rt_wave_grid(k_gi_wf_shade<2>);
+            g_shade[3] = rt_wave_grid(k_gi_wf_shade<3>);
+            g_shade[4] = rt_wave_grid(k_gi_wf_shade<4>);
+            g_shade[5] = rt_wave_grid(k_gi_wf_shade<5>);
+        }
+        const uint32_t np = p.width * p.height;
+        const unsigned g_pix = (np + 127) / 128;
+        const uint32_t mask = class_mask | 1u;
+        cudaError_t e = cudaMemsetAsync(wf->count, 0, sizeof(uint32_t) * kWfCounters, st);
+        if (e != cudaSuccess) return e;
+        k_gi_wf_start<<<g_pix, 128, 0, st>>>(s, p, b, *wf);
+        ++n;
+        for (uint32_t bounce = 0; bounce < p.gi_max_depth; ++bounce) {
+            const uint32_t cur = bounce & 1u;
+            k_gi_wf_extend<<<g_ext, 128, 0, st>>>(s, *wf, cur);
+            ++n;
+            if (bounce == 0) {
+                k_gi_wf_first<<<g_ext, 128, 0, st>>>(s, b, *wf);
+                ++n;
+            }
+            if (mask & 1u) { k_gi_wf_shade<0><<<g_shade[0], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
+            if (mask & 2u) { k_gi_wf_shade<1><<<g_shade[1], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
+            if (mask & 4u) { k_gi_wf_shade<2><<<g_shade[2], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
+            if (mask & 8u) { k_gi_wf_shade<3><<<g_shade[3], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
+            if (mask & 16u) { k_gi_wf_shade<4><<<g_shade[4], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
+            if (mask & 32u) { k_gi_wf_shade<5><<<g_shade[5], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
+            k_gi_wf_shadow<<<g_shadow, 128, 0, st>>>(s, *wf, radiance);
+            ++n;
+        }
+        k_gi_wf_finish<<<g_pix, 128, 0, st>>>(s, p, b, radiance);
+        ++n;
+    } else {
+        k_gi_initial<<<grid, block, 0, st>>>(s, p, b);
+        ++n;
+    }
     k_gi_temporal<<<grid, block, 0, st>>>(s, p, b);
     k_gi_spatial<<<grid, block, 0, st>>>(s, p, b);
-    n += 3;
+    n += 2;
     uint32_t npix = p.width * p.height;
     k_rt_combine<<<(npix + 255) / 256, 256, 0, st>>>(npix, b, p.di_factor, p.gi_factor, film_index, film);
     ++n;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include "vs_devscene.h"
 #include "vs_restir.h"
+#include "vs_wavefront.h"
 
 namespace vs {
 
@@ -27,8 +28,12 @@ cudaError_t upload_spectral_consts_serve(const float *x, const float *y, const f
 // restir.cu
 cudaError_t upload_spectral_consts_rt(const float *x, const float *y, const float *z, const float *d65, float y_integral);
 cudaError_t launch_rt_reset(uint32_t npix, const RtBuffers &b, cudaStream_t st);
+// wf / radiance (one slot and one float4 per pixel): when given, the initial
+// indirect samples run as wavefront passes (class_mask as for the plain
+// wavefront); otherwise as the one-kernel k_gi_initial.
 cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuffers &b, uint32_t film_index,
-                            float4 *film, cudaStream_t st, unsigned *launches);
+                            float4 *film, const WfBuffers *wf, float4 *radiance, uint32_t class_mask, cudaStream_t st,
+                            unsigned *launches);
 cudaError_t launch_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out, cudaStream_t st);
 
 }  // namespace vs
