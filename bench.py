@@ -68,7 +68,10 @@ DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64, 'serving'
 # DRAM bytes per path of k_render measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch divided by its paths; profiles/).
 NCU_TRAFFIC_PER_PATH = {('large_scene', 'persistent'): 383.6e6 / 2097152,
-                        ('box_room', 'persistent'): 7.42e6 / 1048576}
+                        ('box_room', 'persistent'): 7.42e6 / 1048576,
+                        # all wavefront kernels of one render (2,097,152 and 1,048,576 paths)
+                        ('large_scene', 'wavefront'): 3017.6e6 / 2097152,
+                        ('box_room', 'wavefront'): 1990.0e6 / 1048576}
 
 # Algorithmic bytes per pixel-frame of the ReSTIR frame, from the record sizes
 # (64 B surfaces and reservoirs, 32 B extensions and BSDF samples, 16 B
@@ -392,7 +395,8 @@ def main():
                      'traffic': (NCU_TRAFFIC_PER_PATH[(args.workload, args.schedule)] * paths_per_step * args.steps /
                                  max(render_launches, 1)
                                  if (args.workload, args.schedule) in NCU_TRAFFIC_PER_PATH else None),
-                     'traffic_source': 'ncu dram bytes per path of the committed profile x paths per launch',
+                     'traffic_source': 'ncu dram bytes per path of the committed profile (all kernels of the '
+                                       'schedule for one render) x paths per launch',
                      'kernel': {'persistent': 'k_render_regen', 'grid': 'k_render',
                                 'wavefront': 'wavefront (k_wf_extend, k_wf_shade, k_wf_shadow)'}[args.schedule],
                      'bytes_per_path': bytes_per_path,

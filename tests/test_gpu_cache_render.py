@@ -88,12 +88,20 @@ def test_wavefront_cache_frame_matches_one_kernel_frame(vb, gpu_ctx, room):
     both = a['valid'] & b['valid']
     assert both.mean() > 0.3
 
+    # Features are BF16 codes (compared exactly); records and targets are
+    # FP32 sums whose last bits depend on how each kernel's multiply-adds were
+    # contracted (compared to 1e-4 relative).
     def rows_equal(x, y):
         return np.all(x == y, axis=-1).mean()
+
+    def rows_close(x, y):
+        return np.all(np.abs(x - y) <= 1e-6 + 1e-4 * np.abs(x), axis=-1).mean()
     assert rows_equal(a['qf'][both], b['qf'][both]) >= 0.99
-    assert rows_equal(a['rec'][both], b['rec'][both]) >= 0.99
-    for k in ('tf', 'bf', 'tg', 'sv'):
+    assert rows_close(a['rec'][both], b['rec'][both]) >= 0.99
+    for k in ('tf', 'bf'):
         assert rows_equal(a[k], b[k]) >= 0.98, k
+    for k in ('tg', 'sv'):
+        assert rows_close(a[k], b[k]) >= 0.98, k
     close = np.abs(a['film'] - b['film']) <= 1e-4 + 1e-3 * np.abs(a['film'])
     assert close.all(-1).mean() >= 0.99
     assert abs(a['film'][..., :3].mean() - b['film'][..., :3].mean()) <= 1e-3 * a['film'][..., :3].mean()

@@ -597,10 +597,12 @@ __global__ void k_rt_reset(uint32_t npix, const __grid_constant__ RtBuffers b) {
     b.gi_radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-// Minimum resident blocks per SM of the candidate and spatial kernels
-// (register budget; 1 leaves the compiler free).
+// Minimum resident blocks per SM of the candidate and spatial kernels (a
+// register budget).  3 blocks of 128 (at most 170 registers) measured 5 %
+// faster on the many-light frame than the compiler's own 207 registers
+// (2 blocks), despite the spills it causes in k_di_spatial.
 #ifndef VS_RT_MIN_BLOCKS
-#define VS_RT_MIN_BLOCKS 1
+#define VS_RT_MIN_BLOCKS 3
 #endif
 
 // ReSTIRDI shader0 (direct.cpp:519-557).
