@@ -413,11 +413,12 @@ __device__ VS_OUTLINE DiReservoir di_ris(const DeviceScene &s, const RtParams &p
     Bsdf<RN> bsdf = bsdf_at(s, it, wl);
     float lum_tp = lum3(throughput);
     float Ml = static_cast<float>(p.M_light), Mb = static_cast<float>(p.M_bsdf);
-    for (uint32_t i = 0; i < p.M_light; ++i) {
-        // LightSampler::sample_only (lightsampler.cpp:218-228), AreaLight::sample_only (area.cpp:134-140).
-        DiReservoir cand = di_empty();
-        uint32_t li = select_light(s, smp.next());
-        f2 u = smp.next2();
+    // LightSampler::sample_only (lightsampler.cpp:218-228), AreaLight::sample_only
+    // (area.cpp:134-140): one light candidate from its three draws, with its
+    // target pdf and RIS weight.
+    auto candidate = [&](float u_sel, f2 u, DiReservoir &cand, float &weight) {
+        cand = di_empty();
+        uint32_t li = select_light(s, u_sel);
         AreaLight L = s.lights[li];
         float ux = u.x;
         uint32_t local = alias_sample(s.prim_alias + L.alias_offset, L.prim_count, u.x, &ux);
@@ -432,8 +433,35 @@ __device__ VS_OUTLINE DiReservoir di_ris(const DeviceScene &s, const RtParams &p
         st3(cand.pos, ls.p_light);
         float light_pdf = ls.pdf;
         float mis = light_pdf / (Ml * light_pdf + Mb * bsdf_pdf_point);
-        float weight = safe_weight(mis, cand.p_hat, 1.0f / light_pdf) * lum_tp;
-        di_update(ret, smp.next(), cand, weight);
+        weight = safe_weight(mis, cand.p_hat, 1.0f / light_pdf) * lum_tp;
+    };
+    // Candidates in pairs: the draws of a pair are taken in the reference's
+    // order (selection, surface point, reservoir update of the first, then
+    // of the second) before either candidate is evaluated, so the two
+    // candidates' dependent fetches (light table, primitive table, vertices)
+    // are in flight together; the reservoir sees them in the same order.
+    uint32_t i = 0;
+    for (; i + 1 < p.M_light; i += 2) {
+        const float s0 = smp.next();
+        const f2 u0 = smp.next2();
+        const float r0 = smp.next();
+        const float s1 = smp.next();
+        const f2 u1 = smp.next2();
+        const float r1 = smp.next();
+        DiReservoir c0, c1;
+        float w0, w1;
+        candidate(s0, u0, c0, w0);
+        candidate(s1, u1, c1, w1);
+        di_update(ret, r0, c0, w0);
+        di_update(ret, r1, c1, w1);
+    }
+    if (i < p.M_light) {
+        const float s0 = smp.next();
+        const f2 u0 = smp.next2();
+        DiReservoir c0;
+        float w0;
+        candidate(s0, u0, c0, w0);
+        di_update(ret, smp.next(), c0, w0);
     }
     for (uint32_t i = 0; i < p.M_bsdf; ++i) {
         // ReSTIRDI::Li from a BSDF sample (direct.cpp:39-114).

@@ -366,11 +366,8 @@ struct NodeHits {
     uint32_t tri_hits;       // bits 0..23: triangles of the leaf children that were hit
 };
 
-// Byte i of w as a float, exactly: the byte placed in the low mantissa bits
-// of 2^23 (one byte permute) minus 2^23 (one FP32 add), instead of an
-// integer-to-float conversion, whose pipe has an eighth of the FP32 rate.
 __device__ __forceinline__ float ubyte(uint32_t w, int i) {
-    return __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + static_cast<uint32_t>(i))), 8388608.0f);
+    return static_cast<float>((w >> (8 * i)) & 0xffu);
 }
 
 // Tests the 8 children of one node; returns the new node and triangle groups.
