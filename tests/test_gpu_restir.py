@@ -32,10 +32,17 @@ def _run(vb, ctx, sc, cams, w, h):
         yield f, s, ort
 
 
-def test_restir_frames_match_oracle(vb, gpu_ctx):
+@pytest.mark.parametrize('materials', ['diffuse', 'metal'])
+def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
+    # 'diffuse': diffuse walls and emitters (the kernels compiled for those
+    # materials alone); 'metal': a gold box as well (the general kernels).
     w, h = 96, 64
     sc = scenes.many_lights(w, h, emitters=300, seed=5, M_light=8, history_limit=20, spatial_neighbours=5,
                             spatial_radius=12.0, max_depth=4)
+    if materials == 'metal':
+        for m in sc['materials']:
+            if m['name'] == 'TallBox':
+                m.update({'type': 'metal', 'param': {'material_name': 'Au', 'roughness': 0.3}})
     cams = scenes.camera_spline(6, seed=3)
     for f, s, ort in _run(vb, gpu_ctx, sc, cams, w, h):
         gs, cs = s.restir_buffer('surfaces'), ort.buffer('surfaces', vb.RT_SURFACE_DTYPE)

@@ -111,7 +111,8 @@ __device__ __forceinline__ float4 wl4(const CWl &w, bool pdf) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ DeviceScene s, const __grid_constant__ CacheFrameParams p) {
+__global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ CacheFrameParams p) {
     const uint32_t npix = s.cam.width * s.cam.height;
     const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= npix) return;

@@ -274,7 +274,8 @@ int upload_scene(vs_scene *s) {
     if (!ctx->consts_uploaded) {
         const Cie5 &c = cie5();
         VS_CUDA(upload_spectral_consts(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
-        VS_CUDA(upload_spectral_consts_rt(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        VS_CUDA(rt_all::upload_spectral_consts_rt(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        VS_CUDA(rt_diffuse::upload_spectral_consts_rt(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_serve(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_cache(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_wf(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
@@ -859,7 +860,7 @@ int rt_ensure(vs_scene *s, cudaStream_t st) {
     r.height = hgt;
     r.have_prev = false;
     r.rendered = false;
-    VS_CUDA(launch_rt_reset(static_cast<uint32_t>(n), r.view(), st), "restir reset");
+    VS_CUDA(rt_all::launch_rt_reset(static_cast<uint32_t>(n), r.view(), st), "restir reset");
     add_launches(1);
     return VS_OK;
 }
@@ -901,8 +902,13 @@ int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void
         VS_CUDA(s->radiance.alloc(rt_npix), "radiance alloc");
         wfv = s->wf.view();
     }
-    VS_CUDA(launch_rt_frame(s->device_view(), p, s->rt.view(), film_index, s->film32.ptr, wavefront ? &wfv : nullptr,
-                            wavefront ? s->radiance.ptr : nullptr, shading_classes(s->host), st, &n),
+    // Scenes of diffuse surfaces and emitters only take the kernels compiled
+    // for those materials alone.
+    const uint32_t classes = shading_classes(s->host);
+    const uint32_t diffuse_only = 1u | (1u << (1u + kMatDiffuse)) | (1u << (1u + kMatBlackBody));
+    auto launch = (classes & ~diffuse_only) == 0u ? rt_diffuse::launch_rt_frame : rt_all::launch_rt_frame;
+    VS_CUDA(launch(s->device_view(), p, s->rt.view(), film_index, s->film32.ptr, wavefront ? &wfv : nullptr,
+                   wavefront ? s->radiance.ptr : nullptr, classes, st, &n),
             "restir launch");
     add_launches(n);
     if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
@@ -932,7 +938,7 @@ int vs_restir_reset(vs_scene *s) {
     if (ctx->device < 0 || !s->rt.surf[0].ptr) return VS_OK;
     VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     size_t n = static_cast<size_t>(s->rt.width) * s->rt.height;
-    VS_CUDA(launch_rt_reset(static_cast<uint32_t>(n), s->rt.view(), ctx->stream), "restir reset");
+    VS_CUDA(rt_all::launch_rt_reset(static_cast<uint32_t>(n), s->rt.view(), ctx->stream), "restir reset");
     add_launches(1);
     return VS_OK;
 }

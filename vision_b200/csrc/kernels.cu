@@ -18,8 +18,8 @@ static std::atomic<unsigned long long> g_launches{0};
 unsigned long long launch_count() { return g_launches.load(); }
 void add_launches(unsigned n) { g_launches += n; }
 
-__global__ void __launch_bounds__(128) k_trace_closest(const __grid_constant__ DeviceScene s, const float *rays, uint32_t n, Hit *hits,
-                                                       float *t_out) {
+__global__ void __launch_bounds__(128) k_trace_closest(const __grid_constant__ DeviceScene s, const float *rays,
+                                                       uint32_t n, Hit *hits, float *t_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 *r4 = reinterpret_cast<const float4 *>(rays) + 2u * i;
@@ -37,7 +37,8 @@ __global__ void __launch_bounds__(128) k_trace_closest(const __grid_constant__ D
     }
 }
 
-__global__ void __launch_bounds__(128) k_trace_any(const __grid_constant__ DeviceScene s, const float *rays, uint32_t n, uint32_t *occ) {
+__global__ void __launch_bounds__(128) k_trace_any(const __grid_constant__ DeviceScene s, const float *rays,
+                                                   uint32_t n, uint32_t *occ) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 *r4 = reinterpret_cast<const float4 *>(rays) + 2u * i;
@@ -52,8 +53,8 @@ template <int N>
 #ifndef VS_RENDER_MIN_BLOCKS
 #define VS_RENDER_MIN_BLOCKS 1
 #endif
-__global__ void __launch_bounds__(128, VS_RENDER_MIN_BLOCKS) k_render(const __grid_constant__ DeviceScene s, uint32_t frame_begin, uint64_t path_count,
-                                                float4 *radiance) {
+__global__ void __launch_bounds__(128, VS_RENDER_MIN_BLOCKS)
+    k_render(const __grid_constant__ DeviceScene s, uint32_t frame_begin, uint64_t path_count, float4 *radiance) {
     uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= path_count) return;
     uint32_t npix = s.cam.width * s.cam.height;

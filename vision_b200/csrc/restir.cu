@@ -20,7 +20,19 @@
 
 #include <algorithm>
 
+// The material types compiled into this copy of the ReSTIR kernels and the
+// namespace that holds them: restir.cu builds the general copy (every
+// material); restir_diffuse.cu includes this file again for scenes made of
+// diffuse surfaces and emitters only, whose candidate loops then carry no
+// code for the other materials (the reference's DSL likewise compiles a
+// scene's kernels for the materials it has).
+#ifndef VS_RT_MATERIALS
+#define VS_RT_MATERIALS kAllMaterials
+#define VS_RT_NS rt_all
+#endif
+
 namespace vs {
+namespace VS_RT_NS {
 
 namespace {
 
@@ -160,9 +172,9 @@ __device__ __forceinline__ Interaction it_at(const DeviceScene &s, const Hit &h,
 }
 
 // MaterialEvaluator creation plus SampledWavelengths::check_dispersive.
-__device__ __forceinline__ Bsdf<RN> bsdf_at(const DeviceScene &s, const Interaction &it, RWl &wl) {
+__device__ __forceinline__ Bsdf<RN, VS_RT_MATERIALS> bsdf_at(const DeviceScene &s, const Interaction &it, RWl &wl) {
     Material m = s.materials[it.mat];
-    Bsdf<RN> b = make_bsdf<RN>(s, m, it.shading, it.ng, it.wo, wl);
+    Bsdf<RN, VS_RT_MATERIALS> b = make_bsdf<RN, VS_RT_MATERIALS>(s, m, it.shading, it.ng, it.wo, wl);
     if (b.dispersive) invalidate_secondary<RN>(wl);
     return b;
 }
@@ -194,7 +206,7 @@ __device__ __forceinline__ void classify(const Material &m, uint32_t &flag, floa
 // conductor (MicrofacetLobe::sample_delta_local, lobe.cpp:223-230: mirror
 // direction, uncompensated BxDF) or dielectric (DielectricLobe::sample_delta_local,
 // lobe.cpp:404-425: one draw picks mirror reflection or refraction).
-__device__ VS_OUTLINE BsdfSample<RN> sample_delta(const Bsdf<RN> &b, f3 wo_w, Sampler &smp) {
+__device__ VS_OUTLINE BsdfSample<RN> sample_delta(const Bsdf<RN, VS_RT_MATERIALS> &b, f3 wo_w, Sampler &smp) {
     BsdfSample<RN> bs;
     bs.eta = 1.0f;
     f3 wo = b.frame.to_local(wo_w);
@@ -293,7 +305,7 @@ __device__ __forceinline__ float pdf_point(float pdf_wi, f3 ng, f3 w_un) {
 // ReSTIRDI::Li evaluated for a stored light sample (direct.cpp:116-158) and
 // its p_hat = luminance(f.vec3()).  Optionally returns the BSDF pdf of the
 // point in area measure and the evaluated light sample.
-__device__ VS_OUTLINE float di_p_hat(const DeviceScene &s, const Interaction &it, const Bsdf<RN> &bsdf,
+__device__ VS_OUTLINE float di_p_hat(const DeviceScene &s, const Interaction &it, const Bsdf<RN, VS_RT_MATERIALS> &bsdf,
                                      const DiReservoir &smp, const RWl &wl, float *bsdf_pdf_point, PointEval *out,
                                      RSpec *f_out) {
     PointEval e;
@@ -317,7 +329,7 @@ __device__ VS_OUTLINE float di_p_hat(const DeviceScene &s, const Interaction &it
 // compute_p_hat(it, nullptr, sample): a fresh evaluator at `it`.
 __device__ __forceinline__ float di_p_hat_at(const DeviceScene &s, const Interaction &it, const DiReservoir &smp,
                                              RWl &wl) {
-    Bsdf<RN> b = bsdf_at(s, it, wl);
+    Bsdf<RN, VS_RT_MATERIALS> b = bsdf_at(s, it, wl);
     return di_p_hat(s, it, b, smp, wl, nullptr, nullptr, nullptr);
 }
 
@@ -367,7 +379,7 @@ __device__ VS_OUTLINE PrimaryHit compute_hit(const DeviceScene &s, const RtParam
         bool near_spec = flag == kFlagNearSpec;
         f3 w = make3(0.0f);
         if (near_spec) {
-            Bsdf<RN> b = make_bsdf<RN>(s, m, r.it.shading, r.it.ng, r.it.wo, wl);
+            Bsdf<RN, VS_RT_MATERIALS> b = make_bsdf<RN, VS_RT_MATERIALS>(s, m, r.it.shading, r.it.ng, r.it.wo, wl);
             BsdfSample<RN> bs = sample_delta(b, r.it.wo, smp);
             w = bs.wi;
             RSpec tp = bs.eval.throughput();
@@ -410,7 +422,7 @@ __device__ __forceinline__ uint32_t select_light(const DeviceScene &s, float u) 
 __device__ VS_OUTLINE DiReservoir di_ris(const DeviceScene &s, const RtParams &p, const Interaction &it,
                                          Sampler &smp, RWl &wl, f3 throughput, RtHitBsdf &hb) {
     DiReservoir ret = di_empty();
-    Bsdf<RN> bsdf = bsdf_at(s, it, wl);
+    Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
     float lum_tp = lum3(throughput);
     float Ml = static_cast<float>(p.M_light), Mb = static_cast<float>(p.M_bsdf);
     // LightSampler::sample_only (lightsampler.cpp:218-228), AreaLight::sample_only
@@ -741,7 +753,7 @@ __device__ VS_OUTLINE f3 di_shading(const DeviceScene &s, const RtParams &p, con
         LightPoint lp{it.pos, it.ng, it.prim_area};
         Le = area_Le(L, lp, p.view_pos, wl);
     } else {
-        Bsdf<RN> bsdf = bsdf_at(s, it, wl);
+        Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
         RSpec f;
         di_p_hat(s, it, bsdf, rsv, wl, nullptr, nullptr, &f);
         value = f * spec3(tp) * (1.0f / lum3(tp));
@@ -804,7 +816,7 @@ namespace {
 // GISample::p_hat with ReSTIRGI::eval_bsdf (indirect.cpp:113-128,
 // reservoir.h:166-170): luminance(Lo * f.vec3()) toward the sample point.
 __device__ __forceinline__ f3 gi_f(const DeviceScene &s, const Interaction &it, const GiReservoir &g, RWl &wl) {
-    Bsdf<RN> bsdf = bsdf_at(s, it, wl);
+    Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
     f3 wi = normalize(ld3p(g.sp_pos) - it.pos);
     return vec3(bsdf.evaluate(it.wo, wi, nullptr).f);
 }
@@ -847,7 +859,9 @@ __device__ VS_OUTLINE GiReservoir gi_combine_temporal(const DeviceScene &s, cons
 }  // namespace
 
 // ReSTIRGI initial samples (indirect.cpp:43-111).
-__global__ void __launch_bounds__(128) k_gi_initial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
+__global__ void __launch_bounds__(128) k_gi_initial(const __grid_constant__ DeviceScene s,
+                                                    const __grid_constant__ RtParams p,
+                                                    const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -1013,7 +1027,9 @@ __global__ void __launch_bounds__(128) k_gi_wf_finish(const __grid_constant__ De
 }
 
 // ReSTIRGI temporal pass (indirect.cpp:155-236).
-__global__ void __launch_bounds__(128) k_gi_temporal(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p, const __grid_constant__ RtBuffers b) {
+__global__ void __launch_bounds__(128) k_gi_temporal(const __grid_constant__ DeviceScene s,
+                                                     const __grid_constant__ RtParams p,
+                                                     const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -1135,7 +1151,8 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
 
 // RealTimeIntegrator combine kernel (rt.cpp:118-126) with
 // NormalRadianceCollector::add_sample (normal.cpp:87-101).
-__global__ void k_rt_combine(uint32_t npix, const __grid_constant__ RtBuffers b, float di, float ii, uint32_t film_index, float4 *film) {
+__global__ void k_rt_combine(uint32_t npix, const __grid_constant__ RtBuffers b, float di, float ii,
+                             uint32_t film_index, float4 *film) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npix) return;
     float4 d = b.di_radiance[i], g = b.gi_radiance[i];
@@ -1237,4 +1254,5 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
     return cudaGetLastError();
 }
 
+}  // namespace VS_RT_NS
 }  // namespace vs

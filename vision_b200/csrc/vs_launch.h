@@ -25,15 +25,23 @@ cudaError_t upload_spectral_consts_wf(const float *x, const float *y, const floa
 // server.cu
 cudaError_t upload_spectral_consts_serve(const float *x, const float *y, const float *z, const float *d65,
                                          float y_integral);
-// restir.cu
-cudaError_t upload_spectral_consts_rt(const float *x, const float *y, const float *z, const float *d65, float y_integral);
-cudaError_t launch_rt_reset(uint32_t npix, const RtBuffers &b, cudaStream_t st);
-// wf / radiance (one slot and one float4 per pixel): when given, the initial
-// indirect samples run as wavefront passes (class_mask as for the plain
+// restir.cu (every material) and restir_diffuse.cu (diffuse and black-body
+// surfaces only): the same kernels in two namespaces.  In launch_rt_frame,
+// wf / radiance (one slot and one float4 per pixel), when given, run the
+// initial indirect samples as wavefront passes (class_mask as for the plain
 // wavefront); otherwise as the one-kernel k_gi_initial.
-cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuffers &b, uint32_t film_index,
-                            float4 *film, const WfBuffers *wf, float4 *radiance, uint32_t class_mask, cudaStream_t st,
-                            unsigned *launches);
+#define VS_RT_DECLARE(ns)                                                                                          \
+    namespace ns {                                                                                                 \
+    cudaError_t upload_spectral_consts_rt(const float *x, const float *y, const float *z, const float *d65,       \
+                                          float y_integral);                                                       \
+    cudaError_t launch_rt_reset(uint32_t npix, const RtBuffers &b, cudaStream_t st);                               \
+    cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuffers &b, uint32_t film_index,  \
+                                float4 *film, const WfBuffers *wf, float4 *radiance, uint32_t class_mask,          \
+                                cudaStream_t st, unsigned *launches);                                              \
+    }
+VS_RT_DECLARE(rt_all)
+VS_RT_DECLARE(rt_diffuse)
+#undef VS_RT_DECLARE
 cudaError_t launch_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out, cudaStream_t st);
 
 }  // namespace vs
