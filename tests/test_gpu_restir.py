@@ -32,13 +32,15 @@ def _run(vb, ctx, sc, cams, w, h):
         yield f, s, ort
 
 
-@pytest.mark.parametrize('materials', ['diffuse', 'metal'])
+@pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates'])
 def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
     # 'diffuse': diffuse walls and emitters (the kernels compiled for those
-    # materials alone); 'metal': a gold box as well (the general kernels).
+    # materials alone); 'metal': a gold box as well (the general kernels);
+    # 'two_bsdf_candidates': M_bsdf = 2, which takes the one-kernel direct
+    # pass instead of the staged one.
     w, h = 96, 64
     sc = scenes.many_lights(w, h, emitters=300, seed=5, M_light=8, history_limit=20, spatial_neighbours=5,
-                            spatial_radius=12.0, max_depth=4)
+                            spatial_radius=12.0, max_depth=4, M_bsdf=2 if materials == 'two_bsdf_candidates' else 1)
     if materials == 'metal':
         for m in sc['materials']:
             if m['name'] == 'TallBox':

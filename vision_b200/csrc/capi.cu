@@ -152,6 +152,9 @@ struct vs_scene {
         DevBuf<DiReservoir> di[2], di_pass;
         DevBuf<GiReservoir> gi[2], gi_pass, gi_init;
         DevBuf<float4> di_radiance, gi_radiance;
+        DevBuf<float4> di_stage, di_ray;
+        DevBuf<Hit> di_hit;
+        DevBuf<uint32_t> di_list, di_count;
         uint32_t width = 0, height = 0;
         bool have_prev = false;
         Camera prev_cam{};
@@ -165,6 +168,7 @@ struct vs_scene {
             }
             hit_bsdf.free(); motion.free(); di_pass.free(); gi_pass.free(); gi_init.free();
             di_radiance.free(); gi_radiance.free();
+            di_stage.free(); di_ray.free(); di_hit.free(); di_list.free(); di_count.free();
         }
         RtBuffers view() const {
             RtBuffers b{};
@@ -181,6 +185,11 @@ struct vs_scene {
             b.gi_init = gi_init.ptr;
             b.di_radiance = di_radiance.ptr;
             b.gi_radiance = gi_radiance.ptr;
+            b.di_stage = di_stage.ptr;
+            b.di_ray = di_ray.ptr;
+            b.di_hit = di_hit.ptr;
+            b.di_list = di_list.ptr;
+            b.di_count = di_count.ptr;
             return b;
         }
     } rt;
@@ -856,6 +865,11 @@ int rt_ensure(vs_scene *s, cudaStream_t st) {
     VS_CUDA(r.gi_init.alloc(n), "restir alloc");
     VS_CUDA(r.di_radiance.alloc(n), "restir alloc");
     VS_CUDA(r.gi_radiance.alloc(n), "restir alloc");
+    VS_CUDA(r.di_stage.alloc(4 * n), "restir alloc");
+    VS_CUDA(r.di_ray.alloc(2 * n), "restir alloc");
+    VS_CUDA(r.di_hit.alloc(n), "restir alloc");
+    VS_CUDA(r.di_list.alloc(n), "restir alloc");
+    VS_CUDA(r.di_count.alloc(1), "restir alloc");
     r.width = w;
     r.height = hgt;
     r.have_prev = false;

@@ -344,6 +344,7 @@ struct PrimaryHit {
     RtSurface surf;
     RtSurfaceExt ext;
     Interaction it;
+    f3 last_d;  // direction of the ray that found `it`
     bool hit;
 };
 __device__ VS_OUTLINE PrimaryHit compute_hit(const DeviceScene &s, const RtParams &p, Sampler &smp, RWl &wl,
@@ -368,6 +369,7 @@ __device__ VS_OUTLINE PrimaryHit compute_hit(const DeviceScene &s, const RtParam
         }
         r.surf.hit = h;
         r.it = surface_interaction(s, h, rd, true);
+        r.last_d = rd;
         r.ext.t_max += length(r.it.pos - ro) / length(rd);
         f3 v_pos = cam_o + cam_d * r.ext.t_max;
         Material m = s.materials[r.it.mat];
@@ -419,11 +421,10 @@ __device__ __forceinline__ uint32_t select_light(const DeviceScene &s, float u) 
 }
 
 // ReSTIRDI::RIS (direct.cpp:161-233).
-__device__ VS_OUTLINE DiReservoir di_ris(const DeviceScene &s, const RtParams &p, const Interaction &it,
-                                         Sampler &smp, RWl &wl, f3 throughput, RtHitBsdf &hb) {
+__device__ __forceinline__ DiReservoir di_ris_lights(const DeviceScene &s, const RtParams &p, const Interaction &it,
+                                                     Sampler &smp, RWl &wl, float lum_tp,
+                                                     const Bsdf<RN, VS_RT_MATERIALS> &bsdf) {
     DiReservoir ret = di_empty();
-    Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
-    float lum_tp = lum3(throughput);
     float Ml = static_cast<float>(p.M_light), Mb = static_cast<float>(p.M_bsdf);
     // LightSampler::sample_only (lightsampler.cpp:218-228), AreaLight::sample_only
     // (area.cpp:134-140): one light candidate from its three draws, with its
@@ -475,48 +476,82 @@ __device__ VS_OUTLINE DiReservoir di_ris(const DeviceScene &s, const RtParams &p
         candidate(s0, u0, c0, w0);
         di_update(ret, smp.next(), c0, w0);
     }
+    return ret;
+}
+
+// The BSDF candidate of ReSTIRDI::Li (direct.cpp:39-114), part one: the BSDF
+// sample (recorded as the pixel's HitBSDF) and the ray that looks for an
+// emitter along it.
+__device__ __forceinline__ Ray di_bsdf_ray(const Interaction &it, const Bsdf<RN, VS_RT_MATERIALS> &bsdf,
+                                           Sampler &smp, RtHitBsdf &hb) {
+    BsdfSample<RN> bs = bsdf.sample(it.wo, smp);
+    Ray ray = spawn_ray(it.pos, it.ng, bs.wi);
+    hb.wx = bs.wi.x;
+    hb.wy = bs.wi.y;
+    hb.wz = bs.wi.z;
+    hb.fx = bs.eval.f.v[0];
+    hb.fy = bs.eval.f.v[1];
+    hb.fz = bs.eval.f.v[2];
+    hb.pdf = bs.eval.pdf;
+    return ray;
+}
+
+// Part two: the candidate from what the ray hit (an emitter or nothing) and
+// its RIS weight.
+__device__ __forceinline__ void di_bsdf_candidate(const DeviceScene &s, const RtParams &p, const Interaction &it,
+                                                  const RWl &wl, const RtHitBsdf &hb, bool hit, const Hit &h,
+                                                  f3 ray_d, float lum_tp, DiReservoir &cand, float &weight) {
+    const float Ml = static_cast<float>(p.M_light), Mb = static_cast<float>(p.M_bsdf);
+    cand = di_empty();
+    float pdf = hb.pdf;
+    float eval_pdf = hb.pdf;
+    RSpec eval_f;
+    eval_f.v[0] = hb.fx;
+    eval_f.v[1] = hb.fy;
+    eval_f.v[2] = hb.fz;
+    float light_pdf_point = 0.0f;
+    RSpec f = RSpec::fill(0.0f);
+    if (hit) {
+        Interaction nit = surface_interaction(s, h, ray_d, false);
+        if (nit.light != kInvalid) {
+            // LightSampler::evaluate_hit_point (lightsampler.cpp:269-300).
+            AreaLight L = s.lights[nit.light];
+            LightPoint lp{nit.pos, nit.ng, nit.prim_area};
+            RSpec Le = area_Le(L, lp, it.pos, wl) * light_G(it.pos, lp);
+            float le_pdf = pdf_point(pdf, nit.ng, it.pos - nit.pos);
+            uint32_t local = nit.prim - L.first_prim;
+            light_pdf_point = (1.0f / nit.prim_area) * s.prim_pmf[L.alias_offset + local] *
+                              light_select_pmf(s, nit.light);
+            cand.light_index = nit.light;
+            cand.prim_id = local;
+            cand.bary_u = h.u;
+            cand.bary_v = h.v;
+            f3 w = it.pos - nit.pos;
+            st3(cand.pos, offset_ray_origin(nit.pos, dot(nit.ng, w) > 0.0f ? nit.ng : -nit.ng));
+            eval_pdf = le_pdf;
+            f = eval_f * Le;
+        }
+    }
+    cand.p_hat = lum3(vec3(f));
+    float bp = eval_pdf;
+    weight = safe_weight(bp / (Ml * light_pdf_point + Mb * bp), cand.p_hat, 1.0f / bp) * lum_tp;
+}
+
+// ReSTIRDI::RIS (direct.cpp:161-233): M_light light candidates, then M_bsdf
+// BSDF candidates, each found by tracing its ray.
+__device__ VS_OUTLINE DiReservoir di_ris(const DeviceScene &s, const RtParams &p, const Interaction &it,
+                                         Sampler &smp, RWl &wl, f3 throughput, RtHitBsdf &hb) {
+    Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
+    float lum_tp = lum3(throughput);
+    DiReservoir ret = di_ris_lights(s, p, it, smp, wl, lum_tp, bsdf);
     for (uint32_t i = 0; i < p.M_bsdf; ++i) {
-        // ReSTIRDI::Li from a BSDF sample (direct.cpp:39-114).
-        DiReservoir cand = di_empty();
-        BsdfSample<RN> bs = bsdf.sample(it.wo, smp);
-        Ray ray = spawn_ray(it.pos, it.ng, bs.wi);
+        Ray ray = di_bsdf_ray(it, bsdf, smp, hb);
         Hit h;
         float t;
         bool hit = trace_closest(s, precompute_ray(ray.o, ray.d), ray.tmax, h, t);
-        float pdf = bs.eval.pdf;
-        hb.wx = bs.wi.x;
-        hb.wy = bs.wi.y;
-        hb.wz = bs.wi.z;
-        hb.fx = bs.eval.f.v[0];
-        hb.fy = bs.eval.f.v[1];
-        hb.fz = bs.eval.f.v[2];
-        hb.pdf = pdf;
-        float light_pdf_point = 0.0f;
-        RSpec f = RSpec::fill(0.0f);
-        if (hit) {
-            Interaction nit = surface_interaction(s, h, ray.d, false);
-            if (nit.light != kInvalid) {
-                // LightSampler::evaluate_hit_point (lightsampler.cpp:269-300).
-                AreaLight L = s.lights[nit.light];
-                LightPoint lp{nit.pos, nit.ng, nit.prim_area};
-                RSpec Le = area_Le(L, lp, it.pos, wl) * light_G(it.pos, lp);
-                float le_pdf = pdf_point(pdf, nit.ng, it.pos - nit.pos);
-                uint32_t local = nit.prim - L.first_prim;
-                light_pdf_point = (1.0f / nit.prim_area) * s.prim_pmf[L.alias_offset + local] *
-                                  light_select_pmf(s, nit.light);
-                cand.light_index = nit.light;
-                cand.prim_id = local;
-                cand.bary_u = h.u;
-                cand.bary_v = h.v;
-                f3 w = it.pos - nit.pos;
-                st3(cand.pos, offset_ray_origin(nit.pos, dot(nit.ng, w) > 0.0f ? nit.ng : -nit.ng));
-                bs.eval.pdf = le_pdf;
-                f = bs.eval.f * Le;
-            }
-        }
-        cand.p_hat = lum3(vec3(f));
-        float bp = bs.eval.pdf;
-        float weight = safe_weight(bp / (Ml * light_pdf_point + Mb * bp), cand.p_hat, 1.0f / bp) * lum_tp;
+        DiReservoir cand;
+        float weight;
+        di_bsdf_candidate(s, p, it, wl, hb, hit, h, ray.d, lum_tp, cand, weight);
         di_update(ret, smp.next(), cand, weight);
     }
     di_update_W(ret, ret.p_hat);
@@ -687,6 +722,225 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
         }
     }
     rsv = di_temporal(s, p, b, rsv, ph.surf, ph.ext, mv, p_film, smp, wl);
+    b.di_pass[idx] = rsv;
+}
+
+// ---------------------------------------------------------------------------
+// The same direct pass as k_di_candidates in stages, so that its three
+// traversals (primary chain, BSDF candidate, visibility) run in small kernels
+// and the candidate loop runs without traversal code beside it.  Per pixel the
+// stages pass the sampler state, wavelengths, film position and the direction
+// that found the primary surface through b.di_stage; the hit pixels are
+// listed in b.di_list.  Every pixel makes the same draws in the same order as
+// in k_di_candidates.  Used when M_bsdf <= 1.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ void stage_store(const RtBuffers &b, uint32_t idx, f3 last_d, f2 p_film, const RWl &wl,
+                                            const Sampler &smp, bool hit) {
+    float4 *st = b.di_stage + 4ull * idx;
+    st[0] = make_float4(last_d.x, last_d.y, last_d.z, p_film.x);
+    st[1] = make_float4(p_film.y, wl.lambda[0], wl.lambda[1], wl.lambda[2]);
+    st[2] = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], hit ? 1.0f : 0.0f);
+    st[3] = make_float4(__uint_as_float(static_cast<uint32_t>(smp.state)),
+                        __uint_as_float(static_cast<uint32_t>(smp.state >> 32)), 0.0f, 0.0f);
+}
+
+// Sampler state, wavelengths and film position of a pixel; returns the
+// direction that found its primary surface.
+__device__ __forceinline__ f3 stage_load(const DeviceScene &s, const RtBuffers &b, uint32_t idx, RWl &wl,
+                                         Sampler &smp, f2 &p_film) {
+    const float4 *st = b.di_stage + 4ull * idx;
+    const float4 a = st[0], c = st[1], d = st[2], e = st[3];
+    p_film = make2(a.w, c.x);
+    wl.lambda[0] = c.y;
+    wl.lambda[1] = c.z;
+    wl.lambda[2] = c.w;
+    wl.pdf[0] = d.x;
+    wl.pdf[1] = d.y;
+    wl.pdf[2] = d.z;
+    smp.kind = s.ip.sampler;
+    smp.seed = s.ip.seed;
+    smp.state = static_cast<uint64_t>(__float_as_uint(e.x)) | (static_cast<uint64_t>(__float_as_uint(e.y)) << 32);
+    return make3(a.x, a.y, a.z);
+}
+
+__device__ __forceinline__ void stage_sampler(const RtBuffers &b, uint32_t idx, const Sampler &smp) {
+    b.di_stage[4ull * idx + 3] = make_float4(__uint_as_float(static_cast<uint32_t>(smp.state)),
+                                             __uint_as_float(static_cast<uint32_t>(smp.state >> 32)), 0.0f, 0.0f);
+}
+
+// The primary surface of a listed pixel (compute_hit's interaction) and the
+// throughput of its near-specular chain.
+__device__ __forceinline__ Interaction stage_surface(const DeviceScene &s, const RtParams &p, const RtBuffers &b,
+                                                     uint32_t idx, f3 last_d, f3 &tp) {
+    const uint32_t cur = (p.frame + 1u) & 1u;
+    const RtSurface cs = b.surf[cur][idx];
+    tp = make3(1.0f);
+    if (cs.is_replaced) {
+        const RtSurfaceExt e = b.ext[cur][idx];
+        tp = make3(e.tx, e.ty, e.tz);
+    }
+    return surface_interaction(s, cs.hit, last_d, true);
+}
+
+}  // namespace
+
+// Stage 1: camera ray, primary chain, motion vector; pixels that see nothing
+// get their (empty) reservoir here.
+__global__ void __launch_bounds__(128) k_di_primary(const __grid_constant__ DeviceScene s,
+                                                    const __grid_constant__ RtParams p,
+                                                    const __grid_constant__ RtBuffers b) {
+    uint32_t x, y;
+    if (!tile_pixel(p, x, y)) return;
+    const uint32_t idx = pixel_index(p, x, y);
+    const uint32_t cur = (p.frame + 1u) & 1u;
+    RWl wl = pixel_wavelengths(s, x, y, p.frame);
+    Sampler smp;
+    smp.start(x, y, p.frame, 0u, s.ip.sampler, s.ip.seed);
+    f2 p_film;
+    f3 ro, rd;
+    camera_ray(s.cam, smp, x, y, p_film, ro, rd);
+    PrimaryHit ph = compute_hit(s, p, smp, wl, ro, rd);
+    b.surf[cur][idx] = ph.surf;
+    if (ph.surf.is_replaced) b.ext[cur][idx] = ph.ext;
+    // FrameBuffer::compute_motion_vec (frame_buffer.cpp:325-333).
+    f2 mv = make2(0.0f, 0.0f);
+    if (ph.hit) {
+        f2 pr = prev_raster(p, ro + rd * ph.ext.t_max);
+        mv = p_film - pr;
+    }
+    b.motion[idx] = make_float2(mv.x, mv.y);
+    stage_store(b, idx, ph.last_d, p_film, wl, smp, ph.hit);
+    if (ph.hit) {
+        b.di_list[wf::queue_push(b.di_count)] = idx;
+    } else {
+        RtHitBsdf hb{};
+        hb.pdf = -1.0f;
+        b.hit_bsdf[idx] = hb;
+        DiReservoir rsv = di_empty();
+        di_update_W(rsv, rsv.p_hat);
+        rsv.C = fminf(1.0f, rsv.C);
+        b.di_pass[idx] = rsv;
+    }
+}
+
+// Stage 2: the light candidates and the BSDF candidate's ray.
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_di_lights(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                const __grid_constant__ RtBuffers b) {
+    const uint32_t n = *b.di_count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t idx = b.di_list[k];
+        RWl wl;
+        Sampler smp;
+        f2 p_film;
+        const f3 last_d = stage_load(s, b, idx, wl, smp, p_film);
+        f3 tp;
+        const Interaction it = stage_surface(s, p, b, idx, last_d, tp);
+        Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
+        DiReservoir rsv = di_ris_lights(s, p, it, smp, wl, lum3(tp), bsdf);
+        RtHitBsdf hb{};
+        hb.pdf = -1.0f;
+        if (p.M_bsdf == 1u) {
+            const Ray ray = di_bsdf_ray(it, bsdf, smp, hb);
+            b.di_ray[2ull * idx] = make_float4(ray.o.x, ray.o.y, ray.o.z, ray.tmax);
+            b.di_ray[2ull * idx + 1] = make_float4(ray.d.x, ray.d.y, ray.d.z, 0.0f);
+        } else {
+            di_update_W(rsv, rsv.p_hat);
+            rsv.C = fminf(1.0f, rsv.C);
+        }
+        b.hit_bsdf[idx] = hb;
+        b.di_pass[idx] = rsv;
+        stage_store(b, idx, last_d, p_film, wl, smp, true);
+    }
+}
+
+// Stage 3: the BSDF candidates' closest hits.
+__global__ void __launch_bounds__(128) k_di_bsdf_trace(const __grid_constant__ DeviceScene s,
+                                                       const __grid_constant__ RtParams p,
+                                                       const __grid_constant__ RtBuffers b) {
+    if (p.M_bsdf != 1u) return;
+    const uint32_t n = *b.di_count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t idx = b.di_list[k];
+        const float4 o = b.di_ray[2ull * idx], d = b.di_ray[2ull * idx + 1];
+        Hit h;
+        float t;
+        if (!trace_closest(s, precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z)), o.w, h, t))
+            h = Hit{kInvalid, kInvalid, 0.0f, 0.0f};
+        b.di_hit[idx] = h;
+    }
+}
+
+// Stage 4: the BSDF candidate, the reservoir's weight, and the visibility ray
+// towards the chosen sample.
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_di_bsdf_eval(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                   const __grid_constant__ RtBuffers b) {
+    const uint32_t n = *b.di_count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t idx = b.di_list[k];
+        RWl wl;
+        Sampler smp;
+        f2 p_film;
+        const f3 last_d = stage_load(s, b, idx, wl, smp, p_film);
+        f3 tp;
+        const Interaction it = stage_surface(s, p, b, idx, last_d, tp);
+        DiReservoir rsv = b.di_pass[idx];
+        if (p.M_bsdf == 1u) {
+            const Hit h = b.di_hit[idx];
+            const float4 d = b.di_ray[2ull * idx + 1];
+            DiReservoir cand;
+            float weight;
+            di_bsdf_candidate(s, p, it, wl, b.hit_bsdf[idx], h.inst_id != kInvalid, h, make3(d.x, d.y, d.z), lum3(tp),
+                              cand, weight);
+            di_update(rsv, smp.next(), cand, weight);
+            di_update_W(rsv, rsv.p_hat);
+            rsv.C = fminf(1.0f, rsv.C);
+            b.di_pass[idx] = rsv;
+            stage_sampler(b, idx, smp);
+        }
+        const Ray sh = spawn_ray_to(it.pos, it.ng, ld3p(rsv.pos));
+        b.di_ray[2ull * idx] = make_float4(sh.o.x, sh.o.y, sh.o.z, sh.tmax);
+        b.di_ray[2ull * idx + 1] = make_float4(sh.d.x, sh.d.y, sh.d.z, 0.0f);
+    }
+}
+
+// Stage 5: visibility of the chosen samples (an occluded sample keeps its
+// history count but loses its weight).
+__global__ void __launch_bounds__(128) k_di_visibility(const __grid_constant__ DeviceScene s,
+                                                       const __grid_constant__ RtBuffers b) {
+    const uint32_t n = *b.di_count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t idx = b.di_list[k];
+        const float4 o = b.di_ray[2ull * idx], d = b.di_ray[2ull * idx + 1];
+        if (trace_any(s, precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z)), o.w)) {
+            DiReservoir rsv = b.di_pass[idx];
+            rsv.W = 0.0f;
+            rsv.weight_sum = 0.0;
+            b.di_pass[idx] = rsv;
+        }
+    }
+}
+
+// Stage 6: temporal reuse for every pixel.
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_di_temporal(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                  const __grid_constant__ RtBuffers b) {
+    uint32_t x, y;
+    if (!tile_pixel(p, x, y)) return;
+    const uint32_t idx = pixel_index(p, x, y);
+    const uint32_t cur = (p.frame + 1u) & 1u;
+    RWl wl;
+    Sampler smp;
+    f2 p_film;
+    (void)stage_load(s, b, idx, wl, smp, p_film);
+    const RtSurface cs = b.surf[cur][idx];
+    RtSurfaceExt cext{};
+    if (cs.is_replaced) cext = b.ext[cur][idx];
+    const float2 m = b.motion[idx];
+    DiReservoir rsv = di_temporal(s, p, b, b.di_pass[idx], cs, cext, make2(m.x, m.y), p_film, smp, wl);
     b.di_pass[idx] = rsv;
 }
 
@@ -1196,8 +1450,22 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
     dim3 block(16, 8);
     dim3 grid((p.width + 15) / 16, (p.height + 7) / 8);
     unsigned n = 0;
-    k_di_candidates<<<grid, block, 0, st>>>(s, p, b);
-    ++n;
+    if (p.M_bsdf <= 1u && b.di_stage) {
+        static unsigned g_list = 0;
+        if (!g_list) g_list = rt_wave_grid(k_di_lights);
+        cudaError_t e = cudaMemsetAsync(b.di_count, 0, sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        k_di_primary<<<grid, block, 0, st>>>(s, p, b);
+        k_di_lights<<<g_list, 128, 0, st>>>(s, p, b);
+        k_di_bsdf_trace<<<g_list, 128, 0, st>>>(s, p, b);
+        k_di_bsdf_eval<<<g_list, 128, 0, st>>>(s, p, b);
+        k_di_visibility<<<g_list, 128, 0, st>>>(s, b);
+        k_di_temporal<<<grid, block, 0, st>>>(s, p, b);
+        n += 6;
+    } else {
+        k_di_candidates<<<grid, block, 0, st>>>(s, p, b);
+        ++n;
+    }
     if (p.di.open) {
         k_di_spatial<<<grid, block, 0, st>>>(s, p, b);
         ++n;

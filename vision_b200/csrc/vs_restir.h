@@ -122,6 +122,15 @@ struct RtBuffers {
     GiReservoir *gi_init;    // initial GI samples (GISample; W and C unused)
     float4 *di_radiance;
     float4 *gi_radiance;
+    // Staged direct pass (null: one kernel): per pixel 4 float4 of sampler
+    // state, wavelengths, film position and primary-ray direction; 2 float4
+    // of the pending ray; the BSDF candidate's hit; the list of pixels that
+    // see a surface and its length.
+    float4 *di_stage;
+    float4 *di_ray;
+    Hit *di_hit;
+    uint32_t *di_list;
+    uint32_t *di_count;
 };
 
 }  // namespace vs

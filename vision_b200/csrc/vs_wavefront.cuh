@@ -82,11 +82,19 @@ __device__ __forceinline__ void generate(const DeviceScene &s, const Camera &cam
     }
 }
 
+// The calling thread's lane in its warp (any block shape: a 16 x 8 block's
+// warps hold two rows of threadIdx.x, so threadIdx.x % 32 is not the lane).
+__device__ __forceinline__ int lane_id() {
+    unsigned lane;
+    asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
+    return static_cast<int>(lane);
+}
+
 // Appends one entry per calling lane to a device queue: one atomicAdd per
 // converged group of lanes, positions in lane order.
 __device__ __forceinline__ uint32_t queue_push(uint32_t *counter) {
     const unsigned mask = __activemask();
-    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int lane = lane_id();
     const int leader = __ffs(mask) - 1;
     uint32_t base = 0;
     if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
@@ -99,7 +107,7 @@ __device__ __forceinline__ uint32_t queue_push(uint32_t *counter) {
 __device__ __forceinline__ uint32_t class_push(uint32_t *counts, uint32_t cls) {
     const unsigned active = __activemask();
     const unsigned group = __match_any_sync(active, cls);
-    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int lane = lane_id();
     const int leader = __ffs(group) - 1;
     uint32_t base = 0;
     if (lane == leader) base = atomicAdd(counts + cls, static_cast<uint32_t>(__popc(group)));
@@ -121,7 +129,7 @@ __device__ __forceinline__ uint32_t refill(uint32_t *fetch, uint32_t n, bool act
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
     const uint32_t k = static_cast<uint32_t>(__popc(idle));
     if (k < VS_REFILL_LANES && k != 32u) return n;
-    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int lane = lane_id();
     const int leader = __ffs(idle) - 1;
     uint32_t base = 0;
     if (lane == leader) base = atomicAdd(fetch, k);
