@@ -869,7 +869,7 @@ int rt_ensure(vs_scene *s, cudaStream_t st) {
     VS_CUDA(r.di_ray.alloc(2 * n), "restir alloc");
     VS_CUDA(r.di_hit.alloc(n), "restir alloc");
     VS_CUDA(r.di_list.alloc(n), "restir alloc");
-    VS_CUDA(r.di_count.alloc(1), "restir alloc");
+    VS_CUDA(r.di_count.alloc(3), "restir alloc");
     r.width = w;
     r.height = hgt;
     r.have_prev = false;

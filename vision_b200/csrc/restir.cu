@@ -856,20 +856,34 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
     }
 }
 
-// Stage 3: the BSDF candidates' closest hits.
+// Stage 3: the BSDF candidates' closest hits (warps refill finished lanes,
+// as the wavefront traversal kernels do).
 __global__ void __launch_bounds__(128) k_di_bsdf_trace(const __grid_constant__ DeviceScene s,
                                                        const __grid_constant__ RtParams p,
                                                        const __grid_constant__ RtBuffers b) {
     if (p.M_bsdf != 1u) return;
     const uint32_t n = *b.di_count;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t idx = b.di_list[k];
-        const float4 o = b.di_ray[2ull * idx], d = b.di_ray[2ull * idx + 1];
-        Hit h;
-        float t;
-        if (!trace_closest(s, precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z)), o.w, h, t))
-            h = Hit{kInvalid, kInvalid, 0.0f, 0.0f};
-        b.di_hit[idx] = h;
+    uint2 stack[kStackSize];
+    bool active = false, drained = false;
+    uint32_t idx = 0;
+    RayPre r;
+    TravState t;
+    for (;;) {
+        if (!drained) {
+            const uint32_t k = wf::refill(b.di_count + 1, n, active, drained);
+            if (k < n) {
+                idx = b.di_list[k];
+                const float4 o = b.di_ray[2ull * idx], d = b.di_ray[2ull * idx + 1];
+                r = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
+                trav_init(t, r, o.w);
+                active = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active && closest_step(s, r, t, stack)) {
+            b.di_hit[idx] = trav_hit(s, t);
+            active = false;
+        }
     }
 }
 
@@ -908,18 +922,36 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
 }
 
 // Stage 5: visibility of the chosen samples (an occluded sample keeps its
-// history count but loses its weight).
+// history count but loses its weight), with ray replacement.
 __global__ void __launch_bounds__(128) k_di_visibility(const __grid_constant__ DeviceScene s,
                                                        const __grid_constant__ RtBuffers b) {
     const uint32_t n = *b.di_count;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t idx = b.di_list[k];
-        const float4 o = b.di_ray[2ull * idx], d = b.di_ray[2ull * idx + 1];
-        if (trace_any(s, precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z)), o.w)) {
-            DiReservoir rsv = b.di_pass[idx];
-            rsv.W = 0.0f;
-            rsv.weight_sum = 0.0;
-            b.di_pass[idx] = rsv;
+    uint2 stack[kStackSize];
+    bool active = false, drained = false;
+    uint32_t idx = 0;
+    RayPre r;
+    TravState t;
+    for (;;) {
+        if (!drained) {
+            const uint32_t k = wf::refill(b.di_count + 2, n, active, drained);
+            if (k < n) {
+                idx = b.di_list[k];
+                const float4 o = b.di_ray[2ull * idx], d = b.di_ray[2ull * idx + 1];
+                r = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
+                trav_init(t, r, o.w);
+                active = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        bool occluded = false;
+        if (active && any_step(s, r, t, stack, occluded)) {
+            if (occluded) {
+                DiReservoir rsv = b.di_pass[idx];
+                rsv.W = 0.0f;
+                rsv.weight_sum = 0.0;
+                b.di_pass[idx] = rsv;
+            }
+            active = false;
         }
     }
 }
@@ -1451,15 +1483,21 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
     dim3 grid((p.width + 15) / 16, (p.height + 7) / 8);
     unsigned n = 0;
     if (p.M_bsdf <= 1u && b.di_stage) {
-        static unsigned g_list = 0;
-        if (!g_list) g_list = rt_wave_grid(k_di_lights);
-        cudaError_t e = cudaMemsetAsync(b.di_count, 0, sizeof(uint32_t), st);
+        // One resident wave of each list kernel (its own occupancy).
+        static unsigned g_lights = 0, g_trace = 0, g_eval = 0, g_vis = 0;
+        if (!g_lights) {
+            g_lights = rt_wave_grid(k_di_lights);
+            g_trace = rt_wave_grid(k_di_bsdf_trace);
+            g_eval = rt_wave_grid(k_di_bsdf_eval);
+            g_vis = rt_wave_grid(k_di_visibility);
+        }
+        cudaError_t e = cudaMemsetAsync(b.di_count, 0, 3 * sizeof(uint32_t), st);
         if (e != cudaSuccess) return e;
         k_di_primary<<<grid, block, 0, st>>>(s, p, b);
-        k_di_lights<<<g_list, 128, 0, st>>>(s, p, b);
-        k_di_bsdf_trace<<<g_list, 128, 0, st>>>(s, p, b);
-        k_di_bsdf_eval<<<g_list, 128, 0, st>>>(s, p, b);
-        k_di_visibility<<<g_list, 128, 0, st>>>(s, b);
+        k_di_lights<<<g_lights, 128, 0, st>>>(s, p, b);
+        k_di_bsdf_trace<<<g_trace, 128, 0, st>>>(s, p, b);
+        k_di_bsdf_eval<<<g_eval, 128, 0, st>>>(s, p, b);
+        k_di_visibility<<<g_vis, 128, 0, st>>>(s, b);
         k_di_temporal<<<grid, block, 0, st>>>(s, p, b);
         n += 6;
     } else {

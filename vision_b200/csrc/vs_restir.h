@@ -125,7 +125,7 @@ struct RtBuffers {
     // Staged direct pass (null: one kernel): per pixel 4 float4 of sampler
     // state, wavelengths, film position and primary-ray direction; 2 float4
     // of the pending ray; the BSDF candidate's hit; the list of pixels that
-    // see a surface and its length.
+    // see a surface; its length and the two traversal stages' fetch counters.
     float4 *di_stage;
     float4 *di_ray;
     Hit *di_hit;
