@@ -155,6 +155,10 @@ struct vs_scene {
         DevBuf<float4> di_stage, di_ray;
         DevBuf<Hit> di_hit;
         DevBuf<uint32_t> di_list, di_count;
+        DevBuf<float2> gs_nb;
+        DevBuf<float4> gs_ray;
+        DevBuf<uint8_t> gs_vis;
+        DevBuf<uint32_t> gs_list, gs_count;
         uint32_t width = 0, height = 0;
         bool have_prev = false;
         Camera prev_cam{};
@@ -169,6 +173,7 @@ struct vs_scene {
             hit_bsdf.free(); motion.free(); di_pass.free(); gi_pass.free(); gi_init.free();
             di_radiance.free(); gi_radiance.free();
             di_stage.free(); di_ray.free(); di_hit.free(); di_list.free(); di_count.free();
+            gs_nb.free(); gs_ray.free(); gs_vis.free(); gs_list.free(); gs_count.free();
         }
         RtBuffers view() const {
             RtBuffers b{};
@@ -190,6 +195,11 @@ struct vs_scene {
             b.di_hit = di_hit.ptr;
             b.di_list = di_list.ptr;
             b.di_count = di_count.ptr;
+            b.gs_nb = gs_nb.ptr;
+            b.gs_ray = gs_ray.ptr;
+            b.gs_vis = gs_vis.ptr;
+            b.gs_list = gs_list.ptr;
+            b.gs_count = gs_count.ptr;
             return b;
         }
     } rt;
@@ -870,6 +880,11 @@ int rt_ensure(vs_scene *s, cudaStream_t st) {
     VS_CUDA(r.di_hit.alloc(n), "restir alloc");
     VS_CUDA(r.di_list.alloc(n), "restir alloc");
     VS_CUDA(r.di_count.alloc(3), "restir alloc");
+    VS_CUDA(r.gs_nb.alloc(n * kMaxSpatialNeighbours), "restir alloc");
+    VS_CUDA(r.gs_ray.alloc(2 * n * kMaxSpatialNeighbours), "restir alloc");
+    VS_CUDA(r.gs_vis.alloc(n * kMaxSpatialNeighbours), "restir alloc");
+    VS_CUDA(r.gs_list.alloc(n * kMaxSpatialNeighbours), "restir alloc");
+    VS_CUDA(r.gs_count.alloc(2), "restir alloc");
     r.width = w;
     r.height = hgt;
     r.have_prev = false;

@@ -1,14 +1,21 @@
 // sm_100a kernels of the real-time ReSTIR frame (RealTimeIntegrator::render,
 // src/render_core/integrators/rt.cpp:144-160):
 //   k_rt_reset        - default surfaces and reservoirs (ReSTIRDI/GI::prepare)
-//   k_di_candidates   - primary hit with its near-specular chain, RIS over
-//                       M_light light + M_bsdf BSDF candidates, visibility,
-//                       motion vector, temporal reuse (direct.cpp:519-557)
+//   k_di_primary .. k_di_temporal
+//                     - the direct pass (direct.cpp:519-557) in six stages:
+//                       primary hit with its near-specular chain and motion
+//                       vector, RIS over M_light light candidates, the BSDF
+//                       candidate's ray, its evaluation, visibility, temporal
+//                       reuse; k_di_candidates does it in one kernel (used when
+//                       M_bsdf > 1)
 //   k_di_spatial      - spatial reuse and shading (direct.cpp:638-674)
-//   k_gi_initial      - one path suffix per pixel from the direct pass's BSDF
-//                       direction (indirect.cpp:83-111)
+//   k_gi_wf_*         - one path suffix per pixel from the direct pass's BSDF
+//                       direction (indirect.cpp:83-111) as wavefront passes;
+//                       k_gi_initial does it in one kernel (grid and
+//                       persistent schedules)
 //   k_gi_temporal     - GI temporal reuse (indirect.cpp:205-236)
-//   k_gi_spatial      - GI spatial reuse and shading (indirect.cpp:311-332)
+//   k_gi_sp_*         - GI spatial reuse and shading (indirect.cpp:238-332) in
+//                       three stages (neighbours, visibility rays, combine)
 //   k_rt_combine      - direct * di + indirect * ii into the film (rt.cpp:118-126)
 // One thread per pixel, 16 x 8 pixel tiles.  Spectral work runs on 3 hero
 // wavelengths: the reference's ReSTIR code moves spectra through float3
@@ -1380,10 +1387,19 @@ __global__ void __launch_bounds__(128) k_gi_temporal(const __grid_constant__ Dev
     b.gi_pass[idx] = rsv;
 }
 
-// ReSTIRGI spatial reuse and shading (indirect.cpp:238-332).
+// ---------------------------------------------------------------------------
+// ReSTIRGI spatial reuse and shading (indirect.cpp:238-332) in stages, so its
+// visibility rays (one per neighbour) run in a small traversal kernel:
+// k_gi_sp_select picks the neighbours (same draws as the reference),
+// computes each one's target pdf, Jacobian and weight and queues its
+// visibility ray; k_gi_sp_vis traces them; k_gi_sp_combine merges the
+// neighbours in order (same draws) and shades.  Per pixel the stages pass the
+// sampler state and wavelengths through b.di_stage (free after the direct
+// pass) and the neighbours through b.gs_nb.
+// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
-    k_gi_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
-                 const __grid_constant__ RtBuffers b) {
+    k_gi_sp_select(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                   const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -1393,16 +1409,14 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
     if (cs.hit.inst_id == kInvalid) return;
     Sampler smp;
     smp.start(x, y, p.frame, 5u, s.ip.sampler, s.ip.seed);
-    GiReservoir rsv = b.gi_pass[idx];
     f3 view_pos = p.view_pos;
     if (cs.is_replaced) {
         RtSurfaceExt e = b.ext[cur][idx];
         view_pos = make3(e.vx, e.vy, e.vz);
     }
     Interaction cit = it_at(s, cs.hit, view_pos);
+    uint32_t count = 0;
     if (p.gi.spatial) {
-        uint32_t nb[kMaxSpatialNeighbours];
-        uint32_t count = 0;
         for (uint32_t i = 0; i < p.gi.s_count; ++i) {
             f2 d = square_to_disk2(smp.next2());
             int qx = static_cast<int>(x) + f2i(roundf(d.x * p.gi.s_radius));
@@ -1411,25 +1425,107 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
             qy = min(max(qy, 0), static_cast<int>(p.height) - 1);
             uint32_t q = pixel_index(p, static_cast<uint32_t>(qx), static_cast<uint32_t>(qy));
             RtSurface os = b.surf[cur][q];
-            if (valid_neighbor(cs, os, p.gi.s_dot, p.gi.s_depth, p.gi.diff_factor)) nb[count++] = q;
+            if (valid_neighbor(cs, os, p.gi.s_dot, p.gi.s_depth, p.gi.diff_factor)) {
+                const size_t e = static_cast<size_t>(idx) * kMaxSpatialNeighbours + count;
+                float w = 0.0f;
+                GiReservoir nr = b.gi_pass[q];
+                if (lum3(ld3p(nr.Lo)) > 0.0f) {
+                    RtSurface ns = b.surf[cur][q];
+                    Interaction nit = it_at(s, ns.hit, view_pos);
+                    float ph = gi_p_hat(s, cit, nr, wl) * jacobian(cit.pos, nit.pos, nr);
+                    w = safe_weight(nr.C, ph, nr.W);
+                    const Ray sh = spawn_ray_to(cit.pos, cit.ng, ld3p(nr.sp_pos));
+                    b.gs_ray[2 * e] = make_float4(sh.o.x, sh.o.y, sh.o.z, sh.tmax);
+                    b.gs_ray[2 * e + 1] = make_float4(sh.d.x, sh.d.y, sh.d.z, 0.0f);
+                    b.gs_vis[e] = 1u;
+                    b.gs_list[wf::queue_push(b.gs_count)] = static_cast<uint32_t>(e);
+                }
+                b.gs_nb[e] = make_float2(__uint_as_float(q), w);
+                ++count;
+            }
         }
-        // ReSTIRGI::constant_combine (indirect.cpp:238-262).
+    }
+    float4 *st = b.di_stage + 4ull * idx;
+    st[0] = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.pdf[0]);
+    st[1] = make_float4(wl.pdf[1], wl.pdf[2], __uint_as_float(count), 0.0f);
+    st[2] = make_float4(__uint_as_float(static_cast<uint32_t>(smp.state)),
+                        __uint_as_float(static_cast<uint32_t>(smp.state >> 32)), 0.0f, 0.0f);
+}
+
+// Visibility of the queued neighbour samples (ray replacement).
+__global__ void __launch_bounds__(128) k_gi_sp_vis(const __grid_constant__ DeviceScene s,
+                                                   const __grid_constant__ RtBuffers b) {
+    const uint32_t n = b.gs_count[0];
+    uint2 stack[kStackSize];
+    bool active = false, drained = false;
+    uint32_t e = 0;
+    RayPre r;
+    TravState t;
+    for (;;) {
+        if (!drained) {
+            const uint32_t k = wf::refill(b.gs_count + 1, n, active, drained);
+            if (k < n) {
+                e = b.gs_list[k];
+                const float4 o = b.gs_ray[2ull * e], d = b.gs_ray[2ull * e + 1];
+                r = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
+                trav_init(t, r, o.w);
+                active = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        bool occluded = false;
+        if (active && any_step(s, r, t, stack, occluded)) {
+            if (occluded) b.gs_vis[e] = 0u;
+            active = false;
+        }
+    }
+}
+
+// ReSTIRGI::constant_combine (indirect.cpp:238-262) and shading (:264-278).
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_gi_sp_combine(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                    const __grid_constant__ RtBuffers b) {
+    uint32_t x, y;
+    if (!tile_pixel(p, x, y)) return;
+    const uint32_t idx = pixel_index(p, x, y);
+    const uint32_t cur = (p.frame + 1u) & 1u;
+    RtSurface cs = b.surf[cur][idx];
+    if (cs.hit.inst_id == kInvalid) return;
+    const float4 *st = b.di_stage + 4ull * idx;
+    const float4 s0 = st[0], s1 = st[1], s2 = st[2];
+    RWl wl;
+    wl.lambda[0] = s0.x;
+    wl.lambda[1] = s0.y;
+    wl.lambda[2] = s0.z;
+    wl.pdf[0] = s0.w;
+    wl.pdf[1] = s1.x;
+    wl.pdf[2] = s1.y;
+    const uint32_t count = __float_as_uint(s1.z);
+    Sampler smp;
+    smp.kind = s.ip.sampler;
+    smp.seed = s.ip.seed;
+    smp.state = static_cast<uint64_t>(__float_as_uint(s2.x)) | (static_cast<uint64_t>(__float_as_uint(s2.y)) << 32);
+    GiReservoir rsv = b.gi_pass[idx];
+    f3 view_pos = p.view_pos;
+    if (cs.is_replaced) {
+        RtSurfaceExt e = b.ext[cur][idx];
+        view_pos = make3(e.vx, e.vy, e.vz);
+    }
+    Interaction cit = it_at(s, cs.hit, view_pos);
+    if (p.gi.spatial) {
         GiReservoir ret = rsv;
         for (uint32_t k = 0; k < count; ++k) {
-            GiReservoir nr = b.gi_pass[nb[k]];
+            const size_t e = static_cast<size_t>(idx) * kMaxSpatialNeighbours + k;
+            const float2 nbw = b.gs_nb[e];
+            GiReservoir nr = b.gi_pass[__float_as_uint(nbw.x)];
             if (lum3(ld3p(nr.Lo)) > 0.0f) {
-                RtSurface ns = b.surf[cur][nb[k]];
-                Interaction nit = it_at(s, ns.hit, view_pos);
-                float ph = gi_p_hat(s, cit, nr, wl) * jacobian(cit.pos, nit.pos, nr);
-                float v = occluded_to(s, cit, ld3p(nr.sp_pos)) ? 0.0f : 1.0f;
-                float w = safe_weight(nr.C, ph, nr.W);
-                gi_update(ret, smp.next(), nr, w * v, nr.C * v);
+                float v = b.gs_vis[e] ? 1.0f : 0.0f;
+                gi_update(ret, smp.next(), nr, nbw.y * v, nr.C * v);
             }
         }
         gi_update_W(ret, gi_p_hat(s, cit, ret, wl));
         rsv = ret;
     }
-    // ReSTIRGI::shading (indirect.cpp:264-278).
     f3 L = ld3p(rsv.Lo) * gi_f(s, cit, rsv, wl) * rsv.W;
     b.gi_radiance[idx] = make_float4(L.x, L.y, L.z, 1.0f);
     b.gi[cur][idx] = rsv;
@@ -1551,7 +1647,16 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
         ++n;
     }
     k_gi_temporal<<<grid, block, 0, st>>>(s, p, b);
-    k_gi_spatial<<<grid, block, 0, st>>>(s, p, b);
+    {
+        static unsigned g_vis = 0;
+        if (!g_vis) g_vis = rt_wave_grid(k_gi_sp_vis);
+        cudaError_t e = cudaMemsetAsync(b.gs_count, 0, 2 * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        k_gi_sp_select<<<grid, block, 0, st>>>(s, p, b);
+        k_gi_sp_vis<<<g_vis, 128, 0, st>>>(s, b);
+        k_gi_sp_combine<<<grid, block, 0, st>>>(s, p, b);
+        n += 2;
+    }
     n += 2;
     uint32_t npix = p.width * p.height;
     k_rt_combine<<<(npix + 255) / 256, 256, 0, st>>>(npix, b, p.di_factor, p.gi_factor, film_index, film);

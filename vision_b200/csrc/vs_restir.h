@@ -131,6 +131,13 @@ struct RtBuffers {
     Hit *di_hit;
     uint32_t *di_list;
     uint32_t *di_count;
+    // Staged indirect spatial pass, kMaxSpatialNeighbours entries per pixel: neighbour index (bits) and weight; visibility ray;
+    // visibility; the queued entries, their count and the fetch counter.
+    float2 *gs_nb;
+    float4 *gs_ray;
+    uint8_t *gs_vis;
+    uint32_t *gs_list;
+    uint32_t *gs_count;
 };
 
 }  // namespace vs
