@@ -8,7 +8,8 @@
 //                       candidate's ray, its evaluation, visibility, temporal
 //                       reuse; k_di_candidates does it in one kernel (used when
 //                       M_bsdf > 1)
-//   k_di_spatial      - spatial reuse and shading (direct.cpp:638-674)
+//   k_di_sp_*         - spatial reuse and shading (direct.cpp:638-674) in three
+//                       stages (combine, shading rays, shading)
 //   k_gi_wf_*         - one path suffix per pixel from the direct pass's BSDF
 //                       direction (indirect.cpp:83-111) as wavefront passes;
 //                       k_gi_initial does it in one kernel (grid and
@@ -682,7 +683,7 @@ __global__ void k_rt_reset(uint32_t npix, const __grid_constant__ RtBuffers b) {
 // Minimum resident blocks per SM of the candidate and spatial kernels (a
 // register budget).  3 blocks of 128 (at most 170 registers) measured 5 %
 // faster on the many-light frame than the compiler's own 207 registers
-// (2 blocks), despite the spills it causes in k_di_spatial.
+// (2 blocks), despite the spills it caused in the one-kernel spatial pass.
 #ifndef VS_RT_MIN_BLOCKS
 #define VS_RT_MIN_BLOCKS 3
 #endif
@@ -1026,45 +1027,19 @@ __device__ VS_OUTLINE DiReservoir di_combine_spatial(const DeviceScene &s, const
     return ret;
 }
 
-// ReSTIRDI::shading (direct.cpp:583-636).  The BSDF-sampled emission the
-// reference computes there is overwritten before use, so it is not traced.
-__device__ VS_OUTLINE f3 di_shading(const DeviceScene &s, const RtParams &p, const RtBuffers &b, DiReservoir rsv,
-                                    const RtSurface &cs, uint32_t idx, RWl &wl) {
-    const uint32_t cur = (p.frame + 1u) & 1u;
-    f3 view_pos = p.view_pos;
-    f3 tp = make3(1.0f);
-    if (cs.is_replaced) {
-        RtSurfaceExt e = b.ext[cur][idx];
-        tp = make3(e.tx, e.ty, e.tz);
-        view_pos = make3(e.vx, e.vy, e.vz);
-    }
-    Interaction it = it_at(s, cs.hit, view_pos);
-    RSpec value = RSpec::fill(0.0f);
-    RSpec Le = RSpec::fill(0.0f);
-    if (it.light != kInvalid) {
-        AreaLight L = s.lights[it.light];
-        LightPoint lp{it.pos, it.ng, it.prim_area};
-        Le = area_Le(L, lp, p.view_pos, wl);
-    } else {
-        Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
-        RSpec f;
-        di_p_hat(s, it, bsdf, rsv, wl, nullptr, nullptr, &f);
-        value = f * spec3(tp) * (1.0f / lum3(tp));
-        if (occluded_to(s, it, ld3p(rsv.pos))) {
-            rsv.W = 0.0f;
-            rsv.weight_sum = 0.0;
-        }
-        value = value * rsv.W;
-    }
-    return linear_srgb<RN>(value + Le, wl);
-}
 
 }  // namespace
 
-// ReSTIRDI shader1 (direct.cpp:638-674).
+
+// ReSTIRDI shader1 (direct.cpp:638-674) in stages, so the shading ray runs in
+// a small traversal kernel: k_di_sp_combine (neighbours and combine; pixels
+// that see nothing or an emitter are shaded here), k_di_sp_vis (the shading
+// rays of the others), k_di_sp_shade (ReSTIRDI::shading with that
+// visibility).  The shading rays and the listed pixels reuse the direct
+// pass's ray and list buffers; the wavelengths pass through b.di_stage.
 __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
-    k_di_spatial(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
-                 const __grid_constant__ RtBuffers b) {
+    k_di_sp_combine(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                    const __grid_constant__ RtBuffers b) {
     uint32_t x, y;
     if (!tile_pixel(p, x, y)) return;
     const uint32_t idx = pixel_index(p, x, y);
@@ -1078,6 +1053,11 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
     smp.start(x, y, p.frame, 1u, s.ip.sampler, s.ip.seed);
     RtSurface cs = b.surf[cur][idx];
     DiReservoir rsv = b.di_pass[idx];
+    f3 view_pos = p.view_pos;
+    if (cs.is_replaced) {
+        RtSurfaceExt e = b.ext[cur][idx];
+        view_pos = make3(e.vx, e.vy, e.vz);
+    }
     if (p.di.spatial) {
         uint32_t nb[kMaxSpatialNeighbours];
         uint32_t count = 0;
@@ -1091,17 +1071,102 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
             RtSurface os = b.surf[cur][q];
             if (valid_neighbor(cs, os, p.di.s_dot, p.di.s_depth, p.di.diff_factor)) nb[count++] = q;
         }
-        f3 view_pos = p.view_pos;
-        if (cs.is_replaced) {
-            RtSurfaceExt e = b.ext[cur][idx];
-            view_pos = make3(e.vx, e.vy, e.vz);
-        }
         if (cs.hit.inst_id != kInvalid) rsv = di_combine_spatial(s, p, b, rsv, cs, view_pos, nb, count, smp, wl);
     }
-    f3 L = make3(0.0f);
-    if (cs.hit.inst_id != kInvalid) L = di_shading(s, p, b, rsv, cs, idx, wl);
-    b.di_radiance[idx] = make_float4(L.x, L.y, L.z, 1.0f);
     b.di[cur][idx] = rsv;
+    f3 L = make3(0.0f);
+    if (cs.hit.inst_id != kInvalid) {
+        Interaction it = it_at(s, cs.hit, view_pos);
+        if (it.light != kInvalid) {
+            AreaLight Ls = s.lights[it.light];
+            LightPoint lp{it.pos, it.ng, it.prim_area};
+            RSpec Le = area_Le(Ls, lp, p.view_pos, wl);
+            L = linear_srgb<RN>(RSpec::fill(0.0f) + Le, wl);
+        } else {
+            const Ray sh = spawn_ray_to(it.pos, it.ng, ld3p(rsv.pos));
+            b.di_ray[2ull * idx] = make_float4(sh.o.x, sh.o.y, sh.o.z, sh.tmax);
+            b.di_ray[2ull * idx + 1] = make_float4(sh.d.x, sh.d.y, sh.d.z, 0.0f);
+            float4 *st = b.di_stage + 4ull * idx;
+            st[0] = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.pdf[0]);
+            st[1] = make_float4(wl.pdf[1], wl.pdf[2], 0.0f, 0.0f);
+            b.di_list[wf::queue_push(b.di_count)] = idx;
+            return;
+        }
+    }
+    b.di_radiance[idx] = make_float4(L.x, L.y, L.z, 1.0f);
+}
+
+// Shading rays of the listed pixels (ray replacement); w of the direction
+// record becomes 1 when the ray is occluded.
+__global__ void __launch_bounds__(128) k_di_sp_vis(const __grid_constant__ DeviceScene s,
+                                                   const __grid_constant__ RtBuffers b) {
+    const uint32_t n = *b.di_count;
+    uint2 stack[kStackSize];
+    bool active = false, drained = false;
+    uint32_t idx = 0;
+    RayPre r;
+    TravState t;
+    for (;;) {
+        if (!drained) {
+            const uint32_t k = wf::refill(b.di_count + 1, n, active, drained);
+            if (k < n) {
+                idx = b.di_list[k];
+                const float4 o = b.di_ray[2ull * idx], d = b.di_ray[2ull * idx + 1];
+                r = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));
+                trav_init(t, r, o.w);
+                active = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        bool occluded = false;
+        if (active && any_step(s, r, t, stack, occluded)) {
+            b.di_ray[2ull * idx + 1].w = occluded ? 1.0f : 0.0f;
+            active = false;
+        }
+    }
+}
+
+// ReSTIRDI::shading (direct.cpp:583-636) of the listed pixels.  The
+// BSDF-sampled emission the reference computes there is overwritten before
+// use, so it is not traced.
+__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+    k_di_sp_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
+                  const __grid_constant__ RtBuffers b) {
+    const uint32_t n = *b.di_count;
+    const uint32_t cur = (p.frame + 1u) & 1u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t idx = b.di_list[k];
+        const RtSurface cs = b.surf[cur][idx];
+        DiReservoir rsv = b.di[cur][idx];
+        const float4 *st = b.di_stage + 4ull * idx;
+        const float4 s0 = st[0], s1 = st[1];
+        RWl wl;
+        wl.lambda[0] = s0.x;
+        wl.lambda[1] = s0.y;
+        wl.lambda[2] = s0.z;
+        wl.pdf[0] = s0.w;
+        wl.pdf[1] = s1.x;
+        wl.pdf[2] = s1.y;
+        f3 view_pos = p.view_pos;
+        f3 tp = make3(1.0f);
+        if (cs.is_replaced) {
+            RtSurfaceExt e = b.ext[cur][idx];
+            tp = make3(e.tx, e.ty, e.tz);
+            view_pos = make3(e.vx, e.vy, e.vz);
+        }
+        Interaction it = it_at(s, cs.hit, view_pos);
+        Bsdf<RN, VS_RT_MATERIALS> bsdf = bsdf_at(s, it, wl);
+        RSpec f;
+        di_p_hat(s, it, bsdf, rsv, wl, nullptr, nullptr, &f);
+        RSpec value = f * spec3(tp) * (1.0f / lum3(tp));
+        if (b.di_ray[2ull * idx + 1].w != 0.0f) {
+            rsv.W = 0.0f;
+            rsv.weight_sum = 0.0;
+        }
+        value = value * rsv.W;
+        const f3 L = linear_srgb<RN>(value + RSpec::fill(0.0f), wl);
+        b.di_radiance[idx] = make_float4(L.x, L.y, L.z, 1.0f);
+    }
 }
 
 namespace {
@@ -1601,8 +1666,17 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
         ++n;
     }
     if (p.di.open) {
-        k_di_spatial<<<grid, block, 0, st>>>(s, p, b);
-        ++n;
+        static unsigned g_vis = 0, g_shade = 0;
+        if (!g_vis) {
+            g_vis = rt_wave_grid(k_di_sp_vis);
+            g_shade = rt_wave_grid(k_di_sp_shade);
+        }
+        cudaError_t e = cudaMemsetAsync(b.di_count, 0, 3 * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        k_di_sp_combine<<<grid, block, 0, st>>>(s, p, b);
+        k_di_sp_vis<<<g_vis, 128, 0, st>>>(s, b);
+        k_di_sp_shade<<<g_shade, 128, 0, st>>>(s, p, b);
+        n += 3;
     }
     if (wf && radiance) {
         static unsigned g_ext = 0, g_shadow = 0, g_shade[kWfClasses] = {};
