@@ -462,6 +462,16 @@ __device__ __forceinline__ DiReservoir di_ris_lights(const DeviceScene &s, const
     // candidates' dependent fetches (light table, primitive table, vertices)
     // are in flight together; the reservoir sees them in the same order.
     uint32_t i = 0;
+#ifdef VS_RIS_SINGLE
+    for (; i < p.M_light; ++i) {
+        const float s0 = smp.next();
+        const f2 u0 = smp.next2();
+        DiReservoir c0;
+        float w0;
+        candidate(s0, u0, c0, w0);
+        di_update(ret, smp.next(), c0, w0);
+    }
+#endif
     for (; i + 1 < p.M_light; i += 2) {
         const float s0 = smp.next();
         const f2 u0 = smp.next2();
