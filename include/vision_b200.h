@@ -218,7 +218,7 @@ int vs_restir_reset(vs_scene *scene);
 /* Parameter block that vs_restir_frame(scene, frame_index, ...) would use now
  * (resampling settings, camera transforms, previous camera):
  * VS_RESTIR_PARAMS_BYTES bytes.  Works on host-only contexts. */
-#define VS_RESTIR_PARAMS_BYTES 432
+#define VS_RESTIR_PARAMS_BYTES 448
 int vs_restir_params(const vs_scene *scene, uint32_t frame_index, void *dst, size_t bytes);
 
 /* Copies a per-pixel ReSTIR buffer of the last frame to host memory. */

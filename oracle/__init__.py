@@ -156,7 +156,7 @@ class OracleRestir:
     def frame(self, camera, params, film_index, threads=None):
         camera = np.ascontiguousarray(camera).view(np.uint8)
         params = np.ascontiguousarray(params).view(np.uint8)
-        assert camera.nbytes == 112 and params.nbytes == 432
+        assert camera.nbytes == 128 and params.nbytes == 448
         rc = lib().oracle_rt_frame(self.h, _p(camera), _p(params), film_index, threads or os.cpu_count())
         if rc != 0:
             raise ValueError('oracle_rt_frame rejected the parameters')

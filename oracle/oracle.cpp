@@ -71,8 +71,11 @@ struct Camera {
     float tan_half_fov, screen_lo_x, screen_hi_y, screen_span_x, screen_span_y, filter_rx, filter_ry;
     uint32_t width, height;
     float exposure;
-    uint32_t pad0, pad1;
+    uint32_t filter;     // 0 box, 1 triangle, 2 gaussian, 3 mitchell, 4 sinc
+    uint32_t thin_lens;  // 1: ThinLensCamera
+    float lens_radius, focal_distance, filter_p0, filter_p1;
 };
+static_assert(sizeof(Camera) == 128, "Camera layout");
 struct EnvLight {
     float w2o[4][4];
     float o2w[4][4];
@@ -295,6 +298,11 @@ struct Scene {
     };
     std::vector<Node> nodes;
     std::vector<uint32_t> order;
+    // FilterSampler tables (fitted_curve.h:36-58) of the tabulated filters.
+    static constexpr uint32_t kFilterN = 20;
+    std::vector<float> f_lut, f_marginal_func, f_cond_func;
+    std::vector<Alias> f_marginal, f_cond;
+    float f_integral = 0.0f;
 
     V3 P(uint32_t v) const { return {s->pos[3 * v], s->pos[3 * v + 1], s->pos[3 * v + 2]}; }
     V3 N(uint32_t v) const { return {s->nrm[3 * v], s->nrm[3 * v + 1], s->nrm[3 * v + 2]}; }
@@ -349,6 +357,93 @@ struct Scene {
         return id;
     }
 
+    // AliasTable::build (warpers/alias.h:86-118): probabilities scaled by
+    // n / sum (sum in double), over-full slots fill under-full ones from the
+    // back of both lists; the row integral is sum / n.
+    static float alias_build(const float *w, uint32_t n, Alias *out) {
+        double total = 0.0;
+        for (uint32_t i = 0; i < n; ++i) total += w[i];
+        const double scale = static_cast<double>(n) / total;
+        std::vector<uint32_t> big, small;
+        for (uint32_t i = 0; i < n; ++i) {
+            out[i].prob = static_cast<float>(w[i] * scale);
+            out[i].alias = i;
+            if (out[i].prob > 1.0f) big.push_back(i);
+            else small.push_back(i);
+        }
+        while (!big.empty() && !small.empty()) {
+            const uint32_t b = big.back(), l = small.back();
+            big.pop_back();
+            small.pop_back();
+            out[b].prob -= 1.0f - out[l].prob;
+            out[l].alias = b;
+            if (out[b].prob > 1.0f) big.push_back(b);
+            else if (out[b].prob < 1.0f) small.push_back(b);
+        }
+        for (uint32_t i : big) out[i] = {1.0f, i};
+        for (uint32_t i : small) out[i] = {1.0f, i};
+        return static_cast<float>(total / static_cast<double>(n));
+    }
+
+    // GaussianFilter / MitchellFilter / LanczosSincFilter ::evaluate
+    // (filters/gaussian.cpp:36-40, mitchell.cpp, sinc.cpp) at p in [0, r]^2.
+    float filter_eval(float x, float y) const {
+        const float pi = 3.14159265358979323846f;
+        if (cam.filter == 2u) {
+            const float sg = cam.filter_p0;
+            auto gauss = [&](float v) { return 1.0f / std::sqrt(2.0f * pi * sg * sg) * std::exp(-(v * v) / (2.0f * sg * sg)); };
+            return std::max(0.0f, gauss(x) - gauss(cam.filter_rx)) * std::max(0.0f, gauss(y) - gauss(cam.filter_ry));
+        }
+        if (cam.filter == 3u) {
+            const float B = cam.filter_p0, C = cam.filter_p1;
+            auto mitchell = [&](float v) {
+                v = std::fabs(v);
+                float r = 0.0f;
+                if (v <= 1.0f)
+                    r = (12.0f - 9.0f * B - 6.0f * C) * v * v * v + (-18.0f + 12.0f * B + 6.0f * C) * v * v +
+                        (6.0f - 2.0f * B);
+                else if (v <= 2.0f)
+                    r = (-B - 6.0f * C) * v * v * v + (6.0f * B + 30.0f * C) * v * v + (-12.0f * B - 48.0f * C) * v +
+                        (8.0f * B + 24.0f * C);
+                return r * (1.0f / 6.0f);
+            };
+            return mitchell(2.0f * x / cam.filter_rx) * mitchell(2.0f * y / cam.filter_ry);
+        }
+        const float tau = cam.filter_p0;
+        auto sinc = [&](float v) {
+            const float a = pi * v;
+            return 1.0f + a * a == 1.0f ? 1.0f : std::sin(a) / a;
+        };
+        auto windowed = [&](float v, float r) { return std::fabs(v) > r ? 0.0f : sinc(v) * sinc(v / tau); };
+        return windowed(x, cam.filter_rx) * windowed(y, cam.filter_ry) * 4.0f;
+    }
+
+    // FilterSampler::build (fitted_curve.h:36-58) + AliasTable2D::build
+    // (warpers/alias2d.cpp:32-67): the filter at cell centres of [0, r]^2,
+    // normalised by its average; rows and marginal over |filter|.
+    void build_filter() {
+        const uint32_t n = kFilterN;
+        f_lut.assign(n * n, 0.0f);
+        f_cond_func.assign(n * n, 0.0f);
+        for (uint32_t y = 0; y < n; ++y)
+            for (uint32_t x = 0; x < n; ++x) {
+                const float v = filter_eval((static_cast<float>(x) + 0.5f) / static_cast<float>(n) * cam.filter_rx,
+                                            (static_cast<float>(y) + 0.5f) / static_cast<float>(n) * cam.filter_ry);
+                f_lut[y * n + x] = v;
+                f_cond_func[y * n + x] = std::fabs(v);
+            }
+        float total = 0.0f;
+        for (float v : f_lut) total += v;
+        const float mean = total / static_cast<float>(n * n);
+        for (float &v : f_lut) v = v / mean;
+        f_cond.resize(n * n);
+        f_marginal_func.resize(n);
+        for (uint32_t y = 0; y < n; ++y)
+            f_marginal_func[y] = alias_build(f_cond_func.data() + y * n, n, f_cond.data() + y * n);
+        f_marginal.resize(n);
+        f_integral = alias_build(f_marginal_func.data(), n, f_marginal.data());
+    }
+
     explicit Scene(const oracle_scene *sc) : s(sc) {
         inst = static_cast<const Instance *>(sc->instances);
         mat = static_cast<const Material *>(sc->materials);
@@ -361,6 +456,7 @@ struct Scene {
             std::memcpy(&env, sc->env, sizeof(EnvLight));
             has_env = true;
         }
+        if (cam.filter >= 2u) build_filter();
         order.resize(sc->prim_count);
         for (uint32_t i = 0; i < sc->prim_count; ++i) order[i] = i;
         nodes.reserve(sc->prim_count / 2 + 8);
@@ -1185,22 +1281,77 @@ static void check_dispersive(const Bsdf &bsdf, Swl &w) {
     }
 }
 
-// Sampler::sensor_sample + box filter + Sensor::generate_ray (5 draws).
-static void camera_ray(const Camera &cam, Sampler &smp, uint32_t px, uint32_t py, float &film_x, float &film_y, V3 &ro,
-                       V3 &rd) {
+// math/warp.h:132-145 sample_linear / sample_tent (the tent filter).
+static float sample_linear_o(float u, float a, float b) {
+    float x = u * (a + b) / (a + std::sqrt(a * a + u * (b * b - a * a)));
+    x = std::min(x, kOneMinusEps);
+    return (u == 0.0f && a == 0.0f) ? 0.0f : x;
+}
+static float sample_tent_o(float u, float r) {
+    return u < 0.5f ? -r * sample_linear_o((0.5f - u) * 2.0f, 1.0f, 0.0f)
+                    : r * sample_linear_o((u - 0.5f) * 2.0f, 1.0f, 0.0f);
+}
+static float sign_o(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+
+// FilterSampler::sample (fitted_curve.h:72-80) over the scene's filter table.
+static void fitted_sample(const Scene &sc, float ux, float uy, float &fx, float &fy, float &weight) {
+    const uint32_t n = Scene::kFilterN;
+    ux = ux * 2.0f - 1.0f;
+    uy = uy * 2.0f - 1.0f;
+    uint32_t iv, iu;
+    float fv = alias_cont(sc.f_marginal.data(), n, std::fabs(uy), iv);
+    float pdf_v = sc.f_integral > 0.0f ? sc.f_marginal_func[iv] / sc.f_integral : 0.0f;
+    float fu = alias_cont(sc.f_cond.data() + iv * n, n, std::fabs(ux), iu);
+    float integral_u = sc.f_marginal_func[iv];
+    float pdf_u = integral_u > 0.0f ? sc.f_cond_func[iv * n + iu] / integral_u : 0.0f;
+    weight = sc.f_lut[iv * n + iu] / (pdf_u * pdf_v);
+    fx = fu * sign_o(ux);
+    fy = fv * sign_o(uy);
+}
+
+// Sampler::sensor_sample + the scene's filter + Sensor::generate_ray, with
+// ThinLensCamera's lens (thin_lens.cpp:36-43) (5 draws); returns the filter
+// weight.
+static float camera_ray(const Scene &sc, const Camera &cam, Sampler &smp, uint32_t px, uint32_t py, float &film_x,
+                        float &film_y, V3 &ro, V3 &rd) {
     float fu = smp.next(), fv = smp.next();
-    float fx = -cam.filter_rx + fu * (cam.filter_rx - -cam.filter_rx);
-    float fy = -cam.filter_ry + fv * (cam.filter_ry - -cam.filter_ry);
-    smp.next(); smp.next(); smp.next();
+    float fx, fy, weight = 1.0f;
+    if (cam.filter == 0u) {
+        fx = -cam.filter_rx + fu * (cam.filter_rx - -cam.filter_rx);
+        fy = -cam.filter_ry + fv * (cam.filter_ry - -cam.filter_ry);
+    } else if (cam.filter == 1u) {
+        fx = sample_tent_o(fu, cam.filter_rx);
+        fy = sample_tent_o(fv, cam.filter_ry);
+    } else {
+        fitted_sample(sc, fu, fv, fx, fy, weight);
+        fx *= cam.filter_rx;
+        fy *= cam.filter_ry;
+    }
+    float lu = smp.next(), lv = smp.next();
+    smp.next();
     film_x = static_cast<float>(px) + 0.5f + fx;
     film_y = static_cast<float>(py) + 0.5f + fy;
     float sx = cam.screen_lo_x + film_x / static_cast<float>(cam.width) * cam.screen_span_x;
     float sy = cam.screen_hi_y - film_y / static_cast<float>(cam.height) * cam.screen_span_y;
     V3 dc = normalize(v3(sx * cam.tan_half_fov, sy * cam.tan_half_fov, 1.0f));
     const float(*m)[4] = cam.c2w;
-    ro = {m[3][0], m[3][1], m[3][2]};
+    V3 o_local = {0.0f, 0.0f, 0.0f};
+    if (cam.thin_lens) {
+        // square_to_disk (warp.h:24-28): r = sqrt(u.x), theta = 2 pi u.y.
+        float r = std::sqrt(lu), th = 2.0f * kPi * lv;
+        o_local = {r * std::cos(th) * cam.lens_radius, r * std::sin(th) * cam.lens_radius, 0.0f};
+        float ft = cam.focal_distance / dc.z;
+        V3 pf = {dc.x * ft, dc.y * ft, dc.z * ft};
+        dc = normalize(v3(pf.x - o_local.x, pf.y - o_local.y, pf.z - o_local.z));
+        ro = {m[0][0] * o_local.x + m[1][0] * o_local.y + m[2][0] * o_local.z + m[3][0],
+              m[0][1] * o_local.x + m[1][1] * o_local.y + m[2][1] * o_local.z + m[3][1],
+              m[0][2] * o_local.x + m[1][2] * o_local.y + m[2][2] * o_local.z + m[3][2]};
+    } else {
+        ro = {m[3][0], m[3][1], m[3][2]};
+    }
     rd = normalize(v3(m[0][0] * dc.x + m[1][0] * dc.y + m[2][0] * dc.z, m[0][1] * dc.x + m[1][1] * dc.y + m[2][1] * dc.z,
                       m[0][2] * dc.x + m[1][2] * dc.y + m[2][2] * dc.z));
+    return weight;
 }
 
 // IlluminationIntegrator::Li from ray (ro, rd) with a starting scatter pdf and
@@ -1306,10 +1457,11 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
     smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
     float film_x, film_y;
     V3 ro, rd;
-    camera_ray(sc.cam, smp, px, py, film_x, film_y, ro, rd);
+    float fw = camera_ray(sc, sc.cam, smp, px, py, film_x, film_y, ro, rd);
     float thr[8];
     for (int i = 0; i < n; ++i) thr[i] = 1.0f;
-    return path_li(sc, smp, w, ro, rd, 1e16f, thr, ip.max_depth, nullptr, nullptr);
+    V3 L = path_li(sc, smp, w, ro, rd, 1e16f, thr, ip.max_depth, nullptr, nullptr);
+    return {L.x * fw, L.y * fw, L.z * fw};
 }
 
 #include "restir.inc"
@@ -1473,8 +1625,8 @@ void *oracle_rt_open(void *handle, uint32_t width, uint32_t height) {
 }
 void oracle_rt_close(void *rt) { delete static_cast<oracle::rt::Frame *>(rt); }
 
-// One frame with the given camera block (112 bytes) and parameter block
-// (432 bytes, as vs_restir_params returns it).
+// One frame with the given camera block (128 bytes) and parameter block
+// (448 bytes, as vs_restir_params returns it).
 int oracle_rt_frame(void *rt, const void *camera, const void *params, uint32_t film_index, uint32_t threads) {
     auto *f = static_cast<oracle::rt::Frame *>(rt);
     oracle::Camera cam;

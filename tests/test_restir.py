@@ -29,8 +29,8 @@ def _fields(p):
     out.update({k: float(f[i]) for k, i in PARAM_F32.items()})
     m = f[40:56].reshape(4, 4)   # w2c, column-major
     out['w2c'] = m.T.copy()
-    out['view_pos'] = f[100:103].copy()
-    out['prev_view_pos'] = f[103:106].copy()
+    out['view_pos'] = f[104:107].copy()
+    out['prev_view_pos'] = f[107:110].copy()
     return out
 
 
@@ -111,8 +111,8 @@ def _oracle_frames(vb, ctx, sc, cams, w, h, threads=4):
             pv = prev.view('<f4')
             pp = p.view('<f4')
             pp[56:72] = pv[40:56]            # prev_w2c <- w2c
-            pp[72:100] = prev_cam.view('<f4')  # prev_cam
-            pp[103:106] = pv[100:103]        # prev_view_pos
+            pp[72:104] = prev_cam.view('<f4')  # prev_cam
+            pp[107:110] = pv[104:107]        # prev_view_pos
         prev_cam = s.export('camera').copy()
         ort.frame(s.export('camera'), p, 0, threads)
         prev = p

@@ -69,6 +69,34 @@ def test_camera_look_at(vb, host_ctx):
     assert abs(cam[16] - math.tan(math.radians(20))) < 1e-6
 
 
+@pytest.mark.parametrize('ftype, param, code, p0, p1', [
+    ('box', {}, 0, 0.0, 0.0),
+    ('triangle', {}, 1, 0.0, 0.0),
+    ('gaussian', {}, 2, 1.0, 0.0),                  # GaussianFilter sigma default (gaussian.cpp:21)
+    ('gaussian', {'sigma': 0.4}, 2, 0.4, 0.0),
+    ('mitchell', {}, 3, 1.0 / 3.0, 1.0 / 3.0),      # b, c defaults (mitchell.cpp:20-21)
+    ('sinc', {}, 4, 3.0, 0.0),                      # tau default (sinc.cpp:20)
+])
+def test_camera_filter_and_lens_parse(vb, host_ctx, ftype, param, code, p0, p1):
+    sc = scenes.box_room(width=4, height=4)
+    sc['camera']['type'] = 'thin_lens'
+    sc['camera']['param'].update(lens_radius=0.05, focal_distance=2.5)
+    sc['camera']['param']['filter'] = {'type': ftype, 'param': dict(param, radius=[1.25, 0.75])}
+    cam = vb.Scene(host_ctx, sc).export('camera', np.float32)
+    u = cam.view(np.uint32)
+    assert cam.nbytes == 128
+    np.testing.assert_allclose(cam[21:23], [1.25, 0.75])
+    assert (u[26], u[27]) == (code, 1)
+    np.testing.assert_allclose(cam[28:32], [0.05, 2.5, p0, p1], rtol=1e-6)
+
+
+def test_unknown_filter_is_unsupported(vb, host_ctx):
+    sc = scenes.box_room(width=4, height=4)
+    sc['camera']['param']['filter'] = {'type': 'lanczos2', 'param': {}}
+    with pytest.raises(vb.UnsupportedError):
+        vb.Scene(host_ctx, sc)
+
+
 def test_rgb_light_is_normalised(vb, host_ctx):
     # Light::Light + NumberArray::normalize: [17,17,17] -> colour 1, scale 17.
     s = vb.Scene(host_ctx, scenes.box_room(width=4, height=4, rgb_light=True))

@@ -173,7 +173,7 @@ DI_RESERVOIR_DTYPE = np.dtype([('weight_sum', '<f8'), ('C', '<f4'), ('W', '<f4')
 GI_RESERVOIR_DTYPE = np.dtype([('weight_sum', '<f8'), ('C', '<f4'), ('W', '<f4'), ('sp_pos', '<f4', 3),
                                ('sp_ng', '<f4', 3), ('Lo', '<f4', 3), ('age', '<f4'), ('pad', '<u4', 2)])
 HIT_BSDF_DTYPE = np.dtype([('wi', '<f4', 3), ('f', '<f4', 3), ('pdf', '<f4'), ('pad', '<u4')])
-RESTIR_PARAMS_BYTES = 432
+RESTIR_PARAMS_BYTES = 448
 RESTIR = dict(di_radiance=(0, np.dtype(('<f4', 4))), gi_radiance=(1, np.dtype(('<f4', 4))),
               motion=(2, np.dtype(('<f4', 2))), surfaces=(3, RT_SURFACE_DTYPE), di_reservoirs=(4, DI_RESERVOIR_DTYPE),
               gi_reservoirs=(5, GI_RESERVOIR_DTYPE), hit_bsdf=(6, HIT_BSDF_DTYPE), gi_samples=(7, GI_RESERVOIR_DTYPE))

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ Dev
     smp.start(px, py, p.frame, 0u, ip.sampler, ip.seed);
     f2 p_film;
     f3 ro, rd;
-    camera_ray(s.cam, smp, px, py, p_film, ro, rd);
+    const float filter_w = camera_ray(s, s.cam, smp, px, py, p_film, ro, rd);
 
     CSpec throughput = CSpec::fill(1.0f);
     f3 ret = make3(0.0f);               // radiance before the query vertex (linear sRGB)
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ Dev
         }
         if (bounce == p.query_depth) {
             encode(p, it, wl.lambda[0], p.q_feat + static_cast<size_t>(pix) * 64u);
-            rec.t = spec4(throughput, 0.0f);
+            rec.t = spec4(throughput, filter_w);
             rec.lambda = wl4(wl, false);
             rec.pdf = wl4(wl, true);
             rec.l_valid = make_float4(ret.x, ret.y, ret.z, 1.0f);
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ Dev
         ro = nr.o;
         rd = nr.d;
     }
-    if (!wrote_query) rec.l_valid = make_float4(ret.x, ret.y, ret.z, 0.0f);
+    if (!wrote_query) rec.l_valid = make_float4(ret.x * filter_w, ret.y * filter_w, ret.z * filter_w, 0.0f);
     p.q_rec[pix] = rec;
     if (train && (in_suffix || !wrote_query)) {
         // The suffix ended before its last vertex (no bootstrap term), or the
@@ -289,6 +289,7 @@ __global__ void k_cache_resolve(const __grid_constant__ DeviceScene s, const __g
         if (r.l_valid.w != 0.0f) {
             CWl wl = wl_of(r.lambda, r.pdf);
             L += linear_srgb<CN>(spec_of(r.t) * cache_radiance(p.q_out[i]), wl);
+            L = L * r.t.w;  // the camera sample's filter weight
         }
         if (bad3(L)) L = make3(0.0f);
         float4 acc = film_index == 0 ? make_float4(0, 0, 0, 0) : film32[i];
@@ -407,14 +408,15 @@ __global__ void __launch_bounds__(128) k_cache_query(const __grid_constant__ Dev
         const Hit h = b.hit[slot];
         if (h.inst_id == kInvalid) {
             miss_emission<CN>(s, ps, RgbAcc<CN>{});
-            ended[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);
+            const f3 Lw = ps.L * ps.filter_w;
+            ended[slot] = make_float4(Lw.x, Lw.y, Lw.z, 1.0f);
             continue;
         }
         const Interaction it = surface_interaction(s, h, ps.rd, true);
         hit_emission<CN>(s, ps, it, RgbAcc<CN>{});
         encode(p, it, ps.wl.lambda[0], p.q_feat + static_cast<size_t>(slot) * 64u);
         CacheQueryRec rec;
-        rec.t = spec4(ps.throughput, 0.0f);
+        rec.t = spec4(ps.throughput, ps.filter_w);
         rec.lambda = wl4(ps.wl, false);
         rec.pdf = wl4(ps.wl, true);
         rec.l_valid = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);

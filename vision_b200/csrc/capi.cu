@@ -73,7 +73,8 @@ struct vs_scene {
     DevBuf<AliasEntry> prim_alias, light_alias;
     DevBuf<float> prim_pmf, light_pmf, spd, luts;
     DevBuf<float> env_tex, env_marginal_func, env_cond_func, rgb2spec;
-    DevBuf<AliasEntry> env_marginal, env_cond;
+    DevBuf<AliasEntry> env_marginal, env_cond, filter_alias;
+    DevBuf<float> filter_tab;
     // Film and per-sample radiance (scratch between the megakernel and the film pass).
     DevBuf<float4> film32, exposed;
     DevBuf<double> film64;
@@ -211,6 +212,7 @@ struct vs_scene {
         nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
         prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
         env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
+        filter_tab.free(); filter_alias.free();
         film32.free(); exposed.free(); film64.free(); radiance.free(); path_counter.free(); wf.free();
         rt.free();
         cachebuf.free();
@@ -240,6 +242,9 @@ struct vs_scene {
         d.env_cond = env_cond.ptr;
         d.env_cond_func = env_cond_func.ptr;
         d.rgb2spec = reinterpret_cast<const float4 *>(rgb2spec.ptr);
+        d.filter_tab = filter_tab.ptr;
+        d.filter_alias = filter_alias.ptr;
+        d.filter_integral = host.filter_integral;
         d.cam = host.cam;
         d.ip = host.ip;
         d.node_count = static_cast<uint32_t>(host.nodes.size());
@@ -338,6 +343,10 @@ int upload_scene(vs_scene *s) {
         const float *t = rgb2spec_table("");
         std::vector<float> tab(t, t + static_cast<size_t>(3) * 64 * 64 * 64 * 4);
         VS_CUDA(s->rgb2spec.upload(tab), "upload rgb2spec");
+    }
+    if (!h.filter_tab.empty()) {
+        VS_CUDA(s->filter_tab.upload(h.filter_tab), "upload filter table");
+        VS_CUDA(s->filter_alias.upload(h.filter_alias), "upload filter table");
     }
     s->uploaded = true;
     return VS_OK;

@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(128, VS_RENDER_MIN_BLOCKS)
             bool more = path_bounce<N>(s, ps, nullptr);
             if (more) more = ++ps.bounce < max_depth;
             if (!more) {
-                radiance[p] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);
+                const f3 Lw = ps.L * ps.filter_w;
+                radiance[p] = make_float4(Lw.x, Lw.y, Lw.z, 1.0f);
                 active = false;
             }
         }

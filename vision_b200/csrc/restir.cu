@@ -462,16 +462,6 @@ __device__ __forceinline__ DiReservoir di_ris_lights(const DeviceScene &s, const
     // candidates' dependent fetches (light table, primitive table, vertices)
     // are in flight together; the reservoir sees them in the same order.
     uint32_t i = 0;
-#ifdef VS_RIS_SINGLE
-    for (; i < p.M_light; ++i) {
-        const float s0 = smp.next();
-        const f2 u0 = smp.next2();
-        DiReservoir c0;
-        float w0;
-        candidate(s0, u0, c0, w0);
-        di_update(ret, smp.next(), c0, w0);
-    }
-#endif
     for (; i + 1 < p.M_light; i += 2) {
         const float s0 = smp.next();
         const f2 u0 = smp.next2();
@@ -711,7 +701,7 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
     smp.start(x, y, p.frame, 0u, s.ip.sampler, s.ip.seed);
     f2 p_film;
     f3 ro, rd;
-    camera_ray(s.cam, smp, x, y, p_film, ro, rd);
+    (void)camera_ray(s, s.cam, smp, x, y, p_film, ro, rd);
     PrimaryHit ph = compute_hit(s, p, smp, wl, ro, rd);
     b.surf[cur][idx] = ph.surf;
     if (ph.surf.is_replaced) b.ext[cur][idx] = ph.ext;
@@ -818,7 +808,7 @@ __global__ void __launch_bounds__(128) k_di_primary(const __grid_constant__ Devi
     smp.start(x, y, p.frame, 0u, s.ip.sampler, s.ip.seed);
     f2 p_film;
     f3 ro, rd;
-    camera_ray(s.cam, smp, x, y, p_film, ro, rd);
+    (void)camera_ray(s, s.cam, smp, x, y, p_film, ro, rd);
     PrimaryHit ph = compute_hit(s, p, smp, wl, ro, rd);
     b.surf[cur][idx] = ph.surf;
     if (ph.surf.is_replaced) b.ext[cur][idx] = ph.ext;
@@ -1059,7 +1049,7 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
     smp.start(x, y, p.frame, 0u, s.ip.sampler, s.ip.seed);
     f2 p_film;
     f3 ro, rd;
-    camera_ray(s.cam, smp, x, y, p_film, ro, rd);
+    (void)camera_ray(s, s.cam, smp, x, y, p_film, ro, rd);
     smp.start(x, y, p.frame, 1u, s.ip.sampler, s.ip.seed);
     RtSurface cs = b.surf[cur][idx];
     DiReservoir rsv = b.di_pass[idx];
@@ -1330,6 +1320,7 @@ __global__ void __launch_bounds__(128) k_gi_wf_start(const __grid_constant__ Dev
         ps.L = make3(0.0f);
         ps.eta_scale = 1.0f;
         ps.bounce = 0;
+        ps.filter_w = 1.0f;
         GiReservoir g{};
         b.gi_init[idx] = g;
         if (p.gi_max_depth == 0u) continue;
@@ -1409,7 +1400,7 @@ __global__ void __launch_bounds__(128) k_gi_temporal(const __grid_constant__ Dev
     smp.start(x, y, p.frame, 0u, s.ip.sampler, s.ip.seed);
     f2 p_film;
     f3 ro, rd;
-    camera_ray(s.cam, smp, x, y, p_film, ro, rd);
+    (void)camera_ray(s, s.cam, smp, x, y, p_film, ro, rd);
     smp.start(x, y, p.frame, 4u, s.ip.sampler, s.ip.seed);
     GiReservoir sample = b.gi_init[idx];
     RtHitBsdf hb = b.hit_bsdf[idx];

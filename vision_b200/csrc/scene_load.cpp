@@ -10,7 +10,10 @@
 #include "json.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <numeric>
 #include <stdexcept>
@@ -67,6 +70,87 @@ void build_alias(const std::vector<float> &weights, std::vector<AliasEntry> &tab
         pmf[i] = integral > 0.0f ? weights[i] / (integral * static_cast<float>(n)) : 0.0f;
 }
 
+// Filter::evaluate of the tabulated filters at p in [0, r]^2.
+float filter_value(const Camera &c, float x, float y) {
+    const float kPiF = 3.14159265358979323846f;
+    if (c.filter == kFilterGaussian) {
+        // GaussianFilter::evaluate (gaussian.cpp:36-40), gaussian() of math/util.h:37-42.
+        const float sigma = c.filter_p0;
+        auto g = [&](float v) {
+            return 1.0f / std::sqrt(2.0f * kPiF * sigma * sigma) * std::exp(-(v * v) / (2.0f * sigma * sigma));
+        };
+        const float vx = g(x) - g(c.filter_rx), vy = g(y) - g(c.filter_ry);
+        return std::max(0.0f, vx) * std::max(0.0f, vy);
+    }
+    if (c.filter == kFilterMitchell) {
+        // MitchellFilter::mitchell_1d / evaluate (mitchell.cpp).
+        const float b = c.filter_p0, cc = c.filter_p1;
+        auto m1 = [&](float v) {
+            v = std::fabs(v);
+            if (v <= 1.0f)
+                return ((12.0f - 9.0f * b - 6.0f * cc) * v * v * v + (-18.0f + 12.0f * b + 6.0f * cc) * v * v +
+                        (6.0f - 2.0f * b)) * (1.0f / 6.0f);
+            if (v <= 2.0f)
+                return ((-b - 6.0f * cc) * v * v * v + (6.0f * b + 30.0f * cc) * v * v + (-12.0f * b - 48.0f * cc) * v +
+                        (8.0f * b + 24.0f * cc)) * (1.0f / 6.0f);
+            return 0.0f;
+        };
+        return m1(2.0f * x / c.filter_rx) * m1(2.0f * y / c.filter_ry);
+    }
+    // LanczosSincFilter::evaluate (sinc.cpp): windowed_sinc(x, r, tau) per axis, times 4.
+    const float tau = c.filter_p0;
+    auto sinc = [&](float v) {
+        const float a = kPiF * v;
+        return 1.0f + a * a == 1.0f ? 1.0f : std::sin(a) / a;
+    };
+    auto ws = [&](float v, float r) { return std::fabs(v) > r ? 0.0f : sinc(v) * sinc(v / tau); };
+    return ws(x, c.filter_rx) * ws(y, c.filter_ry) * 4.0f;
+}
+
+// FilterSampler::build (fitted_curve.h:36-58): the filter at the centres of a
+// kFilterTable^2 grid over [0, r]^2, normalised by its average, and the 2D
+// alias warper over its absolute value (AliasTable2D::build, alias2d.cpp).
+void build_filter_table(const Camera &c, std::vector<float> &tab, std::vector<AliasEntry> &alias, float &integral) {
+    tab.clear();
+    alias.clear();
+    integral = 0.0f;
+    if (c.filter != kFilterGaussian && c.filter != kFilterMitchell && c.filter != kFilterSinc) return;
+    const uint32_t n = kFilterTable;
+    std::vector<float> lut(n * n), func(n * n);
+    for (uint32_t i = 0; i < n * n; ++i) {
+        const uint32_t x = i % n, y = i / n;
+        const float px = (static_cast<float>(x) + 0.5f) / static_cast<float>(n) * c.filter_rx;
+        const float py = (static_cast<float>(y) + 0.5f) / static_cast<float>(n) * c.filter_ry;
+        const float v = filter_value(c, px, py);
+        func[i] = std::fabs(v);
+        lut[i] = v;
+    }
+    float sum = 0.0f;
+    for (float v : lut) sum += v;
+    const float avg = sum / static_cast<float>(n * n);
+    for (float &v : lut) v = v / avg;
+    std::vector<float> marginal(n), cond_func;
+    std::vector<AliasEntry> cond;
+    for (uint32_t v = 0; v < n; ++v) {
+        std::vector<float> row(func.begin() + v * n, func.begin() + (v + 1) * n);
+        std::vector<AliasEntry> t;
+        std::vector<float> pmf;
+        float row_integral = 0.0f;
+        build_alias(row, t, pmf, &row_integral);
+        marginal[v] = row_integral;
+        cond.insert(cond.end(), t.begin(), t.end());
+        cond_func.insert(cond_func.end(), row.begin(), row.end());
+    }
+    std::vector<AliasEntry> mtab;
+    std::vector<float> mpmf;
+    build_alias(marginal, mtab, mpmf, &integral);
+    tab = lut;
+    tab.insert(tab.end(), marginal.begin(), marginal.end());
+    tab.insert(tab.end(), cond_func.begin(), cond_func.end());
+    alias = mtab;
+    alias.insert(alias.end(), cond.begin(), cond.end());
+}
+
 namespace {
 
 std::runtime_error unsupported(const std::string &what) {
@@ -89,6 +173,20 @@ m4 translation(f3 t) {
 m4 scale_m(f3 s) {
     m4 m = m4_identity();
     m.m[0][0] = s.x; m.m[1][1] = s.y; m.m[2][2] = s.z;
+    return m;
+}
+// Right-handed rotation by `deg` degrees about `axis` (Rodrigues):
+// R e_j = cos e_j + sin (k x e_j) + (1 - cos) k k_j.
+m4 rot_axis(f3 axis, float deg) {
+    const f3 k = normalize(axis);
+    const float a = deg * kPi / 180.0f, c = std::cos(a), sn = std::sin(a);
+    const float kk[3] = {k.x, k.y, k.z};
+    m4 m = m4_identity();
+    for (int j = 0; j < 3; ++j) {
+        f3 e = make3(j == 0 ? 1.0f : 0.0f, j == 1 ? 1.0f : 0.0f, j == 2 ? 1.0f : 0.0f);
+        f3 col = e * c + cross(k, e) * sn + k * ((1.0f - c) * kk[j]);
+        m.m[j][0] = col.x; m.m[j][1] = col.y; m.m[j][2] = col.z;
+    }
     return m;
 }
 // Right-handed rotations about the axes, angle in degrees.
@@ -171,6 +269,13 @@ m4 parse_transform(const Json &t) {
         m4 roll = rot_z(p["roll"].as_float(0.0f));
         m4 pitch = rot_x(p["pitch"].as_float(0.0f));
         return translation(as_f3(p["position"], make3(0.0f))) * pitch * roll * yaw;
+    }
+    if (type == "trs") {
+        // TransformDesc "trs" (node_desc.cpp:48-52): T * R * S, r = (axis, degrees).
+        std::vector<float> r = p["r"].as_floats();
+        if (r.size() < 4) r = {1.0f, 0.0f, 0.0f, 0.0f};
+        return translation(as_f3(p["t"], make3(0.0f))) * rot_axis(make3(r[0], r[1], r[2]), r[3]) *
+               scale_m(as_f3(p["s"], make3(1.0f)));
     }
     throw unsupported("transform type '" + type + "'");
 }
@@ -258,6 +363,182 @@ MeshData make_inline_mesh(const Json &p) {
         m.uv.push_back(UV.size() >= 2 * (i + 1) ? f2{UV[2 * i], UV[2 * i + 1]} : f2{0, 0});
     }
     for (size_t i = 0; i < I.size(); ++i) m.idx.push_back(I[i].as_uint());
+    return m;
+}
+
+// Model (src/render_core/shapes/model.cpp:27-37) reads its file through
+// AssimpParser (importers/assimp_parser.cpp:231-340, assimp's OBJ importer and
+// post-processing).  Restated here for Wavefront OBJ:
+//   * `v`, `vt`, `vn` records and `f` faces with `i`, `i/t`, `i//n`, `i/t/n`
+//     references, 1-based or negative (relative to the end);
+//   * every distinct (position, uv, normal) triple is one vertex, numbered in
+//     order of first use (JoinIdenticalVertices);
+//   * polygons are split as a fan from their first corner (Triangulate; the
+//     two triangles of a quad are (0,1,2), (0,2,3) as in parse_meshes);
+//   * a face without normals gets its geometric normal normalize((p1-p0) x
+//     (p2-p0)): on its own vertices (GenNormals), or with `smooth`, summed
+//     over the faces without normals that share the position record and
+//     normalised (GenSmoothNormals);
+//   * uv defaults to (0, 0); `flip_uv` (default true) maps v to 1 - v;
+//     non-finite normals and uvs become zero (parse_meshes);
+//   * `swap_handed` negates z of positions and normals and reverses the
+//     winding (MakeLeftHanded | FlipWindingOrder);
+//   * groups, objects and `usemtl` are ignored: the model is one mesh with the
+//     shape's material.
+MeshData load_obj(const std::string &path, bool smooth, bool flip_uv, bool swap_handed) {
+    std::FILE *fp = std::fopen(path.c_str(), "rb");
+    if (!fp) throw std::runtime_error("model: cannot open '" + path + "'");
+    std::string text;
+    char buf[1 << 16];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof(buf), fp)) > 0) text.append(buf, got);
+    std::fclose(fp);
+
+    std::vector<f3> P, N;
+    std::vector<f2> T;
+    struct Corner {
+        int v, t, n;
+    };
+    std::vector<Corner> corners;    // triangle corners, 3 per triangle
+    std::vector<uint32_t> tri_face;  // face number of each triangle
+    uint32_t face_count = 0;
+    auto fail = [&](size_t line, const std::string &why) {
+        throw std::runtime_error("model '" + path + "' line " + std::to_string(line) + ": " + why);
+    };
+    size_t pos = 0, line_no = 0;
+    std::vector<Corner> poly;
+    while (pos < text.size()) {
+        size_t end = text.find('\n', pos);
+        if (end == std::string::npos) end = text.size();
+        std::string line = text.substr(pos, end - pos);
+        pos = end + 1;
+        ++line_no;
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        const char *c = line.c_str();
+        while (*c == ' ' || *c == '\t') ++c;
+        auto floats = [&](const char *q, float *out, int n) {
+            int k = 0;
+            while (k < n) {
+                char *e;
+                float v = std::strtof(q, &e);
+                if (e == q) break;
+                out[k++] = v;
+                q = e;
+            }
+            return k;
+        };
+        if (c[0] == 'v' && (c[1] == ' ' || c[1] == '\t')) {
+            float v[3];
+            if (floats(c + 2, v, 3) != 3) fail(line_no, "vertex needs 3 coordinates");
+            P.push_back({v[0], v[1], v[2]});
+        } else if (c[0] == 'v' && c[1] == 't' && (c[2] == ' ' || c[2] == '\t')) {
+            float v[2] = {0.0f, 0.0f};
+            if (floats(c + 3, v, 2) < 1) fail(line_no, "texture coordinate needs a value");
+            T.push_back({v[0], v[1]});
+        } else if (c[0] == 'v' && c[1] == 'n' && (c[2] == ' ' || c[2] == '\t')) {
+            float v[3];
+            if (floats(c + 3, v, 3) != 3) fail(line_no, "normal needs 3 components");
+            N.push_back({v[0], v[1], v[2]});
+        } else if (c[0] == 'f' && (c[1] == ' ' || c[1] == '\t')) {
+            poly.clear();
+            const char *q = c + 2;
+            auto resolve = [&](long r, size_t count, const char *what) -> int {
+                long i = r > 0 ? r - 1 : static_cast<long>(count) + r;
+                if (r == 0 || i < 0 || i >= static_cast<long>(count)) fail(line_no, std::string(what) + " index out of range");
+                return static_cast<int>(i);
+            };
+            while (*q) {
+                while (*q == ' ' || *q == '\t') ++q;
+                if (!*q) break;
+                char *e;
+                long vi = std::strtol(q, &e, 10);
+                if (e == q) fail(line_no, "bad face corner");
+                Corner k{resolve(vi, P.size(), "position"), -1, -1};
+                q = e;
+                if (*q == '/') {
+                    ++q;
+                    if (*q != '/') {
+                        long ti = std::strtol(q, &e, 10);
+                        if (e == q) fail(line_no, "bad texture index");
+                        k.t = resolve(ti, T.size(), "texture coordinate");
+                        q = e;
+                    }
+                    if (*q == '/') {
+                        ++q;
+                        long ni = std::strtol(q, &e, 10);
+                        if (e == q) fail(line_no, "bad normal index");
+                        k.n = resolve(ni, N.size(), "normal");
+                        q = e;
+                    }
+                }
+                if (*q && *q != ' ' && *q != '\t') fail(line_no, "bad face corner");
+                poly.push_back(k);
+            }
+            if (poly.size() < 3) continue;  // points and lines carry no surface
+            for (size_t i = 1; i + 1 < poly.size(); ++i) {
+                corners.push_back(poly[0]);
+                corners.push_back(poly[i]);
+                corners.push_back(poly[i + 1]);
+                tri_face.push_back(face_count);
+            }
+            ++face_count;
+        }
+    }
+    if (swap_handed) {
+        for (f3 &p : P) p.z = -p.z;
+        for (f3 &n : N) n.z = -n.z;
+        for (size_t t = 0; t < corners.size(); t += 3) std::swap(corners[t + 1], corners[t + 2]);
+    }
+    // Geometric normals of the triangles whose corners lack a normal.
+    const size_t ntri = corners.size() / 3;
+    std::vector<f3> tri_n(ntri, f3{0.0f, 0.0f, 0.0f});
+    std::vector<f3> smooth_n;
+    if (smooth) smooth_n.assign(P.size(), f3{0.0f, 0.0f, 0.0f});
+    for (size_t t = 0; t < ntri; ++t) {
+        const Corner *k = &corners[3 * t];
+        if (k[0].n >= 0 && k[1].n >= 0 && k[2].n >= 0) continue;
+        f3 g = cross(P[k[1].v] - P[k[0].v], P[k[2].v] - P[k[0].v]);
+        const float l = length(g);
+        tri_n[t] = l > 0.0f ? g / l : f3{0.0f, 0.0f, 0.0f};
+        if (smooth)
+            for (int i = 0; i < 3; ++i) smooth_n[k[i].v] = smooth_n[k[i].v] + tri_n[t];
+    }
+    auto finite3 = [](f3 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+    MeshData m;
+    std::map<std::array<int64_t, 3>, uint32_t> seen;
+    for (size_t t = 0; t < ntri; ++t) {
+        for (int i = 0; i < 3; ++i) {
+            const Corner &k = corners[3 * t + i];
+            // A generated flat normal belongs to its face: key it by face.
+            const int64_t nkey = k.n >= 0 ? k.n : (smooth ? -1 : -2 - static_cast<int64_t>(tri_face[t]));
+            const std::array<int64_t, 3> key{k.v, k.t, nkey};
+            auto it = seen.find(key);
+            if (it != seen.end()) {
+                m.idx.push_back(it->second);
+                continue;
+            }
+            const uint32_t id = static_cast<uint32_t>(m.p.size());
+            seen.emplace(key, id);
+            m.p.push_back(P[k.v]);
+            f3 n;
+            if (k.n >= 0) {
+                n = N[k.n];
+            } else if (smooth) {
+                const f3 sum = smooth_n[k.v];
+                const float l = length(sum);
+                n = l > 0.0f ? sum / l : f3{0.0f, 0.0f, 0.0f};
+            } else {
+                n = tri_n[t];
+            }
+            m.n.push_back(finite3(n) ? n : f3{0.0f, 0.0f, 0.0f});
+            f2 uv = k.t >= 0 ? T[k.t] : f2{0.0f, 0.0f};
+            if (k.t >= 0 && flip_uv) uv.y = 1.0f - uv.y;
+            if (!std::isfinite(uv.x) || !std::isfinite(uv.y)) uv = f2{0.0f, 0.0f};
+            m.uv.push_back(uv);
+            m.idx.push_back(id);
+        }
+    }
+    if (m.idx.empty()) throw std::runtime_error("model '" + path + "': no faces");
     return m;
 }
 
@@ -476,6 +757,7 @@ struct Loader {
     HostScene &s;
     const float *table;
     std::map<std::string, uint32_t> mat_by_name;
+    std::string base_dir;  // model files are relative to the scene's folder
 
     uint32_t add_spd(const float *v, int n) {
         uint32_t off = static_cast<uint32_t>(s.spd.size());
@@ -689,6 +971,17 @@ struct Loader {
         s.lights.push_back(L);
     }
 
+    MeshData load_model(const Json &p) {
+        if (p["subdiv_level"].as_uint(0u) != 0u) throw unsupported("model subdiv_level (Catmull-Clark subdivision)");
+        const std::string fn = p["fn"].as_string();
+        if (fn.empty()) throw std::runtime_error("model shape needs 'fn'");
+        const bool absolute = fn[0] == '/';
+        const std::string path = absolute || base_dir.empty() ? fn : base_dir + "/" + fn;
+        const std::string ext = fn.size() >= 4 ? fn.substr(fn.size() - 4) : std::string();
+        if (ext != ".obj" && ext != ".OBJ") throw unsupported("model format of '" + fn + "' (only Wavefront .obj)");
+        return load_obj(path, p["smooth"].as_bool(false), p["flip_uv"].as_bool(true), p["swap_handed"].as_bool(false));
+    }
+
     void load_shape(const Json &sh) {
         std::string type = sh["type"].as_string();
         std::string name = sh["name"].as_string();
@@ -700,6 +993,7 @@ struct Loader {
         else if (type == "mesh") mesh = make_inline_mesh(p);
         else if (type == "icosphere") mesh = make_icosphere(p);
         else if (type == "grid") mesh = make_grid(p);
+        else if (type == "model") mesh = load_model(p);
         else throw unsupported("shape type '" + type + "' (" + name + ")");
         const Json *emission = p.contains("emission") ? &p["emission"] : nullptr;
         uint32_t mat = kInvalid;
@@ -853,13 +1147,12 @@ void load_rt(const Json &ip, HostScene &s) {
 
 void load_scene_json(const std::string &text, const std::string &base_dir, const std::string &table_cache,
                      HostScene &s) {
-    (void)base_dir;
     Json root = Json::parse(text);
     if (!table_cache.empty()) {
         size_t slash = table_cache.find_last_of('/');
         s.lut_cache = (slash == std::string::npos ? std::string() : table_cache.substr(0, slash + 1)) + "microfacet_luts.bin";
     }
-    Loader ld{s, rgb2spec_table(table_cache), {}};
+    Loader ld{s, rgb2spec_table(table_cache), {}, base_dir};
     // Spectrum (SpectrumDesc, node_desc.cpp:346-350; hero.cpp:239).
     const Json &sp = root["spectrum"];
     s.spectrum_type = sp["type"].as_string("hero");
@@ -928,12 +1221,37 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     uint32_t w = res.size() >= 2 ? static_cast<uint32_t>(res[0]) : 1280u;
     uint32_t h = res.size() >= 2 ? static_cast<uint32_t>(res[1]) : 720u;
     s.cam.exposure = rc["exposure"].as_float(1.0f);
+    // ThinLensCamera (thin_lens.cpp:11-20): lens radius and focal distance.
+    s.cam.thin_lens = ct == "thin_lens" ? 1u : 0u;
+    s.cam.lens_radius = cp["lens_radius"].as_float(0.0f);
+    s.cam.focal_distance = cp["focal_distance"].as_float(5.0f);
+    // FilterDesc (node_desc.cpp): type and radius, plus the fitted filters'
+    // parameters (gaussian.cpp:18-24, mitchell.cpp, sinc.cpp).
     const Json &fj = cp["filter"];
     std::string ft = fj["type"].as_string("box");
-    if (ft != "box") throw unsupported("filter type '" + ft + "'");
-    std::vector<float> rad = fj["param"]["radius"].as_floats();
+    const Json &fp = fj["param"];
+    std::vector<float> rad = fp["radius"].as_floats();
     s.cam.filter_rx = rad.size() >= 1 ? rad[0] : 0.5f;
     s.cam.filter_ry = rad.size() >= 2 ? rad[1] : s.cam.filter_rx;
+    s.cam.filter_p0 = s.cam.filter_p1 = 0.0f;
+    if (ft == "box") {
+        s.cam.filter = kFilterBox;
+    } else if (ft == "triangle") {
+        s.cam.filter = kFilterTriangle;
+    } else if (ft == "gaussian") {
+        s.cam.filter = kFilterGaussian;
+        s.cam.filter_p0 = fp["sigma"].as_float(1.0f);
+    } else if (ft == "mitchell") {
+        s.cam.filter = kFilterMitchell;
+        s.cam.filter_p0 = fp["b"].as_float(1.0f / 3.0f);
+        s.cam.filter_p1 = fp["c"].as_float(1.0f / 3.0f);
+    } else if (ft == "sinc") {
+        s.cam.filter = kFilterSinc;
+        s.cam.filter_p0 = fp["tau"].as_float(3.0f);
+    } else {
+        throw unsupported("filter type '" + ft + "'");
+    }
+    build_filter_table(s.cam, s.filter_tab, s.filter_alias, s.filter_integral);
     update_camera(s, w, h);
 }
 

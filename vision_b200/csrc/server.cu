@@ -53,7 +53,7 @@ struct ServeItem {
     uint32_t npix;
     uint32_t pad;
 };
-static_assert(sizeof(ServeItem) == 160, "ServeItem layout");
+static_assert(sizeof(ServeItem) == 176, "ServeItem layout");
 
 struct ServeTable {
     unsigned long long next;  // path counter of the persistent kernel (0 at upload)

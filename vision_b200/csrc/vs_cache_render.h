@@ -13,9 +13,10 @@
 
 namespace vs {
 
-// Per-pixel path state at the query vertex: throughput (3 hero wavelengths),
-// wavelengths, wavelength pdfs, radiance gathered before the query (rgb) and
-// a validity flag (w of the last float4).
+// Per-pixel path state at the query vertex: throughput (3 hero wavelengths;
+// w: the camera sample's filter weight), wavelengths, wavelength pdfs,
+// radiance gathered before the query (rgb) and a validity flag (w of the last
+// float4).
 struct CacheQueryRec {
     float4 t, lambda, pdf, l_valid;
 };

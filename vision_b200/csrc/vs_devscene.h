@@ -32,6 +32,13 @@ struct DeviceScene {
     const AliasEntry *env_cond;
     const float *env_cond_func;
     const float4 *rgb2spec;       // 3 x 64^3 coefficient table
+    // Tabulated pixel filter (Gaussian, Mitchell, sinc): kFilterTable^2 table
+    // values over the filter's integral, the marginal function (kFilterTable)
+    // and the conditional functions (kFilterTable^2); the marginal alias table
+    // (kFilterTable) and the conditional ones (kFilterTable^2); the integral.
+    const float *filter_tab;
+    const AliasEntry *filter_alias;
+    float filter_integral;
     Camera cam;
     IntegratorParams ip;
     uint32_t node_count;

@@ -43,6 +43,11 @@ struct HostScene {
     std::vector<float> env_tex;  // 4 floats (RGB, 0) per texel, row-major from the zenith
     std::vector<AliasEntry> env_marginal, env_cond;
     std::vector<float> env_marginal_func, env_cond_func;
+    // Tabulated pixel filter (DeviceScene::filter_tab layout); empty for box
+    // and triangle.
+    std::vector<float> filter_tab;
+    std::vector<AliasEntry> filter_alias;
+    float filter_integral = 0.0f;
     bool needs_luts = false;
     std::string lut_cache;
     Camera cam{};

@@ -174,16 +174,58 @@ __device__ VS_OUTLINE void eval_hit_light(const DeviceScene &s, const Interactio
     pdf = pdf_wi_from_area(pdf_pos, it.ng, w) * light_pmf<N>(s, it.light);
 }
 
-// Sampler::sensor_sample (sampler.h:65-73) with the box filter (box.cpp:16-20)
-// and Sensor::generate_ray (sensor.cpp:44-56,63-76): raster -> screen ->
-// camera -> world.  Draws 2 (filter) + 2 (lens, unused by the pinhole) + 1
-// (time) numbers.
-__device__ __forceinline__ void camera_ray(const Camera &cam, Sampler &smp, uint32_t px, uint32_t py, f2 &p_film,
-                                           f3 &ro, f3 &rd) {
+// sample_linear / sample_tent (math/warp.h:132-145): the tent filter's offset.
+__device__ __forceinline__ float sample_linear(float u, float a, float b) {
+    float x = u * (a + b) / (a + sqrtf(lerpf(u, a * a, b * b)));
+    x = fminf(x, kOneMinusEpsilon);
+    return (u == 0.0f && a == 0.0f) ? 0.0f : x;
+}
+__device__ __forceinline__ float sample_tent(float u, float r) {
+    return u < 0.5f ? -r * sample_linear((0.5f - u) * 2.0f, 1.0f, 0.0f) : r * sample_linear((u - 0.5f) * 2.0f, 1.0f, 0.0f);
+}
+
+__device__ __forceinline__ float sign_of(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+
+// FilterSampler::sample (fitted_curve.h:72-80): the tabulated filter's offset
+// in [-1, 1]^2 (times the radius by the caller) and weight.
+__device__ __forceinline__ f2 fitted_filter_sample(const DeviceScene &s, f2 u, float &weight) {
+    const uint32_t n = kFilterTable;
+    u = make2(u.x * 2.0f - 1.0f, u.y * 2.0f - 1.0f);
+    const float *lut = s.filter_tab;
+    const float *marginal_func = s.filter_tab + n * n;
+    const float *cond_func = marginal_func + n;
+    uint32_t iv, iu;
+    const float fv = alias_continuous(s.filter_alias, n, fabsf(u.y), iv);
+    const float pdf_v = s.filter_integral > 0.0f ? __ldg(&marginal_func[iv]) / s.filter_integral : 0.0f;
+    const float fu = alias_continuous(s.filter_alias + n + static_cast<size_t>(iv) * n, n, fabsf(u.x), iu);
+    const float integral_u = __ldg(&marginal_func[iv]);
+    const float pdf_u = integral_u > 0.0f ? __ldg(&cond_func[iv * n + iu]) / integral_u : 0.0f;
+    const float pdf = pdf_u * pdf_v;
+    weight = __ldg(&lut[iv * n + iu]) / pdf;
+    return make2(fu * sign_of(u.x), fv * sign_of(u.y));
+}
+
+// Sampler::sensor_sample (sampler.h:65-73) with the scene's filter (box.cpp,
+// triangle.cpp, fitted_curve.h) and Sensor::generate_ray (sensor.cpp:44-56,
+// 63-76; ThinLensCamera::generate_ray_in_local_space, thin_lens.cpp:36-43):
+// raster -> screen -> camera -> world.  Draws 2 (filter) + 2 (lens) + 1
+// (time) numbers.  Returns the filter weight the path's radiance is scaled by.
+__device__ __forceinline__ float camera_ray(const DeviceScene &s, const Camera &cam, Sampler &smp, uint32_t px,
+                                            uint32_t py, f2 &p_film, f3 &ro, f3 &rd) {
     f2 uf = smp.next2();
-    float fx = lerpf(uf.x, -cam.filter_rx, cam.filter_rx);
-    float fy = lerpf(uf.y, -cam.filter_ry, cam.filter_ry);
-    (void)smp.next2();
+    float fx, fy, weight = 1.0f;
+    if (cam.filter == kFilterBox) {
+        fx = lerpf(uf.x, -cam.filter_rx, cam.filter_rx);
+        fy = lerpf(uf.y, -cam.filter_ry, cam.filter_ry);
+    } else if (cam.filter == kFilterTriangle) {
+        fx = sample_tent(uf.x, cam.filter_rx);
+        fy = sample_tent(uf.y, cam.filter_ry);
+    } else {
+        f2 q = fitted_filter_sample(s, uf, weight);
+        fx = q.x * cam.filter_rx;
+        fy = q.y * cam.filter_ry;
+    }
+    const f2 u_lens = smp.next2();
     (void)smp.next();
     float film_x = static_cast<float>(px) + 0.5f + fx;
     float film_y = static_cast<float>(py) + 0.5f + fy;
@@ -191,14 +233,26 @@ __device__ __forceinline__ void camera_ray(const Camera &cam, Sampler &smp, uint
     float sx = cam.screen_lo_x + film_x / static_cast<float>(cam.width) * cam.screen_span_x;
     float sy = cam.screen_hi_y - film_y / static_cast<float>(cam.height) * cam.screen_span_y;
     f3 dir_cam = normalize(make3(sx * cam.tan_half_fov, sy * cam.tan_half_fov, 1.0f));
-    ro = xform_point(cam.c2w, make3(0.0f));
-    rd = normalize(xform_vector(cam.c2w, dir_cam));
+    if (cam.thin_lens) {
+        const f2 pl = square_to_disk(u_lens);
+        const f3 o_lens = make3(pl.x * cam.lens_radius, pl.y * cam.lens_radius, 0.0f);
+        const float ft = cam.focal_distance / dir_cam.z;
+        const f3 p_focus = dir_cam * ft;
+        const f3 d_lens = normalize(p_focus - o_lens);
+        ro = xform_point(cam.c2w, o_lens);
+        rd = normalize(xform_vector(cam.c2w, d_lens));
+    } else {
+        ro = xform_point(cam.c2w, make3(0.0f));
+        rd = normalize(xform_vector(cam.c2w, dir_cam));
+    }
+    return weight;
 }
 
 // Mutable state of one camera path between bounces: the sampler, the hero
 // wavelengths, the next ray with the pdf of the direction it was sampled
 // with, the throughput, the radiance gathered so far, the accumulated
-// relative-IOR factor of Russian roulette and the bounce index.
+// relative-IOR factor of Russian roulette, the bounce index and the camera
+// sample's filter weight.
 template <int N>
 struct PathState {
     Sampler smp;
@@ -209,6 +263,7 @@ struct PathState {
     float scatter_pdf;
     float eta_scale;
     uint32_t bounce;
+    float filter_w;  // the camera sample's filter weight (radiance scale at the end)
 };
 
 // Shadow ray of one bounce and the radiance it adds when unoccluded (linear
@@ -381,6 +436,7 @@ __device__ __forceinline__ f3 path_li(const DeviceScene &s, Sampler &smp, Wavele
     ps.L = make3(0.0f);
     ps.scatter_pdf = scatter_pdf;
     ps.eta_scale = 1.0f;
+    ps.filter_w = 1.0f;
     for (ps.bounce = 0; ps.bounce < max_depth; ++ps.bounce)
         if (!path_bounce<N>(s, ps, first)) break;
     smp = ps.smp;
@@ -400,7 +456,7 @@ __device__ __forceinline__ void path_start(const DeviceScene &s, const Camera &c
     ps.wl = sample_wavelengths<N>(ps.smp.next());
     ps.smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
     f2 p_film;
-    camera_ray(cam, ps.smp, px, py, p_film, ps.ro, ps.rd);
+    ps.filter_w = camera_ray(s, cam, ps.smp, px, py, p_film, ps.ro, ps.rd);
     ps.throughput = Spec<N>::fill(1.0f);
     ps.L = make3(0.0f);
     ps.scatter_pdf = 1e16f;
@@ -418,7 +474,7 @@ __device__ __forceinline__ f3 trace_path_cam(const DeviceScene &s, const Camera 
     const uint32_t max_depth = s.ip.max_depth;
     for (; ps.bounce < max_depth; ++ps.bounce)
         if (!path_bounce<N>(s, ps, nullptr)) break;
-    return ps.L;
+    return ps.L * ps.filter_w;
 }
 
 template <int N>

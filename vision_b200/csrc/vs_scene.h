@@ -80,18 +80,30 @@ struct AliasEntry {
     uint32_t alias;
 };
 
-// Pinhole sensor with box filter.  Directions are built from the screen window
-// the way src/base/sensor/sensor.cpp:44-76 builds raster_to_sensor.
+// Pixel filters (src/render_core/filters): box and triangle sample in closed
+// form; Gaussian, Mitchell and Lanczos-sinc through a 20 x 20 table of the
+// filter over [0, r]^2 and a 2D alias warper (fitted_curve.h).
+enum FilterType : uint32_t { kFilterBox = 0, kFilterTriangle = 1, kFilterGaussian = 2, kFilterMitchell = 3,
+                             kFilterSinc = 4 };
+constexpr uint32_t kFilterTable = 20;
+
+// Pinhole or thin-lens sensor (pinhole.cpp, thin_lens.cpp) with its pixel
+// filter.  Directions are built from the screen window the way
+// src/base/sensor/sensor.cpp:44-76 builds raster_to_sensor.
 struct alignas(16) Camera {
     m4 c2w;
     float tan_half_fov;
     float screen_lo_x, screen_hi_y;   // screen window lower.x, upper.y
     float screen_span_x, screen_span_y;
-    float filter_rx, filter_ry;       // box filter radius
+    float filter_rx, filter_ry;       // filter radius
     uint32_t width, height;
     float exposure;
-    uint32_t pad0, pad1;
+    uint32_t filter;                  // FilterType
+    uint32_t thin_lens;               // 1: ThinLensCamera (lens sample), 0: pinhole
+    float lens_radius, focal_distance;
+    float filter_p0, filter_p1;       // sigma (Gaussian), b and c (Mitchell), tau (sinc)
 };
+static_assert(sizeof(Camera) == 128, "Camera layout");
 
 enum SamplerType : uint32_t { kSamplerIndependent = 0, kSamplerPCG = 1 };
 enum LightSamplerType : uint32_t { kLightSamplerUniform = 0, kLightSamplerPower = 1 };

@@ -28,7 +28,7 @@ __device__ __forceinline__ void store(const WfBuffers &b, uint32_t slot, const P
     b.tp[slot] = pack4<N>(ps.throughput.v);
     b.lam[slot] = pack4<N>(ps.wl.lambda);
     b.pdf[slot] = pack4<N>(ps.wl.pdf);
-    b.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
+    b.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, ps.filter_w);
     b.st[slot] = make_uint4(static_cast<uint32_t>(ps.smp.state), static_cast<uint32_t>(ps.smp.state >> 32),
                             ps.bounce, scene);
 }
@@ -51,6 +51,7 @@ __device__ __forceinline__ uint32_t load(const Scenes &scenes, const WfBuffers &
         ps.wl.pdf[i] = comp(pdf, i);
     }
     ps.L = make3(L.x, L.y, L.z);
+    ps.filter_w = L.w;
     ps.smp.state = static_cast<uint64_t>(st.x) | (static_cast<uint64_t>(st.y) << 32);
     ps.smp.kind = s.ip.sampler;
     ps.smp.seed = s.ip.seed;
@@ -212,7 +213,7 @@ __device__ __forceinline__ void shade(const Scenes &scenes, const WfBuffers &b, 
             store<N>(b, slot, ps, scene);
             b.queue[cur ^ 1u][queue_push(&b.count[cur ^ 1u])] = slot;
         } else {
-            b.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
+            b.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, ps.filter_w);
         }
         if (sq.valid) {
             const uint32_t k = queue_push(&b.count[2]);
@@ -220,7 +221,8 @@ __device__ __forceinline__ void shade(const Scenes &scenes, const WfBuffers &b, 
             b.sh_d[k] = make_float4(sq.d.x, sq.d.y, sq.d.z, __uint_as_float(slot | (more ? 0u : 0x80000000u)));
             b.sh_c[k] = make_float4(sq.c.x, sq.c.y, sq.c.z, __uint_as_float(scene));
         } else if (!more) {
-            radiance[base + slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.0f);
+            const f3 Lw = ps.L * ps.filter_w;
+            radiance[base + slot] = make_float4(Lw.x, Lw.y, Lw.z, 1.0f);
         }
     }
 }
@@ -262,10 +264,13 @@ __device__ __forceinline__ void shadow(const Scenes &scenes, const WfBuffers &b,
                 const float4 c = b.sh_c[i];
                 f3 l = make3(L.x, L.y, L.z);
                 l += make3(c.x, c.y, c.z);
-                L = make_float4(l.x, l.y, l.z, 0.0f);
+                L = make_float4(l.x, l.y, l.z, L.w);
                 b.L[slot] = L;
             }
-            if (tag & 0x80000000u) radiance[base + slot] = make_float4(L.x, L.y, L.z, 1.0f);
+            if (tag & 0x80000000u) {
+                const f3 Lw = make3(L.x, L.y, L.z) * L.w;
+                radiance[base + slot] = make_float4(Lw.x, Lw.y, Lw.z, 1.0f);
+            }
             active = false;
         }
     }
