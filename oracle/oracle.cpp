@@ -959,7 +959,7 @@ struct Eval {
 
 // A lobe of the material's lobe set.
 struct Lobe {
-    enum Kind { Lambert, MicrofacetRefl, Dielectric, NoScatter } kind;
+    enum Kind { Lambert, MicrofacetRefl, Dielectric, NoScatter, Substrate } kind;
     enum Fr { Conductor, Schlick, F82, One } fresnel = One;
     float ax = 1, ay = 1;
     bool compensate = false;
@@ -1021,6 +1021,25 @@ static void lobe_eval(const Lobe &l, int n, V3 wo, V3 wi, float *f, float &pdf, 
         float comp = l.compensate ? 1.0f / lut2(kLutPure, std::sqrt(l.ax * l.ay), wo.z) : 1.0f;
         for (int i = 0; i < n; ++i) f[i] = b * F[i] * l.kr[i] * comp;
         pdf = mf::pdf_refl(wo, h, l.ax, l.ay);
+    } else if (l.kind == Lobe::Substrate) {
+        // FresnelBlend (substrate.cpp:12-72) through BxDF::safe_evaluate:
+        // kr = Rd, fa = Rs; specular picked with F_dielectric(|cos wo|, 1.5).
+        flags = kRefl;
+        if (!(wo.z * wi.z > 0.0f)) {
+            for (int i = 0; i < n; ++i) f[i] = 0.0f;
+            pdf = 0.0f;
+            return;
+        }
+        V3 h = normalize(add(wi, wo));
+        float ci = std::fabs(wi.z), co = std::fabs(wo.z);
+        float d = mf::D(h, l.ax, l.ay) / (4.0f * std::fabs(dot(wi, h)) * std::max(ci, co));
+        auto p5 = [](float x) { float x2 = x * x; return x2 * x2 * x; };
+        float w = p5(std::min(std::max(1.0f - dot(wi, h), 0.0f), 1.0f));
+        float g = (28.0f / (23.0f * kPi)) * (1.0f - p5(1.0f - 0.5f * ci)) * (1.0f - p5(1.0f - 0.5f * co));
+        for (int i = 0; i < n; ++i) f[i] = d * (l.fa[i] + w * (1.0f - l.fa[i])) + g * l.kr[i] * (1.0f - l.fa[i]);
+        float fr = mf::fr_dielectric(co, 1.5f);
+        float pd = ci * kInvPi;
+        pdf = pd + fr * (mf::pdf_refl(wo, h, l.ax, l.ay) - pd);
     } else if (l.kind == Lobe::Dielectric) {
         bool refl = wo.z * wi.z > 0.0f;
         float e0 = l.eta[0];
@@ -1110,6 +1129,21 @@ static V3 lobe_sample(const Lobe &l, int n, V3 wo, Sampler &smp, bool &valid) {
         valid = wo.z * wi.z > 0.0f;
         return wi;
     }
+    if (l.kind == Lobe::Substrate) {
+        // FresnelBlend::sample_wi (substrate.cpp:55-71): remapped u.x picks
+        // the microfacet or the cosine-hemisphere direction; always valid.
+        float u0 = smp.next(), u1 = smp.next();
+        float fr = mf::fr_dielectric(std::fabs(wo.z), 1.5f);
+        if (u0 < fr) {
+            u0 = u0 / fr;
+            return mf::reflect(wo, mf::sample_wh(wo, u0, u1, l.ax, l.ay));
+        }
+        u0 = (u0 - fr) / (1.0f - fr);
+        float r = std::sqrt(u0), th = 2.0f * kPi * u1;
+        float dx = r * std::cos(th), dy = r * std::sin(th);
+        float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
+        return {dx, dy, wo.z < 0.0f ? -z : z};
+    }
     // Dielectric: microfacet normal (2D), then reflect/refract choice (1D).
     float u0 = smp.next(), u1 = smp.next();
     V3 h = mf::sample_wh(wo, u0, u1, l.ax, l.ay);
@@ -1181,16 +1215,29 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
     if (m.type == 0) {
         l0.kind = Lobe::Lambert;
         for (int i = 0; i < w.n; ++i) l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
-    } else if (m.type == 2) {  // metal: ConductorLobe
+    } else if (m.type == 2) {  // metal: ConductorLobe; mirror: MirrorLobe (FresnelConstant, kr = colour)
         l0.kind = Lobe::MicrofacetRefl;
-        l0.fresnel = Lobe::Conductor;
+        const bool mirror = (m.flags & 4u) != 0;
+        l0.fresnel = mirror ? Lobe::One : Lobe::Conductor;
         l0.compensate = true;
         l0.ax = m.p[0];
         l0.ay = m.p[1];
         for (int i = 0; i < w.n; ++i) {
-            l0.kr[i] = 1.0f;
-            l0.fa[i] = spd_of(sc.s->spd, m.spd0, w.lambda[i]);
-            l0.fb[i] = spd_of(sc.s->spd, m.spd1, w.lambda[i]);
+            if (mirror) {
+                l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
+            } else {
+                l0.kr[i] = 1.0f;
+                l0.fa[i] = spd_of(sc.s->spd, m.spd0, w.lambda[i]);
+                l0.fb[i] = spd_of(sc.s->spd, m.spd1, w.lambda[i]);
+            }
+        }
+    } else if (m.type == 5) {  // substrate: SubstrateLobe over FresnelBlend
+        l0.kind = Lobe::Substrate;
+        l0.ax = m.p[0];
+        l0.ay = m.p[1];
+        for (int i = 0; i < w.n; ++i) {
+            l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
+            l0.fa[i] = sigmoid_poly(m.p + 2, w.lambda[i]);
         }
     } else if (m.type == 3) {  // glass: DielectricLobe
         l0.kind = Lobe::Dielectric;

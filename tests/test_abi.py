@@ -32,10 +32,10 @@ def test_version(vb):
 def test_unsupported_plugin_is_reported(vb, host_ctx):
     from vision_b200 import scenes
     sc = scenes.box_room()
-    sc['materials'][0]['type'] = 'substrate'
+    sc['materials'][0]['type'] = 'subsurface'
     with pytest.raises(vb.UnsupportedError) as e:
         vb.Scene(host_ctx, sc)
-    assert 'substrate' in str(e.value)
+    assert 'subsurface' in str(e.value)
     assert e.value.code == vb.VS_E_UNSUPPORTED
 
 

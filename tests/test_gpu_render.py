@@ -101,6 +101,50 @@ def test_matched_seed_parity_materials(vb, gpu_ctx):
     assert np.median(np.abs(gb - cb) / (0.5 * (gb + cb) + 1e-3)) < 0.02
 
 
+def test_matched_seed_parity_substrate_mirror(vb, gpu_ctx):
+    # Tinted glossy mirror (constant Fresnel, compensated) and substrate
+    # (FresnelBlend) surfaces: one-bounce agreement per pixel, full depth in
+    # distribution, as for the other microfacet materials.
+    s = vb.Scene(gpu_ctx, scenes.substrate_room(64, 64, max_depth=2)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 1e-3) >= 0.99
+    s = vb.Scene(gpu_ctx, scenes.substrate_room(64, 64)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16, fp64=True)
+    g = s.film(vb.FILM_SUM64)[..., :3] / 16.0
+    _, c64 = o.render(0, 16, fp64=True)
+    c = c64[..., :3] / 16.0
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 2e-3) >= 0.85
+    assert abs(g.mean() - c.mean()) < 1e-2 * c.mean()
+
+
+def test_model_shape_renders_like_the_oracle(vb, gpu_ctx, tmp_path):
+    # The tall box as a Wavefront OBJ model (quads, shared corners, generated
+    # smooth normals) instead of the built-in cube.
+    (tmp_path / 'box.obj').write_text(
+        'v -0.5 0 -0.5\nv 0.5 0 -0.5\nv 0.5 1 -0.5\nv -0.5 1 -0.5\n'
+        'v -0.5 0 0.5\nv 0.5 0 0.5\nv 0.5 1 0.5\nv -0.5 1 0.5\n'
+        'f 1 4 3 2\nf 5 6 7 8\nf 1 2 6 5\nf 4 8 7 3\nf 1 5 8 4\nf 2 3 7 6\n')
+    sc = scenes.box_room(width=48, height=48)
+    for sh in sc['shapes']:
+        if sh['name'] == 'tall_box':
+            sh['type'] = 'model'
+            sh['param'] = {'fn': 'box.obj', 'material': 'TallBox', 'smooth': False,
+                           'transform': {'type': 'trs', 'param': {'t': [-0.17, 0.0, -0.13], 'r': [0, 1, 0, 15],
+                                                                  's': [0.3, 0.6, 0.3]}}}
+    s = vb.Scene(gpu_ctx, sc, base_dir=str(tmp_path)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 8)
+    g, c = s.film(), o.render(0, 8)
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 1e-3) >= 0.97
+    assert abs(g[..., :3].mean() - c[..., :3].mean()) < 2e-3 * c[..., :3].mean()
+
+
 def test_matched_seed_parity_environment(vb, gpu_ctx):
     # The large-scene layout at a small size: displaced icosphere, ground tiles
     # with drawn materials, procedural sky with a 5-degree sun (importance
@@ -129,7 +173,7 @@ def test_large_scene_closest_hit_bit_exact(vb, gpu_ctx):
     assert np.array_equal(t_gpu.view(np.uint32), t_cpu.view(np.uint32))
 
 
-@pytest.mark.parametrize('case', ['box_room', 'materials', 'environment', 'dimension1', 'two_waves'])
+@pytest.mark.parametrize('case', ['box_room', 'materials', 'substrate', 'environment', 'dimension1', 'two_waves'])
 def test_schedules_give_the_same_film(vb, gpu_ctx, case):
     # Path regeneration only changes which thread traces which path, and the
     # wavefront form only where a path's state lives between bounces: each
@@ -139,6 +183,8 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
         sc = scenes.box_room(width=67, height=45)
     elif case == 'materials':
         sc = scenes.material_room(40, 36)
+    elif case == 'substrate':
+        sc = scenes.substrate_room(38, 34)
     elif case == 'environment':
         sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
     elif case == 'dimension1':

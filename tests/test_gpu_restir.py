@@ -32,7 +32,7 @@ def _run(vb, ctx, sc, cams, w, h):
         yield f, s, ort
 
 
-@pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates'])
+@pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates', 'substrate_mirror'])
 def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
     # 'diffuse': diffuse walls and emitters (the kernels compiled for those
     # materials alone); 'metal': a gold box as well (the general kernels);
@@ -45,6 +45,14 @@ def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
         for m in sc['materials']:
             if m['name'] == 'TallBox':
                 m.update({'type': 'metal', 'param': {'material_name': 'Au', 'roughness': 0.3}})
+    if materials == 'substrate_mirror':
+        # A glossy mirror (Glossy flag) and a substrate floor.
+        for m in sc['materials']:
+            if m['name'] == 'TallBox':
+                m.update({'type': 'mirror', 'param': {'color': [0.9, 0.8, 0.7], 'roughness': 0.3}})
+            if m['name'] == 'Floor':
+                m.update({'type': 'substrate', 'param': {'color': [0.6, 0.5, 0.4], 'roughness': 0.2,
+                                                         'remapping_roughness': False}})
     cams = scenes.camera_spline(6, seed=3)
     for f, s, ort in _run(vb, gpu_ctx, sc, cams, w, h):
         gs, cs = s.restir_buffer('surfaces'), ort.buffer('surfaces', vb.RT_SURFACE_DTYPE)

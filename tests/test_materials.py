@@ -79,11 +79,48 @@ def test_principled_nonzero_coat_is_unsupported(vb, host_ctx):
 
 
 def test_metal_names(vb, host_ctx):
-    for name, ok in (('Au', True), ('Cu', True), ('Al', True), ('Ag', True), ('Unobtainium', True), ('Ti', False)):
+    # The ten conductors of metal_ior.inl.h each get their own (eta, k)
+    # table; an unknown name falls back to silver (metal.cpp:104-110).
+    def eta_k(name):
         sc = scenes.box_room(width=4, height=4)
         sc['materials'][0] = {'type': 'metal', 'name': 'Floor', 'param': {'material_name': name}}
-        if ok:
-            vb.Scene(host_ctx, sc)
-        else:
-            with pytest.raises(vb.UnsupportedError):
-                vb.Scene(host_ctx, sc)
+        s = vb.Scene(host_ctx, sc)
+        spd = s.export('spd', np.float32)
+        return spd.copy()
+    names = ['Ag', 'Al', 'Au', 'Cu', 'CuZn', 'Fe', 'Ti', 'V', 'VN', 'Li']
+    tables = {n: eta_k(n) for n in names}
+    for i, a in enumerate(names):
+        for b in names[i + 1:]:
+            assert not np.array_equal(tables[a], tables[b]), (a, b)
+    np.testing.assert_array_equal(eta_k('Unobtainium'), tables['Ag'])
+
+
+def test_mirror_and_substrate_records(vb, host_ctx):
+    s = vb.Scene(host_ctx, scenes.substrate_room(8, 8))
+    mats = s.export('materials', np.uint32).reshape(-1, 16)
+    matf = mats.view(np.float32)
+    names = ['Floor', 'Ceiling', 'BackWall', 'LeftWall', 'RightWall', 'TallBox', 'ShortBox', 'Light']
+    rec = {n: (mats[i], matf[i]) for i, n in enumerate(names)}
+    # Mirror: a metal record with the constant-Fresnel flag, colour
+    # coefficients, roughness 0.05 remapped to alpha 0.0025 (mirror.cpp:59-74).
+    u, f = rec['TallBox']
+    assert u[0] == 2 and (u[1] & 4) and u[2] == 0xffffffff
+    assert abs(f[8] - 0.0025) < 1e-9 and abs(f[9] - 0.0025) < 1e-9
+    assert np.any(f[4:7] != 0.0)
+    # Substrate with remapping squares twice: 0.6 -> 0.36 -> 0.1296
+    # (substrate.cpp:133-139); Rs coefficients in p[2..4].
+    u, f = rec['ShortBox']
+    assert u[0] == 5
+    np.testing.assert_allclose(f[8:10], [0.6 ** 4] * 2, rtol=1e-6)
+    assert np.any(f[10:13] != 0.0)
+    # Unremapped alphas stay as given.
+    u, f = rec['Floor']
+    assert u[0] == 5
+    np.testing.assert_allclose(f[8:10], [0.1, 0.1], rtol=1e-6)
+    # Rs defaults to 0.05 grey: the same coefficients as an explicit 0.05.
+    sc = scenes.substrate_room(8, 8)
+    for m in sc['materials']:
+        if m['name'] == 'Floor':
+            m['param']['spec'] = [0.05, 0.05, 0.05]
+    f2 = vb.Scene(host_ctx, sc).export('materials', np.float32).reshape(-1, 16)[0]
+    np.testing.assert_array_equal(f2[10:13], f[10:13])

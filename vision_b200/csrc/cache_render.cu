@@ -538,6 +538,7 @@ cudaError_t launch_cache_frame_wavefront(const DeviceScene &s, const CacheFrameP
         cw_shade<3>(mask, sv, b, cur, ended, st, n);
         cw_shade<4>(mask, sv, b, cur, ended, st, n);
         cw_shade<5>(mask, sv, b, cur, ended, st, n);
+        cw_shade<6>(mask, sv, b, cur, ended, st, n);
         k_cw_shadow<<<g_shadow, 128, 0, st>>>(sv, b, ended);
         n += 2;
     }

@@ -201,6 +201,11 @@ __device__ __forceinline__ void classify(const Material &m, uint32_t &flag, floa
     } else if (m.type == kMatGlass) {
         flag = fminf(m.p[0], m.p[1]) < kAlphaThreshold ? kFlagNearSpec : kFlagGlossy;
         diffuse = sqrtf(m.p[0]);
+    } else if (m.type == kMatSubstrate) {
+        // SubstrateLobe: always Glossy (substrate.cpp:147), diffuse factor
+        // sqrt of the microfacet lobe's (substrate.cpp:74-80).
+        flag = kFlagGlossy;
+        diffuse = sqrtf(sqrtf(sqrtf(m.p[0] * m.p[1])));
     } else if (m.type == kMatDiffuse) {
         flag = kFlagDiffRefl;
     } else if (m.type == kMatBlackBody) {
@@ -1690,6 +1695,7 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
             g_shade[3] = rt_wave_grid(k_gi_wf_shade<3>);
             g_shade[4] = rt_wave_grid(k_gi_wf_shade<4>);
             g_shade[5] = rt_wave_grid(k_gi_wf_shade<5>);
+            g_shade[6] = rt_wave_grid(k_gi_wf_shade<6>);
         }
         const uint32_t np = p.width * p.height;
         const unsigned g_pix = (np + 127) / 128;
@@ -1712,6 +1718,7 @@ cudaError_t launch_rt_frame(const DeviceScene &s, const RtParams &p, const RtBuf
             if (mask & 8u) { k_gi_wf_shade<3><<<g_shade[3], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
             if (mask & 16u) { k_gi_wf_shade<4><<<g_shade[4], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
             if (mask & 32u) { k_gi_wf_shade<5><<<g_shade[5], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
+            if (mask & 64u) { k_gi_wf_shade<6><<<g_shade[6], 128, 0, st>>>(s, *wf, cur, radiance); ++n; }
             k_gi_wf_shadow<<<g_shadow, 128, 0, st>>>(s, *wf, radiance);
             ++n;
         }

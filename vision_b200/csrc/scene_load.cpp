@@ -668,12 +668,6 @@ f3 xform_normal(const m4 &m, f3 n) {
             static_cast<float>(inv[0][2] * n.x + inv[1][2] * n.y + inv[2][2] * n.z)};
 }
 
-bool is_known_metal(const std::string &m) {
-    for (const char *n : {"Ag", "Al", "Au", "Cu", "CuZn", "Fe", "Li", "Ti", "V", "VN"})
-        if (m == n) return true;
-    return false;
-}
-
 // calculate_alpha (src/base/scattering/microfacet.h:43-58).
 void alpha_aniso(float a, float aniso, float &ax, float &ay) {
     if (std::fabs(aniso) <= 1e-4f) {
@@ -787,11 +781,24 @@ struct Loader {
             mat.type = kMatMetal;
             std::string metal = p["material_name"].as_string();
             const float *eta = nullptr, *k = nullptr;
-            if (metal == "Au") { eta = VS_METAL_AU_ETA; k = VS_METAL_AU_K; }
-            else if (metal == "Al") { eta = VS_METAL_AL_ETA; k = VS_METAL_AL_K; }
-            else if (metal == "Cu") { eta = VS_METAL_CU_ETA; k = VS_METAL_CU_K; }
-            else if (metal == "Ag" || metal.empty() || !is_known_metal(metal)) { eta = VS_METAL_AG_ETA; k = VS_METAL_AG_K; }
-            else throw unsupported("metal '" + metal + "' (" + name + ")");
+            static const struct {
+                const char *name;
+                const float *eta, *k;
+            } kMetals[] = {
+                {"Ag", VS_METAL_AG_ETA, VS_METAL_AG_K},       {"Al", VS_METAL_AL_ETA, VS_METAL_AL_K},
+                {"Au", VS_METAL_AU_ETA, VS_METAL_AU_K},       {"Cu", VS_METAL_CU_ETA, VS_METAL_CU_K},
+                {"CuZn", VS_METAL_CUZN_ETA, VS_METAL_CUZN_K}, {"Fe", VS_METAL_FE_ETA, VS_METAL_FE_K},
+                {"Ti", VS_METAL_TI_ETA, VS_METAL_TI_K},       {"V", VS_METAL_V_ETA, VS_METAL_V_K},
+                {"VN", VS_METAL_VN_ETA, VS_METAL_VN_K},       {"Li", VS_METAL_LI_ETA, VS_METAL_LI_K},
+            };
+            // An unknown or empty name falls back to silver.
+            eta = VS_METAL_AG_ETA;
+            k = VS_METAL_AG_K;
+            for (const auto &mt : kMetals)
+                if (metal == mt.name) {
+                    eta = mt.eta;
+                    k = mt.k;
+                }
             mat.spd0 = add_spd(eta, 95);
             mat.spd1 = add_spd(k, 95);
             float r = clampf(slot_scalar(p["roughness"], 0.01f), 0.0001f, 1.0f);
@@ -854,6 +861,43 @@ struct Loader {
                     throw unsupported(std::string("principled_bsdf ") + key + " > 0 (" + name + ")");
             }
             s.needs_luts = true;
+        } else if (type == "mirror") {
+            // MirrorMaterial (mirror.cpp:18-74): the compensated GGX
+            // reflection lobe of a metal with a constant Fresnel term and the
+            // colour slot as kr; roughness default 0.001, remapped to r^2.
+            mat.type = kMatMetal;
+            mat.flags |= kMatFlagConstantFresnel;
+            rgb = slot_rgb(p["color"], make3(1.0f));
+            float in[3] = {rgb.x, rgb.y, rgb.z};
+            rgb2spec_decode_albedo(table, in, mat.coef);
+            float r = clampf(slot_scalar(p["roughness"], 0.001f), 0.0001f, 1.0f);
+            float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
+            float a = p["remapping_roughness"].as_bool(true) ? r * r : r;
+            alpha_aniso(a, aniso, mat.p[0], mat.p[1]);
+            s.needs_luts = true;
+        } else if (type == "substrate") {
+            // SubstrateMaterial (substrate.cpp:96-148): colour (Rd, default 1)
+            // and spec (Rs, default 0.05) slots, roughness default 0.5.  With
+            // remapping the reference squares the roughness and then the
+            // anisotropic alphas once more; alphas clamp to [1e-4, 1].
+            mat.type = kMatSubstrate;
+            rgb = slot_rgb(p["color"], make3(1.0f));
+            float in[3] = {rgb.x, rgb.y, rgb.z};
+            rgb2spec_decode_albedo(table, in, mat.coef);
+            f3 spec = slot_rgb(p["spec"], make3(0.05f));
+            float sin[3] = {spec.x, spec.y, spec.z}, sc[4];
+            rgb2spec_decode_albedo(table, sin, sc);
+            mat.p[2] = sc[0]; mat.p[3] = sc[1]; mat.p[4] = sc[2];
+            float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.0001f, 1.0f);
+            float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
+            const bool remap = p["remapping_roughness"].as_bool(true);
+            alpha_aniso(remap ? r * r : r, aniso, mat.p[0], mat.p[1]);
+            if (remap) {
+                mat.p[0] = mat.p[0] * mat.p[0];
+                mat.p[1] = mat.p[1] * mat.p[1];
+            }
+            mat.p[0] = clampf(mat.p[0], 0.0001f, 1.0f);
+            mat.p[1] = clampf(mat.p[1], 0.0001f, 1.0f);
         } else {
             throw unsupported("material type '" + type + "' (" + name + ")");
         }

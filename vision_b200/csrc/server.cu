@@ -334,6 +334,7 @@ public:
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[3], k_sv_shade<3>, 128, 0);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[4], k_sv_shade<4>, 128, 0);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[5], k_sv_shade<5>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[6], k_sv_shade<6>, 128, 0);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shadow, k_sv_shadow, 128, 0);
         if (e != cudaSuccess) return e;
         auto grid_of = [&](int per) { return static_cast<unsigned>(std::max(1, sms * std::max(per, 1))); };
@@ -364,6 +365,7 @@ public:
                     k_sv_shade<3><<<g_shade[3], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
                     k_sv_shade<4><<<g_shade[4], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
                     k_sv_shade<5><<<g_shade[5], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shade<6><<<g_shade[6], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
                     k_sv_shadow<<<g_shadow, 128, 0, stream>>>(d_scenes, wfb[k], base, d_rad[k]);
                 }
             }

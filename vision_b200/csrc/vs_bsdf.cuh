@@ -215,7 +215,7 @@ struct DielLobe {
 
 // Material types compiled into a Bsdf: bit t set for MaterialType t.  Kernels
 // that shade one material class at a time instantiate only its code.
-constexpr uint32_t kAllMaterials = 0x1fu;
+constexpr uint32_t kAllMaterials = 0x3fu;
 template <uint32_t M>
 __device__ __forceinline__ constexpr bool has_mat(uint32_t t) {
     return ((M >> t) & 1u) != 0u;
@@ -228,8 +228,10 @@ struct Bsdf {
     f3 ng;
     const float *luts;
     bool dispersive;
-    // Diffuse colour (diffuse, principled diffuse lobe).
+    // Diffuse colour (diffuse, principled diffuse lobe, substrate Rd).
     Spec<N> kd;
+    // Substrate specular colour Rs.
+    Spec<N> ks;
     // Microfacet lobes: metal uses mf[0]; principled uses mf[0] = metallic,
     // mf[1] = specular.
     MfLobe<N> mf[2];
@@ -239,6 +241,47 @@ struct Bsdf {
     float w_metal, w_trans, w_spec, w_diff;
     float trans_scale;
     bool has_trans;
+
+    // FresnelBlend (substrate.cpp:12-72) inside its MicrofacetLobe, through
+    // BxDF::safe_evaluate (bxdf.cpp:30-43): Ashikhmin-Shirley glossy
+    // specular over a diffuse base; the lobe picks specular with probability
+    // F_dielectric(|cos wo|, 1.5) (the lobe's FresnelDielectric).
+    __device__ __forceinline__ void substrate_eval(f3 wo, f3 wi, Spec<N> &f, float &pdf) const {
+        if (!(wo.z * wi.z > 0.0f)) {
+            f = Spec<N>::fill(0.0f);
+            pdf = 0.0f;
+            return;
+        }
+        const float ax = mf[0].ax, ay = mf[0].ay;
+        const f3 wh = normalize(wi + wo);
+        const float ci = fabsf(wi.z), co = fabsf(wo.z);
+        const float d = ggx_D(wh, ax, ay) / (4.0f * fabsf(dot(wi, wh)) * fmaxf(ci, co));
+        const float sw = pow5(clampf(1.0f - dot(wi, wh), 0.0f, 1.0f));
+        const float mi = 1.0f - 0.5f * ci, mo = 1.0f - 0.5f * co;
+        const float g = (28.0f / (23.0f * kPi)) * (1.0f - pow5(mi)) * (1.0f - pow5(mo));
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const float spec = d * (ks.v[i] + sw * (1.0f - ks.v[i]));
+            const float diff = g * kd.v[i] * (1.0f - ks.v[i]);
+            f.v[i] = spec + diff;
+        }
+        const float fr = fresnel_dielectric(co, 1.5f);
+        const float pd = ci * kInvPi;
+        pdf = pd + fr * (ggx_pdf_reflection(wo, wh, ax, ay) - pd);
+    }
+    __device__ __forceinline__ f3 substrate_sample(f3 wo, f2 u) const {
+        const float fr = fresnel_dielectric(fabsf(wo.z), 1.5f);
+        f3 wi;
+        if (u.x < fr) {
+            u.x = u.x / fr;
+            wi = reflect_dir(wo, ggx_sample_vndf(wo, u, mf[0].ax, mf[0].ay));
+        } else {
+            u.x = (u.x - fr) / (1.0f - fr);
+            wi = cosine_hemisphere(u);
+            wi.z = wo.z < 0.0f ? -wi.z : wi.z;
+        }
+        return wi;
+    }
 
     // Zero the pdf of a direction whose geometric side contradicts the flags
     // (MaterialEvaluator::evaluate, material.cpp:137-147).
@@ -265,6 +308,10 @@ struct Bsdf {
         } else if (has_mat<M>(kMatGlass) && type == kMatGlass) {
             dl.eval_local(wo, wi, luts, e.f, e.pdf, e.flags, eta);
             e.f = e.f * acos_i;
+        } else if (has_mat<M>(kMatSubstrate) && type == kMatSubstrate) {
+            substrate_eval(wo, wi, e.f, e.pdf);
+            e.f = e.f * acos_i;
+            e.flags = kFlagReflection;
         } else if (has_mat<M>(kMatPrincipled) && type == kMatPrincipled) {
             // LobeSet::evaluate_impl (lobe.cpp:665-681): sum of the lobes, each
             // masked by its own hemisphere test, pdfs weighted by the
@@ -329,6 +376,8 @@ struct Bsdf {
             wi = mf[0].sample_local(wo, smp.next2(), valid);
         } else if (has_mat<M>(kMatGlass) && type == kMatGlass) {
             wi = dl.sample_local(wo, smp, valid);
+        } else if (has_mat<M>(kMatSubstrate) && type == kMatSubstrate) {
+            wi = substrate_sample(wo, smp.next2());
         } else if (has_mat<M>(kMatPrincipled) && type == kMatPrincipled) {
             // LobeSet::sample_wi_impl (lobe.cpp:598-627): 1D lobe choice, an
             // unused 2D draw, then the chosen lobe's own draws.
@@ -386,17 +435,23 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
         MfLobe<N> &l = b.mf[0];
         l.ax = m.p[0];
         l.ay = m.p[1];
-        l.fresnel = kFresnelConductor;
         l.compensate = true;
-        l.kr = Spec<N>::fill(1.0f);
-        const float *eta = s.spd + m.spd0;
-        const float *k = s.spd + m.spd1;
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-            l.fa.v[i] = spd_eval(eta + 1, static_cast<int>(eta[0]), wl.lambda[i]);
-            l.fb.v[i] = spd_eval(k + 1, static_cast<int>(k[0]), wl.lambda[i]);
-        }
         l.eta0 = 1.0f;
+        if (m.flags & kMatFlagConstantFresnel) {
+            // MirrorMaterial::create_lobe_set (mirror.cpp:59-74): FresnelConstant, kr = colour.
+            l.fresnel = kFresnelConstant;
+            l.kr = albedo_spectrum<N>(m.coef, wl);
+        } else {
+            l.fresnel = kFresnelConductor;
+            l.kr = Spec<N>::fill(1.0f);
+            const float *eta = s.spd + m.spd0;
+            const float *k = s.spd + m.spd1;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                l.fa.v[i] = spd_eval(eta + 1, static_cast<int>(eta[0]), wl.lambda[i]);
+                l.fb.v[i] = spd_eval(k + 1, static_cast<int>(k[0]), wl.lambda[i]);
+            }
+        }
     } else if (has_mat<M>(kMatGlass) && m.type == kMatGlass) {
         // GlassMaterial::create_lobe_set (glass.cpp:240-257).
         DielLobe<N> &d = b.dl;
@@ -411,6 +466,12 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
                                            : m.p[2];
             d.eta.v[i] = front ? ior : 1.0f / ior;
         }
+    } else if (has_mat<M>(kMatSubstrate) && m.type == kMatSubstrate) {
+        // SubstrateMaterial::create_lobe_set (substrate.cpp:126-148).
+        b.kd = albedo_spectrum<N>(m.coef, wl);
+        b.ks = albedo_spectrum<N>(m.p + 2, wl);
+        b.mf[0].ax = m.p[0];
+        b.mf[0].ay = m.p[1];
     } else if (has_mat<M>(kMatPrincipled) && m.type == kMatPrincipled) {
         // PrincipledBSDF::create_lobe_set (principled_bsdf.cpp:352-461) with
         // sheen and coat at weight 0 (their lobes then contribute nothing).

@@ -58,6 +58,7 @@ VS_HD f3 vmin(f3 a, f3 b) { return {fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z,
 VS_HD f3 vmax(f3 a, f3 b) { return {fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)}; }
 VS_HD float max3(f3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
 VS_HD float sqr(float x) { return x * x; }
+VS_HD float pow5(float x) { const float x2 = x * x; return x2 * x2 * x; }
 VS_HD float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
 VS_HD float lerpf(float t, float a, float b) { return a + t * (b - a); }
 VS_HD float safe_sqrt(float x) { return sqrtf(fmaxf(x, 0.0f)); }

@@ -15,11 +15,13 @@ enum MaterialType : uint32_t {
     kMatMetal = 2,       // metal.cpp: GGX conductor with complex Fresnel
     kMatGlass = 3,       // glass.cpp: rough dielectric, optionally dispersive
     kMatPrincipled = 4,  // principled_bsdf.cpp
+    kMatSubstrate = 5,   // substrate.cpp: FresnelBlend (glossy coat over diffuse)
 };
 
 enum MaterialFlag : uint32_t {
     kMatFlagDispersive = 1u,
     kMatFlagRemapRoughness = 2u,
+    kMatFlagConstantFresnel = 4u,  // kMatMetal written by a `mirror` (mirror.cpp): F = 1, kr = colour
 };
 
 // 64 bytes.  `coef` holds RGB->spectrum sigmoid coefficients (c0, c1, c2) of

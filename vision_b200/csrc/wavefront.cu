@@ -116,6 +116,7 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
     if ((e = shade_grid<N, 3>(dev, sg)) != cudaSuccess) return e;
     if ((e = shade_grid<N, 4>(dev, sg)) != cudaSuccess) return e;
     if ((e = shade_grid<N, 5>(dev, sg)) != cudaSuccess) return e;
+    if ((e = shade_grid<N, 6>(dev, sg)) != cudaSuccess) return e;
     const uint32_t mask = class_mask | 1u;
     unsigned n_launch = 0;
     for (uint64_t base = 0; base < paths; base += b.capacity) {
@@ -132,6 +133,7 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
             launch_shade<N, 3>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 4>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 5>(sg, mask, s, b, cur, base, radiance, st, n_launch);
+            launch_shade<N, 6>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             k_wf_shadow<<<grid_shadow, 128, 0, st>>>(s, b, base, radiance);
             n_launch += 2;
         }

@@ -97,6 +97,21 @@ def material_room(width=64, height=64, dimension=4, sampler="independent", max_d
     return sc
 
 
+def substrate_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
+    """The box room with the remaining reference materials: a near-specular
+    tinted mirror tall box, a glossy substrate short box (roughness remapped)
+    and a substrate floor with plain alphas (the reference's coffee-scene
+    plastics: Rd, Rs 0.05 default, roughness 0.1 unremapped)."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    mats = {m["name"]: m for m in sc["materials"]}
+    mats["TallBox"].update({"type": "mirror", "param": {"color": [0.95, 0.9, 0.8], "roughness": 0.05}})
+    mats["ShortBox"].update({"type": "substrate", "param": {
+        "color": [0.2, 0.4, 0.8], "spec": [0.08, 0.08, 0.08], "roughness": 0.6}})
+    mats["Floor"].update({"type": "substrate", "param": {
+        "color": [0.58, 0.58, 0.58], "roughness": [0.1, 0.1], "remapping_roughness": False}})
+    return sc
+
+
 def _draw_material(rng, name):
     """One of the three material families, drawn uniformly, with the
     parameter distributions of the large-scene workload."""
