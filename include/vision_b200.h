@@ -39,8 +39,15 @@ extern "C" {
 
 /* Film buffers for vs_film_download. */
 #define VS_FILM_LINEAR 0     /* FP32 running mean, float4 per pixel (rt_buffer) */
-#define VS_FILM_EXPOSED 1    /* 1 - exp(-linear * exposure), float4 per pixel */
+#define VS_FILM_EXPOSED 1    /* tone_mapper(1 - exp(-linear * exposure)), float4 per pixel */
 #define VS_FILM_SUM64 2      /* FP64 sums: double4 (r, g, b, samples) per pixel */
+/* The final picture (Pipeline::final_picture, pipeline.cpp:313-329): the
+ * collector's output (exposure, tone mapper) mapped once more by the tone
+ * mapper, with the sRGB gamma (DISPLAY, float4; RGBA8, 8-bit RGBA rounded to
+ * the nearest step) or without it (HDR: the exr/hdr outputs). */
+#define VS_FILM_DISPLAY 3
+#define VS_FILM_HDR 4
+#define VS_FILM_RGBA8 5
 
 typedef struct vs_context vs_context;
 typedef struct vs_scene vs_scene;
@@ -332,6 +339,13 @@ int vs_cache_download(vs_scene *scene, int which, void *dst, size_t bytes);
  * the same tables regenerated from the lobe definitions (apps/precompute's
  * job), cached in cache_path.  No device work. */
 int vs_albedo_luts(int which, const char *cache_path, float *out, size_t count);
+
+/* Regenerates the albedo tables on the context's GPU with strata^2 stratified
+ * samples per cell (strata = 32 evaluates the same estimator as
+ * vs_albedo_luts(1, ...); the reference's apps/precompute used 2^21 samples,
+ * material.h:121-163).  out holds `count` = the table's float count.
+ * strata in [1, 4096], else VS_E_RANGE; VS_E_NO_DEVICE on host-only contexts. */
+int vs_albedo_luts_gpu(vs_context *ctx, uint32_t strata, float *out, size_t count);
 
 /* RGB -> sigmoid coefficients with the uplift table (reference
  * RGBToSpectrumTable::decode_albedo / decode_unbound, hero.cpp:92-141).

@@ -124,3 +124,12 @@ def test_mirror_and_substrate_records(vb, host_ctx):
             m['param']['spec'] = [0.05, 0.05, 0.05]
     f2 = vb.Scene(host_ctx, sc).export('materials', np.float32).reshape(-1, 16)[0]
     np.testing.assert_array_equal(f2[10:13], f[10:13])
+
+
+def test_gpu_albedo_tables_need_a_device_and_a_valid_strata(vb, host_ctx):
+    with pytest.raises(vb.VisionError) as e:
+        vb.albedo_luts_gpu(host_ctx, 32)
+    assert e.value.code == vb.VS_E_NO_DEVICE
+    with pytest.raises(vb.VisionError) as e:
+        vb.albedo_luts_gpu(host_ctx, 0)
+    assert e.value.code == vb.VS_E_RANGE

@@ -214,3 +214,14 @@ def test_large_scene_counts(vb, host_ctx):
     assert i['instance_count'] == 101
     types = s.export('materials', np.uint32).reshape(-1, 16)[:, 0]
     assert set(types.tolist()) == {2, 3, 4}
+
+
+@pytest.mark.parametrize('kind, ok', [('linear', True), ('aces', True), ('reinhard', True), ('filmic', False)])
+def test_tone_mapper_parse(vb, host_ctx, kind, ok):
+    sc = scenes.box_room(width=4, height=4)
+    sc['camera']['param']['radiance_collector']['param']['tone_mapper'] = {'type': kind}
+    if ok:
+        vb.Scene(host_ctx, sc)
+    else:
+        with pytest.raises(vb.UnsupportedError, match='tone mapper'):
+            vb.Scene(host_ctx, sc)

@@ -30,6 +30,9 @@ FILM_FP64 = 1
 FILM_LINEAR = 0
 FILM_EXPOSED = 1
 FILM_SUM64 = 2
+FILM_DISPLAY = 3
+FILM_HDR = 4
+FILM_RGBA8 = 5
 
 EXPORT = dict(pos=0, nrm=1, uv=2, idx=3, prim_inst=4, instances=5, materials=6, lights=7, prim_alias=8,
               prim_pmf=9, light_alias=10, light_pmf=11, camera=12, integrator=13, spd=14, material_rgb=15,
@@ -107,6 +110,7 @@ def _load():
         'vs_render_schedule_set': ([P, ctypes.c_int], ctypes.c_int),
         'vs_cache_download': ([P, ctypes.c_int, P, ctypes.c_size_t], ctypes.c_int),
         'vs_albedo_luts': ([ctypes.c_int, ctypes.c_char_p, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_albedo_luts_gpu': ([P, U32, P, ctypes.c_size_t], ctypes.c_int),
         'vs_restir_frame': ([P, U32, U32, P], ctypes.c_int),
         'vs_restir_reset': ([P], ctypes.c_int),
         'vs_restir_params': ([P, U32, P, ctypes.c_size_t], ctypes.c_int),
@@ -144,7 +148,7 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_scene_info_get', 'vs_scene_export_size', 'vs_scene_export', 'vs_render', 'vs_synchronize',
                       'vs_film_download', 'vs_trace_closest_device', 'vs_trace_closest_host', 'vs_trace_any_device',
                       'vs_trace_any_host', 'vs_rgb_to_spectrum', 'vs_launch_count', 'vs_render_stats', 'vs_timing_enable',
-                      'vs_timing_read', 'vs_render_noalloc', 'vs_albedo_luts', 'vs_restir_frame',
+                      'vs_timing_read', 'vs_render_noalloc', 'vs_albedo_luts', 'vs_albedo_luts_gpu', 'vs_restir_frame',
                       'vs_restir_reset', 'vs_restir_params', 'vs_restir_download', 'vs_server_create',
                       'vs_server_destroy', 'vs_server_add_scene', 'vs_server_submit', 'vs_server_poll',
                       'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error', 'vs_cache_create',
@@ -195,6 +199,15 @@ def albedo_luts(regenerated=False):
                             out.ctypes.data_as(ctypes.c_void_p), out.size)
     if rc != VS_OK:
         raise VisionError(rc, 'vs_albedo_luts failed')
+    return out
+
+
+def albedo_luts_gpu(ctx, strata=32):
+    """Albedo tables regenerated on the context's GPU with strata^2 samples
+    per cell (strata = 32: the estimator of albedo_luts(regenerated=True))."""
+    out = np.zeros(LUT_FLOATS, np.float32)
+    ctx.check(lib.vs_albedo_luts_gpu(ctx.handle, int(strata), out.ctypes.data_as(ctypes.c_void_p), out.size),
+              'albedo_luts_gpu')
     return out
 
 
@@ -285,6 +298,8 @@ class Scene:
         npix = i['width'] * i['height']
         if which == FILM_SUM64:
             out = np.zeros((i['height'], i['width'], 4), np.float64)
+        elif which == FILM_RGBA8:
+            out = np.zeros((i['height'], i['width'], 4), np.uint8)
         else:
             out = np.zeros((i['height'], i['width'], 4), np.float32)
         self.ctx.check(lib.vs_film_download(self.handle, _ptr(out), out.nbytes, which), 'film download')

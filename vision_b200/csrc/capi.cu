@@ -647,15 +647,24 @@ int vs_film_download(vs_scene *s, void *dst, size_t bytes, int which) {
     if (s->film_frames == 0) return fail(ctx, VS_E_STATE, "nothing rendered");
     VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     cudaStream_t st = ctx->stream;
-    if (which == VS_FILM_LINEAR || which == VS_FILM_EXPOSED) {
+    if (which == VS_FILM_LINEAR || which == VS_FILM_EXPOSED || which == VS_FILM_DISPLAY || which == VS_FILM_HDR) {
         if (bytes != npix * 16) return fail(ctx, VS_E_INVALID, "film size mismatch");
         const float4 *src = s->film32.ptr;
-        if (which == VS_FILM_EXPOSED) {
-            VS_CUDA(launch_exposure(s->film32.ptr, static_cast<uint32_t>(npix), s->host.cam.exposure, s->exposed.ptr, st),
-                    "exposure");
+        if (which != VS_FILM_LINEAR) {
+            const uint32_t passes = which == VS_FILM_EXPOSED ? 1u : 2u;
+            VS_CUDA(launch_picture(s->film32.ptr, static_cast<uint32_t>(npix), s->host.cam.exposure, s->host.tone_mapper,
+                                   passes, which == VS_FILM_DISPLAY, s->exposed.ptr, nullptr, st),
+                    "picture");
             src = s->exposed.ptr;
         }
         VS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), "film copy");
+    } else if (which == VS_FILM_RGBA8) {
+        if (bytes != npix * 4) return fail(ctx, VS_E_INVALID, "film size mismatch");
+        uchar4 *out8 = reinterpret_cast<uchar4 *>(s->exposed.ptr);
+        VS_CUDA(launch_picture(s->film32.ptr, static_cast<uint32_t>(npix), s->host.cam.exposure, s->host.tone_mapper, 2u,
+                               true, nullptr, out8, st),
+                "picture");
+        VS_CUDA(cudaMemcpyAsync(dst, out8, bytes, cudaMemcpyDeviceToHost, st), "film copy");
     } else if (which == VS_FILM_SUM64) {
         if (!s->film64_valid) return fail(ctx, VS_E_STATE, "FP64 film not rendered");
         if (bytes != npix * 32) return fail(ctx, VS_E_INVALID, "film size mismatch");
@@ -1446,6 +1455,23 @@ int vs_albedo_luts(int which, const char *cache_path, float *out, size_t count) 
     if (!out || count != static_cast<size_t>(kLutFloats)) return VS_E_INVALID;
     const float *t = which == 0 ? microfacet_luts() : regenerate_microfacet_luts(cache_path ? cache_path : "");
     std::memcpy(out, t, count * sizeof(float));
+    return VS_OK;
+}
+
+int vs_albedo_luts_gpu(vs_context *ctx, uint32_t strata, float *out, size_t count) {
+    if (!ctx) return VS_E_INVALID;
+    if (!out || count != static_cast<size_t>(kLutFloats)) return fail(ctx, VS_E_INVALID, "out must hold the table floats");
+    if (strata < 1u || strata > 4096u) return fail(ctx, VS_E_RANGE, "strata must be in [1, 4096]");
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot generate on the GPU");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    struct Owned {
+        DevBuf<float> b;
+        ~Owned() { b.free(); }
+    } d;
+    VS_CUDA(d.b.alloc(count), "lut alloc");
+    VS_CUDA(launch_albedo_luts(d.b.ptr, strata, ctx->stream), "albedo luts");
+    VS_CUDA(cudaMemcpyAsync(out, d.b.ptr, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream), "lut copy");
+    VS_CUDA(cudaStreamSynchronize(ctx->stream), "lut sync");
     return VS_OK;
 }
 

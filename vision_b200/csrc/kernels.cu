@@ -159,13 +159,45 @@ __global__ void k_film_sum64(const float4 *radiance, uint32_t npix, uint32_t fra
     reinterpret_cast<double4 *>(sum4)[i] = acc;
 }
 
-// Exposure + linear tone map of the linear film (RadianceCollector::apply_exposure,
-// radiance_collector.cpp:24-26).
-__global__ void k_film_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out) {
+// The tone mappers of tonemappers/impl.cpp: linear (identity), ACES (the
+// fitted curve x(2.51x + 0.03) / (x(2.43x + 0.59) + 0.14), saturated) and
+// Reinhard x / (x + 1).
+__device__ __forceinline__ float tone_map(float x, uint32_t tm) {
+    if (tm == kToneAces) return __saturatef((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f));
+    if (tm == kToneReinhard) return x / (x + 1.0f);
+    return x;
+}
+
+// sRGB transfer function (IEC 61966-2-1), the gamma of the final picture.
+__device__ __forceinline__ float linear_to_srgb(float v) {
+    return v <= 0.0031308f ? 12.92f * v : 1.055f * powf(v, 1.0f / 2.4f) - 0.055f;
+}
+
+// The pictures of the linear film: exposure 1 - exp(-L * exposure)
+// (RadianceCollector::apply_exposure, radiance_collector.cpp:24-26) and the
+// tone mapper give the collector's output buffer (normal.cpp:86-101); the
+// final picture maps that once more and applies the sRGB gamma unless the
+// output is HDR (Postprocessor::tone_mapping, postprocessor.cpp:13-22;
+// Pipeline::final_picture, pipeline.cpp:313-329).  8-bit output rounds the
+// clamped value to the nearest of 255 steps.  One pixel per thread, float4
+// in, float4 or uchar4 out.
+__global__ void k_film_picture(const float4 *film, uint32_t npix, float exposure, uint32_t tm, uint32_t passes,
+                               bool gamma, float4 *out, uchar4 *out8) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npix) return;
-    float4 v = film[i];
-    out[i] = make_float4(1.0f - expf(-v.x * exposure), 1.0f - expf(-v.y * exposure), 1.0f - expf(-v.z * exposure), 1.0f);
+    const float4 v = film[i];
+    float c[3] = {1.0f - expf(-v.x * exposure), 1.0f - expf(-v.y * exposure), 1.0f - expf(-v.z * exposure)};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        for (uint32_t p = 0; p < passes; ++p) c[k] = tone_map(c[k], tm);
+        if (gamma) c[k] = linear_to_srgb(c[k]);
+    }
+    if (out8) {
+        auto q = [](float x) { return static_cast<unsigned char>(__float2int_rn(__saturatef(x) * 255.0f)); };
+        out8[i] = make_uchar4(q(c[0]), q(c[1]), q(c[2]), 255);
+    } else {
+        out[i] = make_float4(c[0], c[1], c[2], 1.0f);
+    }
 }
 
 cudaError_t upload_spectral_consts(const float *x, const float *y, const float *z, const float *d65, float y_integral) {
@@ -253,8 +285,9 @@ cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_be
     return cudaGetLastError();
 }
 
-cudaError_t launch_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out, cudaStream_t st) {
-    k_film_exposure<<<(npix + 255) / 256, 256, 0, st>>>(film, npix, exposure, out);
+cudaError_t launch_picture(const float4 *film, uint32_t npix, float exposure, uint32_t tone_mapper, uint32_t passes,
+                           bool gamma, float4 *out, uchar4 *out8, cudaStream_t st) {
+    k_film_picture<<<(npix + 255) / 256, 256, 0, st>>>(film, npix, exposure, tone_mapper, passes, gamma, out, out8);
     g_launches++;
     return cudaGetLastError();
 }

@@ -1265,6 +1265,12 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     uint32_t w = res.size() >= 2 ? static_cast<uint32_t>(res[0]) : 1280u;
     uint32_t h = res.size() >= 2 ? static_cast<uint32_t>(res[1]) : 720u;
     s.cam.exposure = rc["exposure"].as_float(1.0f);
+    // ToneMapperDesc (node_desc.cpp:201-207): radiance_collector.param.tone_mapper.type.
+    const std::string tm = rc["tone_mapper"]["type"].as_string("linear");
+    if (tm == "linear") s.tone_mapper = kToneLinear;
+    else if (tm == "aces") s.tone_mapper = kToneAces;
+    else if (tm == "reinhard") s.tone_mapper = kToneReinhard;
+    else throw unsupported("tone mapper '" + tm + "'");
     // ThinLensCamera (thin_lens.cpp:11-20): lens radius and focal distance.
     s.cam.thin_lens = ct == "thin_lens" ? 1u : 0u;
     s.cam.lens_radius = cp["lens_radius"].as_float(0.0f);

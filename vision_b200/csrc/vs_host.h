@@ -48,6 +48,8 @@ struct HostScene {
     std::vector<float> filter_tab;
     std::vector<AliasEntry> filter_alias;
     float filter_integral = 0.0f;
+    // Tone mapper of the radiance collector (ToneMapper).
+    uint32_t tone_mapper = 0;
     bool needs_luts = false;
     std::string lut_cache;
     Camera cam{};

@@ -22,6 +22,10 @@ unsigned long long launch_count();
 void add_launches(unsigned n);
 // wavefront.cu
 cudaError_t upload_spectral_consts_wf(const float *x, const float *y, const float *z, const float *d65, float y_integral);
+
+// Albedo tables (kLutFloats floats at `out`, device memory) with strata^2
+// samples per cell (lut_gen.cu).
+cudaError_t launch_albedo_luts(float *out, uint32_t strata, cudaStream_t st);
 // server.cu
 cudaError_t upload_spectral_consts_serve(const float *x, const float *y, const float *z, const float *d65,
                                          float y_integral);
@@ -42,6 +46,10 @@ cudaError_t upload_spectral_consts_serve(const float *x, const float *y, const f
 VS_RT_DECLARE(rt_all)
 VS_RT_DECLARE(rt_diffuse)
 #undef VS_RT_DECLARE
-cudaError_t launch_exposure(const float4 *film, uint32_t npix, float exposure, float4 *out, cudaStream_t st);
+// Exposed and tone-mapped pictures of the linear film (k_film_picture):
+// `passes` applications of the tone mapper, then the sRGB gamma if asked;
+// float4 to `out`, or 8-bit RGBA to `out8` when it is not null.
+cudaError_t launch_picture(const float4 *film, uint32_t npix, float exposure, uint32_t tone_mapper, uint32_t passes,
+                           bool gamma, float4 *out, uchar4 *out8, cudaStream_t st);
 
 }  // namespace vs

@@ -85,6 +85,9 @@ struct AliasEntry {
 // Pixel filters (src/render_core/filters): box and triangle sample in closed
 // form; Gaussian, Mitchell and Lanczos-sinc through a 20 x 20 table of the
 // filter over [0, r]^2 and a 2D alias warper (fitted_curve.h).
+// Tone mappers of the radiance collector (tonemappers/impl.cpp).
+enum ToneMapper : uint32_t { kToneLinear = 0, kToneAces = 1, kToneReinhard = 2 };
+
 enum FilterType : uint32_t { kFilterBox = 0, kFilterTriangle = 1, kFilterGaussian = 2, kFilterMitchell = 3,
                              kFilterSinc = 4 };
 constexpr uint32_t kFilterTable = 20;
