@@ -58,7 +58,12 @@ struct AreaLight {
     float scale, lum_power;
     float coef[4];
     float rgb_avg[4];
+    uint32_t shape;  // 0 area, 1 point, 2 spot
+    float cos_angle, cos_start;
+    uint32_t pad;
+    float pos[4], dir[4];
 };
+static_assert(sizeof(AreaLight) == 112, "light record layout");
 struct Instance {
     uint32_t mat_id, light_id, first_prim, prim_count;
 };
@@ -790,6 +795,26 @@ static LS sample_light(const Scene &sc, const It &it, float ul, float ux, float 
         return ls;
     }
     const AreaLight &L = sc.lights[li];
+    if (L.shape != 0) {
+        // Point / spot light (point.cpp:36-41, spot.cpp:47-67): colour * scale
+        // / d^2 (times the spot falloff); pdf -pmf marks the delta light.
+        V3 lp = {L.pos[0], L.pos[1], L.pos[2]};
+        V3 wu = sub(it.pos, lp);
+        float g = 1.0f / dot(wu, wu);
+        if (L.shape == 2) {
+            float ct = dot(V3{L.dir[0], L.dir[1], L.dir[2]}, normalize(wu));
+            float c = std::min(std::max(ct, L.cos_angle), L.cos_start);
+            float range = L.cos_start - L.cos_angle;
+            float f = range > 0.0f ? (c - L.cos_angle) / range : (ct >= L.cos_start ? 1.0f : 0.0f);
+            float f2 = f * f;
+            g *= f2 * f2;
+        }
+        emitter(L, w, ls.L);
+        for (int i = 0; i < w.n; ++i) ls.L[i] *= g;
+        ls.pdf = -pmf_l;
+        ls.p = lp;
+        return ls;
+    }
     float ur = ux;
     uint32_t local = alias_sample(sc.prim_alias + L.alias_offset, L.prim_count, ux, &ur);
     float pmf_p = sc.s->prim_pmf[L.alias_offset + local];
@@ -1466,11 +1491,15 @@ static V3 path_li(const Scene &sc, Sampler &smp, Swl &w, V3 ro, V3 rd, float sca
         V3 wi_s;
         float bs_eta = 1.0f;
         Eval be = bsdf_sample(bsdf, it.wo, smp, wi_s, bs_eta, mt.type == 1);
-        float wmis = ls.pdf / (ls.pdf + se.pdf);
+        // direct_lighting (integrator.cpp:29-31): a delta light (pdf < 0)
+        // weighs 1 and divides by its pmf.
+        bool delta = ls.pdf < 0.0f;
+        float lpdf = delta ? -ls.pdf : ls.pdf;
+        float wmis = delta ? 1.0f : ls.pdf / (ls.pdf + se.pdf);
         if (ip.mis_mode == 1) wmis = 1.0f;
-        if (!occ && se.pdf > 0.0f && ls.pdf > 0.0f && ip.mis_mode != 2) {
+        if (!occ && se.pdf > 0.0f && lpdf > 0.0f && ip.mis_mode != 2) {
             float d[8];
-            for (int i = 0; i < n; ++i) d[i] = thr[i] * (ls.L[i] * se.f[i] * (wmis / ls.pdf));
+            for (int i = 0; i < n; ++i) d[i] = thr[i] * (ls.L[i] * se.f[i] * (wmis / lpdf));
             ret = add(ret, linear_srgb(d, w));
         }
         eta_scale *= bs_eta * bs_eta;

@@ -100,7 +100,7 @@ def test_unknown_filter_is_unsupported(vb, host_ctx):
 def test_rgb_light_is_normalised(vb, host_ctx):
     # Light::Light + NumberArray::normalize: [17,17,17] -> colour 1, scale 17.
     s = vb.Scene(host_ctx, scenes.box_room(width=4, height=4, rgb_light=True))
-    L = s.export('lights', np.float32).reshape(-1, 16)
+    L = s.export('lights', np.float32).reshape(-1, 28)
     Lu = L.view(np.uint32)
     assert Lu[0, 5] == 0  # RGB emitter
     assert L[0, 6] == np.float32(17.0)
@@ -125,7 +125,7 @@ def test_alias_tables_match_reference_algorithm(vb, host_ctx):
         'positions': P, 'indices': I, 'material': 'Light',
         'emission': {'type': 'area', 'param': {'color': [1, 1, 1], 'scale': 1.0}}}})
     s = vb.Scene(host_ctx, sc)
-    L = s.export('lights', np.uint32).reshape(-1, 16)
+    L = s.export('lights', np.uint32).reshape(-1, 28)
     assert L.shape[0] == 2
     off, cnt = L[1, 3], L[1, 2]
     tab = s.export('prim_alias', np.uint8).view([('prob', np.float32), ('alias', np.uint32)])[off:off + cnt]
@@ -171,7 +171,7 @@ def test_golden_alias_tables(vb, host_ctx):
             'positions': P, 'indices': I, 'material': 'Light',
             'emission': {'type': 'area', 'param': {'color': [1, 1, 1]}}}})
         s = vb.Scene(host_ctx, sc)
-        L = s.export('lights', np.uint32).reshape(-1, 16)
+        L = s.export('lights', np.uint32).reshape(-1, 28)
         off, cnt = L[1, 3], L[1, 2]
         pmf = s.export('prim_pmf', np.float32)[off:off + cnt]
         np.testing.assert_allclose(pmf, c['pmf'], rtol=1e-4)
@@ -179,7 +179,7 @@ def test_golden_alias_tables(vb, host_ctx):
 
 def test_unsupported_light_in_light_sampler(vb, host_ctx):
     sc = scenes.box_room(width=4, height=4)
-    sc['light_sampler']['param']['lights'] = [{'type': 'point', 'param': {}}]
+    sc['light_sampler']['param']['lights'] = [{'type': 'projector', 'param': {}}]
     with pytest.raises(vb.UnsupportedError):
         vb.Scene(host_ctx, sc)
 
@@ -225,3 +225,31 @@ def test_tone_mapper_parse(vb, host_ctx, kind, ok):
     else:
         with pytest.raises(vb.UnsupportedError, match='tone mapper'):
             vb.Scene(host_ctx, sc)
+
+
+def test_point_and_spot_light_records(vb, host_ctx):
+    # PointLight / SpotLight (point.cpp:20-43, spot.cpp:19-70): appended after
+    # the area light; spot angles clamped and turned into cosines; powers
+    # 4 pi avg and 2 pi avg (1 - (2 angle + falloff) / 2), angles in radians.
+    s = vb.Scene(host_ctx, scenes.point_light_room(8, 8, light_sampler='power'))
+    L = s.export('lights', np.float32).reshape(-1, 28)
+    U = L.view(np.uint32)
+    assert L.shape[0] == 3 and list(U[:, 16]) == [0, 1, 2]
+    np.testing.assert_allclose(L[1, 20:23], [-0.2, 0.9, 0.1])
+    d = np.array([-0.3, -1.0, -0.4]) / np.linalg.norm([-0.3, -1.0, -0.4])
+    np.testing.assert_allclose(L[2, 24:27], d, rtol=1e-6)
+    a, f = math.radians(30.0), math.radians(12.0)
+    np.testing.assert_allclose(L[2, 17:19], [math.cos(a), math.cos(a - f)], rtol=1e-6)
+    y = lambda rgb: 0.212671 * rgb[0] + 0.715160 * rgb[1] + 0.072169 * rgb[2]
+    np.testing.assert_allclose(L[1, 7], y(L[1, 12:15]) * 4 * math.pi, rtol=1e-5)
+    np.testing.assert_allclose(L[2, 7], y(L[2, 12:15]) * 2 * math.pi * (1 - 0.5 * (2 * a + f)), rtol=1e-5)
+    # The power sampler's pmf follows those powers.
+    pmf = s.export('light_pmf', np.float32)
+    np.testing.assert_allclose(pmf, L[:, 7] / L[:, 7].sum(), rtol=1e-5)
+
+
+def test_delta_lights_with_the_rt_integrator_are_unsupported(vb, host_ctx):
+    sc = scenes.point_light_room(8, 8)
+    sc['integrator'] = {'type': 'rt', 'param': {'max_depth': 4}}
+    with pytest.raises(vb.UnsupportedError, match='point and spot'):
+        vb.Scene(host_ctx, sc)

@@ -214,9 +214,11 @@ __global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ Dev
         BsdfEval<CN> se = bsdf.evaluate(it.wo, wi_light, nullptr);
         BsdfSample<CN> bs = bsdf.sample(it.wo, smp);
         CSpec Ld = CSpec::fill(0.0f);
-        float w_mis = ls.pdf / (ls.pdf + se.pdf);
+        const bool delta = ls.pdf < 0.0f;
+        const float l_pdf = delta ? -ls.pdf : ls.pdf;
+        float w_mis = delta ? 1.0f : ls.pdf / (ls.pdf + se.pdf);
         if (ip.mis_mode == 1u) w_mis = 1.0f;
-        if (!occluded && se.valid() && ls.pdf > 0.0f) Ld = ls.L * se.f * (w_mis / ls.pdf);
+        if (!occluded && se.valid() && l_pdf > 0.0f) Ld = ls.L * se.f * (w_mis / l_pdf);
         if (ip.mis_mode != 2u) gather(throughput * Ld);
         eta_scale *= sqr(bs.eta);
         float lum = throughput.max();

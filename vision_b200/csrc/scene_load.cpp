@@ -954,6 +954,63 @@ struct Loader {
         L.first_prim = inst.first_prim;
         L.prim_count = inst.prim_count;
         L.two_sided = p["two_sided"].as_bool(false) ? 1u : 0u;
+        L.shape = kLightArea;
+        emitter_colour(p, L);
+        // Per-primitive alias table over world-space triangle areas.
+        std::vector<float> areas;
+        float total = 0.0f;
+        for (uint32_t t = 0; t < inst.prim_count; ++t) {
+            uint32_t pr = inst.first_prim + t;
+            f3 p0 = s.pos[s.idx[3 * pr]], p1 = s.pos[s.idx[3 * pr + 1]], p2 = s.pos[s.idx[3 * pr + 2]];
+            float a = 0.5f * length(cross(p0 - p2, p1 - p2));
+            areas.push_back(a);
+            total += a;
+        }
+        std::vector<AliasEntry> tab;
+        std::vector<float> pmf;
+        build_alias(areas, tab, pmf);
+        L.alias_offset = static_cast<uint32_t>(s.prim_alias.size());
+        s.prim_alias.insert(s.prim_alias.end(), tab.begin(), tab.end());
+        s.prim_pmf.insert(s.prim_pmf.end(), pmf.begin(), pmf.end());
+        // AreaLight::power (area.cpp:87-89).
+        f3 power = L.two_sided ? make3(2.0f) * make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]) * (total * kPi)
+                               : make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]) * (total * kPi);
+        L.lum_power = linear_srgb_to_y(power);
+        s.lights.push_back(L);
+    }
+
+    // PointLight (lights/point.cpp:20-43) and SpotLight (lights/spot.cpp:19-70)
+    // of the light sampler's list: colour slot and scale as an area light's,
+    // position; a spot adds its axis, cone angle (degrees, clamped to
+    // [1, 89]) and falloff range (degrees, clamped to [0, angle]).
+    void add_point_light(const std::string &type, const Json &p) {
+        AreaLight L{};
+        L.inst = L.first_prim = L.prim_count = L.alias_offset = kInvalid;
+        L.shape = type == "spot" ? kLightSpot : kLightPoint;
+        emitter_colour(p, L);
+        const f3 pos = as_f3(p["position"], make3(0.0f));
+        L.pos[0] = pos.x; L.pos[1] = pos.y; L.pos[2] = pos.z;
+        const f3 avg = make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]);
+        if (L.shape == kLightPoint) {
+            // PointLight::power: 4 pi * average.
+            L.lum_power = linear_srgb_to_y(avg * (4.0f * kPi));
+        } else {
+            const f3 d = normalize(as_f3(p["direction"], make3(0.0f, 0.0f, 1.0f)));
+            L.dir[0] = d.x; L.dir[1] = d.y; L.dir[2] = d.z;
+            const float angle = clampf(p["angle"].as_float(45.0f), 1.0f, 89.0f) * kPi / 180.0f;
+            const float falloff = std::min(std::max(p["falloff"].as_float(10.0f) * kPi / 180.0f, 0.0f), angle);
+            L.cos_angle = std::cos(angle);
+            L.cos_start = std::cos(std::max(0.0f, angle - falloff));
+            // SpotLight::power: 2 pi * average * (1 - (2 angle + falloff) / 2), angles in radians.
+            L.lum_power = linear_srgb_to_y(avg * (2.0f * kPi * (1.0f - 0.5f * (angle * 2.0f + falloff))));
+        }
+        s.lights.push_back(L);
+    }
+
+    // Light::Light (light.cpp:10-17): the colour slot (RGB illumination or the
+    // blackbody emitter) and the scale, with RGB colours normalised so that
+    // the largest channel is folded into the scale; also the average colour.
+    void emitter_colour(const Json &p, AreaLight &L) {
         float scale = p["scale"].is_number() ? p["scale"].as_float() : 1.0f;
         f3 avg;
         if (is_blackbody_slot(p["color"])) {
@@ -992,27 +1049,6 @@ struct Loader {
         L.rgb_avg[0] = avg.x * scale;
         L.rgb_avg[1] = avg.y * scale;
         L.rgb_avg[2] = avg.z * scale;
-        // Per-primitive alias table over world-space triangle areas.
-        std::vector<float> areas;
-        float total = 0.0f;
-        for (uint32_t t = 0; t < inst.prim_count; ++t) {
-            uint32_t pr = inst.first_prim + t;
-            f3 p0 = s.pos[s.idx[3 * pr]], p1 = s.pos[s.idx[3 * pr + 1]], p2 = s.pos[s.idx[3 * pr + 2]];
-            float a = 0.5f * length(cross(p0 - p2, p1 - p2));
-            areas.push_back(a);
-            total += a;
-        }
-        std::vector<AliasEntry> tab;
-        std::vector<float> pmf;
-        build_alias(areas, tab, pmf);
-        L.alias_offset = static_cast<uint32_t>(s.prim_alias.size());
-        s.prim_alias.insert(s.prim_alias.end(), tab.begin(), tab.end());
-        s.prim_pmf.insert(s.prim_pmf.end(), pmf.begin(), pmf.end());
-        // AreaLight::power (area.cpp:87-89).
-        f3 power = L.two_sided ? make3(2.0f) * make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]) * (total * kPi)
-                               : make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]) * (total * kPi);
-        L.lum_power = linear_srgb_to_y(power);
-        s.lights.push_back(L);
     }
 
     MeshData load_model(const Json &p) {
@@ -1215,6 +1251,10 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     else throw unsupported("light sampler '" + lst + "'");
     for (const Json &l : lsj["param"]["lights"].elements()) {
         std::string lt = l["type"].as_string("area");
+        if (lt == "point" || lt == "spot") {
+            ld.add_point_light(lt, l["param"]);
+            continue;
+        }
         if (lt != "spherical") throw unsupported("light type '" + lt + "' in light_sampler");
         if (s.has_env) throw unsupported("more than one environment light");
         load_spherical(l["param"], root, s);
@@ -1236,7 +1276,11 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     s.ip.min_depth = ip["min_depth"].as_uint(5u);
     s.ip.rr_threshold = ip["rr_threshold"].as_float(1.0f);
     s.ip.mis_mode = ip["mis_mode"].as_uint(0u);
-    if (it == "rt") load_rt(ip, s);
+    if (it == "rt") {
+        for (const AreaLight &L : s.lights)
+            if (L.shape != kLightArea) throw unsupported("point and spot lights with the rt integrator");
+        load_rt(ip, s);
+    }
     // Sampler.
     const Json &smp = root["sampler"];
     std::string st = smp["type"].as_string("independent");

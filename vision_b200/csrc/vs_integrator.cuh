@@ -111,6 +111,17 @@ __device__ __forceinline__ float light_pmf(const DeviceScene &s, uint32_t light)
     return 1.0f / static_cast<float>(s.ip.light_count);
 }
 
+// SpotLight::falloff (spot.cpp:47-55): ((cos - cos_angle) / (cos_start -
+// cos_angle))^4 with cos clamped to [cos_angle, cos_start]; a cone without a
+// falloff range is a hard edge.
+__device__ __forceinline__ float spot_falloff(const AreaLight &L, float cos_theta) {
+    const float c = clampf(cos_theta, L.cos_angle, L.cos_start);
+    const float range = L.cos_start - L.cos_angle;
+    const float f = range > 0.0f ? (c - L.cos_angle) / range : (cos_theta >= L.cos_start ? 1.0f : 0.0f);
+    const float f2 = f * f;
+    return f2 * f2;
+}
+
 template <int N>
 __device__ VS_OUTLINE LightSample<N> sample_light(const DeviceScene &s, const Interaction &it, float u_light,
                                                        f2 u, const Wavelengths<N> &wl) {
@@ -131,7 +142,22 @@ __device__ VS_OUTLINE LightSample<N> sample_light(const DeviceScene &s, const In
         ls.pdf *= pmf_light;
         return ls;
     }
-    AreaLight L = s.lights[li];
+    const AreaLight &L = s.lights[li];
+    if (L.shape != kLightArea) {
+        // IPointLight::sample_wi (light.cpp:42-51) with PointLight::Le /
+        // SpotLight::Le: colour * scale / distance^2, times the spot's
+        // falloff.  A negative pdf marks the delta light (direct_lighting,
+        // integrator.cpp:29-31: MIS weight 1, pdf = the light's pmf).
+        const f3 lp = make3(L.pos[0], L.pos[1], L.pos[2]);
+        const f3 w_un = it.pos - lp;
+        float g = 1.0f / length_sq(w_un);
+        if (L.shape == kLightSpot)
+            g *= spot_falloff(L, dot(make3(L.dir[0], L.dir[1], L.dir[2]), normalize(w_un)));
+        ls.L = emitter_spectrum<N>(L, wl) * g;
+        ls.pdf = -pmf_light;
+        ls.p_light = lp;
+        return ls;
+    }
     float ux = u.x;
     uint32_t local = alias_sample(s.prim_alias + L.alias_offset, L.prim_count, u.x, &ux);
     float pmf_prim = s.prim_pmf[L.alias_offset + local];
@@ -369,14 +395,16 @@ __device__ __forceinline__ bool path_shade_acc(const DeviceScene &s, PathState<N
     f3 wi_light = normalize(ls.p_light - it.pos);
     BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, nullptr);
     BsdfSample<N> bs = bsdf.sample(it.wo, ps.smp);
-    float w_mis = ls.pdf / (ls.pdf + se.pdf);
+    const bool delta = ls.pdf < 0.0f;
+    const float l_pdf = delta ? -ls.pdf : ls.pdf;
+    float w_mis = delta ? 1.0f : ls.pdf / (ls.pdf + se.pdf);
     if (ip.mis_mode == 1u) w_mis = 1.0f;
     if (kTraceShadow) {
         Spec<N> Ld = Spec<N>::fill(0.0f);
-        if (!occluded && se.valid() && ls.pdf > 0.0f) Ld = ls.L * se.f * (w_mis / ls.pdf);
+        if (!occluded && se.valid() && l_pdf > 0.0f) Ld = ls.L * se.f * (w_mis / l_pdf);
         if (ip.mis_mode != 2u) acc(ps, ps.throughput * Ld);
-    } else if (ip.mis_mode != 2u && se.valid() && ls.pdf > 0.0f) {
-        Spec<N> Ld = ls.L * se.f * (w_mis / ls.pdf);
+    } else if (ip.mis_mode != 2u && se.valid() && l_pdf > 0.0f) {
+        Spec<N> Ld = ls.L * se.f * (w_mis / l_pdf);
         sq.o = sh.o;
         sq.d = sh.d;
         sq.tmax = sh.tmax;

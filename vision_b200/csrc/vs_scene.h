@@ -41,7 +41,11 @@ enum EmitterKind : uint32_t {
     kEmitBlackbody = 1,  // Planck spectrum at temperature T, peak-normalised
 };
 
-// 64 bytes.
+// Shape of a light record: an emissive instance, or one of the delta
+// lights of the light sampler's list (IPointLight, light.h:220-249).
+enum LightShape : uint32_t { kLightArea = 0, kLightPoint = 1, kLightSpot = 2 };
+
+// 112 bytes.  Point and spot lights leave the instance fields unused.
 struct alignas(16) AreaLight {
     uint32_t inst;         // emitting instance
     uint32_t first_prim;   // first global primitive of the instance
@@ -53,6 +57,12 @@ struct alignas(16) AreaLight {
     float lum_power;       // luminance of the light power (power light sampler)
     float coef[4];         // RGB: (c0, c1, c2, scale2); blackbody: (T, 1/peak, 0, 0)
     float rgb_avg[4];      // average colour * scale (reference Light::average)
+    uint32_t shape;        // LightShape
+    float cos_angle;       // spot: cos of the cone half-angle
+    float cos_start;       // spot: cos of the angle where the falloff starts
+    uint32_t pad;
+    float pos[4];          // point, spot: position
+    float dir[4];          // spot: unit axis
 };
 
 // One instance of a mesh in the flattened scene.

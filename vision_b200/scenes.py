@@ -112,6 +112,23 @@ def substrate_room(width=64, height=64, dimension=4, sampler="independent", max_
     return sc
 
 
+def point_light_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8, light_sampler="uniform",
+                     area_light=True):
+    """The box room lit by a white point light near the ceiling and a warm
+    spot light aimed at the short box (PointLight / SpotLight of the light
+    sampler's list), with or without the room's area light."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    if not area_light:
+        sc["shapes"] = [s for s in sc["shapes"] if s["name"] != "light"]
+    point = {"type": "point", "param": {"color": {"channels": "xyz", "node": [1.0, 1.0, 1.0]},
+                                        "position": [-0.2, 0.9, 0.1], "scale": 0.15}}
+    spot = {"type": "spot", "param": {"color": {"channels": "xyz", "node": [1.0, 0.8, 0.5]},
+                                      "position": [0.35, 0.95, 0.4], "direction": [-0.3, -1.0, -0.4],
+                                      "angle": 30.0, "falloff": 12.0, "scale": 0.4}}
+    sc["light_sampler"] = {"type": light_sampler, "param": {"lights": [point, spot]}}
+    return sc
+
+
 def _draw_material(rng, name):
     """One of the three material families, drawn uniformly, with the
     parameter distributions of the large-scene workload."""
