@@ -91,7 +91,7 @@ struct EnvLight {
 struct Integrator {
     uint32_t max_depth, min_depth;
     float rr_threshold;
-    uint32_t mis_mode, spectrum_dim, scatter_pdf_dim, sampler, seed, light_sampler, light_count, pad0, pad1;
+    uint32_t mis_mode, spectrum_dim, scatter_pdf_dim, sampler, seed, light_sampler, light_count, srgb, pad1;
 };
 
 }  // namespace oracle
@@ -239,6 +239,27 @@ struct Swl {
     float lambda[8];
     float pdf[8];
 };
+// SRGBSpectrum (srgb.cpp:16-24): three channels at the sRGB primaries' peak
+// wavelengths, stored negated to mark RGB transport (colour decodes pass RGB
+// through; spectral curves are read at |lambda|).
+static Swl rgb_wavelengths(int n) {
+    const float peak[3] = {602.785f, 539.285f, 445.772f};
+    Swl w;
+    w.n = n;
+    for (int i = 0; i < n; ++i) {
+        w.lambda[i] = -peak[i < 3 ? i : 2];
+        w.pdf[i] = 1.0f;
+    }
+    return w;
+}
+static bool is_rgb(const Swl &w) { return w.lambda[0] < 0.0f; }
+// A colour slot's value on channel i: the colour itself under RGB transport,
+// else the sigmoid spectrum at the channel's wavelength.
+static float sigmoid_poly(const float *c, float l);
+static float alb(const float *c, const Swl &w, int i) {
+    return is_rgb(w) ? c[i < 3 ? i : 2] : sigmoid_poly(c, w.lambda[i]);
+}
+
 static Swl sample_wavelengths(int n, float u) {
     Swl w;
     w.n = n;
@@ -256,6 +277,7 @@ static Swl sample_wavelengths(int n, float u) {
 
 // HeroWavelengthSpectrum::cie_xyz / linear_srgb (hero.cpp:261-285; cie.h:414-421).
 static V3 linear_srgb(const float *s, const Swl &w) {
+    if (is_rgb(w)) return {s[0], s[w.n > 1 ? 1 : 0], s[w.n > 2 ? 2 : 0]};
     const Tables &T = tables();
     double dummy = 0;
     (void)dummy;
@@ -636,6 +658,10 @@ static It interaction(const Scene &sc, uint32_t prim, float u, float v, V3 ray_d
 // ----- emitters (area.cpp:91-149, light.cpp, lightsampler.cpp:159-267) --------
 static void emitter(const AreaLight &L, const Swl &w, float *out) {
     const Tables &T = tables();
+    if (is_rgb(w)) {
+        for (int i = 0; i < w.n; ++i) out[i] = L.rgb_avg[i < 3 ? i : 2];
+        return;
+    }
     for (int i = 0; i < w.n; ++i) {
         float l = w.lambda[i];
         float e = L.kind == 0 ? sigmoid_poly(L.coef, l) * L.coef[3] * spd_eval(T.d65, 94, l) : planck(l, L.coef[0]) * L.coef[1];
@@ -719,6 +745,10 @@ static void env_L(const Scene &sc, float u, float v, const Swl &w, float *out) {
         float cc = t[(y1 * W + x0) * 4 + c], d = t[(y1 * W + x1) * 4 + c];
         float top = a + tx * (b - a), bot = cc + tx * (d - cc);
         rgb[c] = top + ty * (bot - top);
+    }
+    if (is_rgb(w)) {
+        for (int i = 0; i < w.n; ++i) out[i] = rgb[i < 3 ? i : 2] * sc.env.scale;
+        return;
     }
     float co[4];
     decode_unbound(sc.s->rgb2spec, rgb[0], rgb[1], rgb[2], co);
@@ -1234,12 +1264,12 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
     b.n = w.n;
     b.fr = it.sh;
     b.ng = it.ng;
-    b.dispersive = (m.flags & 1u) != 0;
+    b.dispersive = (m.flags & 1u) != 0 && !is_rgb(w);
     Lobe &l0 = b.lobes[0];
     b.count = 1;
     if (m.type == 0) {
         l0.kind = Lobe::Lambert;
-        for (int i = 0; i < w.n; ++i) l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
+        for (int i = 0; i < w.n; ++i) l0.kr[i] = alb(m.coef, w, i);
     } else if (m.type == 2) {  // metal: ConductorLobe; mirror: MirrorLobe (FresnelConstant, kr = colour)
         l0.kind = Lobe::MicrofacetRefl;
         const bool mirror = (m.flags & 4u) != 0;
@@ -1249,11 +1279,11 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         l0.ay = m.p[1];
         for (int i = 0; i < w.n; ++i) {
             if (mirror) {
-                l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
+                l0.kr[i] = alb(m.coef, w, i);
             } else {
                 l0.kr[i] = 1.0f;
-                l0.fa[i] = spd_of(sc.s->spd, m.spd0, w.lambda[i]);
-                l0.fb[i] = spd_of(sc.s->spd, m.spd1, w.lambda[i]);
+                l0.fa[i] = spd_of(sc.s->spd, m.spd0, std::fabs(w.lambda[i]));
+                l0.fb[i] = spd_of(sc.s->spd, m.spd1, std::fabs(w.lambda[i]));
             }
         }
     } else if (m.type == 5) {  // substrate: SubstrateLobe over FresnelBlend
@@ -1261,8 +1291,8 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         l0.ax = m.p[0];
         l0.ay = m.p[1];
         for (int i = 0; i < w.n; ++i) {
-            l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
-            l0.fa[i] = sigmoid_poly(m.p + 2, w.lambda[i]);
+            l0.kr[i] = alb(m.coef, w, i);
+            l0.fa[i] = alb(m.p + 2, w, i);
         }
     } else if (m.type == 3) {  // glass: DielectricLobe
         l0.kind = Lobe::Dielectric;
@@ -1270,8 +1300,8 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         l0.ay = m.p[1];
         bool front = dot(it.wo, it.ng) > 0.0f;  // Interaction::correct_eta
         for (int i = 0; i < w.n; ++i) {
-            l0.kr[i] = sigmoid_poly(m.coef, w.lambda[i]);
-            float ior = m.spd0 != kInvalid ? spd_of(sc.s->spd, m.spd0, w.lambda[i]) : m.p[2];
+            l0.kr[i] = alb(m.coef, w, i);
+            float ior = m.spd0 != kInvalid ? spd_of(sc.s->spd, m.spd0, is_rgb(w) ? -w.lambda[0] : w.lambda[i]) : m.p[2];
             l0.eta[i] = front ? ior : 1.0f / ior;
         }
     } else if (m.type == 4) {  // principled_bsdf: metallic, specular, diffuse
@@ -1281,8 +1311,8 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         float color[8], tint[8], weight[8];
         const float tc[3] = {m.p[4], m.p[5], m.p[6]};
         for (int i = 0; i < n; ++i) {
-            color[i] = sigmoid_poly(m.coef, w.lambda[i]);
-            tint[i] = sigmoid_poly(tc, w.lambda[i]);
+            color[i] = alb(m.coef, w, i);
+            tint[i] = alb(tc, w, i);
             weight[i] = 1.0f;
         }
         float cos_theta = dot(it.wo, it.ng);
@@ -1529,7 +1559,7 @@ static V3 trace_path(const Scene &sc, uint32_t px, uint32_t py, uint32_t frame) 
     int n = static_cast<int>(ip.spectrum_dim);
     Sampler smp;
     smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
-    Swl w = sample_wavelengths(n, smp.next());
+    Swl w = ip.srgb ? rgb_wavelengths(n) : sample_wavelengths(n, smp.next());
     smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
     float film_x, film_y;
     V3 ro, rd;

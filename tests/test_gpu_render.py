@@ -158,6 +158,26 @@ def test_matched_seed_parity_point_and_spot_lights(vb, gpu_ctx, sampler, area):
     assert abs(g[..., :3].mean() - c[..., :3].mean()) < 2e-3 * c[..., :3].mean()
 
 
+@pytest.mark.parametrize('builder', ['box_room', 'material_room', 'large_scene'])
+def test_matched_seed_parity_srgb_spectrum(vb, gpu_ctx, builder):
+    # RGB transport (the schema's default spectrum): colours pass through,
+    # conductor and glass curves are read at the primaries' peak wavelengths.
+    if builder == 'large_scene':
+        sc = scenes.large_scene(width=40, height=40, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128,
+                                sampler='independent')
+    else:
+        sc = getattr(scenes, builder)(width=48, height=48)
+    sc.pop('spectrum')
+    s = vb.Scene(gpu_ctx, sc).build_accel()
+    assert s.info()['spectrum_dim'] == 3
+    o = oracle.OracleScene(s)
+    s.render(0, 8)
+    g, c = s.film(), o.render(0, 8)
+    assert np.all(np.isfinite(g)) and g[..., :3].mean() > 0
+    assert _match(g, c, 2e-3) >= (0.97 if builder == 'box_room' else 0.85)
+    assert abs(g[..., :3].mean() - c[..., :3].mean()) < 1e-2 * c[..., :3].mean()
+
+
 def test_matched_seed_parity_environment(vb, gpu_ctx):
     # The large-scene layout at a small size: displaced icosphere, ground tiles
     # with drawn materials, procedural sky with a 5-degree sun (importance
@@ -186,8 +206,8 @@ def test_large_scene_closest_hit_bit_exact(vb, gpu_ctx):
     assert np.array_equal(t_gpu.view(np.uint32), t_cpu.view(np.uint32))
 
 
-@pytest.mark.parametrize('case', ['box_room', 'materials', 'substrate', 'point_lights', 'environment', 'dimension1',
-                                  'two_waves'])
+@pytest.mark.parametrize('case', ['box_room', 'materials', 'substrate', 'point_lights', 'srgb', 'environment',
+                                  'dimension1', 'two_waves'])
 def test_schedules_give_the_same_film(vb, gpu_ctx, case):
     # Path regeneration only changes which thread traces which path, and the
     # wavefront form only where a path's state lives between bounces: each
@@ -201,6 +221,9 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
         sc = scenes.substrate_room(38, 34)
     elif case == 'point_lights':
         sc = scenes.point_light_room(36, 30, light_sampler='power')
+    elif case == 'srgb':
+        sc = scenes.material_room(35, 33)
+        sc.pop('spectrum')
     elif case == 'environment':
         sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
     elif case == 'dimension1':

@@ -253,3 +253,22 @@ def test_delta_lights_with_the_rt_integrator_are_unsupported(vb, host_ctx):
     sc['integrator'] = {'type': 'rt', 'param': {'max_depth': 4}}
     with pytest.raises(vb.UnsupportedError, match='point and spot'):
         vb.Scene(host_ctx, sc)
+
+
+def test_default_spectrum_is_srgb(vb, host_ctx):
+    # SpectrumDesc::init defaults to "srgb" (node_desc.cpp:347-350): three RGB
+    # channels, colours stored as RGB rather than sigmoid coefficients.
+    sc = scenes.box_room(width=4, height=4)
+    sc.pop('spectrum')
+    s = vb.Scene(host_ctx, sc)
+    assert s.info()['spectrum_dim'] == 3
+    integ = s.export('integrator', np.uint32)
+    assert integ[10] == 1
+    mats = s.export('materials', np.float32).reshape(-1, 16)
+    left = [m for m in sc['materials'] if m['name'] == 'LeftWall'][0]['param']['color']
+    np.testing.assert_allclose(mats[3, 4:7], left, rtol=1e-6)
+    hero = vb.Scene(host_ctx, scenes.box_room(width=4, height=4))
+    assert hero.export('integrator', np.uint32)[10] == 0
+    sc['spectrum'] = {'type': 'spectral_upsampling'}
+    with pytest.raises(vb.UnsupportedError, match='spectrum'):
+        vb.Scene(host_ctx, sc)

@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ Dev
     }
     Sampler smp;
     smp.start(px, py, p.frame, 0xffffffffu, ip.sampler, ip.seed);
-    CWl wl = sample_wavelengths<CN>(smp.next());
+    CWl wl = ip.srgb ? rgb_wavelengths<CN>() : sample_wavelengths<CN>(smp.next());
     smp.start(px, py, p.frame, 0u, ip.sampler, ip.seed);
     f2 p_film;
     f3 ro, rd;

@@ -652,6 +652,7 @@ __device__ __forceinline__ bool tile_pixel(const RtParams &p, uint32_t &x, uint3
 
 __device__ __forceinline__ RWl pixel_wavelengths(const DeviceScene &s, uint32_t x, uint32_t y, uint32_t frame) {
     Sampler w;
+    if (s.ip.srgb) return rgb_wavelengths<RN>();
     w.start(x, y, frame, 0xffffffffu, s.ip.sampler, s.ip.seed);
     return sample_wavelengths<RN>(w.next());
 }

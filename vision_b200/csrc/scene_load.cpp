@@ -752,6 +752,21 @@ struct Loader {
     const float *table;
     std::map<std::string, uint32_t> mat_by_name;
     std::string base_dir;  // model files are relative to the scene's folder
+    bool srgb = false;     // RGB spectrum: colour slots are stored as RGB
+
+    // A colour slot as the material record stores it: sigmoid coefficients
+    // for the hero spectrum (RGBAlbedoSpectrum), the colour itself for the
+    // RGB spectrum (SRGBSpectrum::albedo_params, srgb.cpp:26-28).
+    void albedo_coef(const float rgb[3], float out[4]) const {
+        if (srgb) {
+            out[0] = rgb[0];
+            out[1] = rgb[1];
+            out[2] = rgb[2];
+            out[3] = 0.0f;
+        } else {
+            rgb2spec_decode_albedo(table, rgb, out);
+        }
+    }
 
     uint32_t add_spd(const float *v, int n) {
         uint32_t off = static_cast<uint32_t>(s.spd.size());
@@ -772,7 +787,7 @@ struct Loader {
             mat.type = kMatDiffuse;
             rgb = slot_rgb(p["color"], make3(0.5f));
             float in[3] = {rgb.x, rgb.y, rgb.z};
-            rgb2spec_decode_albedo(table, in, mat.coef);
+            albedo_coef(in, mat.coef);
         } else if (type == "black_body") {
             mat.type = kMatBlackBody;
         } else if (type == "metal") {
@@ -813,7 +828,7 @@ struct Loader {
             mat.type = kMatGlass;
             rgb = slot_rgb(p["color"], make3(1.0f));
             float in[3] = {rgb.x, rgb.y, rgb.z};
-            rgb2spec_decode_albedo(table, in, mat.coef);
+            albedo_coef(in, mat.coef);
             std::string glass = p["material_name"].as_string();
             const Json &ior = p["ior"];
             const Json &ion = slot_node(ior);
@@ -844,7 +859,7 @@ struct Loader {
             mat.type = kMatPrincipled;
             rgb = slot_rgb(p["color"], make3(1.0f));
             float in[3] = {rgb.x, rgb.y, rgb.z};
-            rgb2spec_decode_albedo(table, in, mat.coef);
+            albedo_coef(in, mat.coef);
             float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.0001f, 1.0f);
             float aniso = slot_scalar(p["anisotropic"], 0.0f);
             float aspect = std::sqrt(1.0f - aniso * 0.9f);
@@ -854,7 +869,7 @@ struct Loader {
             mat.p[3] = slot_scalar(p["ior"], 1.5f);
             f3 tint = slot_rgb(p["spec_tint"], make3(1.0f));
             float tin[3] = {tint.x, tint.y, tint.z}, tc[4];
-            rgb2spec_decode_albedo(table, tin, tc);
+            albedo_coef(tin, tc);
             mat.p[4] = tc[0]; mat.p[5] = tc[1]; mat.p[6] = tc[2];
             for (const char *key : {"sheen_weight", "coat_weight", "transmission_weight"}) {
                 if (slot_scalar(p[key], 0.0f) != 0.0f)
@@ -869,7 +884,7 @@ struct Loader {
             mat.flags |= kMatFlagConstantFresnel;
             rgb = slot_rgb(p["color"], make3(1.0f));
             float in[3] = {rgb.x, rgb.y, rgb.z};
-            rgb2spec_decode_albedo(table, in, mat.coef);
+            albedo_coef(in, mat.coef);
             float r = clampf(slot_scalar(p["roughness"], 0.001f), 0.0001f, 1.0f);
             float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
             float a = p["remapping_roughness"].as_bool(true) ? r * r : r;
@@ -883,10 +898,10 @@ struct Loader {
             mat.type = kMatSubstrate;
             rgb = slot_rgb(p["color"], make3(1.0f));
             float in[3] = {rgb.x, rgb.y, rgb.z};
-            rgb2spec_decode_albedo(table, in, mat.coef);
+            albedo_coef(in, mat.coef);
             f3 spec = slot_rgb(p["spec"], make3(0.05f));
             float sin[3] = {spec.x, spec.y, spec.z}, sc[4];
-            rgb2spec_decode_albedo(table, sin, sc);
+            albedo_coef(sin, sc);
             mat.p[2] = sc[0]; mat.p[3] = sc[1]; mat.p[4] = sc[2];
             float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.0001f, 1.0f);
             float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
@@ -1235,10 +1250,21 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     Loader ld{s, rgb2spec_table(table_cache), {}, base_dir};
     // Spectrum (SpectrumDesc, node_desc.cpp:346-350; hero.cpp:239).
     const Json &sp = root["spectrum"];
-    s.spectrum_type = sp["type"].as_string("hero");
-    if (s.spectrum_type != "hero") throw unsupported("spectrum type '" + s.spectrum_type + "'");
-    s.ip.spectrum_dim = sp["param"]["dimension"].as_uint(3u);
-    if (s.ip.spectrum_dim < 1 || s.ip.spectrum_dim > 4) throw unsupported("hero dimension " + std::to_string(s.ip.spectrum_dim));
+    // The schema's default is the RGB spectrum (SpectrumDesc::init: "srgb").
+    s.spectrum_type = sp["type"].as_string("srgb");
+    if (s.spectrum_type == "srgb") {
+        // SRGBSpectrum: three RGB channels (Spectrum::dimension, spectrum.h:264).
+        s.ip.srgb = 1u;
+        s.ip.spectrum_dim = 3u;
+    } else if (s.spectrum_type == "hero") {
+        s.ip.srgb = 0u;
+        s.ip.spectrum_dim = sp["param"]["dimension"].as_uint(3u);
+        if (s.ip.spectrum_dim < 1 || s.ip.spectrum_dim > 4)
+            throw unsupported("hero dimension " + std::to_string(s.ip.spectrum_dim));
+    } else {
+        throw unsupported("spectrum type '" + s.spectrum_type + "'");
+    }
+    ld.srgb = s.ip.srgb != 0u;
     // Materials, then shapes (which reference materials by name).
     for (const Json &m : root["materials"].elements()) ld.load_material(m);
     for (const Json &sh : root["shapes"].elements()) ld.load_shape(sh);
@@ -1290,7 +1316,8 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     s.ip.seed = smp["param"]["seed"].as_uint(0u);
     bool dispersive = false;
     for (const Material &m : s.materials) dispersive = dispersive || (m.flags & kMatFlagDispersive);
-    s.ip.scatter_pdf_dim = dispersive ? s.ip.spectrum_dim : 1u;
+    // RGB transport has no dispersion (a glass IOR curve is read at one wavelength).
+    s.ip.scatter_pdf_dim = dispersive && !s.ip.srgb ? s.ip.spectrum_dim : 1u;
     // Camera (SensorDesc, node_desc.cpp:84-95; Sensor::init, sensor.cpp:20-26).
     const Json &cj = root["camera"];
     std::string ct = cj["type"].as_string("pinhole");

@@ -424,7 +424,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
     b.frame = frame;
     b.ng = ng;
     b.luts = s.luts;
-    b.dispersive = (m.flags & kMatFlagDispersive) != 0u;
+    b.dispersive = (m.flags & kMatFlagDispersive) != 0u && !is_rgb(wl);
     b.w_metal = b.w_trans = b.w_spec = b.w_diff = 0.0f;
     b.has_trans = false;
     b.trans_scale = 0.0f;
@@ -448,8 +448,8 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
             const float *k = s.spd + m.spd1;
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                l.fa.v[i] = spd_eval(eta + 1, static_cast<int>(eta[0]), wl.lambda[i]);
-                l.fb.v[i] = spd_eval(k + 1, static_cast<int>(k[0]), wl.lambda[i]);
+                l.fa.v[i] = spd_eval(eta + 1, static_cast<int>(eta[0]), fabsf(wl.lambda[i]));
+                l.fb.v[i] = spd_eval(k + 1, static_cast<int>(k[0]), fabsf(wl.lambda[i]));
             }
         }
     } else if (has_mat<M>(kMatGlass) && m.type == kMatGlass) {
@@ -462,7 +462,10 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
         bool front = dot(wo, ng) > 0.0f;
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-            float ior = m.spd0 != kInvalid ? spd_eval(s.spd + m.spd0 + 1, static_cast<int>(s.spd[m.spd0]), wl.lambda[i])
+            // RGB transport reads the curve at the first channel's wavelength
+            // for every channel (GlassMaterial::init_ior, glass.cpp:224-228).
+            const float lam = is_rgb(wl) ? -wl.lambda[0] : wl.lambda[i];
+            float ior = m.spd0 != kInvalid ? spd_eval(s.spd + m.spd0 + 1, static_cast<int>(s.spd[m.spd0]), lam)
                                            : m.p[2];
             d.eta.v[i] = front ? ior : 1.0f / ior;
         }

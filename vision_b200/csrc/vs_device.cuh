@@ -161,6 +161,27 @@ struct Wavelengths {
     float pdf[N];
 };
 
+// SRGBSpectrum (spectra/srgb.cpp:16-24): three channels at the peak
+// wavelengths of the sRGB primaries (the published constant of the ocarina
+// module the reference builds on, absent from its tree: unpinned), pdf 1.
+// The wavelengths are stored negated: the sign marks RGB transport, so that
+// colour decodes pass RGB through and spectral data (conductor and glass
+// IOR curves) is read at |lambda|.
+template <int N>
+__device__ __forceinline__ Wavelengths<N> rgb_wavelengths() {
+    Wavelengths<N> w;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        w.lambda[i] = i == 0 ? -602.785f : (i == 1 ? -539.285f : -445.772f);
+        w.pdf[i] = 1.0f;
+    }
+    return w;
+}
+template <int N>
+__device__ __forceinline__ bool is_rgb(const Wavelengths<N> &w) {
+    return w.lambda[0] < 0.0f;
+}
+
 __device__ __forceinline__ float cie_spd(const float *tab, float lambda) {
     return spd_eval(tab, kSpd5Count, lambda);
 }
@@ -184,6 +205,8 @@ __device__ __forceinline__ Wavelengths<N> sample_wavelengths(float u) {
 // HeroWavelengthSpectrum::cie_xyz + xyz_to_linear_srgb (hero.cpp:261-285).
 template <int N>
 __device__ VS_OUTLINE f3 linear_srgb(const Spec<N> &s, const Wavelengths<N> &w) {
+    // SRGBSpectrum::linear_srgb: the channels themselves.
+    if (is_rgb(w)) return make3(s.v[0], s.v[N > 1 ? 1 : 0], s.v[N > 2 ? 2 : 0]);
     f3 sum = make3(0.0f);
     int valid = 0;
 #pragma unroll
@@ -203,6 +226,12 @@ __device__ VS_OUTLINE f3 linear_srgb(const Spec<N> &s, const Wavelengths<N> &w) 
 template <int N>
 __device__ __forceinline__ Spec<N> albedo_spectrum(const float *c, const Wavelengths<N> &w) {
     Spec<N> r;
+    if (is_rgb(w)) {
+        // SRGBSpectrum::decode_to_albedo: the colour itself (c holds RGB).
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.v[i] = c[i < 3 ? i : 2];
+        return r;
+    }
 #pragma unroll
     for (int i = 0; i < N; ++i) r.v[i] = sigmoid_poly(c[0], c[1], c[2], w.lambda[i]);
     return r;
@@ -213,6 +242,12 @@ __device__ __forceinline__ Spec<N> albedo_spectrum(const float *c, const Wavelen
 template <int N>
 __device__ __forceinline__ Spec<N> emitter_spectrum(const AreaLight &L, const Wavelengths<N> &w) {
     Spec<N> r;
+    if (is_rgb(w)) {
+        // SRGBSpectrum::decode_to_illumination: the colour times the scale.
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.v[i] = L.rgb_avg[i < 3 ? i : 2];
+        return r;
+    }
 #pragma unroll
     for (int i = 0; i < N; ++i) {
         float l = w.lambda[i];

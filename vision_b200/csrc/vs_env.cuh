@@ -73,9 +73,15 @@ __device__ __forceinline__ f3 env_texel(const DeviceScene &s, float u, float v) 
 template <int N>
 __device__ __forceinline__ Spec<N> env_L(const DeviceScene &s, float u, float v, const Wavelengths<N> &wl) {
     f3 rgb = env_texel(s, u, v);
+    Spec<N> r;
+    if (is_rgb(wl)) {
+        const float ch[3] = {rgb.x, rgb.y, rgb.z};
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.v[i] = ch[i < 3 ? i : 2] * s.env.scale;
+        return r;
+    }
     float c[4];
     rgb2spec_unbound(s.rgb2spec, rgb, c);
-    Spec<N> r;
 #pragma unroll
     for (int i = 0; i < N; ++i)
         r.v[i] = sigmoid_poly(c[0], c[1], c[2], wl.lambda[i]) * c[3] * cie_spd(c_spec.d65, wl.lambda[i]) * s.env.scale;

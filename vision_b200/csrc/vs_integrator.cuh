@@ -481,7 +481,7 @@ __device__ __forceinline__ void path_start(const DeviceScene &s, const Camera &c
                                            uint32_t frame, PathState<N> &ps) {
     const IntegratorParams &ip = s.ip;
     ps.smp.start(px, py, frame, 0xffffffffu, ip.sampler, ip.seed);
-    ps.wl = sample_wavelengths<N>(ps.smp.next());
+    ps.wl = ip.srgb ? rgb_wavelengths<N>() : sample_wavelengths<N>(ps.smp.next());
     ps.smp.start(px, py, frame, 0u, ip.sampler, ip.seed);
     f2 p_film;
     ps.filter_w = camera_ray(s, cam, ps.smp, px, py, p_film, ps.ro, ps.rd);

@@ -134,7 +134,8 @@ struct alignas(16) IntegratorParams {
     uint32_t seed;            // PCG seed
     uint32_t light_sampler;   // LightSamplerType
     uint32_t light_count;
-    uint32_t pad0, pad1;
+    uint32_t srgb;            // 1: SRGBSpectrum (three RGB channels), 0: hero wavelengths
+    uint32_t pad1;
 };
 
 // Compressed 8-wide BVH node: 80 bytes = 5 x 16-byte words.
