@@ -48,3 +48,17 @@ def test_pictures_follow_the_output_path(vb, gpu_ctx, kind):
     assert np.all(rgba[..., 3] == 255)
     for which in (vb.FILM_EXPOSED, vb.FILM_HDR, vb.FILM_DISPLAY):
         assert np.all(s.film(which)[..., 3] == 1.0)
+
+
+def test_full_hd_picture(vb, gpu_ctx):
+    # A 1920 x 1080 film (one frame, depth 2): the picture kernels at the
+    # size a display pipeline reads, against the same restatement.
+    sc = scenes.box_room(width=1920, height=1080, max_depth=2)
+    sc['camera']['param']['radiance_collector']['param']['tone_mapper'] = {'type': 'aces'}
+    s = vb.Scene(gpu_ctx, sc).build_accel()
+    s.render(0, 1)
+    lin = s.film()[..., :3]
+    disp = _srgb(_tm(_tm(1.0 - np.exp(-lin), 'aces'), 'aces'))
+    np.testing.assert_allclose(s.film(vb.FILM_DISPLAY)[..., :3], disp, atol=1e-5, rtol=1e-5)
+    rgba = s.film(vb.FILM_RGBA8)
+    assert np.abs(rgba[..., :3].astype(np.int32) - np.rint(np.clip(disp, 0, 1) * 255.0)).max() <= 1
