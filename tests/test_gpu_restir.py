@@ -32,7 +32,7 @@ def _run(vb, ctx, sc, cams, w, h):
         yield f, s, ort
 
 
-@pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates', 'substrate_mirror'])
+@pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates', 'substrate_mirror', 'srgb'])
 def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
     # 'diffuse': diffuse walls and emitters (the kernels compiled for those
     # materials alone); 'metal': a gold box as well (the general kernels);
@@ -45,6 +45,12 @@ def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
         for m in sc['materials']:
             if m['name'] == 'TallBox':
                 m.update({'type': 'metal', 'param': {'material_name': 'Au', 'roughness': 0.3}})
+    if materials == 'srgb':
+        # The RGB spectrum (the schema's default) with a conductor.
+        sc.pop('spectrum')
+        for m in sc['materials']:
+            if m['name'] == 'TallBox':
+                m.update({'type': 'metal', 'param': {'material_name': 'Cu', 'roughness': 0.2}})
     if materials == 'substrate_mirror':
         # A glossy mirror (Glossy flag) and a substrate floor.
         for m in sc['materials']:

@@ -192,3 +192,18 @@ def test_model_unsupported_options(vb, host_ctx, tmp_path):
         vb.Scene(host_ctx, _model_scene('apple.gltf'), base_dir=str(tmp_path))
     with pytest.raises(vb.VisionError, match='cannot open'):
         vb.Scene(host_ctx, _model_scene('missing.obj'), base_dir=str(tmp_path))
+
+
+def test_model_reader_tolerates_layout_variants(vb, host_ctx, tmp_path):
+    # CRLF line ends, tabs, comments, 3-component texture coordinates and a
+    # 'w' on positions parse like the plain form.
+    plain = 'v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nvt 0 0\nvt 1 0\nvt 1 1\nvt 0 1\nf 1/1 2/2 3/3 4/4\n'
+    variant = ('# quad\r\nv\t0 0 0 1\r\nv 1 0 0 1\r\nv 1 1 0\r\nv 0 1 0\r\n'
+               'vt 0 0 0\r\nvt 1 0 0\r\nvt\t1 1 0\r\nvt 0 1 0\r\n\r\ns off\r\nf\t1/1 2/2\t3/3 4/4\r\n')
+    out = []
+    for name, text in (('plain.obj', plain), ('variant.obj', variant)):
+        (tmp_path / name).write_bytes(text.encode())
+        s = vb.Scene(host_ctx, _model_scene(name), base_dir=str(tmp_path))
+        out.append(_model_arrays(s))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
