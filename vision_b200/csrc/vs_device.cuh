@@ -177,8 +177,11 @@ __device__ __forceinline__ Wavelengths<N> rgb_wavelengths() {
     }
     return w;
 }
+// RGB transport always has three channels (the loader sets the dimension),
+// so the test compiles away for the other widths.
 template <int N>
 __device__ __forceinline__ bool is_rgb(const Wavelengths<N> &w) {
+    if constexpr (N != 3) return false;
     return w.lambda[0] < 0.0f;
 }
 
