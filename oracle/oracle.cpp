@@ -1014,7 +1014,7 @@ struct Eval {
 
 // A lobe of the material's lobe set.
 struct Lobe {
-    enum Kind { Lambert, MicrofacetRefl, Dielectric, NoScatter, Substrate } kind;
+    enum Kind { Lambert, MicrofacetRefl, Dielectric, NoScatter, Substrate, Plastic } kind;
     enum Fr { Conductor, Schlick, F82, One } fresnel = One;
     float ax = 1, ay = 1;
     bool compensate = false;
@@ -1076,6 +1076,22 @@ static void lobe_eval(const Lobe &l, int n, V3 wo, V3 wi, float *f, float &pdf, 
         float comp = l.compensate ? 1.0f / lut2(kLutPure, std::sqrt(l.ax * l.ay), wo.z) : 1.0f;
         for (int i = 0; i < n; ++i) f[i] = b * F[i] * l.kr[i] * comp;
         pdf = mf::pdf_refl(wo, h, l.ax, l.ay);
+    } else if (l.kind == Lobe::Plastic) {
+        // PlasticLobe::evaluate_local_impl (plastic.cpp:27-46): no hemisphere
+        // test; kr = Rd, Schlick F (fa = F0(ior) * Rs, eta0 = ior) at |wh . wo|.
+        flags = kRefl;
+        V3 h = normalize(add(wo, wi));
+        float F[8];
+        fresnel_eval(l, n, std::fabs(dot(h, wo)), F);
+        float b = mf::brdf(wo, h, wi, l.ax, l.ay);
+        float fs = 0.0f;
+        for (int i = 0; i < n; ++i) {
+            f[i] = l.kr[i] * kInvPi * (1.0f - F[i]) + b * F[i];
+            fs += F[i];
+        }
+        float fa = fs * (1.0f / n);
+        float pd = std::fabs(wi.z) * kInvPi;
+        pdf = pd + fa * (mf::pdf_refl(wo, h, l.ax, l.ay) - pd);
     } else if (l.kind == Lobe::Substrate) {
         // FresnelBlend (substrate.cpp:12-72) through BxDF::safe_evaluate:
         // kr = Rd, fa = Rs; specular picked with F_dielectric(|cos wo|, 1.5).
@@ -1184,6 +1200,24 @@ static V3 lobe_sample(const Lobe &l, int n, V3 wo, Sampler &smp, bool &valid) {
         valid = wo.z * wi.z > 0.0f;
         return wi;
     }
+    if (l.kind == Lobe::Plastic) {
+        // PlasticLobe::sample_wi_local_impl (plastic.cpp:61-78).
+        float u0 = smp.next(), u1 = smp.next();
+        V3 h = mf::sample_wh(wo, u0, u1, l.ax, l.ay);
+        float F[8], fs = 0.0f;
+        fresnel_eval(l, n, std::fabs(wo.z), F);
+        for (int i = 0; i < n; ++i) fs += F[i];
+        float uc = smp.next();
+        if (uc < fs * (1.0f / n)) {
+            V3 wi = mf::reflect(wo, h);
+            valid = wo.z * wi.z > 0.0f;
+            return wi;
+        }
+        float v0 = smp.next(), v1 = smp.next();
+        float r = std::sqrt(v0), th = 2.0f * kPi * v1;
+        float dx = r * std::cos(th), dy = r * std::sin(th);
+        return {dx, dy, std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy))};
+    }
     if (l.kind == Lobe::Substrate) {
         // FresnelBlend::sample_wi (substrate.cpp:55-71): remapped u.x picks
         // the microfacet or the cosine-hemisphere direction; always valid.
@@ -1285,6 +1319,17 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
                 l0.fa[i] = spd_of(sc.s->spd, m.spd0, std::fabs(w.lambda[i]));
                 l0.fb[i] = spd_of(sc.s->spd, m.spd1, std::fabs(w.lambda[i]));
             }
+        }
+    } else if (m.type == 5 && (m.flags & 8u)) {  // plastic: PlasticLobe
+        l0.kind = Lobe::Plastic;
+        l0.ax = m.p[0];
+        l0.ay = m.p[1];
+        l0.fresnel = Lobe::Schlick;
+        l0.eta0 = m.p[5];
+        float f0 = ((m.p[5] - 1.0f) / (m.p[5] + 1.0f)) * ((m.p[5] - 1.0f) / (m.p[5] + 1.0f));
+        for (int i = 0; i < w.n; ++i) {
+            l0.kr[i] = alb(m.coef, w, i);
+            l0.fa[i] = f0 * alb(m.p + 2, w, i);
         }
     } else if (m.type == 5) {  // substrate: SubstrateLobe over FresnelBlend
         l0.kind = Lobe::Substrate;

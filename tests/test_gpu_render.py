@@ -122,6 +122,22 @@ def test_matched_seed_parity_substrate_mirror(vb, gpu_ctx):
     assert abs(g.mean() - c.mean()) < 1e-2 * c.mean()
 
 
+def test_matched_seed_parity_plastic(vb, gpu_ctx):
+    # PlasticLobe: Lambert (1 - F) plus Schlick-weighted GGX reflection.
+    s = vb.Scene(gpu_ctx, scenes.plastic_room(64, 64, max_depth=2)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 1e-3) >= 0.99
+    s = vb.Scene(gpu_ctx, scenes.plastic_room(64, 64)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert _match(g, c, 2e-3) >= 0.85
+    assert abs(g[..., :3].mean() - c[..., :3].mean()) < 1e-2 * c[..., :3].mean()
+
+
 def test_model_shape_renders_like_the_oracle(vb, gpu_ctx, tmp_path):
     # The tall box as a Wavefront OBJ model (quads, shared corners, generated
     # smooth normals) instead of the built-in cube.
@@ -206,8 +222,8 @@ def test_large_scene_closest_hit_bit_exact(vb, gpu_ctx):
     assert np.array_equal(t_gpu.view(np.uint32), t_cpu.view(np.uint32))
 
 
-@pytest.mark.parametrize('case', ['box_room', 'materials', 'substrate', 'point_lights', 'srgb', 'environment',
-                                  'dimension1', 'two_waves'])
+@pytest.mark.parametrize('case', ['box_room', 'materials', 'substrate', 'plastic', 'point_lights', 'srgb',
+                                  'environment', 'dimension1', 'two_waves'])
 def test_schedules_give_the_same_film(vb, gpu_ctx, case):
     # Path regeneration only changes which thread traces which path, and the
     # wavefront form only where a path's state lives between bounces: each
@@ -219,6 +235,8 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
         sc = scenes.material_room(40, 36)
     elif case == 'substrate':
         sc = scenes.substrate_room(38, 34)
+    elif case == 'plastic':
+        sc = scenes.plastic_room(38, 34)
     elif case == 'point_lights':
         sc = scenes.point_light_room(36, 30, light_sampler='power')
     elif case == 'srgb':

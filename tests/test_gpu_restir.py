@@ -32,7 +32,8 @@ def _run(vb, ctx, sc, cams, w, h):
         yield f, s, ort
 
 
-@pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates', 'substrate_mirror', 'srgb'])
+@pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates', 'substrate_mirror', 'srgb',
+                                       'plastic'])
 def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
     # 'diffuse': diffuse walls and emitters (the kernels compiled for those
     # materials alone); 'metal': a gold box as well (the general kernels);
@@ -45,6 +46,11 @@ def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
         for m in sc['materials']:
             if m['name'] == 'TallBox':
                 m.update({'type': 'metal', 'param': {'material_name': 'Au', 'roughness': 0.3}})
+    if materials == 'plastic':
+        # A near-specular plastic (delta sampling of its reflection BxDF).
+        for m in sc['materials']:
+            if m['name'] == 'TallBox':
+                m.update({'type': 'plastic', 'param': {'color': [0.7, 0.7, 0.7], 'roughness': 0.1}})
     if materials == 'srgb':
         # The RGB spectrum (the schema's default) with a conductor.
         sc.pop('spectrum')

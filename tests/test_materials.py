@@ -133,3 +133,15 @@ def test_gpu_albedo_tables_need_a_device_and_a_valid_strata(vb, host_ctx):
     with pytest.raises(vb.VisionError) as e:
         vb.albedo_luts_gpu(host_ctx, 0)
     assert e.value.code == vb.VS_E_RANGE
+
+
+def test_plastic_records(vb, host_ctx):
+    # PlasticMaterial (plastic.cpp:80-129): a substrate-class record with the
+    # plastic flag, ior in p[5], roughness remapped twice.
+    s = vb.Scene(host_ctx, scenes.plastic_room(8, 8))
+    mats = s.export('materials', np.uint32).reshape(-1, 16)
+    matf = mats.view(np.float32)
+    for i, alpha, ior in ((5, 0.1 ** 4, 1.3), (6, 0.3 ** 4, 1.5)):
+        assert mats[i, 0] == 5 and (mats[i, 1] & 8)
+        np.testing.assert_allclose(matf[i, 8:10], [max(alpha, 1e-4)] * 2, rtol=1e-5)
+        np.testing.assert_allclose(matf[i, 13], ior, rtol=1e-6)

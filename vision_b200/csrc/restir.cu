@@ -201,6 +201,11 @@ __device__ __forceinline__ void classify(const Material &m, uint32_t &flag, floa
     } else if (m.type == kMatGlass) {
         flag = fminf(m.p[0], m.p[1]) < kAlphaThreshold ? kFlagNearSpec : kFlagGlossy;
         diffuse = sqrtf(m.p[0]);
+    } else if (m.type == kMatSubstrate && (m.flags & kMatFlagPlastic)) {
+        // PlasticLobe: NearSpec below alpha 0.022 (plastic.cpp:120-121), the
+        // microfacet lobe's diffuse factor.
+        flag = fminf(m.p[0], m.p[1]) < kAlphaThreshold ? kFlagNearSpec : kFlagGlossy;
+        diffuse = sqrtf(sqrtf(m.p[0] * m.p[1]));
     } else if (m.type == kMatSubstrate) {
         // SubstrateLobe: always Glossy (substrate.cpp:147), diffuse factor
         // sqrt of the microfacet lobe's (substrate.cpp:74-80).
@@ -224,7 +229,9 @@ __device__ VS_OUTLINE BsdfSample<RN> sample_delta(const Bsdf<RN, VS_RT_MATERIALS
     bs.eta = 1.0f;
     f3 wo = b.frame.to_local(wo_w);
     f3 wi;
-    if (b.type == kMatMetal) {
+    if (b.type == kMatMetal || b.type == kMatSubstrate) {
+        // Metal, mirror, and a near-specular plastic: the microfacet
+        // reflection BxDF of the lobe (kr 1 for plastic).
         wi = make3(-wo.x, -wo.y, wo.z);
         MfLobe<RN> l = b.mf[0];
         l.compensate = false;

@@ -890,6 +890,30 @@ struct Loader {
             float a = p["remapping_roughness"].as_bool(true) ? r * r : r;
             alpha_aniso(a, aniso, mat.p[0], mat.p[1]);
             s.needs_luts = true;
+        } else if (type == "plastic") {
+            // PlasticMaterial (plastic.cpp:80-129): colour (Rd, default 1), spec
+            // (Rs, default 0.05), ior (default 1.3), roughness (default 0.5)
+            // remapped twice like the substrate's; Schlick F0 = F0(ior) * Rs.
+            mat.type = kMatSubstrate;
+            mat.flags |= kMatFlagPlastic;
+            rgb = slot_rgb(p["color"], make3(1.0f));
+            float in[3] = {rgb.x, rgb.y, rgb.z};
+            albedo_coef(in, mat.coef);
+            f3 spec = slot_rgb(p["spec"], make3(0.05f));
+            float sin[3] = {spec.x, spec.y, spec.z}, sc[4];
+            albedo_coef(sin, sc);
+            mat.p[2] = sc[0]; mat.p[3] = sc[1]; mat.p[4] = sc[2];
+            mat.p[5] = clampf(slot_scalar(p["ior"], 1.3f), 1.003f, 5.0f);
+            float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.0001f, 1.0f);
+            float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
+            const bool remap = p["remapping_roughness"].as_bool(true);
+            alpha_aniso(remap ? r * r : r, aniso, mat.p[0], mat.p[1]);
+            if (remap) {
+                mat.p[0] = mat.p[0] * mat.p[0];
+                mat.p[1] = mat.p[1] * mat.p[1];
+            }
+            mat.p[0] = clampf(mat.p[0], 0.0001f, 1.0f);
+            mat.p[1] = clampf(mat.p[1], 0.0001f, 1.0f);
         } else if (type == "substrate") {
             // SubstrateMaterial (substrate.cpp:96-148): colour (Rd, default 1)
             // and spec (Rs, default 0.05) slots, roughness default 0.5.  With

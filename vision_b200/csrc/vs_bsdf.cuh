@@ -230,8 +230,10 @@ struct Bsdf {
     bool dispersive;
     // Diffuse colour (diffuse, principled diffuse lobe, substrate Rd).
     Spec<N> kd;
-    // Substrate specular colour Rs.
+    // Substrate specular colour Rs; plastic: the lobe's Schlick Fresnel sits
+    // in mf[0] (F0 = schlick_F0(ior) * Rs, eta0 = ior).
     Spec<N> ks;
+    bool plastic;
     // Microfacet lobes: metal uses mf[0]; principled uses mf[0] = metallic,
     // mf[1] = specular.
     MfLobe<N> mf[2];
@@ -268,6 +270,35 @@ struct Bsdf {
         const float fr = fresnel_dielectric(co, 1.5f);
         const float pd = ci * kInvPi;
         pdf = pd + fr * (ggx_pdf_reflection(wo, wh, ax, ay) - pd);
+    }
+    // PlasticLobe (plastic.cpp:27-59), evaluated without a hemisphere test
+    // (evaluate_local_impl): Lambert(Rd) (1 - F) + GGX reflection with the
+    // Schlick F at |wh . wo|; pdf lerp(avg F, cosine, GGX reflection).
+    __device__ __forceinline__ void plastic_eval(f3 wo, f3 wi, Spec<N> &f, float &pdf) const {
+        const float ax = mf[0].ax, ay = mf[0].ay;
+        const f3 wh = normalize(wo + wi);
+        const Spec<N> F = mf[0].F(fabsf(dot(wh, wo)));
+        const float brdf = ggx_brdf(wo, wh, wi, ax, ay);
+#pragma unroll
+        for (int i = 0; i < N; ++i) f.v[i] = kd.v[i] * kInvPi * (1.0f - F.v[i]) + brdf * F.v[i];
+        const float pd = fabsf(wi.z) * kInvPi;
+        pdf = pd + avg(F) * (ggx_pdf_reflection(wo, wh, ax, ay) - pd);
+    }
+    // PlasticLobe::sample_wi_local_impl (plastic.cpp:61-78): a microfacet
+    // normal (2D) and one number against avg F(|cos wo|) pick the mirror
+    // direction (valid on wo's side) or a fresh cosine-hemisphere direction
+    // (2D, upper hemisphere).
+    __device__ __forceinline__ f3 plastic_sample(f3 wo, Sampler &smp, bool &valid) const {
+        const f3 wh = ggx_sample_vndf(wo, smp.next2(), mf[0].ax, mf[0].ay);
+        const Spec<N> F = mf[0].F(fabsf(wo.z));
+        const float uc = smp.next();
+        if (uc < avg(F)) {
+            const f3 wi = reflect_dir(wo, wh);
+            valid = wo.z * wi.z > 0.0f;
+            return wi;
+        }
+        valid = true;
+        return cosine_hemisphere(smp.next2());
     }
     __device__ __forceinline__ f3 substrate_sample(f3 wo, f2 u) const {
         const float fr = fresnel_dielectric(fabsf(wo.z), 1.5f);
@@ -309,7 +340,8 @@ struct Bsdf {
             dl.eval_local(wo, wi, luts, e.f, e.pdf, e.flags, eta);
             e.f = e.f * acos_i;
         } else if (has_mat<M>(kMatSubstrate) && type == kMatSubstrate) {
-            substrate_eval(wo, wi, e.f, e.pdf);
+            if (plastic) plastic_eval(wo, wi, e.f, e.pdf);
+            else substrate_eval(wo, wi, e.f, e.pdf);
             e.f = e.f * acos_i;
             e.flags = kFlagReflection;
         } else if (has_mat<M>(kMatPrincipled) && type == kMatPrincipled) {
@@ -377,7 +409,8 @@ struct Bsdf {
         } else if (has_mat<M>(kMatGlass) && type == kMatGlass) {
             wi = dl.sample_local(wo, smp, valid);
         } else if (has_mat<M>(kMatSubstrate) && type == kMatSubstrate) {
-            wi = substrate_sample(wo, smp.next2());
+            if (plastic) wi = plastic_sample(wo, smp, valid);
+            else wi = substrate_sample(wo, smp.next2());
         } else if (has_mat<M>(kMatPrincipled) && type == kMatPrincipled) {
             // LobeSet::sample_wi_impl (lobe.cpp:598-627): 1D lobe choice, an
             // unused 2D draw, then the chosen lobe's own draws.
@@ -426,6 +459,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
     b.luts = s.luts;
     b.dispersive = (m.flags & kMatFlagDispersive) != 0u && !is_rgb(wl);
     b.w_metal = b.w_trans = b.w_spec = b.w_diff = 0.0f;
+    b.plastic = false;
     b.has_trans = false;
     b.trans_scale = 0.0f;
     if (has_mat<M>(kMatDiffuse) && m.type == kMatDiffuse) {
@@ -470,11 +504,22 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
             d.eta.v[i] = front ? ior : 1.0f / ior;
         }
     } else if (has_mat<M>(kMatSubstrate) && m.type == kMatSubstrate) {
-        // SubstrateMaterial::create_lobe_set (substrate.cpp:126-148).
+        // SubstrateMaterial::create_lobe_set (substrate.cpp:126-148);
+        // PlasticMaterial::create_lobe_set (plastic.cpp:105-129).
         b.kd = albedo_spectrum<N>(m.coef, wl);
         b.ks = albedo_spectrum<N>(m.p + 2, wl);
         b.mf[0].ax = m.p[0];
         b.mf[0].ay = m.p[1];
+        b.plastic = (m.flags & kMatFlagPlastic) != 0u;
+        if (b.plastic) {
+            b.mf[0].fresnel = kFresnelSchlick;
+            b.mf[0].eta0 = m.p[5];
+            b.mf[0].compensate = false;
+            b.mf[0].kr = Spec<N>::fill(1.0f);
+            const float f0 = schlick_F0_from_ior(m.p[5]);
+#pragma unroll
+            for (int i = 0; i < N; ++i) b.mf[0].fa.v[i] = f0 * b.ks.v[i];
+        }
     } else if (has_mat<M>(kMatPrincipled) && m.type == kMatPrincipled) {
         // PrincipledBSDF::create_lobe_set (principled_bsdf.cpp:352-461) with
         // sheen and coat at weight 0 (their lobes then contribute nothing).

@@ -22,6 +22,7 @@ enum MaterialFlag : uint32_t {
     kMatFlagDispersive = 1u,
     kMatFlagRemapRoughness = 2u,
     kMatFlagConstantFresnel = 4u,  // kMatMetal written by a `mirror` (mirror.cpp): F = 1, kr = colour
+    kMatFlagPlastic = 8u,          // kMatSubstrate written by a `plastic` (plastic.cpp): PlasticLobe
 };
 
 // 64 bytes.  `coef` holds RGB->spectrum sigmoid coefficients (c0, c1, c2) of

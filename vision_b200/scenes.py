@@ -112,6 +112,18 @@ def substrate_room(width=64, height=64, dimension=4, sampler="independent", max_
     return sc
 
 
+def plastic_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
+    """The box room with plastic boxes (PlasticLobe): a glossy blue short box
+    (ior 1.5, roughness 0.3) and a near-specular white tall box (roughness
+    0.1, remapped twice to alpha 1e-4)."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    mats = {m["name"]: m for m in sc["materials"]}
+    mats["ShortBox"].update({"type": "plastic", "param": {
+        "color": [0.1, 0.2, 0.7], "spec": [1.0, 1.0, 1.0], "ior": 1.5, "roughness": 0.3}})
+    mats["TallBox"].update({"type": "plastic", "param": {"color": [0.8, 0.8, 0.8], "roughness": 0.1}})
+    return sc
+
+
 def point_light_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8, light_sampler="uniform",
                      area_light=True):
     """The box room lit by a white point light near the ceiling and a warm
