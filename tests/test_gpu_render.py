@@ -152,6 +152,10 @@ def test_model_shape_renders_like_the_oracle(vb, gpu_ctx, tmp_path):
             sh['param'] = {'fn': 'box.obj', 'material': 'TallBox', 'smooth': False,
                            'transform': {'type': 'trs', 'param': {'t': [-0.17, 0.0, -0.13], 'r': [0, 1, 0, 15],
                                                                   's': [0.3, 0.6, 0.3]}}}
+    # And a UV sphere (sphere.cpp) on the short box.
+    sc['shapes'].append({'type': 'sphere', 'name': 'ball', 'param': {
+        'radius': 0.08, 'sub_div': 16, 'material': 'ShortBox',
+        'transform': {'type': 'trs', 'param': {'t': [0.17, 0.38, 0.12]}}}})
     s = vb.Scene(gpu_ctx, sc, base_dir=str(tmp_path)).build_accel()
     o = oracle.OracleScene(s)
     s.render(0, 8)

@@ -272,3 +272,27 @@ def test_default_spectrum_is_srgb(vb, host_ctx):
     sc['spectrum'] = {'type': 'spectral_upsampling'}
     with pytest.raises(vb.UnsupportedError, match='spectrum'):
         vb.Scene(host_ctx, sc)
+
+
+def test_sphere_matches_reference_tessellation(vb, host_ctx):
+    # Sphere (sphere.cpp:17-87): 2 + (n - 1) * 2n vertices on the sphere,
+    # 2n + (n - 2) * 4n + 2n triangles, every one facing outwards.
+    n, R = 6, 0.25
+    sc = scenes.box_room(width=4, height=4)
+    sc['shapes'].append({'type': 'sphere', 'name': 'ball', 'param': {
+        'radius': R, 'sub_div': n, 'material': 'TallBox',
+        'transform': {'type': 'trs', 'param': {'t': [0.0, 0.3, 0.0]}}}})
+    s = vb.Scene(host_ctx, sc)
+    pos = s.export('pos', np.float32).reshape(-1, 3)
+    idx = s.export('idx', np.uint32).reshape(-1, 3)
+    nv, nt = 2 + (n - 1) * 2 * n, 2 * n + (n - 2) * 4 * n + 2 * n
+    ball_p = pos[-nv:] - [0.0, 0.3, 0.0]
+    np.testing.assert_allclose(np.linalg.norm(ball_p, axis=1), R, rtol=1e-5)
+    tris = idx[-nt:] - (len(pos) - nv)
+    assert tris.min() == 0 and tris.max() == nv - 1
+    p = ball_p[tris]
+    ng = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+    assert np.all(np.einsum('ij,ij->i', ng, p.mean(1)) > 0)
+    # The reference's first fan triangle and first band triangle.
+    np.testing.assert_array_equal(tris[0], [0, 2, 1])
+    np.testing.assert_array_equal(tris[2 * n], [1, 2, 1 + 2 * n])

@@ -542,6 +542,59 @@ MeshData load_obj(const std::string &path, bool smooth, bool flip_uv, bool swap_
     return m;
 }
 
+// Sphere (src/render_core/shapes/sphere.cpp:17-87): a UV sphere of `radius`
+// with sub_div rings of latitude (default 60) and twice as many meridians;
+// a pole vertex at +y, the rings from the top (ring i at theta = pi i / n,
+// vertex j at phi = 2 pi j / m, normal = position / radius, uv = (j/m, i/n)),
+// a pole vertex at -y, then the top fan, the bands (two triangles per quad,
+// the last quad of a ring wrapping to its first vertex) and the bottom fan,
+// in the reference's vertex and index order so the triangles are the same.
+MeshData make_sphere(float radius, uint32_t n) {
+    if (n < 2u) throw std::runtime_error("sphere sub_div must be at least 2");
+    const uint32_t m = 2u * n;
+    MeshData s;
+    s.p.push_back({0.0f, radius, 0.0f});
+    s.n.push_back({0.0f, 1.0f, 0.0f});
+    s.uv.push_back({0.0f, 0.0f});
+    for (uint32_t i = 1; i < n; ++i) {
+        const float v = static_cast<float>(i) / static_cast<float>(n);
+        const float theta = kPi * v;
+        const float y = radius * std::cos(theta), r = radius * std::sin(theta);
+        for (uint32_t j = 0; j < m; ++j) {
+            const float u = static_cast<float>(j) / static_cast<float>(m);
+            const float phi = u * 2.0f * kPi;
+            const f3 q = j == 0 ? f3{r, y, 0.0f} : f3{std::cos(phi) * r, y, std::sin(phi) * r};
+            s.p.push_back(q);
+            s.n.push_back(normalize(q));
+            s.uv.push_back({j == 0 ? 0.0f : u, v});
+        }
+    }
+    s.p.push_back({0.0f, -radius, 0.0f});
+    s.n.push_back({0.0f, -1.0f, 0.0f});
+    s.uv.push_back({0.0f, 1.0f});
+    auto tri = [&](uint32_t a, uint32_t b, uint32_t c) {
+        s.idx.push_back(a);
+        s.idx.push_back(b);
+        s.idx.push_back(c);
+    };
+    for (uint32_t i = 0; i < m; ++i) tri(0u, (i + 1u) % m + 1u, i + 1u);
+    for (uint32_t i = 0; i + 2u < n; ++i) {
+        uint32_t vs = 1u + i * m;
+        for (uint32_t j = 0; j < m; ++j, ++vs) {
+            if (j != m - 1u) {
+                tri(vs, vs + 1u, vs + m);
+                tri(vs + 1u, vs + m + 1u, vs + m);
+            } else {
+                tri(vs, vs + 1u - m, vs + m);
+                tri(vs + 1u - m, vs + 1u, vs + m);
+            }
+        }
+    }
+    const uint32_t last = static_cast<uint32_t>(s.p.size()) - 1u;
+    for (uint32_t i = 0; i < m; ++i) tri(last, last - ((1u + i) % m + 1u), last - (i + 1u));
+    return s;
+}
+
 // Lattice value noise in [-1, 1] with smoothstep-weighted trilinear
 // interpolation of hashed corner values.
 float value_noise(f3 p, uint32_t seed) {
@@ -1113,6 +1166,7 @@ struct Loader {
         else if (type == "icosphere") mesh = make_icosphere(p);
         else if (type == "grid") mesh = make_grid(p);
         else if (type == "model") mesh = load_model(p);
+        else if (type == "sphere") mesh = make_sphere(p["radius"].as_float(1.0f), p["sub_div"].as_uint(60u));
         else throw unsupported("shape type '" + type + "' (" + name + ")");
         const Json *emission = p.contains("emission") ? &p["emission"] : nullptr;
         uint32_t mat = kInvalid;
