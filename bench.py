@@ -12,6 +12,11 @@ device time of the K timed steps, in Mpaths/s.  Multi-GPU runs are
 independent replicas (weak scaling); the path has no exchange step.
 --impl reference times the reference integrator's CPU restatement (the
 reference itself does not build offline) on the host cores.
+
+The default run (large_scene, one GPU) also runs the metric's other workloads
+after the headline and reports them under `sub`: the box room, the ReSTIR
+frame, the radiance cache (time to relMSE 1e-2) and a serving run (its job
+count in its config); --no-sub skips them.
 """
 import argparse
 import json
@@ -72,6 +77,14 @@ NCU_TRAFFIC_PER_PATH = {('large_scene', 'persistent'): 383.6e6 / 2097152,
                         # all wavefront kernels of one render (2,097,152 and 1,048,576 paths)
                         ('large_scene', 'wavefront'): 3017.6e6 / 2097152,
                         ('box_room', 'wavefront'): 1990.0e6 / 1048576}
+
+# Issue-slot utilisation and active threads per instruction of the dominant
+# traversal kernel, from the committed one-kernel ncu capture of the same
+# workload's 2-spp case (the binding measure of the L1/L2-resident traversal).
+NCU_ISSUE = {('large_scene', 'wavefront'): {
+    'issue_active': 0.715, 'threads_per_inst': 10.3,
+    'issue_source': 'ncu sm__inst_issued / smsp__thread_inst_executed_per_inst_executed of k_wf_extend '
+                    '(profiles/k_wf_extend_large_scene.md)'}}
 
 # Algorithmic bytes per pixel-frame of the ReSTIR frame, from the record sizes
 # (64 B surfaces and reservoirs, 32 B extensions and BSDF samples, 16 B
@@ -273,6 +286,8 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-sub', action='store_true',
+                    help='skip the other workloads that the default run reports under `sub`')
     ap.add_argument('--schedule', default='wavefront', choices=['wavefront', 'persistent', 'grid'],
                     help='path scheduling of the megakernel (both give the same film)')
     ap.add_argument('--spp', type=int, default=None,
@@ -298,15 +313,42 @@ def main():
     w = dict(WORKLOADS[args.workload])
     if args.spp:
         w['spp'] = args.spp
-    if w['kind'] == 'many_lights':
-        run_restir(args, w, rank, world, local_rank, dist)
-        return
-    if w['kind'] == 'serving':
-        run_serving(args, w, rank, world, local_rank, dist)
-        return
-    if w['kind'] == 'radiance_cache':
-        run_cache(args, w, rank, world, local_rank, dist)
-        return
+    line = RUNNERS[w['kind']](args, w, rank, world, local_rank, dist)
+    if rank == 0 and world == 1 and args.workload == DEFAULT_WORKLOAD and not args.no_sub:
+        line['sub'] = run_sub(args, local_rank)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+# The other workloads of the metric, run after the headline in the default
+# invocation (one GPU) and reported under the line's `sub` key: the box room
+# (the plain tracer's stated target configuration), the ReSTIR frame, the
+# radiance cache's time to relMSE 1e-2 and a serving run of SUB_STEPS['serving']
+# jobs of the seeded Poisson sequence.
+SUB_STEPS = {'box_room': 100, 'many_lights': 32, 'radiance_cache': 16, 'serving': 200}
+
+
+def run_sub(args, local_rank):
+    out = {}
+    for name, steps in SUB_STEPS.items():
+        sub_args = argparse.Namespace(**vars(args))
+        sub_args.workload, sub_args.steps, sub_args.warmup = name, steps, max(args.warmup, 3)
+        sub_args.no_cpu_baseline, sub_args.spp = True, None
+        w = dict(WORKLOADS[name])
+        t0 = time.perf_counter()
+        line = RUNNERS[w['kind']](sub_args, w, 0, 1, local_rank, None)
+        line['wall_s'] = round(time.perf_counter() - t0, 1)
+        out[name] = line
+    return out
+
+
+def run_plain(args, w, rank, world, local_rank, dist):
+    """The plain tracer workloads (large scene, box room): one step renders
+    every pixel at the workload's spp through vs_render."""
+    import torch
+    import vision_b200 as vb
     ctx = vb.Context(local_rank)
     scene = vb.Scene(ctx, workload_scene(args.workload))
     t0 = time.perf_counter()
@@ -408,12 +450,12 @@ def main():
                 'd2h_bytes_per_step': int(film_np.nbytes)},
         'gpu_launches': int(launches),
     }
+    issue = NCU_ISSUE.get((args.workload, args.schedule))
+    if issue:
+        line['roofline'].update(issue)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline(scene, spp)
-    if rank == 0:
-        print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    return line
 
 
 def run_restir(args, w, rank, world, local_rank, dist):
@@ -518,10 +560,7 @@ def run_restir(args, w, rank, world, local_rank, dist):
         line['cpu_baseline'] = {'value': frames * npix / dt / 1e6, 'unit': 'Mpaths/s', 'cores': threads,
                                 'kind': 'port', 'sample': '%d full %dx%d frames of the oracle ReSTIR' % (
                                     frames, w['width'], w['height'])}
-    if rank == 0:
-        print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    return line
 
 
 def relmse(img, ref, eps=1e-2):
@@ -671,8 +710,7 @@ def run_cache(args, w, rank, world, local_rank, dist):
                 'd2h_bytes_per_step': int(film_np.nbytes)},
         'gpu_launches': int(launches),
     }
-    if rank == 0:
-        print(json.dumps(line))
+    return line
 
 
 def serving_scenes():
@@ -781,9 +819,12 @@ def run_serving(args, w, rank, world, local_rank, dist):
                 'd2h_bytes_per_step': int(done_bytes[0] / max(len(jobs), 1))},
         'gpu_launches': int(launches),
     }
-    if rank == 0:
-        print(json.dumps(line))
     srv.close()
+    return line
+
+
+RUNNERS = {'box_room': run_plain, 'large_scene': run_plain, 'many_lights': run_restir,
+           'radiance_cache': run_cache, 'serving': run_serving}
 
 
 if __name__ == '__main__':

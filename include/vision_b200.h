@@ -48,6 +48,10 @@ extern "C" {
 #define VS_FILM_DISPLAY 3
 #define VS_FILM_HDR 4
 #define VS_FILM_RGBA8 5
+/* FP64 sums of squares: double4 (r^2, g^2, b^2, 0) per pixel, kept beside
+ * VS_FILM_SUM64 by vs_render with VS_FILM_FP64 from frame 0; with the sums
+ * they give each pixel's sample variance (the per-pixel z-test of two films). */
+#define VS_FILM_SUMSQ64 6
 
 typedef struct vs_context vs_context;
 typedef struct vs_scene vs_scene;
@@ -176,6 +180,15 @@ int vs_trace_closest_host(vs_scene *scene, const float *rays, uint32_t n, vs_hit
 int vs_trace_any_device(vs_scene *scene, const float *rays, uint32_t n, uint32_t *occluded, void *stream);
 int vs_trace_any_host(vs_scene *scene, const float *rays, uint32_t n, uint32_t *occluded);
 
+/* Device sampler streams (parity hook for the reference's
+ * IndependentSampler::start / next_1d, src/render_core/samplers/independent.cpp:24-42,
+ * and the PCG32 option).  keys4 holds `count` host (px, py, sample, dim)
+ * quadruples; stream i is started from keys4[4i..4i+3] with
+ * kind 0 (independent: TEA seed, 24-bit LCG) or 1 (PCG32, stream `seed`), and
+ * its `draws` draws go to out[i * draws ...] (host memory).  Synchronous. */
+int vs_sampler_stream(vs_context *ctx, int kind, uint32_t seed, const uint32_t *keys4, uint32_t count, uint32_t draws,
+                      float *out);
+
 /* Number of kernels this library has launched since it was loaded. */
 uint64_t vs_launch_count(void);
 
@@ -200,10 +213,13 @@ int vs_render_stats(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count,
  * frame_begin > 0) and the per-path radiance in a fixed 16 MiB array inside
  * the library, so it calls no cudaMalloc, cudaFree or allocating library
  * routine.  The first call on a device looks up that array's device address;
- * make it before any stream capture.  Resolutions above 1048576 pixels return
- * VS_E_RANGE.  All calls share the one array: calls that overlap on the GPU
- * (other streams, other threads) race and must be serialised by the caller.
- * The scene must have been built with vs_scene_build_accel. */
+ * make it before any stream capture.  The address is kept for the process's
+ * life, so do not call this after cudaDeviceReset on that device.
+ * Resolutions above 1048576 pixels return VS_E_RANGE; a film pointer that is
+ * not 16-byte aligned returns VS_E_INVALID.  All calls share the one array:
+ * calls that overlap on the GPU (other streams, other threads) race and must
+ * be serialised by the caller.  The scene must have been built with
+ * vs_scene_build_accel. */
 int vs_render_noalloc(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, float *film, void *stream);
 
 /* Real-time ReSTIR frame for a scene loaded with integrator type "rt"

@@ -30,3 +30,40 @@ def edge_targets(pos, idx):
     t = idx.reshape(-1, 3)
     mids = [(p[t[:, a]] + p[t[:, b]]) * 0.5 for a, b in ((0, 1), (1, 2), (2, 0))]
     return np.concatenate(mids + [p]).astype(np.float32)
+
+
+def pixel_z(sum_a, sq_a, n_a, sum_b, sq_b, n_b):
+    """Per-pixel, per-channel two-sample z statistic of two Monte Carlo
+    estimates given their FP64 sums and sums of squares over n_a and n_b
+    samples: (mean_a - mean_b) / sqrt(var_a / n_a + var_b / n_b), with the
+    unbiased sample variances.  A tiny floor keeps pixels whose samples are
+    all equal (a directly seen emitter, the empty background) finite: equal
+    means give z = 0 there, different means a large |z|."""
+    sum_a, sq_a, sum_b, sq_b = (np.asarray(x, np.float64) for x in (sum_a, sq_a, sum_b, sq_b))
+    ma, mb = sum_a / n_a, sum_b / n_b
+    va = np.maximum(sq_a / n_a - ma * ma, 0.0) * n_a / (n_a - 1.0)
+    vb = np.maximum(sq_b / n_b - mb * mb, 0.0) * n_b / (n_b - 1.0)
+    floor = (1e-6 * (np.abs(ma) + np.abs(mb))) ** 2 + 1e-20
+    return (ma - mb) / np.sqrt(va / n_a + vb / n_b + floor)
+
+
+def path_sums(values):
+    """Sums and sums of squares over axis 0 of per-path radiance
+    (frames, ..., 3), with NaN/Inf samples zeroed as the film does."""
+    v = np.asarray(values, np.float64)
+    bad = ~np.isfinite(v).all(-1, keepdims=True)
+    v = np.where(bad, 0.0, v)
+    return v.sum(0), (v * v).sum(0)
+
+
+def mean_z(sum_a, sq_a, n_a, sum_b, sq_b, n_b):
+    """z statistic of the difference of two images' means (over all pixels
+    and channels), from per-pixel FP64 sums and sums of squares: robust to a
+    few bright paths (a reflected sun) that dominate a plain relative mean."""
+    sum_a, sq_a, sum_b, sq_b = (np.asarray(x, np.float64) for x in (sum_a, sq_a, sum_b, sq_b))
+    ma, mb = sum_a / n_a, sum_b / n_b
+    va = np.maximum(sq_a / n_a - ma * ma, 0.0) * n_a / (n_a - 1.0)
+    vb = np.maximum(sq_b / n_b - mb * mb, 0.0) * n_b / (n_b - 1.0)
+    k = ma.size
+    se = np.sqrt((va / n_a + vb / n_b).sum()) / k
+    return (ma.mean() - mb.mean()) / max(se, 1e-30)

@@ -34,22 +34,6 @@ def test_matched_seed_parity_box_room(vb, gpu_ctx):
     np.testing.assert_allclose(g64[..., :3] / 16.0, g[..., :3], rtol=2e-4, atol=2e-5)
 
 
-def test_independent_seeds_agree_statistically(vb, gpu_ctx):
-    # Frames 0..63 on the GPU versus frames 64..127 on the oracle: independent
-    # samples of the same estimator; per-pixel z-test on 8x8 blocks.
-    s, o = _pair(vb, gpu_ctx, width=32, height=32)
-    s.render(0, 64, fp64=True)
-    g = s.film(vb.FILM_SUM64)[..., :3] / 64.0
-    # The FP32 film is a running mean over the frame index (frames 64.. would
-    # be averaged with 64 empty frames), so compare the FP64 sums.
-    _, c64 = o.render(64, 64, fp64=True)
-    c = c64[..., :3] / 64.0
-    gb = g.reshape(4, 8, 4, 8, 3).mean((1, 3))
-    cb = c.reshape(4, 8, 4, 8, 3).mean((1, 3))
-    rel = np.abs(gb - cb) / (0.5 * (gb + cb) + 1e-3)
-    assert np.median(rel) < 0.05, rel
-
-
 def test_chunked_frames_equal_single_launch(vb, gpu_ctx):
     s, _ = _pair(vb, gpu_ctx, width=48, height=40)
     s.render(0, 8)

@@ -52,3 +52,17 @@ def test_noalloc_rejects_resolution_beyond_scratch(vb):
     rc = vb.lib.vs_render_noalloc(s.handle, 0, 1, ctypes.c_void_p(film.data_ptr()), None)
     assert rc == vb.VS_E_RANGE
     assert '1048576' in vb.lib.vs_last_error(ctx.handle).decode()
+
+
+def test_noalloc_rejects_misaligned_film(vb):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    ctx = vb.Context(0)
+    s = vb.Scene(ctx, scenes.box_room(width=16, height=16)).build_accel()
+    film = torch.zeros((16 * 16 + 1) * 4, dtype=torch.float32, device='cuda')
+    n0 = vb.launch_count()
+    rc = vb.lib.vs_render_noalloc(s.handle, 0, 1, ctypes.c_void_p(film.data_ptr() + 4), None)
+    assert rc == vb.VS_E_INVALID
+    assert 'aligned' in vb.lib.vs_last_error(ctx.handle).decode()
+    assert vb.launch_count() == n0, 'a kernel was launched for a rejected call'

@@ -13,7 +13,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, 'libvision_b200.so')
+# VISION_B200_LIB may name another build of the same library (for example one
+# compiled with different floating-point contraction flags).
+LIB_PATH = os.environ.get('VISION_B200_LIB') or os.path.join(HERE, 'libvision_b200.so')
 TABLE_CACHE = os.path.join(HERE, 'data', 'srgb2spec_64.bin')
 
 VS_OK = 0
@@ -33,6 +35,7 @@ FILM_SUM64 = 2
 FILM_DISPLAY = 3
 FILM_HDR = 4
 FILM_RGBA8 = 5
+FILM_SUMSQ64 = 6
 
 EXPORT = dict(pos=0, nrm=1, uv=2, idx=3, prim_inst=4, instances=5, materials=6, lights=7, prim_alias=8,
               prim_pmf=9, light_alias=10, light_pmf=11, camera=12, integrator=13, spd=14, material_rgb=15,
@@ -103,6 +106,7 @@ def _load():
         'vs_trace_any_host': ([P, P, U32, P], ctypes.c_int),
         'vs_rgb_to_spectrum': ([P, ctypes.c_char_p, P, ctypes.c_int, P], ctypes.c_int),
         'vs_launch_count': ([], ctypes.c_uint64),
+        'vs_sampler_stream': ([P, ctypes.c_int, U32, P, U32, U32, P], ctypes.c_int),
         'vs_render_stats': ([P, U32, U32, P], ctypes.c_int),
         'vs_timing_enable': ([P, ctypes.c_int], ctypes.c_int),
         'vs_timing_read': ([P, P, P, P], ctypes.c_int),
@@ -154,7 +158,7 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error', 'vs_cache_create',
                       'vs_cache_destroy', 'vs_cache_get_weights', 'vs_cache_set_weights', 'vs_cache_set_optimizer',
                       'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient', 'vs_render_cached',
-                      'vs_render_schedule_set', 'vs_cache_download'])
+                      'vs_render_schedule_set', 'vs_cache_download', 'vs_sampler_stream'])
 CACHE_PARAMS = 16576
 SCHEDULE_GRID = 0
 # Buffers of the last cache-terminated frame (include/vision_b200.h VS_CACHE_*).
@@ -187,6 +191,17 @@ assert RT_SURFACE_DTYPE.itemsize == 64 and DI_RESERVOIR_DTYPE.itemsize == 64 and
 def launch_count():
     """Kernels launched by libvision_b200 since it was loaded."""
     return int(lib.vs_launch_count())
+
+
+def sampler_stream(ctx, keys, draws, kind=0, seed=0):
+    """Device sampler draws: keys is (count, 4) uint32 (px, py, sample, dim);
+    returns (count, draws) float32 from the GPU sampler (kind 0 independent,
+    1 PCG32 with stream `seed`)."""
+    keys = np.ascontiguousarray(keys, np.uint32).reshape(-1, 4)
+    out = np.zeros((keys.shape[0], draws), np.float32)
+    ctx.check(lib.vs_sampler_stream(ctx.handle, kind, seed, _ptr(keys), keys.shape[0], draws, _ptr(out)),
+              'sampler_stream')
+    return out
 
 
 LUT_FLOATS = 164864
@@ -296,7 +311,7 @@ class Scene:
     def film(self, which=FILM_LINEAR):
         i = self.info()
         npix = i['width'] * i['height']
-        if which == FILM_SUM64:
+        if which in (FILM_SUM64, FILM_SUMSQ64):
             out = np.zeros((i['height'], i['width'], 4), np.float64)
         elif which == FILM_RGBA8:
             out = np.zeros((i['height'], i['width'], 4), np.uint8)

@@ -139,6 +139,7 @@ struct vs_scene {
     } cachebuf;
     uint32_t film_frames = 0;
     bool film64_valid = false;
+    bool film64sq_valid = false;  // the second half of film64 holds sums of squares
     // Optional CUDA-event timing of the megakernel and film launches.
     bool timing = false;
     std::vector<cudaEvent_t> ev_render, ev_film;  // start/stop pairs
@@ -364,10 +365,14 @@ int ensure_film(vs_scene *s) {
 
 namespace vs {
 
+std::mutex &noalloc_scene_mutex(vs_scene *s) { return s->mu; }
+
+// The caller holds s->mu (noalloc_scene_mutex) for this call and for every
+// launch that uses the returned view, so a concurrent vs_scene_build_accel
+// cannot free the buffers the view points to.
 int noalloc_prepare(vs_scene *s, void *stream, DeviceScene *view, cudaStream_t *st, int *device) {
     vs_context *ctx = s->ctx;
     if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
-    std::lock_guard<std::mutex> lock(s->mu);
     if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render_noalloc");
     VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     *view = s->device_view();
@@ -462,6 +467,7 @@ int vs_set_resolution(vs_scene *s, uint32_t width, uint32_t height) {
     update_camera(s->host, width, height);
     s->film_frames = 0;
     s->film64_valid = false;
+    s->film64sq_valid = false;
     return VS_OK;
 }
 
@@ -474,6 +480,7 @@ int vs_camera_set(vs_scene *s, const float *c2w16, float fov_y_deg) {
     s->host.cam.tan_half_fov = std::tan(fov * kPi / 180.0f * 0.5f);
     s->film_frames = 0;
     s->film64_valid = false;
+    s->film64sq_valid = false;
     return VS_OK;
 }
 
@@ -572,7 +579,8 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     if (rc != VS_OK) return rc;
     cudaStream_t st = pick_stream(s, stream);
     uint64_t npix = static_cast<uint64_t>(s->host.cam.width) * s->host.cam.height;
-    if (film_precision == VS_FILM_FP64) VS_CUDA(s->film64.alloc(npix * 4), "film64 alloc");
+    // Sums (double4 per pixel) followed by sums of squares (double4 per pixel).
+    if (film_precision == VS_FILM_FP64) VS_CUDA(s->film64.alloc(npix * 8), "film64 alloc");
     uint64_t frames_per_chunk = kMaxPathsPerLaunch / npix;
     if (frames_per_chunk == 0) return fail(ctx, VS_E_RANGE, "resolution above the per-launch path limit");
     if (frames_per_chunk > frame_count) frames_per_chunk = frame_count;
@@ -606,7 +614,8 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
         if (s->timing) VS_CUDA(timed_event(s->ev_film), "timing event");
         VS_CUDA(launch_film(s->radiance.ptr, static_cast<uint32_t>(npix), frame_begin + f, fc, s->film32.ptr,
-                            film_precision == VS_FILM_FP64 ? s->film64.ptr : nullptr, st),
+                            film_precision == VS_FILM_FP64 ? s->film64.ptr : nullptr, st,
+                            film_precision == VS_FILM_FP64 ? s->film64.ptr + npix * 4 : nullptr),
                 "film launch");
         if (s->timing) VS_CUDA(timed_event(s->ev_film), "timing event");
     }
@@ -618,6 +627,7 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     }
     s->film_frames = frame_begin + frame_count;
     s->film64_valid = film_precision == VS_FILM_FP64 && (frame_begin == 0 || s->film64_valid);
+    s->film64sq_valid = film_precision == VS_FILM_FP64 && (frame_begin == 0 || s->film64sq_valid);
     return VS_OK;
 }
 
@@ -669,6 +679,10 @@ int vs_film_download(vs_scene *s, void *dst, size_t bytes, int which) {
         if (!s->film64_valid) return fail(ctx, VS_E_STATE, "FP64 film not rendered");
         if (bytes != npix * 32) return fail(ctx, VS_E_INVALID, "film size mismatch");
         VS_CUDA(cudaMemcpyAsync(dst, s->film64.ptr, bytes, cudaMemcpyDeviceToHost, st), "film copy");
+    } else if (which == VS_FILM_SUMSQ64) {
+        if (!s->film64sq_valid) return fail(ctx, VS_E_STATE, "FP64 film with squares not rendered (vs_render, FP64)");
+        if (bytes != npix * 32) return fail(ctx, VS_E_INVALID, "film size mismatch");
+        VS_CUDA(cudaMemcpyAsync(dst, s->film64.ptr + npix * 4, bytes, cudaMemcpyDeviceToHost, st), "film copy");
     } else {
         return fail(ctx, VS_E_INVALID, "unknown film buffer");
     }
@@ -747,6 +761,32 @@ int vs_trace_any_host(vs_scene *s, const float *rays, uint32_t n, uint32_t *occ)
     if (e != cudaSuccess) return cuda_fail(ctx, e, "trace (host buffers)");
     if (rc != VS_OK) return rc;
     if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "trace sync");
+    return VS_OK;
+}
+
+int vs_sampler_stream(vs_context *ctx, int kind, uint32_t seed, const uint32_t *keys4, uint32_t count, uint32_t draws,
+                      float *out) {
+    if (!ctx || (count && draws && (!keys4 || !out))) return fail(ctx, VS_E_INVALID, "null argument");
+    if (kind != kSamplerIndependent && kind != kSamplerPCG)
+        return fail(ctx, VS_E_INVALID, "sampler kind must be 0 (independent) or 1 (pcg)");
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot run kernels");
+    if (count == 0 || draws == 0) return VS_OK;
+    const size_t out_bytes = static_cast<size_t>(count) * draws * 4;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    uint4 *d_keys = nullptr;
+    float *d_out = nullptr;
+    cudaError_t e = cudaMallocAsync(&d_keys, static_cast<size_t>(count) * 16, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_out, out_bytes, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_keys, keys4, static_cast<size_t>(count) * 16, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = launch_sampler_stream(d_keys, count, draws, static_cast<uint32_t>(kind), seed, d_out, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
+    if (d_keys) cudaFreeAsync(d_keys, st);
+    if (d_out) cudaFreeAsync(d_out, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sampler stream");
+    if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "sampler stream sync");
     return VS_OK;
 }
 
@@ -973,6 +1013,7 @@ int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void
     s->rt.rendered = true;
     s->film_frames = film_index + 1u;
     s->film64_valid = false;
+    s->film64sq_valid = false;
     return VS_OK;
 }
 
@@ -1319,7 +1360,7 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     if (rc != VS_OK) return rc;
     const uint32_t npix = h.cam.width * h.cam.height;
     if (train_samples > npix) train_samples = npix;
-    if (film_precision == VS_FILM_FP64) VS_CUDA(s->film64.alloc(static_cast<size_t>(npix) * 4), "film64 alloc");
+    if (film_precision == VS_FILM_FP64) VS_CUDA(s->film64.alloc(static_cast<size_t>(npix) * 8), "film64 alloc");
     vs_scene::CacheBufs &b = s->cachebuf;
     const size_t nt = train_samples ? train_samples : 1;
     VS_CUDA(b.q_feat.alloc(static_cast<size_t>(npix) * 64), "cache alloc");
@@ -1416,6 +1457,7 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     }
     s->film_frames = frame_begin + frame_count;
     s->film64_valid = film_precision == VS_FILM_FP64 && (frame_begin == 0 || s->film64_valid);
+    s->film64sq_valid = false;
     if (frame_count) {
         b.npix = npix;
         b.n_train = train_samples;

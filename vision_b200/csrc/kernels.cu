@@ -141,12 +141,16 @@ __global__ void k_film_running_mean(const float4 *radiance, uint32_t npix, uint3
     film[i] = acc;
 }
 
-// FP64 film: per-pixel sums of the sanitised samples and the sample count.
+// FP64 film: per-pixel sums of the sanitised samples and the sample count,
+// and (when sq4 is given) the sums of their squares, from which the
+// per-pixel variance of the estimate follows.
 __global__ void k_film_sum64(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count,
-                             double *sum4) {
+                             double *sum4, double *sq4) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npix) return;
     double4 acc = frame_begin == 0 ? make_double4(0, 0, 0, 0) : reinterpret_cast<double4 *>(sum4)[i];
+    double4 sq = make_double4(0, 0, 0, 0);
+    if (sq4 && frame_begin != 0) sq = reinterpret_cast<double4 *>(sq4)[i];
     for (uint32_t f = 0; f < frame_count; ++f) {
         float4 v = radiance[static_cast<size_t>(f) * npix + i];
         bool bad = isnan(v.x) || isnan(v.y) || isnan(v.z) || isinf(v.x) || isinf(v.y) || isinf(v.z);
@@ -155,8 +159,12 @@ __global__ void k_film_sum64(const float4 *radiance, uint32_t npix, uint32_t fra
         acc.y += v.y;
         acc.z += v.z;
         acc.w += 1.0;
+        sq.x += static_cast<double>(v.x) * v.x;
+        sq.y += static_cast<double>(v.y) * v.y;
+        sq.z += static_cast<double>(v.z) * v.z;
     }
     reinterpret_cast<double4 *>(sum4)[i] = acc;
+    if (sq4) reinterpret_cast<double4 *>(sq4)[i] = sq;
 }
 
 // The tone mappers of tonemappers/impl.cpp: linear (identity), ACES (the
@@ -208,6 +216,27 @@ cudaError_t launch_trace_closest(const DeviceScene &s, const float *rays, uint32
                                  cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     k_trace_closest<<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, hits, t);
+    g_launches++;
+    return cudaGetLastError();
+}
+
+// Sampler streams (parity hook): stream i starts at keys[i] = (px, py,
+// sample, dim) and writes `draws` consecutive draws to out[i * draws ...].
+__global__ void __launch_bounds__(128) k_sampler_stream(const uint4 *keys, uint32_t count, uint32_t draws,
+                                                        uint32_t kind, uint32_t seed, float *out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    uint4 k = keys[i];
+    Sampler smp;
+    smp.start(k.x, k.y, k.z, k.w, kind, seed);
+    float *o = out + static_cast<uint64_t>(i) * draws;
+    for (uint32_t j = 0; j < draws; ++j) o[j] = smp.next();
+}
+
+cudaError_t launch_sampler_stream(const uint4 *keys, uint32_t count, uint32_t draws, uint32_t kind, uint32_t seed,
+                                  float *out, cudaStream_t st) {
+    if (count == 0 || draws == 0) return cudaSuccess;
+    k_sampler_stream<<<(count + 127) / 128, 128, 0, st>>>(keys, count, draws, kind, seed, out);
     g_launches++;
     return cudaGetLastError();
 }
@@ -272,14 +301,14 @@ cudaError_t launch_render(const DeviceScene &s, uint32_t frame_begin, uint32_t f
 }
 
 cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count, float4 *film32,
-                        double *film64, cudaStream_t st) {
+                        double *film64, cudaStream_t st, double *film64sq) {
     unsigned blocks = (npix + 255) / 256;
     if (film32) {
         k_film_running_mean<<<blocks, 256, 0, st>>>(radiance, npix, frame_begin, frame_count, film32);
         g_launches++;
     }
     if (film64) {
-        k_film_sum64<<<blocks, 256, 0, st>>>(radiance, npix, frame_begin, frame_count, film64);
+        k_film_sum64<<<blocks, 256, 0, st>>>(radiance, npix, frame_begin, frame_count, film64, film64sq);
         g_launches++;
     }
     return cudaGetLastError();

@@ -16,13 +16,21 @@
 // array's name is only a host-side stand-in, not a device address, so the
 // device address is looked up with cudaGetSymbolAddress once per device, the
 // first time this entry point runs with that device current; that first call
-// should therefore happen before any stream capture.  Each chunk's megakernel
-// writes every scratch entry that the following film pass reads, so the array
-// needs no clearing between calls; calls that overlap on the GPU share it and
-// race.
+// should therefore happen before any stream capture.  The looked-up address is
+// kept for the life of the process: after cudaDeviceReset (or anything else
+// that destroys and re-creates the device's primary context) the library's
+// module is loaded again and the kept address is stale, so this entry point
+// must not be used after such a reset.  Each chunk's megakernel writes every
+// scratch entry that the following film pass reads, so the array needs no
+// clearing between calls; calls that overlap on the GPU share it and race.
+//
+// The scene's lock is held from the argument checks to the last launch, as
+// vs_render holds it: a concurrent vs_scene_build_accel (which frees and
+// re-uploads the scene's device buffers) waits until the launches are queued.
 #include "../../include/vision_b200.h"
 #include "vs_launch.h"
 
+#include <cstdint>
 #include <mutex>
 
 namespace vs {
@@ -53,9 +61,11 @@ cudaError_t scratch_address(int device, float4 **out) {
 }
 }  // namespace
 
-// Implemented in capi.cu: checks that the scene is on the device, makes its
-// device current and returns its device view and the render stream.  Neither
-// allocates.
+// Implemented in capi.cu.  noalloc_scene_mutex is the scene's lock;
+// noalloc_prepare (called with that lock held) checks that the scene is on the
+// device, makes its device current and returns its device view and the render
+// stream.  Neither allocates.
+std::mutex &noalloc_scene_mutex(vs_scene *scene);
 int noalloc_prepare(vs_scene *scene, void *stream, DeviceScene *view, cudaStream_t *st, int *device);
 int noalloc_fail(vs_scene *scene, int code, const char *msg);
 
@@ -65,6 +75,10 @@ extern "C" int vs_render_noalloc(vs_scene *scene, uint32_t frame_begin, uint32_t
                                  void *stream) {
     using namespace vs;
     if (!scene || !film) return VS_E_INVALID;
+    if (reinterpret_cast<uintptr_t>(film) % 16 != 0)
+        return noalloc_fail(scene, VS_E_INVALID,
+                            "vs_render_noalloc: film must be 16-byte aligned (it is read and written as float4)");
+    std::lock_guard<std::mutex> lock(noalloc_scene_mutex(scene));
     DeviceScene view;
     cudaStream_t st;
     int device = -1;
@@ -78,13 +92,15 @@ extern "C" int vs_render_noalloc(vs_scene *scene, uint32_t frame_begin, uint32_t
     float4 *scratch = nullptr;
     cudaError_t e = scratch_address(device, &scratch);
     if (e != cudaSuccess) return noalloc_fail(scene, VS_E_CUDA, cudaGetErrorString(e));
-    uint32_t frames_per_chunk = static_cast<uint32_t>(kNoAllocScratchPaths / npix);
+    const uint64_t frames_per_chunk = kNoAllocScratchPaths / npix;
     float4 *film4 = reinterpret_cast<float4 *>(film);
-    for (uint32_t f = 0; f < frame_count; f += frames_per_chunk) {
-        uint32_t fc = frame_count - f < frames_per_chunk ? frame_count - f : frames_per_chunk;
-        e = launch_render(view, frame_begin + f, fc, scratch, st);
-        if (e == cudaSuccess)
-            e = launch_film(scratch, static_cast<uint32_t>(npix), frame_begin + f, fc, film4, nullptr, st);
+    // 64-bit counter: frames_per_chunk reaches 2^20, so a 32-bit f + chunk
+    // could wrap for frame counts near 2^32 and never end the loop.
+    for (uint64_t f = 0; f < frame_count; f += frames_per_chunk) {
+        uint32_t fc = static_cast<uint32_t>(frame_count - f < frames_per_chunk ? frame_count - f : frames_per_chunk);
+        uint32_t fb = frame_begin + static_cast<uint32_t>(f);
+        e = launch_render(view, fb, fc, scratch, st);
+        if (e == cudaSuccess) e = launch_film(scratch, static_cast<uint32_t>(npix), fb, fc, film4, nullptr, st);
         if (e != cudaSuccess) return noalloc_fail(scene, VS_E_CUDA, cudaGetErrorString(e));
     }
     return VS_OK;

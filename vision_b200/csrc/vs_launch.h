@@ -12,12 +12,17 @@ cudaError_t upload_spectral_consts(const float *x, const float *y, const float *
 cudaError_t launch_trace_closest(const DeviceScene &s, const float *rays, uint32_t n, Hit *hits, float *t,
                                  cudaStream_t st);
 cudaError_t launch_trace_any(const DeviceScene &s, const float *rays, uint32_t n, uint32_t *occ, cudaStream_t st);
+// Sampler streams (kernels.cu): `count` streams started at keys (px, py,
+// sample, dim), `draws` draws each, to out (device memory).
+cudaError_t launch_sampler_stream(const uint4 *keys, uint32_t count, uint32_t draws, uint32_t kind, uint32_t seed,
+                                  float *out, cudaStream_t st);
 // path_counter: one device word; when given, the persistent regenerating
 // kernel traces the paths (same output as the one-path-per-thread grid).
 cudaError_t launch_render(const DeviceScene &s, uint32_t frame_begin, uint32_t frame_count, float4 *radiance,
                           cudaStream_t st, unsigned long long *path_counter = nullptr);
+// film64: double4 sums per pixel; film64sq (optional): double4 sums of squares.
 cudaError_t launch_film(const float4 *radiance, uint32_t npix, uint32_t frame_begin, uint32_t frame_count, float4 *film32,
-                        double *film64, cudaStream_t st);
+                        double *film64, cudaStream_t st, double *film64sq = nullptr);
 unsigned long long launch_count();
 void add_launches(unsigned n);
 // wavefront.cu
