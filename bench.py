@@ -103,8 +103,22 @@ def restir_bytes_per_pixel(M, S):
             (64 + 64 + 32 + 8 + 128 + 64) + (64 + 64 + S * 128 + 16 + 64) + (32 + 32))
 
 
+def scenes_module():
+    """The scene builders (vision_b200/scenes.py, plain Python).  Loaded from
+    its file when the vision_b200 package is not imported, so that the
+    reference arm never loads the CUDA library."""
+    if 'vision_b200' in sys.modules:
+        from vision_b200 import scenes
+        return scenes
+    import importlib.util
+    spec = importlib.util.spec_from_file_location('vision_scenes', os.path.join(ROOT, 'vision_b200', 'scenes.py'))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def workload_scene(name):
-    from vision_b200 import scenes
+    scenes = scenes_module()
     w = WORKLOADS[name]
     if w['kind'] == 'box_room':
         return scenes.box_room(width=w['width'], height=w['height'], max_depth=w['max_depth'],
@@ -185,13 +199,14 @@ class ClockSampler:
                 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_baseline(scene, spp, budget_s=12.0):
-    """The oracle (a scalar C++ port of the reference integrator) on all host
-    cores, on a fixed seeded subset of the workload's pixels (at most 262,144),
-    frame after frame (frame indices continue past the workload's spp) until
-    the time budget is used."""
+def cpu_baseline(doc, spp, budget_s=12.0):
+    """The oracle (a scalar C++ port of the reference integrator, with its own
+    scene ingestion of the workload's scene document) on all host cores, on a
+    fixed seeded subset of the workload's pixels (at most 262,144), frame after
+    frame (frame indices continue past the workload's spp) until the time
+    budget is used."""
     import oracle
-    o = oracle.OracleScene(scene)
+    o = oracle.OracleScene.from_json(doc)
     threads = os.cpu_count()
     pixels = sample_pixels(o.width, o.height, min(o.width * o.height, 262144))
     o.paths(pixels[:256], 0, 1, threads=threads)  # warm-up
@@ -232,10 +247,17 @@ def run_reference(args, rank):
     host cores (the reference's CUDA/OptiX build cannot be built offline)."""
     if rank != 0:
         return
-    import vision_b200 as vb
     import oracle
     w = WORKLOADS[args.workload]
+    if w['kind'] not in ('box_room', 'large_scene', 'many_lights'):
+        print(json.dumps({'impl': 'reference', 'unavailable': 'the reference has no %s path (a new workload of this '
+                                                               'build; its CPU restatement is the plain tracer)'
+                          % w['kind']}))
+        return
     if w['kind'] == 'many_lights':
+        # The ReSTIR frame parameters (camera transforms, resampling settings)
+        # still come from the library's host-side scene layer on this arm.
+        import vision_b200 as vb
         ctx = vb.Context(-1)
         scene = vb.Scene(ctx, workload_scene(args.workload)).build_accel()
         restir_cpu_frames(scene, w, args.warmup)
@@ -253,9 +275,9 @@ def run_reference(args, rank):
                 'e2e': {'value': value, 'unit': 'Mpaths/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
         print(json.dumps(line))
         return
-    ctx = vb.Context(-1)
-    scene = vb.Scene(ctx, workload_scene(args.workload)).build_accel()
-    o = oracle.OracleScene(scene)
+    # The oracle's own scene ingestion: the reference arm never loads the
+    # library (vision_b200 is not imported on this path).
+    o = oracle.OracleScene.from_json(workload_scene(args.workload))
     threads = os.cpu_count()
     pixels = sample_pixels(o.width, o.height, min(o.width * o.height, 262144))
     npix = pixels.size
@@ -454,7 +476,7 @@ def run_plain(args, w, rank, world, local_rank, dist):
     if issue:
         line['roofline'].update(issue)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line['cpu_baseline'] = cpu_baseline(scene, spp)
+        line['cpu_baseline'] = cpu_baseline(workload_scene(args.workload), spp)
     return line
 
 

@@ -76,22 +76,32 @@ def _p(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-class OracleScene:
-    """The exported flat scene of a vision_b200.Scene, held alive for the oracle."""
+SCENE_KEYS = ['pos', 'nrm', 'uv', 'idx', 'prim_inst', 'instances', 'materials', 'lights', 'prim_alias', 'prim_pmf',
+              'light_alias', 'light_pmf', 'camera', 'integrator', 'spd']
+ENV_KEYS = ['env', 'env_tex', 'env_marginal', 'env_marginal_func', 'env_cond', 'env_cond_func', 'rgb2spec']
 
-    def __init__(self, scene):
-        keys = ['pos', 'nrm', 'uv', 'idx', 'prim_inst', 'instances', 'materials', 'lights', 'prim_alias', 'prim_pmf',
-                'light_alias', 'light_pmf', 'camera', 'integrator', 'spd']
-        env = scene.export('env')
-        if env.size:
-            keys += ['env', 'env_tex', 'env_marginal', 'env_marginal_func', 'env_cond', 'env_cond_func', 'rgb2spec']
+
+class OracleScene:
+    """A flat scene held alive for the oracle: either the arrays exported by a
+    vision_b200.Scene (OracleScene(scene): the oracle traces exactly the
+    library's triangles and records), or the oracle's own ingestion of the
+    scene document (OracleScene.from_json(doc), oracle/scene.py), which does
+    not load the library at all."""
+
+    def __init__(self, scene=None, arrays=None, info=None):
+        if scene is not None:
+            env = scene.export('env')
+            keys = SCENE_KEYS + (ENV_KEYS if env.size else [])
+            arrays = {k: scene.export(k) for k in keys}
+            info = scene.info()
+        has_env = 'env' in arrays and arrays['env'].size > 0
         self.arr = {}
-        for k in keys:
-            a = scene.export(k)
+        for k in SCENE_KEYS + (ENV_KEYS if has_env else []):
+            a = np.ascontiguousarray(arrays[k])
             if a.size == 0:
                 a = np.zeros(16, np.uint8)
-            self.arr[k] = np.ascontiguousarray(a)
-        info = scene.info()
+            self.arr[k] = a
+        self.info = info
         self.width, self.height = info['width'], info['height']
         a = self.arr
         self.s = OracleSceneStruct(_p(a['pos']), _p(a['nrm']), _p(a['uv']), _p(a['idx']), _p(a['prim_inst']),
@@ -99,10 +109,14 @@ class OracleScene:
                                    _p(a['materials']), info['material_count'], _p(a['lights']), info['light_count'],
                                    _p(a['prim_alias']), _p(a['prim_pmf']), _p(a['light_alias']), _p(a['light_pmf']),
                                    _p(a['camera']), _p(a['integrator']), _p(a['spd']),
-                                   *([_p(a[k]) for k in ('env', 'env_tex', 'env_marginal', 'env_marginal_func',
-                                                         'env_cond', 'env_cond_func', 'rgb2spec')]
-                                     if env.size else [None] * 7))
+                                   *([_p(a[k]) for k in ENV_KEYS] if has_env else [None] * 7))
         self.h = ctypes.c_void_p(lib().oracle_open(ctypes.byref(self.s)))
+
+    @classmethod
+    def from_json(cls, doc, base_dir='.'):
+        from oracle import scene as oscene
+        arrays, info = oscene.build(doc, base_dir)
+        return cls(arrays=arrays, info=info)
 
     def __del__(self):
         try:
