@@ -16,9 +16,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, '_build', 'liboracle.so')
 
 
+FMA_LIB_PATH = os.path.join(HERE, '_build', 'liboracle_fma.so')
+
+
 def build():
-    srcs = [os.path.join(HERE, f) for f in ('oracle.cpp', 'restir.inc')]
-    if os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(s) for s in srcs):
+    srcs = [os.path.join(HERE, f) for f in ('oracle.cpp', 'restir.inc', 'Makefile')]
+    newest = max(os.path.getmtime(s) for s in srcs)
+    if all(os.path.exists(p) and os.path.getmtime(p) >= newest for p in (LIB_PATH, FMA_LIB_PATH)):
         return LIB_PATH
     subprocess.run(['make', '-s', '-C', HERE], check=True)
     return LIB_PATH
@@ -70,6 +74,36 @@ def lib():
         L.oracle_rt_buffer.argtypes = [P, ctypes.c_int, P, ctypes.c_size_t]
         _lib = L
     return _lib
+
+
+_fma_lib = None
+
+
+def fma_lib():
+    """The oracle compiled with FMA contraction (same source, different
+    rounding): renders through it differ from the oracle's by rounding only."""
+    global _fma_lib
+    if _fma_lib is None:
+        build()
+        L = ctypes.CDLL(FMA_LIB_PATH)
+        for fn in ('oracle_open', 'oracle_close', 'oracle_render'):
+            getattr(L, fn).argtypes = getattr(lib(), fn).argtypes
+            getattr(L, fn).restype = getattr(lib(), fn).restype
+        _fma_lib = L
+    return _fma_lib
+
+
+def render_fma(oscene, frame_begin, frame_count, threads=None):
+    """FP64 film sums of an OracleScene rendered by the FMA-contracted oracle."""
+    L = fma_lib()
+    h = ctypes.c_void_p(L.oracle_open(ctypes.byref(oscene.s)))
+    film = np.zeros((oscene.height, oscene.width, 4), np.float32)
+    f64 = np.zeros((oscene.height, oscene.width, 4), np.float64)
+    try:
+        L.oracle_render(h, frame_begin, frame_count, threads or os.cpu_count(), _p(film), _p(f64))
+    finally:
+        L.oracle_close(h)
+    return f64
 
 
 def _p(a):

@@ -195,8 +195,9 @@ def test_restir_at_benchmark_parameters(vb, gpu_ctx):
         s.set_camera(c2w, 40.0)
         params = s.restir_params(f)
         cam = s.export('camera').copy()
-        s.restir_frame(f, f)
-        ort.frame(cam, params, f)
+        # A new camera restarts the film: each frame is film sample 0.
+        s.restir_frame(f, 0)
+        ort.frame(cam, params, 0)
         gs, cs = s.restir_buffer('surfaces'), ort.buffer('surfaces', vb.RT_SURFACE_DTYPE)
         hit_eq = (gs['hit']['prim_id'] == cs['hit']['prim_id'])
         assert hit_eq.mean() >= 0.999, (f, hit_eq.mean())

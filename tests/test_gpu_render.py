@@ -61,10 +61,12 @@ def _match(g, c, tol):
 
 def test_matched_seed_parity_materials(vb, gpu_ctx):
     # Gold conductor, dispersive glass and principled surfaces.  With one
-    # scattering event the GPU and the oracle evaluate the same samples;
-    # longer specular chains amplify last-bit differences (FMA contraction,
-    # transcendental rounding) into different paths, so the full-depth bar is
-    # statistical.
+    # scattering event the GPU and the oracle evaluate the same samples.  At
+    # full depth the glass box's internal paths diverge under any one-ulp
+    # perturbation: the oracle against itself compiled with FMA contraction
+    # agrees on 92.9 % of the pixels at depth 8
+    # (tests/test_rounding_sensitivity.py); the GPU measured 93.4 %, so the
+    # bar is 90 % with the means and block statistics equal.
     s = vb.Scene(gpu_ctx, scenes.material_room(64, 64, max_depth=2)).build_accel()
     o = oracle.OracleScene(s)
     s.render(0, 16)
@@ -78,7 +80,7 @@ def test_matched_seed_parity_materials(vb, gpu_ctx):
     _, c64 = o.render(0, 16, fp64=True)
     c = c64[..., :3] / 16.0
     assert np.all(np.isfinite(g))
-    assert _match(g, c, 2e-3) >= 0.85
+    assert _match(g, c, 2e-3) >= 0.90
     assert abs(g.mean() - c.mean()) < 1e-2 * c.mean()
     gb = g.reshape(8, 8, 8, 8, 3).mean((1, 3))
     cb = c.reshape(8, 8, 8, 8, 3).mean((1, 3))
@@ -102,7 +104,8 @@ def test_matched_seed_parity_substrate_mirror(vb, gpu_ctx):
     _, c64 = o.render(0, 16, fp64=True)
     c = c64[..., :3] / 16.0
     assert np.all(np.isfinite(g))
-    assert _match(g, c, 2e-3) >= 0.85
+    # Measured on B200: every pixel within 2e-3 at full depth.
+    assert _match(g, c, 2e-3) >= 0.99
     assert abs(g.mean() - c.mean()) < 1e-2 * c.mean()
 
 
@@ -118,7 +121,8 @@ def test_matched_seed_parity_plastic(vb, gpu_ctx):
     o = oracle.OracleScene(s)
     s.render(0, 16)
     g, c = s.film(), o.render(0, 16)
-    assert _match(g, c, 2e-3) >= 0.85
+    # Measured on B200: every pixel within 2e-3 at full depth.
+    assert _match(g, c, 2e-3) >= 0.99
     assert abs(g[..., :3].mean() - c[..., :3].mean()) < 1e-2 * c[..., :3].mean()
 
 
@@ -194,7 +198,9 @@ def test_matched_seed_parity_environment(vb, gpu_ctx):
     g = s.film()
     c = o.render(0, 8)
     assert np.all(np.isfinite(g))
-    assert _match(g, c, 2e-3) >= 0.85
+    # Measured on B200: 99.8 % of pixels within 2e-3 (the glass tiles' paths
+    # are rounding-sensitive, tests/test_rounding_sensitivity.py).
+    assert _match(g, c, 2e-3) >= 0.98
     assert abs(g[..., :3].mean() - c[..., :3].mean()) < 1e-2 * c[..., :3].mean()
 
 
