@@ -97,6 +97,37 @@ int vs_scene_load_json(vs_context *ctx, const char *json, size_t len, const char
                        const char *table_cache, vs_scene **out);
 void vs_scene_destroy(vs_scene *scene);
 
+/* One vertex of an SDK instance (reference sdk::Vertex, src/sdk/vision.h:24-30):
+ * position, normal, uv and a second (lightmap) uv, 40 bytes. */
+typedef struct vs_vertex {
+    float pos[3];
+    float n[3];
+    float uv[2];
+    float uv2[2];
+} vs_vertex;
+
+/* Appends a mesh instance (reference VisionRenderer::add_instance with an
+ * sdk::Instance, src/sdk/vision.h:52-59,75 and vision.cpp:160-188): vert_num
+ * vertices, tri_num triangles as index triples, `mat4` the object-to-world
+ * 4x4, column-major (mat4[4c + r]; NULL = identity), and `material` the name
+ * of a material of the scene, a material node as JSON text
+ * ({"type", "name", "param"}, the reference's MaterialDesc) or NULL/"" for a
+ * default diffuse material.  The instance id goes to *instance_id (may be
+ * NULL).  The mesh is placed in world space; call vs_scene_build_accel before
+ * rendering again.  Not while a render server uses the scene. */
+int vs_scene_add_instance(vs_scene *scene, const vs_vertex *vertices, uint32_t vert_num, const uint32_t *triangles,
+                          uint32_t tri_num, const float *mat4, const char *material, uint32_t *instance_id);
+
+/* Removes every shape instance and the area lights on them; materials,
+ * point, spot and environment lights stay (reference
+ * VisionRenderer::clear_geometries, vision.cpp:120-123).  Add geometry and
+ * call vs_scene_build_accel before rendering again. */
+int vs_scene_clear_geometries(vs_scene *scene);
+
+/* Restarts the film: the next vs_render must begin at frame 0 (reference
+ * VisionRenderer::invalidation, vision.cpp:104-106). */
+int vs_scene_invalidate(vs_scene *scene);
+
 /* Builds the compressed BVH8 and uploads the scene to the device
  * (reference Geometry::build_accel, src/base/mgr/geometry.cpp:36-52;
  * SDK VisionRenderer::build_accel, src/sdk/vision.h:66-80). */

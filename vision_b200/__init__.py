@@ -93,6 +93,9 @@ def _load():
         'vs_scene_destroy': ([P], None),
         'vs_scene_build_accel': ([P], ctypes.c_int),
         'vs_set_resolution': ([P, U32, U32], ctypes.c_int),
+        'vs_scene_add_instance': ([P, P, U32, P, U32, P, ctypes.c_char_p, ctypes.POINTER(U32)], ctypes.c_int),
+        'vs_scene_clear_geometries': ([P], ctypes.c_int),
+        'vs_scene_invalidate': ([P], ctypes.c_int),
         'vs_camera_set': ([P, P, ctypes.c_float], ctypes.c_int),
         'vs_scene_info_get': ([P, ctypes.POINTER(SceneInfo)], ctypes.c_int),
         'vs_scene_export_size': ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
@@ -158,7 +161,8 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_server_result', 'vs_server_stats_get', 'vs_server_last_error', 'vs_cache_create',
                       'vs_cache_destroy', 'vs_cache_get_weights', 'vs_cache_set_weights', 'vs_cache_set_optimizer',
                       'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient', 'vs_render_cached',
-                      'vs_render_schedule_set', 'vs_cache_download', 'vs_sampler_stream'])
+                      'vs_render_schedule_set', 'vs_cache_download', 'vs_sampler_stream', 'vs_scene_add_instance',
+                      'vs_scene_clear_geometries', 'vs_scene_invalidate'])
 CACHE_PARAMS = 16576
 SCHEDULE_GRID = 0
 # Buffers of the last cache-terminated frame (include/vision_b200.h VS_CACHE_*).
@@ -295,6 +299,35 @@ class Scene:
         buf = np.zeros(max(n.value, 1), np.uint8)
         self.ctx.check(lib.vs_scene_export(self.handle, key, _ptr(buf), n.value), 'export')
         return buf[:n.value].view(dtype)
+
+    def add_instance(self, positions, triangles, normals=None, uvs=None, o2w=None, material=None):
+        """VisionRenderer::add_instance: positions (n, 3), triangles (m, 3),
+        optional normals (n, 3) and uvs (n, 2), o2w a row-major 4x4 (stored
+        column-major for the C ABI), material a name, a dict (material node)
+        or None.  Returns the instance id; build_accel must follow."""
+        p = np.asarray(positions, np.float32).reshape(-1, 3)
+        v = np.zeros((p.shape[0], 10), np.float32)
+        v[:, 0:3] = p
+        if normals is not None:
+            v[:, 3:6] = np.asarray(normals, np.float32).reshape(-1, 3)
+        if uvs is not None:
+            v[:, 6:8] = np.asarray(uvs, np.float32).reshape(-1, 2)
+        t = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+        m = None if o2w is None else np.ascontiguousarray(np.asarray(o2w, np.float32).T)
+        mat = material if material is None or isinstance(material, str) else json.dumps(material)
+        inst = ctypes.c_uint32()
+        self.ctx.check(lib.vs_scene_add_instance(self.handle, _ptr(v), p.shape[0], _ptr(t), t.shape[0], _ptr(m),
+                                                 mat.encode() if mat else None, ctypes.byref(inst)), 'add_instance')
+        self.frames = 0
+        return inst.value
+
+    def clear_geometries(self):
+        self.ctx.check(lib.vs_scene_clear_geometries(self.handle), 'clear_geometries')
+        self.frames = 0
+
+    def invalidate(self):
+        self.ctx.check(lib.vs_scene_invalidate(self.handle), 'invalidate')
+        self.frames = 0
 
     def set_resolution(self, w, h):
         self.ctx.check(lib.vs_set_resolution(self.handle, w, h), 'set_resolution')

@@ -448,6 +448,8 @@ int vs_scene_build_accel(vs_scene *s) {
     if (!s) return VS_E_INVALID;
     vs_context *ctx = s->ctx;
     std::lock_guard<std::mutex> lock(s->mu);
+    if (s->host.prim_inst.empty()) return fail(ctx, VS_E_STATE, "build_accel: the scene has no geometry");
+    if (s->host.ip.light_count == 0) return fail(ctx, VS_E_STATE, "build_accel: the scene has no lights");
     try {
         build_bvh8(s->host);
     } catch (const std::exception &e) {
@@ -458,6 +460,59 @@ int vs_scene_build_accel(vs_scene *s) {
         int rc = upload_scene(s);
         if (rc != VS_OK) return rc;
     }
+    return VS_OK;
+}
+
+int vs_scene_add_instance(vs_scene *s, const vs_vertex *vertices, uint32_t vert_num, const uint32_t *triangles,
+                          uint32_t tri_num, const float *mat4, const char *material, uint32_t *instance_id) {
+    if (!s || (vert_num && !vertices) || (tri_num && !triangles)) return fail(s ? s->ctx : nullptr, VS_E_INVALID, "null argument");
+    vs_context *ctx = s->ctx;
+    if (tri_num == 0 || vert_num == 0) return fail(ctx, VS_E_INVALID, "add_instance: empty mesh");
+    for (size_t i = 0; i < 3u * static_cast<size_t>(tri_num); ++i)
+        if (triangles[i] >= vert_num) return fail(ctx, VS_E_INVALID, "add_instance: triangle index out of range");
+    m4 o2w = m4_identity();
+    if (mat4)
+        for (int c = 0; c < 4; ++c)
+            for (int r = 0; r < 4; ++r) o2w.m[c][r] = mat4[4 * c + r];
+    std::lock_guard<std::mutex> lock(s->mu);
+    uint32_t id = 0;
+    try {
+        static_assert(sizeof(vs_vertex) == 40, "sdk::Vertex is 40 bytes");
+        id = scene_add_instance(s->host, reinterpret_cast<const float *>(vertices), vert_num, triangles, tri_num, o2w,
+                                material ? std::string(material) : std::string());
+    } catch (const std::exception &e) {
+        std::string m = e.what();
+        if (m.rfind("unsupported", 0) == 0) return fail(ctx, VS_E_UNSUPPORTED, m);
+        if (m.rfind("json", 0) == 0) return fail(ctx, VS_E_PARSE, m);
+        return fail(ctx, VS_E_INVALID, m);
+    }
+    s->built = false;
+    s->uploaded = false;
+    s->film_frames = 0;
+    s->film64_valid = false;
+    s->film64sq_valid = false;
+    if (instance_id) *instance_id = id;
+    return VS_OK;
+}
+
+int vs_scene_clear_geometries(vs_scene *s) {
+    if (!s) return VS_E_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    scene_clear_geometries(s->host);
+    s->built = false;
+    s->uploaded = false;
+    s->film_frames = 0;
+    s->film64_valid = false;
+    s->film64sq_valid = false;
+    return VS_OK;
+}
+
+int vs_scene_invalidate(vs_scene *s) {
+    if (!s) return VS_E_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->film_frames = 0;
+    s->film64_valid = false;
+    s->film64sq_valid = false;
     return VS_OK;
 }
 

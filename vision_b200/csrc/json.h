@@ -38,6 +38,11 @@ public:
         return it == obj_.end() ? null_json : it->second;
     }
     bool contains(const std::string &k) const { return kind_ == Object && obj_.count(k) != 0; }
+    // Sets (or adds) a member of an object.
+    void set(const std::string &k, Json v) {
+        if (kind_ != Object) throw std::runtime_error("json: set on a non-object");
+        obj_[k] = std::move(v);
+    }
     const std::map<std::string, Json> &items() const { return obj_; }
     const std::vector<Json> &elements() const { return arr_; }
 

@@ -22,6 +22,9 @@
 
 namespace vs {
 
+void update_env_world(HostScene &s);
+void rebuild_light_alias(HostScene &s);
+
 const Cie5 &cie5() {
     static Cie5 c = [] {
         Cie5 r{};
@@ -1185,6 +1188,87 @@ struct Loader {
 
 }  // namespace
 
+// VisionRenderer::add_instance (src/sdk/vision.cpp:160-188, from_sdk_instance:
+// vertices, triangles and the column-major o2w of an sdk::Instance) on the
+// flattened scene: the mesh goes to world space like a JSON shape's.  The
+// material is the name of a material of the scene, a material node as JSON
+// text ({"type", "name", "param"}, MaterialDesc as the reference parses it),
+// or empty for a default diffuse material.
+uint32_t scene_add_instance(HostScene &s, const float *vertices40, uint32_t vert_num, const uint32_t *triangles,
+                            uint32_t tri_num, const m4 &o2w, const std::string &material) {
+    Loader ld{s, rgb2spec_table(""), {}, ""};
+    ld.srgb = s.ip.srgb != 0u;
+    for (size_t i = 0; i < s.material_names.size(); ++i) ld.mat_by_name[s.material_names[i]] = static_cast<uint32_t>(i);
+    uint32_t mat = kInvalid;
+    if (material.empty()) {
+        auto it = ld.mat_by_name.find("__sdk_default__");
+        if (it == ld.mat_by_name.end()) {
+            ld.load_material(Json::parse("{\"type\":\"diffuse\",\"name\":\"__sdk_default__\",\"param\":{}}"));
+            it = ld.mat_by_name.find("__sdk_default__");
+        }
+        mat = it->second;
+    } else if (material[0] == '{') {
+        Json m = Json::parse(material);
+        std::string name = m["name"].as_string();
+        if (!m.is_object()) throw std::runtime_error("add_instance: material JSON must be an object");
+        if (name.empty() || ld.mat_by_name.count(name)) {
+            name = "__sdk_material_" + std::to_string(s.materials.size()) + "__";
+            m.set("name", Json::string(name));
+        }
+        ld.load_material(m);
+        mat = ld.mat_by_name[name];
+    } else {
+        auto it = ld.mat_by_name.find(material);
+        if (it == ld.mat_by_name.end()) throw std::runtime_error("add_instance: unknown material '" + material + "'");
+        mat = it->second;
+    }
+    MeshData mesh;
+    mesh.p.resize(vert_num);
+    mesh.n.resize(vert_num);
+    mesh.uv.resize(vert_num);
+    for (uint32_t i = 0; i < vert_num; ++i) {
+        const float *v = vertices40 + 10u * i;  // sdk::Vertex: pos[3], n[3], uv[2], uv2[2]
+        mesh.p[i] = {v[0], v[1], v[2]};
+        mesh.n[i] = {v[3], v[4], v[5]};
+        mesh.uv[i] = {v[6], v[7]};
+    }
+    mesh.idx.assign(triangles, triangles + 3u * static_cast<size_t>(tri_num));
+    const uint32_t inst = static_cast<uint32_t>(s.instances.size());
+    ld.add_mesh(mesh, o2w, mat, "__sdk_instance_" + std::to_string(inst) + "__", nullptr);
+    update_env_world(s);
+    rebuild_light_alias(s);
+    return inst;
+}
+
+// Pipeline::clear_geometry as the SDK's clear_geometries calls it
+// (src/sdk/vision.cpp:120-123): every shape instance and the area lights they
+// carry go; point, spot and environment lights stay, as do the materials.
+void scene_clear_geometries(HostScene &s) {
+    s.pos.clear();
+    s.nrm.clear();
+    s.uv.clear();
+    s.idx.clear();
+    s.prim_inst.clear();
+    s.instances.clear();
+    s.instance_names.clear();
+    std::vector<AreaLight> keep;
+    std::vector<f3> keep_rgb;
+    for (size_t i = 0; i < s.lights.size(); ++i)
+        if (s.lights[i].shape != kLightArea) {
+            keep.push_back(s.lights[i]);
+            keep_rgb.push_back(s.light_rgb[i]);
+        }
+    s.lights = keep;
+    s.light_rgb = keep_rgb;
+    s.prim_alias.clear();
+    s.prim_pmf.clear();
+    s.nodes.clear();
+    s.tri_v.clear();
+    s.bvh_depth = 0;
+    update_env_world(s);
+    rebuild_light_alias(s);
+}
+
 void update_camera(HostScene &s, uint32_t width, uint32_t height) { s.cam = camera_at_resolution(s.cam, width, height); }
 
 Camera camera_at_resolution(const Camera &base, uint32_t width, uint32_t height) {
@@ -1252,20 +1336,38 @@ static void load_spherical(const Json &p, const Json &root, HostScene &s) {
     std::vector<float> mpmf;
     build_alias(marginal_func, s.env_marginal, mpmf, &e.integral);
     s.env_marginal_func = marginal_func;
+    s.min_world_radius = root["render_setting"]["min_world_radius"].as_float(10.0f);
+    double n = static_cast<double>(W) * H;
+    s.env_avg = make3(float(avg[0] / n), float(avg[1] / n), float(avg[2] / n)) * e.scale;
+    s.has_env = true;
+    update_env_world(s);
+}
+
+void update_env_world(HostScene &s) {
+    if (!s.has_env) return;
+    EnvLight &e = s.env;
     // World bounds (Scene::world_radius: max(aabb radius, min_world_radius)).
     f3 lo = make3(3.4e38f), hi = make3(-3.4e38f);
     for (const f3 &q : s.pos) {
         lo = vmin(lo, q);
         hi = vmax(hi, q);
     }
-    float min_radius = root["render_setting"]["min_world_radius"].as_float(10.0f);
-    float radius = std::max(0.5f * length(hi - lo), min_radius);
+    float radius = s.pos.empty() ? s.min_world_radius : std::max(0.5f * length(hi - lo), s.min_world_radius);
     e.world_diameter = 2.0f * radius;
     // SphericalMap::power (spherical.cpp:58-61).
-    double n = static_cast<double>(W) * H;
-    f3 a = make3(float(avg[0] / n), float(avg[1] / n), float(avg[2] / n)) * e.scale;
-    e.lum_power = linear_srgb_to_y(a * (kPi * radius * radius));
-    s.has_env = true;
+    e.lum_power = linear_srgb_to_y(s.env_avg * (kPi * radius * radius));
+}
+
+// LightSampler::prepare with PowerLightSampler weights (power.cpp:16-30):
+// one alias table over the lights' luminance powers, the environment last.
+void rebuild_light_alias(HostScene &s) {
+    std::vector<float> w;
+    for (const AreaLight &L : s.lights) w.push_back(L.lum_power);
+    if (s.has_env) w.push_back(s.env.lum_power);
+    s.ip.light_count = static_cast<uint32_t>(w.size());
+    s.light_alias.clear();
+    s.light_pmf.clear();
+    if (!w.empty()) build_alias(w, s.light_alias, s.light_pmf);
 }
 
 namespace {
@@ -1365,12 +1467,7 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     }
     s.ip.light_count = static_cast<uint32_t>(s.lights.size()) + (s.has_env ? 1u : 0u);
     if (s.ip.light_count == 0) throw unsupported("scene without lights");
-    {
-        std::vector<float> w;
-        for (const AreaLight &L : s.lights) w.push_back(L.lum_power);
-        if (s.has_env) w.push_back(s.env.lum_power);
-        build_alias(w, s.light_alias, s.light_pmf);
-    }
+    rebuild_light_alias(s);
     // Integrator (IlluminationIntegrator ctor, integrator.cpp:60-67).
     const Json &ij = root["integrator"];
     std::string it = ij["type"].as_string("pt");

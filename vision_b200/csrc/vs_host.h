@@ -43,6 +43,8 @@ struct HostScene {
     std::vector<float> env_tex;  // 4 floats (RGB, 0) per texel, row-major from the zenith
     std::vector<AliasEntry> env_marginal, env_cond;
     std::vector<float> env_marginal_func, env_cond_func;
+    f3 env_avg{};                  // average texel colour times the light's scale
+    float min_world_radius = 10.0f; // render_setting.min_world_radius
     // Tabulated pixel filter (DeviceScene::filter_tab layout); empty for box
     // and triangle.
     std::vector<float> filter_tab;
@@ -70,6 +72,20 @@ struct HostScene {
 // message naming the offending key or plugin type.
 void load_scene_json(const std::string &text, const std::string &base_dir, const std::string &table_cache,
                      HostScene &scene);
+
+// SDK geometry edits (src/sdk/vision.h:66-80): append a mesh instance
+// (sdk::Vertex records of 10 floats, triangles as index triples, a column-major
+// object-to-world matrix, a material name, JSON material node or "") and return
+// its instance id; remove every shape instance and its area light.  Both keep
+// the light sampler's tables and the environment's world bounds current; the
+// scene needs build_bvh8 (vs_scene_build_accel) afterwards.
+uint32_t scene_add_instance(HostScene &scene, const float *vertices40, uint32_t vert_num, const uint32_t *triangles,
+                            uint32_t tri_num, const m4 &o2w, const std::string &material);
+void scene_clear_geometries(HostScene &scene);
+// Environment world diameter and power from the current geometry bounds;
+// light-sampler alias table from the current lights.
+void update_env_world(HostScene &scene);
+void rebuild_light_alias(HostScene &scene);
 
 // Sets resolution / camera-derived fields after load or on update.
 void update_camera(HostScene &scene, uint32_t width, uint32_t height);
