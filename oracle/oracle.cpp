@@ -872,7 +872,8 @@ static LS sample_light(const Scene &sc, const It &it, float ul, float ux, float 
 // Materials: diffuse (diffuse.cpp), black_body (black_body.cpp), metal
 // (metal.cpp + ConductorLobe/PureReflectionLobe, lobe.cpp:716-735), glass
 // (glass.cpp + DielectricLobe, lobe.cpp:253-450), principled_bsdf
-// (principled_bsdf.cpp:352-461, with zero sheen/coat/transmission weights).
+// (principled_bsdf.cpp:352-461: sheen LTC, coat, metallic F82, transmission,
+// Schlick specular, diffuse).
 // Everything is evaluated in world space through per-lobe local frames the way
 // MaterialEvaluator::evaluate/sample do with individual shading normals
 // (material.cpp:132-184).
@@ -973,6 +974,7 @@ static float fr_conductor(float c, float eta, float k) {
 }  // namespace mf
 
 #include "../vision_b200/csrc/data/albedo_luts.inc"
+#include "../vision_b200/csrc/data/principled_luts.inc"
 
 // MaterialLut::sample: normalised coordinates, linear filter, clamp to edge.
 static float lut_axis(float u, int &i0, int &i1) {
@@ -1001,10 +1003,21 @@ static float lut3(const float *t, int ch, float u, float v, float w) {
     float c0 = c00 + fy * (c10 - c00), c1 = c01 + fy * (c11 - c01);
     return c0 + fz * (c1 - c0);
 }
+// 2D table with `ch` channels per texel, index [y][x][c].
+static float lut2c(const float *t, int ch, int c, float u, float v) {
+    int x0, x1, y0, y1;
+    float fx = lut_axis(u, x0, x1), fy = lut_axis(v, y0, y1);
+    auto at = [&](int x, int y) { return t[(y * 32 + x) * ch + c]; };
+    float a = at(x0, y0) + fx * (at(x1, y0) - at(x0, y0));
+    float b = at(x0, y1) + fx * (at(x1, y1) - at(x0, y1));
+    return a + fy * (b - a);
+}
 static const float *kLutPure = VS_ALBEDO_LUTS;
 static const float *kLutDiel = VS_ALBEDO_LUTS + 1024;
 static const float *kLutDielInv = VS_ALBEDO_LUTS + 1024 + 65536;
 static const float *kLutSpec = VS_ALBEDO_LUTS + 1024 + 131072;
+static const float *kLutCoat = VS_COAT_LUT;     // CoatLobe albedo (precomputed_table.h)
+static const float *kLutSheen = VS_SHEEN_LTC;   // SheenLTC Approximate fits (ltc_sheen_table.h)
 
 struct Eval {
     float f[8];
@@ -1014,21 +1027,25 @@ struct Eval {
 
 // A lobe of the material's lobe set.
 struct Lobe {
-    enum Kind { Lambert, MicrofacetRefl, Dielectric, NoScatter, Substrate, Plastic } kind;
-    enum Fr { Conductor, Schlick, F82, One } fresnel = One;
+    enum Kind { Lambert, MicrofacetRefl, Dielectric, NoScatter, Substrate, Plastic, Sheen } kind;
+    // Fresnel of a microfacet lobe; a Dielectric lobe uses Schlick (F0 in fa,
+    // eta[0]) or, by default, the dielectric Fresnel at each eta[i].
+    enum Fr { Conductor, Schlick, F82, One, DielectricFr } fresnel = One;
     float ax = 1, ay = 1;
     bool compensate = false;
     float kr[8], fa[8], fb[8];
     float eta0 = 1.0f;
     float eta[8];
     float sample_weight = 1.0f;
+    float weight = 1.0f;               // WeightedLobe::weight: scales f in the lobe set
+    float ltc_a = 1.0f, ltc_b = 0.0f;  // Sheen: the LTC matrix entries
 };
 
 struct Bsdf {
     int n = 1;
     Frame fr;
     V3 ng;
-    Lobe lobes[3];
+    Lobe lobes[6];
     int count = 0;
     bool lobe_set = false;  // LobeSet: world-space hemisphere factors and a 1D lobe choice
     bool dispersive = false;
@@ -1047,10 +1064,26 @@ static void fresnel_eval(const Lobe &l, int n, float c, float *F) {
             float mu5 = mu * mu * mu * mu * mu;
             float fs = l.fa[i] + mu5 * (1.0f - l.fa[i]);
             F[i] = std::min(std::max(fs - l.fb[i] * c * mu5 * mu, 0.0f), 1.0f);
+        } else if (l.fresnel == Lobe::DielectricFr) {
+            F[i] = mf::fr_dielectric(c, l.eta0);  // FresnelDielectric (fresnel.h:74-90)
         } else {
             F[i] = 1.0f;
         }
     }
+}
+
+// Fresnel of a dielectric lobe: per-wavelength dielectric (glass), or
+// FresnelSchlick (fresnel.h:60-67) with F0 = fa and eta[0] (the principled
+// transmission lobe).
+static void diel_fresnel(const Lobe &l, int n, float c, float *F) {
+    if (l.fresnel == Lobe::Schlick) {
+        float fr = mf::fr_dielectric(c, l.eta[0]);
+        float f0 = ((l.eta[0] - 1.0f) / (l.eta[0] + 1.0f)) * ((l.eta[0] - 1.0f) / (l.eta[0] + 1.0f));
+        float t = std::min(std::max((fr - f0) / (1.0f - f0), 0.0f), 1.0f);
+        for (int i = 0; i < n; ++i) F[i] = l.fa[i] + t * (1.0f - l.fa[i]);
+        return;
+    }
+    for (int i = 0; i < n; ++i) F[i] = mf::fr_dielectric(c, l.eta[i]);
 }
 
 // Local evaluation of one lobe: f (without the cosine), pdf, flags.
@@ -1111,6 +1144,18 @@ static void lobe_eval(const Lobe &l, int n, V3 wo, V3 wi, float *f, float &pdf, 
         float fr = mf::fr_dielectric(co, 1.5f);
         float pd = ci * kInvPi;
         pdf = pd + fr * (mf::pdf_refl(wo, h, l.ax, l.ay) - pd);
+    } else if (l.kind == Lobe::Sheen) {
+        // SheenLTC::evaluate_local_impl (principled_bsdf.cpp:61-75):
+        // eval_ltc(wi) = cosine pdf of M^-1 wi / |M^-1 wi| times a^2 / |M^-1 wi|^3.
+        flags = kGlossyRefl;
+        V3 w = {l.ltc_a * wi.x + l.ltc_b * wi.z, l.ltc_a * wi.y, wi.z};
+        float L = len(w);
+        w = {w.x / L, w.y / L, w.z / L};
+        float jac = (l.ltc_a * l.ltc_a) / (L * L * L);
+        float ltc = w.z * kInvPi * jac;
+        bool below = wi.z < 0.0f || wo.z < 0.0f;
+        for (int i = 0; i < n; ++i) f[i] = below ? 0.0f : (ltc * l.kr[i]) / wi.z;
+        pdf = ltc;
     } else if (l.kind == Lobe::Dielectric) {
         bool refl = wo.z * wi.z > 0.0f;
         float e0 = l.eta[0];
@@ -1119,7 +1164,7 @@ static void lobe_eval(const Lobe &l, int n, V3 wo, V3 wi, float *f, float &pdf, 
         V3 h = normalize(add(wo, mul(wi, ep)));
         if (dot(h, wo) < 0.0f) h = neg(h);
         float F[8], T[8];
-        for (int i = 0; i < n; ++i) F[i] = mf::fr_dielectric(std::fabs(dot(h, wo)), l.eta[i]);
+        diel_fresnel(l, n, std::fabs(dot(h, wo)), F);
         float sf = 0, st = 0;
         for (int i = 0; i < n; ++i) {
             sf += F[i];
@@ -1172,7 +1217,7 @@ static Eval bsdf_eval(const Bsdf &b, V3 wo_w, V3 wi_w, float *eta_out) {
             float et;
             lobe_eval(l, b.n, wo, wi, f, p, fl, et);
             float factor = (l.kind == Lobe::Dielectric || same) ? 1.0f : 0.0f;
-            for (int i = 0; i < b.n; ++i) e.f[i] += f[i] * ac * factor;
+            for (int i = 0; i < b.n; ++i) e.f[i] += (f[i] * ac) * (l.weight * factor);
             e.pdf += p * l.sample_weight * factor;
             e.flags |= fl;
             if (l.kind == Lobe::Dielectric) eta = et;
@@ -1233,12 +1278,21 @@ static V3 lobe_sample(const Lobe &l, int n, V3 wo, Sampler &smp, bool &valid) {
         float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
         return {dx, dy, wo.z < 0.0f ? -z : z};
     }
+    if (l.kind == Lobe::Sheen) {
+        // SheenLTC::sample_wi_local_impl (principled_bsdf.cpp:101-110): a
+        // cosine-hemisphere direction through M, normalised.
+        float u0 = smp.next(), u1 = smp.next();
+        float r = std::sqrt(u0), th = 2.0f * kPi * u1;
+        float dx = r * std::cos(th), dy = r * std::sin(th);
+        float z = std::sqrt(std::max(0.0f, 1.0f - dx * dx - dy * dy));
+        return normalize({dx / l.ltc_a - z * l.ltc_b / l.ltc_a, dy / l.ltc_a, z});
+    }
     // Dielectric: microfacet normal (2D), then reflect/refract choice (1D).
     float u0 = smp.next(), u1 = smp.next();
     V3 h = mf::sample_wh(wo, u0, u1, l.ax, l.ay);
     float F[8], sf = 0, st = 0;
+    diel_fresnel(l, n, std::fabs(dot(wo, h)), F);
     for (int i = 0; i < n; ++i) {
-        F[i] = mf::fr_dielectric(std::fabs(dot(wo, h)), l.eta[i]);
         sf += F[i];
         st += (1.0f - F[i]) * l.kr[i] + F[i];
     }
@@ -1349,7 +1403,10 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
             float ior = m.spd0 != kInvalid ? spd_of(sc.s->spd, m.spd0, is_rgb(w) ? -w.lambda[0] : w.lambda[i]) : m.p[2];
             l0.eta[i] = front ? ior : 1.0f / ior;
         }
-    } else if (m.type == 4) {  // principled_bsdf: metallic, specular, diffuse
+    } else if (m.type == 4) {
+        // PrincipledBSDF::create_lobe_set (principled_bsdf.cpp:352-461): sheen,
+        // coat, metallic, transmission, specular, diffuse, each layer's albedo
+        // taking its share of the remaining weight (layering_weight, :209-214).
         b.lobe_set = true;
         int n = w.n;
         float ax = m.p[0], ay = m.p[1], metallic = m.p[2], ior = m.p[3];
@@ -1367,6 +1424,51 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
             for (int i = 0; i < n; ++i) a += v[i];
             return a * (1.0f / n);
         };
+        auto layering = [&](const float *albedo) {
+            float mx = -FLT_MAX;
+            for (int i = 0; i < n; ++i) mx = std::max(mx, weight[i] == 0.0f ? 0.0f : albedo[i] / weight[i]);
+            float lw = std::min(std::max(1.0f - mx, 0.0f), 1.0f);
+            for (int i = 0; i < n; ++i) weight[i] = weight[i] * lw;
+        };
+        // Sheen / coat / transmission parameters: a 12-float SPD-table block.
+        const float *xp = m.spd0 != kInvalid ? sc.s->spd + m.spd0 + 1 : nullptr;
+        Lobe sheen, coat, trans;
+        sheen.kind = Lobe::Sheen;
+        sheen.sample_weight = 0.0f;
+        coat.kind = Lobe::MicrofacetRefl;
+        coat.sample_weight = 0.0f;
+        trans.kind = Lobe::Dielectric;
+        trans.sample_weight = 0.0f;
+        if (xp && xp[0] != 0.0f) {
+            // SheenLTC with the Approximate fits at (cos theta, roughness).
+            float sw = xp[0] * front;
+            float c0 = lut2c(kLutSheen, 4, 0, cos_theta, xp[1]);
+            float c1 = lut2c(kLutSheen, 4, 1, cos_theta, xp[1]);
+            float c2 = lut2c(kLutSheen, 4, 2, cos_theta, xp[1]);
+            sheen.ltc_a = c0;
+            sheen.ltc_b = c1;
+            for (int i = 0; i < n; ++i) sheen.kr[i] = alb(xp + 2, w, i) * sw * weight[i] * c2;
+            sheen.sample_weight = mean(sheen.kr);
+            layering(sheen.kr);
+        }
+        if (xp && xp[5] != 0.0f) {
+            // CoatLobe: dielectric Fresnel (coat ior), alpha = roughness^2,
+            // albedo = CoatLobe table (sqrt(alpha), cos theta, ior ratio) * kr.
+            float cw = xp[5] * front;
+            float cr = std::min(std::max(xp[6], 0.0001f), 1.0f);
+            cr = cr * cr;
+            coat.fresnel = Lobe::DielectricFr;
+            coat.ax = coat.ay = cr;
+            coat.eta0 = xp[7];
+            float s3 = lut3(kLutCoat, 1, std::sqrt(std::sqrt(cr * cr)), cos_theta, (xp[7] - 1.003f) / (4.0f - 1.003f));
+            float ca[8];
+            for (int i = 0; i < n; ++i) {
+                coat.kr[i] = cw * weight[i] * alb(xp + 8, w, i);
+                ca[i] = s3 * coat.kr[i];
+            }
+            coat.sample_weight = mean(ca);
+            layering(ca);
+        }
         Lobe met;
         met.kind = Lobe::MicrofacetRefl;
         met.fresnel = Lobe::F82;
@@ -1383,31 +1485,51 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         }
         met.sample_weight = mm * mean(weight);
         for (int i = 0; i < n; ++i) weight[i] *= (1.0f - mm);
+        if (xp && xp[11] != 0.0f) {
+            // Transmission: compensated DielectricLobe with FresnelSchlick
+            // (F0 = schlick_F0(eta) * tint, eta = correct_eta(ior)), kt =
+            // colour; f and sampling weighted by mean(transmission * weight).
+            float tw = xp[11];
+            float eta = cos_theta > 0.0f ? ior : 1.0f / ior;
+            float f0 = ((eta - 1.0f) / (eta + 1.0f)) * ((eta - 1.0f) / (eta + 1.0f));
+            trans.fresnel = Lobe::Schlick;
+            trans.ax = ax;
+            trans.ay = ay;
+            float t_w[8];
+            for (int i = 0; i < n; ++i) {
+                trans.kr[i] = color[i];
+                trans.eta[i] = eta;
+                trans.fa[i] = tint[i] * f0;
+                t_w[i] = weight[i] * tw;
+            }
+            trans.sample_weight = mean(t_w);
+            trans.weight = trans.sample_weight;
+            for (int i = 0; i < n; ++i) weight[i] *= (1.0f - tw);
+        }
         Lobe spec;
         spec.kind = Lobe::MicrofacetRefl;
         spec.fresnel = Lobe::Schlick;
         spec.ax = ax;
         spec.ay = ay;
         spec.eta0 = ior;
-        float f0 = ((ior - 1.0f) / (ior + 1.0f)) * ((ior - 1.0f) / (ior + 1.0f));
+        float f0s = ((ior - 1.0f) / (ior + 1.0f)) * ((ior - 1.0f) / (ior + 1.0f));
         float sl = lut3(kLutSpec, 1, std::sqrt(std::sqrt(ax * ay)), cos_theta, std::sqrt(std::fabs((ior - 1.0f) / (ior + 1.0f))));
-        float alb[8];
-        float mx = -FLT_MAX;
+        float alb_s[8];
         for (int i = 0; i < n; ++i) {
             spec.kr[i] = weight[i];
-            spec.fa[i] = f0 * tint[i];
-            alb[i] = (spec.fa[i] + sl * (1.0f - spec.fa[i])) * weight[i];
-            mx = std::max(mx, weight[i] == 0.0f ? 0.0f : alb[i] / weight[i]);
+            spec.fa[i] = f0s * tint[i];
+            alb_s[i] = (spec.fa[i] + sl * (1.0f - spec.fa[i])) * weight[i];
         }
-        spec.sample_weight = mean(alb);
-        float lw = std::min(std::max(1.0f - mx, 0.0f), 1.0f);
+        spec.sample_weight = mean(alb_s);
+        layering(alb_s);
         Lobe dif;
         dif.kind = Lobe::Lambert;
-        for (int i = 0; i < n; ++i) dif.kr[i] = color[i] * (weight[i] * lw) * front;
+        for (int i = 0; i < n; ++i) dif.kr[i] = color[i] * weight[i] * front;
         dif.sample_weight = mean(dif.kr);
-        float sum = met.sample_weight + spec.sample_weight + dif.sample_weight;
+        float sum = sheen.sample_weight + coat.sample_weight + met.sample_weight + trans.sample_weight +
+                    spec.sample_weight + dif.sample_weight;
         b.count = 0;
-        for (Lobe *l : {&met, &spec, &dif}) {
+        for (Lobe *l : {&sheen, &coat, &met, &trans, &spec, &dif}) {
             if (!(l->sample_weight > 0.0f)) continue;
             l->sample_weight /= sum;
             b.lobes[b.count++] = *l;

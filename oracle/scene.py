@@ -713,9 +713,18 @@ class _Builder:
             r['p'][2] = _slot_scalar(p.get('metallic'), 0.0)
             r['p'][3] = _slot_scalar(p.get('ior'), 1.5)
             r['p'][4:7] = self.colour(_slot_rgb(p.get('spec_tint'), 1.0))[:3]
-            for key in ('sheen_weight', 'coat_weight', 'transmission_weight'):
-                if _slot_scalar(p.get(key), 0.0) != 0.0:
-                    raise Unsupported('principled_bsdf ' + key)
+            # Sheen, coat and transmission layers (initialize_slots,
+            # principled_bsdf.cpp:287-302) as a 12-float block of the SPD
+            # table when any of their weights is non-zero.
+            sw, cw, tw = (_slot_scalar(p.get(k), 0.0) for k in ('sheen_weight', 'coat_weight',
+                                                                 'transmission_weight'))
+            if sw != 0.0 or cw != 0.0 or tw != 0.0:
+                block = [sw, _slot_scalar(p.get('sheen_roughness'), 0.5)]
+                block += list(self.colour(_slot_rgb(p.get('sheen_tint'), 1.0))[:3])
+                block += [cw, _slot_scalar(p.get('coat_roughness'), 0.2), _slot_scalar(p.get('coat_ior'), 1.5)]
+                block += list(self.colour(_slot_rgb(p.get('coat_tint'), 1.0))[:3])
+                block += [tw]
+                r['spd0'] = self.add_spd(np.array(block, np.float32))
             self.needs_luts = True
         elif t in ('substrate', 'plastic'):
             r['type'] = SUBSTRATE

@@ -109,6 +109,31 @@ def test_matched_seed_parity_substrate_mirror(vb, gpu_ctx):
     assert abs(g.mean() - c.mean()) < 1e-2 * c.mean()
 
 
+def test_matched_seed_parity_principled_layers(vb, gpu_ctx):
+    # PrincipledBSDF with sheen (LTC), coat, metallic, transmission, specular
+    # and diffuse lobes (principled_bsdf.cpp:352-461).  One scattering event
+    # agrees per pixel; at full depth the transmissive box is
+    # rounding-sensitive like the glass, so the bar is statistical.
+    from helpers import mean_z, path_sums, pixel_z
+    s = vb.Scene(gpu_ctx, scenes.principled_room(64, 64, max_depth=2)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 1e-3) >= 0.99
+    s = vb.Scene(gpu_ctx, scenes.principled_room(48, 48)).build_accel()
+    o = oracle.OracleScene.from_json(scenes.principled_room(48, 48))
+    s.render(0, 32, fp64=True)
+    gs, gq = s.film(vb.FILM_SUM64)[..., :3], s.film(vb.FILM_SUMSQ64)[..., :3]
+    cs, cq = path_sums(o.paths(np.arange(48 * 48, dtype=np.uint32), 0, 32))
+    cs, cq = cs.reshape(48, 48, 3), cq.reshape(48, 48, 3)
+    assert np.all(np.isfinite(gs))
+    z = pixel_z(gs, gq, 32, cs, cq, 32)
+    assert (np.abs(z) > 4.0).mean() <= 0.005
+    assert abs(mean_z(gs, gq, 32, cs, cq, 32)) < 4.0
+    assert _match(gs / 32, cs / 32, 2e-3) >= 0.85
+
+
 def test_matched_seed_parity_plastic(vb, gpu_ctx):
     # PlasticLobe: Lambert (1 - F) plus Schlick-weighted GGX reflection.
     s = vb.Scene(gpu_ctx, scenes.plastic_room(64, 64, max_depth=2)).build_accel()
@@ -217,7 +242,7 @@ def test_large_scene_closest_hit_bit_exact(vb, gpu_ctx):
 
 
 @pytest.mark.parametrize('case', ['box_room', 'materials', 'substrate', 'plastic', 'point_lights', 'srgb',
-                                  'environment', 'dimension1', 'two_waves'])
+                                  'environment', 'dimension1', 'two_waves', 'principled'])
 def test_schedules_give_the_same_film(vb, gpu_ctx, case):
     # Path regeneration only changes which thread traces which path, and the
     # wavefront form only where a path's state lives between bounces: each
@@ -238,6 +263,8 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
         sc.pop('spectrum')
     elif case == 'environment':
         sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
+    elif case == 'principled':
+        sc = scenes.principled_room(37, 35)
     elif case == 'dimension1':
         sc = scenes.box_room(width=33, height=31, dimension=1)
     else:

@@ -68,14 +68,25 @@ def test_metal_glass_principled_records(vb, host_ctx):
     assert abs(pr[8] - 0.35 ** 2) < 1e-6 and abs(pr[10] - 0.4) < 1e-7 and abs(pr[11] - 1.5) < 1e-7
 
 
-def test_principled_nonzero_coat_is_unsupported(vb, host_ctx):
-    sc = scenes.material_room(8, 8)
-    for m in sc['materials']:
-        if m['type'] == 'principled_bsdf':
-            m['param']['coat_weight'] = 0.5
-    with pytest.raises(vb.UnsupportedError) as e:
-        vb.Scene(host_ctx, sc)
-    assert 'coat_weight' in str(e.value)
+def test_principled_layers_are_recorded(vb, host_ctx):
+    # Sheen, coat and transmission parameters (principled_bsdf.cpp:287-302)
+    # go to a 12-float block of the SPD table; a principled material without
+    # them keeps spd0 unset.
+    sc = scenes.principled_room(8, 8)
+    s = vb.Scene(host_ctx, sc)
+    mats = s.export('materials', np.uint32).reshape(-1, 16)
+    names = [m['name'] for m in sc['materials']]
+    spd = s.export('spd', np.float32)
+    tall = mats[names.index('TallBox')]
+    assert tall[0] == 4 and tall[2] != 0xffffffff
+    blk = spd[tall[2]:tall[2] + 13]
+    assert blk[0] == 12
+    np.testing.assert_allclose(blk[[1, 2, 6, 7, 8, 12]], [0.8, 0.4, 0.7, 0.15, 1.6, 0.0], rtol=1e-7)
+    short = mats[names.index('ShortBox')]
+    blk = spd[short[2]:short[2] + 13]
+    np.testing.assert_allclose(blk[[1, 2, 6, 7, 8, 12]], [0.0, 0.5, 0.3, 0.1, 1.5, 0.8], rtol=1e-7)
+    plain = vb.Scene(host_ctx, scenes.material_room(8, 8)).export('materials', np.uint32).reshape(-1, 16)
+    assert plain[[m['name'] for m in scenes.material_room(8, 8)['materials']].index('Floor')][2] == 0xffffffff
 
 
 def test_metal_names(vb, host_ctx):

@@ -333,6 +333,8 @@ int upload_scene(vs_scene *s) {
     if (h.needs_luts) {
         const float *t = microfacet_luts();
         luts.assign(t, t + kLutFloats);
+        luts.insert(luts.end(), coat_lut(), coat_lut() + (kLutSheen - kLutCoat));
+        luts.insert(luts.end(), sheen_ltc_lut(), sheen_ltc_lut() + (kLutDeviceFloats - kLutSheen));
     }
     VS_CUDA(s->luts.upload(luts), "upload luts");
     if (h.has_env) {

@@ -17,6 +17,7 @@
 #include "vs_lut_samples.h"
 
 #include "data/albedo_luts.inc"
+#include "data/principled_luts.inc"
 
 #include <atomic>
 #include <fstream>
@@ -58,6 +59,8 @@ std::vector<float> g_luts;
 }  // namespace
 
 const float *microfacet_luts() { return VS_ALBEDO_LUTS; }
+const float *coat_lut() { return VS_COAT_LUT; }
+const float *sheen_ltc_lut() { return VS_SHEEN_LTC; }
 
 const float *regenerate_microfacet_luts(const std::string &cache_path) {
     std::lock_guard<std::mutex> lock(g_mutex);

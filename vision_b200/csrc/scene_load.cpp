@@ -927,9 +927,23 @@ struct Loader {
             float tin[3] = {tint.x, tint.y, tint.z}, tc[4];
             albedo_coef(tin, tc);
             mat.p[4] = tc[0]; mat.p[5] = tc[1]; mat.p[6] = tc[2];
-            for (const char *key : {"sheen_weight", "coat_weight", "transmission_weight"}) {
-                if (slot_scalar(p[key], 0.0f) != 0.0f)
-                    throw unsupported(std::string("principled_bsdf ") + key + " > 0 (" + name + ")");
+            // Sheen, coat and transmission layers (initialize_slots,
+            // principled_bsdf.cpp:287-302): when any weight is non-zero their
+            // parameters go to a 12-float block of the SPD table at spd0:
+            // sheen weight, roughness, tint (3 coefficients); coat weight,
+            // roughness, ior, tint (3 coefficients); transmission weight.
+            const float sheen_w = slot_scalar(p["sheen_weight"], 0.0f);
+            const float coat_w = slot_scalar(p["coat_weight"], 0.0f);
+            const float trans_w = slot_scalar(p["transmission_weight"], 0.0f);
+            if (sheen_w != 0.0f || coat_w != 0.0f || trans_w != 0.0f) {
+                f3 st = slot_rgb(p["sheen_tint"], make3(1.0f)), ct = slot_rgb(p["coat_tint"], make3(1.0f));
+                float sin3[3] = {st.x, st.y, st.z}, cin3[3] = {ct.x, ct.y, ct.z}, sc[4], cc[4];
+                albedo_coef(sin3, sc);
+                albedo_coef(cin3, cc);
+                const float block[12] = {sheen_w, slot_scalar(p["sheen_roughness"], 0.5f), sc[0], sc[1], sc[2],
+                                         coat_w, slot_scalar(p["coat_roughness"], 0.2f),
+                                         slot_scalar(p["coat_ior"], 1.5f), cc[0], cc[1], cc[2], trans_w};
+                mat.spd0 = add_spd(block, 12);
             }
             s.needs_luts = true;
         } else if (type == "mirror") {

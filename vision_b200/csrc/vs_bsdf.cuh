@@ -8,9 +8,9 @@
 // Materials: diffuse (diffuse.cpp), black_body (black_body.cpp), metal
 // (metal.cpp: GGX conductor with complex Fresnel and albedo compensation),
 // glass (glass.cpp: rough dielectric, optionally dispersive, compensated) and
-// principled_bsdf (principled_bsdf.cpp: metallic F82 + Schlick specular +
-// diffuse; the scene loader rejects non-zero sheen, coat and transmission
-// weights, whose lobes are otherwise inert).
+// principled_bsdf (principled_bsdf.cpp: the lobe set sheen (LTC), coat,
+// metallic F82, transmission, Schlick specular and diffuse, layered by
+// albedo).
 #pragma once
 
 #include "vs_device.cuh"
@@ -73,7 +73,8 @@ __device__ __forceinline__ float avg(const Spec<N> &s) {
 }
 
 // Fresnel variants of the microfacet lobes (src/base/scattering/fresnel.h).
-enum FresnelKind : uint32_t { kFresnelConductor = 0, kFresnelSchlick = 1, kFresnelF82 = 2, kFresnelConstant = 3 };
+enum FresnelKind : uint32_t { kFresnelConductor = 0, kFresnelSchlick = 1, kFresnelF82 = 2, kFresnelConstant = 3,
+                               kFresnelDielectric = 4 };
 
 // One microfacet reflection lobe: MicrofacetReflection + Fresnel, with the
 // PureReflectionLobe albedo compensation when `compensate` is set.
@@ -108,6 +109,11 @@ struct MfLobe {
                 float fs = fa.v[i] + mu5 * (1.0f - fa.v[i]);
                 r.v[i] = clampf(fs - fb.v[i] * c * mu5 * mu, 0.0f, 1.0f);
             }
+        } else if (fresnel == kFresnelDielectric) {
+            // FresnelDielectric (fresnel.h:74-90) with one eta for every channel.
+            const float fr = fresnel_dielectric(c, eta0);
+#pragma unroll
+            for (int i = 0; i < N; ++i) r.v[i] = fr;
         } else {
             r = Spec<N>::fill(1.0f);
         }
@@ -148,9 +154,22 @@ struct DielLobe {
     Spec<N> eta;  // per wavelength, already corrected for the side (Interaction::correct_eta)
     Spec<N> kt;
     bool compensate;
+    // Fresnel: dielectric per wavelength (glass), or FresnelSchlick with F0
+    // per channel and eta[0] (the principled transmission lobe).
+    bool schlick;
+    Spec<N> f0;
 
     __device__ __forceinline__ Spec<N> F(float c) const {
         Spec<N> r;
+        if (schlick) {
+            // FresnelSchlick::evaluate (fresnel.h:60-67).
+            const float f_real = fresnel_dielectric(c, eta.v[0]);
+            const float f0_real = schlick_F0_from_ior(eta.v[0]);
+            const float t = clampf((f_real - f0_real) / (1.0f - f0_real), 0.0f, 1.0f);
+#pragma unroll
+            for (int i = 0; i < N; ++i) r.v[i] = f0.v[i] + t * (1.0f - f0.v[i]);
+            return r;
+        }
 #pragma unroll
         for (int i = 0; i < N; ++i) r.v[i] = fresnel_dielectric(c, eta.v[i]);
         return r;
@@ -213,6 +232,35 @@ struct DielLobe {
     }
 };
 
+// SheenLTC (principled_bsdf.cpp:17-118, Zeltner et al. 2022): a linearly
+// transformed cosine lobe whose (a, b) and albedo scale come from the fitted
+// table at (cos theta of wo against the geometric normal, sheen roughness).
+template <int N>
+struct SheenLobe {
+    float a, b;
+    Spec<N> tint;  // sheen tint * weight * layer weight * the table's scale
+    // eval_ltc: the cosine density of M^-1 wi times the Jacobian a^2 / |M^-1 wi|^3.
+    __device__ __forceinline__ float eval_ltc(f3 wi) const {
+        f3 w = make3(a * wi.x + b * wi.z, a * wi.y, wi.z);
+        const float len = length(w);
+        w = make3(w.x / len, w.y / len, w.z / len);
+        const float jac = (a * a) / (len * len * len);
+        return w.z * kInvPi * jac;
+    }
+    __device__ __forceinline__ void eval_local(f3 wo, f3 wi, Spec<N> &f, float &pdf) const {
+        const float ltc = eval_ltc(wi);
+        const bool below = wi.z < 0.0f || wo.z < 0.0f;
+#pragma unroll
+        for (int i = 0; i < N; ++i) f.v[i] = below ? 0.0f : (ltc * tint.v[i]) / wi.z;
+        pdf = ltc;
+    }
+    // A cosine-hemisphere direction through M = [[1/a, 0, -b/a], [0, 1/a, 0], [0, 0, 1]].
+    __device__ __forceinline__ f3 sample_local(f2 u) const {
+        const f3 w = cosine_hemisphere(u);
+        return normalize(make3(w.x / a - w.z * b / a, w.y / a, w.z));
+    }
+};
+
 // Material types compiled into a Bsdf: bit t set for MaterialType t.  Kernels
 // that shade one material class at a time instantiate only its code.
 constexpr uint32_t kAllMaterials = 0x3fu;
@@ -235,12 +283,14 @@ struct Bsdf {
     Spec<N> ks;
     bool plastic;
     // Microfacet lobes: metal uses mf[0]; principled uses mf[0] = metallic,
-    // mf[1] = specular.
-    MfLobe<N> mf[2];
+    // mf[1] = specular, mf[2] = coat.
+    MfLobe<N> mf[3];
     DielLobe<N> dl;
-    // Principled lobe-set sample weights (normalised): metallic, transmission,
-    // specular, diffuse; and whether the transmission lobe is present.
-    float w_metal, w_trans, w_spec, w_diff;
+    SheenLobe<N> sh;
+    // Principled lobe-set sample weights (normalised) in the reference's lobe
+    // order: sheen, coat, metallic, transmission, specular, diffuse; and
+    // whether the transmission lobe is present.
+    float w_sheen, w_coat, w_metal, w_trans, w_spec, w_diff;
     float trans_scale;
     bool has_trans;
 
@@ -354,6 +404,22 @@ struct Bsdf {
             bool same = wo.z * wi.z > 0.0f;
             Spec<N> f;
             float p;
+            if (w_sheen > 0.0f) {
+                sh.eval_local(wo, wi, f, p);
+                if (same) {
+                    e.f = e.f + f * acos_i;
+                    e.pdf += p * w_sheen;
+                }
+                e.flags |= kFlagGlossyRefl;
+            }
+            if (w_coat > 0.0f) {
+                mf[2].eval_local(wo, wi, luts, f, p);
+                if (same) {
+                    e.f = e.f + f * acos_i;
+                    e.pdf += p * w_coat;
+                }
+                e.flags |= kFlagGlossyRefl;
+            }
             if (w_metal > 0.0f) {
                 mf[0].eval_local(wo, wi, luts, f, p);
                 if (same) {
@@ -365,7 +431,8 @@ struct Bsdf {
             if (has_trans) {
                 uint32_t fl;
                 dl.eval_local(wo, wi, luts, f, p, fl, eta);
-                e.f = e.f + f * (acos_i * trans_scale);
+                // Lobe::evaluate's |cos| first, then WeightedLobe::weight (lobe.cpp:686-697).
+                e.f = e.f + (f * acos_i) * trans_scale;
                 e.pdf += p * w_trans;
                 e.flags |= fl;
             }
@@ -418,17 +485,20 @@ struct Bsdf {
             (void)smp.next2();
             int strategy = 0;
             float sum = 0.0f;
-            const float ws[4] = {w_metal, w_trans, w_spec, w_diff};
-            const bool present[4] = {w_metal > 0.0f, has_trans, w_spec > 0.0f, w_diff > 0.0f};
+            const float ws[6] = {w_sheen, w_coat, w_metal, w_trans, w_spec, w_diff};
+            const bool present[6] = {w_sheen > 0.0f, w_coat > 0.0f, w_metal > 0.0f, has_trans, w_spec > 0.0f,
+                                     w_diff > 0.0f};
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
+            for (int i = 0; i < 6; ++i) {
                 if (!present[i]) continue;
                 strategy = uc > sum ? i : strategy;
                 sum += ws[i];
             }
-            if (strategy == 0) wi = mf[0].sample_local(wo, smp.next2(), valid);
-            else if (strategy == 1) wi = dl.sample_local(wo, smp, valid);
-            else if (strategy == 2) wi = mf[1].sample_local(wo, smp.next2(), valid);
+            if (strategy == 0) wi = sh.sample_local(smp.next2());
+            else if (strategy == 1) wi = mf[2].sample_local(wo, smp.next2(), valid);
+            else if (strategy == 2) wi = mf[0].sample_local(wo, smp.next2(), valid);
+            else if (strategy == 3) wi = dl.sample_local(wo, smp, valid);
+            else if (strategy == 4) wi = mf[1].sample_local(wo, smp.next2(), valid);
             else {
                 wi = cosine_hemisphere(smp.next2());
                 wi.z = wo.z < 0.0f ? -wi.z : wi.z;
@@ -458,7 +528,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
     b.ng = ng;
     b.luts = s.luts;
     b.dispersive = (m.flags & kMatFlagDispersive) != 0u && !is_rgb(wl);
-    b.w_metal = b.w_trans = b.w_spec = b.w_diff = 0.0f;
+    b.w_sheen = b.w_coat = b.w_metal = b.w_trans = b.w_spec = b.w_diff = 0.0f;
     b.plastic = false;
     b.has_trans = false;
     b.trans_scale = 0.0f;
@@ -493,6 +563,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
         d.ay = m.p[1];
         d.kt = albedo_spectrum<N>(m.coef, wl);
         d.compensate = true;
+        d.schlick = false;
         bool front = dot(wo, ng) > 0.0f;
 #pragma unroll
         for (int i = 0; i < N; ++i) {
@@ -521,8 +592,9 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
             for (int i = 0; i < N; ++i) b.mf[0].fa.v[i] = f0 * b.ks.v[i];
         }
     } else if (has_mat<M>(kMatPrincipled) && m.type == kMatPrincipled) {
-        // PrincipledBSDF::create_lobe_set (principled_bsdf.cpp:352-461) with
-        // sheen and coat at weight 0 (their lobes then contribute nothing).
+        // PrincipledBSDF::create_lobe_set (principled_bsdf.cpp:352-461): the
+        // lobes in the reference's order, each layer's albedo taking its share
+        // of the weight left for the layers below (layering_weight, :209-214).
         float ax = m.p[0], ay = m.p[1];
         float metallic_param = m.p[2];
         float ior = m.p[3];
@@ -532,7 +604,46 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
         float cos_theta = dot(wo, ng);
         float front = cos_theta > 0.0f ? 1.0f : 0.0f;
         Spec<N> weight = Spec<N>::fill(1.0f);
-        float sw_metal = 0.0f, sw_trans = 0.0f, sw_spec = 0.0f, sw_diff = 0.0f;
+        float sw_sheen = 0.0f, sw_coat = 0.0f, sw_metal = 0.0f, sw_trans = 0.0f, sw_spec = 0.0f, sw_diff = 0.0f;
+        // The sheen / coat / transmission parameter block (zero weights without one).
+        const float *xp = m.spd0 != kInvalid ? s.spd + m.spd0 + 1 : nullptr;
+        auto layer = [&](const Spec<N> &alb) {
+            float mx = -3.402823466e+38f;
+#pragma unroll
+            for (int i = 0; i < N; ++i) mx = fmaxf(mx, safe_div(alb.v[i], weight.v[i]));
+            weight = weight * clampf(1.0f - mx, 0.0f, 1.0f);
+        };
+        if (xp && xp[0] != 0.0f) {
+            // SheenLTC (principled_bsdf.cpp:372-383).
+            const float sheen_w = xp[0] * front;
+            const float c0 = lut_sample2c(s.luts + kLutSheen, 4, 0, cos_theta, xp[1]);
+            const float c1 = lut_sample2c(s.luts + kLutSheen, 4, 1, cos_theta, xp[1]);
+            const float c2 = lut_sample2c(s.luts + kLutSheen, 4, 2, cos_theta, xp[1]);
+            b.sh.a = c0;
+            b.sh.b = c1;
+            b.sh.tint = albedo_spectrum<N>(xp + 2, wl) * sheen_w * weight * c2;
+            sw_sheen = avg(b.sh.tint);
+            layer(b.sh.tint);
+        }
+        if (xp && xp[5] != 0.0f) {
+            // CoatLobe (principled_bsdf.cpp:384-400): GGX reflection with
+            // alpha = roughness^2 and a dielectric Fresnel; albedo from its table.
+            MfLobe<N> &l = b.mf[2];
+            const float cc_w = xp[5] * front;
+            float cc_r = clampf(xp[6], 0.0001f, 1.0f);
+            cc_r = cc_r * cc_r;
+            l.ax = l.ay = cc_r;
+            l.fresnel = kFresnelDielectric;
+            l.compensate = false;
+            l.eta0 = xp[7];
+            l.kr = weight * cc_w * albedo_spectrum<N>(xp + 8, wl);
+            const float x = sqrtf(sqrtf(cc_r * cc_r));
+            const float z = (xp[7] - kCoatIorLower) / (kCoatIorUpper - kCoatIorLower);
+            const float sc = lut_sample3(s.luts + kLutCoat, 1, 0, x, cos_theta, z);
+            const Spec<N> alb = l.kr * sc;
+            sw_coat = avg(alb);
+            layer(alb);
+        }
         // Metallic: F82 tint (F0 = colour, F82 = specular tint).
         float metallic = metallic_param * front;
         {
@@ -554,6 +665,27 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
             sw_metal = metallic * avg(weight);
             weight = weight * (1.0f - metallic);
         }
+        if (xp && xp[11] != 0.0f) {
+            // Transmission (principled_bsdf.cpp:415-428): a compensated
+            // DielectricLobe with FresnelSchlick (F0 = schlick_F0(eta) * tint),
+            // kt = colour, weighted in f and in sampling by the mean of
+            // transmission weight * layer weight.
+            const float trans_w = xp[11];
+            DielLobe<N> &d = b.dl;
+            d.ax = ax;
+            d.ay = ay;
+            d.kt = color;
+            d.compensate = true;
+            d.schlick = true;
+            const float eta = cos_theta > 0.0f ? ior : 1.0f / ior;
+            d.eta = Spec<N>::fill(eta);
+            d.f0 = tint * schlick_F0_from_ior(eta);
+            const Spec<N> tw = weight * trans_w;
+            sw_trans = avg(tw);
+            b.trans_scale = sw_trans;
+            b.has_trans = true;
+            weight = weight * (1.0f - trans_w);
+        }
         // Specular: Schlick with F0 = schlick(ior) * tint; albedo from its table.
         {
             MfLobe<N> &l = b.mf[1];
@@ -572,17 +704,15 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
 #pragma unroll
             for (int i = 0; i < N; ++i) alb.v[i] = (l.fa.v[i] + sl * (1.0f - l.fa.v[i])) * weight.v[i];
             sw_spec = avg(alb);
-            // layering_weight (principled_bsdf.cpp:209-214).
-            float mx = -3.402823466e+38f;
-#pragma unroll
-            for (int i = 0; i < N; ++i) mx = fmaxf(mx, safe_div(alb.v[i], weight.v[i]));
-            weight = weight * clampf(1.0f - mx, 0.0f, 1.0f);
+            layer(alb);
         }
         // Diffuse.
         b.kd = color * weight * front;
         sw_diff = avg(b.kd);
         // LobeSet::normalize_sampled_weight (lobe.cpp:483-492).
-        float sum = sw_metal + sw_trans + sw_spec + sw_diff;
+        float sum = sw_sheen + sw_coat + sw_metal + sw_trans + sw_spec + sw_diff;
+        b.w_sheen = sw_sheen / sum;
+        b.w_coat = sw_coat / sum;
         b.w_metal = sw_metal / sum;
         b.w_trans = b.has_trans ? sw_trans / sum : 0.0f;
         b.w_spec = sw_spec / sum;

@@ -111,6 +111,11 @@ void rgb2spec_decode_unbound(const float *table, const float rgb[3], float out[4
 // reference's shipped values, and the same tables regenerated from the lobe
 // definitions (built on first use, cached in `cache_path`).
 const float *microfacet_luts();
+// The principled BSDF's tables as shipped by the reference: CoatLobe albedo
+// (precomputed_table.h, 32^3) and the SheenLTC fits (ltc_sheen_table.h,
+// Approximate mode, 32^2 x 4).
+const float *coat_lut();
+const float *sheen_ltc_lut();
 const float *regenerate_microfacet_luts(const std::string &cache_path);
 
 // CIE tables downsampled to the reference's 94-entry 5 nm SPDs and the CIE Y

@@ -169,12 +169,32 @@ VS_HD float lut_sample3(const float *t, int ch, int c, float u, float v, float w
     return c0 + fz * (c1 - c0);
 }
 
+// 2D table with `ch` channels per texel, index [y][x][c].
+VS_HD float lut_sample2c(const float *t, int ch, int c, float u, float v) {
+    int x0, x1, y0, y1;
+    float fx = lut_coord(u, x0, x1), fy = lut_coord(v, y0, y1);
+    auto at = [&](int x, int y) { return t[(y * kLutRes + x) * ch + c]; };
+    float a = at(x0, y0) + fx * (at(x1, y0) - at(x0, y0));
+    float b = at(x0, y1) + fx * (at(x1, y1) - at(x0, y1));
+    return a + fy * (b - a);
+}
+
 // Offsets of the tables in the concatenated LUT buffer.
 constexpr int kLutPureReflection = 0;                             // 32^2, 1 channel
 constexpr int kLutDielectric = kLutPureReflection + 32 * 32;        // 32^3, 2 channels
 constexpr int kLutDielectricInv = kLutDielectric + 2 * 32 * 32 * 32; // 32^3, 2 channels
 constexpr int kLutSpecular = kLutDielectricInv + 2 * 32 * 32 * 32;   // 32^3, 1 channel
 constexpr int kLutFloats = kLutSpecular + 32 * 32 * 32;
+// The principled BSDF's tables follow the compensation tables in the device
+// buffer: the CoatLobe albedo (32^3, 1 channel: roughness ratio, cos theta,
+// ior ratio) and the SheenLTC fits (32^2, 4 channels (a, b, scale, 0): cos
+// theta, sheen roughness).
+constexpr int kLutCoat = kLutFloats;
+constexpr int kLutSheen = kLutCoat + 32 * 32 * 32;
+constexpr int kLutDeviceFloats = kLutSheen + 32 * 32 * 4;
+// CoatLobe's ior range (principled_bsdf.cpp:124-125).
+constexpr float kCoatIorLower = 1.003f;
+constexpr float kCoatIorUpper = 4.0f;
 
 // Lobe constants (src/base/scattering/lobe.h:24-25,181-185).
 constexpr float kAlphaLower = 0.001f;

@@ -112,6 +112,26 @@ def substrate_room(width=64, height=64, dimension=4, sampler="independent", max_
     return sc
 
 
+def principled_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
+    """The box room with principled BSDFs that use every layer: a sheen-and-
+    coat tall box over a metallic base, a transmissive short box with a coat,
+    and a sheen floor (PrincipledBSDF's sheen LTC, coat, metallic,
+    transmission, specular and diffuse lobes)."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    mats = {m["name"]: m for m in sc["materials"]}
+    mats["TallBox"].update({"type": "principled_bsdf", "param": {
+        "color": [0.7, 0.3, 0.2], "metallic": 0.5, "roughness": 0.4, "spec_tint": [0.9, 0.9, 1.0],
+        "sheen_weight": 0.8, "sheen_roughness": 0.4, "sheen_tint": [0.9, 0.8, 0.6],
+        "coat_weight": 0.7, "coat_roughness": 0.15, "coat_ior": 1.6, "coat_tint": [0.95, 0.95, 0.9]}})
+    mats["ShortBox"].update({"type": "principled_bsdf", "param": {
+        "color": [0.85, 0.9, 0.95], "roughness": 0.25, "ior": 1.45, "transmission_weight": 0.8,
+        "coat_weight": 0.3, "coat_roughness": 0.1}})
+    mats["Floor"].update({"type": "principled_bsdf", "param": {
+        "color": [0.5, 0.45, 0.4], "roughness": 0.6, "sheen_weight": 1.0, "sheen_roughness": 0.7,
+        "sheen_tint": [0.6, 0.7, 0.9]}})
+    return sc
+
+
 def plastic_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
     """The box room with plastic boxes (PlasticLobe): a glossy blue short box
     (ior 1.5, roughness 0.3) and a near-specular white tall box (roughness
