@@ -312,6 +312,15 @@ def main():
                     help='skip the other workloads that the default run reports under `sub`')
     ap.add_argument('--schedule', default='wavefront', choices=['wavefront', 'persistent', 'grid'],
                     help='path scheduling of the megakernel (both give the same film)')
+    ap.add_argument('--reference-spp', type=int, default=None,
+                    help='radiance_cache: spp of the FP64 plain reference (default 1024; the full specification '
+                         'is 65536)')
+    ap.add_argument('--decompose', action='store_true',
+                    help='radiance_cache: also measure relMSE at 16 spp of the plain tracer cut after 1, 2, 3 '
+                         'and all bounces (what bounds the cache speed-up)')
+    ap.add_argument('--rates', default=None,
+                    help='serving: comma-separated arrival rates (jobs/s) measured one after another on the same '
+                         'resident scenes; the first is the headline, all are listed under `sweep`')
     ap.add_argument('--spp', type=int, default=None,
                     help='override the workload spp (profiling runs on a smaller launch; reported in config)')
     args = ap.parse_args()
@@ -335,6 +344,8 @@ def main():
     w = dict(WORKLOADS[args.workload])
     if args.spp:
         w['spp'] = args.spp
+    if args.reference_spp and w['kind'] == 'radiance_cache':
+        w['reference_spp'] = args.reference_spp
     line = RUNNERS[w['kind']](args, w, rank, world, local_rank, dist)
     if rank == 0 and world == 1 and args.workload == DEFAULT_WORKLOAD and not args.no_sub:
         line['sub'] = run_sub(args, local_rank)
@@ -696,6 +707,27 @@ def run_cache(args, w, rank, world, local_rank, dist):
         return need * dt / spp, need
     tp_m, spp_p_m = time_model(plain_curve)
     tc_m, spp_c_m = time_model(cached_curve)
+    decomposition = None
+    if getattr(args, 'decompose', False):
+        # What bounds the cache's speed-up: the plain tracer cut after d
+        # bounces (emission and next-event estimates of the first d vertices)
+        # against its own converged FP64 reference at equal spp.  With the
+        # cache ending paths after 2 bounces, relMSE(full) / relMSE(d = 2) at
+        # 16 spp, times the frame-time ratio, is the speed-up a perfect,
+        # free cache would give.
+        decomposition = []
+        for d in (1, 2, 3, w['max_depth']):
+            dsc = scenes.box_room(w['width'], w['height'], max_depth=d, dimension=w['dimension'],
+                                  sampler=w['sampler'], seed=w['seed'])
+            dref_sc = dict(dsc, sampler={'type': w['sampler'], 'param': {'seed': w['seed'] + 7919}})
+            dref = vb.Scene(ctx, dref_sc).build_accel()
+            dref.render(0, 1024, fp64=True, stream=sp)
+            dref.synchronize()
+            r = dref.film(vb.FILM_SUM64)[..., :3] / 1024.0
+            ds = vb.Scene(ctx, dsc).build_accel()
+            dt = timed(lambda: ds.render(0, 16, stream=sp))
+            decomposition.append({'max_depth': d, 'relmse_16spp': relmse(ds.film()[..., :3], r), 's_16spp': dt})
+            del ds, dref
     # Algorithmic flops of the network per frame: inference on every pixel's
     # query and every suffix end, training forward + backward on the samples.
     nt = w['train_samples']
@@ -722,7 +754,8 @@ def run_cache(args, w, rank, world, local_rank, dist):
                     'speedup_warm': (tp / tc) if (tp and tc) else None,
                     'speedup_cold': (tp / tc_cold) if (tp and tc_cold) else None,
                     'at_target_1_over_spp': {'plain_s': tp_m, 'plain_spp': spp_p_m, 'cached_s': tc_m,
-                                             'cached_spp': spp_c_m, 'speedup_warm': tp_m / tc_m}},
+                                             'cached_spp': spp_c_m, 'speedup_warm': tp_m / tc_m},
+                    'variance_by_depth': decomposition},
         'roofline': {'bound': 'tensor', 'achieved': achieved_tf, 'peak': peak_tf, 'unit': 'TFLOP/s',
                      'frac': achieved_tf / peak_tf, 'peak_source': 'measured', 'traffic': None,
                      'kernel': 'radiance-cache frame (network share of the frame time)',
@@ -782,6 +815,26 @@ def run_serving(args, w, rank, world, local_rank, dist):
     for i in range(args.warmup):
         warm.result(warm.submit(wids[w['scenes'][i % 4]], 256, 256, 1, frame_begin=i), timeout=600)
     warm.close()
+    peak, peak_src = measured_peaks()
+    rates = [float(r) for r in args.rates.split(',')] if getattr(args, 'rates', None) else [w['rate']]
+    runs = []
+    for rate in rates:
+        wr = dict(w, rate=rate)
+        runs.append(serve_once(args, wr, make_server, bpp, peak, vb, torch))
+    line = runs[0]
+    line['config'].update({'scene_build_s': round(build_s, 1), 'parallelism': 'replicas%d' % world})
+    if len(runs) > 1:
+        # Latency and throughput per arrival rate, same job sequence (the
+        # seeded arrival times scale with 1 / rate).
+        line['sweep'] = [{'rate': r['config']['rate'], 'value': r['value'], 'latency_ms': r['latency_ms'],
+                          'gpu_busy_s': r['server']['gpu_busy_s'], 'wall_s': r['ms_per_step'] * r['steps'] / 1e3}
+                         for r in runs]
+    return line
+
+
+def serve_once(args, w, make_server, bpp, peak, vb, torch):
+    """One serving run of args.steps jobs at arrival rate w['rate'] on a fresh
+    server over the already resident scenes."""
     srv, ids = make_server()
     jobs = serving_jobs(w, args.steps)
     results = []
@@ -818,22 +871,20 @@ def run_serving(args, w, rank, world, local_rank, dist):
     paths = float(sum(p for _, p in results))
     value = paths / wall / 1e6
     mean_bpp = sum(bpp[w['scenes'][s]] * p for s, p in results) / paths
-    peak, peak_src = measured_peaks()
     gpu_s = st['gpu_busy_s']
     achieved = mean_bpp * paths / gpu_s / 1e9 if gpu_s > 0 else None
     line = {
-        'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': world, 'steps': len(jobs),
+        'metric': 'Mpaths/s', 'value': value, 'unit': 'Mpaths/s', 'n_gpus': 1, 'steps': len(jobs),
         'warmup': args.warmup, 'ms_per_step': wall * 1e3 / len(jobs), 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
         'config': {'workload': args.workload, **{k: v for k, v in w.items() if k != 'kind'},
-                   'jobs_submitted': len(jobs), 'step': 'one job (submit -> film on the host)',
-                   'parallelism': 'replicas%d' % world, 'scene_build_s': round(build_s, 1)},
+                   'jobs_submitted': len(jobs), 'step': 'one job (submit -> film on the host)'},
         'latency_ms': {'p50': st['p50_ms'], 'p95': st['p95_ms'], 'p99': st['p99_ms'], 'mean': st['mean_ms'],
                        'max': st['max_ms']},
         'server': {k: st[k] for k in ('completed', 'batches', 'graph_launches', 'gpu_busy_s', 'peak_jobs',
-                                      'peak_bytes')},
+                                      'peak_bytes', 'resident_bytes', 'scratch_bytes')},
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                     'frac': achieved / peak if achieved else None, 'peak_source': peak_src, 'traffic': None,
+                     'frac': achieved / peak if achieved else None, 'peak_source': 'measured', 'traffic': None,
                      'kernel': 'serving batches (wavefront kernels k_sv_*)', 'bytes_per_path': mean_bpp,
                      'gpu_busy_s': gpu_s},
         'clocks': clk,

@@ -290,8 +290,10 @@ int vs_restir_download(vs_scene *scene, int which, void *dst, size_t bytes);
  * resolution and spp over resident scenes.  No reference counterpart (the
  * reference renders one scene interactively); it serves the path above.
  * A native scheduler thread admits jobs while job slots and `hbm_budget`
- * bytes allow (each job holds a float4 film; two batch buffers of
- * `paths_per_batch` float4 paths are reserved at creation), then keeps the GPU
+ * bytes allow: the budget covers the resident scenes' device memory (counted
+ * by vs_server_add_scene, which fails with VS_E_RANGE when a scene does not
+ * fit), the two batch buffers of `paths_per_batch` paths reserved at creation
+ * and each admitted job's float4 film.  The scheduler then keeps the GPU
  * busy with batches of whole frames from all admitted jobs, each batch one
  * CUDA-graph launch (work-table upload, persistent path kernel, film pass).
  * A job's film equals vs_render of the same scene, camera, resolution and
@@ -316,6 +318,8 @@ typedef struct vs_server_stats {
     double p50_ms, p95_ms, p99_ms, mean_ms, max_ms; /* submission -> film on the host */
     uint64_t peak_bytes;    /* largest admitted job memory */
     uint32_t peak_jobs;     /* most jobs in flight at once */
+    uint64_t resident_bytes; /* device memory of the resident scenes */
+    uint64_t scratch_bytes;  /* the two batch buffers reserved at creation */
 } vs_server_stats;
 int vs_server_create(vs_context *ctx, uint64_t hbm_budget, uint32_t max_jobs, uint64_t paths_per_batch,
                      vs_server **out);

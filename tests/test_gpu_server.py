@@ -83,3 +83,29 @@ def test_server_rejects(vb, gpu_ctx, served):
     with pytest.raises(vb.UnsupportedError):
         srv.add_scene(rt)
     srv.close()
+
+
+def test_server_budget_counts_resident_scenes(vb, gpu_ctx, served):
+    # The HBM budget covers the resident scenes as well as the batch scratch
+    # and the job films: a scene that does not fit beside the others is
+    # refused, and the stats report the resident and scratch bytes.
+    box, big = served
+    srv = vb.Server(gpu_ctx, hbm_budget=4 << 30, max_jobs=4, paths_per_batch=1 << 15)
+    srv.add_scene(box)
+    r_box = srv.stats()['resident_bytes']
+    srv.add_scene(big)
+    st = srv.stats()
+    r_big = st['resident_bytes'] - r_box
+    scratch = st['scratch_bytes']
+    srv.close()
+    assert r_box > 0 and r_big > 12 << 20 and scratch > 0  # the sky's RGB table alone is 12.6 MB
+    srv = vb.Server(gpu_ctx, hbm_budget=scratch + r_box + r_big // 2, max_jobs=4, paths_per_batch=1 << 15)
+    srv.add_scene(box)
+    with pytest.raises(vb.VisionError) as e:
+        srv.add_scene(big)
+    assert 'budget' in str(e.value)
+    assert srv.stats()['resident_bytes'] == r_box
+    # A job whose film does not fit beside the resident scene is refused too.
+    with pytest.raises(vb.VisionError):
+        srv.submit(0, 4096, 4096, 1)
+    srv.close()

@@ -74,7 +74,8 @@ class ServerStats(ctypes.Structure):
                                                'kernel_launches')] + \
                [(n, ctypes.c_double) for n in ('paths', 'wall_s', 'gpu_busy_s', 'p50_ms', 'p95_ms', 'p99_ms',
                                                'mean_ms', 'max_ms')] + \
-               [('peak_bytes', ctypes.c_uint64), ('peak_jobs', ctypes.c_uint32)]
+               [('peak_bytes', ctypes.c_uint64), ('peak_jobs', ctypes.c_uint32),
+                ('resident_bytes', ctypes.c_uint64), ('scratch_bytes', ctypes.c_uint64)]
 
 
 def _load():

@@ -219,6 +219,16 @@ struct vs_scene {
         cachebuf.free();
     }
 
+    // Device memory of the scene proper (geometry, BVH, materials, lights,
+    // sampling tables, environment, filter and LUTs), not its film or render
+    // scratch.
+    uint64_t device_bytes() const {
+        auto b = [](const auto &buf) { return static_cast<uint64_t>(buf.count) * sizeof(*buf.ptr); };
+        return b(nodes) + b(tri_v) + b(vtx) + b(prims) + b(instances) + b(materials) + b(lights) + b(prim_alias) +
+               b(light_alias) + b(prim_pmf) + b(light_pmf) + b(spd) + b(luts) + b(env_tex) + b(env_marginal_func) +
+               b(env_cond_func) + b(rgb2spec) + b(env_marginal) + b(env_cond) + b(filter_tab) + b(filter_alias);
+    }
+
     DeviceScene device_view() const {
         DeviceScene d{};
         d.nodes = reinterpret_cast<const uint4 *>(nodes.ptr);
@@ -1166,13 +1176,15 @@ void vs_server_destroy(vs_server *s) {
 int vs_server_add_scene(vs_server *s, vs_scene *scene, uint32_t *scene_id) {
     if (!s || !scene || !scene_id) return VS_E_INVALID;
     DeviceScene dv;
+    uint64_t bytes = 0;
     {
         std::lock_guard<std::mutex> lock(scene->mu);
         if (!scene->uploaded) return s->fail(VS_E_STATE, "vs_scene_build_accel must precede vs_server_add_scene");
         dv = scene->device_view();
+        bytes = scene->device_bytes();
     }
     std::string err;
-    int rc = server_add_scene(s->impl, dv, scene_id, err);
+    int rc = server_add_scene(s->impl, dv, bytes, scene_id, err);
     return rc == VS_OK ? VS_OK : s->fail(rc, err);
 }
 
@@ -1235,6 +1247,8 @@ int vs_server_stats_get(vs_server *s, vs_server_stats *out) {
     out->max_ms = st.max_ms;
     out->peak_bytes = st.peak_bytes;
     out->peak_jobs = st.peak_jobs;
+    out->resident_bytes = st.resident_bytes;
+    out->scratch_bytes = st.scratch_bytes;
     return VS_OK;
 }
 

@@ -228,6 +228,7 @@ public:
     std::deque<Inflight> inflight;
     uint64_t next_id = 1;
     uint64_t mem_used = 0;
+    uint64_t resident = 0;  // device memory of the resident scenes
     uint64_t batch_no = 0;
     bool stop = false;
     std::string error;
@@ -427,9 +428,10 @@ public:
             std::vector<std::shared_ptr<Job>> work;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                // Admission: job slots and the HBM budget (films + the two scratch buffers).
+                // Admission: job slots and the HBM budget (resident scenes, the
+                // two batch scratch buffers and the admitted jobs' films).
                 while (!pending.empty() && active.size() < max_jobs &&
-                       scratch + mem_used + pending.front()->bytes <= budget) {
+                       scratch + resident + mem_used + pending.front()->bytes <= budget) {
                     std::shared_ptr<Job> j = pending.front();
                     pending.pop_front();
                     cudaError_t e = cudaMallocAsync(&j->film, j->bytes, stream);
@@ -572,6 +574,7 @@ int server_create(int device, uint64_t hbm_budget, uint32_t max_jobs, uint64_t p
         err = "HBM budget below the batch scratch buffers";
         return VS_E_RANGE;
     }
+    s->st.scratch_bytes = s->scratch;
     cudaError_t e = s->init();
     if (e != cudaSuccess) {
         err = std::string("server init: ") + cudaGetErrorString(e);
@@ -583,10 +586,14 @@ int server_create(int device, uint64_t hbm_budget, uint32_t max_jobs, uint64_t p
 
 void server_destroy(Server *s) { delete s; }
 
-int server_add_scene(Server *s, const DeviceScene &scene, uint32_t *id, std::string &err) {
+int server_add_scene(Server *s, const DeviceScene &scene, uint64_t bytes, uint32_t *id, std::string &err) {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->nscenes >= kMaxServeScenes) {
         err = "too many resident scenes";
+        return VS_E_RANGE;
+    }
+    if (s->scratch + s->resident + bytes > s->budget) {
+        err = "resident scenes above the HBM budget";
         return VS_E_RANGE;
     }
     if (scene.ip.spectrum_dim != SN) {
@@ -603,6 +610,8 @@ int server_add_scene(Server *s, const DeviceScene &scene, uint32_t *id, std::str
     }
     s->scene_cam[s->nscenes] = scene.cam;
     s->need_depth = std::max(s->need_depth, scene.ip.max_depth);
+    s->resident += bytes;
+    s->st.resident_bytes = s->resident;
     *id = s->nscenes++;
     return VS_OK;
 }
@@ -635,7 +644,7 @@ int server_submit(Server *s, const ServeJob &job, uint64_t *id, std::string &err
     j->desc = job;
     j->npix = static_cast<uint32_t>(npix);
     j->bytes = npix * sizeof(float4);
-    if (s->scratch + j->bytes > s->budget) {
+    if (s->scratch + s->resident + j->bytes > s->budget) {
         err = "job larger than the HBM budget";
         return VS_E_RANGE;
     }

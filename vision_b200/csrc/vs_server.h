@@ -29,6 +29,8 @@ struct ServeStats {
     double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;  // submit -> film on the host
     uint64_t peak_bytes;     // largest admitted job memory
     uint32_t peak_jobs;      // largest number of jobs in flight
+    uint64_t resident_bytes; // device memory of the resident scenes
+    uint64_t scratch_bytes;  // the two batch buffers reserved at creation
 };
 
 class Server;
@@ -37,7 +39,9 @@ class Server;
 int server_create(int device, uint64_t hbm_budget, uint32_t max_jobs, uint64_t paths_per_batch, Server **out,
                   std::string &err);
 void server_destroy(Server *s);
-int server_add_scene(Server *s, const DeviceScene &scene, uint32_t *id, std::string &err);
+// `bytes`: the scene's device memory, counted against the HBM budget for as
+// long as the server holds the scene.
+int server_add_scene(Server *s, const DeviceScene &scene, uint64_t bytes, uint32_t *id, std::string &err);
 // The sensor of a resident scene (its camera when it was added).
 int server_scene_camera(Server *s, uint32_t id, const Camera **cam, std::string &err);
 int server_submit(Server *s, const ServeJob &job, uint64_t *id, std::string &err);
