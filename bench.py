@@ -310,7 +310,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-sub', action='store_true',
                     help='skip the other workloads that the default run reports under `sub`')
-    ap.add_argument('--schedule', default='wavefront', choices=['wavefront', 'persistent', 'grid'],
+    ap.add_argument('--schedule', default='wavefront', choices=['wavefront', 'wavefront_binned', 'persistent', 'grid'],
                     help='path scheduling of the megakernel (both give the same film)')
     ap.add_argument('--reference-spp', type=int, default=None,
                     help='radiance_cache: spp of the FP64 plain reference (default 1024; the full specification '
@@ -473,7 +473,9 @@ def run_plain(args, w, rank, world, local_rank, dist):
                      'traffic_source': 'ncu dram bytes per path of the committed profile (all kernels of the '
                                        'schedule for one render) x paths per launch',
                      'kernel': {'persistent': 'k_render_regen', 'grid': 'k_render',
-                                'wavefront': 'wavefront (k_wf_extend, k_wf_shade, k_wf_shadow)'}[args.schedule],
+                                'wavefront': 'wavefront (k_wf_extend, k_wf_shade, k_wf_shadow)',
+                                'wavefront_binned': 'wavefront (k_wf_extend, k_wf_shade, k_wf_shadow; binned rays)'}[
+                                    args.schedule],
                      'bytes_per_path': bytes_per_path,
                      'per_path': {'segments': segs / paths_per_step, 'nodes': nodes / paths_per_step,
                                   'tris': tris / paths_per_step},

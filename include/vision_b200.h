@@ -193,6 +193,12 @@ int vs_render(vs_scene *scene, uint32_t frame_begin, uint32_t frame_count, int f
 #define VS_SCHEDULE_GRID 0
 #define VS_SCHEDULE_PERSISTENT 1
 #define VS_SCHEDULE_WAVEFRONT 2
+/* The wavefront schedule with ray binning: before each traversal pass after
+ * the camera rays, the queued rays are grouped by direction octant and the
+ * cell of their origin in an 8 x 8 x 8 grid over the scene (a counting sort,
+ * three small kernels), so that each warp traces rays that start close
+ * together and visit children in the same order; 12 more bytes per slot. */
+#define VS_SCHEDULE_WAVEFRONT_BINNED 3
 int vs_render_schedule_set(vs_scene *scene, int schedule);
 
 /* Waits for all work queued on the scene's stream. */

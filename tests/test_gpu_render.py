@@ -271,13 +271,13 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
         # 5 frames of 1024 x 1024 exceed one wavefront wave (2^22 paths).
         sc = scenes.box_room(width=1024, height=1024, max_depth=4, sampler='pcg')
     films = {}
-    for schedule in ('grid', 'persistent', 'wavefront'):
+    for schedule in ('grid', 'persistent', 'wavefront', 'wavefront_binned'):
         s = vb.Scene(gpu_ctx, sc).build_accel()
         s.set_schedule(schedule)
         s.render(0, 5, fp64=True)
         s.render(5, 4, fp64=True)
         films[schedule] = (s.film(), s.film(vb.FILM_SUM64))
-    for schedule in ('persistent', 'wavefront'):
+    for schedule in ('persistent', 'wavefront', 'wavefront_binned'):
         assert np.array_equal(films['grid'][0], films[schedule][0]), schedule
         assert np.array_equal(films['grid'][1], films[schedule][1]), schedule
         assert np.all(films[schedule][1][..., 3] == 9.0)

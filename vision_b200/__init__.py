@@ -175,6 +175,7 @@ CACHE_BUFFERS = dict(query_features=(0, np.dtype(('<u2', 64)), True), query_reco
                      suffix_output=(6, np.dtype(('<f4', 4)), False), targets=(7, np.dtype(('<f4', 4)), False))
 SCHEDULE_PERSISTENT = 1
 SCHEDULE_WAVEFRONT = 2
+SCHEDULE_WAVEFRONT_BINNED = 3
 
 # Per-pixel ReSTIR records (vision_b200/csrc/vs_restir.h) as numpy dtypes.
 HIT_DTYPE = np.dtype([('inst_id', '<u4'), ('prim_id', '<u4'), ('u', '<f4'), ('v', '<f4')])
@@ -377,8 +378,11 @@ class Scene:
     def set_schedule(self, schedule):
         """Path scheduling of render(): 'wavefront' (bounces as separate
         kernels over path state in device memory, the default), 'persistent'
-        (regenerating resident wave) or 'grid' (one path per thread)."""
-        code = {'grid': SCHEDULE_GRID, 'persistent': SCHEDULE_PERSISTENT, 'wavefront': SCHEDULE_WAVEFRONT}[schedule]
+        (regenerating resident wave), 'grid' (one path per thread) or
+        'wavefront_binned' (the wavefront with rays grouped by direction octant
+        and origin cell before each traversal pass)."""
+        code = {'grid': SCHEDULE_GRID, 'persistent': SCHEDULE_PERSISTENT, 'wavefront': SCHEDULE_WAVEFRONT,
+                'wavefront_binned': SCHEDULE_WAVEFRONT_BINNED}[schedule]
         self.ctx.check(lib.vs_render_schedule_set(self.handle, code), 'render_schedule_set')
 
     def timing_enable(self, on=True):

@@ -12,6 +12,8 @@
 #include "vs_host.h"
 
 #include <algorithm>
+#include <array>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -45,15 +47,21 @@ struct Node2 {
 constexpr int kBins = 32;
 constexpr uint32_t kMaxLeaf = 3;
 
+// Subtrees at least this large are built on their own thread (down to
+// kParallelDepth levels): the binary build is the bulk of the host work, and
+// the two halves of a split touch disjoint ranges of `order`.
+constexpr uint32_t kParallelPrims = 1u << 15;
+constexpr uint32_t kParallelDepth = 5;
+
 struct Builder2 {
     const std::vector<Box> &boxes;
     const std::vector<f3> &cent;
     std::vector<uint32_t> &order;
-    std::vector<Node2> nodes;
+    std::vector<Node2> nodes;          // sized 2 n up front; ids handed out by `next`
+    std::atomic<uint32_t> next{0};
 
-    uint32_t build(uint32_t first, uint32_t count) {
-        uint32_t id = static_cast<uint32_t>(nodes.size());
-        nodes.emplace_back();
+    uint32_t build(uint32_t first, uint32_t count, uint32_t depth = 0) {
+        uint32_t id = next.fetch_add(1);
         Box bb, cb;
         for (uint32_t i = first; i < first + count; ++i) {
             bb.grow(boxes[order[i]]);
@@ -66,20 +74,60 @@ struct Builder2 {
             nodes[id].count = count;
             return id;
         }
-        // Binned SAH over centroids.
+        // Binned SAH over centroids.  The bins of a large node are filled by
+        // several threads over chunks of its range and merged (min / max and
+        // counts: the same bins in any order).
         int best_axis = -1, best_split = -1;
         float best_cost = FLT_MAX;
+        Box all_bins[3][kBins];
+        uint32_t all_cnt[3][kBins] = {};
+        auto fill = [&](uint32_t b0, uint32_t b1, Box (*bb)[kBins], uint32_t (*bc)[kBins]) {
+            for (int axis = 0; axis < 3; ++axis) {
+                float lo = comp(cb.lo, axis), hi = comp(cb.hi, axis);
+                if (!(hi > lo)) continue;
+                float k = kBins / (hi - lo);
+                for (uint32_t i = b0; i < b1; ++i) {
+                    int b = std::min(kBins - 1, static_cast<int>((comp(cent[order[i]], axis) - lo) * k));
+                    bc[axis][b]++;
+                    bb[axis][b].grow(boxes[order[i]]);
+                }
+            }
+        };
+        const uint32_t chunks = count >= (1u << 17) ? 8u : 1u;
+        if (chunks == 1) {
+            fill(first, first + count, all_bins, all_cnt);
+        } else {
+            std::vector<std::array<std::array<Box, kBins>, 3>> cbox(chunks);
+            std::vector<std::array<std::array<uint32_t, kBins>, 3>> ccnt(chunks);
+            std::vector<std::thread> th;
+            for (uint32_t c = 0; c < chunks; ++c) {
+                for (auto &a : ccnt[c]) a.fill(0u);
+                th.emplace_back([&, c] {
+                    const uint32_t b0 = first + static_cast<uint32_t>(static_cast<uint64_t>(count) * c / chunks);
+                    const uint32_t b1 = first + static_cast<uint32_t>(static_cast<uint64_t>(count) * (c + 1) / chunks);
+                    Box lb[3][kBins];
+                    uint32_t lc[3][kBins] = {};
+                    fill(b0, b1, lb, lc);
+                    for (int a = 0; a < 3; ++a)
+                        for (int b = 0; b < kBins; ++b) {
+                            cbox[c][a][b] = lb[a][b];
+                            ccnt[c][a][b] = lc[a][b];
+                        }
+                });
+            }
+            for (auto &t : th) t.join();
+            for (uint32_t c = 0; c < chunks; ++c)
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < kBins; ++b) {
+                        all_bins[a][b].grow(cbox[c][a][b]);
+                        all_cnt[a][b] += ccnt[c][a][b];
+                    }
+        }
         for (int axis = 0; axis < 3; ++axis) {
             float lo = comp(cb.lo, axis), hi = comp(cb.hi, axis);
             if (!(hi > lo)) continue;
-            Box bin_box[kBins];
-            uint32_t bin_cnt[kBins] = {0};
-            float k = kBins / (hi - lo);
-            for (uint32_t i = first; i < first + count; ++i) {
-                int b = std::min(kBins - 1, static_cast<int>((comp(cent[order[i]], axis) - lo) * k));
-                bin_cnt[b]++;
-                bin_box[b].grow(boxes[order[i]]);
-            }
+            const Box *bin_box = all_bins[axis];
+            const uint32_t *bin_cnt = all_cnt[axis];
             float right_area[kBins];
             uint32_t right_cnt[kBins];
             Box acc;
@@ -117,8 +165,15 @@ struct Builder2 {
             mid = static_cast<uint32_t>(it - order.begin());
             if (mid == first || mid == first + count) mid = first + count / 2;
         }
-        uint32_t l = build(first, mid - first);
-        uint32_t r = build(mid, first + count - mid);
+        uint32_t l = 0, r = 0;
+        if (count >= kParallelPrims && depth < kParallelDepth) {
+            std::thread left([&] { l = build(first, mid - first, depth + 1); });
+            r = build(mid, first + count - mid, depth + 1);
+            left.join();
+        } else {
+            l = build(first, mid - first, depth + 1);
+            r = build(mid, first + count - mid, depth + 1);
+        }
         nodes[id].left = l;
         nodes[id].right = r;
         return id;
@@ -298,17 +353,27 @@ void build_bvh8(HostScene &s) {
     uint32_t n = static_cast<uint32_t>(s.prim_inst.size());
     std::vector<Box> boxes(n);
     std::vector<f3> cent(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        Box b;
-        for (int k = 0; k < 3; ++k) b.grow(s.pos[s.idx[3 * i + k]]);
-        boxes[i] = b;
-        cent[i] = b.center();
+    {
+        const uint32_t nt = n >= (1u << 17) ? 8u : 1u;
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                for (uint32_t i = static_cast<uint32_t>(static_cast<uint64_t>(n) * t / nt);
+                     i < static_cast<uint32_t>(static_cast<uint64_t>(n) * (t + 1) / nt); ++i) {
+                    Box b;
+                    for (int k = 0; k < 3; ++k) b.grow(s.pos[s.idx[3 * i + k]]);
+                    boxes[i] = b;
+                    cent[i] = b.center();
+                }
+            });
+        for (auto &x : th) x.join();
     }
     std::vector<uint32_t> order(n);
     for (uint32_t i = 0; i < n; ++i) order[i] = i;
     Builder2 b2{boxes, cent, order, {}};
-    b2.nodes.reserve(2 * n);
+    b2.nodes.resize(2 * static_cast<size_t>(n));
     b2.build(0, n);
+    b2.nodes.resize(b2.next.load());
     s.nodes.clear();
     s.tri_v.clear();
     s.tri_v.reserve(static_cast<size_t>(n) * 12);

@@ -88,14 +88,19 @@ struct vs_scene {
         DevBuf<uint4> st;
         DevBuf<Hit> hit;
         DevBuf<uint32_t> q0, q1, tq, count;
+        DevBuf<uint32_t> bin_key, bins, binned, sh_perm;  // ray binning (VS_SCHEDULE_WAVEFRONT_BINNED)
         uint32_t capacity = 0;
+        bool binning = false;
         void free() {
             o.free(); d.free(); tp.free(); lam.free(); pdf.free(); L.free(); sh_o.free(); sh_d.free(); sh_c.free();
             st.free(); hit.free(); q0.free(); q1.free(); tq.free(); count.free();
+            bin_key.free(); bins.free(); binned.free(); sh_perm.free();
             capacity = 0;
+            binning = false;
         }
-        cudaError_t ensure(uint32_t n) {
-            if (n <= capacity) return cudaSuccess;
+        cudaError_t ensure(uint32_t n, bool with_bins) {
+            if (n <= capacity && (binning || !with_bins)) return cudaSuccess;
+            n = std::max(n, capacity);
             free();
             cudaError_t e = cudaSuccess;
             for (DevBuf<float4> *b : {&o, &d, &tp, &lam, &pdf, &L, &sh_o, &sh_d, &sh_c})
@@ -106,11 +111,23 @@ struct vs_scene {
             if (e == cudaSuccess) e = q1.alloc(n);
             if (e == cudaSuccess) e = tq.alloc(static_cast<size_t>(n) * kWfClasses);
             if (e == cudaSuccess) e = count.alloc(kWfCounters);
+            if (with_bins) {
+                if (e == cudaSuccess) e = bin_key.alloc(n);
+                if (e == cudaSuccess) e = binned.alloc(n);
+                if (e == cudaSuccess) e = sh_perm.alloc(n);
+                if (e == cudaSuccess) e = bins.alloc(2 * kWfBins);
+                // The sizes half must start at zero; k_bin_scan clears it after each use.
+                if (e == cudaSuccess) e = cudaMemset(bins.ptr, 0, 2 * kWfBins * sizeof(uint32_t));
+                // Valid slot and entry indices from the start.
+                if (e == cudaSuccess) e = cudaMemset(binned.ptr, 0, static_cast<size_t>(n) * sizeof(uint32_t));
+                if (e == cudaSuccess) e = cudaMemset(sh_perm.ptr, 0, static_cast<size_t>(n) * sizeof(uint32_t));
+            }
             if (e != cudaSuccess) {
                 free();
                 return e;
             }
             capacity = n;
+            binning = with_bins;
             return cudaSuccess;
         }
         WfBuffers view() const {
@@ -119,6 +136,17 @@ struct vs_scene {
             b.o = o.ptr; b.d = d.ptr; b.tp = tp.ptr; b.lam = lam.ptr; b.pdf = pdf.ptr; b.L = L.ptr;
             b.st = st.ptr; b.hit = hit.ptr; b.queue[0] = q0.ptr; b.queue[1] = q1.ptr;
             b.sh_o = sh_o.ptr; b.sh_d = sh_d.ptr; b.sh_c = sh_c.ptr; b.tq = tq.ptr; b.count = count.ptr;
+            return b;
+        }
+        // The view with the ray-binning buffers (all four or none).
+        WfBuffers view_binned() const {
+            WfBuffers b = view();
+            if (binning) {
+                b.bin_key = bin_key.ptr;
+                b.bins = bins.ptr;
+                b.binned = binned.ptr;
+                b.sh_perm = sh_perm.ptr;
+            }
             return b;
         }
     } wf;
@@ -653,8 +681,10 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     if (frames_per_chunk > frame_count) frames_per_chunk = frame_count;
     VS_CUDA(s->radiance.alloc(static_cast<size_t>(frames_per_chunk * npix)), "radiance alloc");
     if (s->schedule == VS_SCHEDULE_PERSISTENT) VS_CUDA(s->path_counter.alloc(1), "path counter alloc");
-    if (s->schedule == VS_SCHEDULE_WAVEFRONT)
-        VS_CUDA(s->wf.ensure(static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk * npix, kWfWaveSlots))),
+    const bool wavefront = s->schedule == VS_SCHEDULE_WAVEFRONT || s->schedule == VS_SCHEDULE_WAVEFRONT_BINNED;
+    if (wavefront)
+        VS_CUDA(s->wf.ensure(static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk * npix, kWfWaveSlots)),
+                             s->schedule == VS_SCHEDULE_WAVEFRONT_BINNED),
                 "wavefront slots alloc");
     DeviceScene dv = s->device_view();
     auto timed_event = [&](std::vector<cudaEvent_t> &v) -> cudaError_t {
@@ -667,9 +697,11 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     for (uint32_t f = 0; f < frame_count; f += static_cast<uint32_t>(frames_per_chunk)) {
         uint32_t fc = static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk, frame_count - f));
         if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
-        if (s->schedule == VS_SCHEDULE_WAVEFRONT) {
+        if (wavefront) {
             unsigned n = 0;
-            VS_CUDA(launch_render_wavefront(dv, frame_begin + f, fc, s->radiance.ptr, s->wf.view(),
+            VS_CUDA(launch_render_wavefront(dv, frame_begin + f, fc, s->radiance.ptr,
+                                            s->schedule == VS_SCHEDULE_WAVEFRONT_BINNED ? s->wf.view_binned()
+                                                                                        : s->wf.view(),
                                             shading_classes(s->host), st, &n),
                     "wavefront render");
             add_launches(n);
@@ -700,8 +732,10 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
 
 int vs_render_schedule_set(vs_scene *s, int schedule) {
     if (!s) return VS_E_INVALID;
-    if (schedule != VS_SCHEDULE_GRID && schedule != VS_SCHEDULE_PERSISTENT && schedule != VS_SCHEDULE_WAVEFRONT)
-        return fail(s->ctx, VS_E_INVALID, "schedule must be VS_SCHEDULE_GRID, _PERSISTENT or _WAVEFRONT");
+    if (schedule != VS_SCHEDULE_GRID && schedule != VS_SCHEDULE_PERSISTENT && schedule != VS_SCHEDULE_WAVEFRONT &&
+        schedule != VS_SCHEDULE_WAVEFRONT_BINNED)
+        return fail(s->ctx, VS_E_INVALID,
+                    "schedule must be VS_SCHEDULE_GRID, _PERSISTENT, _WAVEFRONT or _WAVEFRONT_BINNED");
     std::lock_guard<std::mutex> lock(s->mu);
     s->schedule = schedule;
     return VS_OK;
@@ -1052,7 +1086,7 @@ int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void
     const bool wavefront = s->schedule == VS_SCHEDULE_WAVEFRONT && rt_npix <= kWfWaveSlots;
     WfBuffers wfv{};
     if (wavefront) {
-        VS_CUDA(s->wf.ensure(static_cast<uint32_t>(rt_npix)), "wavefront slots alloc");
+        VS_CUDA(s->wf.ensure(static_cast<uint32_t>(rt_npix), false), "wavefront slots alloc");
         VS_CUDA(s->radiance.alloc(rt_npix), "radiance alloc");
         wfv = s->wf.view();
     }
@@ -1479,7 +1513,7 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     // Wavefront frames need one path slot per pixel.
     const bool wavefront = s->schedule == VS_SCHEDULE_WAVEFRONT && npix <= kWfWaveSlots;
     if (wavefront) {
-        VS_CUDA(s->wf.ensure(npix), "wavefront slots alloc");
+        VS_CUDA(s->wf.ensure(npix, false), "wavefront slots alloc");
         VS_CUDA(s->radiance.alloc(npix), "radiance alloc");
         VS_CUDA(b.suffix_list.alloc(nt), "cache alloc");
         VS_CUDA(b.suffix_count.alloc(1), "cache alloc");

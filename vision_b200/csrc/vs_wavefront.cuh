@@ -246,7 +246,7 @@ __device__ __forceinline__ void shadow(const Scenes &scenes, const WfBuffers &b,
         if (!drained) {
             const uint32_t k = refill(b.count + kWfFetchShadow, n, active, drained);
             if (k < n) {
-                i = k;
+                i = b.sh_perm ? b.sh_perm[k] : k;
                 const float4 o = b.sh_o[i], d = b.sh_d[i];
                 s = &scenes(__float_as_uint(b.sh_c[i].w));
                 r = precompute_ray(make3(o.x, o.y, o.z), make3(d.x, d.y, d.z));

@@ -31,7 +31,21 @@ struct WfBuffers {
     uint32_t *count; // [0], [1]: path queue lengths; [2]: shadow queue length;
                      // [3 + c]: length of shading class c; [kWfFetchExtend],
                      // [kWfFetchShadow]: rays handed out by the traversal kernels
+    // Ray binning (all null: off).  Before a traversal pass the queued rays
+    // are grouped by a key of direction octant and origin cell: bin_key holds
+    // each entry's key, bins 2 x kWfBins counters (sizes, then write
+    // positions), binned the path queue in bin order, sh_perm the shadow
+    // queue's entries in bin order.
+    uint32_t *bin_key;
+    uint32_t *bins;
+    uint32_t *binned;
+    uint32_t *sh_perm;
 };
+
+// Ray-binning keys: 3 bits of direction octant above a 9-bit Morton code of
+// the ray origin's cell in an 8 x 8 x 8 grid over the scene's bounds.
+constexpr uint32_t kWfBinBits = 12;
+constexpr uint32_t kWfBins = 1u << kWfBinBits;
 
 // Shading classes of a hit: 0 = miss, 1 + MaterialType otherwise.  Each class
 // is shaded by its own kernel, compiled with that material's code only.

@@ -60,6 +60,100 @@ __global__ void __launch_bounds__(128) k_wf_shadow(const __grid_constant__ Devic
     wf::shadow(OneScene{&s}, b, base, radiance);
 }
 
+// ---------------------------------------------------------------------------
+// Ray binning: a counting sort of a queue by ray key (direction octant, then
+// the Morton cell of the origin), so that the warps of the traversal pass
+// take rays that start close together and visit the children in the same
+// order.  The order of entries inside a bin is arbitrary; every path's result
+// is independent of the order in which rays are traced.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    v &= 7u;
+    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+}
+
+// Key of a ray: the scene box is the BVH root's quantisation grid (origin p,
+// 255 steps of 2^e per axis).
+__device__ __forceinline__ uint32_t ray_key(const uint4 &root, const float4 &o, const float4 &d) {
+    const float px = __uint_as_float(root.x), py = __uint_as_float(root.y), pz = __uint_as_float(root.z);
+    const float sx = __uint_as_float((root.w & 0xffu) << 23) * (8.0f / 255.0f);
+    const float sy = __uint_as_float(((root.w >> 8) & 0xffu) << 23) * (8.0f / 255.0f);
+    const float sz = __uint_as_float(((root.w >> 16) & 0xffu) << 23) * (8.0f / 255.0f);
+    const uint32_t cx = static_cast<uint32_t>(fminf(fmaxf((o.x - px) / sx, 0.0f), 7.0f));
+    const uint32_t cy = static_cast<uint32_t>(fminf(fmaxf((o.y - py) / sy, 0.0f), 7.0f));
+    const uint32_t cz = static_cast<uint32_t>(fminf(fmaxf((o.z - pz) / sz, 0.0f), 7.0f));
+    const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    return (oct << 9) | spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
+}
+
+// Pass 1: the key of every entry of a queue of n = *len entries (src: the
+// queue's slots, or null for entries 0..n-1 of the shadow queue) and the
+// sizes of the bins.
+__global__ void __launch_bounds__(256) k_bin_count(const __grid_constant__ DeviceScene s, const uint32_t *len,
+                                                   const uint32_t *src, const float4 *o, const float4 *d,
+                                                   uint32_t *keys, uint32_t *bins) {
+    const uint32_t n = *len;
+    const uint4 root = __ldg(s.nodes);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t e = src ? src[i] : i;
+        const uint32_t key = ray_key(root, o[e], d[e]);
+        keys[i] = key;
+        const unsigned active = __activemask();
+        const unsigned group = __match_any_sync(active, key);
+        if (wf::lane_id() == __ffs(group) - 1) atomicAdd(bins + key, static_cast<uint32_t>(__popc(group)));
+    }
+}
+
+// Pass 2 (one block of 1024 threads): bin write positions (exclusive prefix
+// sums) to bins[kWfBins ...], sizes cleared for the next use.
+__global__ void __launch_bounds__(1024) k_bin_scan(uint32_t *bins) {
+    constexpr uint32_t per = kWfBins / 1024u;
+    __shared__ uint32_t part[1024];
+    uint32_t local[per];
+    uint32_t sum = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < per; ++k) {
+        local[k] = bins[threadIdx.x * per + k];
+        sum += local[k];
+    }
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024u; off <<= 1) {
+        const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t pos = part[threadIdx.x] - sum;
+#pragma unroll
+    for (uint32_t k = 0; k < per; ++k) {
+        bins[kWfBins + threadIdx.x * per + k] = pos;
+        pos += local[k];
+        bins[threadIdx.x * per + k] = 0u;
+    }
+}
+
+// Pass 3: every entry to its bin (dst: the binned queue's slots, or the
+// shadow queue's entry indices).
+__global__ void __launch_bounds__(256) k_bin_scatter(const uint32_t *len, const uint32_t *src, const uint32_t *keys,
+                                                     uint32_t *bins, uint32_t *dst) {
+    const uint32_t n = *len;
+    uint32_t *pos = bins + kWfBins;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t key = keys[i];
+        const unsigned active = __activemask();
+        const unsigned group = __match_any_sync(active, key);
+        const int lane = wf::lane_id();
+        const int leader = __ffs(group) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(pos + key, static_cast<uint32_t>(__popc(group)));
+        base = __shfl_sync(active, base, leader);
+        // The bin sizes of pass 1 sum to n, so every position is below n.
+        const uint32_t p = base + static_cast<uint32_t>(__popc(group & ((1u << lane) - 1u)));
+        if (p < n) dst[p] = src ? src[i] : i;
+    }
+}
+
 namespace {
 
 // Resident blocks of 128 threads per SM for each kernel, per device.
@@ -119,6 +213,14 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
     if ((e = shade_grid<N, 6>(dev, sg)) != cudaSuccess) return e;
     const uint32_t mask = class_mask | 1u;
     unsigned n_launch = 0;
+    const bool binning = b.bin_key && b.bins && b.binned && b.sh_perm;
+    int sms = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const unsigned grid_bin = static_cast<unsigned>(sms) * 8u;
+    // The traversal passes read the binned queue (path slots) or the shadow
+    // permutation instead of the queues in push order.
+    WfBuffers bs = b;
+    bs.sh_perm = binning ? b.sh_perm : nullptr;
     for (uint64_t base = 0; base < paths; base += b.capacity) {
         const uint32_t n = static_cast<uint32_t>(std::min<uint64_t>(b.capacity, paths - base));
         const unsigned g = std::min<unsigned>(grid_gen, (n + 127u) / 128u);
@@ -126,7 +228,18 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
         ++n_launch;
         for (uint32_t bounce = 0; bounce < s.ip.max_depth; ++bounce) {
             const uint32_t cur = bounce & 1u;
-            k_wf_extend<<<grid_ext, 128, 0, st>>>(s, b, cur);
+            // Camera rays (bounce 0) arrive in pixel order, already coherent.
+            const bool bin_paths = binning && bounce > 0;
+            WfBuffers be = b;
+            be.sh_perm = nullptr;
+            if (bin_paths) {
+                k_bin_count<<<grid_bin, 256, 0, st>>>(s, b.count + cur, b.queue[cur], b.o, b.d, b.bin_key, b.bins);
+                k_bin_scan<<<1, 1024, 0, st>>>(b.bins);
+                k_bin_scatter<<<grid_bin, 256, 0, st>>>(b.count + cur, b.queue[cur], b.bin_key, b.bins, b.binned);
+                be.queue[cur] = b.binned;
+                n_launch += 3;
+            }
+            k_wf_extend<<<grid_ext, 128, 0, st>>>(s, be, cur);
             launch_shade<N, 0>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 1>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 2>(sg, mask, s, b, cur, base, radiance, st, n_launch);
@@ -134,7 +247,13 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
             launch_shade<N, 4>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 5>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 6>(sg, mask, s, b, cur, base, radiance, st, n_launch);
-            k_wf_shadow<<<grid_shadow, 128, 0, st>>>(s, b, base, radiance);
+            if (binning) {
+                k_bin_count<<<grid_bin, 256, 0, st>>>(s, b.count + 2, nullptr, b.sh_o, b.sh_d, b.bin_key, b.bins);
+                k_bin_scan<<<1, 1024, 0, st>>>(b.bins);
+                k_bin_scatter<<<grid_bin, 256, 0, st>>>(b.count + 2, nullptr, b.bin_key, b.bins, b.sh_perm);
+                n_launch += 3;
+            }
+            k_wf_shadow<<<grid_shadow, 128, 0, st>>>(s, bs, base, radiance);
             n_launch += 2;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
