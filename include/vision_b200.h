@@ -78,6 +78,8 @@ typedef struct vs_scene_info {
     uint32_t spectrum_dim;
     uint32_t max_depth;
     uint32_t accel_built;
+    uint32_t two_level;  /* 1: one BVH8 per mesh under a top level over instances */
+    uint32_t mesh_count; /* distinct object-space meshes */
 } vs_scene_info;
 
 /* Library version: major * 10000 + minor * 100 + patch. */
@@ -130,7 +132,12 @@ int vs_scene_invalidate(vs_scene *scene);
 
 /* Builds the compressed BVH8 and uploads the scene to the device
  * (reference Geometry::build_accel, src/base/mgr/geometry.cpp:36-52;
- * SDK VisionRenderer::build_accel, src/sdk/vision.h:66-80). */
+ * SDK VisionRenderer::build_accel, src/sdk/vision.h:66-80).  Shapes with the
+ * same vertices and triangles share one mesh; when a mesh has several
+ * instances the acceleration structure has two levels, as the reference's
+ * BLAS-per-mesh plus IAS: one BVH8 per mesh over its object-space triangles
+ * and a top-level BVH8 over the instances' world boxes.  Scenes whose JSON
+ * sets render_setting.instancing to false keep one BVH8 over world space. */
 int vs_scene_build_accel(vs_scene *scene);
 
 /* Film resolution (reference RadianceCollector::update_resolution,
@@ -172,6 +179,13 @@ int vs_scene_info_get(const vs_scene *scene, vs_scene_info *out);
 #define VS_EXPORT_ENV_COND 24           /* alias entries per texel (row-major) */
 #define VS_EXPORT_ENV_COND_FUNC 25      /* float weight per texel */
 #define VS_EXPORT_RGB2SPEC 26   /* float[4] x 3 x 64^3 RGB -> spectrum coefficient table */
+/* Instancing: the distinct object-space meshes and each instance's mesh and
+ * world-to-object transform (the two-level BVH traces rays in object space). */
+#define VS_EXPORT_MESH_POS 27   /* float[3] per object-space vertex */
+#define VS_EXPORT_MESH_IDX 28   /* uint32[3] per mesh triangle, relative to its mesh's first vertex */
+#define VS_EXPORT_MESHES 29     /* 24 bytes per mesh: first vertex, vertex count, first triangle, count, hash */
+#define VS_EXPORT_INST_MESH 30  /* uint32 per instance */
+#define VS_EXPORT_INST_W2O 31   /* float[16] per instance, column-major world-to-object */
 int vs_scene_export_size(const vs_scene *scene, int what, size_t *bytes);
 int vs_scene_export(const vs_scene *scene, int what, void *dst, size_t bytes);
 

@@ -39,7 +39,10 @@ class OracleSceneStruct(ctypes.Structure):
                 ('camera', ctypes.c_void_p), ('integrator', ctypes.c_void_p), ('spd', ctypes.c_void_p),
                 ('env', ctypes.c_void_p), ('env_tex', ctypes.c_void_p), ('env_marginal', ctypes.c_void_p),
                 ('env_marginal_func', ctypes.c_void_p), ('env_cond', ctypes.c_void_p),
-                ('env_cond_func', ctypes.c_void_p), ('rgb2spec', ctypes.c_void_p)]
+                ('env_cond_func', ctypes.c_void_p), ('rgb2spec', ctypes.c_void_p),
+                ('two_level', ctypes.c_uint32), ('mesh_count', ctypes.c_uint32), ('mesh_pos', ctypes.c_void_p),
+                ('mesh_idx', ctypes.c_void_p), ('meshes', ctypes.c_void_p), ('inst_mesh', ctypes.c_void_p),
+                ('inst_w2o', ctypes.c_void_p)]
 
 
 _lib = None
@@ -113,6 +116,7 @@ def _p(a):
 SCENE_KEYS = ['pos', 'nrm', 'uv', 'idx', 'prim_inst', 'instances', 'materials', 'lights', 'prim_alias', 'prim_pmf',
               'light_alias', 'light_pmf', 'camera', 'integrator', 'spd']
 ENV_KEYS = ['env', 'env_tex', 'env_marginal', 'env_marginal_func', 'env_cond', 'env_cond_func', 'rgb2spec']
+INSTANCE_KEYS = ['mesh_pos', 'mesh_idx', 'meshes', 'inst_mesh', 'inst_w2o']
 
 
 class OracleScene:
@@ -125,12 +129,13 @@ class OracleScene:
     def __init__(self, scene=None, arrays=None, info=None):
         if scene is not None:
             env = scene.export('env')
-            keys = SCENE_KEYS + (ENV_KEYS if env.size else [])
-            arrays = {k: scene.export(k) for k in keys}
             info = scene.info()
+            keys = SCENE_KEYS + (ENV_KEYS if env.size else []) + (INSTANCE_KEYS if info.get('two_level') else [])
+            arrays = {k: scene.export(k) for k in keys}
         has_env = 'env' in arrays and arrays['env'].size > 0
+        two_level = bool(info.get('two_level')) and 'mesh_pos' in arrays
         self.arr = {}
-        for k in SCENE_KEYS + (ENV_KEYS if has_env else []):
+        for k in SCENE_KEYS + (ENV_KEYS if has_env else []) + (INSTANCE_KEYS if two_level else []):
             a = np.ascontiguousarray(arrays[k])
             if a.size == 0:
                 a = np.zeros(16, np.uint8)
@@ -143,7 +148,9 @@ class OracleScene:
                                    _p(a['materials']), info['material_count'], _p(a['lights']), info['light_count'],
                                    _p(a['prim_alias']), _p(a['prim_pmf']), _p(a['light_alias']), _p(a['light_pmf']),
                                    _p(a['camera']), _p(a['integrator']), _p(a['spd']),
-                                   *([_p(a[k]) for k in ENV_KEYS] if has_env else [None] * 7))
+                                   *([_p(a[k]) for k in ENV_KEYS] if has_env else [None] * 7),
+                                   1 if two_level else 0, int(info.get('mesh_count', 0)) if two_level else 0,
+                                   *([_p(a[k]) for k in INSTANCE_KEYS] if two_level else [None] * 5))
         self.h = ctypes.c_void_p(lib().oracle_open(ctypes.byref(self.s)))
 
     @classmethod

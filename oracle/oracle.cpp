@@ -127,6 +127,18 @@ struct oracle_scene {
     const void *env_cond;
     const float *env_cond_func;
     const float *rgb2spec;
+    // Instancing (two_level = 1): the distinct object-space meshes (6 uint32
+    // per mesh: first vertex, vertex count, first triangle, triangle count,
+    // hash), each instance's mesh and column-major world-to-object transform.
+    // Rays are traced in each instance's object space, as the library's
+    // two-level BVH does.
+    uint32_t two_level;
+    uint32_t mesh_count;
+    const float *mesh_pos;
+    const uint32_t *mesh_idx;
+    const uint32_t *meshes;
+    const uint32_t *inst_mesh;
+    const float *inst_w2o;
 };
 }
 
@@ -484,10 +496,101 @@ struct Scene {
             has_env = true;
         }
         if (cam.filter >= 2u) build_filter();
+        if (sc->two_level) {
+            build_instances();
+            return;
+        }
         order.resize(sc->prim_count);
         for (uint32_t i = 0; i < sc->prim_count; ++i) order[i] = i;
         nodes.reserve(sc->prim_count / 2 + 8);
         build(0, sc->prim_count);
+    }
+
+    // Two-level scenes: a median-split BVH per mesh over its object-space
+    // triangles, each instance's world box (from its world-space vertices)
+    // and world-to-object rows.
+    struct MeshBvh {
+        const float *pos;
+        const uint32_t *idx;
+        std::vector<Node> nodes;
+        std::vector<uint32_t> order;
+        V3 Pm(uint32_t v) const { return {pos[3 * v], pos[3 * v + 1], pos[3 * v + 2]}; }
+        uint32_t build(uint32_t first, uint32_t count) {
+            uint32_t id = static_cast<uint32_t>(nodes.size());
+            nodes.push_back({});
+            float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+            for (uint32_t i = first; i < first + count; ++i)
+                for (int k = 0; k < 3; ++k) {
+                    V3 v = Pm(idx[3 * order[i] + k]);
+                    for (int a = 0; a < 3; ++a) {
+                        lo[a] = std::min(lo[a], at(v, a));
+                        hi[a] = std::max(hi[a], at(v, a));
+                    }
+                }
+            std::memcpy(nodes[id].lo, lo, sizeof(lo));
+            std::memcpy(nodes[id].hi, hi, sizeof(hi));
+            if (count <= 4) {
+                nodes[id].first = first;
+                nodes[id].count = count;
+                return id;
+            }
+            int axis = 0;
+            for (int a = 1; a < 3; ++a)
+                if (hi[a] - lo[a] > hi[axis] - lo[axis]) axis = a;
+            uint32_t mid = first + count / 2;
+            auto key = [&](uint32_t t) {
+                float c = 0.0f;
+                for (int k = 0; k < 3; ++k) c += at(Pm(idx[3 * t + k]), axis);
+                return c;
+            };
+            std::nth_element(order.begin() + first, order.begin() + mid, order.begin() + first + count,
+                             [&](uint32_t a, uint32_t b) { return key(a) < key(b) || (key(a) == key(b) && a < b); });
+            uint32_t l = build(first, mid - first);
+            uint32_t r = build(mid, first + count - mid);
+            nodes[id].left = l;
+            nodes[id].right = r;
+            nodes[id].count = 0;
+            return id;
+        }
+    };
+    std::vector<MeshBvh> mesh_bvh;
+    std::vector<float> inst_lo, inst_hi, inst_rows;  // 3, 3 and 12 floats per instance
+
+    void build_instances() {
+        mesh_bvh.resize(s->mesh_count);
+        for (uint32_t m = 0; m < s->mesh_count; ++m) {
+            const uint32_t *r = s->meshes + 6 * m;
+            MeshBvh &b = mesh_bvh[m];
+            b.pos = s->mesh_pos + 3 * static_cast<size_t>(r[0]);
+            b.idx = s->mesh_idx + 3 * static_cast<size_t>(r[2]);
+            b.order.resize(r[3]);
+            for (uint32_t i = 0; i < r[3]; ++i) b.order[i] = i;
+            b.build(0, r[3]);
+        }
+        inst_lo.assign(3 * s->instance_count, FLT_MAX);
+        inst_hi.assign(3 * s->instance_count, -FLT_MAX);
+        inst_rows.resize(12 * s->instance_count);
+        for (uint32_t i = 0; i < s->instance_count; ++i) {
+            const Instance &in = inst[i];
+            for (uint32_t p = in.first_prim; p < in.first_prim + in.prim_count; ++p)
+                for (int k = 0; k < 3; ++k) {
+                    V3 v = P(s->idx[3 * p + k]);
+                    for (int a = 0; a < 3; ++a) {
+                        inst_lo[3 * i + a] = std::min(inst_lo[3 * i + a], at(v, a));
+                        inst_hi[3 * i + a] = std::max(inst_hi[3 * i + a], at(v, a));
+                    }
+                }
+            // Pad the box a little: it only culls instances, and a hit found in
+            // object space may lie a rounding step outside the world box.
+            for (int a = 0; a < 3; ++a) {
+                const float pad = 1e-5f * std::max(std::fabs(inst_lo[3 * i + a]), std::fabs(inst_hi[3 * i + a])) + 1e-6f;
+                inst_lo[3 * i + a] -= pad;
+                inst_hi[3 * i + a] += pad;
+            }
+            const float *m = s->inst_w2o + 16 * static_cast<size_t>(i);  // m[4 c + r]
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 4; ++c) inst_rows[12 * i + 4 * r + c] = m[4 * c + r];
+        }
     }
 };
 
@@ -561,8 +664,86 @@ struct HitRec {
     float t = 0, u = 0, v = 0;
 };
 
+// The ray in an instance's object space: rows r[0..11] of the world-to-object
+// transform, products and sums in the GPU's order (no contraction).
+static RayPre instance_ray(const float *w, const RayPre &r) {
+    V3 o = {((w[0] * r.o.x + w[1] * r.o.y) + w[2] * r.o.z) + w[3], ((w[4] * r.o.x + w[5] * r.o.y) + w[6] * r.o.z) + w[7],
+            ((w[8] * r.o.x + w[9] * r.o.y) + w[10] * r.o.z) + w[11]};
+    V3 d = {(w[0] * r.d.x + w[1] * r.d.y) + w[2] * r.d.z, (w[4] * r.d.x + w[5] * r.d.y) + w[6] * r.d.z,
+            (w[8] * r.d.x + w[9] * r.d.y) + w[10] * r.d.z};
+    return precompute(o, d);
+}
+
+// Two-level closest hit: every instance whose world box the ray meets, its
+// mesh's triangles in object space; global ids first_prim + triangle index,
+// exact ties in t to the lower global id.
+static HitRec closest_instanced(const Scene &sc, const RayPre &rw, float tmax) {
+    HitRec best;
+    best.t = tmax;
+    for (uint32_t i = 0; i < sc.s->instance_count; ++i) {
+        if (!box_hit(rw, &sc.inst_lo[3 * i], &sc.inst_hi[3 * i], best.t * 1.000001f)) continue;
+        const RayPre r = instance_ray(&sc.inst_rows[12 * i], rw);
+        const Scene::MeshBvh &b = sc.mesh_bvh[sc.s->inst_mesh[i]];
+        const uint32_t first = sc.inst[i].first_prim;
+        uint32_t stack[128];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp) {
+            const Scene::Node &n = b.nodes[stack[--sp]];
+            if (!box_hit(r, n.lo, n.hi, best.t * 1.000001f)) continue;
+            if (n.count) {
+                for (uint32_t k = n.first; k < n.first + n.count; ++k) {
+                    uint32_t t3 = b.order[k];
+                    float t, u, v;
+                    float lim = best.prim == kInvalid ? tmax : best.t * 1.000001f;
+                    if (tri_hit(r, b.Pm(b.idx[3 * t3]), b.Pm(b.idx[3 * t3 + 1]), b.Pm(b.idx[3 * t3 + 2]), 0.0f, lim, t, u,
+                                v)) {
+                        uint32_t p = first + t3;
+                        if (t < best.t || (t == best.t && p < best.prim)) {
+                            best.prim = p; best.t = t; best.u = u; best.v = v;
+                        }
+                    }
+                }
+            } else {
+                stack[sp++] = n.left;
+                stack[sp++] = n.right;
+            }
+        }
+    }
+    return best;
+}
+
+static bool any_instanced(const Scene &sc, const RayPre &rw, float tmax) {
+    for (uint32_t i = 0; i < sc.s->instance_count; ++i) {
+        if (!box_hit(rw, &sc.inst_lo[3 * i], &sc.inst_hi[3 * i], tmax * 1.000001f)) continue;
+        const RayPre r = instance_ray(&sc.inst_rows[12 * i], rw);
+        const Scene::MeshBvh &b = sc.mesh_bvh[sc.s->inst_mesh[i]];
+        uint32_t stack[128];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp) {
+            const Scene::Node &n = b.nodes[stack[--sp]];
+            if (!box_hit(r, n.lo, n.hi, tmax * 1.000001f)) continue;
+            if (n.count) {
+                for (uint32_t k = n.first; k < n.first + n.count; ++k) {
+                    uint32_t t3 = b.order[k];
+                    float t, u, v;
+                    if (tri_hit(r, b.Pm(b.idx[3 * t3]), b.Pm(b.idx[3 * t3 + 1]), b.Pm(b.idx[3 * t3 + 2]), 0.0f, tmax, t,
+                                u, v))
+                        return true;
+                }
+            } else {
+                stack[sp++] = n.left;
+                stack[sp++] = n.right;
+            }
+        }
+    }
+    return false;
+}
+
 // Closest hit over t in (0, tmax); exact ties in t go to the lower primitive id.
 static HitRec closest(const Scene &sc, const RayPre &r, float tmax) {
+    if (sc.s->two_level) return closest_instanced(sc, r, tmax);
     HitRec best;
     best.t = tmax;
     uint32_t stack[128];
@@ -592,6 +773,7 @@ static HitRec closest(const Scene &sc, const RayPre &r, float tmax) {
 }
 
 static bool any_hit(const Scene &sc, const RayPre &r, float tmax) {
+    if (sc.s->two_level) return any_instanced(sc, r, tmax);
     uint32_t stack[128];
     int sp = 0;
     stack[sp++] = 0;

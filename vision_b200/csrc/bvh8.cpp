@@ -17,6 +17,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <stdexcept>
 #include <thread>
 
@@ -183,9 +184,12 @@ struct Builder2 {
 struct Collapse {
     const std::vector<Node2> &n2;
     const std::vector<uint32_t> &order;
-    const HostScene &scene;
+    // Writes the leaf entry of primitive `prim` (a triangle's 12 floats, or a
+    // top-level leaf's instance id) and returns nothing; leaf_base() is the
+    // index the next entry will get.
+    std::function<void(uint32_t)> emit;
+    std::function<uint32_t()> leaf_base;
     std::vector<Bvh8Node> &out;
-    std::vector<float> &tri_v;
     std::vector<uint32_t> subtree_count;
     uint32_t max_depth = 0;
 
@@ -207,16 +211,6 @@ struct Collapse {
     }
 
     bool is_leaf_child(uint32_t id) const { return n2[id].leaf || subtree_count[id] <= kMaxLeaf; }
-
-    void emit_tri(uint32_t prim) {
-        for (int k = 0; k < 3; ++k) {
-            f3 p = scene.pos[scene.idx[3 * prim + k]];
-            tri_v.push_back(p.x);
-            tri_v.push_back(p.y);
-            tri_v.push_back(p.z);
-            tri_v.push_back(k == 0 ? bits_float(prim) : 0.0f);
-        }
-    }
 
     // Writes node `slot_index` of `out` for binary node `id` and recurses.
     void build(uint32_t id, uint32_t out_index, uint32_t depth) {
@@ -304,7 +298,7 @@ struct Collapse {
         for (int sl = 0; sl < 8; ++sl)
             if (child_at[sl] >= 0 && !is_leaf_child(ch[child_at[sl]])) internal_count++;
         node.base_child = static_cast<uint32_t>(out.size());
-        node.base_tri = static_cast<uint32_t>(tri_v.size() / 12);
+        node.base_tri = leaf_base();
         out.resize(out.size() + internal_count);
         uint32_t tri_offset = 0;
         std::vector<std::pair<uint32_t, uint32_t>> recurse;  // (binary id, out index)
@@ -334,7 +328,7 @@ struct Collapse {
                 if (prims.size() > kMaxLeaf || tri_offset + prims.size() > 24)
                     throw std::runtime_error("bvh8: leaf too large");
                 node.meta[sl] = static_cast<uint8_t>((((1u << prims.size()) - 1u) << 5) | tri_offset);
-                for (uint32_t pr : prims) emit_tri(pr);
+                for (uint32_t pr : prims) emit(pr);
                 tri_offset += static_cast<uint32_t>(prims.size());
             } else {
                 node.imask |= static_cast<uint8_t>(1u << sl);
@@ -349,41 +343,140 @@ struct Collapse {
 
 }  // namespace
 
-void build_bvh8(HostScene &s) {
-    uint32_t n = static_cast<uint32_t>(s.prim_inst.size());
-    std::vector<Box> boxes(n);
+namespace {
+
+// Binned-SAH binary tree over `n` primitive boxes, collapsed into BVH8 nodes
+// appended to `out` (root at the returned index); leaf entries written by
+// `emit` (see Collapse).  Returns the depth of the collapsed tree.
+uint32_t build_tree(const std::vector<Box> &boxes, std::vector<Bvh8Node> &out, uint32_t &root,
+                    const std::function<void(uint32_t)> &emit, const std::function<uint32_t()> &leaf_base) {
+    const uint32_t n = static_cast<uint32_t>(boxes.size());
     std::vector<f3> cent(n);
-    {
-        const uint32_t nt = n >= (1u << 17) ? 8u : 1u;
-        std::vector<std::thread> th;
-        for (uint32_t t = 0; t < nt; ++t)
-            th.emplace_back([&, t] {
-                for (uint32_t i = static_cast<uint32_t>(static_cast<uint64_t>(n) * t / nt);
-                     i < static_cast<uint32_t>(static_cast<uint64_t>(n) * (t + 1) / nt); ++i) {
-                    Box b;
-                    for (int k = 0; k < 3; ++k) b.grow(s.pos[s.idx[3 * i + k]]);
-                    boxes[i] = b;
-                    cent[i] = b.center();
-                }
-            });
-        for (auto &x : th) x.join();
-    }
+    for (uint32_t i = 0; i < n; ++i) cent[i] = boxes[i].center();
     std::vector<uint32_t> order(n);
     for (uint32_t i = 0; i < n; ++i) order[i] = i;
     Builder2 b2{boxes, cent, order, {}};
     b2.nodes.resize(2 * static_cast<size_t>(n));
     b2.build(0, n);
     b2.nodes.resize(b2.next.load());
+    Collapse col{b2.nodes, order, emit, leaf_base, out, std::vector<uint32_t>(b2.nodes.size(), 0)};
+    col.count_tris(0);
+    root = static_cast<uint32_t>(out.size());
+    out.resize(out.size() + 1);
+    col.build(0, root, 1);
+    if (col.max_depth + 1 > 32) throw std::runtime_error("bvh8: tree deeper than the traversal stack");
+    return col.max_depth;
+}
+
+std::vector<Box> triangle_boxes(const f3 *pos, const uint32_t *idx, uint32_t n) {
+    std::vector<Box> boxes(n);
+    const uint32_t nt = n >= (1u << 17) ? 8u : 1u;
+    std::vector<std::thread> th;
+    for (uint32_t t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (uint32_t i = static_cast<uint32_t>(static_cast<uint64_t>(n) * t / nt);
+                 i < static_cast<uint32_t>(static_cast<uint64_t>(n) * (t + 1) / nt); ++i) {
+                Box b;
+                for (int k = 0; k < 3; ++k) b.grow(pos[idx[3 * i + k]]);
+                boxes[i] = b;
+            }
+        });
+    for (auto &x : th) x.join();
+    return boxes;
+}
+
+}  // namespace
+
+void build_bvh8(HostScene &s) {
+    const uint32_t n = static_cast<uint32_t>(s.prim_inst.size());
     s.nodes.clear();
     s.tri_v.clear();
-    s.tri_v.reserve(static_cast<size_t>(n) * 12);
-    Collapse col{b2.nodes, order, s, s.nodes, s.tri_v, std::vector<uint32_t>(b2.nodes.size(), 0)};
-    col.count_tris(0);
+    s.tlas_inst.clear();
+    s.blas_root.clear();
+    // Two levels when meshes are shared: always (instancing 2), or (1, auto)
+    // when the scene is large (2^20 triangles or more) and its instances hold
+    // at least 8 times the distinct meshes' triangles, where the smaller
+    // structure and build pay for the extra level; otherwise one BVH8 over
+    // world space traces faster.
+    std::vector<uint32_t> uses(s.meshes.size(), 0);
+    for (uint32_t m : s.inst_mesh) uses[m]++;
+    uint64_t unique_tris = 0;
+    for (const HostScene::MeshRec &r : s.meshes) unique_tris += r.tri_count;
+    const bool shared = std::any_of(uses.begin(), uses.end(), [](uint32_t u) { return u > 1; });
+    // The real-time ReSTIR kernels trace one world-space BVH8.
+    s.two_level = !s.rt && s.inst_mesh.size() == s.instances.size() && shared &&
+                  (s.instancing == 2 ||
+                   (s.instancing == 1 && n >= (1u << 20) && static_cast<uint64_t>(n) >= 8 * unique_tris));
+    if (!s.two_level) {
+        // One BVH8 over the world-space triangles; tri_v w = global primitive id.
+        std::vector<Box> boxes = triangle_boxes(s.pos.data(), s.idx.data(), n);
+        s.tri_v.reserve(static_cast<size_t>(n) * 12);
+        auto emit = [&](uint32_t prim) {
+            for (int k = 0; k < 3; ++k) {
+                f3 p = s.pos[s.idx[3 * prim + k]];
+                s.tri_v.push_back(p.x);
+                s.tri_v.push_back(p.y);
+                s.tri_v.push_back(p.z);
+                s.tri_v.push_back(k == 0 ? bits_float(prim) : 0.0f);
+            }
+        };
+        uint32_t root = 0;
+        s.bvh_depth = build_tree(boxes, s.nodes, root, emit, [&] { return static_cast<uint32_t>(s.tri_v.size() / 12); });
+        if (s.tri_v.size() != static_cast<size_t>(n) * 12) throw std::runtime_error("bvh8: primitive count mismatch");
+        s.tlas_root = 0;
+        return;
+    }
+    // Bottom level: one BVH8 per mesh over its object-space triangles
+    // (tri_v w = the triangle's index in the mesh).  The top level's root goes
+    // first so that node 0 bounds the whole scene.
     s.nodes.resize(1);
-    col.build(0, 0, 1);
-    s.bvh_depth = col.max_depth;
-    if (s.tri_v.size() != static_cast<size_t>(n) * 12) throw std::runtime_error("bvh8: primitive count mismatch");
-    if (col.max_depth + 1 > 32) throw std::runtime_error("bvh8: tree deeper than the traversal stack");
+    uint32_t depth = 0;
+    for (uint32_t m = 0; m < s.meshes.size(); ++m) {
+        const HostScene::MeshRec &r = s.meshes[m];
+        std::vector<Box> boxes = triangle_boxes(s.mesh_pos.data() + r.first_vertex, s.mesh_idx.data() + 3u * r.first_tri,
+                                                r.tri_count);
+        const f3 *mp = s.mesh_pos.data() + r.first_vertex;
+        const uint32_t *mi = s.mesh_idx.data() + 3u * r.first_tri;
+        auto emit = [&](uint32_t tri) {
+            for (int k = 0; k < 3; ++k) {
+                f3 p = mp[mi[3 * tri + k]];
+                s.tri_v.push_back(p.x);
+                s.tri_v.push_back(p.y);
+                s.tri_v.push_back(p.z);
+                s.tri_v.push_back(k == 0 ? bits_float(tri) : 0.0f);
+            }
+        };
+        uint32_t root = 0;
+        depth = std::max(depth, build_tree(boxes, s.nodes, root, emit,
+                                           [&] { return static_cast<uint32_t>(s.tri_v.size() / 12); }));
+        s.blas_root.push_back(root);
+    }
+    // Top level over the instances' world boxes (the bounds of their
+    // world-space vertices); leaf entries are instance ids.
+    std::vector<Box> iboxes(s.instances.size());
+    for (uint32_t i = 0; i < s.instances.size(); ++i) {
+        const uint32_t first = s.instances[i].first_prim;
+        Box wb;
+        for (uint32_t t = 0; t < s.instances[i].prim_count; ++t)
+            for (int k = 0; k < 3; ++k) wb.grow(s.pos[s.idx[3 * (first + t) + k]]);
+        iboxes[i] = wb;
+    }
+    std::vector<Bvh8Node> top;
+    uint32_t troot = 0;
+    auto emit_inst = [&](uint32_t inst) { s.tlas_inst.push_back(inst); };
+    depth = std::max(depth, build_tree(iboxes, top, troot, emit_inst,
+                                       [&] { return static_cast<uint32_t>(s.tlas_inst.size()); }));
+    // Append the top level after the meshes, its root at node 0: child
+    // indices of the top level move by the offset of its other nodes.
+    const uint32_t off = static_cast<uint32_t>(s.nodes.size()) - 1u;
+    for (size_t k = 0; k < top.size(); ++k) {
+        Bvh8Node nd = top[k];
+        if (nd.imask) nd.base_child += off;  // children of a node always follow the root
+        if (k == troot) s.nodes[0] = nd;
+        else s.nodes.push_back(nd);
+    }
+    s.tlas_root = 0;
+    s.bvh_depth = depth;
 }
 
 }  // namespace vs

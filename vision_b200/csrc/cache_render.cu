@@ -380,9 +380,10 @@ __global__ void __launch_bounds__(128) k_cw_generate(const __grid_constant__ Dev
     wf::generate<CN>(s, s.cam, b, frame, 0, n, ended);
 }
 
+template <int L>
 __global__ void __launch_bounds__(128) k_cw_extend(const __grid_constant__ DeviceScene s,
                                                    const __grid_constant__ WfBuffers b, uint32_t cur) {
-    wf::extend(CacheScene{&s}, b, cur);
+    wf::extend<L>(CacheScene{&s}, b, cur);
 }
 
 template <uint32_t C>
@@ -391,9 +392,10 @@ __global__ void __launch_bounds__(128) k_cw_shade(const __grid_constant__ Device
     wf::shade<CN, C>(CacheScene{&s}, b, cur, 0, ended);
 }
 
+template <int L>
 __global__ void __launch_bounds__(128) k_cw_shadow(const __grid_constant__ DeviceScene s,
                                                    const __grid_constant__ WfBuffers b, float4 *ended) {
-    wf::shadow(CacheScene{&s}, b, 0, ended);
+    wf::shadow<L>(CacheScene{&s}, b, 0, ended);
 }
 
 // Query vertices (the hits of the bounce-`query_depth` rays of queue `cur`).
@@ -507,14 +509,21 @@ cudaError_t launch_cache_frame_wavefront(const DeviceScene &s, const CacheFrameP
                                          uint32_t *suffix_count, cudaStream_t st, unsigned *launches) {
     const uint32_t npix = s.cam.width * s.cam.height;
     if (npix > b.capacity) return cudaErrorInvalidValue;
-    static unsigned g_gen = 0, g_ext = 0, g_shadow = 0, g_query = 0, g_suffix = 0;
+    static unsigned g_gen = 0, g_ext = 0, g_shadow = 0, g_query = 0, g_suffix = 0, g_ext2 = 0, g_shadow2 = 0;
     if (!g_gen) {
         g_gen = wave_grid(k_cw_generate);
-        g_ext = wave_grid(k_cw_extend);
-        g_shadow = wave_grid(k_cw_shadow);
+        g_ext = wave_grid(k_cw_extend<kLevelsFlat>);
+        g_shadow = wave_grid(k_cw_shadow<kLevelsFlat>);
+        g_ext2 = wave_grid(k_cw_extend<kLevelsTwo>);
+        g_shadow2 = wave_grid(k_cw_shadow<kLevelsTwo>);
         g_query = wave_grid(k_cache_query);
         g_suffix = wave_grid(k_cache_suffix);
     }
+    const bool two = s.two_level != 0u;
+    auto extend = [&](uint32_t cur) {
+        if (two) k_cw_extend<kLevelsTwo><<<g_ext2, 128, 0, st>>>(sv, b, cur);
+        else k_cw_extend<kLevelsFlat><<<g_ext, 128, 0, st>>>(sv, b, cur);
+    };
     // The prefix ends at the query vertex, not at the scene's depth limit
     // (k_cache_paths does not apply it either).
     DeviceScene sv = s;
@@ -533,7 +542,7 @@ cudaError_t launch_cache_frame_wavefront(const DeviceScene &s, const CacheFrameP
     ++n;
     for (uint32_t bounce = 0; bounce < p.query_depth; ++bounce) {
         const uint32_t cur = bounce & 1u;
-        k_cw_extend<<<g_ext, 128, 0, st>>>(sv, b, cur);
+        extend(cur);
         cw_shade<0>(mask, sv, b, cur, ended, st, n);
         cw_shade<1>(mask, sv, b, cur, ended, st, n);
         cw_shade<2>(mask, sv, b, cur, ended, st, n);
@@ -541,11 +550,12 @@ cudaError_t launch_cache_frame_wavefront(const DeviceScene &s, const CacheFrameP
         cw_shade<4>(mask, sv, b, cur, ended, st, n);
         cw_shade<5>(mask, sv, b, cur, ended, st, n);
         cw_shade<6>(mask, sv, b, cur, ended, st, n);
-        k_cw_shadow<<<g_shadow, 128, 0, st>>>(sv, b, ended);
+        if (two) k_cw_shadow<kLevelsTwo><<<g_shadow2, 128, 0, st>>>(sv, b, ended);
+        else k_cw_shadow<kLevelsFlat><<<g_shadow, 128, 0, st>>>(sv, b, ended);
         n += 2;
     }
     const uint32_t cur = p.query_depth & 1u;
-    k_cw_extend<<<g_ext, 128, 0, st>>>(sv, b, cur);
+    extend(cur);
     k_cache_query<<<g_query, 128, 0, st>>>(sv, p, b, cur, ended, suffix_list, suffix_count);
     n += 2;
     if (p.n_train) {

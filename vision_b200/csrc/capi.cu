@@ -75,6 +75,9 @@ struct vs_scene {
     DevBuf<float> env_tex, env_marginal_func, env_cond_func, rgb2spec;
     DevBuf<AliasEntry> env_marginal, env_cond, filter_alias;
     DevBuf<float> filter_tab;
+    // Two-level scenes: top-level leaf entries and per-instance transforms.
+    DevBuf<uint32_t> tlas_inst;
+    DevBuf<float4> inst_xf;
     // Film and per-sample radiance (scratch between the megakernel and the film pass).
     DevBuf<float4> film32, exposed;
     DevBuf<double> film64;
@@ -241,7 +244,7 @@ struct vs_scene {
         nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
         prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
         env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
-        filter_tab.free(); filter_alias.free();
+        filter_tab.free(); filter_alias.free(); tlas_inst.free(); inst_xf.free();
         film32.free(); exposed.free(); film64.free(); radiance.free(); path_counter.free(); wf.free();
         rt.free();
         cachebuf.free();
@@ -254,7 +257,8 @@ struct vs_scene {
         auto b = [](const auto &buf) { return static_cast<uint64_t>(buf.count) * sizeof(*buf.ptr); };
         return b(nodes) + b(tri_v) + b(vtx) + b(prims) + b(instances) + b(materials) + b(lights) + b(prim_alias) +
                b(light_alias) + b(prim_pmf) + b(light_pmf) + b(spd) + b(luts) + b(env_tex) + b(env_marginal_func) +
-               b(env_cond_func) + b(rgb2spec) + b(env_marginal) + b(env_cond) + b(filter_tab) + b(filter_alias);
+               b(env_cond_func) + b(rgb2spec) + b(env_marginal) + b(env_cond) + b(filter_tab) + b(filter_alias) +
+               b(tlas_inst) + b(inst_xf);
     }
 
     DeviceScene device_view() const {
@@ -288,6 +292,9 @@ struct vs_scene {
         d.ip = host.ip;
         d.node_count = static_cast<uint32_t>(host.nodes.size());
         d.prim_count = static_cast<uint32_t>(host.prim_inst.size());
+        d.two_level = host.two_level ? 1u : 0u;
+        d.tlas_inst = tlas_inst.ptr;
+        d.inst_xf = inst_xf.ptr;
         d.stats = nullptr;
         return d;
     }
@@ -329,6 +336,19 @@ uint32_t shading_classes(const HostScene &h) {
     uint32_t m = 1u;
     for (const Material &mt : h.materials) m |= 1u << (1u + mt.type);
     return m;
+}
+
+// Per instance: the world-to-object rows and (mesh root node, first
+// primitive) as bits (DeviceScene::inst_xf).
+std::vector<float4> instance_transforms(const HostScene &h) {
+    std::vector<float4> x(4 * h.instances.size());
+    for (size_t i = 0; i < h.instances.size(); ++i) {
+        const m4 &m = h.inst_w2o[i];
+        for (int r = 0; r < 3; ++r) x[4 * i + r] = make_float4(m.m[0][r], m.m[1][r], m.m[2][r], m.m[3][r]);
+        x[4 * i + 3] = make_float4(bits_float(h.blas_root[h.inst_mesh[i]]), bits_float(h.instances[i].first_prim),
+                                   bits_float(h.inst_mesh[i]), 0.0f);
+    }
+    return x;
 }
 
 int upload_scene(vs_scene *s) {
@@ -388,6 +408,12 @@ int upload_scene(vs_scene *s) {
     if (!h.filter_tab.empty()) {
         VS_CUDA(s->filter_tab.upload(h.filter_tab), "upload filter table");
         VS_CUDA(s->filter_alias.upload(h.filter_alias), "upload filter table");
+    }
+    s->tlas_inst.free();
+    s->inst_xf.free();
+    if (h.two_level) {
+        VS_CUDA(s->tlas_inst.upload(h.tlas_inst), "upload top level");
+        VS_CUDA(s->inst_xf.upload(instance_transforms(h)), "upload instances");
     }
     s->uploaded = true;
     return VS_OK;
@@ -596,6 +622,8 @@ int vs_scene_info_get(const vs_scene *s, vs_scene_info *o) {
     o->spectrum_dim = h.ip.spectrum_dim;
     o->max_depth = h.ip.max_depth;
     o->accel_built = s->built ? 1u : 0u;
+    o->two_level = h.two_level ? 1u : 0u;
+    o->mesh_count = static_cast<uint32_t>(h.meshes.size());
     return VS_OK;
 }
 
@@ -633,6 +661,11 @@ ExportView export_view(const vs_scene *s, int what) {
         case VS_EXPORT_ENV_COND: return {h.env_cond.data(), h.env_cond.size() * sizeof(AliasEntry)};
         case VS_EXPORT_ENV_COND_FUNC: return {h.env_cond_func.data(), h.env_cond_func.size() * 4};
         case VS_EXPORT_RGB2SPEC: return {rgb2spec_table(""), static_cast<size_t>(3) * 64 * 64 * 64 * 16};
+        case VS_EXPORT_MESH_POS: return {h.mesh_pos.data(), h.mesh_pos.size() * sizeof(f3)};
+        case VS_EXPORT_MESH_IDX: return {h.mesh_idx.data(), h.mesh_idx.size() * 4};
+        case VS_EXPORT_MESHES: return {h.meshes.data(), h.meshes.size() * sizeof(HostScene::MeshRec)};
+        case VS_EXPORT_INST_MESH: return {h.inst_mesh.data(), h.inst_mesh.size() * 4};
+        case VS_EXPORT_INST_W2O: return {h.inst_w2o.data(), h.inst_w2o.size() * sizeof(m4)};
         case VS_EXPORT_LUTS: {
             if (!h.needs_luts) return {nullptr, 0};
             return {microfacet_luts(), static_cast<size_t>(kLutFloats) * 4};

@@ -1370,12 +1370,12 @@ __global__ void __launch_bounds__(128) k_gi_wf_shade(const __grid_constant__ Dev
 
 __global__ void __launch_bounds__(128) k_gi_wf_extend(const __grid_constant__ DeviceScene s,
                                                       const __grid_constant__ WfBuffers w, uint32_t cur) {
-    wf::extend(RtScene{&s}, w, cur);
+    wf::extend<kLevelsFlat>(RtScene{&s}, w, cur);
 }
 
 __global__ void __launch_bounds__(128) k_gi_wf_shadow(const __grid_constant__ DeviceScene s,
                                                       const __grid_constant__ WfBuffers w, float4 *radiance) {
-    wf::shadow(RtScene{&s}, w, 0, radiance);
+    wf::shadow<kLevelsFlat>(RtScene{&s}, w, 0, radiance);
 }
 
 // Radiance of each suffix over the BSDF weight, times the chain throughput.

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <numeric>
 #include <stdexcept>
@@ -1024,9 +1025,36 @@ struct Loader {
         return mat_by_name["__black_body__"];
     }
 
+    // The object-space mesh of a new instance: an existing mesh with the same
+    // positions and triangles, or a new one.
+    uint32_t register_mesh(const MeshData &mesh) {
+        uint64_t h = 1469598103934665603ull;
+        auto mix = [&](const void *p, size_t n) {
+            const unsigned char *c = static_cast<const unsigned char *>(p);
+            for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+        };
+        mix(mesh.p.data(), mesh.p.size() * sizeof(f3));
+        mix(mesh.idx.data(), mesh.idx.size() * sizeof(uint32_t));
+        for (uint32_t m = 0; m < s.meshes.size(); ++m) {
+            const HostScene::MeshRec &r = s.meshes[m];
+            if (r.hash != h || r.vertex_count != mesh.p.size() || 3u * r.tri_count != mesh.idx.size()) continue;
+            if (std::memcmp(&s.mesh_pos[r.first_vertex], mesh.p.data(), mesh.p.size() * sizeof(f3)) == 0 &&
+                std::memcmp(&s.mesh_idx[3u * r.first_tri], mesh.idx.data(), mesh.idx.size() * sizeof(uint32_t)) == 0)
+                return m;
+        }
+        HostScene::MeshRec r{static_cast<uint32_t>(s.mesh_pos.size()), static_cast<uint32_t>(mesh.p.size()),
+                             static_cast<uint32_t>(s.mesh_idx.size() / 3), static_cast<uint32_t>(mesh.idx.size() / 3), h};
+        s.mesh_pos.insert(s.mesh_pos.end(), mesh.p.begin(), mesh.p.end());
+        s.mesh_idx.insert(s.mesh_idx.end(), mesh.idx.begin(), mesh.idx.end());
+        s.meshes.push_back(r);
+        return static_cast<uint32_t>(s.meshes.size() - 1);
+    }
+
     void add_mesh(const MeshData &mesh, const m4 &o2w, uint32_t mat, const std::string &name, const Json *emission) {
         uint32_t inst_id = static_cast<uint32_t>(s.instances.size());
         uint32_t vbase = static_cast<uint32_t>(s.pos.size());
+        s.inst_mesh.push_back(register_mesh(mesh));
+        s.inst_w2o.push_back(invert_affine(o2w));
         for (size_t i = 0; i < mesh.p.size(); ++i) {
             s.pos.push_back(xform_point(o2w, mesh.p[i]));
             s.nrm.push_back(is_zero(mesh.n[i]) ? mesh.n[i] : xform_normal(o2w, mesh.n[i]));
@@ -1265,6 +1293,14 @@ void scene_clear_geometries(HostScene &s) {
     s.prim_inst.clear();
     s.instances.clear();
     s.instance_names.clear();
+    s.mesh_pos.clear();
+    s.mesh_idx.clear();
+    s.meshes.clear();
+    s.inst_mesh.clear();
+    s.inst_w2o.clear();
+    s.tlas_inst.clear();
+    s.blas_root.clear();
+    s.two_level = false;
     std::vector<AreaLight> keep;
     std::vector<f3> keep_rgb;
     for (size_t i = 0; i < s.lights.size(); ++i)
@@ -1459,6 +1495,10 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
         throw unsupported("spectrum type '" + s.spectrum_type + "'");
     }
     ld.srgb = s.ip.srgb != 0u;
+    {
+        const Json &inst = root["render_setting"]["instancing"];
+        s.instancing = inst.is_bool() ? (inst.as_bool() ? 2 : 0) : (inst.as_string("auto") == "auto" ? 1 : 0);
+    }
     // Materials, then shapes (which reference materials by name).
     for (const Json &m : root["materials"].elements()) ld.load_material(m);
     for (const Json &sh : root["shapes"].elements()) ld.load_shape(sh);

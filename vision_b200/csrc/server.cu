@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(128) k_sv_extend(const DeviceScene *scenes, co
                                                    uint32_t cur) {
     __shared__ DeviceScene s_scene[kMaxServeScenes];
     load_scenes(scenes, s_scene);
-    wf::extend(SharedScenes{s_scene}, b, cur);
+    wf::extend<kLevelsAny>(SharedScenes{s_scene}, b, cur);
 }
 
 // Shading of class C (0: misses, 1 + MaterialType: hits of that material).
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(128) k_sv_shadow(const DeviceScene *scenes, co
                                                    uint64_t base, float4 *radiance) {
     __shared__ DeviceScene s_scene[kMaxServeScenes];
     load_scenes(scenes, s_scene);
-    wf::shadow(SharedScenes{s_scene}, b, base, radiance);
+    wf::shadow<kLevelsAny>(SharedScenes{s_scene}, b, base, radiance);
 }
 
 // NormalRadianceCollector::add_sample (normal.cpp:87-101) per job pixel over

@@ -465,6 +465,103 @@ __device__ __forceinline__ void count_traversal(const DeviceScene &s, uint32_t n
     }
 }
 
+// ---------------------------------------------------------------------------
+// Two-level traversal (instancing): the top level is the same BVH8 walk over
+// instance boxes; a leaf entry's instance takes the ray into object space
+// (world-to-object rows, explicitly rounded so that the oracle gets the same
+// bits) and walks its mesh's BVH8.  Hits report global primitive ids (the
+// instance's first primitive + the triangle's index in its mesh), and exact t
+// ties go to the lower global id as in the one-level walk.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ f3 xf_point(const float4 &r0, const float4 &r1, const float4 &r2, f3 p) {
+    return {__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(r0.x, p.x), __fmul_rn(r0.y, p.y)), __fmul_rn(r0.z, p.z)), r0.w),
+            __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(r1.x, p.x), __fmul_rn(r1.y, p.y)), __fmul_rn(r1.z, p.z)), r1.w),
+            __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(r2.x, p.x), __fmul_rn(r2.y, p.y)), __fmul_rn(r2.z, p.z)), r2.w)};
+}
+__device__ __forceinline__ f3 xf_vector(const float4 &r0, const float4 &r1, const float4 &r2, f3 v) {
+    return {__fadd_rn(__fadd_rn(__fmul_rn(r0.x, v.x), __fmul_rn(r0.y, v.y)), __fmul_rn(r0.z, v.z)),
+            __fadd_rn(__fadd_rn(__fmul_rn(r1.x, v.x), __fmul_rn(r1.y, v.y)), __fmul_rn(r1.z, v.z)),
+            __fadd_rn(__fadd_rn(__fmul_rn(r2.x, v.x), __fmul_rn(r2.y, v.y)), __fmul_rn(r2.z, v.z))};
+}
+
+// The closest hit inside instance `inst` with t below the current best.
+static __device__ __noinline__ void instance_closest(const DeviceScene &s, const RayPre &rw, uint32_t inst,
+                                                      float tmax, float &best_t, uint32_t &best_prim, float &best_u,
+                                                      float &best_v, uint32_t &visits) {
+    const float4 *x = s.inst_xf + 4u * inst;
+    const float4 r0 = __ldg(x), r1 = __ldg(x + 1), r2 = __ldg(x + 2), meta = __ldg(x + 3);
+    const uint32_t first = __float_as_uint(meta.y);
+    const RayPre r = precompute_ray(xf_point(r0, r1, r2, rw.o), xf_vector(r0, r1, r2, rw.d));
+    uint2 stack[kStackSize];
+    int sp = 0;
+    uint2 ng = make_uint2(__float_as_uint(meta.x), (1u << (24u + (0u ^ r.oct))) | 1u);
+    uint2 tg;
+    while (true) {
+        {
+            uint32_t bit = __ffs(ng.y & 0xff000000u) - 1u;
+            ng.y &= ~(1u << bit);
+            uint32_t slot = (bit - 24u) ^ r.oct;
+            uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
+            if ((ng.y & 0xff000000u) != 0u && sp < kStackSize) stack[sp++] = ng;
+            intersect_children(s.nodes, child, r, best_t * kBoxSlack, ng, tg);
+            ++visits;
+        }
+        while (tg.y & 0x00ffffffu) {
+            uint32_t bit = __ffs(tg.y & 0x00ffffffu) - 1u;
+            tg.y &= ~(1u << bit);
+            const float4 *tp = s.tri_v + static_cast<size_t>(tg.x + bit) * 3u;
+            float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t, u, v;
+            float tri_tmax = best_prim == kInvalid ? tmax : best_t * kBoxSlack;
+            if (intersect_triangle(r, a, b, c, 0.0f, tri_tmax, t, u, v)) {
+                uint32_t prim = first + __float_as_uint(a.w);
+                if (t < best_t || (t == best_t && prim < best_prim)) {
+                    best_t = t; best_prim = prim; best_u = u; best_v = v;
+                }
+            }
+        }
+        if (ng.y <= 0x00ffffffu) {
+            if (sp == 0) break;
+            ng = stack[--sp];
+        }
+    }
+}
+
+// Whether the ray hits anything inside instance `inst` with t in (0, tmax).
+static __device__ __noinline__ bool instance_any(const DeviceScene &s, const RayPre &rw, uint32_t inst, float tmax,
+                                                 uint32_t &visits) {
+    const float4 *x = s.inst_xf + 4u * inst;
+    const float4 r0 = __ldg(x), r1 = __ldg(x + 1), r2 = __ldg(x + 2), meta = __ldg(x + 3);
+    const RayPre r = precompute_ray(xf_point(r0, r1, r2, rw.o), xf_vector(r0, r1, r2, rw.d));
+    uint2 stack[kStackSize];
+    int sp = 0;
+    uint2 ng = make_uint2(__float_as_uint(meta.x), (1u << (24u + (0u ^ r.oct))) | 1u);
+    uint2 tg;
+    while (true) {
+        {
+            uint32_t bit = __ffs(ng.y & 0xff000000u) - 1u;
+            ng.y &= ~(1u << bit);
+            uint32_t slot = (bit - 24u) ^ r.oct;
+            uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
+            if ((ng.y & 0xff000000u) != 0u && sp < kStackSize) stack[sp++] = ng;
+            intersect_children(s.nodes, child, r, tmax * kBoxSlack, ng, tg);
+            ++visits;
+        }
+        while (tg.y & 0x00ffffffu) {
+            uint32_t bit = __ffs(tg.y & 0x00ffffffu) - 1u;
+            tg.y &= ~(1u << bit);
+            const float4 *tp = s.tri_v + static_cast<size_t>(tg.x + bit) * 3u;
+            float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t, u, v;
+            if (intersect_triangle(r, a, b, c, 0.0f, tmax, t, u, v)) return true;
+        }
+        if (ng.y <= 0x00ffffffu) {
+            if (sp == 0) return false;
+            ng = stack[--sp];
+        }
+    }
+}
+
 // Closest hit with t in (0, tmax).  Returns false on a miss.
 static __device__ __noinline__ bool trace_closest(const DeviceScene &s, const RayPre &r, float tmax, Hit &hit,
                                            float &t_hit) {
@@ -487,6 +584,14 @@ static __device__ __noinline__ bool trace_closest(const DeviceScene &s, const Ra
             if ((ng.y & 0xff000000u) != 0u && sp < kStackSize) stack[sp++] = ng;
             intersect_children(s.nodes, child, r, best_t * kBoxSlack, ng, tg);
             ++nodes_visited;
+        }
+        if (s.two_level) {
+            while (tg.y & 0x00ffffffu) {
+                uint32_t bit = __ffs(tg.y & 0x00ffffffu) - 1u;
+                tg.y &= ~(1u << bit);
+                instance_closest(s, r, __ldg(s.tlas_inst + tg.x + bit), tmax, best_t, best_prim, best_u, best_v,
+                                 nodes_visited);
+            }
         }
         while (tg.y & 0x00ffffffu) {
             uint32_t bit = __ffs(tg.y & 0x00ffffffu) - 1u;
@@ -537,6 +642,16 @@ static __device__ __noinline__ bool trace_any(const DeviceScene &s, const RayPre
             intersect_children(s.nodes, child, r, tmax * kBoxSlack, ng, tg);
             ++nodes_visited;
         }
+        if (s.two_level) {
+            while (tg.y & 0x00ffffffu) {
+                uint32_t bit = __ffs(tg.y & 0x00ffffffu) - 1u;
+                tg.y &= ~(1u << bit);
+                if (instance_any(s, r, __ldg(s.tlas_inst + tg.x + bit), tmax, nodes_visited)) {
+                    count_traversal(s, nodes_visited, tris_tested);
+                    return true;
+                }
+            }
+        }
         while (tg.y & 0x00ffffffu) {
             uint32_t bit = __ffs(tg.y & 0x00ffffffu) - 1u;
             tg.y &= ~(1u << bit);
@@ -584,8 +699,16 @@ __device__ __forceinline__ void trav_init(TravState &t, const RayPre &r, float t
     t.best_v = 0.0f;
 }
 
+// Which traversal code a kernel compiles: kLevelsFlat (one world-space BVH8
+// only), kLevelsTwo (instanced scenes only) or kLevelsAny (decided per ray
+// from the scene: kernels that serve several scenes at once).  Kernels of one
+// scene pick their instantiation on the host, so the flat traversal keeps its
+// registers.
+constexpr int kLevelsFlat = 0, kLevelsTwo = 1, kLevelsAny = 2;
+
 // One step of the closest-hit traversal; true when the traversal has ended
 // (the result is in t.best_*).
+template <int Levels = kLevelsFlat>
 __device__ __forceinline__ bool closest_step(const DeviceScene &s, const RayPre &r, TravState &t, uint2 *stack) {
     {
         uint32_t bit = __ffs(t.ng.y & 0xff000000u) - 1u;
@@ -594,6 +717,15 @@ __device__ __forceinline__ bool closest_step(const DeviceScene &s, const RayPre 
         uint32_t child = t.ng.x + __popc(t.ng.y & 0xffu & ((1u << slot) - 1u));
         if ((t.ng.y & 0xff000000u) != 0u && t.sp < kStackSize) stack[t.sp++] = t.ng;
         intersect_children(s.nodes, child, r, t.best_t * kBoxSlack, t.ng, t.tg);
+    }
+    if (Levels == kLevelsTwo || (Levels == kLevelsAny && s.two_level)) {
+        uint32_t visits = 0;
+        while (t.tg.y & 0x00ffffffu) {
+            uint32_t bit = __ffs(t.tg.y & 0x00ffffffu) - 1u;
+            t.tg.y &= ~(1u << bit);
+            instance_closest(s, r, __ldg(s.tlas_inst + t.tg.x + bit), t.tmax, t.best_t, t.best_prim, t.best_u,
+                             t.best_v, visits);
+        }
     }
     while (t.tg.y & 0x00ffffffu) {
         uint32_t bit = __ffs(t.tg.y & 0x00ffffffu) - 1u;
@@ -628,6 +760,7 @@ __device__ __forceinline__ Hit trav_hit(const DeviceScene &s, const TravState &t
 
 // One step of the any-hit traversal; true when it has ended, with `hit` set
 // when an intersection was found.
+template <int Levels = kLevelsFlat>
 __device__ __forceinline__ bool any_step(const DeviceScene &s, const RayPre &r, TravState &t, uint2 *stack,
                                          bool &hit) {
     {
@@ -637,6 +770,17 @@ __device__ __forceinline__ bool any_step(const DeviceScene &s, const RayPre &r, 
         uint32_t child = t.ng.x + __popc(t.ng.y & 0xffu & ((1u << slot) - 1u));
         if ((t.ng.y & 0xff000000u) != 0u && t.sp < kStackSize) stack[t.sp++] = t.ng;
         intersect_children(s.nodes, child, r, t.tmax * kBoxSlack, t.ng, t.tg);
+    }
+    if (Levels == kLevelsTwo || (Levels == kLevelsAny && s.two_level)) {
+        uint32_t visits = 0;
+        while (t.tg.y & 0x00ffffffu) {
+            uint32_t bit = __ffs(t.tg.y & 0x00ffffffu) - 1u;
+            t.tg.y &= ~(1u << bit);
+            if (instance_any(s, r, __ldg(s.tlas_inst + t.tg.x + bit), t.tmax, visits)) {
+                hit = true;
+                return true;
+            }
+        }
     }
     while (t.tg.y & 0x00ffffffu) {
         uint32_t bit = __ffs(t.tg.y & 0x00ffffffu) - 1u;

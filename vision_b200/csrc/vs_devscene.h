@@ -43,6 +43,13 @@ struct DeviceScene {
     IntegratorParams ip;
     uint32_t node_count;
     uint32_t prim_count;
+    // Two-level scenes (instancing): node 0 is the top level's root, whose
+    // leaf entries index tlas_inst (instance ids); per instance, inst_xf holds
+    // 4 float4: the world-to-object rows (x' = r.x x + r.y y + r.z z + r.w)
+    // and (root node of its mesh's BVH8, first global primitive, -, -) as bits.
+    uint32_t two_level;
+    const uint32_t *tlas_inst;
+    const float4 *inst_xf;
     // Optional traversal counters (null in normal launches): [0] ray segments
     // traced, [1] BVH8 nodes visited, [2] triangle tests.
     unsigned long long *stats;

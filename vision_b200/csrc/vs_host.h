@@ -66,6 +66,30 @@ struct HostScene {
     std::vector<Bvh8Node> nodes;
     std::vector<float> tri_v;  // 12 floats per primitive in leaf order
     uint32_t bvh_depth = 0;
+    // Instancing (Geometry::build_accel builds one BLAS per mesh and an IAS
+    // over the instances, geometry.cpp:20-52): the distinct object-space
+    // meshes (shapes with equal vertices and triangles share one) and each
+    // instance's mesh and world-to-object transform.  With instancing 2 (JSON
+    // render_setting.instancing true) whenever some mesh has several
+    // instances, and with 1 (the default, "auto") when the scene has at least
+    // 2^20 triangles and 8 times those of its distinct meshes, build_bvh8 builds a
+    // bottom-level BVH8 per mesh over its object-space
+    // triangles (tri_v w = the triangle's index in its mesh) and a top-level
+    // BVH8 over the instances' world boxes whose leaf entries index tlas_inst.
+    struct MeshRec {
+        uint32_t first_vertex, vertex_count, first_tri, tri_count;
+        uint64_t hash;
+    };
+    std::vector<f3> mesh_pos;
+    std::vector<uint32_t> mesh_idx;  // 3 per triangle, relative to the mesh's first vertex
+    std::vector<MeshRec> meshes;
+    std::vector<uint32_t> inst_mesh;  // per instance
+    std::vector<m4> inst_w2o;         // per instance
+    int instancing = 1;  // 0: one world-space BVH8; 1: auto; 2: two levels when any mesh is shared
+    bool two_level = false;
+    uint32_t tlas_root = 0;
+    std::vector<uint32_t> tlas_inst;  // top-level leaf entries: instance ids
+    std::vector<uint32_t> blas_root;  // per mesh: root node index
 };
 
 // Parses a vision_scene.json document.  Throws std::runtime_error with a

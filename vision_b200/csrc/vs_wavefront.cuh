@@ -147,7 +147,7 @@ __device__ __forceinline__ uint32_t refill(uint32_t *fetch, uint32_t n, bool act
 // kernels of one stream run in order; the class counters and this kernel's
 // fetch counter were cleared by the previous shadow pass or by the wave's
 // generate kernel).
-template <class Scenes>
+template <int Levels, class Scenes>
 __device__ __forceinline__ void extend(const Scenes &scenes, const WfBuffers &b, uint32_t cur) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         b.count[cur ^ 1u] = 0u;
@@ -175,7 +175,7 @@ __device__ __forceinline__ void extend(const Scenes &scenes, const WfBuffers &b,
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;
-        if (active && closest_step(*s, r, t, stack)) {
+        if (active && closest_step<Levels>(*s, r, t, stack)) {
             const Hit h = trav_hit(*s, t);
             const uint32_t cls = h.inst_id == kInvalid ? 0u : 1u + s->materials[s->instances[h.inst_id].mat_id].type;
             b.hit[slot] = h;
@@ -231,7 +231,7 @@ __device__ __forceinline__ void shade(const Scenes &scenes, const WfBuffers &b, 
 // contribution when unoccluded; write the radiance of paths that ended at
 // this bounce.  Clears the class counters and the extend fetch counter for
 // the next bounce (every shading pass of this one has finished).
-template <class Scenes>
+template <int Levels, class Scenes>
 __device__ __forceinline__ void shadow(const Scenes &scenes, const WfBuffers &b, uint64_t base, float4 *radiance) {
     if (blockIdx.x == 0 && threadIdx.x < kWfClasses) b.count[3 + threadIdx.x] = 0u;
     if (blockIdx.x == 0 && threadIdx.x == 32) b.count[kWfFetchExtend] = 0u;
@@ -256,7 +256,7 @@ __device__ __forceinline__ void shadow(const Scenes &scenes, const WfBuffers &b,
         }
         if (!__any_sync(0xffffffffu, active)) break;
         bool occluded = false;
-        if (active && any_step(*s, r, t, stack, occluded)) {
+        if (active && any_step<Levels>(*s, r, t, stack, occluded)) {
             const uint32_t tag = __float_as_uint(b.sh_d[i].w);
             const uint32_t slot = tag & 0x7fffffffu;
             float4 L = b.L[slot];

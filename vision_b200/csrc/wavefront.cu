@@ -41,9 +41,11 @@ __global__ void __launch_bounds__(128) k_wf_generate(const __grid_constant__ Dev
     wf::generate<N>(s, s.cam, b, frame_begin, base, n, radiance);
 }
 
+// L: kLevelsFlat or kLevelsTwo, picked on the host from the scene.
+template <int L>
 __global__ void __launch_bounds__(128) k_wf_extend(const __grid_constant__ DeviceScene s,
                                                    const __grid_constant__ WfBuffers b, uint32_t cur) {
-    wf::extend(OneScene{&s}, b, cur);
+    wf::extend<L>(OneScene{&s}, b, cur);
 }
 
 // Shading of class C (0: misses, 1 + MaterialType: hits of that material).
@@ -54,10 +56,11 @@ __global__ void __launch_bounds__(128) k_wf_shade(const __grid_constant__ Device
     wf::shade<N, C>(OneScene{&s}, b, cur, base, radiance);
 }
 
+template <int L>
 __global__ void __launch_bounds__(128) k_wf_shadow(const __grid_constant__ DeviceScene s,
                                                    const __grid_constant__ WfBuffers b, uint64_t base,
                                                    float4 *radiance) {
-    wf::shadow(OneScene{&s}, b, base, radiance);
+    wf::shadow<L>(OneScene{&s}, b, base, radiance);
 }
 
 // ---------------------------------------------------------------------------
@@ -194,7 +197,7 @@ void launch_shade(const ShadeGrids &sg, uint32_t mask, const DeviceScene &s, con
 template <int N>
 cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths, float4 *radiance,
                       const WfBuffers &b, uint32_t class_mask, cudaStream_t st, unsigned *launches) {
-    static std::atomic<int> g_gen[64], g_ext[64], g_shadow[64];
+    static std::atomic<int> g_gen[64], g_ext[64], g_shadow[64], g_ext2[64], g_shadow2[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -202,8 +205,13 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
     unsigned grid_gen, grid_ext, grid_shadow;
     ShadeGrids sg{};
     if ((e = resident_grid(k_wf_generate<N>, dev, g_gen[dev], &grid_gen)) != cudaSuccess) return e;
-    if ((e = resident_grid(k_wf_extend, dev, g_ext[dev], &grid_ext)) != cudaSuccess) return e;
-    if ((e = resident_grid(k_wf_shadow, dev, g_shadow[dev], &grid_shadow)) != cudaSuccess) return e;
+    const bool two = s.two_level != 0u;
+    if ((e = two ? resident_grid(k_wf_extend<kLevelsTwo>, dev, g_ext2[dev], &grid_ext)
+                 : resident_grid(k_wf_extend<kLevelsFlat>, dev, g_ext[dev], &grid_ext)) != cudaSuccess)
+        return e;
+    if ((e = two ? resident_grid(k_wf_shadow<kLevelsTwo>, dev, g_shadow2[dev], &grid_shadow)
+                 : resident_grid(k_wf_shadow<kLevelsFlat>, dev, g_shadow[dev], &grid_shadow)) != cudaSuccess)
+        return e;
     if ((e = shade_grid<N, 0>(dev, sg)) != cudaSuccess) return e;
     if ((e = shade_grid<N, 1>(dev, sg)) != cudaSuccess) return e;
     if ((e = shade_grid<N, 2>(dev, sg)) != cudaSuccess) return e;
@@ -239,7 +247,8 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
                 be.queue[cur] = b.binned;
                 n_launch += 3;
             }
-            k_wf_extend<<<grid_ext, 128, 0, st>>>(s, be, cur);
+            if (two) k_wf_extend<kLevelsTwo><<<grid_ext, 128, 0, st>>>(s, be, cur);
+            else k_wf_extend<kLevelsFlat><<<grid_ext, 128, 0, st>>>(s, be, cur);
             launch_shade<N, 0>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 1>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 2>(sg, mask, s, b, cur, base, radiance, st, n_launch);
@@ -253,7 +262,8 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
                 k_bin_scatter<<<grid_bin, 256, 0, st>>>(b.count + 2, nullptr, b.bin_key, b.bins, b.sh_perm);
                 n_launch += 3;
             }
-            k_wf_shadow<<<grid_shadow, 128, 0, st>>>(s, bs, base, radiance);
+            if (two) k_wf_shadow<kLevelsTwo><<<grid_shadow, 128, 0, st>>>(s, bs, base, radiance);
+            else k_wf_shadow<kLevelsFlat><<<grid_shadow, 128, 0, st>>>(s, bs, base, radiance);
             n_launch += 2;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -334,12 +334,14 @@ def many_lights(width=1920, height=1080, emitters=10000, seed=7, M_light=32, M_b
 
 def instanced_scene(width=1024, height=1024, copies=64, seed=11, subdivisions=6, patch=200, max_depth=16,
                     dimension=4, sampler="pcg"):
-    """Serving scene of ~10 M triangles: `copies` seeded copies of one mesh
-    group modelled on the large scene's geometry (a displaced icosphere with
+    """Serving scene of ~10 M triangles: `copies` instances of one mesh group
+    modelled on the large scene's geometry (a displaced icosphere with
     `subdivisions` levels, 81,920 triangles at 6, on a `patch` x `patch` grid
     tile, 80,000 triangles at 200), each with a random position on an 8 x 8
     layout, y rotation and scale, and a material drawn like the large scene's;
-    lit by the same procedural sky.  64 copies give 10,362,880 triangles."""
+    lit by the same procedural sky.  64 copies give 10,362,880 triangles of two
+    distinct meshes, so the scene is traced through a two-level BVH (one BVH8
+    per mesh under a top level over the 128 instances)."""
     import numpy as np
     rng = np.random.default_rng(seed)
     shapes, materials = [], []
@@ -358,7 +360,7 @@ def instanced_scene(width=1024, height=1024, copies=64, seed=11, subdivisions=6,
         rot = ((ca * s, 0.0, -sa * s), (0.0, s, 0.0), (sa * s, 0.0, ca * s))
         shapes.append({"type": "icosphere", "name": "copy_%d_sphere" % c,
                        "param": {"subdivisions": subdivisions, "radius": 1.0, "material": mat["name"],
-                                 "displacement": {"amplitude": 0.05, "frequency": 4.0, "seed": seed + c},
+                                 "displacement": {"amplitude": 0.05, "frequency": 4.0, "seed": seed},
                                  "transform": _cols(rot[0], rot[1], rot[2], (cx, s, cz))}})
         shapes.append({"type": "grid", "name": "copy_%d_ground" % c,
                        "param": {"nx": patch, "nz": patch, "size_x": spacing * 0.9, "size_z": spacing * 0.9,
