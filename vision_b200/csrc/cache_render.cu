@@ -519,15 +519,15 @@ cudaError_t launch_cache_frame_wavefront(const DeviceScene &s, const CacheFrameP
         g_query = wave_grid(k_cache_query);
         g_suffix = wave_grid(k_cache_suffix);
     }
+    // The prefix ends at the query vertex, not at the scene's depth limit
+    // (k_cache_paths does not apply it either).
+    DeviceScene sv = s;
+    sv.ip.max_depth = 0xffffffffu;
     const bool two = s.two_level != 0u;
     auto extend = [&](uint32_t cur) {
         if (two) k_cw_extend<kLevelsTwo><<<g_ext2, 128, 0, st>>>(sv, b, cur);
         else k_cw_extend<kLevelsFlat><<<g_ext, 128, 0, st>>>(sv, b, cur);
     };
-    // The prefix ends at the query vertex, not at the scene's depth limit
-    // (k_cache_paths does not apply it either).
-    DeviceScene sv = s;
-    sv.ip.max_depth = 0xffffffffu;
     cudaError_t e = cudaMemsetAsync(p.q_rec, 0, sizeof(CacheQueryRec) * npix, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(suffix_count, 0, sizeof(uint32_t), st);
     if (e == cudaSuccess && p.n_train) {
