@@ -317,8 +317,19 @@ int vs_restir_download(vs_scene *scene, int which, void *dst, size_t bytes);
  * busy with batches of whole frames from all admitted jobs, each batch one
  * CUDA-graph launch (work-table upload, persistent path kernel, film pass).
  * A job's film equals vs_render of the same scene, camera, resolution and
- * frames [frame_begin, frame_begin + spp).  Scenes must stay alive while the
- * server uses them and must use 4 hero wavelengths.  vs_server_destroy waits
+ * frames [frame_begin, frame_begin + spp).  Path-tracing scenes must use 4
+ * hero wavelengths.
+ * Real-time scenes (integrator "rt") are served with their ReSTIR buffers
+ * resident: vs_server_add_scene allocates the scene's reservoirs, surfaces,
+ * film and frame scratch at its resolution and counts them with the scene.
+ * A job on such a scene renders spp ReSTIR frames (frame indices frame_begin
+ * ..., one frame per batch, jobs of one scene in submission order) at the
+ * scene's resolution with the job's camera; its film is the running mean of
+ * its frames and equals vs_camera_set + vs_restir_frame(frame_begin + i, i)
+ * on the scene.  The reservoirs and the previous camera carry over from one
+ * job to the next, so a client's successive jobs continue one temporal
+ * history; the server drives the scene's camera and film while it holds it.
+ * Scenes must stay alive while the server uses them.  vs_server_destroy waits
  * for submitted jobs. */
 typedef struct vs_server vs_server;
 typedef struct vs_job_desc {

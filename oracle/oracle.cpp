@@ -958,6 +958,24 @@ static void env_eval(const Scene &sc, V3 dir, const Swl &w, float *L, float &pdf
     pdf = st == 0.0f ? 0.0f : p;
 }
 
+// Point / spot light radiance at p_ref (point.cpp:36-41, spot.cpp:47-67):
+// colour * scale / d^2, times the spot falloff.
+static void delta_L(const AreaLight &L, V3 p_ref, const Swl &w, float *out) {
+    V3 lp = {L.pos[0], L.pos[1], L.pos[2]};
+    V3 wu = sub(p_ref, lp);
+    float g = 1.0f / dot(wu, wu);
+    if (L.shape == 2) {
+        float ct = dot(V3{L.dir[0], L.dir[1], L.dir[2]}, normalize(wu));
+        float c = std::min(std::max(ct, L.cos_angle), L.cos_start);
+        float range = L.cos_start - L.cos_angle;
+        float f = range > 0.0f ? (c - L.cos_angle) / range : (ct >= L.cos_start ? 1.0f : 0.0f);
+        float f2 = f * f;
+        g *= f2 * f2;
+    }
+    emitter(L, w, out);
+    for (int i = 0; i < w.n; ++i) out[i] *= g;
+}
+
 static float alias_cont(const Alias *tab, uint32_t size, float u, uint32_t &ofs) {
     u = u * static_cast<float>(size);
     uint32_t idx = std::min(static_cast<uint32_t>(u), size - 1u);
@@ -966,6 +984,35 @@ static float alias_cont(const Alias *tab, uint32_t size, float u, uint32_t &ofs)
     float ur = keep ? std::min(u / tab[idx].prob, kOneMinusEps) : std::min((1.0f - u) / (1.0f - tab[idx].prob), kOneMinusEps);
     ofs = keep ? idx : tab[idx].alias;
     return (static_cast<float>(ofs) + ur) / static_cast<float>(size);
+}
+
+// SphericalMap::sample_only (spherical.cpp:127-132): map coordinates only.
+static void env_sample_uv(const Scene &sc, float ux, float uy, float &fu, float &fv) {
+    uint32_t iv, iu;
+    fv = alias_cont(static_cast<const Alias *>(sc.s->env_marginal), sc.env.height, uy, iv);
+    fu = alias_cont(static_cast<const Alias *>(sc.s->env_cond) + (size_t)iv * sc.env.width, sc.env.width, ux, iu);
+}
+
+// SphericalMap::evaluate_point -> evaluate (spherical.cpp:105-125,134-141):
+// radiance, solid-angle pdf from the map's PDF(uv), world direction.
+static void env_eval_uv(const Scene &sc, float u, float v, const Swl &w, float *L, float &pdf, V3 &wd) {
+    float theta = v * kPi, phi = u * 2.0f * kPi;
+    float st = std::sin(theta), ct = std::cos(theta);
+    V3 local = {st * std::cos(phi), st * std::sin(phi), ct};
+    wd = normalize(mat_vec(sc.env.o2w, local));
+    float p = env_pdf_map(sc, u, v) / (2.0f * kPi * kPi * st);
+    pdf = std::isinf(p) ? 0.0f : p;
+    env_L(sc, u, v, w, L);
+}
+
+// Environment::convert_to_bary (spherical.cpp:70-73).
+static void env_dir_uv(const Scene &sc, V3 dir, float &u, float &v) {
+    V3 local = normalize(mat_vec(sc.env.w2o, dir));
+    float theta = std::acos(std::min(std::max(local.z, -1.0f), 1.0f));
+    float phi = std::atan2(local.y, local.x);
+    if (phi < 0.0f) phi += 2.0f * kPi;
+    u = phi * (1.0f / (2.0f * kPi));
+    v = theta * kInvPi;
 }
 
 struct LS {
@@ -1010,21 +1057,9 @@ static LS sample_light(const Scene &sc, const It &it, float ul, float ux, float 
     if (L.shape != 0) {
         // Point / spot light (point.cpp:36-41, spot.cpp:47-67): colour * scale
         // / d^2 (times the spot falloff); pdf -pmf marks the delta light.
-        V3 lp = {L.pos[0], L.pos[1], L.pos[2]};
-        V3 wu = sub(it.pos, lp);
-        float g = 1.0f / dot(wu, wu);
-        if (L.shape == 2) {
-            float ct = dot(V3{L.dir[0], L.dir[1], L.dir[2]}, normalize(wu));
-            float c = std::min(std::max(ct, L.cos_angle), L.cos_start);
-            float range = L.cos_start - L.cos_angle;
-            float f = range > 0.0f ? (c - L.cos_angle) / range : (ct >= L.cos_start ? 1.0f : 0.0f);
-            float f2 = f * f;
-            g *= f2 * f2;
-        }
-        emitter(L, w, ls.L);
-        for (int i = 0; i < w.n; ++i) ls.L[i] *= g;
+        delta_L(L, it.pos, w, ls.L);
         ls.pdf = -pmf_l;
-        ls.p = lp;
+        ls.p = V3{L.pos[0], L.pos[1], L.pos[2]};
         return ls;
     }
     float ur = ux;

@@ -24,7 +24,10 @@ def test_two_level_hits_bit_exact(vb, gpu_ctx, case):
         sc = _forced_box_room(width=16, height=16)
         lo, hi = [-0.45, 0.05, -0.45], [0.45, 0.95, 0.45]
     else:
+        # A reduced instanced scene: below the automatic two-level threshold
+        # (2^20 triangles), so instancing is asked for.
         sc = scenes.instanced_scene(width=16, height=16, copies=16, subdivisions=5, patch=100)
+        sc['render_setting']['instancing'] = True
         lo, hi = [-9.0, 0.05, -9.0], [9.0, 3.0, 9.0]
     s = vb.Scene(gpu_ctx, sc).build_accel()
     assert s.info()['two_level'] == 1

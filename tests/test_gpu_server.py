@@ -1,7 +1,8 @@
 """Render-job server: a job's film equals vs_render of the same scene, camera,
 resolution and frames; the same job gives the same film alone and inside a
-mix of concurrent jobs of other scenes, resolutions and spp; admission keeps
-the job-slot limit; latency statistics are ordered."""
+mix of concurrent jobs of other scenes, resolutions and spp; real-time jobs
+continue their scene's resident ReSTIR history; admission keeps the job-slot
+limit; latency statistics are ordered."""
 import numpy as np
 import pytest
 
@@ -56,6 +57,43 @@ def test_server_same_alone_and_in_mix(vb, gpu_ctx, served):
     assert st['batches'] > 1 and st['graph_launches'] == st['batches']
     assert st['p50_ms'] <= st['p95_ms'] <= st['p99_ms'] <= st['max_ms']
     srv.close()
+
+
+def test_server_realtime_jobs_keep_reservoirs_resident(vb, gpu_ctx, served):
+    # Real-time (ReSTIR) jobs on a resident rt scene: each job renders its
+    # frames into the scene's film with the scene's reservoirs resident, so
+    # consecutive jobs continue one temporal history (job k's camera is the
+    # previous camera of job k + 1's first frame).  Each job's film equals
+    # vs_restir_frame run directly on a twin scene with the same cameras,
+    # frame indices and film restarts, while path-tracing jobs of another
+    # scene share the batches.
+    box, _ = served
+    w, h = 48, 32
+    sc = scenes.many_lights(w, h, emitters=200, seed=5, M_light=8, history_limit=20, spatial_neighbours=5,
+                            spatial_radius=8.0, max_depth=4)
+    rt = vb.Scene(gpu_ctx, sc).build_accel()
+    twin = vb.Scene(gpu_ctx, sc).build_accel()
+    cams = scenes.camera_spline(3, seed=3)
+    srv = vb.Server(gpu_ctx, hbm_budget=4 << 30, max_jobs=8, paths_per_batch=1 << 15)
+    r, b = srv.add_scene(rt), srv.add_scene(box)
+    assert srv.stats()['resident_bytes'] > 64 * w * h * 9  # reservoirs and surfaces count against the budget
+    jobs, pt_jobs = [], []
+    for k in range(3):
+        jobs.append(srv.submit(r, w, h, 3, frame_begin=3 * k, c2w=cams[k], fov_y=40.0))
+        pt_jobs.append(srv.submit(b, 32, 32, 4, frame_begin=k))
+    got = [srv.result(j, timeout=120) for j in jobs]
+    for j in pt_jobs:
+        srv.result(j, timeout=120)
+    with pytest.raises(vb.VisionError):
+        srv.submit(r, w + 8, h, 1)  # real-time jobs render at their scene's resolution
+    st = srv.stats()
+    assert st['completed'] == 6
+    srv.close()
+    for k in range(3):
+        twin.set_camera(cams[k], 40.0)
+        for i in range(3):
+            twin.restir_frame(3 * k + i, i)
+        assert np.array_equal(got[k], twin.film()), k
 
 
 def test_server_admission_limit(vb, gpu_ctx, served):

@@ -172,3 +172,41 @@ def test_oracle_restir_deterministic(vb, host_ctx):
     b = [ort.buffer('film', np.dtype(('<f4', 4))).copy() for _, ort, _ in _oracle_frames(vb, host_ctx, sc, cams, 32, 24, 4)]
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+def test_oracle_restir_direct_light_is_unbiased_for_environment_and_delta_lights(vb, host_ctx):
+    # ReSTIR DI draws light candidates through the generic light sampler: the
+    # environment (map coordinates, solid-angle pdf), point and spot lights
+    # (MIS weight 1 / M_light) beside area lights, and BSDF candidates that
+    # escape to the environment.  With temporal and spatial reuse off, a frame
+    # is an unbiased estimate of the direct light at the primary hit, so its
+    # mean over frames must match the path tracer at max_depth 1 with light
+    # sampling only (mis_mode 1), up to noise (a z-test on the image mean).
+    import copy
+    w, h, frames = 48, 32, 200
+    sc = scenes.many_lights(w, h, emitters=20, seed=5, M_light=4, max_depth=4, gi=False)
+    sc['shapes'] = [x for x in sc['shapes'] if x['name'] != 'back']
+    sc['light_sampler']['param']['lights'] = [{'type': 'spherical', 'param': {
+        'color': {'channels': 'xyz', 'node': {'type': 'sky', 'param': {
+            'width': 64, 'height': 32, 'sun_elevation': 20.0, 'sun_azimuth': 180.0, 'sun_radius': 8.0,
+            'sun_peak': 40.0}}}, 'scale': 1.0}}] + scenes.point_light_room()['light_sampler']['param']['lights']
+    d = sc['integrator']['param']['direct']
+    d['spatial'] = {'open': False}
+    d['temporal'] = {'open': False}
+    s = vb.Scene(host_ctx, sc).build_accel()
+    ort = oracle.OracleRestir(oracle.OracleScene(s), w, h)
+    cam = s.export('camera').copy()
+    means, acc, picked = [], 0.0, set()
+    for f in range(frames):
+        ort.frame(cam, s.restir_params(f), 0, 4)
+        x = ort.buffer('di_radiance', np.dtype(('<f4', 4)))[..., :3]
+        means.append(x.mean())
+        picked |= set(np.unique(ort.buffer('di_reservoirs', vb.DI_RESERVOIR_DTYPE)['light_index']).tolist())
+    n_lights = s.export('integrator', np.uint32)[9]
+    # Reservoirs chose the sky (the last light), the point and the spot light.
+    assert {n_lights - 1, n_lights - 2, n_lights - 3} <= picked
+    pt = copy.deepcopy(sc)
+    pt['integrator'] = {'type': 'pt', 'param': {'max_depth': 1, 'min_depth': 5, 'rr_threshold': 1.0, 'mis_mode': 1}}
+    ref = oracle.OracleScene(vb.Scene(host_ctx, pt).build_accel()).render(0, 1024, threads=4)[..., :3].mean()
+    rt, se = np.mean(means), np.std(means) / np.sqrt(frames)
+    assert abs(rt - ref) <= 4.0 * se + 0.003 * ref, (rt, ref, se)

@@ -248,11 +248,17 @@ def test_point_and_spot_light_records(vb, host_ctx):
     np.testing.assert_allclose(pmf, L[:, 7] / L[:, 7].sum(), rtol=1e-5)
 
 
-def test_delta_lights_with_the_rt_integrator_are_unsupported(vb, host_ctx):
-    sc = scenes.point_light_room(8, 8)
+def test_rt_integrator_takes_delta_and_environment_lights(vb, host_ctx):
+    # ReSTIR DI draws its candidates through the generic light sampler, so
+    # point, spot and environment lights load with the rt integrator.
+    sc = scenes.point_light_room(8, 8, dimension=3)
     sc['integrator'] = {'type': 'rt', 'param': {'max_depth': 4}}
-    with pytest.raises(vb.UnsupportedError, match='point and spot'):
-        vb.Scene(host_ctx, sc)
+    sc['light_sampler']['param']['lights'].append(scenes.large_scene()['light_sampler']['param']['lights'][0])
+    sc['light_sampler']['param']['lights'][-1]['param']['color']['node']['param'].update(width=32, height=16)
+    s = vb.Scene(host_ctx, sc)
+    assert s.info()['light_count'] == 3  # the area light, the point and the spot
+    # The light sampler draws over those and the sky.
+    assert s.export('integrator', np.uint32)[9] == 4
 
 
 def test_default_spectrum_is_srgb(vb, host_ctx):

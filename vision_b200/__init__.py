@@ -468,7 +468,8 @@ class Scene:
 
 class Server:
     """Render-job server (vs_server_*): continuous batching of path-tracing
-    jobs over resident scenes."""
+    jobs over resident scenes; jobs on a real-time (rt) scene run ReSTIR
+    frames with the scene's reservoirs resident from job to job."""
 
     def __init__(self, ctx, hbm_budget=150 << 30, max_jobs=64, paths_per_batch=1 << 23):
         h = ctypes.c_void_p()

@@ -71,7 +71,10 @@ def up_to_date():
 
 
 def build(force=False, verbose=False):
-    if not force and up_to_date():
+    # The digest of the sources as they are now: a source edited while the
+    # build runs leaves the library stale, not stamped as current.
+    lib_digest = _library_digest()
+    if not force and _stamp_ok(LIB, lib_digest):
         return LIB
     os.makedirs(BUILD, exist_ok=True)
 
@@ -96,7 +99,7 @@ def build(force=False, verbose=False):
     subprocess.run([nvcc()] + ARCH + ['-shared', '-o', tmp] + objs + ['-lcudart', '-lpthread'], check=True)
     os.replace(tmp, LIB)
     with open(LIB + '.stamp', 'w') as f:
-        f.write(_library_digest())
+        f.write(lib_digest)
     return LIB
 
 

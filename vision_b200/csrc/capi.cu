@@ -261,6 +261,22 @@ struct vs_scene {
                b(tlas_inst) + b(inst_xf);
     }
 
+    // Device memory of the per-pixel buffers a real-time frame keeps resident:
+    // reservoirs, surfaces and the other ReSTIR buffers, the film and, on the
+    // wavefront schedule, the path slots.
+    uint64_t rt_resident_bytes() const {
+        auto b = [](const auto &buf) { return static_cast<uint64_t>(buf.count) * sizeof(*buf.ptr); };
+        uint64_t n = b(film32) + b(exposed) + b(radiance);
+        for (int k = 0; k < 2; ++k) n += b(rt.surf[k]) + b(rt.ext[k]) + b(rt.di[k]) + b(rt.gi[k]);
+        n += b(rt.hit_bsdf) + b(rt.motion) + b(rt.di_pass) + b(rt.gi_pass) + b(rt.gi_init) + b(rt.di_radiance) +
+             b(rt.gi_radiance) + b(rt.di_stage) + b(rt.di_ray) + b(rt.di_hit) + b(rt.di_list) + b(rt.di_count) +
+             b(rt.gs_nb) + b(rt.gs_ray) + b(rt.gs_vis) + b(rt.gs_list) + b(rt.gs_count);
+        n += b(wf.o) + b(wf.d) + b(wf.tp) + b(wf.lam) + b(wf.pdf) + b(wf.L) + b(wf.sh_o) + b(wf.sh_d) + b(wf.sh_c) +
+             b(wf.st) + b(wf.hit) + b(wf.q0) + b(wf.q1) + b(wf.tq) + b(wf.count) + b(wf.bin_key) + b(wf.bins) +
+             b(wf.binned) + b(wf.sh_perm);
+        return n;
+    }
+
     DeviceScene device_view() const {
         DeviceScene d{};
         d.nodes = reinterpret_cast<const uint4 *>(nodes.ptr);
@@ -1086,21 +1102,12 @@ int rt_ensure(vs_scene *s, cudaStream_t st) {
     return VS_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void *stream) {
-    if (!s) return VS_E_INVALID;
+// One ReSTIR frame on `st`; the caller holds s->mu and has checked the
+// scene.  `launches` gets the kernels launched.
+int restir_frame_locked(vs_scene *s, uint32_t frame_index, uint32_t film_index, cudaStream_t st,
+                        unsigned *launches) {
     vs_context *ctx = s->ctx;
-    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
-    std::lock_guard<std::mutex> lock(s->mu);
-    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_restir_frame");
-    if (!s->host.rt) return fail(ctx, VS_E_STATE, "scene integrator is not \"rt\"");
-    if (film_index != 0 && film_index != s->film_frames)
-        return fail(ctx, VS_E_STATE, "film_index must continue the film or restart at 0");
     VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-    cudaStream_t st = pick_stream(s, stream);
     int rc = ensure_film(s);
     if (rc != VS_OK) return rc;
     rc = rt_ensure(s, st);
@@ -1132,6 +1139,7 @@ int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void
                    wavefront ? s->radiance.ptr : nullptr, classes, st, &n),
             "restir launch");
     add_launches(n);
+    if (launches) *launches += n;
     if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
     if (st != ctx->stream) {
         if (!s->ev_join) VS_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "join event");
@@ -1149,6 +1157,42 @@ int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void
     s->film64_valid = false;
     s->film64sq_valid = false;
     return VS_OK;
+}
+
+// The per-pixel buffers a real-time frame uses, allocated up front so that a
+// server can count them and its scheduler allocates nothing; the caller holds
+// s->mu.
+int restir_prepare_locked(vs_scene *s) {
+    vs_context *ctx = s->ctx;
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    int rc = ensure_film(s);
+    if (rc != VS_OK) return rc;
+    rc = rt_ensure(s, ctx->stream);
+    if (rc != VS_OK) return rc;
+    const uint64_t npix = static_cast<uint64_t>(s->host.cam.width) * s->host.cam.height;
+    if (s->schedule == VS_SCHEDULE_WAVEFRONT && npix <= kWfWaveSlots) {
+        VS_CUDA(s->wf.ensure(static_cast<uint32_t>(npix), false), "wavefront slots alloc");
+        VS_CUDA(s->radiance.alloc(npix), "radiance alloc");
+    }
+    VS_CUDA(cudaStreamSynchronize(ctx->stream), "restir prepare");
+    return VS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vs_restir_frame(vs_scene *s, uint32_t frame_index, uint32_t film_index, void *stream) {
+    if (!s) return VS_E_INVALID;
+    vs_context *ctx = s->ctx;
+    if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_restir_frame");
+    if (!s->host.rt) return fail(ctx, VS_E_STATE, "scene integrator is not \"rt\"");
+    if (film_index != 0 && film_index != s->film_frames)
+        return fail(ctx, VS_E_STATE, "film_index must continue the film or restart at 0");
+    VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return restir_frame_locked(s, frame_index, film_index, pick_stream(s, stream), nullptr);
 }
 
 int vs_restir_reset(vs_scene *s) {
@@ -1244,14 +1288,47 @@ int vs_server_add_scene(vs_server *s, vs_scene *scene, uint32_t *scene_id) {
     if (!s || !scene || !scene_id) return VS_E_INVALID;
     DeviceScene dv;
     uint64_t bytes = 0;
+    bool rt = false;
+    Camera cam{};
+    const float4 *film = nullptr;
     {
         std::lock_guard<std::mutex> lock(scene->mu);
         if (!scene->uploaded) return s->fail(VS_E_STATE, "vs_scene_build_accel must precede vs_server_add_scene");
-        dv = scene->device_view();
-        bytes = scene->device_bytes();
+        if (scene->ctx->device != s->ctx->device) return s->fail(VS_E_INVALID, "scene on another device");
+        rt = scene->host.rt;
+        if (rt) {
+            // The real-time buffers are allocated now and stay resident: the
+            // scheduler allocates nothing and the budget counts them.
+            int rc = restir_prepare_locked(scene);
+            if (rc != VS_OK) return s->fail(rc, vs_last_error(scene->ctx));
+            bytes = scene->device_bytes() + scene->rt_resident_bytes();
+            cam = scene->host.cam;
+            film = scene->film32.ptr;
+        } else {
+            dv = scene->device_view();
+            bytes = scene->device_bytes();
+        }
     }
     std::string err;
-    int rc = server_add_scene(s->impl, dv, bytes, scene_id, err);
+    int rc;
+    if (rt) {
+        RtServeHooks hooks;
+        hooks.film = film;
+        // One frame with the job's sensor, under the scene's lock.  The
+        // scene's camera becomes the job's, so the frame's motion vectors and
+        // temporal reuse see the previous frame's camera (the last job's).
+        hooks.frame = [scene](const Camera &c, uint32_t frame, uint32_t film_index, cudaStream_t st,
+                              unsigned *launches, std::string &e) {
+            std::lock_guard<std::mutex> lock(scene->mu);
+            scene->host.cam = c;
+            int r = restir_frame_locked(scene, frame, film_index, st, launches);
+            if (r != VS_OK) e = vs_last_error(scene->ctx);
+            return r;
+        };
+        rc = server_add_rt_scene(s->impl, cam, bytes, std::move(hooks), scene_id, err);
+    } else {
+        rc = server_add_scene(s->impl, dv, bytes, scene_id, err);
+    }
     return rc == VS_OK ? VS_OK : s->fail(rc, err);
 }
 

@@ -292,26 +292,59 @@ __device__ __forceinline__ float light_select_pmf(const DeviceScene &s, uint32_t
                                                     : 1.0f / static_cast<float>(s.ip.light_count);
 }
 
-// LightSampler::evaluate_point for an area-light sample point
-// (lightsampler.cpp:230-240, AreaLight::evaluate_point area.cpp:157-167):
-// L = Le * G, pdf in area measure = PDF_pos * PMF(prim) * PMF(light), and the
-// robust light position.
+// LightSampler::evaluate_point (lightsampler.cpp:230-240) of a stored light
+// sample, multiplied by the light's selection pmf:
+//  * area light (AreaLight::evaluate_point, area.cpp:157-167): L = Le * G, pdf
+//    in area measure = PDF_pos * PMF(prim), and the robust light position;
+//  * point or spot light (IPointLight::evaluate_point, light.h:237-246): L =
+//    Le at p_ref, pdf = -1 (the delta marker), the light's position;
+//  * environment (SphericalMap::evaluate_point, spherical.cpp:134-141): the
+//    map coordinates in (bary_u, bary_v) give the direction, L and the
+//    solid-angle pdf; the point lies world_diameter along the direction.
+// lp carries the LightEvalContext (compute_light_eval_context) that
+// Light::PDF_point reads: the point and its normal.
+enum : uint32_t { kPointArea = 0u, kPointDelta = 1u, kPointEnv = 2u };
 struct PointEval {
     RSpec L;
     float pdf;
     f3 p_light;
     LightPoint lp;
+    uint32_t kind;
 };
 __device__ __forceinline__ PointEval eval_light_point(const DeviceScene &s, f3 p_ref, uint32_t light, uint32_t prim,
                                                       float bu, float bv, const RWl &wl) {
     PointEval e;
+    const float pmf = light_select_pmf(s, light);
+    if (s.has_env && light == s.env_index) {
+        f3 wd;
+        env_eval_uv<RN>(s, bu, bv, wl, e.L, e.pdf, wd);
+        e.pdf *= pmf;
+        e.p_light = p_ref + wd * s.env.world_diameter;
+        e.lp.pos = e.p_light;
+        e.lp.ng = -wd;
+        e.lp.area = 0.0f;
+        e.kind = kPointEnv;
+        return e;
+    }
     AreaLight L = s.lights[light];
+    if (L.shape != kLightArea) {
+        const f3 lpos = make3(L.pos[0], L.pos[1], L.pos[2]);
+        e.L = delta_light_L<RN>(L, p_ref, wl);
+        e.pdf = -1.0f * pmf;
+        e.p_light = lpos;
+        e.lp.pos = lpos;
+        e.lp.ng = normalize(p_ref - lpos);
+        e.lp.area = 0.0f;
+        e.kind = kPointDelta;
+        return e;
+    }
     e.lp = light_point(s, L.first_prim + prim, bu, bv);
     e.L = area_Le(L, e.lp, p_ref, wl) * light_G(p_ref, e.lp);
     float pmf_prim = s.prim_pmf[L.alias_offset + prim];
-    e.pdf = (1.0f / e.lp.area) * pmf_prim * light_select_pmf(s, light);
+    e.pdf = (1.0f / e.lp.area) * pmf_prim * pmf;
     f3 w = p_ref - e.lp.pos;
     e.p_light = offset_ray_origin(e.lp.pos, dot(e.lp.ng, w) > 0.0f ? e.lp.ng : -e.lp.ng);
+    e.kind = kPointArea;
     return e;
 }
 
@@ -335,12 +368,17 @@ __device__ VS_OUTLINE float di_p_hat(const DeviceScene &s, const Interaction &it
     e.lp.pos = make3(0.0f);
     e.lp.ng = make3(0.0f);
     e.lp.area = 0.0f;
+    e.kind = kPointArea;
     bool valid = smp.light_index != kInvalid;
     if (valid) e = eval_light_point(s, it.pos, smp.light_index, smp.prim_id, smp.bary_u, smp.bary_v, wl);
     f3 wi = normalize(e.p_light - it.pos);
     BsdfEval<RN> ev = bsdf.evaluate(it.wo, wi, nullptr);
     RSpec f = ev.f * e.L;
-    if (bsdf_pdf_point) *bsdf_pdf_point = valid ? pdf_point(ev.pdf, e.lp.ng, it.pos - e.lp.pos) : 0.0f;
+    // LightSampler::PDF_point: the environment keeps the solid-angle pdf
+    // (spherical.cpp:143-146); area and delta lights convert it to area
+    // measure at their LightEvalContext (light.h:141-146).
+    if (bsdf_pdf_point)
+        *bsdf_pdf_point = !valid ? 0.0f : e.kind == kPointEnv ? ev.pdf : pdf_point(ev.pdf, e.lp.ng, it.pos - e.lp.pos);
     if (out) *out = e;
     if (f_out) *f_out = f;
     return lum3(vec3(f));
@@ -446,26 +484,43 @@ __device__ __forceinline__ DiReservoir di_ris_lights(const DeviceScene &s, const
                                                      const Bsdf<RN, VS_RT_MATERIALS> &bsdf) {
     DiReservoir ret = di_empty();
     float Ml = static_cast<float>(p.M_light), Mb = static_cast<float>(p.M_bsdf);
-    // LightSampler::sample_only (lightsampler.cpp:218-228), AreaLight::sample_only
-    // (area.cpp:134-140): one light candidate from its three draws, with its
-    // target pdf and RIS weight.
+    // LightSampler::sample_only (lightsampler.cpp:218-228): one light candidate
+    // from its three draws, with its target pdf and RIS weight.  The
+    // light-surface point is AreaLight::sample_only's primitive and
+    // barycentrics (area.cpp:134-140), the environment's map coordinates
+    // (spherical.cpp:127-132), or Light::sample_only's raw pair for a point or
+    // spot light (light.h:177-182).  A delta light's negative pdf selects the
+    // MIS weight 1 / M_light (direct.cpp:180-186).
     auto candidate = [&](float u_sel, f2 u, DiReservoir &cand, float &weight) {
         cand = di_empty();
         uint32_t li = select_light(s, u_sel);
-        AreaLight L = s.lights[li];
-        float ux = u.x;
-        uint32_t local = alias_sample(s.prim_alias + L.alias_offset, L.prim_count, u.x, &ux);
-        float su0 = sqrtf(ux);
         cand.light_index = li;
-        cand.prim_id = local;
-        cand.bary_u = 1.0f - su0;
-        cand.bary_v = u.y * su0;
+        cand.prim_id = 0u;
+        if (s.has_env && li == s.env_index) {
+            const f2 uv = env_sample_uv(s, u);
+            cand.bary_u = uv.x;
+            cand.bary_v = uv.y;
+        } else {
+            AreaLight L = s.lights[li];
+            if (L.shape == kLightArea) {
+                float ux = u.x;
+                uint32_t local = alias_sample(s.prim_alias + L.alias_offset, L.prim_count, u.x, &ux);
+                float su0 = sqrtf(ux);
+                cand.prim_id = local;
+                cand.bary_u = 1.0f - su0;
+                cand.bary_v = u.y * su0;
+            } else {
+                cand.bary_u = u.x;
+                cand.bary_v = u.y;
+            }
+        }
         PointEval ls;
         float bsdf_pdf_point = 0.0f;
         cand.p_hat = di_p_hat(s, it, bsdf, cand, wl, &bsdf_pdf_point, &ls, nullptr);
         st3(cand.pos, ls.p_light);
-        float light_pdf = ls.pdf;
-        float mis = light_pdf / (Ml * light_pdf + Mb * bsdf_pdf_point);
+        const bool delta = ls.pdf < 0.0f;
+        const float light_pdf = delta ? -ls.pdf : ls.pdf;
+        const float mis = delta ? 1.0f / Ml : light_pdf / (Ml * light_pdf + Mb * bsdf_pdf_point);
         weight = safe_weight(mis, cand.p_hat, 1.0f / light_pdf) * lum_tp;
     };
     // Candidates in pairs: the draws of a pair are taken in the reference's
@@ -551,6 +606,24 @@ __device__ __forceinline__ void di_bsdf_candidate(const DeviceScene &s, const Rt
             eval_pdf = le_pdf;
             f = eval_f * Le;
         }
+    } else if (s.has_env) {
+        // LightSampler::evaluate_miss_point (lightsampler.cpp:315-327): the
+        // environment along the BSDF direction; the candidate keeps the
+        // BSDF's solid-angle pdf and stores the direction's map coordinates
+        // and the point world_diameter along it.
+        const f3 wd = make3(hb.wx, hb.wy, hb.wz);
+        const f3 pl = it.pos + wd * s.env.world_diameter;
+        RSpec Le;
+        float env_pdf;
+        env_eval<RN>(s, normalize(pl - it.pos), wl, Le, env_pdf);
+        light_pdf_point = env_pdf * light_select_pmf(s, s.env_index);
+        const f2 uv = env_dir_uv(s, wd);
+        cand.light_index = s.env_index;
+        cand.prim_id = 0u;
+        cand.bary_u = uv.x;
+        cand.bary_v = uv.y;
+        st3(cand.pos, pl);
+        f = eval_f * Le;
     }
     cand.p_hat = lum3(vec3(f));
     float bp = eval_pdf;
@@ -1105,6 +1178,12 @@ __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
             b.di_list[wf::queue_push(b.di_count)] = idx;
             return;
         }
+    } else if (s.has_env) {
+        // LightSampler::evaluate_miss_wi along the camera ray (direct.cpp:659-668).
+        RSpec Le;
+        float env_pdf;
+        env_eval<RN>(s, normalize((ro + rd) - ro), wl, Le, env_pdf);
+        L = linear_srgb<RN>(Le, wl);
     }
     b.di_radiance[idx] = make_float4(L.x, L.y, L.z, 1.0f);
 }

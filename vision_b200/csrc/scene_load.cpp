@@ -1454,7 +1454,6 @@ RtStage load_rt_stage(const Json &d) {
 // paths of the indirect samples.
 void load_rt(const Json &ip, HostScene &s) {
     if (s.ip.spectrum_dim != 3) throw unsupported("rt integrator with a hero dimension other than 3");
-    if (s.has_env) throw unsupported("environment light with the rt integrator");
     if (s.ip.max_depth < 3) throw unsupported("rt integrator with max_depth below 3");
     s.rt = true;
     s.ip.max_depth -= 1u;
@@ -1531,11 +1530,7 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     s.ip.min_depth = ip["min_depth"].as_uint(5u);
     s.ip.rr_threshold = ip["rr_threshold"].as_float(1.0f);
     s.ip.mis_mode = ip["mis_mode"].as_uint(0u);
-    if (it == "rt") {
-        for (const AreaLight &L : s.lights)
-            if (L.shape != kLightArea) throw unsupported("point and spot lights with the rt integrator");
-        load_rt(ip, s);
-    }
+    if (it == "rt") load_rt(ip, s);
     // Sampler.
     const Json &smp = root["sampler"];
     std::string st = smp["type"].as_string("independent");

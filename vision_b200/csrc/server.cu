@@ -183,7 +183,9 @@ struct Job {
     uint64_t id = 0;
     ServeJob desc{};
     uint32_t npix = 0;
-    uint64_t bytes = 0;
+    uint64_t bytes = 0;       // device memory counted against the budget
+    uint64_t host_bytes = 0;  // the film on the host (float4 per pixel)
+    bool rt = false;          // frames of a resident real-time scene
     float4 *film = nullptr;
     float *host = nullptr;   // pinned result
     uint32_t scheduled = 0;  // frames put into batches
@@ -209,6 +211,8 @@ public:
     DeviceScene *d_scenes = nullptr;
     uint32_t nscenes = 0;
     Camera scene_cam[kMaxServeScenes];
+    bool scene_rt[kMaxServeScenes] = {};
+    RtServeHooks rt_hooks[kMaxServeScenes];
     ServeTable *h_tab[2] = {nullptr, nullptr};
     ServeTable *d_tab[2] = {nullptr, nullptr};
     float4 *d_rad[2] = {nullptr, nullptr};
@@ -425,7 +429,7 @@ public:
     void run() {
         cudaSetDevice(device);
         for (;;) {
-            std::vector<std::shared_ptr<Job>> work;
+            std::vector<std::shared_ptr<Job>> work, rt_work;
             {
                 std::unique_lock<std::mutex> lk(mu);
                 // Admission: job slots and the HBM budget (resident scenes, the
@@ -434,7 +438,7 @@ public:
                        scratch + resident + mem_used + pending.front()->bytes <= budget) {
                     std::shared_ptr<Job> j = pending.front();
                     pending.pop_front();
-                    cudaError_t e = cudaMallocAsync(&j->film, j->bytes, stream);
+                    cudaError_t e = j->rt ? cudaSuccess : cudaMallocAsync(&j->film, j->bytes, stream);
                     if (e != cudaSuccess) {
                         j->failed = j->done = true;
                         j->film = nullptr;
@@ -447,15 +451,26 @@ public:
                     st.peak_bytes = std::max(st.peak_bytes, mem_used);
                     st.peak_jobs = std::max<uint32_t>(st.peak_jobs, static_cast<uint32_t>(active.size()));
                 }
-                for (auto &j : active)
-                    if (j->scheduled < j->desc.spp) work.push_back(j);
-                if (work.empty() && inflight.empty()) {
+                // Path-tracing jobs with frames left, and the oldest admitted
+                // real-time job of each real-time scene (its frames follow the
+                // scene's earlier jobs).
+                bool rt_taken[kMaxServeScenes] = {};
+                for (auto &j : active) {
+                    if (j->scheduled >= j->desc.spp) continue;
+                    if (!j->rt) {
+                        work.push_back(j);
+                    } else if (!rt_taken[j->desc.scene]) {
+                        rt_taken[j->desc.scene] = true;
+                        rt_work.push_back(j);
+                    }
+                }
+                if (work.empty() && rt_work.empty() && inflight.empty()) {
                     if (stop) return;
                     cv_work.wait(lk, [&] { return stop || !pending.empty(); });
                     continue;
                 }
             }
-            if (work.empty()) {
+            if (work.empty() && rt_work.empty()) {
                 complete_oldest();
                 continue;
             }
@@ -474,19 +489,20 @@ public:
                     continue;
                 }
             }
-            launch_batch(work);
+            launch_batch(work, rt_work);
         }
     }
 
-    // One batch: a fair share of the batch's paths for every job with frames
+    // One batch: one ReSTIR frame of each real-time job in `rt_work`, then a
+    // fair share of the batch's paths for every path-tracing job with frames
     // left (whole frames, at least one), then the remaining capacity in
     // admission order; one item per job with contiguous frames.
-    void launch_batch(const std::vector<std::shared_ptr<Job>> &work) {
+    void launch_batch(const std::vector<std::shared_ptr<Job>> &work, const std::vector<std::shared_ptr<Job>> &rt_work) {
         const int slot = static_cast<int>(batch_no & 1u);
         ServeTable &t = *h_tab[slot];
         std::vector<uint32_t> frames(work.size(), 0);
         uint64_t left = batch_paths;
-        uint64_t share = std::max<uint64_t>(batch_paths / work.size(), 1);
+        uint64_t share = work.empty() ? batch_paths : std::max<uint64_t>(batch_paths / work.size(), 1);
         size_t nitems = 0;
         for (size_t i = 0; i < work.size() && nitems < kMaxServeItems; ++i) {
             const Job &j = *work[i];
@@ -535,22 +551,46 @@ public:
         t.total_paths = paths;
         t.total_pix = pix;
         cudaError_t e = cudaEventRecord(ev_start[slot], stream);
-        if (e == cudaSuccess) e = cudaGraphLaunch(graph[slot], stream);
-        for (auto &j : b.finishing) {
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(j->host, j->film, j->bytes, cudaMemcpyDeviceToHost, stream);
-            if (e == cudaSuccess) e = cudaFreeAsync(j->film, stream);
+        // Real-time frames first, in stream order: a finished job's film is
+        // copied out before the scene's next job restarts it.
+        unsigned rt_launches = 0;
+        std::string rt_err;
+        int rt_rc = VS_OK;
+        for (size_t i = 0; i < rt_work.size() && e == cudaSuccess && rt_rc == VS_OK; ++i) {
+            Job &j = *rt_work[i];
+            const RtServeHooks &h = rt_hooks[j.desc.scene];
+            rt_rc = h.frame(j.desc.cam, j.desc.frame_begin + j.scheduled, j.scheduled, stream, &rt_launches, rt_err);
+            if (rt_rc != VS_OK) break;
+            j.scheduled += 1;
+            if (j.scheduled == j.desc.spp) {
+                e = cudaMemcpyAsync(j.host, h.film, j.host_bytes, cudaMemcpyDeviceToHost, stream);
+                b.finishing.push_back(rt_work[i]);
+            }
+        }
+        if (e == cudaSuccess && rt_rc == VS_OK && t.count > 0) e = cudaGraphLaunch(graph[slot], stream);
+        for (size_t i = 0; i < b.finishing.size() && t.count > 0; ++i) {
+            Job &j = *b.finishing[i];
+            if (j.rt) continue;
+            if (e == cudaSuccess) e = cudaMemcpyAsync(j.host, j.film, j.host_bytes, cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess) e = cudaFreeAsync(j.film, stream);
         }
         if (e == cudaSuccess) e = cudaEventRecord(ev_end[slot], stream);
         std::lock_guard<std::mutex> lk(mu);
+        if (rt_rc != VS_OK) {
+            fail_locked("server real-time frame: " + rt_err);
+            return;
+        }
         if (e != cudaSuccess) {
             fail_locked(std::string("server launch: ") + cudaGetErrorString(e));
             return;
         }
         st.batches += 1;
-        st.graph_launches += 1;
-        st.kernel_launches += graph_kernels;
-        add_launches(graph_kernels);
+        st.kernel_launches += rt_launches;
+        if (t.count > 0) {
+            st.graph_launches += 1;
+            st.kernel_launches += graph_kernels;
+            add_launches(graph_kernels);
+        }
         ++batch_no;
         inflight.push_back(std::move(b));
     }
@@ -616,6 +656,32 @@ int server_add_scene(Server *s, const DeviceScene &scene, uint64_t bytes, uint32
     return VS_OK;
 }
 
+int server_add_rt_scene(Server *s, const Camera &cam, uint64_t bytes, RtServeHooks hooks, uint32_t *id,
+                        std::string &err) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->nscenes >= kMaxServeScenes) {
+        err = "too many resident scenes";
+        return VS_E_RANGE;
+    }
+    if (s->scratch + s->resident + bytes > s->budget) {
+        err = "resident scenes above the HBM budget";
+        return VS_E_RANGE;
+    }
+    if (!hooks.frame || !hooks.film) {
+        err = "real-time scene without its frame hooks";
+        return VS_E_INVALID;
+    }
+    // Its slot of the path-tracing scene table stays zero: path-tracing
+    // batches never name it.
+    s->scene_cam[s->nscenes] = cam;
+    s->scene_rt[s->nscenes] = true;
+    s->rt_hooks[s->nscenes] = std::move(hooks);
+    s->resident += bytes;
+    s->st.resident_bytes = s->resident;
+    *id = s->nscenes++;
+    return VS_OK;
+}
+
 int server_scene_camera(Server *s, uint32_t id, const Camera **cam, std::string &err) {
     std::lock_guard<std::mutex> lk(s->mu);
     if (id >= s->nscenes) {
@@ -636,20 +702,33 @@ int server_submit(Server *s, const ServeJob &job, uint64_t *id, std::string &err
         err = "unknown scene id";
         return VS_E_INVALID;
     }
-    if (npix > s->batch_paths) {
+    bool rt;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        rt = s->scene_rt[job.scene];
+        if (rt && (job.cam.width != s->scene_cam[job.scene].width || job.cam.height != s->scene_cam[job.scene].height)) {
+            err = "real-time jobs render at their scene's resolution";
+            return VS_E_INVALID;
+        }
+    }
+    if (!rt && npix > s->batch_paths) {
         err = "job resolution above the batch size";
         return VS_E_RANGE;
     }
     auto j = std::make_shared<Job>();
     j->desc = job;
     j->npix = static_cast<uint32_t>(npix);
-    j->bytes = npix * sizeof(float4);
+    j->rt = rt;
+    j->host_bytes = npix * sizeof(float4);
+    // A real-time job renders into its scene's resident film: no device memory
+    // of its own.
+    j->bytes = rt ? 0 : j->host_bytes;
     if (s->scratch + s->resident + j->bytes > s->budget) {
         err = "job larger than the HBM budget";
         return VS_E_RANGE;
     }
     cudaSetDevice(s->device);
-    cudaError_t e = cudaHostAlloc(&j->host, j->bytes, cudaHostAllocDefault);
+    cudaError_t e = cudaHostAlloc(&j->host, j->host_bytes, cudaHostAllocDefault);
     if (e != cudaSuccess) {
         err = std::string("result buffer: ") + cudaGetErrorString(e);
         return VS_E_CUDA;
@@ -699,7 +778,7 @@ int server_result(Server *s, uint64_t id, float *dst, size_t bytes, double timeo
         return VS_E_INVALID;
     }
     std::shared_ptr<Job> j = it->second;
-    if (bytes != j->bytes) {
+    if (bytes != j->host_bytes) {
         err = "result size mismatch";
         return VS_E_INVALID;
     }

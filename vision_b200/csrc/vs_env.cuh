@@ -155,4 +155,37 @@ __device__ VS_OUTLINE void env_sample(const DeviceScene &s, f3 p_ref, f2 u, cons
     p_light = p_ref + world_dir * s.env.world_diameter;
 }
 
+// SphericalMap::sample_only (spherical.cpp:127-132): the map coordinates of a
+// sampled direction alone (the light-surface point a reservoir stores).
+__device__ __forceinline__ f2 env_sample_uv(const DeviceScene &s, f2 u) {
+    uint32_t iv, iu;
+    const float fv = alias_continuous(s.env_marginal, s.env.height, u.y, iv);
+    const float fu = alias_continuous(s.env_cond + static_cast<size_t>(iv) * s.env.width, s.env.width, u.x, iu);
+    return {fu, fv};
+}
+
+// SphericalMap::evaluate_point -> evaluate (spherical.cpp:105-125,134-141) for
+// stored map coordinates: the radiance, the solid-angle pdf from the map's
+// own PDF(uv), and the world direction (compute_light_eval_context,
+// spherical.cpp:148-160, places the light point world_diameter along it).
+template <int N>
+__device__ __forceinline__ void env_eval_uv(const DeviceScene &s, float u, float v, const Wavelengths<N> &wl,
+                                            Spec<N> &L, float &pdf, f3 &world_dir) {
+    const float theta = v * kPi, phi = u * k2Pi;
+    const float st = sinf(theta), ct = cosf(theta);
+    const f3 local = {st * cosf(phi), st * sinf(phi), ct};
+    world_dir = normalize(xform_vector(s.env.o2w, local));
+    const float p = env_map_pdf(s, u, v) / (k2Pi * kPi * st);
+    pdf = isinf(p) ? 0.0f : p;
+    L = env_L<N>(s, u, v, wl);
+}
+
+// Environment::convert_to_bary (spherical.cpp:70-73): map coordinates of a
+// world direction.
+__device__ __forceinline__ f2 env_dir_uv(const DeviceScene &s, f3 world_dir) {
+    float u, v, st;
+    env_uv(normalize(xform_vector(s.env.w2o, world_dir)), u, v, st);
+    return {u, v};
+}
+
 }  // namespace vs

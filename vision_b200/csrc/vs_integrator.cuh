@@ -122,6 +122,17 @@ __device__ __forceinline__ float spot_falloff(const AreaLight &L, float cos_thet
     return f2 * f2;
 }
 
+// PointLight::Le / SpotLight::Le seen from p_ref: colour * scale / distance^2,
+// times the spot's falloff.
+template <int N>
+__device__ __forceinline__ Spec<N> delta_light_L(const AreaLight &L, f3 p_ref, const Wavelengths<N> &wl) {
+    const f3 lp = make3(L.pos[0], L.pos[1], L.pos[2]);
+    const f3 w_un = p_ref - lp;
+    float g = 1.0f / length_sq(w_un);
+    if (L.shape == kLightSpot) g *= spot_falloff(L, dot(make3(L.dir[0], L.dir[1], L.dir[2]), normalize(w_un)));
+    return emitter_spectrum<N>(L, wl) * g;
+}
+
 template <int N>
 __device__ VS_OUTLINE LightSample<N> sample_light(const DeviceScene &s, const Interaction &it, float u_light,
                                                        f2 u, const Wavelengths<N> &wl) {
@@ -148,14 +159,9 @@ __device__ VS_OUTLINE LightSample<N> sample_light(const DeviceScene &s, const In
         // SpotLight::Le: colour * scale / distance^2, times the spot's
         // falloff.  A negative pdf marks the delta light (direct_lighting,
         // integrator.cpp:29-31: MIS weight 1, pdf = the light's pmf).
-        const f3 lp = make3(L.pos[0], L.pos[1], L.pos[2]);
-        const f3 w_un = it.pos - lp;
-        float g = 1.0f / length_sq(w_un);
-        if (L.shape == kLightSpot)
-            g *= spot_falloff(L, dot(make3(L.dir[0], L.dir[1], L.dir[2]), normalize(w_un)));
-        ls.L = emitter_spectrum<N>(L, wl) * g;
+        ls.L = delta_light_L<N>(L, it.pos, wl);
         ls.pdf = -pmf_light;
-        ls.p_light = lp;
+        ls.p_light = make3(L.pos[0], L.pos[1], L.pos[2]);
         return ls;
     }
     float ux = u.x;

@@ -3,7 +3,10 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <string>
+
+#include <cuda_runtime.h>
 
 #include "vs_devscene.h"
 
@@ -33,6 +36,19 @@ struct ServeStats {
     uint64_t scratch_bytes;  // the two batch buffers reserved at creation
 };
 
+// A resident real-time (ReSTIR) scene driven by the server.  `frame` renders
+// one ReSTIR frame of the scene with the job's sensor into the scene's own
+// film (film_index 0 restarts the running mean) on `stream` and adds its
+// kernel launches to *launches; `film` is that film (float4 per pixel).  The
+// scene's reservoirs, surfaces and previous camera stay resident between
+// calls, so consecutive jobs on the scene continue one temporal history.
+struct RtServeHooks {
+    std::function<int(const Camera &cam, uint32_t frame, uint32_t film_index, cudaStream_t stream,
+                      unsigned *launches, std::string &err)>
+        frame;
+    const float4 *film = nullptr;
+};
+
 class Server;
 
 // Status codes follow include/vision_b200.h (0 = OK); `err` gets the message.
@@ -42,6 +58,12 @@ void server_destroy(Server *s);
 // `bytes`: the scene's device memory, counted against the HBM budget for as
 // long as the server holds the scene.
 int server_add_scene(Server *s, const DeviceScene &scene, uint64_t bytes, uint32_t *id, std::string &err);
+// A real-time scene: `bytes` counts its geometry and its resident per-pixel
+// buffers (reservoirs, surfaces, film), all allocated before the call.  Jobs
+// on it render at the scene's resolution, one frame per batch, in submission
+// order.
+int server_add_rt_scene(Server *s, const Camera &cam, uint64_t bytes, RtServeHooks hooks, uint32_t *id,
+                        std::string &err);
 // The sensor of a resident scene (its camera when it was added).
 int server_scene_camera(Server *s, uint32_t id, const Camera **cam, std::string &err);
 int server_submit(Server *s, const ServeJob &job, uint64_t *id, std::string &err);
