@@ -24,8 +24,10 @@ def _dev(x, t):
     return xd, td
 
 
-@pytest.mark.parametrize('n', [1000, 4096])
+@pytest.mark.parametrize('n', [1000, 4096, 300001])
 def test_cache_forward_matches_oracle(vb, gpu_ctx, n):
+    # 300,001 rows: several tiles per pipeline (the next tile streamed while
+    # the current one runs) and a ragged last tile read past the end.
     cache = vb.RadianceCache(gpu_ctx, seed=3)
     w = cache.weights()
     x, t = _batch(n, 1)
@@ -39,6 +41,10 @@ def test_cache_forward_matches_oracle(vb, gpu_ctx, n):
     # rounding of a hidden activation by one unit.
     assert np.abs(got - y).max() <= 2e-2 * np.abs(y).max(), np.abs(got - y).max()
     assert np.mean(np.abs(got - y) <= 1e-3 * (1 + np.abs(y))) >= 0.99
+    again = torch.zeros_like(out)
+    cache.infer(xd.data_ptr(), n, again.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(out, again)
     cache.close()
 
 

@@ -3,11 +3,16 @@
 // Network: 64 BF16 inputs -> 4 hidden layers of 64 (ReLU) -> 3 outputs, no
 // biases.  Every layer is a tcgen05.mma.kind::f16 with BF16 operands in
 // shared memory and the FP32 accumulator in tensor memory:
-//   inference  (k_mlp_infer): persistent CTAs of 128 threads, one 128-row
-//     tile at a time; M=128 x N=64 (N=16 for the padded output layer), K=64 as
-//     four K=16 steps.  Thread t owns tile row t: it writes its features, and
-//     after each layer reads its accumulator row with tcgen05.ld (32x32b),
-//     applies ReLU, rounds to BF16 and writes the next layer's operand row.
+//   inference  (k_mlp_infer): one CTA per SM holding the forward weights once
+//     and running kInferGroups independent 4-warp pipelines, each with its
+//     own 64 tensor-memory columns and two tile buffers; while a pipeline runs
+//     the five layers of one 128-row tile, the TMA engine loads its next tile
+//     into the other buffer (128-byte swizzle, rows past n zero-filled).
+//     M=128 x N=64 (N=16 for the padded output layer), K=64 as four K=16
+//     steps.  Thread t of a pipeline owns tile row t: after each layer it
+//     reads its accumulator row with tcgen05.ld (32x32b), applies ReLU, rounds
+//     to BF16 and writes the next layer's operand row in the no-swizzle
+//     layout, over the consumed feature tile.
 //   training   (k_mlp_train): the same forward pass keeping every layer's
 //     BF16 input; the relative-L2 loss gradient; the backward data products
 //     dX = dZ W^T (M=128) masked by ReLU'; and the weight gradients
@@ -26,6 +31,8 @@
 // returns.
 #include "vs_mlp.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -101,6 +108,24 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Issues the loads of 64 accumulator columns (four 32x32b.x16) and waits for
+// them once.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v) {
+    uint32_t r[64];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[16 * q + 0]), "=r"(r[16 * q + 1]), "=r"(r[16 * q + 2]), "=r"(r[16 * q + 3]),
+              "=r"(r[16 * q + 4]), "=r"(r[16 * q + 5]), "=r"(r[16 * q + 6]), "=r"(r[16 * q + 7]),
+              "=r"(r[16 * q + 8]), "=r"(r[16 * q + 9]), "=r"(r[16 * q + 10]), "=r"(r[16 * q + 11]),
+              "=r"(r[16 * q + 12]), "=r"(r[16 * q + 13]), "=r"(r[16 * q + 14]), "=r"(r[16 * q + 15])
+            : "r"(taddr + 16u * q));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
@@ -193,21 +218,62 @@ __device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t cols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
 }
 
-constexpr uint32_t kInferSmem = kPackFwdBytes + kTileBytes + 64;
+// A 128-row feature tile written by TMA with the 128-byte swizzle (row r at
+// 128 r, its 16-byte chunk c at (c ^ (r & 7)) * 16, 1024-byte aligned) as a
+// K-major operand, K step s: SBO 1024 B between 8-row groups, the K=16 step
+// 32 B further inside the swizzle atom, layout type SWIZZLE_128B.
+__device__ __forceinline__ uint64_t tile_sw128_desc(uint32_t base, int s) {
+    return sdesc(base + s * 32u, 16u, 1024u) | (2ull << 61);
+}
 
-__global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t *__restrict__ feat, uint32_t n,
-                                                   const uint4 *__restrict__ wpack, float4 *__restrict__ out,
-                                                   int *err) {
-    extern __shared__ __align__(1024) uint8_t smem[];
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// One 2D tile of the feature tensor map into shared memory (no multicast),
+// completing on `mbar` with its byte count.
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(map), "r"(x), "r"(y), "r"(mbar)
+        : "memory");
+}
+
+// Named barrier over the 128 threads of pipeline g (barrier 1 + g), returning
+// whether every thread passed true.
+__device__ __forceinline__ bool group_sync_and(uint32_t g, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\tbarrier.cta.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"(static_cast<uint32_t>(v)), "r"(1u + g)
+        : "memory");
+    return r != 0u;
+}
+
+constexpr uint32_t kInferGroups = 5;
+constexpr uint32_t kInferThreads = 128u * kInferGroups;
+constexpr uint32_t kInferBars = 3u * kInferGroups;  // per pipeline: two tile loads, one MMA
+constexpr uint32_t kInferSmem = 1024u + kPackFwdBytes + kInferGroups * 2u * kTileBytes + 8u * kInferBars + 16u;
+static_assert(kInferSmem <= 232448u, "inference shared memory above the per-CTA limit");
+
+__global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const __grid_constant__ CUtensorMap fmap, uint32_t n,
+                                                                const uint4 *__restrict__ wpack,
+                                                                float4 *__restrict__ out, int *err) {
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte alignment for the swizzled TMA destinations.
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
     uint8_t *w = smem;
-    uint8_t *tile = smem + kPackFwdBytes;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kPackFwdBytes + kTileBytes);
-    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kPackFwdBytes + kTileBytes + 8);
-    const uint32_t tid = threadIdx.x;
-    const uint32_t mbar_s = smem_u32(mbar);
-    if (tid < 32) tmem_alloc(smem_u32(slot), 64);
+    uint8_t *bufs = smem + kPackFwdBytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(bufs + kInferGroups * 2u * kTileBytes);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + kInferBars);
+    const uint32_t tid = threadIdx.x, g = tid >> 7, gt = tid & 127u;
+    if (tid < 32) tmem_alloc(smem_u32(slot), 512);
     if (tid == 0) {
-        mbar_init(mbar_s, 1);
+        for (uint32_t i = 0; i < kInferBars; ++i) mbar_init(smem_u32(bars + i), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     copy_to_smem(w, wpack, kPackFwdBytes);
@@ -215,54 +281,86 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t *__restrict__ 
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = *slot;
-    const uint32_t wbase = smem_u32(w), tbase = smem_u32(tile);
-    uint32_t phase = 0;
-    bool ok = true;
+    // Pipeline g: accumulator columns [64 g, 64 g + 64), tile buffers
+    // buf0 + {0, kTileBytes}, barriers load[0], load[1], mma.
+    const uint32_t tmem = *slot + 64u * g;
+    const uint32_t lane = (gt & ~31u) << 16;
+    const uint32_t wbase = smem_u32(w);
+    uint8_t *tile0 = bufs + g * 2u * kTileBytes;
+    const uint32_t buf0 = smem_u32(tile0);
+    const uint32_t mb_load = smem_u32(bars + 3u * g), mb_mma = mb_load + 16u;
     const uint32_t tiles = (n + kTile - 1) / kTile;
-    for (uint32_t tt = blockIdx.x; tt < tiles && ok; tt += gridDim.x) {
-        const uint64_t row = static_cast<uint64_t>(tt) * kTile + tid;
-        load_features(tile, tid, feat, row, n);
-        fence_async_smem();
-        fence_before();
-        __syncthreads();
-        fence_after();
-        for (int l = 0; l < 5 && ok; ++l) {
-            if (tid == 0) {
+    const uint32_t stride = gridDim.x * kInferGroups;
+    uint32_t tt = blockIdx.x * kInferGroups + g;
+    uint32_t ph_load = 0u, ph_mma = 0u;  // parity bits (bit b: buffer b)
+    bool pending[2] = {false, false};
+    if (gt == 0 && tt < tiles) {
+        mbar_expect_tx(mb_load, kTileBytes);
+        tma_load_tile(buf0, &fmap, 0, static_cast<int>(tt * kTile), mb_load);
+    }
+    pending[0] = tt < tiles;
+    bool ok = true;
+    for (uint32_t k = 0; tt < tiles && ok; tt += stride, ++k) {
+        const uint32_t cur = k & 1u, nxt = cur ^ 1u;
+        const uint32_t buf = buf0 + cur * kTileBytes;
+        uint8_t *tile = tile0 + cur * kTileBytes;
+        // The other buffer held the previous tile, whose last MMA has
+        // completed: load the next tile into it now.
+        if (tt + stride < tiles) {
+            if (gt == 0) {
+                mbar_expect_tx(mb_load + 8u * nxt, kTileBytes);
+                tma_load_tile(buf0 + nxt * kTileBytes, &fmap, 0, static_cast<int>((tt + stride) * kTile),
+                              mb_load + 8u * nxt);
+            }
+            pending[nxt] = true;
+        }
+        bool done = mbar_wait(mb_load + 8u * cur, (ph_load >> cur) & 1u);
+        ph_load ^= 1u << cur;
+        pending[cur] = !done;
+        ok = group_sync_and(g, done);
+        if (!ok) break;
+        const uint64_t row = static_cast<uint64_t>(tt) * kTile + gt;
+        for (int l = 0; l < 5; ++l) {
+            if (gt == 0) {
                 const uint32_t id = l < 4 ? idesc(128, 64, 0, 0) : idesc(128, 16, 0, 0);
 #pragma unroll
-                for (int s = 0; s < 4; ++s) mma(tmem, tile_kdesc(tbase, s), w_fwd_desc(wbase, l, s), id, s > 0);
-                commit(mbar_s);
+                for (int s = 0; s < 4; ++s)
+                    mma(tmem, l == 0 ? tile_sw128_desc(buf, s) : tile_kdesc(buf, s), w_fwd_desc(wbase, l, s), id,
+                        s > 0);
+                commit(mb_mma);
             }
-            // Every thread waits; the CTA agrees on the outcome so that all
-            // threads take the same barriers afterwards.
-            const bool done = mbar_wait(mbar_s, phase);
-            phase ^= 1u;
-            ok = __syncthreads_and(done) != 0;
+            done = mbar_wait(mb_mma, ph_mma);
+            ph_mma ^= 1u;
             fence_after();
-            if (!ok) break;
-            if (l < 4) {
+            // The epilogue of a thread whose wait ran out is skipped; the
+            // barrier that follows makes the pipeline agree to stop.
+            if (done && l < 4) {
                 float v[64];
-                ld_row64(tmem, 0, v);
+                tmem_ld64(tmem + lane, v);
 #pragma unroll
                 for (int i = 0; i < 64; ++i) v[i] = fmaxf(v[i], 0.0f);
-                st_row64(tile, tid, v);
+                st_row64(tile, gt, v);
                 fence_async_smem();
-            } else {
+            } else if (done) {
                 float v[16];
-                tmem_ld16(tmem + ((tid & ~31u) << 16), v);
+                tmem_ld16(tmem + lane, v);
                 if (row < n) out[row] = make_float4(v[0], v[1], v[2], 0.0f);
             }
             fence_before();
-            __syncthreads();
+            ok = group_sync_and(g, done);
             fence_after();
+            if (!ok) break;
         }
     }
-    if (!ok && tid == 0) atomicExch(err, 1);
+    // A pipeline that stopped early waits (bounded) for the loads it still
+    // has in flight before the CTA releases its shared memory.
+    for (uint32_t b = 0; b < 2; ++b)
+        if (pending[b]) (void)mbar_wait(mb_load + 8u * b, (ph_load >> b) & 1u);
+    if (!ok && gt == 0) atomicExch(err, 1);
     fence_before();
     __syncthreads();
     fence_after();
-    if (tid < 32) tmem_free(tmem, 64);
+    if (tid < 32) tmem_free(*slot, 512);
 }
 
 // Training shared memory: forward and backward weight images, the input tile
@@ -520,6 +618,37 @@ static cudaError_t sm_count(int &n) {
     return cudaSuccess;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+
+static cudaError_t encode_fn() {
+    if (g_encode_tiled) return cudaSuccess;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorSymbolNotFound;
+    g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return cudaSuccess;
+}
+
+// The feature matrix (n rows of 64 BF16, 128-byte rows, 16-byte aligned) as a
+// TMA tensor map with 128-row x 64-column boxes and the 128-byte swizzle.
+static cudaError_t feature_map(const uint16_t *feat, uint32_t n, CUtensorMap *map) {
+    cudaError_t e = encode_fn();
+    if (e != cudaSuccess) return e;
+    if (reinterpret_cast<uintptr_t>(feat) & 15u) return cudaErrorMisalignedAddress;
+    cuuint64_t dims[2] = {64u, n};
+    cuuint64_t strides[1] = {128u};
+    cuuint32_t box[2] = {64u, static_cast<cuuint32_t>(kTile)};
+    cuuint32_t elem[2] = {1u, 1u};
+    CUresult r = g_encode_tiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t *>(feat), dims, strides,
+                                box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 cudaError_t mlp_infer(const MlpState &s, const uint16_t *feat, uint32_t n, float4 *out, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     static bool attr = false;
@@ -528,13 +657,17 @@ cudaError_t mlp_infer(const MlpState &s, const uint16_t *feat, uint32_t n, float
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    int sms = 0;
-    cudaError_t e = sm_count(sms);
+    CUtensorMap map;
+    cudaError_t e = feature_map(feat, n, &map);
     if (e != cudaSuccess) return e;
-    uint32_t tiles = (n + kTile - 1) / kTile;
-    uint32_t grid = static_cast<uint32_t>(sms) * 4u;
-    if (grid > tiles) grid = tiles;
-    k_mlp_infer<<<grid, 128, kInferSmem, st>>>(feat, n, reinterpret_cast<const uint4 *>(s.pack), out, s.err);
+    int sms = 0;
+    e = sm_count(sms);
+    if (e != cudaSuccess) return e;
+    const uint32_t tiles = (n + kTile - 1) / kTile;
+    uint32_t grid = static_cast<uint32_t>(sms);
+    const uint32_t need = (tiles + kInferGroups - 1) / kInferGroups;
+    if (grid > need) grid = need;
+    k_mlp_infer<<<grid, kInferThreads, kInferSmem, st>>>(map, n, reinterpret_cast<const uint4 *>(s.pack), out, s.err);
     return cudaGetLastError();
 }
 
