@@ -304,7 +304,37 @@ int vs_restir_params(const vs_scene *scene, uint32_t frame_index, void *dst, siz
 #define VS_RESTIR_GI_RESERVOIRS 5 /* 64 bytes: indirect reservoirs after spatial reuse */
 #define VS_RESTIR_HIT_BSDF 6     /* 32 bytes: BSDF sample of the direct pass */
 #define VS_RESTIR_GI_SAMPLES 7   /* 64 bytes: initial indirect samples */
+/* Of the last frame rendered with the denoiser on: */
+#define VS_RESTIR_DENOISED 8      /* float4: the SVGF output (illumination * albedo + emission) */
+#define VS_RESTIR_GBUFFER 9       /* 32 bytes: PixelGeometry (normal + width, film position,
+                                     depth gradient, linear depth; -1: miss) */
+#define VS_RESTIR_SVGF_ALBEDO 10  /* float4: material albedo, linear sRGB */
+#define VS_RESTIR_SVGF_EMISSION 11 /* float4: emission seen by the camera ray */
+#define VS_RESTIR_SVGF_DATA 12    /* 32 bytes: SVGFData (illumination, variance, history, moments)
+                                     after the last a-trous pass */
+#define VS_RESTIR_SVGF_MOTION 13  /* float2: G-buffer motion vector in pixels */
+#define VS_RESTIR_SVGF_HISTORY 14 /* float: history length */
 int vs_restir_download(vs_scene *scene, int which, void *dst, size_t bytes);
+
+/* SVGF denoiser of the real-time frame (src/render_core/denoisers/SVGF/,
+ * SVGF::dispatch svgf.cpp:86-101; the switch the reference sets from its GUI,
+ * svgf.cpp:22).  When on, every vs_restir_frame ends with the SVGF passes over
+ * the frame's film: a G-buffer of the camera rays (FrameBuffer::compute_geom
+ * and compute_gradient), demodulation by the material albedo, temporal
+ * reprojection with history, the moment filter, N a-trous passes and
+ * modulation, the result read with VS_RESTIR_DENOISED.  Its settings come
+ * from the integrator's "denoiser" node ({"type": "svgf", "param": {N, alpha,
+ * moments_alpha, history_limit, moments_filter_radius, sigma_rt,
+ * sigma_normal}}, the reference's defaults otherwise); vs_restir_reset clears
+ * its history too.  Unlike the reference, whose moment filter and a-trous
+ * passes overwrite the buffer they read, each pass reads one buffer and
+ * writes another, so the output does not depend on thread scheduling. */
+int vs_denoiser_enable(vs_scene *scene, int on);
+/* The 48-byte SVGF settings block (N, alpha, moments_alpha, history_limit,
+ * moments_filter_radius, sigma_rt, sigma_normal, reproject, filter_moments).
+ * Works on host-only contexts. */
+#define VS_DENOISER_PARAMS_BYTES 48
+int vs_denoiser_params(const vs_scene *scene, void *dst, size_t bytes);
 
 /* Render-job server: continuous batching of vs_render-equivalent jobs of mixed
  * resolution and spp over resident scenes.  No reference counterpart (the

@@ -75,6 +75,7 @@ def lib():
         L.oracle_rt_close.argtypes = [P]
         L.oracle_rt_frame.argtypes = [P, P, P, U, U]
         L.oracle_rt_buffer.argtypes = [P, ctypes.c_int, P, ctypes.c_size_t]
+        L.oracle_rt_svgf.argtypes = [P, P, P, P, P, U]
         _lib = L
     return _lib
 
@@ -201,7 +202,8 @@ class OracleRestir:
     """CPU restatement of the real-time ReSTIR frame over an OracleScene."""
 
     BUFFERS = dict(di_radiance=0, gi_radiance=1, motion=2, surfaces=3, di_reservoirs=4, gi_reservoirs=5,
-                   hit_bsdf=6, gi_samples=7, film=8)
+                   hit_bsdf=6, gi_samples=7, film=8, denoised=9, gbuffer=10, svgf_albedo=11, svgf_emission=12,
+                   svgf_data=13, svgf_motion=14, svgf_history=15)
 
     def __init__(self, oscene, width, height):
         self.oscene = oscene
@@ -215,6 +217,20 @@ class OracleRestir:
         rc = lib().oracle_rt_frame(self.h, _p(camera), _p(params), film_index, threads or os.cpu_count())
         if rc != 0:
             raise ValueError('oracle_rt_frame rejected the parameters')
+
+    def svgf(self, camera, params, svgf_params, radiance, threads=None):
+        """SVGF over a film (height x width x 4 float32) with the frame's camera
+        and parameter blocks and the 48-byte SVGF settings."""
+        camera = np.ascontiguousarray(camera).view(np.uint8)
+        params = np.ascontiguousarray(params).view(np.uint8)
+        svgf_params = np.ascontiguousarray(svgf_params).view(np.uint8)
+        radiance = np.ascontiguousarray(radiance, np.float32)
+        assert camera.nbytes == 128 and params.nbytes == 448 and svgf_params.nbytes == 48
+        assert radiance.size == 4 * self.width * self.height
+        rc = lib().oracle_rt_svgf(self.h, _p(camera), _p(params), _p(svgf_params), _p(radiance),
+                                  threads or os.cpu_count())
+        if rc != 0:
+            raise ValueError('oracle_rt_svgf rejected the parameters')
 
     def buffer(self, which, dtype):
         out = np.zeros(self.width * self.height, dtype)

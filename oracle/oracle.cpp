@@ -1757,6 +1757,46 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
     return b;
 }
 
+// MaterialEvaluator::albedo (material.cpp:91-98) at c = dot(shading normal,
+// wo): each lobe's albedo times its WeightedLobe weight (LobeSet::albedo,
+// lobe.cpp:564-570).  Lambert kr; microfacet kr * F(c) (lobe.cpp:208-210),
+// the coat and specular lobes with their table values
+// (principled_bsdf.cpp:154-160,198-205); dielectric kt (1 - F) + F at |c|
+// (lobe.cpp:308-313); FresnelBlend Rd * F_dielectric(c, 1.5); plastic its
+// Schlick F (MicrofacetReflection of one); sheen its tint; a black body
+// nothing.
+static void bsdf_albedo(const Bsdf &b, float c, float *out) {
+    const int n = b.n;
+    for (int i = 0; i < n; ++i) out[i] = 0.0f;
+    for (int k = 0; k < b.count; ++k) {
+        const Lobe &l = b.lobes[k];
+        float a[8] = {0, 0, 0, 0, 0, 0, 0, 0}, F[8];
+        if (l.kind == Lobe::Lambert || l.kind == Lobe::Sheen) {
+            for (int i = 0; i < n; ++i) a[i] = l.kr[i];
+        } else if (l.kind == Lobe::MicrofacetRefl && l.fresnel == Lobe::DielectricFr) {
+            float sc = lut3(kLutCoat, 1, std::sqrt(std::sqrt(l.ax * l.ax)), c, (l.eta0 - 1.003f) / (4.0f - 1.003f));
+            for (int i = 0; i < n; ++i) a[i] = l.kr[i] * sc;
+        } else if (l.kind == Lobe::MicrofacetRefl && l.fresnel == Lobe::Schlick) {
+            float sl = lut3(kLutSpec, 1, std::sqrt(std::sqrt(l.ax * l.ay)), c,
+                            std::sqrt(std::fabs((l.eta0 - 1.0f) / (l.eta0 + 1.0f))));
+            for (int i = 0; i < n; ++i) a[i] = (l.fa[i] + sl * (1.0f - l.fa[i])) * l.kr[i];
+        } else if (l.kind == Lobe::MicrofacetRefl) {
+            fresnel_eval(l, n, c, F);
+            for (int i = 0; i < n; ++i) a[i] = l.kr[i] * F[i];
+        } else if (l.kind == Lobe::Dielectric) {
+            diel_fresnel(l, n, std::fabs(c), F);
+            for (int i = 0; i < n; ++i) a[i] = l.kr[i] * (1.0f - F[i]) + F[i];
+        } else if (l.kind == Lobe::Substrate) {
+            float f = mf::fr_dielectric(c, 1.5f);
+            for (int i = 0; i < n; ++i) a[i] = l.kr[i] * f;
+        } else if (l.kind == Lobe::Plastic) {
+            fresnel_eval(l, n, c, F);
+            for (int i = 0; i < n; ++i) a[i] = F[i];
+        }
+        for (int i = 0; i < n; ++i) out[i] += a[i] * l.weight;
+    }
+}
+
 // ----- the path (pt.cpp:53-72; integrator.cpp:134-283) ------------------------
 static void check_dispersive(const Bsdf &bsdf, Swl &w) {
     if (bsdf.dispersive && w.n > 1) {  // SampledWavelengths::check_dispersive
@@ -2130,9 +2170,29 @@ int oracle_rt_frame(void *rt, const void *camera, const void *params, uint32_t f
     return 0;
 }
 
+// SVGF over a film (4 floats per pixel) with the frame's camera and
+// parameter blocks and the 48-byte SVGF settings (as vs_denoiser_params
+// returns them).
+int oracle_rt_svgf(void *rt, const void *camera, const void *params, const void *svgf_params, const float *radiance,
+                   uint32_t threads) {
+    auto *f = static_cast<oracle::rt::Frame *>(rt);
+    oracle::Camera cam;
+    oracle::rt::Params p;
+    oracle::rt::Frame::SvParams sp;
+    static_assert(sizeof(sp) == 48, "SVGF settings block");
+    std::memcpy(&cam, camera, sizeof(cam));
+    std::memcpy(&p, params, sizeof(p));
+    std::memcpy(&sp, svgf_params, sizeof(sp));
+    if (p.width * p.height != f->npix || sp.N > 10u || sp.mradius < 0 || sp.mradius > 5) return 1;
+    f->svgf(cam, p, sp, radiance, threads);
+    return 0;
+}
+
 // Per-pixel buffers of the last frame: 0 direct radiance, 1 indirect
 // radiance, 2 motion, 3 surfaces, 4 direct reservoirs, 5 indirect
-// reservoirs, 6 BSDF samples, 7 initial indirect samples, 8 film.
+// reservoirs, 6 BSDF samples, 7 initial indirect samples, 8 film; of the
+// last SVGF pass: 9 output, 10 G-buffer, 11 albedo, 12 emission, 13 filtered
+// SVGFData, 14 G-buffer motion, 15 history.
 int oracle_rt_buffer(void *rt, int which, void *dst, size_t bytes) {
     auto *f = static_cast<oracle::rt::Frame *>(rt);
     uint32_t c = f->cur();
@@ -2148,6 +2208,13 @@ int oracle_rt_buffer(void *rt, int which, void *dst, size_t bytes) {
         case 6: src = f->hit_bsdf.data(); n = f->hit_bsdf.size() * sizeof(oracle::rt::HitBsdf); break;
         case 7: src = f->gi_init.data(); n = f->gi_init.size() * sizeof(oracle::rt::GiRes); break;
         case 8: src = f->film.data(); n = f->film.size() * 4; break;
+        case 9: src = f->sout.data(); n = f->sout.size() * 4; break;
+        case 10: src = f->sgeom[c].data(); n = f->sgeom[c].size() * sizeof(oracle::rt::Frame::SvGeom); break;
+        case 11: src = f->salb.data(); n = f->salb.size() * 4; break;
+        case 12: src = f->semi.data(); n = f->semi.size() * 4; break;
+        case 13: src = f->sprev.data(); n = f->sprev.size() * sizeof(oracle::rt::Frame::SvData); break;
+        case 14: src = f->smot.data(); n = f->smot.size() * 4; break;
+        case 15: src = f->shist[c].data(); n = f->shist[c].size() * 4; break;
         default: return 1;
     }
     if (n != bytes) return 2;

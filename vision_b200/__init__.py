@@ -125,6 +125,8 @@ def _load():
         'vs_restir_reset': ([P], ctypes.c_int),
         'vs_restir_params': ([P, U32, P, ctypes.c_size_t], ctypes.c_int),
         'vs_restir_download': ([P, ctypes.c_int, P, ctypes.c_size_t], ctypes.c_int),
+        'vs_denoiser_enable': ([P, ctypes.c_int], ctypes.c_int),
+        'vs_denoiser_params': ([P, P, ctypes.c_size_t], ctypes.c_int),
         'vs_server_create': ([P, ctypes.c_uint64, U32, ctypes.c_uint64, ctypes.POINTER(P)], ctypes.c_int),
         'vs_server_destroy': ([P], None),
         'vs_server_add_scene': ([P, P, ctypes.POINTER(U32)], ctypes.c_int),
@@ -165,7 +167,8 @@ ABI_SYMBOLS = sorted(['vs_version', 'vs_context_create', 'vs_context_destroy', '
                       'vs_cache_destroy', 'vs_cache_get_weights', 'vs_cache_set_weights', 'vs_cache_set_optimizer',
                       'vs_cache_infer', 'vs_cache_train', 'vs_cache_gradient', 'vs_render_cached',
                       'vs_render_schedule_set', 'vs_cache_download', 'vs_sampler_stream', 'vs_scene_add_instance',
-                      'vs_scene_clear_geometries', 'vs_scene_invalidate'])
+                      'vs_scene_clear_geometries', 'vs_scene_invalidate', 'vs_denoiser_enable',
+                      'vs_denoiser_params'])
 CACHE_PARAMS = 16576
 SCHEDULE_GRID = 0
 # Buffers of the last cache-terminated frame (include/vision_b200.h VS_CACHE_*).
@@ -190,9 +193,22 @@ GI_RESERVOIR_DTYPE = np.dtype([('weight_sum', '<f8'), ('C', '<f4'), ('W', '<f4')
                                ('sp_ng', '<f4', 3), ('Lo', '<f4', 3), ('age', '<f4'), ('pad', '<u4', 2)])
 HIT_BSDF_DTYPE = np.dtype([('wi', '<f4', 3), ('f', '<f4', 3), ('pdf', '<f4'), ('pad', '<u4')])
 RESTIR_PARAMS_BYTES = 448
+# SVGF records: PixelGeometry and SVGFData (vs_restir.h SvgfGeom / SvgfData).
+SVGF_GEOM_DTYPE = np.dtype([('normal', '<f4', 3), ('fwidth', '<f4'), ('p_film', '<f4', 2), ('depth_gradient', '<f4'),
+                            ('linear_depth', '<f4')])
+SVGF_DATA_DTYPE = np.dtype([('illumination', '<f4', 3), ('variance', '<f4'), ('history', '<f4'), ('moments', '<f4', 2),
+                            ('pad', '<f4')])
+SVGF_PARAMS_DTYPE = np.dtype([('N', '<u4'), ('alpha', '<f4'), ('moments_alpha', '<f4'), ('history_limit', '<u4'),
+                              ('moments_radius', '<i4'), ('sigma_rt', '<f4'), ('sigma_normal', '<f4'),
+                              ('reproject', '<u4'), ('filter_moments', '<u4'), ('pad', '<u4', 3)])
 RESTIR = dict(di_radiance=(0, np.dtype(('<f4', 4))), gi_radiance=(1, np.dtype(('<f4', 4))),
               motion=(2, np.dtype(('<f4', 2))), surfaces=(3, RT_SURFACE_DTYPE), di_reservoirs=(4, DI_RESERVOIR_DTYPE),
-              gi_reservoirs=(5, GI_RESERVOIR_DTYPE), hit_bsdf=(6, HIT_BSDF_DTYPE), gi_samples=(7, GI_RESERVOIR_DTYPE))
+              gi_reservoirs=(5, GI_RESERVOIR_DTYPE), hit_bsdf=(6, HIT_BSDF_DTYPE), gi_samples=(7, GI_RESERVOIR_DTYPE),
+              denoised=(8, np.dtype(('<f4', 4))), gbuffer=(9, SVGF_GEOM_DTYPE),
+              svgf_albedo=(10, np.dtype(('<f4', 4))), svgf_emission=(11, np.dtype(('<f4', 4))),
+              svgf_data=(12, SVGF_DATA_DTYPE), svgf_motion=(13, np.dtype(('<f4', 2))),
+              svgf_history=(14, np.dtype('<f4')))
+assert SVGF_GEOM_DTYPE.itemsize == 32 and SVGF_DATA_DTYPE.itemsize == 32 and SVGF_PARAMS_DTYPE.itemsize == 48
 assert RT_SURFACE_DTYPE.itemsize == 64 and DI_RESERVOIR_DTYPE.itemsize == 64 and GI_RESERVOIR_DTYPE.itemsize == 64
 
 
@@ -420,6 +436,16 @@ class Scene:
         out = np.zeros(RESTIR_PARAMS_BYTES, np.uint8)
         self.ctx.check(lib.vs_restir_params(self.handle, frame_index, _ptr(out), out.nbytes), 'restir_params')
         return out
+
+    def denoiser_enable(self, on=True):
+        """SVGF after every restir_frame (read with restir_buffer('denoised'))."""
+        self.ctx.check(lib.vs_denoiser_enable(self.handle, 1 if on else 0), 'denoiser_enable')
+
+    def denoiser_params(self):
+        """The SVGF settings block (SVGF_PARAMS_DTYPE)."""
+        out = np.zeros(1, SVGF_PARAMS_DTYPE)
+        self.ctx.check(lib.vs_denoiser_params(self.handle, _ptr(out), out.nbytes), 'denoiser_params')
+        return out[0]
 
     def restir_buffer(self, which):
         key, dt = RESTIR[which]

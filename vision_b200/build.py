@@ -19,10 +19,14 @@ BUILD = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libvision_b200.so')
 INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 
-SOURCES = ['kernels.cu', 'wavefront.cu', 'restir.cu', 'restir_diffuse.cu', 'server.cu', 'mlp.cu', 'cache_render.cu', 'capi.cu', 'noalloc.cu', 'scene_load.cpp', 'bvh8.cpp', 'rgb2spec.cpp', 'luts.cpp', 'lut_gen.cu']
+SOURCES = ['kernels.cu', 'wavefront.cu', 'restir.cu', 'restir_diffuse.cu', 'svgf.cu', 'server.cu', 'mlp.cu', 'cache_render.cu', 'capi.cu', 'noalloc.cu', 'scene_load.cpp', 'bvh8.cpp', 'rgb2spec.cpp', 'luts.cpp', 'lut_gen.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 COMMON = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC,-ffp-contract=off,-pthread',
           '-I', CSRC, '-I', INCLUDE]
+# Per-source device flags.  svgf.cu: no multiply-add contraction, as in the
+# host oracle; its edge-stopping weights (exp of depth and luminance
+# differences over small sigmas) magnify one-ulp differences in the G-buffer.
+SOURCE_FLAGS = {'svgf.cu': ['--fmad=false']}
 
 
 def nvcc():
@@ -52,11 +56,12 @@ def _headers():
 
 
 def _source_digest(src):
-    return _digest([os.path.join(CSRC, src)] + _headers(), ARCH + COMMON)
+    return _digest([os.path.join(CSRC, src)] + _headers(), ARCH + COMMON + SOURCE_FLAGS.get(src, []))
 
 
 def _library_digest():
-    return _digest([os.path.join(CSRC, s) for s in SOURCES] + _headers(), ARCH + COMMON + SOURCES)
+    flags = [f for src in SOURCES for f in SOURCE_FLAGS.get(src, [])]
+    return _digest([os.path.join(CSRC, s) for s in SOURCES] + _headers(), ARCH + COMMON + SOURCES + flags)
 
 
 def _stamp_ok(path, digest):
@@ -83,7 +88,7 @@ def build(force=False, verbose=False):
         digest = _source_digest(src)
         if not force and _stamp_ok(obj, digest):
             return obj
-        cmd = [nvcc()] + ARCH + COMMON + ['-c', os.path.join(CSRC, src), '-o', obj]
+        cmd = [nvcc()] + ARCH + COMMON + SOURCE_FLAGS.get(src, []) + ['-c', os.path.join(CSRC, src), '-o', obj]
         if src.endswith('.cu') and verbose:
             cmd += ['-Xptxas', '-v']
         if verbose:

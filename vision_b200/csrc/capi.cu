@@ -237,6 +237,44 @@ struct vs_scene {
         }
     } rt;
 
+    // SVGF denoiser of the real-time frame: G-buffer and history by frame
+    // parity, three rotating SVGFData buffers, the denoised frame.
+    struct Svgf {
+        DevBuf<SvgfGeom> geom[2];
+        DevBuf<float> history[2];
+        DevBuf<float2> motion;
+        DevBuf<float4> albedo, emission, out;
+        DevBuf<SvgfData> data[3];
+        uint32_t width = 0, height = 0;
+        uint32_t prev = 0;      // SVGFData buffer holding the previous frame's result
+        bool on = false;        // vs_denoiser_enable
+        bool rendered = false;  // a frame ran with the denoiser
+        void free() {
+            for (int k = 0; k < 2; ++k) {
+                geom[k].free();
+                history[k].free();
+            }
+            for (int k = 0; k < 3; ++k) data[k].free();
+            motion.free(); albedo.free(); emission.free(); out.free();
+            width = height = 0;
+            rendered = false;
+        }
+        SvgfBuffers view(const float4 *radiance) const {
+            SvgfBuffers b{};
+            for (int k = 0; k < 2; ++k) {
+                b.geom[k] = geom[k].ptr;
+                b.history[k] = history[k].ptr;
+            }
+            for (int k = 0; k < 3; ++k) b.data[k] = data[k].ptr;
+            b.motion = motion.ptr;
+            b.albedo = albedo.ptr;
+            b.emission = emission.ptr;
+            b.radiance = radiance;
+            b.out = out.ptr;
+            return b;
+        }
+    } svgf;
+
     ~vs_scene() {
         for (cudaEvent_t e : ev_render) cudaEventDestroy(e);
         for (cudaEvent_t e : ev_film) cudaEventDestroy(e);
@@ -247,6 +285,7 @@ struct vs_scene {
         filter_tab.free(); filter_alias.free(); tlas_inst.free(); inst_xf.free();
         film32.free(); exposed.free(); film64.free(); radiance.free(); path_counter.free(); wf.free();
         rt.free();
+        svgf.free();
         cachebuf.free();
     }
 
@@ -271,6 +310,9 @@ struct vs_scene {
         n += b(rt.hit_bsdf) + b(rt.motion) + b(rt.di_pass) + b(rt.gi_pass) + b(rt.gi_init) + b(rt.di_radiance) +
              b(rt.gi_radiance) + b(rt.di_stage) + b(rt.di_ray) + b(rt.di_hit) + b(rt.di_list) + b(rt.di_count) +
              b(rt.gs_nb) + b(rt.gs_ray) + b(rt.gs_vis) + b(rt.gs_list) + b(rt.gs_count);
+        for (int k = 0; k < 2; ++k) n += b(svgf.geom[k]) + b(svgf.history[k]);
+        for (int k = 0; k < 3; ++k) n += b(svgf.data[k]);
+        n += b(svgf.motion) + b(svgf.albedo) + b(svgf.emission) + b(svgf.out);
         n += b(wf.o) + b(wf.d) + b(wf.tp) + b(wf.lam) + b(wf.pdf) + b(wf.L) + b(wf.sh_o) + b(wf.sh_d) + b(wf.sh_c) +
              b(wf.st) + b(wf.hit) + b(wf.q0) + b(wf.q1) + b(wf.tq) + b(wf.count) + b(wf.bin_key) + b(wf.bins) +
              b(wf.binned) + b(wf.sh_perm);
@@ -378,6 +420,7 @@ int upload_scene(vs_scene *s) {
         VS_CUDA(upload_spectral_consts_serve(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_cache(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         VS_CUDA(upload_spectral_consts_wf(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
+        VS_CUDA(upload_spectral_consts_svgf(c.x, c.y, c.z, c.d65, c.y_integral), "spectral constants");
         ctx->consts_uploaded = true;
     }
     const HostScene &h = s->host;
@@ -1102,6 +1145,48 @@ int rt_ensure(vs_scene *s, cudaStream_t st) {
     return VS_OK;
 }
 
+// Clears the denoiser's history: SVGFData and history lengths to zero, the
+// G-buffer to PixelGeometry's defaults (linear depth -1: nothing to
+// reproject from).
+int svgf_reset(vs_scene *s, cudaStream_t st) {
+    vs_context *ctx = s->ctx;
+    vs_scene::Svgf &v = s->svgf;
+    const size_t n = static_cast<size_t>(v.width) * v.height;
+    if (n == 0) return VS_OK;
+    std::vector<SvgfGeom> g(n, SvgfGeom{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f});
+    for (int k = 0; k < 2; ++k) {
+        VS_CUDA(cudaMemcpyAsync(v.geom[k].ptr, g.data(), n * sizeof(SvgfGeom), cudaMemcpyHostToDevice, st),
+                "svgf reset");
+        VS_CUDA(cudaMemsetAsync(v.history[k].ptr, 0, n * sizeof(float), st), "svgf reset");
+    }
+    for (int k = 0; k < 3; ++k) VS_CUDA(cudaMemsetAsync(v.data[k].ptr, 0, n * sizeof(SvgfData), st), "svgf reset");
+    VS_CUDA(cudaStreamSynchronize(st), "svgf reset");
+    v.prev = 0;
+    v.rendered = false;
+    return VS_OK;
+}
+
+int svgf_ensure(vs_scene *s, cudaStream_t st) {
+    vs_context *ctx = s->ctx;
+    vs_scene::Svgf &v = s->svgf;
+    const uint32_t w = s->host.cam.width, h = s->host.cam.height;
+    if (v.width == w && v.height == h && v.out.ptr) return VS_OK;
+    const size_t n = static_cast<size_t>(w) * h;
+    v.free();
+    for (int k = 0; k < 2; ++k) {
+        VS_CUDA(v.geom[k].alloc(n), "svgf alloc");
+        VS_CUDA(v.history[k].alloc(n), "svgf alloc");
+    }
+    for (int k = 0; k < 3; ++k) VS_CUDA(v.data[k].alloc(n), "svgf alloc");
+    VS_CUDA(v.motion.alloc(n), "svgf alloc");
+    VS_CUDA(v.albedo.alloc(n), "svgf alloc");
+    VS_CUDA(v.emission.alloc(n), "svgf alloc");
+    VS_CUDA(v.out.alloc(n), "svgf alloc");
+    v.width = w;
+    v.height = h;
+    return svgf_reset(s, st);
+}
+
 // One ReSTIR frame on `st`; the caller holds s->mu and has checked the
 // scene.  `launches` gets the kernels launched.
 int restir_frame_locked(vs_scene *s, uint32_t frame_index, uint32_t film_index, cudaStream_t st,
@@ -1140,6 +1225,20 @@ int restir_frame_locked(vs_scene *s, uint32_t frame_index, uint32_t film_index, 
             "restir launch");
     add_launches(n);
     if (launches) *launches += n;
+    if (s->svgf.on) {
+        // The denoiser over the frame's film (SVGF::dispatch after the combine, rt.cpp:157-158).
+        rc = svgf_ensure(s, st);
+        if (rc != VS_OK) return rc;
+        unsigned m = 0;
+        uint32_t final_d = 0;
+        VS_CUDA(launch_svgf(s->device_view(), p, s->host.svgf, s->svgf.view(s->film32.ptr), s->svgf.prev, &final_d, st,
+                            &m),
+                "svgf launch");
+        s->svgf.prev = final_d;
+        s->svgf.rendered = true;
+        add_launches(m);
+        if (launches) *launches += m;
+    }
     if (s->timing) VS_CUDA(timed_event(s->ev_render), "timing event");
     if (st != ctx->stream) {
         if (!s->ev_join) VS_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "join event");
@@ -1174,6 +1273,10 @@ int restir_prepare_locked(vs_scene *s) {
         VS_CUDA(s->wf.ensure(static_cast<uint32_t>(npix), false), "wavefront slots alloc");
         VS_CUDA(s->radiance.alloc(npix), "radiance alloc");
     }
+    if (s->svgf.on) {
+        rc = svgf_ensure(s, ctx->stream);
+        if (rc != VS_OK) return rc;
+    }
     VS_CUDA(cudaStreamSynchronize(ctx->stream), "restir prepare");
     return VS_OK;
 }
@@ -1206,7 +1309,7 @@ int vs_restir_reset(vs_scene *s) {
     size_t n = static_cast<size_t>(s->rt.width) * s->rt.height;
     VS_CUDA(rt_all::launch_rt_reset(static_cast<uint32_t>(n), s->rt.view(), ctx->stream), "restir reset");
     add_launches(1);
-    return VS_OK;
+    return svgf_reset(s, ctx->stream);
 }
 
 int vs_restir_params(const vs_scene *s, uint32_t frame_index, void *dst, size_t bytes) {
@@ -1237,12 +1340,47 @@ int vs_restir_download(vs_scene *s, int which, void *dst, size_t bytes) {
         case VS_RESTIR_GI_RESERVOIRS: src = s->rt.gi[cur].ptr; elem = sizeof(GiReservoir); break;
         case VS_RESTIR_HIT_BSDF: src = s->rt.hit_bsdf.ptr; elem = sizeof(RtHitBsdf); break;
         case VS_RESTIR_GI_SAMPLES: src = s->rt.gi_init.ptr; elem = sizeof(GiReservoir); break;
+        case VS_RESTIR_DENOISED:
+        case VS_RESTIR_GBUFFER:
+        case VS_RESTIR_SVGF_ALBEDO:
+        case VS_RESTIR_SVGF_EMISSION:
+        case VS_RESTIR_SVGF_DATA:
+        case VS_RESTIR_SVGF_MOTION:
+        case VS_RESTIR_SVGF_HISTORY: {
+            if (!s->svgf.rendered) return fail(ctx, VS_E_STATE, "no frame rendered with the denoiser");
+            const vs_scene::Svgf &v = s->svgf;
+            if (which == VS_RESTIR_DENOISED) { src = v.out.ptr; elem = 16; }
+            if (which == VS_RESTIR_GBUFFER) { src = v.geom[cur].ptr; elem = sizeof(SvgfGeom); }
+            if (which == VS_RESTIR_SVGF_ALBEDO) { src = v.albedo.ptr; elem = 16; }
+            if (which == VS_RESTIR_SVGF_EMISSION) { src = v.emission.ptr; elem = 16; }
+            if (which == VS_RESTIR_SVGF_DATA) { src = v.data[v.prev].ptr; elem = sizeof(SvgfData); }
+            if (which == VS_RESTIR_SVGF_MOTION) { src = v.motion.ptr; elem = 8; }
+            if (which == VS_RESTIR_SVGF_HISTORY) { src = v.history[cur].ptr; elem = 4; }
+            break;
+        }
         default: return fail(ctx, VS_E_INVALID, "unknown ReSTIR buffer");
     }
     if (bytes != n * elem) return fail(ctx, VS_E_INVALID, "ReSTIR buffer size mismatch");
     VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     VS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream), "restir copy");
     VS_CUDA(cudaStreamSynchronize(ctx->stream), "restir sync");
+    return VS_OK;
+}
+
+int vs_denoiser_enable(vs_scene *s, int on) {
+    if (!s) return VS_E_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!s->host.rt) return fail(s->ctx, VS_E_STATE, "scene integrator is not \"rt\"");
+    s->svgf.on = on != 0;
+    return VS_OK;
+}
+
+int vs_denoiser_params(const vs_scene *s, void *dst, size_t bytes) {
+    if (!s || !dst) return VS_E_INVALID;
+    if (bytes != sizeof(SvgfParams)) return fail(s->ctx, VS_E_INVALID, "denoiser params size mismatch");
+    std::lock_guard<std::mutex> lock(const_cast<vs_scene *>(s)->mu);
+    if (!s->host.rt) return fail(s->ctx, VS_E_STATE, "scene integrator is not \"rt\"");
+    std::memcpy(dst, &s->host.svgf, sizeof(SvgfParams));
     return VS_OK;
 }
 

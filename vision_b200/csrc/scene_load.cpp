@@ -1460,6 +1460,27 @@ void load_rt(const Json &ip, HostScene &s) {
     const Json &dj = ip["direct"];
     s.rt_di = load_rt_stage(dj);
     s.rt_gi = load_rt_stage(ip["indirect"]);
+    // The denoiser node (SVGF::SVGF, svgf.h:41-51).  The reference turns SVGF
+    // on from its GUI only; here vs_denoiser_enable does.  The OIDN and OptiX
+    // denoisers are not built.
+    const Json &dn = ip["denoiser"];
+    if (dn.is_object()) {
+        const std::string t = dn["type"].as_string();
+        if (t != "svgf") throw unsupported("denoiser type '" + t + "'");
+        const Json &dp = dn["param"];
+        s.svgf.N = dp["N"].as_uint(3u);
+        if (s.svgf.N > 10u) throw unsupported("SVGF with more than 10 a-trous iterations");
+        s.svgf.alpha = dp["alpha"].as_float(0.05f);
+        s.svgf.moments_alpha = dp["moments_alpha"].as_float(0.2f);
+        s.svgf.history_limit = dp["history_limit"].as_uint(32u);
+        s.svgf.moments_radius = dp["moments_filter_radius"].as_int(3);
+        if (s.svgf.moments_radius < 0 || s.svgf.moments_radius > 5)
+            throw unsupported("SVGF moments_filter_radius outside 0..5");
+        s.svgf.sigma_rt = dp["sigma_rt"].as_float(10.0f);
+        s.svgf.sigma_normal = dp["sigma_normal"].as_float(30.0f);
+        s.svgf.reproject = dp["reproject"].as_bool(true) ? 1u : 0u;
+        s.svgf.filter_moments = dp["filter_moments"].as_bool(true) ? 1u : 0u;
+    }
     s.rt_gi.t_mis = 0u;
     s.rt_M_light = dj["M_light"].as_uint(10u);
     s.rt_M_bsdf = dj["M_bsdf"].as_uint(1u);

@@ -364,6 +364,59 @@ struct Bsdf {
         return wi;
     }
 
+    // MaterialEvaluator::albedo (material.cpp:91-98) at c = dot(shading
+    // normal, wo), as each lobe defines it: Lambert kd; MicrofacetLobe
+    // kr * F(c) (lobe.cpp:208-210: metal, mirror, plastic with kr = 1 and its
+    // Schlick F, substrate with FresnelBlend's Rd and the dielectric F at 1.5);
+    // DielectricLobe kt (1 - F) + F at |c| (lobe.cpp:308-313); the principled
+    // lobe set summed with each lobe's weight (LobeSet::albedo, lobe.cpp:
+    // 564-570): SheenLTC's tint, CoatLobe's and SpecularLobe's table values
+    // (principled_bsdf.cpp:154-160,198-205), the F82 metallic lobe, the
+    // transmission lobe; a black body reflects nothing.
+    __device__ VS_OUTLINE Spec<N> albedo(float c) const {
+        Spec<N> r = Spec<N>::fill(0.0f);
+        if (has_mat<M>(kMatDiffuse) && type == kMatDiffuse) {
+            r = kd;
+        } else if (has_mat<M>(kMatMetal) && type == kMatMetal) {
+            r = mf[0].kr * mf[0].F(c);
+        } else if (has_mat<M>(kMatGlass) && type == kMatGlass) {
+            const Spec<N> F = dl.F(fabsf(c));
+#pragma unroll
+            for (int i = 0; i < N; ++i) r.v[i] = dl.kt.v[i] * (1.0f - F.v[i]) + F.v[i];
+        } else if (has_mat<M>(kMatSubstrate) && type == kMatSubstrate) {
+            if (plastic) {
+                r = mf[0].F(c);
+            } else {
+                const float F = fresnel_dielectric(c, 1.5f);
+#pragma unroll
+                for (int i = 0; i < N; ++i) r.v[i] = kd.v[i] * F;
+            }
+        } else if (has_mat<M>(kMatPrincipled) && type == kMatPrincipled) {
+            if (w_sheen > 0.0f) r = r + sh.tint;
+            if (w_coat > 0.0f) {
+                const float x = sqrtf(sqrtf(mf[2].ax * mf[2].ax));
+                const float z = (mf[2].eta0 - kCoatIorLower) / (kCoatIorUpper - kCoatIorLower);
+                r = r + mf[2].kr * lut_sample3(luts + kLutCoat, 1, 0, x, c, z);
+            }
+            if (w_metal > 0.0f) r = r + mf[0].kr * mf[0].F(c);
+            if (has_trans) {
+                const Spec<N> F = dl.F(fabsf(c));
+#pragma unroll
+                for (int i = 0; i < N; ++i) r.v[i] += (dl.kt.v[i] * (1.0f - F.v[i]) + F.v[i]) * trans_scale;
+            }
+            if (w_spec > 0.0f) {
+                const float ior = mf[1].eta0;
+                const float x = sqrtf(sqrtf(mf[1].ax * mf[1].ay));
+                const float z = sqrtf(fabsf((ior - 1.0f) / (ior + 1.0f)));
+                const float sl = lut_sample3(luts + kLutSpecular, 1, 0, x, c, z);
+#pragma unroll
+                for (int i = 0; i < N; ++i) r.v[i] += (mf[1].fa.v[i] + sl * (1.0f - mf[1].fa.v[i])) * mf[1].kr.v[i];
+            }
+            if (w_diff > 0.0f) r = r + kd;
+        }
+        return r;
+    }
+
     // Zero the pdf of a direction whose geometric side contradicts the flags
     // (MaterialEvaluator::evaluate, material.cpp:137-147).
     __device__ __forceinline__ void discard_check(f3 wo, f3 wi, BsdfEval<N> &e) const {

@@ -61,6 +61,8 @@ struct HostScene {
     bool rt = false;
     RtStage rt_di{}, rt_gi{};
     uint32_t rt_M_light = 10, rt_M_bsdf = 1, rt_max_recursion = 5, rt_pairwise = 0;
+    // SVGF denoiser settings (the integrator's "denoiser" node; svgf.h:41-51 defaults).
+    SvgfParams svgf{3u, 0.05f, 0.2f, 32u, 3, 10.0f, 30.0f, 1u, 1u, {0u, 0u, 0u}};
     std::string spectrum_type = "hero";
     // Compressed BVH8 over the primitives.
     std::vector<Bvh8Node> nodes;

@@ -51,6 +51,14 @@ cudaError_t upload_spectral_consts_serve(const float *x, const float *y, const f
 VS_RT_DECLARE(rt_all)
 VS_RT_DECLARE(rt_diffuse)
 #undef VS_RT_DECLARE
+// svgf.cu: the SVGF passes after a real-time frame (G-buffer, gradients,
+// demodulation, reprojection, moment filter, N a-trous passes, modulation).
+// `prev_d` is the SVGFData buffer that holds the previous frame's result;
+// *final_d gets the one that holds this frame's.
+cudaError_t upload_spectral_consts_svgf(const float *x, const float *y, const float *z, const float *d65,
+                                       float y_integral);
+cudaError_t launch_svgf(const DeviceScene &s, const RtParams &p, const SvgfParams &sp, const SvgfBuffers &b,
+                        uint32_t prev_d, uint32_t *final_d, cudaStream_t st, unsigned *launches);
 // Exposed and tone-mapped pictures of the linear film (k_film_picture):
 // `passes` applications of the tone mapper, then the sRGB gamma if asked;
 // float4 to `out`, or 8-bit RGBA to `out8` when it is not null.

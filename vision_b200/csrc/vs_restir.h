@@ -140,4 +140,57 @@ struct RtBuffers {
     uint32_t *gs_count;
 };
 
+// SVGF denoiser of the real-time frame (src/render_core/denoisers/SVGF/).
+// Settings (svgf.h:28-51; reproject / filter_moments are its pass switches),
+// 48 bytes.
+struct SvgfParams {
+    uint32_t N;               // a-trous iterations (step widths 1, 2, 4, ...)
+    float alpha;              // temporal blend of the illumination
+    float moments_alpha;      // temporal blend of the moments
+    uint32_t history_limit;
+    int32_t moments_radius;   // spatial variance estimate while history < 4
+    float sigma_rt;           // luminance edge stop
+    float sigma_normal;       // normal edge stop (exponent)
+    uint32_t reproject;
+    uint32_t filter_moments;
+    uint32_t pad[3];
+};
+static_assert(sizeof(SvgfParams) == 48, "SvgfParams must be 48 bytes");
+
+// PixelGeometry (frame_buffer.h:15-21), 32 bytes: shading normal and its
+// screen-space width, film position, depth gradient, linear depth (-1: the
+// camera ray left the scene).
+struct alignas(16) SvgfGeom {
+    float nx, ny, nz, fwidth;
+    float px, py;
+    float depth_gradient;
+    float linear_depth;
+};
+static_assert(sizeof(SvgfGeom) == 32, "SvgfGeom must be 32 bytes");
+
+// SVGFData (utils.h:19-24), 32 bytes: demodulated illumination and its
+// variance, history length, first and second luminance moments.
+struct alignas(16) SvgfData {
+    float ix, iy, iz, var;
+    float history;
+    float m1, m2;
+    float pad;
+};
+static_assert(sizeof(SvgfData) == 32, "SvgfData must be 32 bytes");
+
+// Buffers of the denoiser.  The G-buffer and the history lengths are
+// double-buffered by frame parity (frame f writes (f+1)&1, reads f&1); the
+// three SVGFData buffers rotate: `prev` holds the last frame's filtered
+// result, `cur` and `tmp` take this frame's passes in turn.
+struct SvgfBuffers {
+    SvgfGeom *geom[2];
+    float *history[2];
+    float2 *motion;
+    float4 *albedo;
+    float4 *emission;
+    SvgfData *data[3];
+    const float4 *radiance;  // the frame's film (running mean), demodulated
+    float4 *out;             // the denoised frame
+};
+
 }  // namespace vs
