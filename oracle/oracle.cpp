@@ -1262,7 +1262,7 @@ struct Bsdf {
     int n = 1;
     Frame fr;
     V3 ng;
-    Lobe lobes[6];
+    Lobe lobes[12];  // a mix of two principled materials holds two lobe sets
     int count = 0;
     bool lobe_set = false;  // LobeSet: world-space hemisphere factors and a 1D lobe choice
     bool dispersive = false;
@@ -1750,6 +1750,34 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
             if (!(l->sample_weight > 0.0f)) continue;
             l->sample_weight /= sum;
             b.lobes[b.count++] = *l;
+        }
+    } else if (m.type == 6) {
+        // MixMaterial / AddMaterial (mix.cpp:62-68, add.cpp:56-59):
+        // LobeSet::create_mix / create_add (lobe.cpp:495-521), flattened
+        // (LobeSet::flatten, lobe.cpp:533-560): a principled child's lobes
+        // with weight and sample weight scaled by its sample weight, a
+        // single-lobe child's lobe with its weight and sample weight.  mix:
+        // (1 - frac, frac) for both; add: weights 1, sample weights 1/2.  The
+        // lobe set is not dispersive (LobeSet keeps Lobe::is_dispersive).
+        const bool add = (m.flags & 16u) != 0;
+        const float wt[2] = {add ? 1.0f : 1.0f - m.p[0], add ? 1.0f : m.p[0]};
+        const float swt[2] = {add ? 0.5f : 1.0f - m.p[0], add ? 0.5f : m.p[0]};
+        const Bsdf c[2] = {make_bsdf(sc, sc.mat[m.spd0], it, w), make_bsdf(sc, sc.mat[m.spd1], it, w)};
+        b.count = 0;
+        b.lobe_set = true;
+        b.dispersive = false;
+        for (int k = 0; k < 2; ++k) {
+            for (int j = 0; j < c[k].count; ++j) {
+                Lobe l = c[k].lobes[j];
+                if (c[k].lobe_set) {
+                    l.weight *= swt[k];
+                    l.sample_weight *= swt[k];
+                } else {
+                    l.weight = wt[k];
+                    l.sample_weight = swt[k];
+                }
+                b.lobes[b.count++] = l;
+            }
         }
     } else {
         l0.kind = Lobe::NoScatter;

@@ -63,8 +63,8 @@ assert MATERIAL.itemsize == 64 and LIGHT.itemsize == 112 and CAMERA.itemsize == 
 assert INTEGRATOR.itemsize == 48 and ENV.itemsize == 160
 
 # Material types and flags of the flat format.
-DIFFUSE, BLACK_BODY, METAL, GLASS, PRINCIPLED, SUBSTRATE = range(6)
-FLAG_DISPERSIVE, FLAG_REMAP, FLAG_CONST_FRESNEL, FLAG_PLASTIC = 1, 2, 4, 8
+DIFFUSE, BLACK_BODY, METAL, GLASS, PRINCIPLED, SUBSTRATE, MIX = range(7)
+FLAG_DISPERSIVE, FLAG_REMAP, FLAG_CONST_FRESNEL, FLAG_PLASTIC, FLAG_ADD = 1, 2, 4, 8, 16
 EMIT_RGB, EMIT_BLACKBODY = 0, 1
 LIGHT_AREA, LIGHT_POINT, LIGHT_SPOT = 0, 1, 2
 FILTERS = {'box': 0, 'triangle': 1, 'gaussian': 2, 'mitchell': 3, 'sinc': 4}
@@ -643,7 +643,8 @@ class _Builder:
 
     def material(self, m):
         """Material records (diffuse.cpp, black_body.cpp, metal.cpp, glass.cpp,
-        principled_bsdf.cpp, mirror.cpp, substrate.cpp, plastic.cpp)."""
+        principled_bsdf.cpp, mirror.cpp, substrate.cpp, plastic.cpp, mix.cpp,
+        add.cpp)."""
         t, p = m.get('type', 'diffuse'), m.get('param', {}) or {}
         r = np.zeros(1, MATERIAL)[0]
         r['spd0'] = r['spd1'] = INVALID
@@ -656,7 +657,25 @@ class _Builder:
 
         def clamp(x, lo, hi):
             return F(min(max(F(x), F(lo)), F(hi)))
-        if t == 'diffuse':
+        if t in ('mix', 'add'):
+            # MixMaterial / AddMaterial (mix.cpp:20-68, add.cpp:12-59): the two
+            # inline material nodes (node_desc.cpp:155-161) as records of their
+            # own, named after this one, then this record with their indices.
+            r['type'] = MIX
+            if t == 'add':
+                r['flags'] |= FLAG_ADD
+            else:
+                r['p'][0] = _slot_scalar(p.get('frac'), 0.5)
+            for k in (0, 1):
+                c = p.get('mat%d' % k)
+                if not isinstance(c, dict):
+                    raise ValueError('material %s: missing mat%d' % (m.get('name', ''), k))
+                if c.get('type', 'diffuse') in ('mix', 'add', 'black_body'):
+                    raise Unsupported('%s inside a mix / add material' % c.get('type'))
+                c = dict(c, name='%s/mat%d' % (m.get('name', ''), k))
+                self.material(c)
+                r['spd0' if k == 0 else 'spd1'] = len(self.materials) - 1
+        elif t == 'diffuse':
             r['type'] = DIFFUSE
             r['coef'] = self.colour(_slot_rgb(p.get('color'), 0.5))
         elif t == 'black_body':

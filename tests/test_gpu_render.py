@@ -134,6 +134,41 @@ def test_matched_seed_parity_principled_layers(vb, gpu_ctx):
     assert _match(gs / 32, cs / 32, 2e-3) >= 0.85
 
 
+def test_matched_seed_parity_mix_and_add(vb, gpu_ctx):
+    # MixMaterial / AddMaterial over glass pairs, diffuse + conductor, diffuse
+    # + principled and plastic + substrate (LobeSet::create_mix / create_add,
+    # flattened).  One scattering event agrees per pixel; at full depth the
+    # mixed glass box is rounding-sensitive like the glass, so the bar is a
+    # per-pixel z-test.  The megakernel schedules do not compile mixes.
+    from helpers import mean_z, path_sums, pixel_z
+    s = vb.Scene(gpu_ctx, scenes.mix_room(64, 64, max_depth=2)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 1e-3) >= 0.99
+    s = vb.Scene(gpu_ctx, scenes.mix_room(48, 48)).build_accel()
+    o = oracle.OracleScene.from_json(scenes.mix_room(48, 48))
+    s.render(0, 32, fp64=True)
+    gs, gq = s.film(vb.FILM_SUM64)[..., :3], s.film(vb.FILM_SUMSQ64)[..., :3]
+    cs, cq = path_sums(o.paths(np.arange(48 * 48, dtype=np.uint32), 0, 32))
+    cs, cq = cs.reshape(48, 48, 3), cq.reshape(48, 48, 3)
+    assert np.all(np.isfinite(gs))
+    z = pixel_z(gs, gq, 32, cs, cq, 32)
+    assert (np.abs(z) > 4.0).mean() <= 0.005
+    assert abs(mean_z(gs, gq, 32, cs, cq, 32)) < 4.0
+    films = []
+    for schedule in ('wavefront', 'wavefront_binned'):
+        t = vb.Scene(gpu_ctx, scenes.mix_room(32, 32)).build_accel()
+        t.set_schedule(schedule)
+        t.render(0, 4)
+        films.append(t.film())
+    assert np.array_equal(films[0], films[1])
+    t.set_schedule('grid')
+    with pytest.raises(vb.UnsupportedError, match='wavefront'):
+        t.render(0, 1)
+
+
 def test_matched_seed_parity_plastic(vb, gpu_ctx):
     # PlasticLobe: Lambert (1 - F) plus Schlick-weighted GGX reflection.
     s = vb.Scene(gpu_ctx, scenes.plastic_room(64, 64, max_depth=2)).build_accel()

@@ -156,3 +156,33 @@ def test_plastic_records(vb, host_ctx):
         assert mats[i, 0] == 5 and (mats[i, 1] & 8)
         np.testing.assert_allclose(matf[i, 8:10], [max(alpha, 1e-4)] * 2, rtol=1e-5)
         np.testing.assert_allclose(matf[i, 13], ior, rtol=1e-6)
+
+
+def test_mix_and_add_records(vb, host_ctx):
+    # MixMaterial / AddMaterial: the inline children become records of their
+    # own, in front of the mix record, which holds their indices, the mix
+    # fraction and the add flag.
+    s = vb.Scene(host_ctx, scenes.mix_room(16, 16))
+    from oracle.scene import MATERIAL, MIX, FLAG_ADD, GLASS, DIFFUSE, METAL, PRINCIPLED
+    m = s.export('materials').view(MATERIAL)
+    mixes = np.nonzero(m['type'] == MIX)[0]
+    assert len(mixes) == 4
+    kinds = sorted((int(m['type'][m['spd0'][i]]), int(m['type'][m['spd1'][i]]), bool(m['flags'][i] & FLAG_ADD),
+                    round(float(m['p'][i][0]), 3)) for i in mixes)
+    assert (GLASS, GLASS, False, 0.5) in kinds and (DIFFUSE, METAL, False, 0.3) in kinds
+    assert any(k[:3] == (DIFFUSE, PRINCIPLED, True) for k in kinds)
+    for i in mixes:
+        assert m['spd0'][i] < i and m['spd1'][i] < i
+
+
+def test_mix_refusals(vb, host_ctx):
+    sc = scenes.mix_room(16, 16)
+    for mt in sc['materials']:
+        if mt['name'] == 'TallBox':
+            mt['param']['mat1'] = {'type': 'mix', 'param': {'mat0': {'type': 'diffuse'}, 'mat1': {'type': 'diffuse'}}}
+    with pytest.raises(vb.UnsupportedError, match='mix'):
+        vb.Scene(host_ctx, sc)
+    sc = scenes.mix_room(16, 16, dimension=3)
+    sc['integrator'] = {'type': 'rt', 'param': {'max_depth': 4}}
+    with pytest.raises(vb.UnsupportedError, match='rt integrator'):
+        vb.Scene(host_ctx, sc)

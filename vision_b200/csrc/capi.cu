@@ -390,6 +390,17 @@ cudaStream_t pick_stream(const vs_scene *s, void *stream) {
 
 // Shading classes of the wavefront that a scene can produce: misses and one
 // class per material type present.
+// Mix / add materials have a shading class of their own (a composite BSDF of
+// two child lobe sets), compiled only into the wavefront schedule's class
+// kernels; the kernels built for a fixed material set (megakernel schedules,
+// the allocation-free render, the instrumented render, the radiance-cache
+// frame, the render server) do not take them.
+bool has_mix(const HostScene &h) {
+    for (const Material &mt : h.materials)
+        if (mt.type == kMatMix) return true;
+    return false;
+}
+
 uint32_t shading_classes(const HostScene &h) {
     uint32_t m = 1u;
     for (const Material &mt : h.materials) m |= 1u << (1u + mt.type);
@@ -499,6 +510,7 @@ int noalloc_prepare(vs_scene *s, void *stream, DeviceScene *view, cudaStream_t *
     vs_context *ctx = s->ctx;
     if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
     if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render_noalloc");
+    if (has_mix(s->host)) return fail(ctx, VS_E_UNSUPPORTED, "mix / add materials in the allocation-free render");
     VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     *view = s->device_view();
     *st = pick_stream(s, stream);
@@ -774,6 +786,8 @@ int vs_render(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, int film_
     VS_CUDA(s->radiance.alloc(static_cast<size_t>(frames_per_chunk * npix)), "radiance alloc");
     if (s->schedule == VS_SCHEDULE_PERSISTENT) VS_CUDA(s->path_counter.alloc(1), "path counter alloc");
     const bool wavefront = s->schedule == VS_SCHEDULE_WAVEFRONT || s->schedule == VS_SCHEDULE_WAVEFRONT_BINNED;
+    if (!wavefront && has_mix(s->host))
+        return fail(ctx, VS_E_UNSUPPORTED, "mix / add materials render with the wavefront schedules only");
     if (wavefront)
         VS_CUDA(s->wf.ensure(static_cast<uint32_t>(std::min<uint64_t>(frames_per_chunk * npix, kWfWaveSlots)),
                              s->schedule == VS_SCHEDULE_WAVEFRONT_BINNED),
@@ -1025,6 +1039,7 @@ int vs_render_stats(vs_scene *s, uint32_t frame_begin, uint32_t frame_count, uin
     if (ctx->device < 0) return fail(ctx, VS_E_NO_DEVICE, "host-only context cannot render");
     std::lock_guard<std::mutex> lock(s->mu);
     if (!s->uploaded) return fail(ctx, VS_E_STATE, "vs_scene_build_accel must precede vs_render_stats");
+    if (has_mix(s->host)) return fail(ctx, VS_E_UNSUPPORTED, "mix / add materials in the instrumented render");
     VS_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     uint64_t npix = static_cast<uint64_t>(s->host.cam.width) * s->host.cam.height;
     if (npix * frame_count > kMaxPathsPerLaunch) return fail(ctx, VS_E_RANGE, "too many paths for one instrumented launch");
@@ -1432,6 +1447,7 @@ int vs_server_add_scene(vs_server *s, vs_scene *scene, uint32_t *scene_id) {
     {
         std::lock_guard<std::mutex> lock(scene->mu);
         if (!scene->uploaded) return s->fail(VS_E_STATE, "vs_scene_build_accel must precede vs_server_add_scene");
+        if (has_mix(scene->host)) return s->fail(VS_E_UNSUPPORTED, "mix / add materials in served scenes");
         if (scene->ctx->device != s->ctx->device) return s->fail(VS_E_INVALID, "scene on another device");
         rt = scene->host.rt;
         if (rt) {
@@ -1703,6 +1719,7 @@ int vs_render_cached(vs_scene *s, vs_cache *c, uint32_t frame_begin, uint32_t fr
     const HostScene &h = s->host;
     if (h.ip.spectrum_dim != 3)
         return fail(ctx, VS_E_UNSUPPORTED, "cache rendering needs 3 hero wavelengths (the cache's 3 outputs)");
+    if (has_mix(h)) return fail(ctx, VS_E_UNSUPPORTED, "mix / add materials in cache rendering");
     if (frame_begin != 0 && frame_begin != s->film_frames)
         return fail(ctx, VS_E_STATE, "frames must continue the film (frame_begin == frames rendered) or restart at 0");
     if (film_precision == VS_FILM_FP64 && frame_begin != 0 && !s->film64_valid)

@@ -839,7 +839,28 @@ struct Loader {
         Material mat{};
         mat.spd0 = mat.spd1 = kInvalid;
         f3 rgb = make3(0.0f);
-        if (type == "diffuse") {
+        if (type == "mix" || type == "add") {
+            // MixMaterial / AddMaterial (mix.cpp:20-68, add.cpp:12-59): two
+            // inline material nodes (MaterialDesc::init, node_desc.cpp:155-161)
+            // loaded as records of their own (named after this one), and the
+            // mix fraction slot (default 0.5).
+            mat.type = kMatMix;
+            if (type == "add") mat.flags |= kMatFlagAdd;
+            else mat.p[0] = slot_scalar(p["frac"], 0.5f);
+            uint32_t child[2];
+            for (int k = 0; k < 2; ++k) {
+                Json c = p[k == 0 ? "mat0" : "mat1"];
+                if (!c.is_object()) throw std::runtime_error("material '" + name + "': missing mat" + std::to_string(k));
+                const std::string ct = c["type"].as_string("diffuse");
+                if (ct == "mix" || ct == "add") throw unsupported("mix / add material inside a mix / add (" + name + ")");
+                if (ct == "black_body") throw unsupported("black_body inside a mix / add material (" + name + ")");
+                c.set("name", Json::string(name + "/mat" + std::to_string(k)));
+                load_material(c);
+                child[k] = static_cast<uint32_t>(s.materials.size()) - 1u;
+            }
+            mat.spd0 = child[0];
+            mat.spd1 = child[1];
+        } else if (type == "diffuse") {
             // DiffuseMaterial: colour slot, default 0.5 (diffuse.cpp:37-44).
             mat.type = kMatDiffuse;
             rgb = slot_rgb(p["color"], make3(0.5f));
@@ -1454,6 +1475,8 @@ RtStage load_rt_stage(const Json &d) {
 // paths of the indirect samples.
 void load_rt(const Json &ip, HostScene &s) {
     if (s.ip.spectrum_dim != 3) throw unsupported("rt integrator with a hero dimension other than 3");
+    for (const Material &m : s.materials)
+        if (m.type == kMatMix) throw unsupported("mix / add materials with the rt integrator");
     if (s.ip.max_depth < 3) throw unsupported("rt integrator with max_depth below 3");
     s.rt = true;
     s.ip.max_depth -= 1u;

@@ -425,10 +425,10 @@ struct Bsdf {
         if (same == trans) e.pdf = 0.0f;
     }
 
-    __device__ VS_OUTLINE BsdfEval<N> evaluate(f3 wo_w, f3 wi_w, float *eta_out) const {
+    // The lobe set at local directions, before MaterialEvaluator's check of
+    // the geometric side; a dielectric lobe sets eta.
+    __device__ __forceinline__ BsdfEval<N> eval_core(f3 wo, f3 wi, float &eta) const {
         BsdfEval<N> e;
-        f3 wo = frame.to_local(wo_w), wi = frame.to_local(wi_w);
-        float eta = 1.0f;
         float acos_i = fabsf(wi.z);
         if (has_mat<M>(kMatDiffuse) && type == kMatDiffuse) {
             bool s = wo.z * wi.z > 0.0f;
@@ -510,17 +510,37 @@ struct Bsdf {
             e.pdf = 1.0f;
             e.flags = kFlagUnset;
         }
+        return e;
+    }
+
+    __device__ VS_OUTLINE BsdfEval<N> evaluate(f3 wo_w, f3 wi_w, float *eta_out) const {
+        f3 wo = frame.to_local(wo_w), wi = frame.to_local(wi_w);
+        float eta = 1.0f;
+        BsdfEval<N> e = eval_core(wo, wi, eta);
         if (eta_out) *eta_out = eta;
         discard_check(wo_w, wi_w, e);
         return e;
     }
 
-    __device__ VS_OUTLINE BsdfSample<N> sample(f3 wo_w, Sampler &smp) const {
-        BsdfSample<N> bs;
-        bs.eta = 1.0f;
-        f3 wo = frame.to_local(wo_w);
-        bool valid = true;
+    // Lobe k of the principled lobe set (sheen, coat, metallic, transmission,
+    // specular, diffuse) drawing its own direction.
+    __device__ __forceinline__ f3 sample_principled_lobe(int k, f3 wo, Sampler &smp, bool &valid) const {
         f3 wi;
+        if (k == 0) wi = sh.sample_local(smp.next2());
+        else if (k == 1) wi = mf[2].sample_local(wo, smp.next2(), valid);
+        else if (k == 2) wi = mf[0].sample_local(wo, smp.next2(), valid);
+        else if (k == 3) wi = dl.sample_local(wo, smp, valid);
+        else if (k == 4) wi = mf[1].sample_local(wo, smp.next2(), valid);
+        else {
+            wi = cosine_hemisphere(smp.next2());
+            wi.z = wo.z < 0.0f ? -wi.z : wi.z;
+        }
+        return wi;
+    }
+
+    // The direction draws of a scattering material's lobe (set).
+    __device__ __forceinline__ f3 sample_dir(f3 wo, Sampler &smp, bool &valid) const {
+        f3 wi = wo;
         if (has_mat<M>(kMatDiffuse) && type == kMatDiffuse) {
             wi = cosine_hemisphere(smp.next2());
             wi.z = wo.z < 0.0f ? -wi.z : wi.z;
@@ -547,22 +567,28 @@ struct Bsdf {
                 strategy = uc > sum ? i : strategy;
                 sum += ws[i];
             }
-            if (strategy == 0) wi = sh.sample_local(smp.next2());
-            else if (strategy == 1) wi = mf[2].sample_local(wo, smp.next2(), valid);
-            else if (strategy == 2) wi = mf[0].sample_local(wo, smp.next2(), valid);
-            else if (strategy == 3) wi = dl.sample_local(wo, smp, valid);
-            else if (strategy == 4) wi = mf[1].sample_local(wo, smp.next2(), valid);
-            else {
-                wi = cosine_hemisphere(smp.next2());
-                wi.z = wo.z < 0.0f ? -wi.z : wi.z;
-            }
-        } else {
+            wi = sample_principled_lobe(strategy, wo, smp, valid);
+        }
+        return wi;
+    }
+
+    __device__ VS_OUTLINE BsdfSample<N> sample(f3 wo_w, Sampler &smp) const {
+        BsdfSample<N> bs;
+        bs.eta = 1.0f;
+        const bool scatters = (has_mat<M>(kMatDiffuse) && type == kMatDiffuse) ||
+                              (has_mat<M>(kMatMetal) && type == kMatMetal) ||
+                              (has_mat<M>(kMatGlass) && type == kMatGlass) ||
+                              (has_mat<M>(kMatSubstrate) && type == kMatSubstrate) ||
+                              (has_mat<M>(kMatPrincipled) && type == kMatPrincipled);
+        if (!scatters) {
             bs.wi = wo_w;
             bs.eval.f = Spec<N>::fill(0.0f);
             bs.eval.pdf = 1.0f;
             bs.eval.flags = kFlagDiffRefl;
             return bs;
         }
+        bool valid = true;
+        const f3 wi = sample_dir(frame.to_local(wo_w), smp, valid);
         bs.wi = frame.to_world(wi);
         bs.eval = evaluate(wo_w, bs.wi, &bs.eta);
         if (!valid) bs.eval.pdf = 0.0f;
@@ -773,5 +799,126 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
     }
     return b;
 }
+
+// MixMaterial / AddMaterial (mix.cpp:62-68, add.cpp:56-59): LobeSet::create_mix
+// / create_add (lobe.cpp:495-521) over the two materials' lobe sets,
+// flattened (LobeSet::flatten, lobe.cpp:533-560, the registry's default): a
+// child that is itself a lobe set (principled) contributes its lobes with
+// weights and sample weights scaled by its sample weight; a single-lobe child
+// contributes its lobe with its weight and sample weight, masked by the lobe's
+// hemisphere factor (valid_world_factor, lobe.cpp:35-38; 1 for a dielectric
+// lobe).  mix: weights = sample weights = (1 - frac, frac); add: weights 1,
+// sample weights normalised to 1/2 (LobeSet::initialize), so a principled
+// child of an add counts at half weight.  LobeSet does not override
+// is_dispersive, so a mix leaves the secondary wavelengths alone.
+template <int N>
+struct MixBsdf {
+    Bsdf<N> c[2];
+    float w[2], sw[2];
+    bool dispersive;
+
+    __device__ __forceinline__ static bool multi(const Bsdf<N> &b) { return b.type == kMatPrincipled; }
+
+    __device__ VS_OUTLINE BsdfEval<N> evaluate(f3 wo_w, f3 wi_w, float *eta_out) const {
+        const f3 wo = c[0].frame.to_local(wo_w), wi = c[0].frame.to_local(wi_w);
+        const bool same = wo.z * wi.z > 0.0f;
+        float eta = 1.0f;
+        BsdfEval<N> e;
+        e.f = Spec<N>::fill(0.0f);
+        e.pdf = 0.0f;
+        e.flags = 0u;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const BsdfEval<N> ek = c[k].eval_core(wo, wi, eta);
+            const bool m = multi(c[k]);
+            const float factor = (m || c[k].type == kMatGlass || same) ? 1.0f : 0.0f;
+            e.f = e.f + ek.f * ((m ? sw[k] : w[k]) * factor);
+            e.pdf += ek.pdf * (sw[k] * factor);
+            e.flags |= ek.flags;
+        }
+        if (eta_out) *eta_out = eta;
+        c[0].discard_check(wo_w, wi_w, e);
+        return e;
+    }
+
+    // LobeSet::sample_wi_impl (lobe.cpp:598-627) over the flattened lobes.
+    __device__ VS_OUTLINE BsdfSample<N> sample(f3 wo_w, Sampler &smp) const {
+        const f3 wo = c[0].frame.to_local(wo_w);
+        const float uc = smp.next();
+        (void)smp.next2();
+        int child = 0, lobe = -1;
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const Bsdf<N> &b = c[k];
+            if (multi(b)) {
+                const float ws[6] = {b.w_sheen, b.w_coat, b.w_metal, b.w_trans, b.w_spec, b.w_diff};
+                const bool present[6] = {b.w_sheen > 0.0f, b.w_coat > 0.0f, b.w_metal > 0.0f, b.has_trans,
+                                         b.w_spec > 0.0f, b.w_diff > 0.0f};
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    if (!present[i]) continue;
+                    if (uc > sum) {
+                        child = k;
+                        lobe = i;
+                    }
+                    sum += ws[i] * sw[k];
+                }
+            } else {
+                if (uc > sum) {
+                    child = k;
+                    lobe = -1;
+                }
+                sum += sw[k];
+            }
+        }
+        bool valid = true;
+        const Bsdf<N> &b = c[child];
+        const f3 wi = lobe < 0 ? b.sample_dir(wo, smp, valid) : b.sample_principled_lobe(lobe, wo, smp, valid);
+        BsdfSample<N> bs;
+        bs.eta = 1.0f;
+        bs.wi = c[0].frame.to_world(wi);
+        bs.eval = evaluate(wo_w, bs.wi, &bs.eta);
+        if (!valid) bs.eval.pdf = 0.0f;
+        return bs;
+    }
+};
+
+template <int N>
+__device__ VS_OUTLINE MixBsdf<N> make_mix_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng,
+                                              f3 wo, const Wavelengths<N> &wl) {
+    MixBsdf<N> r;
+    r.c[0] = make_bsdf<N>(s, s.materials[m.spd0], frame, ng, wo, wl);
+    r.c[1] = make_bsdf<N>(s, s.materials[m.spd1], frame, ng, wo, wl);
+    if (m.flags & kMatFlagAdd) {
+        r.w[0] = r.w[1] = 1.0f;
+        r.sw[0] = r.sw[1] = 0.5f;
+    } else {
+        r.w[0] = r.sw[0] = 1.0f - m.p[0];
+        r.w[1] = r.sw[1] = m.p[0];
+    }
+    r.dispersive = false;
+    return r;
+}
+
+// The BSDF type path shading builds for a material mask: the mix class gets
+// the composite, every other mask the one-material Bsdf.
+constexpr uint32_t kMixMask = 1u << kMatMix;
+template <int N, uint32_t M>
+struct ShadeBsdf {
+    using type = Bsdf<N, M>;
+    __device__ __forceinline__ static type make(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng,
+                                                f3 wo, const Wavelengths<N> &wl) {
+        return make_bsdf<N, M>(s, m, frame, ng, wo, wl);
+    }
+};
+template <int N>
+struct ShadeBsdf<N, kMixMask> {
+    using type = MixBsdf<N>;
+    __device__ __forceinline__ static type make(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng,
+                                                f3 wo, const Wavelengths<N> &wl) {
+        return make_mix_bsdf<N>(s, m, frame, ng, wo, wl);
+    }
+};
 
 }  // namespace vs

@@ -16,6 +16,7 @@ enum MaterialType : uint32_t {
     kMatGlass = 3,       // glass.cpp: rough dielectric, optionally dispersive
     kMatPrincipled = 4,  // principled_bsdf.cpp
     kMatSubstrate = 5,   // substrate.cpp: FresnelBlend (glossy coat over diffuse)
+    kMatMix = 6,         // mix.cpp / add.cpp: two materials' lobe sets; spd0 / spd1 hold their indices
 };
 
 enum MaterialFlag : uint32_t {
@@ -23,6 +24,7 @@ enum MaterialFlag : uint32_t {
     kMatFlagRemapRoughness = 2u,
     kMatFlagConstantFresnel = 4u,  // kMatMetal written by a `mirror` (mirror.cpp): F = 1, kr = colour
     kMatFlagPlastic = 8u,          // kMatSubstrate written by a `plastic` (plastic.cpp): PlasticLobe
+    kMatFlagAdd = 16u,             // kMatMix written by an `add` (add.cpp): weights 1, sample weights 1/2
 };
 
 // 64 bytes.  `coef` holds RGB->spectrum sigmoid coefficients (c0, c1, c2) of

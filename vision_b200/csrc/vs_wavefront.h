@@ -49,7 +49,7 @@ constexpr uint32_t kWfBins = 1u << kWfBinBits;
 
 // Shading classes of a hit: 0 = miss, 1 + MaterialType otherwise.  Each class
 // is shaded by its own kernel, compiled with that material's code only.
-constexpr uint32_t kWfClasses = 7;
+constexpr uint32_t kWfClasses = 8;
 constexpr uint32_t kWfFetchExtend = 3 + kWfClasses;
 constexpr uint32_t kWfFetchShadow = kWfFetchExtend + 1;
 constexpr uint32_t kWfCounters = kWfFetchShadow + 1;

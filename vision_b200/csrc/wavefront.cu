@@ -219,6 +219,8 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
     if ((e = shade_grid<N, 4>(dev, sg)) != cudaSuccess) return e;
     if ((e = shade_grid<N, 5>(dev, sg)) != cudaSuccess) return e;
     if ((e = shade_grid<N, 6>(dev, sg)) != cudaSuccess) return e;
+    if ((class_mask >> 7) & 1u)
+        if ((e = shade_grid<N, 7>(dev, sg)) != cudaSuccess) return e;
     const uint32_t mask = class_mask | 1u;
     unsigned n_launch = 0;
     const bool binning = b.bin_key && b.bins && b.binned && b.sh_perm;
@@ -256,6 +258,7 @@ cudaError_t wave_loop(const DeviceScene &s, uint32_t frame_begin, uint64_t paths
             launch_shade<N, 4>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 5>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             launch_shade<N, 6>(sg, mask, s, b, cur, base, radiance, st, n_launch);
+            launch_shade<N, 7>(sg, mask, s, b, cur, base, radiance, st, n_launch);
             if (binning) {
                 k_bin_count<<<grid_bin, 256, 0, st>>>(s, b.count + 2, nullptr, b.sh_o, b.sh_d, b.bin_key, b.bins);
                 k_bin_scan<<<1, 1024, 0, st>>>(b.bins);

@@ -144,6 +144,33 @@ def plastic_room(width=64, height=64, dimension=4, sampler="independent", max_de
     return sc
 
 
+def mix_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
+    """The box room with mix and add materials (MixMaterial / AddMaterial):
+    the tall box mixes two BK7 glasses half and half (the reference's
+    cbox/vision_scene.json `mix` material), the short box mixes a diffuse
+    and a gold conductor (frac 0.3), the floor adds a diffuse and a coated
+    principled BSDF, the back wall mixes a plastic and a substrate (frac
+    0.6)."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    mats = {m["name"]: m for m in sc["materials"]}
+    glass = {"type": "glass", "param": {"material_name": "BK7", "color": {"channels": "xyz", "node": [1, 1, 1]},
+                                        "roughness": [0.001, 0.001]}}
+    mats["TallBox"].update({"type": "mix", "param": {"mat0": glass, "mat1": dict(glass)}})
+    mats["ShortBox"].update({"type": "mix", "param": {
+        "frac": 0.3,
+        "mat0": {"type": "diffuse", "param": {"color": [0.7, 0.3, 0.2]}},
+        "mat1": {"type": "metal", "param": {"material_name": "Au", "roughness": 0.2}}}})
+    mats["Floor"].update({"type": "add", "param": {
+        "mat0": {"type": "diffuse", "param": {"color": [0.3, 0.3, 0.35]}},
+        "mat1": {"type": "principled_bsdf", "param": {"color": [0.6, 0.5, 0.4], "metallic": 0.2, "roughness": 0.4,
+                                                      "coat_weight": 0.5, "coat_roughness": 0.1}}}})
+    mats["BackWall"].update({"type": "mix", "param": {
+        "frac": 0.6,
+        "mat0": {"type": "plastic", "param": {"color": [0.2, 0.4, 0.7], "roughness": 0.2}},
+        "mat1": {"type": "substrate", "param": {"color": [0.6, 0.5, 0.3], "roughness": 0.3}}}})
+    return sc
+
+
 def point_light_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8, light_sampler="uniform",
                      area_light=True):
     """The box room lit by a white point light near the ceiling and a warm
