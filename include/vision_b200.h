@@ -186,6 +186,8 @@ int vs_scene_info_get(const vs_scene *scene, vs_scene_info *out);
 #define VS_EXPORT_MESHES 29     /* 24 bytes per mesh: first vertex, vertex count, first triangle, count, hash */
 #define VS_EXPORT_INST_MESH 30  /* uint32 per instance */
 #define VS_EXPORT_INST_W2O 31   /* float[16] per instance, column-major world-to-object */
+#define VS_EXPORT_TEXELS 32     /* float[4] per texel of the image-node textures (linear RGB, 0) */
+#define VS_EXPORT_TEXTURES 33   /* 16 bytes per texture: texel offset, width, height, 0 */
 int vs_scene_export_size(const vs_scene *scene, int what, size_t *bytes);
 int vs_scene_export(const vs_scene *scene, int what, void *dst, size_t bytes);
 

@@ -42,7 +42,8 @@ class OracleSceneStruct(ctypes.Structure):
                 ('env_cond_func', ctypes.c_void_p), ('rgb2spec', ctypes.c_void_p),
                 ('two_level', ctypes.c_uint32), ('mesh_count', ctypes.c_uint32), ('mesh_pos', ctypes.c_void_p),
                 ('mesh_idx', ctypes.c_void_p), ('meshes', ctypes.c_void_p), ('inst_mesh', ctypes.c_void_p),
-                ('inst_w2o', ctypes.c_void_p)]
+                ('inst_w2o', ctypes.c_void_p), ('tex_texels', ctypes.c_void_p), ('textures', ctypes.c_void_p),
+                ('texture_count', ctypes.c_uint32)]
 
 
 _lib = None
@@ -118,6 +119,7 @@ SCENE_KEYS = ['pos', 'nrm', 'uv', 'idx', 'prim_inst', 'instances', 'materials', 
               'light_alias', 'light_pmf', 'camera', 'integrator', 'spd']
 ENV_KEYS = ['env', 'env_tex', 'env_marginal', 'env_marginal_func', 'env_cond', 'env_cond_func', 'rgb2spec']
 INSTANCE_KEYS = ['mesh_pos', 'mesh_idx', 'meshes', 'inst_mesh', 'inst_w2o']
+TEXTURE_KEYS = ['tex_texels', 'textures']
 
 
 class OracleScene:
@@ -131,12 +133,17 @@ class OracleScene:
         if scene is not None:
             env = scene.export('env')
             info = scene.info()
+            textures = scene.export('textures')
             keys = SCENE_KEYS + (ENV_KEYS if env.size else []) + (INSTANCE_KEYS if info.get('two_level') else [])
-            arrays = {k: scene.export(k) for k in keys}
+            keys += TEXTURE_KEYS + ['rgb2spec'] if textures.size else []
+            arrays = {k: scene.export(k) for k in dict.fromkeys(keys)}
         has_env = 'env' in arrays and arrays['env'].size > 0
         two_level = bool(info.get('two_level')) and 'mesh_pos' in arrays
+        has_tex = 'textures' in arrays and arrays['textures'].size > 0
         self.arr = {}
-        for k in SCENE_KEYS + (ENV_KEYS if has_env else []) + (INSTANCE_KEYS if two_level else []):
+        keys = SCENE_KEYS + (ENV_KEYS if has_env else []) + (INSTANCE_KEYS if two_level else [])
+        keys += TEXTURE_KEYS + ['rgb2spec'] if has_tex else []
+        for k in dict.fromkeys(keys):
             a = np.ascontiguousarray(arrays[k])
             if a.size == 0:
                 a = np.zeros(16, np.uint8)
@@ -149,9 +156,12 @@ class OracleScene:
                                    _p(a['materials']), info['material_count'], _p(a['lights']), info['light_count'],
                                    _p(a['prim_alias']), _p(a['prim_pmf']), _p(a['light_alias']), _p(a['light_pmf']),
                                    _p(a['camera']), _p(a['integrator']), _p(a['spd']),
-                                   *([_p(a[k]) for k in ENV_KEYS] if has_env else [None] * 7),
+                                   *([_p(a[k]) for k in ENV_KEYS[:-1]] if has_env else [None] * 6),
+                                   _p(a['rgb2spec']) if has_env or has_tex else None,
                                    1 if two_level else 0, int(info.get('mesh_count', 0)) if two_level else 0,
-                                   *([_p(a[k]) for k in INSTANCE_KEYS] if two_level else [None] * 5))
+                                   *([_p(a[k]) for k in INSTANCE_KEYS] if two_level else [None] * 5),
+                                   *([_p(a[k]) for k in TEXTURE_KEYS] if has_tex else [None] * 2),
+                                   a['textures'].view(np.uint8).size // 16 if has_tex else 0)
         self.h = ctypes.c_void_p(lib().oracle_open(ctypes.byref(self.s)))
 
     @classmethod

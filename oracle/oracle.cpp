@@ -139,6 +139,11 @@ struct oracle_scene {
     const uint32_t *meshes;
     const uint32_t *inst_mesh;
     const float *inst_w2o;
+    // Textures of `image` shader nodes: linear RGB texels (4 floats each) and
+    // per texture its texel offset, width, height and 0.
+    const float *tex_texels;
+    const uint32_t *textures;
+    uint32_t texture_count;
 };
 }
 
@@ -805,6 +810,7 @@ struct Frame {
 struct It {
     V3 pos, ng, wo;
     Frame sh;
+    float tu, tv;  // interpolated texture coordinates
     float area;
     uint32_t prim, mat, light;
 };
@@ -821,6 +827,8 @@ static It interaction(const Scene &sc, uint32_t prim, float u, float v, V3 ray_d
     const float *uv = sc.s->uv;
     float u0 = uv[2 * ix[0]], v0 = uv[2 * ix[0] + 1], u1 = uv[2 * ix[1]], v1 = uv[2 * ix[1] + 1], u2 = uv[2 * ix[2]],
           v2 = uv[2 * ix[2] + 1];
+    it.tu = u0 * w + u1 * u + u2 * v;
+    it.tv = v0 * w + v1 * u + v2 * v;
     float du02 = u0 - u2, dv02 = v0 - v2, du12 = u1 - u2, dv12 = v1 - v2;
     float det = du02 * dv12 - dv02 * du12;
     V3 dp_dv = std::fabs(det) < 1e-8f ? normalize(sub(p2, p0)) : mul(sub(mul(dp12, du02), mul(dp02, du12)), 1.0f / det);
@@ -877,14 +885,11 @@ static V3 mat_vec(const float (*m)[4], V3 v) {
             m[0][2] * v.x + m[1][2] * v.y + m[2][2] * v.z};
 }
 
-// RGBToSpectrumTable::decode_unbound with the table's trilinear lookup.
-static void decode_unbound(const float *table, float r, float g, float b, float c[4]) {
-    float rgb[3] = {std::max(r, 0.0f), std::max(g, 0.0f), std::max(b, 0.0f)};
-    float m = std::max(rgb[0], std::max(rgb[1], rgb[2]));
-    float sc = 2.0f * m;
+// RGBToSpectrumTable::decode_albedo (hero.cpp:92-133): sigmoid coefficients
+// of the colour clamped to [0, 1], by the table's trilinear lookup.
+static void decode_albedo(const float *table, const float rgb[3], float c[3]) {
     float q[3];
-    for (int k = 0; k < 3; ++k) q[k] = std::min(std::max(sc == 0.0f ? 0.0f : rgb[k] / sc, 0.0f), 1.0f);
-    c[3] = sc;
+    for (int k = 0; k < 3; ++k) q[k] = std::min(std::max(rgb[k], 0.0f), 1.0f);
     if (q[0] == q[1] && q[1] == q[2]) {
         c[0] = c[1] = 0.0f;
         c[2] = (q[0] - 0.5f) / std::sqrt(q[0] * (1.0f - q[0]));
@@ -907,6 +912,43 @@ static void decode_unbound(const float *table, float r, float g, float b, float 
         };
         c[i] = L(dz, L(dy, L(dx, co(0, 0, 0), co(1, 0, 0)), L(dx, co(0, 1, 0), co(1, 1, 0))),
                  L(dy, L(dx, co(0, 0, 1), co(1, 0, 1)), L(dx, co(0, 1, 1), co(1, 1, 1))));
+    }
+}
+
+// RGBToSpectrumTable::decode_unbound (hero.cpp:135-141): the coefficients of
+// rgb / (2 max) and the scale 2 max in c[3].
+static void decode_unbound(const float *table, float r, float g, float b, float c[4]) {
+    float rgb[3] = {std::max(r, 0.0f), std::max(g, 0.0f), std::max(b, 0.0f)};
+    float m = std::max(rgb[0], std::max(rgb[1], rgb[2]));
+    float sc = 2.0f * m;
+    float q[3];
+    for (int k = 0; k < 3; ++k) q[k] = sc == 0.0f ? 0.0f : rgb[k] / sc;
+    c[3] = sc;
+    decode_albedo(table, q, c);
+}
+
+// The `image` shader node's lookup (shadernodes/image.cpp:80-88): bilinear
+// between the four nearest texel centres ((i + 0.5) / size), both axes
+// repeating, row 0 of the file at v = 0.
+static void texture_rgb(const Scene &sc, uint32_t id, float u, float v, float rgb[3]) {
+    const uint32_t *r = sc.s->textures + 4 * id;
+    const int W = static_cast<int>(r[1]), H = static_cast<int>(r[2]);
+    const float *t = sc.s->tex_texels + 4 * static_cast<size_t>(r[0]);
+    float x = (u - std::floor(u)) * W - 0.5f, y = (v - std::floor(v)) * H - 0.5f;
+    float fx = std::floor(x), fy = std::floor(y);
+    float tx = x - fx, ty = y - fy;
+    int x0 = static_cast<int>(fx), y0 = static_cast<int>(fy);
+    int x1 = x0 + 1, y1 = y0 + 1;
+    auto wrap = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
+    x0 = wrap(x0, W);
+    x1 = wrap(x1, W);
+    y0 = wrap(y0, H);
+    y1 = wrap(y1, H);
+    for (int c = 0; c < 3; ++c) {
+        float a = t[(y0 * W + x0) * 4 + c], b = t[(y0 * W + x1) * 4 + c];
+        float cc = t[(y1 * W + x0) * 4 + c], d = t[(y1 * W + x1) * 4 + c];
+        float top = a + tx * (b - a), bot = cc + tx * (d - cc);
+        rgb[c] = top + ty * (bot - top);
     }
 }
 
@@ -1563,9 +1605,34 @@ static float spd_of(const float *spd, uint32_t off, float lambda) {
     return spd_eval(spd + off + 1, static_cast<int>(spd[off]), lambda);
 }
 
+// A material's colour slot (ShaderNodeSlot::eval_albedo_spectrum,
+// shader_node.cpp:299-303): the record's constant, or (flag 32) the texture
+// lookup at the hit's uv times the constant factor held in coef as RGB,
+// decoded as an albedo (the RGB spectrum keeps the colour itself).
+static void colour(const Scene &sc, const Material &m, const It &it, const Swl &w, float *out) {
+    if (!(m.flags & 32u)) {
+        for (int i = 0; i < w.n; ++i) out[i] = alb(m.coef, w, i);
+        return;
+    }
+    uint32_t id;
+    std::memcpy(&id, &m.p[7], 4);
+    float rgb[3];
+    texture_rgb(sc, id, it.tu, it.tv, rgb);
+    for (int c = 0; c < 3; ++c) rgb[c] *= m.coef[c];
+    if (is_rgb(w)) {
+        for (int i = 0; i < w.n; ++i) out[i] = rgb[i < 3 ? i : 2];
+        return;
+    }
+    float c[3];
+    decode_albedo(sc.s->rgb2spec, rgb, c);
+    for (int i = 0; i < w.n; ++i) out[i] = sigmoid_poly(c, w.lambda[i]);
+}
+
 // Material::create_evaluator for the supported plugins.
 static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Swl &w) {
     Bsdf b;
+    float col[8];
+    colour(sc, m, it, w, col);
     b.n = w.n;
     b.fr = it.sh;
     b.ng = it.ng;
@@ -1574,7 +1641,22 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
     b.count = 1;
     if (m.type == 0) {
         l0.kind = Lobe::Lambert;
-        for (int i = 0; i < w.n; ++i) l0.kr[i] = alb(m.coef, w, i);
+        for (int i = 0; i < w.n; ++i) l0.kr[i] = col[i];
+    } else if (m.type == 2 && (m.flags & 64u)) {
+        // metallic: MetallicLobe (metallic.cpp:42-60), kr = colour, F82 tint
+        // with F0 = colour and the edge tint (fresnel.h:114-120).
+        l0.kind = Lobe::MicrofacetRefl;
+        l0.fresnel = Lobe::F82;
+        l0.compensate = true;
+        l0.ax = m.p[0];
+        l0.ay = m.p[1];
+        const float f = 6.0f / 7.0f, f5 = f * f * f * f * f;
+        for (int i = 0; i < w.n; ++i) {
+            l0.kr[i] = col[i];
+            l0.fa[i] = col[i];
+            float fs = col[i] + f5 * (1.0f - col[i]);
+            l0.fb[i] = fs * (7.0f / (f5 * f)) * (1.0f - alb(m.p + 2, w, i));
+        }
     } else if (m.type == 2) {  // metal: ConductorLobe; mirror: MirrorLobe (FresnelConstant, kr = colour)
         l0.kind = Lobe::MicrofacetRefl;
         const bool mirror = (m.flags & 4u) != 0;
@@ -1584,7 +1666,7 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         l0.ay = m.p[1];
         for (int i = 0; i < w.n; ++i) {
             if (mirror) {
-                l0.kr[i] = alb(m.coef, w, i);
+                l0.kr[i] = col[i];
             } else {
                 l0.kr[i] = 1.0f;
                 l0.fa[i] = spd_of(sc.s->spd, m.spd0, std::fabs(w.lambda[i]));
@@ -1599,7 +1681,7 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         l0.eta0 = m.p[5];
         float f0 = ((m.p[5] - 1.0f) / (m.p[5] + 1.0f)) * ((m.p[5] - 1.0f) / (m.p[5] + 1.0f));
         for (int i = 0; i < w.n; ++i) {
-            l0.kr[i] = alb(m.coef, w, i);
+            l0.kr[i] = col[i];
             l0.fa[i] = f0 * alb(m.p + 2, w, i);
         }
     } else if (m.type == 5) {  // substrate: SubstrateLobe over FresnelBlend
@@ -1607,7 +1689,7 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         l0.ax = m.p[0];
         l0.ay = m.p[1];
         for (int i = 0; i < w.n; ++i) {
-            l0.kr[i] = alb(m.coef, w, i);
+            l0.kr[i] = col[i];
             l0.fa[i] = alb(m.p + 2, w, i);
         }
     } else if (m.type == 3) {  // glass: DielectricLobe
@@ -1616,7 +1698,7 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         l0.ay = m.p[1];
         bool front = dot(it.wo, it.ng) > 0.0f;  // Interaction::correct_eta
         for (int i = 0; i < w.n; ++i) {
-            l0.kr[i] = alb(m.coef, w, i);
+            l0.kr[i] = col[i];
             float ior = m.spd0 != kInvalid ? spd_of(sc.s->spd, m.spd0, is_rgb(w) ? -w.lambda[0] : w.lambda[i]) : m.p[2];
             l0.eta[i] = front ? ior : 1.0f / ior;
         }
@@ -1630,7 +1712,7 @@ static Bsdf make_bsdf(const Scene &sc, const Material &m, const It &it, const Sw
         float color[8], tint[8], weight[8];
         const float tc[3] = {m.p[4], m.p[5], m.p[6]};
         for (int i = 0; i < n; ++i) {
-            color[i] = alb(m.coef, w, i);
+            color[i] = col[i];
             tint[i] = alb(tc, w, i);
             weight[i] = 1.0f;
         }

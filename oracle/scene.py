@@ -64,7 +64,7 @@ assert INTEGRATOR.itemsize == 48 and ENV.itemsize == 160
 
 # Material types and flags of the flat format.
 DIFFUSE, BLACK_BODY, METAL, GLASS, PRINCIPLED, SUBSTRATE, MIX = range(7)
-FLAG_DISPERSIVE, FLAG_REMAP, FLAG_CONST_FRESNEL, FLAG_PLASTIC, FLAG_ADD = 1, 2, 4, 8, 16
+FLAG_DISPERSIVE, FLAG_REMAP, FLAG_CONST_FRESNEL, FLAG_PLASTIC, FLAG_ADD, FLAG_TEXTURE, FLAG_F82 = 1, 2, 4, 8, 16, 32, 64
 EMIT_RGB, EMIT_BLACKBODY = 0, 1
 LIGHT_AREA, LIGHT_POINT, LIGHT_SPOT = 0, 1, 2
 FILTERS = {'box': 0, 'triangle': 1, 'gaussian': 2, 'mitchell': 3, 'sinc': 4}
@@ -526,6 +526,20 @@ SHAPES = {'quad': quad, 'cube': cube, 'sphere': sphere, 'mesh': inline_mesh, 'ic
 
 
 # ----- spectra of slots ---------------------------------------------------------------------
+def _node_type(n):
+    """ShaderNodeDesc::init (node_desc.cpp:292-320): {"type", "param"}, or
+    the parameters inline, where an object naming a file is an image node."""
+    if not isinstance(n, dict):
+        return None
+    if 'param' in n:
+        return n.get('type', 'number')
+    return n.get('type', 'image' if 'fn' in n else 'number')
+
+
+def _node_param(n):
+    return n.get('param', {}) or {} if 'param' in n else n
+
+
 def _slot(j):
     """SlotDesc::init (node_desc.cpp:127-150): a number, a list, a
     {"channels", "node"} pair or a number/constant node, as a float list."""
@@ -536,7 +550,7 @@ def _slot(j):
     if isinstance(j, dict):
         if 'channels' in j:
             return _slot(j['node'])
-        t = j.get('type', 'number')
+        t = _node_type(j)
         if t in ('number', 'constant'):
             return _slot(j.get('param', j).get('value'))
         raise Unsupported('shader node ' + t)
@@ -559,6 +573,54 @@ def _slot_scalar(j, default):
 
 def _node(j):
     return j['node'] if isinstance(j, dict) and 'channels' in j else j
+
+
+def srgb_to_linear(c):
+    """The sRGB transfer function removed (IEC 61966-2-1), in float32."""
+    c = np.asarray(c, np.float32)
+    hi = np.power(((c + F(0.055)) / F(1.055)).astype(np.float32), F(2.4)).astype(np.float32)
+    return np.where(c <= F(0.04045), (c / F(12.92)).astype(np.float32), hi).astype(np.float32)
+
+
+def load_texels(node, base_dir):
+    """The file of an `image` node (ImagePool::load_texture,
+    image_pool.cpp:13-35) as (H, W, 4) float32 linear RGB texels and 0: the
+    path relative to the scene's folder, the colour space "srgb" by default
+    ("linear" for Radiance HDR) with its transfer function removed, grey
+    replicated to RGB, alpha dropped.  Decoded by OpenCV: PNG and Radiance
+    HDR exactly as the library does; baseline JPEG to within a few levels of
+    8 bits (libjpeg's integer IDCT against the library's float IDCT)."""
+    import cv2
+    p = _node_param(node)
+    fn = p.get('fn', '')
+    if not fn:
+        raise ValueError('image node without fn')
+    path = fn if os.path.isabs(fn) or not base_dir else os.path.join(base_dir, fn)
+    ext = fn.rsplit('.', 1)[-1].lower() if '.' in fn else ''
+    if ext not in ('png', 'jpg', 'jpeg', 'hdr'):
+        raise Unsupported('image file format ' + ext)
+    cs = p.get('color_space') or ('linear' if ext == 'hdr' else 'srgb')
+    if cs not in ('srgb', 'linear'):
+        raise Unsupported('image colour space ' + cs)
+    im = cv2.imread(path, cv2.IMREAD_UNCHANGED)
+    if im is None:
+        raise ValueError('cannot decode ' + path)
+    if im.dtype == np.uint8:
+        f = im.astype(np.float32) / F(255.0)
+    elif im.dtype == np.uint16:
+        f = im.astype(np.float32) / F(65535.0)
+    else:
+        f = im.astype(np.float32)
+    if f.ndim == 2:
+        rgb = np.repeat(f[..., None], 3, axis=2)
+    elif f.shape[2] == 2:
+        rgb = np.repeat(f[..., :1], 3, axis=2)
+    else:
+        rgb = f[..., 2::-1] if f.shape[2] >= 3 else f
+    rgb = srgb_to_linear(rgb) if cs == 'srgb' else rgb
+    tex = np.zeros(rgb.shape[:2] + (4,), np.float32)
+    tex[..., :3] = rgb
+    return tex
 
 
 def _to_list(f):
@@ -629,6 +691,48 @@ class _Builder:
         self.spd = []
         self.spd_len = 0
         self.needs_luts = False
+        self.tex_texels, self.textures, self.tex_by_key, self.tex_avg = [], [], {}, []
+        self.tex_len = 0
+
+    def texture(self, node):
+        """The id of an image node's texture, each file and colour space loaded once."""
+        p = _node_param(node)
+        key = (p.get('fn', ''), p.get('color_space', ''))
+        if key not in self.tex_by_key:
+            tex = load_texels(node, self.base_dir)
+            H, W = tex.shape[:2]
+            self.tex_by_key[key] = len(self.textures)
+            self.textures.append((self.tex_len, W, H, 0))
+            self.tex_texels.append(tex.reshape(-1))
+            self.tex_len += W * H
+            self.tex_avg.append(tex.reshape(-1, 4)[:, :3].astype(np.float64).mean(0).astype(np.float32))
+        return self.tex_by_key[key]
+
+    def colour_slot(self, j, default, r):
+        """A material colour slot: a constant (sigmoid coefficients, or the
+        colour itself for the RGB spectrum), an `image` node, or a `multiply`
+        of an image node and a constant (math.cpp).  A texture sets flag 32,
+        the id's bits in p[7] and the constant factor as RGB in coef."""
+        n = _node(j)
+        img, factor = None, [F(1.0)] * 3
+        if _node_type(n) == 'image':
+            img = n
+        elif _node_type(n) == 'multiply':
+            q = n.get('param', {}) or {}
+            lhs, rhs = _node(q.get('lhs')), _node(q.get('rhs'))
+            li = _node_type(lhs) == 'image'
+            ri = _node_type(rhs) == 'image'
+            if li == ri:
+                raise Unsupported('multiply node other than an image times a constant')
+            img = lhs if li else rhs
+            factor = _slot_rgb(q.get('rhs') if li else q.get('lhs'), 1.0)
+        if img is None:
+            r['coef'] = self.colour(_slot_rgb(j, default))
+            return
+        tid = self.texture(img)
+        r['flags'] |= FLAG_TEXTURE
+        r['p'][7] = np.array([tid], np.uint32).view(np.float32)[0]
+        r['coef'] = [factor[0], factor[1], factor[2], 0.0]
 
     def colour(self, rgb):
         if self.srgb:
@@ -677,7 +781,7 @@ class _Builder:
                 r['spd0' if k == 0 else 'spd1'] = len(self.materials) - 1
         elif t == 'diffuse':
             r['type'] = DIFFUSE
-            r['coef'] = self.colour(_slot_rgb(p.get('color'), 0.5))
+            self.colour_slot(p.get('color'), 0.5, r)
         elif t == 'black_body':
             r['type'] = BLACK_BODY
         elif t in ('metal', 'mirror'):
@@ -692,15 +796,26 @@ class _Builder:
                 rough = clamp(_slot_scalar(p.get('roughness'), 0.01), 0.0001, 1.0)
             else:
                 r['flags'] |= FLAG_CONST_FRESNEL
-                r['coef'] = self.colour(_slot_rgb(p.get('color'), 1.0))
+                self.colour_slot(p.get('color'), 1.0, r)
                 rough = clamp(_slot_scalar(p.get('roughness'), 0.001), 0.0001, 1.0)
             aniso = clamp(_slot_scalar(p.get('anisotropic'), 0.0), -0.9, 0.9)
             a = F(rough * rough) if p.get('remapping_roughness', True) else rough
             r['p'][0], r['p'][1] = alphas(a, aniso)
             self.needs_luts = True
+        elif t == 'metallic':
+            # MetallicMaterial (metallic.cpp:26-60): colour, edge tint (an
+            # albedo in p[2..4]), roughness in [0.01, 1] always remapped.
+            r['type'] = METAL
+            r['flags'] |= FLAG_F82
+            self.colour_slot(p.get('color'), 1.0, r)
+            r['p'][2:5] = self.colour(_slot_rgb(p.get('edge_tint'), 1.0))[:3]
+            rough = clamp(_slot_scalar(p.get('roughness'), 0.5), 0.01, 1.0)
+            aniso = clamp(_slot_scalar(p.get('anisotropic'), 0.0), -0.9, 0.9)
+            r['p'][0], r['p'][1] = alphas(F(rough * rough), aniso)
+            self.needs_luts = True
         elif t == 'glass':
             r['type'] = GLASS
-            r['coef'] = self.colour(_slot_rgb(p.get('color'), 1.0))
+            self.colour_slot(p.get('color'), 1.0, r)
             ior = p.get('ior')
             node = _node(ior)
             curve = None
@@ -723,7 +838,7 @@ class _Builder:
             self.needs_luts = True
         elif t == 'principled_bsdf':
             r['type'] = PRINCIPLED
-            r['coef'] = self.colour(_slot_rgb(p.get('color'), 1.0))
+            self.colour_slot(p.get('color'), 1.0, r)
             rough = clamp(_slot_scalar(p.get('roughness'), 0.5), 0.0001, 1.0)
             aniso = _slot_scalar(p.get('anisotropic'), 0.0)
             aspect = F(math.sqrt(F(F(1.0) - F(aniso * F(0.9)))))
@@ -750,7 +865,7 @@ class _Builder:
             if t == 'plastic':
                 r['flags'] |= FLAG_PLASTIC
                 r['p'][5] = clamp(_slot_scalar(p.get('ior'), 1.3), 1.003, 5.0)
-            r['coef'] = self.colour(_slot_rgb(p.get('color'), 1.0))
+            self.colour_slot(p.get('color'), 1.0, r)
             r['p'][2:5] = self.colour(_slot_rgb(p.get('spec'), 0.05))[:3]
             rough = clamp(_slot_scalar(p.get('roughness'), 0.5), 0.0001, 1.0)
             aniso = clamp(_slot_scalar(p.get('anisotropic'), 0.0), -0.9, 0.9)
@@ -904,9 +1019,14 @@ class _Builder:
         AliasTable2D (alias2d.cpp:30-66) from luminance * sin(theta) weights
         (calculate_weights, spherical.cpp:150-185)."""
         node = _node(p.get('color'))
-        if not (isinstance(node, dict) and node.get('type') == 'sky'):
-            raise Unsupported('spherical light colour other than the procedural sky')
-        tex, W, H = self.sky(node.get('param', {}))
+        kind = _node_type(node)
+        if kind not in ('sky', 'image'):
+            raise Unsupported('spherical light colour other than an image or the procedural sky')
+        if kind == 'sky':
+            tex, W, H = self.sky(node.get('param', {}))
+        else:
+            tex = load_texels(node, self.base_dir)
+            H, W = tex.shape[:2]
         env = np.zeros(1, ENV)[0]
         env['width'], env['height'] = W, H
         env['scale'] = F(p['scale']) if isinstance(p.get('scale'), (int, float)) else F(1.0)
@@ -1061,6 +1181,10 @@ class _Builder:
         if self.env is not None:
             arr.update(self.env)
             arr['env'] = np.array([self.env['env']], ENV)
+            arr['rgb2spec'] = np.ascontiguousarray(rgb2spec_table()).reshape(-1)
+        if self.textures:
+            arr['tex_texels'] = np.concatenate(self.tex_texels).astype(np.float32)
+            arr['textures'] = np.array(self.textures, np.uint32).ravel()
             arr['rgb2spec'] = np.ascontiguousarray(rgb2spec_table()).reshape(-1)
         info = dict(vertex_count=self.nverts, prim_count=self.nprims, instance_count=len(self.instances),
                     material_count=len(self.materials), light_count=len(self.lights),

@@ -67,3 +67,23 @@ def mean_z(sum_a, sq_a, n_a, sum_b, sq_b, n_b):
     k = ma.size
     se = np.sqrt((va / n_a + vb / n_b).sum()) / k
     return (ma.mean() - mb.mean()) / max(se, 1e-30)
+
+
+def write_room_textures(folder, seed=7):
+    """The image files of scenes.textured_room, written with OpenCV from a
+    seeded generator: an RGB checker PNG with noise, a grey gradient PNG and
+    a smooth RGB JPEG (4:2:0)."""
+    import os
+    import cv2
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:48, 0:64]
+    check = ((xx // 8 + yy // 8) % 2).astype(bool)
+    rgb = np.where(check[..., None], np.array([200, 60, 40]), np.array([30, 120, 220]))
+    rgb = np.clip(rgb + rng.integers(-20, 21, rgb.shape), 0, 255).astype(np.uint8)
+    cv2.imwrite(os.path.join(folder, 'checker.png'), rgb[..., ::-1])
+    g = (np.add.outer(np.arange(32) * 5, np.arange(32) * 3) % 256).astype(np.uint8)
+    cv2.imwrite(os.path.join(folder, 'gradient.png'), g)
+    y, x = np.mgrid[0:24, 0:40] / 8.0
+    photo = np.stack([128 + 100 * np.sin(x + 0.3 * y), 128 + 90 * np.cos(0.7 * x - y), 128 + 80 * np.sin(x * y / 3)], -1)
+    cv2.imwrite(os.path.join(folder, 'photo.jpg'), np.clip(photo, 0, 255).astype(np.uint8)[..., ::-1],
+                [cv2.IMWRITE_JPEG_QUALITY, 90])

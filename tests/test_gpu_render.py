@@ -169,6 +169,68 @@ def test_matched_seed_parity_mix_and_add(vb, gpu_ctx):
         t.render(0, 1)
 
 
+def test_matched_seed_parity_metallic(vb, gpu_ctx):
+    # MetallicMaterial: compensated GGX reflection, kr = colour, F82-tint
+    # Fresnel (metallic.cpp:42-60), isotropic, anisotropic and near-specular.
+    from helpers import mean_z, path_sums, pixel_z
+    s = vb.Scene(gpu_ctx, scenes.metallic_room(64, 64, max_depth=2)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 1e-3) >= 0.99
+    s = vb.Scene(gpu_ctx, scenes.metallic_room(48, 48)).build_accel()
+    o = oracle.OracleScene.from_json(scenes.metallic_room(48, 48))
+    s.render(0, 32, fp64=True)
+    gs, gq = s.film(vb.FILM_SUM64)[..., :3], s.film(vb.FILM_SUMSQ64)[..., :3]
+    cs, cq = path_sums(o.paths(np.arange(48 * 48, dtype=np.uint32), 0, 32))
+    cs, cq = cs.reshape(48, 48, 3), cq.reshape(48, 48, 3)
+    z = pixel_z(gs, gq, 32, cs, cq, 32)
+    assert (np.abs(z) > 4.0).mean() <= 0.005
+    assert abs(mean_z(gs, gq, 32, cs, cq, 32)) < 4.0
+
+
+@pytest.mark.parametrize('spectrum', ['hero', 'srgb'])
+def test_matched_seed_parity_textures(vb, gpu_ctx, tmp_path, spectrum):
+    # `image` nodes in the colour slots of a diffuse, a multiply(image,
+    # constant) diffuse, a principled BSDF (JPEG) and a plastic (linear grey):
+    # bilinear repeat lookups at the hit's uv, decoded as albedo spectra (the
+    # colour itself for the RGB spectrum).  The oracle reads the library's
+    # texels (matched seeds, one bounce), then decodes the PNG files itself
+    # (full depth, per-pixel z-test).
+    from helpers import mean_z, path_sums, pixel_z, write_room_textures
+    write_room_textures(str(tmp_path))
+
+    def doc(w, h, **kw):
+        d = scenes.textured_room(w, h, **kw)
+        if spectrum == 'srgb':
+            d['spectrum'] = {'type': 'srgb'}
+        return d
+    s = vb.Scene(gpu_ctx, doc(64, 64, max_depth=2), base_dir=str(tmp_path)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert np.all(np.isfinite(g))
+    assert _match(g, c, 1e-3) >= 0.99
+    s = vb.Scene(gpu_ctx, doc(48, 48, jpeg=False), base_dir=str(tmp_path)).build_accel()
+    o = oracle.OracleScene.from_json(doc(48, 48, jpeg=False), str(tmp_path))
+    s.render(0, 32, fp64=True)
+    gs, gq = s.film(vb.FILM_SUM64)[..., :3], s.film(vb.FILM_SUMSQ64)[..., :3]
+    cs, cq = path_sums(o.paths(np.arange(48 * 48, dtype=np.uint32), 0, 32))
+    cs, cq = cs.reshape(48, 48, 3), cq.reshape(48, 48, 3)
+    z = pixel_z(gs, gq, 32, cs, cq, 32)
+    assert (np.abs(z) > 4.0).mean() <= 0.005
+    assert abs(mean_z(gs, gq, 32, cs, cq, 32)) < 4.0
+    # Every schedule samples the textures alike.
+    films = []
+    for schedule in ('wavefront', 'grid', 'persistent'):
+        t = vb.Scene(gpu_ctx, doc(32, 32), base_dir=str(tmp_path)).build_accel()
+        t.set_schedule(schedule)
+        t.render(0, 4)
+        films.append(t.film())
+    assert all(_match(f, films[0], 1e-3) >= 0.99 for f in films[1:])
+
+
 def test_matched_seed_parity_plastic(vb, gpu_ctx):
     # PlasticLobe: Lambert (1 - F) plus Schlick-weighted GGX reflection.
     s = vb.Scene(gpu_ctx, scenes.plastic_room(64, 64, max_depth=2)).build_accel()
@@ -277,7 +339,7 @@ def test_large_scene_closest_hit_bit_exact(vb, gpu_ctx):
 
 
 @pytest.mark.parametrize('case', ['box_room', 'materials', 'substrate', 'plastic', 'point_lights', 'srgb',
-                                  'environment', 'dimension1', 'two_waves', 'principled'])
+                                  'environment', 'dimension1', 'two_waves', 'principled', 'metallic'])
 def test_schedules_give_the_same_film(vb, gpu_ctx, case):
     # Path regeneration only changes which thread traces which path, and the
     # wavefront form only where a path's state lives between bounces: each
@@ -300,6 +362,8 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
         sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
     elif case == 'principled':
         sc = scenes.principled_room(37, 35)
+    elif case == 'metallic':
+        sc = scenes.metallic_room(36, 34)
     elif case == 'dimension1':
         sc = scenes.box_room(width=33, height=31, dimension=1)
     else:

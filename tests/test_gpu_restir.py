@@ -19,8 +19,8 @@ def _close(a, b, rtol=2e-3, atol=1e-4):
     return (np.abs(a - b) <= atol + rtol * np.abs(b))
 
 
-def _run(vb, ctx, sc, cams, w, h):
-    s = vb.Scene(ctx, sc).build_accel()
+def _run(vb, ctx, sc, cams, w, h, base_dir='.'):
+    s = vb.Scene(ctx, sc, base_dir=base_dir).build_accel()
     o = oracle.OracleScene(s)
     ort = oracle.OracleRestir(o, w, h)
     for f, c2w in enumerate(cams):
@@ -33,8 +33,8 @@ def _run(vb, ctx, sc, cams, w, h):
 
 
 @pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates', 'substrate_mirror', 'srgb',
-                                       'plastic', 'point_spot', 'environment'])
-def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
+                                       'plastic', 'point_spot', 'environment', 'textured'])
+def test_restir_frames_match_oracle(vb, gpu_ctx, tmp_path, materials):
     # 'diffuse': diffuse walls and emitters (the kernels compiled for those
     # materials alone); 'metal': a gold box as well (the general kernels);
     # 'two_bsdf_candidates': M_bsdf = 2, which takes the one-kernel direct
@@ -42,7 +42,8 @@ def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
     # among the candidates (delta lights: MIS weight 1 / M_light);
     # 'environment': an open back wall and a sky map, so light candidates,
     # BSDF candidates that escape and camera rays that miss all reach the
-    # environment.
+    # environment; 'textured': `image` nodes in the floor's and a plastic
+    # box's colour slots.
     w, h = 96, 64
     sc = scenes.many_lights(w, h, emitters=300, seed=5, M_light=8, history_limit=20, spatial_neighbours=5,
                             spatial_radius=12.0, max_depth=4, M_bsdf=2 if materials == 'two_bsdf_candidates' else 1)
@@ -78,8 +79,19 @@ def test_restir_frames_match_oracle(vb, gpu_ctx, materials):
             if m['name'] == 'Floor':
                 m.update({'type': 'substrate', 'param': {'color': [0.6, 0.5, 0.4], 'roughness': 0.2,
                                                          'remapping_roughness': False}})
+    base_dir = '.'
+    if materials == 'textured':
+        from helpers import write_room_textures
+        write_room_textures(str(tmp_path))
+        base_dir = str(tmp_path)
+        for m in sc['materials']:
+            if m['name'] == 'Floor':
+                m.update({'type': 'diffuse', 'param': {'color': {'type': 'image', 'param': {'fn': 'checker.png'}}}})
+            if m['name'] == 'TallBox':
+                m.update({'type': 'plastic', 'param': {'color': {'type': 'image', 'param': {'fn': 'gradient.png'}},
+                                                       'roughness': 0.3}})
     cams = scenes.camera_spline(6, seed=3)
-    for f, s, ort in _run(vb, gpu_ctx, sc, cams, w, h):
+    for f, s, ort in _run(vb, gpu_ctx, sc, cams, w, h, base_dir):
         gs, cs = s.restir_buffer('surfaces'), ort.buffer('surfaces', vb.RT_SURFACE_DTYPE)
         hit_eq = (gs['hit']['inst_id'] == cs['hit']['inst_id']) & (gs['hit']['prim_id'] == cs['hit']['prim_id'])
         assert hit_eq.mean() >= 0.999, (f, hit_eq.mean())

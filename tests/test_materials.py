@@ -137,6 +137,32 @@ def test_mirror_and_substrate_records(vb, host_ctx):
     np.testing.assert_array_equal(f2[10:13], f[10:13])
 
 
+def test_metallic_records(vb, host_ctx):
+    # MetallicMaterial (metallic.cpp:26-60): a metal record with the F82
+    # flag, colour coefficients, the edge tint's coefficients in p[2..4],
+    # roughness clamped to [0.01, 1] and squared, anisotropy as for metal.
+    s = vb.Scene(host_ctx, scenes.metallic_room(8, 8))
+    mats = s.export('materials', np.uint32).reshape(-1, 16)
+    matf = mats.view(np.float32)
+    names = ['Floor', 'Ceiling', 'BackWall', 'LeftWall', 'RightWall', 'TallBox', 'ShortBox', 'Light']
+    rec = {n: (mats[i], matf[i]) for i, n in enumerate(names)}
+    u, f = rec['TallBox']
+    assert u[0] == 2 and (u[1] & 64) and not (u[1] & 4) and u[2] == 0xffffffff
+    np.testing.assert_allclose(f[8:10], [0.35 ** 2] * 2, rtol=1e-6)
+    assert np.any(f[10:13] != 0.0)
+    u, f = rec['ShortBox']
+    a = np.float32(0.3) ** 2
+    np.testing.assert_allclose(f[8:10], [a * 0.5, a / 0.5], rtol=1e-6)
+    # The edge tint defaults to white; roughness below 0.01 clamps.
+    sc = scenes.metallic_room(8, 8)
+    for m in sc['materials']:
+        if m['name'] == 'BackWall':
+            m['param'] = {'color': [0.9, 0.9, 0.9], 'edge_tint': [1.0, 1.0, 1.0], 'roughness': 0.001}
+    f2 = vb.Scene(host_ctx, sc).export('materials', np.float32).reshape(-1, 16)[2]
+    np.testing.assert_array_equal(f2[10:13], rec['BackWall'][1][10:13])
+    np.testing.assert_allclose(f2[8:10], [1e-4, 1e-4], rtol=1e-6)
+
+
 def test_gpu_albedo_tables_need_a_device_and_a_valid_strata(vb, host_ctx):
     with pytest.raises(vb.VisionError) as e:
         vb.albedo_luts_gpu(host_ctx, 32)

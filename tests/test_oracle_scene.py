@@ -57,7 +57,7 @@ def _compare(vb, ctx, sc):
 
 @pytest.mark.parametrize('name', ['box_room', 'box_room_rgb_light', 'material_room', 'substrate_room',
                                   'plastic_room', 'point_lights', 'srgb', 'many_lights', 'large_scene_small',
-                                  'sphere_trs', 'principled_room', 'mix_room'])
+                                  'sphere_trs', 'principled_room', 'mix_room', 'metallic_room'])
 def test_oracle_scene_equals_library_export(vb, host_ctx, name):
     if name == 'box_room':
         sc = scenes.box_room(64, 48, sampler='pcg')
@@ -73,6 +73,8 @@ def test_oracle_scene_equals_library_export(vb, host_ctx, name):
         sc = scenes.principled_room(32, 32)
     elif name == 'mix_room':
         sc = scenes.mix_room(32, 32)
+    elif name == 'metallic_room':
+        sc = scenes.metallic_room(32, 32)
     elif name == 'point_lights':
         sc = scenes.point_light_room(32, 32, light_sampler='power')
     elif name == 'srgb':

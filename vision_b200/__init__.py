@@ -41,7 +41,8 @@ EXPORT = dict(mesh_pos=27, mesh_idx=28, meshes=29, inst_mesh=30, inst_w2o=31,
               pos=0, nrm=1, uv=2, idx=3, prim_inst=4, instances=5, materials=6, lights=7, prim_alias=8,
               prim_pmf=9, light_alias=10, light_pmf=11, camera=12, integrator=13, spd=14, material_rgb=15,
               light_rgb=16, bvh_nodes=17, bvh_tris=18, luts=19, env=20, env_tex=21,
-              env_marginal=22, env_marginal_func=23, env_cond=24, env_cond_func=25, rgb2spec=26)
+              env_marginal=22, env_marginal_func=23, env_cond=24, env_cond_func=25, rgb2spec=26,
+              tex_texels=32, textures=33)
 
 
 class VisionError(RuntimeError):

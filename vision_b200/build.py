@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libvision_b200.so')
 INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 
-SOURCES = ['kernels.cu', 'wavefront.cu', 'restir.cu', 'restir_diffuse.cu', 'svgf.cu', 'server.cu', 'mlp.cu', 'cache_render.cu', 'capi.cu', 'noalloc.cu', 'scene_load.cpp', 'bvh8.cpp', 'rgb2spec.cpp', 'luts.cpp', 'lut_gen.cu']
+SOURCES = ['kernels.cu', 'wavefront.cu', 'restir.cu', 'restir_diffuse.cu', 'svgf.cu', 'server.cu', 'mlp.cu', 'cache_render.cu', 'capi.cu', 'noalloc.cu', 'scene_load.cpp', 'image_io.cpp', 'bvh8.cpp', 'rgb2spec.cpp', 'luts.cpp', 'lut_gen.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 COMMON = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC,-ffp-contract=off,-pthread',
           '-I', CSRC, '-I', INCLUDE]

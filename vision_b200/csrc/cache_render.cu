@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(128) k_cache_paths(const __grid_constant__ Dev
         Ray sh = spawn_ray_to(it.pos, it.ng, ls.p_light);
         bool occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
         Material mat = s.materials[it.mat];
-        Bsdf<CN> bsdf = make_bsdf<CN>(s, mat, it.shading, it.ng, it.wo, wl);
+        Bsdf<CN> bsdf = make_bsdf<CN>(s, mat, it.shading, it.ng, it.wo, it.uv, wl);
         if (bsdf.dispersive) invalidate_secondary<CN>(wl);
         f3 wi_light = normalize(ls.p_light - it.pos);
         BsdfEval<CN> se = bsdf.evaluate(it.wo, wi_light, nullptr);

@@ -73,6 +73,8 @@ struct vs_scene {
     DevBuf<AliasEntry> prim_alias, light_alias;
     DevBuf<float> prim_pmf, light_pmf, spd, luts;
     DevBuf<float> env_tex, env_marginal_func, env_cond_func, rgb2spec;
+    DevBuf<float> tex_texels;
+    DevBuf<TextureRec> textures;
     DevBuf<AliasEntry> env_marginal, env_cond, filter_alias;
     DevBuf<float> filter_tab;
     // Two-level scenes: top-level leaf entries and per-instance transforms.
@@ -282,6 +284,7 @@ struct vs_scene {
         nodes.free(); tri_v.free(); vtx.free(); prims.free(); instances.free(); materials.free(); lights.free();
         prim_alias.free(); light_alias.free(); prim_pmf.free(); light_pmf.free(); spd.free(); luts.free();
         env_tex.free(); env_marginal_func.free(); env_cond_func.free(); rgb2spec.free(); env_marginal.free(); env_cond.free();
+        tex_texels.free(); textures.free();
         filter_tab.free(); filter_alias.free(); tlas_inst.free(); inst_xf.free();
         film32.free(); exposed.free(); film64.free(); radiance.free(); path_counter.free(); wf.free();
         rt.free();
@@ -297,6 +300,7 @@ struct vs_scene {
         return b(nodes) + b(tri_v) + b(vtx) + b(prims) + b(instances) + b(materials) + b(lights) + b(prim_alias) +
                b(light_alias) + b(prim_pmf) + b(light_pmf) + b(spd) + b(luts) + b(env_tex) + b(env_marginal_func) +
                b(env_cond_func) + b(rgb2spec) + b(env_marginal) + b(env_cond) + b(filter_tab) + b(filter_alias) +
+               b(tex_texels) + b(textures) +
                b(tlas_inst) + b(inst_xf);
     }
 
@@ -343,6 +347,8 @@ struct vs_scene {
         d.env_cond = env_cond.ptr;
         d.env_cond_func = env_cond_func.ptr;
         d.rgb2spec = reinterpret_cast<const float4 *>(rgb2spec.ptr);
+        d.tex_texels = reinterpret_cast<const float4 *>(tex_texels.ptr);
+        d.textures = reinterpret_cast<const uint4 *>(textures.ptr);
         d.filter_tab = filter_tab.ptr;
         d.filter_alias = filter_alias.ptr;
         d.filter_integral = host.filter_integral;
@@ -471,9 +477,22 @@ int upload_scene(vs_scene *s) {
         VS_CUDA(s->env_marginal_func.upload(h.env_marginal_func), "upload env");
         VS_CUDA(s->env_cond.upload(h.env_cond), "upload env");
         VS_CUDA(s->env_cond_func.upload(h.env_cond_func), "upload env");
+    }
+    // The RGB -> spectrum table: the environment's texels and textured
+    // colour slots decode through it on the device.
+    if (h.has_env || (!h.textures.empty() && !h.ip.srgb)) {
         const float *t = rgb2spec_table("");
         std::vector<float> tab(t, t + static_cast<size_t>(3) * 64 * 64 * 64 * 4);
         VS_CUDA(s->rgb2spec.upload(tab), "upload rgb2spec");
+    } else {
+        s->rgb2spec.free();
+    }
+    if (!h.textures.empty()) {
+        VS_CUDA(s->tex_texels.upload(h.tex_texels), "upload textures");
+        VS_CUDA(s->textures.upload(h.textures), "upload textures");
+    } else {
+        s->tex_texels.free();
+        s->textures.free();
     }
     if (!h.filter_tab.empty()) {
         VS_CUDA(s->filter_tab.upload(h.filter_tab), "upload filter table");
@@ -735,6 +754,8 @@ ExportView export_view(const vs_scene *s, int what) {
         case VS_EXPORT_MESH_POS: return {h.mesh_pos.data(), h.mesh_pos.size() * sizeof(f3)};
         case VS_EXPORT_MESH_IDX: return {h.mesh_idx.data(), h.mesh_idx.size() * 4};
         case VS_EXPORT_MESHES: return {h.meshes.data(), h.meshes.size() * sizeof(HostScene::MeshRec)};
+        case VS_EXPORT_TEXELS: return {h.tex_texels.data(), h.tex_texels.size() * sizeof(float)};
+        case VS_EXPORT_TEXTURES: return {h.textures.data(), h.textures.size() * sizeof(TextureRec)};
         case VS_EXPORT_INST_MESH: return {h.inst_mesh.data(), h.inst_mesh.size() * 4};
         case VS_EXPORT_INST_W2O: return {h.inst_w2o.data(), h.inst_w2o.size() * sizeof(m4)};
         case VS_EXPORT_LUTS: {

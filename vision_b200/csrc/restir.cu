@@ -182,7 +182,7 @@ __device__ __forceinline__ Interaction it_at(const DeviceScene &s, const Hit &h,
 // MaterialEvaluator creation plus SampledWavelengths::check_dispersive.
 __device__ __forceinline__ Bsdf<RN, VS_RT_MATERIALS> bsdf_at(const DeviceScene &s, const Interaction &it, RWl &wl) {
     Material m = s.materials[it.mat];
-    Bsdf<RN, VS_RT_MATERIALS> b = make_bsdf<RN, VS_RT_MATERIALS>(s, m, it.shading, it.ng, it.wo, wl);
+    Bsdf<RN, VS_RT_MATERIALS> b = make_bsdf<RN, VS_RT_MATERIALS>(s, m, it.shading, it.ng, it.wo, it.uv, wl);
     if (b.dispersive) invalidate_secondary<RN>(wl);
     return b;
 }
@@ -439,7 +439,7 @@ __device__ VS_OUTLINE PrimaryHit compute_hit(const DeviceScene &s, const RtParam
         bool near_spec = flag == kFlagNearSpec;
         f3 w = make3(0.0f);
         if (near_spec) {
-            Bsdf<RN, VS_RT_MATERIALS> b = make_bsdf<RN, VS_RT_MATERIALS>(s, m, r.it.shading, r.it.ng, r.it.wo, wl);
+            Bsdf<RN, VS_RT_MATERIALS> b = make_bsdf<RN, VS_RT_MATERIALS>(s, m, r.it.shading, r.it.ng, r.it.wo, r.it.uv, wl);
             BsdfSample<RN> bs = sample_delta(b, r.it.wo, smp);
             w = bs.wi;
             RSpec tp = bs.eval.throughput();

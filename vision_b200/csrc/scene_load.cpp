@@ -15,6 +15,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+
+#include "vs_image.h"
 #include <map>
 #include <numeric>
 #include <stdexcept>
@@ -284,12 +286,22 @@ m4 parse_transform(const Json &t) {
     throw unsupported("transform type '" + type + "'");
 }
 
+// A shader node's type and parameters (ShaderNodeDesc::init,
+// node_desc.cpp:292-320): {"type", "param"}, or the parameters inline, where
+// an object naming a file ("fn") is an image node.
+std::string node_type(const Json &n) {
+    if (!n.is_object()) return "";
+    if (n.contains("param")) return n["type"].as_string("number");
+    return n["type"].as_string(n.contains("fn") ? "image" : "number");
+}
+const Json &node_param(const Json &n) { return n.contains("param") ? n["param"] : n; }
+
 // Slot value as a flat float list (SlotDesc::init, node_desc.cpp:127-150).
 std::vector<float> slot_values(const Json &j) {
     if (j.is_number() || j.is_array()) return j.as_floats();
     if (j.is_object()) {
         if (j.contains("channels")) return slot_values(j["node"]);
-        std::string type = j["type"].as_string("number");
+        std::string type = node_type(j);
         if (type == "number" || type == "constant") {
             const Json &p = j.contains("param") ? j["param"] : j;
             return p["value"].as_floats();
@@ -314,6 +326,37 @@ f3 slot_rgb(const Json &j, f3 def) {
 float slot_scalar(const Json &j, float def) {
     std::vector<float> v = slot_values(j);
     return v.empty() ? def : v[0];
+}
+
+// The file of an `image` shader node (image.cpp) as linear RGB texels (4
+// floats each, RGB and 0): the sRGB transfer function removed for the colour
+// space "srgb" (the default of 8-bit files; "linear" for Radiance HDR); a grey
+// file replicated to three channels.
+std::vector<float> load_texture_texels(const Json &node, const std::string &base_dir, uint32_t &w, uint32_t &h) {
+    const Json &p = node_param(node);
+    const std::string fn = p["fn"].as_string();
+    if (fn.empty()) throw std::runtime_error("image node without 'fn'");
+    const bool absolute = !fn.empty() && fn[0] == '/';
+    const std::string path = absolute || base_dir.empty() ? fn : base_dir + "/" + fn;
+    const size_t dot = path.find_last_of('.');
+    std::string ext = dot == std::string::npos ? "" : path.substr(dot + 1);
+    for (char &c : ext) c = static_cast<char>(std::tolower(static_cast<unsigned char>(c)));
+    if (ext != "png" && ext != "jpg" && ext != "jpeg" && ext != "hdr")
+        throw unsupported("image file format '" + ext + "' (" + fn + ")");
+    std::string cs = p["color_space"].as_string("");
+    if (cs.empty()) cs = ext == "hdr" ? "linear" : "srgb";
+    if (cs != "srgb" && cs != "linear") throw unsupported("image colour space '" + cs + "'");
+    const Image im = load_image(path);
+    w = im.width;
+    h = im.height;
+    std::vector<float> t(static_cast<size_t>(w) * h * 4, 0.0f);
+    for (size_t i = 0; i < static_cast<size_t>(w) * h; ++i) {
+        for (int c = 0; c < 3; ++c) {
+            const float v = im.data[i * im.channels + (im.channels >= 3 ? c : 0)];
+            t[4 * i + c] = cs == "srgb" ? srgb_to_linear(v) : v;
+        }
+    }
+    return t;
 }
 
 struct MeshData {
@@ -810,6 +853,72 @@ struct Loader {
     std::map<std::string, uint32_t> mat_by_name;
     std::string base_dir;  // model files are relative to the scene's folder
     bool srgb = false;     // RGB spectrum: colour slots are stored as RGB
+    std::map<std::string, uint32_t> tex_by_key;  // texture ids by file and colour space
+    std::vector<f3> tex_avg;                      // mean texel of each texture (ShaderNode::average)
+
+    // The texture of an `image` node, loaded once per file and colour space.
+    uint32_t texture(const Json &node) {
+        const Json &p = node_param(node);
+        const std::string key = p["fn"].as_string() + "|" + p["color_space"].as_string("");
+        auto it = tex_by_key.find(key);
+        if (it != tex_by_key.end()) return it->second;
+        uint32_t w = 0, h = 0;
+        std::vector<float> t = load_texture_texels(node, base_dir, w, h);
+        TextureRec r{static_cast<uint32_t>(s.tex_texels.size() / 4), w, h, 0u};
+        s.tex_texels.insert(s.tex_texels.end(), t.begin(), t.end());
+        const uint32_t id = static_cast<uint32_t>(s.textures.size());
+        s.textures.push_back(r);
+        double sum[3] = {0.0, 0.0, 0.0};
+        for (size_t i = 0; i < t.size(); i += 4)
+            for (int c = 0; c < 3; ++c) sum[c] += t[i + c];
+        const double n = static_cast<double>(w) * h;
+        tex_avg.push_back({static_cast<float>(sum[0] / n), static_cast<float>(sum[1] / n), static_cast<float>(sum[2] / n)});
+        tex_by_key[key] = id;
+        return id;
+    }
+
+    // A colour slot that is an `image` node, or a `multiply` node (math.cpp)
+    // of an image node and a constant: the texture and the constant factor.
+    bool texture_slot(const Json &slot, uint32_t &id, f3 &factor) {
+        const Json &n = slot_node(slot);
+        if (!n.is_object()) return false;
+        const std::string t = node_type(n);
+        if (t == "image") {
+            id = texture(n);
+            factor = make3(1.0f);
+            return true;
+        }
+        if (t != "multiply") return false;
+        const Json &lhs = slot_node(n["param"]["lhs"]), &rhs = slot_node(n["param"]["rhs"]);
+        const bool li = node_type(lhs) == "image";
+        const bool ri = node_type(rhs) == "image";
+        if (li == ri) throw unsupported("multiply node other than an image times a constant");
+        id = texture(li ? lhs : rhs);
+        factor = slot_rgb(n["param"][li ? "rhs" : "lhs"], make3(1.0f));
+        return true;
+    }
+
+    // A material's colour slot: a constant stored through albedo_coef, or a
+    // texture (flag kMatFlagTexture, id in p[7]) whose constant factor is
+    // stored as RGB in coef; the device decodes each lookup.  Returns the
+    // slot's average colour (the texture's mean texel times the factor).
+    f3 colour_slot(const Json &slot, f3 def, Material &mat) {
+        uint32_t id;
+        f3 factor;
+        if (texture_slot(slot, id, factor)) {
+            mat.flags |= kMatFlagTexture;
+            mat.p[7] = bits_float(id);
+            mat.coef[0] = factor.x;
+            mat.coef[1] = factor.y;
+            mat.coef[2] = factor.z;
+            mat.coef[3] = 0.0f;
+            return {tex_avg[id].x * factor.x, tex_avg[id].y * factor.y, tex_avg[id].z * factor.z};
+        }
+        const f3 rgb = slot_rgb(slot, def);
+        const float in[3] = {rgb.x, rgb.y, rgb.z};
+        albedo_coef(in, mat.coef);
+        return rgb;
+    }
 
     // A colour slot as the material record stores it: sigmoid coefficients
     // for the hero spectrum (RGBAlbedoSpectrum), the colour itself for the
@@ -863,9 +972,7 @@ struct Loader {
         } else if (type == "diffuse") {
             // DiffuseMaterial: colour slot, default 0.5 (diffuse.cpp:37-44).
             mat.type = kMatDiffuse;
-            rgb = slot_rgb(p["color"], make3(0.5f));
-            float in[3] = {rgb.x, rgb.y, rgb.z};
-            albedo_coef(in, mat.coef);
+            rgb = colour_slot(p["color"], make3(0.5f), mat);
         } else if (type == "black_body") {
             mat.type = kMatBlackBody;
         } else if (type == "metal") {
@@ -900,13 +1007,30 @@ struct Loader {
             float a = remap ? r * r : r;
             alpha_aniso(a, aniso, mat.p[0], mat.p[1]);
             s.needs_luts = true;
+        } else if (type == "metallic") {
+            // MetallicMaterial (metallic.cpp:26-60): MetallicLobe, a
+            // compensated GGX reflection with kr = colour and the F82-tint
+            // Fresnel (F0 = colour, F82 = edge tint); roughness clamped to
+            // [0.01, 1] and always remapped to alpha = r^2.
+            mat.type = kMatMetal;
+            mat.flags |= kMatFlagF82;
+            rgb = colour_slot(p["color"], make3(1.0f), mat);
+            const f3 et = slot_rgb(p["edge_tint"], make3(1.0f));
+            const float ein[3] = {et.x, et.y, et.z};
+            float ec[4];
+            albedo_coef(ein, ec);
+            mat.p[2] = ec[0];
+            mat.p[3] = ec[1];
+            mat.p[4] = ec[2];
+            const float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.01f, 1.0f);
+            const float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
+            alpha_aniso(r * r, aniso, mat.p[0], mat.p[1]);
+            s.needs_luts = true;
         } else if (type == "glass") {
             // GlassMaterial (glass.cpp:169-257): colour, ior (number, spd node,
             // named Sellmeier glass, or a Cauchy curve), roughness, anisotropy.
             mat.type = kMatGlass;
-            rgb = slot_rgb(p["color"], make3(1.0f));
-            float in[3] = {rgb.x, rgb.y, rgb.z};
-            albedo_coef(in, mat.coef);
+            rgb = colour_slot(p["color"], make3(1.0f), mat);
             std::string glass = p["material_name"].as_string();
             const Json &ior = p["ior"];
             const Json &ion = slot_node(ior);
@@ -935,9 +1059,7 @@ struct Loader {
         } else if (type == "principled_bsdf") {
             // PrincipledBSDF (principled_bsdf.cpp:263-461).
             mat.type = kMatPrincipled;
-            rgb = slot_rgb(p["color"], make3(1.0f));
-            float in[3] = {rgb.x, rgb.y, rgb.z};
-            albedo_coef(in, mat.coef);
+            rgb = colour_slot(p["color"], make3(1.0f), mat);
             float r = clampf(slot_scalar(p["roughness"], 0.5f), 0.0001f, 1.0f);
             float aniso = slot_scalar(p["anisotropic"], 0.0f);
             float aspect = std::sqrt(1.0f - aniso * 0.9f);
@@ -974,9 +1096,7 @@ struct Loader {
             // colour slot as kr; roughness default 0.001, remapped to r^2.
             mat.type = kMatMetal;
             mat.flags |= kMatFlagConstantFresnel;
-            rgb = slot_rgb(p["color"], make3(1.0f));
-            float in[3] = {rgb.x, rgb.y, rgb.z};
-            albedo_coef(in, mat.coef);
+            rgb = colour_slot(p["color"], make3(1.0f), mat);
             float r = clampf(slot_scalar(p["roughness"], 0.001f), 0.0001f, 1.0f);
             float aniso = clampf(slot_scalar(p["anisotropic"], 0.0f), -0.9f, 0.9f);
             float a = p["remapping_roughness"].as_bool(true) ? r * r : r;
@@ -988,9 +1108,7 @@ struct Loader {
             // remapped twice like the substrate's; Schlick F0 = F0(ior) * Rs.
             mat.type = kMatSubstrate;
             mat.flags |= kMatFlagPlastic;
-            rgb = slot_rgb(p["color"], make3(1.0f));
-            float in[3] = {rgb.x, rgb.y, rgb.z};
-            albedo_coef(in, mat.coef);
+            rgb = colour_slot(p["color"], make3(1.0f), mat);
             f3 spec = slot_rgb(p["spec"], make3(0.05f));
             float sin[3] = {spec.x, spec.y, spec.z}, sc[4];
             albedo_coef(sin, sc);
@@ -1012,9 +1130,7 @@ struct Loader {
             // remapping the reference squares the roughness and then the
             // anisotropic alphas once more; alphas clamp to [1e-4, 1].
             mat.type = kMatSubstrate;
-            rgb = slot_rgb(p["color"], make3(1.0f));
-            float in[3] = {rgb.x, rgb.y, rgb.z};
-            albedo_coef(in, mat.coef);
+            rgb = colour_slot(p["color"], make3(1.0f), mat);
             f3 spec = slot_rgb(p["spec"], make3(0.05f));
             float sin[3] = {spec.x, spec.y, spec.z}, sc[4];
             albedo_coef(sin, sc);
@@ -1364,12 +1480,15 @@ Camera camera_at_resolution(const Camera &base, uint32_t width, uint32_t height)
 // SphericalMap (spherical.cpp:26-215) with a procedural sky image and its
 // AliasTable2D (alias2d.cpp:30-66) built from luminance * sin(theta) weights
 // (calculate_weights, spherical.cpp:187-213).
-static void load_spherical(const Json &p, const Json &root, HostScene &s) {
+static void load_spherical(const Json &p, const Json &root, HostScene &s, const std::string &base_dir) {
     const Json &cn = slot_node(p["color"]);
-    if (!cn.is_object() || cn["type"].as_string() != "sky")
-        throw unsupported("spherical light colour other than a procedural 'sky' node");
+    const std::string ct = node_type(cn);
+    if (ct != "sky" && ct != "image")
+        throw unsupported("spherical light colour other than an 'image' or a procedural 'sky' node");
     uint32_t W, H;
-    s.env_tex = make_sky(cn["param"], W, H);
+    // The map's texels as the image node gives them (width along phi, height
+    // along theta), or the procedural sky.
+    s.env_tex = ct == "sky" ? make_sky(cn["param"], W, H) : load_texture_texels(cn, base_dir, W, H);
     EnvLight &e = s.env;
     e.width = W;
     e.height = H;
@@ -1560,7 +1679,7 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
         }
         if (lt != "spherical") throw unsupported("light type '" + lt + "' in light_sampler");
         if (s.has_env) throw unsupported("more than one environment light");
-        load_spherical(l["param"], root, s);
+        load_spherical(l["param"], root, s, ld.base_dir);
     }
     s.ip.light_count = static_cast<uint32_t>(s.lights.size()) + (s.has_env ? 1u : 0u);
     if (s.ip.light_count == 0) throw unsupported("scene without lights");

@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) k_svgf_geom(const __grid_constant__ Devic
         g.nz = n.z;
         g.linear_depth = xform_point(p.w2c, it.pos).z;
         if (it.mat != kInvalid) {
-            const Bsdf<3> bsdf = make_bsdf<3>(s, s.materials[it.mat], it.shading, it.ng, it.wo, wl);
+            const Bsdf<3> bsdf = make_bsdf<3>(s, s.materials[it.mat], it.shading, it.ng, it.wo, it.uv, wl);
             albedo = linear_srgb<3>(bsdf.albedo(dot(n, it.wo)), wl);
         }
         if (it.light != kInvalid) {

@@ -13,7 +13,7 @@
 // albedo).
 #pragma once
 
-#include "vs_device.cuh"
+#include "vs_texture.cuh"
 #include "vs_microfacet.h"
 
 namespace vs {
@@ -600,7 +600,7 @@ struct Bsdf {
 // come from the 64-byte material record written by the scene loader.
 template <int N, uint32_t M = kAllMaterials>
 __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng, f3 wo,
-                                const Wavelengths<N> &wl) {
+                                f2 uv, const Wavelengths<N> &wl) {
     Bsdf<N, M> b;
     b.type = m.type;
     b.frame = frame;
@@ -612,7 +612,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
     b.has_trans = false;
     b.trans_scale = 0.0f;
     if (has_mat<M>(kMatDiffuse) && m.type == kMatDiffuse) {
-        b.kd = albedo_spectrum<N>(m.coef, wl);
+        b.kd = colour_spectrum<N>(s, m, uv, wl);
     } else if (has_mat<M>(kMatMetal) && m.type == kMatMetal) {
         // MetalMaterial::create_lobe_set (metal.cpp:137-156).
         MfLobe<N> &l = b.mf[0];
@@ -623,7 +623,22 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
         if (m.flags & kMatFlagConstantFresnel) {
             // MirrorMaterial::create_lobe_set (mirror.cpp:59-74): FresnelConstant, kr = colour.
             l.fresnel = kFresnelConstant;
-            l.kr = albedo_spectrum<N>(m.coef, wl);
+            l.kr = colour_spectrum<N>(s, m, uv, wl);
+        } else if (m.flags & kMatFlagF82) {
+            // MetallicMaterial::create_lobe_set (metallic.cpp:42-60): kr =
+            // colour, FresnelF82Tint with F0 = colour and init_from_F82(edge
+            // tint) (fresnel.h:114-120).
+            l.fresnel = kFresnelF82;
+            l.kr = colour_spectrum<N>(s, m, uv, wl);
+            const Spec<N> edge = albedo_spectrum<N>(m.p + 2, wl);
+            const float f = 6.0f / 7.0f;
+            const float f5 = f * f * f * f * f;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                l.fa.v[i] = l.kr.v[i];
+                const float fs = l.kr.v[i] + f5 * (1.0f - l.kr.v[i]);
+                l.fb.v[i] = fs * (7.0f / (f5 * f)) * (1.0f - edge.v[i]);
+            }
         } else {
             l.fresnel = kFresnelConductor;
             l.kr = Spec<N>::fill(1.0f);
@@ -640,7 +655,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
         DielLobe<N> &d = b.dl;
         d.ax = m.p[0];
         d.ay = m.p[1];
-        d.kt = albedo_spectrum<N>(m.coef, wl);
+        d.kt = colour_spectrum<N>(s, m, uv, wl);
         d.compensate = true;
         d.schlick = false;
         bool front = dot(wo, ng) > 0.0f;
@@ -656,7 +671,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
     } else if (has_mat<M>(kMatSubstrate) && m.type == kMatSubstrate) {
         // SubstrateMaterial::create_lobe_set (substrate.cpp:126-148);
         // PlasticMaterial::create_lobe_set (plastic.cpp:105-129).
-        b.kd = albedo_spectrum<N>(m.coef, wl);
+        b.kd = colour_spectrum<N>(s, m, uv, wl);
         b.ks = albedo_spectrum<N>(m.p + 2, wl);
         b.mf[0].ax = m.p[0];
         b.mf[0].ay = m.p[1];
@@ -677,7 +692,7 @@ __device__ VS_OUTLINE Bsdf<N, M> make_bsdf(const DeviceScene &s, const Material 
         float ax = m.p[0], ay = m.p[1];
         float metallic_param = m.p[2];
         float ior = m.p[3];
-        Spec<N> color = albedo_spectrum<N>(m.coef, wl);
+        Spec<N> color = colour_spectrum<N>(s, m, uv, wl);
         const float tint_coef[3] = {m.p[4], m.p[5], m.p[6]};
         Spec<N> tint = albedo_spectrum<N>(tint_coef, wl);
         float cos_theta = dot(wo, ng);
@@ -886,10 +901,10 @@ struct MixBsdf {
 
 template <int N>
 __device__ VS_OUTLINE MixBsdf<N> make_mix_bsdf(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng,
-                                              f3 wo, const Wavelengths<N> &wl) {
+                                              f3 wo, f2 uv, const Wavelengths<N> &wl) {
     MixBsdf<N> r;
-    r.c[0] = make_bsdf<N>(s, s.materials[m.spd0], frame, ng, wo, wl);
-    r.c[1] = make_bsdf<N>(s, s.materials[m.spd1], frame, ng, wo, wl);
+    r.c[0] = make_bsdf<N>(s, s.materials[m.spd0], frame, ng, wo, uv, wl);
+    r.c[1] = make_bsdf<N>(s, s.materials[m.spd1], frame, ng, wo, uv, wl);
     if (m.flags & kMatFlagAdd) {
         r.w[0] = r.w[1] = 1.0f;
         r.sw[0] = r.sw[1] = 0.5f;
@@ -908,16 +923,16 @@ template <int N, uint32_t M>
 struct ShadeBsdf {
     using type = Bsdf<N, M>;
     __device__ __forceinline__ static type make(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng,
-                                                f3 wo, const Wavelengths<N> &wl) {
-        return make_bsdf<N, M>(s, m, frame, ng, wo, wl);
+                                                f3 wo, f2 uv, const Wavelengths<N> &wl) {
+        return make_bsdf<N, M>(s, m, frame, ng, wo, uv, wl);
     }
 };
 template <int N>
 struct ShadeBsdf<N, kMixMask> {
     using type = MixBsdf<N>;
     __device__ __forceinline__ static type make(const DeviceScene &s, const Material &m, const Frame &frame, f3 ng,
-                                                f3 wo, const Wavelengths<N> &wl) {
-        return make_mix_bsdf<N>(s, m, frame, ng, wo, wl);
+                                                f3 wo, f2 uv, const Wavelengths<N> &wl) {
+        return make_mix_bsdf<N>(s, m, frame, ng, wo, uv, wl);
     }
 };
 

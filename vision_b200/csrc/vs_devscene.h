@@ -27,6 +27,8 @@ struct DeviceScene {
     uint32_t has_env;
     uint32_t env_index;           // light index of the environment (last)
     const float4 *env_tex;
+    const float4 *tex_texels;     // textures of image nodes (TextureRec offsets)
+    const uint4 *textures;        // TextureRec per texture
     const AliasEntry *env_marginal;
     const float *env_marginal_func;
     const AliasEntry *env_cond;

@@ -5,50 +5,9 @@
 // decode of RGBToSpectrumTable::decode_unbound (hero.cpp:92-141).
 #pragma once
 
-#include "vs_device.cuh"
+#include "vs_texture.cuh"
 
 namespace vs {
-
-// decode_albedo / decode_unbound on the device with the exact trilinear
-// interpolation of the host path (hero.cpp:92-141).
-__device__ __forceinline__ void rgb2spec_unbound(const float4 *table, f3 rgb_in, float c[4]) {
-    f3 rgb = vmax(rgb_in, make3(0.0f));
-    float m = max3(rgb);
-    float scale = 2.0f * m;
-    f3 q = scale == 0.0f ? make3(0.0f) : rgb / scale;
-    q = {clampf(q.x, 0.0f, 1.0f), clampf(q.y, 0.0f, 1.0f), clampf(q.z, 0.0f, 1.0f)};
-    c[3] = scale;
-    if (q.x == q.y && q.y == q.z) {
-        c[0] = 0.0f;
-        c[1] = 0.0f;
-        c[2] = (q.x - 0.5f) / sqrtf(q.x * (1.0f - q.x));
-        return;
-    }
-    const int res = 64;
-    uint32_t maxc = (q.x > q.y) ? ((q.x > q.z) ? 0u : 2u) : ((q.y > q.z) ? 1u : 2u);
-    float z = comp(q, maxc);
-    float x = comp(q, (maxc + 1u) % 3u) * (res - 1u) / z;
-    float y = comp(q, (maxc + 2u) % 3u) * (res - 1u) / z;
-    auto inv_ss = [](float v) { return 0.5f - sinf(asinf(1.0f - 2.0f * v) * (1.0f / 3.0f)); };
-    float zz = inv_ss(inv_ss(z)) * (res - 1u);
-    uint32_t xi = min(static_cast<uint32_t>(x), static_cast<uint32_t>(res - 2));
-    uint32_t yi = min(static_cast<uint32_t>(y), static_cast<uint32_t>(res - 2));
-    uint32_t zi = min(static_cast<uint32_t>(zz), static_cast<uint32_t>(res - 2));
-    float dx = x - xi, dy = y - yi, dz = zz - zi;
-    auto co = [&](int ox, int oy, int oz) {
-        return __ldg(&table[(((static_cast<size_t>(maxc) * res + (zi + oz)) * res + (yi + oy)) * res + (xi + ox))]);
-    };
-    float4 c000 = co(0, 0, 0), c100 = co(1, 0, 0), c010 = co(0, 1, 0), c110 = co(1, 1, 0);
-    float4 c001 = co(0, 0, 1), c101 = co(1, 0, 1), c011 = co(0, 1, 1), c111 = co(1, 1, 1);
-    auto tri = [&](float a000, float a100, float a010, float a110, float a001, float a101, float a011, float a111) {
-        float x00 = lerpf(dx, a000, a100), x10 = lerpf(dx, a010, a110);
-        float x01 = lerpf(dx, a001, a101), x11 = lerpf(dx, a011, a111);
-        return lerpf(dz, lerpf(dy, x00, x10), lerpf(dy, x01, x11));
-    };
-    c[0] = tri(c000.x, c100.x, c010.x, c110.x, c001.x, c101.x, c011.x, c111.x);
-    c[1] = tri(c000.y, c100.y, c010.y, c110.y, c001.y, c101.y, c011.y, c111.y);
-    c[2] = tri(c000.z, c100.z, c010.z, c110.z, c001.z, c101.z, c011.z, c111.z);
-}
 
 // Bilinear lookup of the map (texel centres at (i + 0.5) / size, u wraps,
 // v clamps).

@@ -41,6 +41,9 @@ struct HostScene {
     bool has_env = false;
     EnvLight env{};
     std::vector<float> env_tex;  // 4 floats (RGB, 0) per texel, row-major from the zenith
+    // Textures of `image` shader nodes (colour slots): 4 floats per texel.
+    std::vector<float> tex_texels;
+    std::vector<TextureRec> textures;
     std::vector<AliasEntry> env_marginal, env_cond;
     std::vector<float> env_marginal_func, env_cond_func;
     f3 env_avg{};                  // average texel colour times the light's scale

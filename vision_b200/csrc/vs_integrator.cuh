@@ -396,7 +396,7 @@ __device__ __forceinline__ bool path_shade_acc(const DeviceScene &s, PathState<N
     if (kTraceShadow) occluded = trace_any(s, precompute_ray(sh.o, sh.d), sh.tmax);
     // Material evaluation + BSDF sample (direct_lighting, integrator.cpp:20-44).
     Material mat = s.materials[it.mat];
-    const typename ShadeBsdf<N, M>::type bsdf = ShadeBsdf<N, M>::make(s, mat, it.shading, it.ng, it.wo, ps.wl);
+    const typename ShadeBsdf<N, M>::type bsdf = ShadeBsdf<N, M>::make(s, mat, it.shading, it.ng, it.wo, it.uv, ps.wl);
     if (bsdf.dispersive) invalidate_secondary<N>(ps.wl);
     f3 wi_light = normalize(ls.p_light - it.pos);
     BsdfEval<N> se = bsdf.evaluate(it.wo, wi_light, nullptr);

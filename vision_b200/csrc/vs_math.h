@@ -25,6 +25,16 @@ constexpr float kOneMinusEpsilon = 0.99999994039535522461f;
 constexpr float kShadowEpsilon = 0.0001f;
 constexpr uint32_t kInvalid = 0xffffffffu;
 
+// A product the device compiler may not fuse into a multiply-add: where a
+// sum of products is shared by several inlined call sites, the choice of
+// which product to fuse can differ between kernels, and with it the last
+// bit of the result.
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+#else
+inline float mul_rn(float a, float b) { return a * b; }
+#endif
+
 struct f2 { float x, y; };
 struct f3 { float x, y, z; };
 struct alignas(16) f4 { float x, y, z, w; };

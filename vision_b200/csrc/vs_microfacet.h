@@ -86,36 +86,39 @@ VS_HD float fresnel_dielectric(float abs_cos_i, float eta) {
 }
 
 // fresnel_complex (src/math/optics.h:92-115) with the complex arithmetic of
-// src/math/complex.h: eta_c = eta + i k.
+// src/math/complex.h: eta_c = eta + i k.  Products are unfused (mul_rn), so
+// every kernel that inlines the conductor rounds it alike (and as the host).
 struct cplx {
     float re, im;
 };
 VS_HD cplx c_add(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
 VS_HD cplx c_sub(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
-VS_HD cplx c_mul(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
-VS_HD cplx c_div(cplx a, cplx b) {
-    float s = 1.0f / (b.re * b.re + b.im * b.im);
-    return {s * (a.re * b.re + a.im * b.im), s * (a.im * b.re - a.re * b.im)};
+VS_HD cplx c_mul(cplx a, cplx b) {
+    return {mul_rn(a.re, b.re) - mul_rn(a.im, b.im), mul_rn(a.re, b.im) + mul_rn(a.im, b.re)};
 }
-VS_HD float c_norm(cplx z) { return z.re * z.re + z.im * z.im; }
+VS_HD cplx c_div(cplx a, cplx b) {
+    float s = 1.0f / (mul_rn(b.re, b.re) + mul_rn(b.im, b.im));
+    return {mul_rn(s, mul_rn(a.re, b.re) + mul_rn(a.im, b.im)), mul_rn(s, mul_rn(a.im, b.re) - mul_rn(a.re, b.im))};
+}
+VS_HD float c_norm(cplx z) { return mul_rn(z.re, z.re) + mul_rn(z.im, z.im); }
 VS_HD cplx c_sqrt(cplx z) {
     float n = sqrtf(c_norm(z));
-    float t1 = sqrtf(0.5f * (n + fabsf(z.re)));
-    float t2 = 0.5f * z.im / t1;
+    float t1 = sqrtf(mul_rn(0.5f, n + fabsf(z.re)));
+    float t2 = mul_rn(0.5f, z.im) / t1;
     if (n == 0.0f) return {0.0f, 0.0f};
     if (z.re >= 0.0f) return {t1, t2};
     return {fabsf(t2), copysignf(t1, z.im)};
 }
 VS_HD float fresnel_complex(float cos_i, float eta, float k) {
     cplx e = {eta, k};
-    float sin2_i = 1.0f - cos_i * cos_i;
+    float sin2_i = 1.0f - mul_rn(cos_i, cos_i);
     cplx sin2_t = c_div({sin2_i, 0.0f}, c_mul(e, e));
     cplx cos_t = c_sqrt(c_sub({1.0f, 0.0f}, sin2_t));
-    cplx ec = {e.re * cos_i, e.im * cos_i};
+    cplx ec = {mul_rn(e.re, cos_i), mul_rn(e.im, cos_i)};
     cplx r_parl = c_div(c_sub(ec, cos_t), c_add(ec, cos_t));
     cplx ect = c_mul(e, cos_t);
     cplx r_perp = c_div(c_sub({cos_i, 0.0f}, ect), c_add({cos_i, 0.0f}, ect));
-    return (c_norm(r_parl) + c_norm(r_perp)) * 0.5f;
+    return mul_rn(c_norm(r_parl) + c_norm(r_perp), 0.5f);
 }
 
 // refract (src/math/optics.h:27-39).

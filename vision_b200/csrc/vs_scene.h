@@ -25,6 +25,14 @@ enum MaterialFlag : uint32_t {
     kMatFlagConstantFresnel = 4u,  // kMatMetal written by a `mirror` (mirror.cpp): F = 1, kr = colour
     kMatFlagPlastic = 8u,          // kMatSubstrate written by a `plastic` (plastic.cpp): PlasticLobe
     kMatFlagAdd = 16u,             // kMatMix written by an `add` (add.cpp): weights 1, sample weights 1/2
+    kMatFlagTexture = 32u,         // colour slot from an `image` node: texture id in p[7] (bits), coef = RGB factor
+    kMatFlagF82 = 64u,             // kMatMetal written by a `metallic` (metallic.cpp): F82 tint, edge tint in p[2..4]
+};
+
+// A texture of the `image` shader node: linear RGB texels (float4) at
+// `offset` in the scene's texel array, width x height, row 0 the top.
+struct TextureRec {
+    uint32_t offset, width, height, pad;
 };
 
 // 64 bytes.  `coef` holds RGB->spectrum sigmoid coefficients (c0, c1, c2) of

@@ -112,6 +112,20 @@ def substrate_room(width=64, height=64, dimension=4, sampler="independent", max_
     return sc
 
 
+def metallic_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
+    """The box room with `metallic` materials (MetallicMaterial: colour as F0
+    and reflectance, F82 edge tint): a warm tall box, an anisotropic short
+    box with a blue edge tint and a near-specular back wall."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    mats = {m["name"]: m for m in sc["materials"]}
+    mats["TallBox"].update({"type": "metallic", "param": {"color": [0.95, 0.64, 0.37], "edge_tint": [1.0, 0.85, 0.7],
+                                                          "roughness": 0.35}})
+    mats["ShortBox"].update({"type": "metallic", "param": {"color": [0.8, 0.82, 0.85], "edge_tint": [0.6, 0.7, 1.0],
+                                                           "roughness": 0.3, "anisotropic": 0.5}})
+    mats["BackWall"].update({"type": "metallic", "param": {"color": [0.9, 0.9, 0.9], "roughness": 0.1}})
+    return sc
+
+
 def principled_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8):
     """The box room with principled BSDFs that use every layer: a sheen-and-
     coat tall box over a metallic base, a transmissive short box with a coat,
@@ -168,6 +182,29 @@ def mix_room(width=64, height=64, dimension=4, sampler="independent", max_depth=
         "frac": 0.6,
         "mat0": {"type": "plastic", "param": {"color": [0.2, 0.4, 0.7], "roughness": 0.2}},
         "mat1": {"type": "substrate", "param": {"color": [0.6, 0.5, 0.3], "roughness": 0.3}}}})
+    return sc
+
+
+ROOM_TEXTURES = ("checker.png", "gradient.png", "photo.jpg")
+
+
+def textured_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8, jpeg=True):
+    """The box room with `image` shader nodes in its colour slots: the back
+    wall is a diffuse with an RGB image, the floor a diffuse whose colour is
+    multiply(image, constant) with a grey image, the short box a principled
+    BSDF with the JPEG image (jpeg=False: the RGB image) and the tall box a
+    plastic with the grey image.  The files (ROOM_TEXTURES) are looked up in
+    the scene's base folder."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    mats = {m["name"]: m for m in sc["materials"]}
+    img = lambda fn, **kw: {"type": "image", "param": dict(fn=fn, **kw)}
+    mats["BackWall"]["param"] = {"color": {"channels": "xyz", "node": img("checker.png")}}
+    mats["Floor"]["param"] = {"color": {"channels": "xyz", "node": {"type": "multiply", "param": {
+        "lhs": img("gradient.png"), "rhs": [0.8, 0.7, 0.6]}}}}
+    mats["ShortBox"].update({"type": "principled_bsdf", "param": {
+        "color": img("photo.jpg" if jpeg else "checker.png"), "metallic": 0.1, "roughness": 0.5}})
+    mats["TallBox"].update({"type": "plastic", "param": {
+        "color": img("gradient.png", color_space="linear"), "roughness": 0.2}})
     return sc
 
 
