@@ -1000,9 +1000,47 @@ static void env_eval(const Scene &sc, V3 dir, const Swl &w, float *L, float &pdf
     pdf = st == 0.0f ? 0.0f : p;
 }
 
-// Point / spot light radiance at p_ref (point.cpp:36-41, spot.cpp:47-67):
-// colour * scale / d^2, times the spot falloff.
-static void delta_L(const AreaLight &L, V3 p_ref, const Swl &w, float *out) {
+// Projector::Le (projector.cpp:112-125): the reference point in the
+// light's frame (the 3 x 4 world-to-light rows of its SPD-table block), its
+// squared distance there and the colour slot at the projected uv inside the
+// frustum: a texture decoded as an illumination, or the constant emitter.
+static void projector_L(const Scene &sc, const AreaLight &L, V3 p_ref, const Swl &w, float *out) {
+    const float *b = sc.s->spd + L.alias_offset;
+    V3 p = {b[0] * p_ref.x + b[1] * p_ref.y + b[2] * p_ref.z + b[3],
+            b[4] * p_ref.x + b[5] * p_ref.y + b[6] * p_ref.z + b[7],
+            b[8] * p_ref.x + b[9] * p_ref.y + b[10] * p_ref.z + b[11]};
+    float d2 = dot(p, p);
+    float u = (p.x / p.z + b[12]) / (2.0f * b[12]);
+    float v = (p.y / p.z + b[13]) / (2.0f * b[13]);
+    for (int i = 0; i < w.n; ++i) out[i] = 0.0f;
+    if (!(p.z > 0.0f && u >= 0.0f && u <= 1.0f && v >= 0.0f && v <= 1.0f)) return;
+    uint32_t tex;
+    std::memcpy(&tex, &b[14], 4);
+    if (tex == kInvalid) {
+        emitter(L, w, out);
+        for (int i = 0; i < w.n; ++i) out[i] *= 1.0f / d2;
+        return;
+    }
+    float rgb[3];
+    texture_rgb(sc, tex, u, v, rgb);
+    for (int c = 0; c < 3; ++c) rgb[c] *= L.coef[c];
+    if (is_rgb(w)) {
+        for (int i = 0; i < w.n; ++i) out[i] = rgb[i < 3 ? i : 2] * L.scale / d2;
+        return;
+    }
+    float co[4];
+    decode_unbound(sc.s->rgb2spec, rgb[0], rgb[1], rgb[2], co);
+    for (int i = 0; i < w.n; ++i)
+        out[i] = sigmoid_poly(co, w.lambda[i]) * co[3] * spd_eval(tables().d65, 94, w.lambda[i]) * L.scale / d2;
+}
+
+// Delta-position light radiance at p_ref (point.cpp:36-41, spot.cpp:47-67,
+// projector.cpp:112-125): colour * scale / d^2, times the spot falloff.
+static void delta_L(const Scene &sc, const AreaLight &L, V3 p_ref, const Swl &w, float *out) {
+    if (L.shape == 3) {
+        projector_L(sc, L, p_ref, w, out);
+        return;
+    }
     V3 lp = {L.pos[0], L.pos[1], L.pos[2]};
     V3 wu = sub(p_ref, lp);
     float g = 1.0f / dot(wu, wu);
@@ -1099,7 +1137,7 @@ static LS sample_light(const Scene &sc, const It &it, float ul, float ux, float 
     if (L.shape != 0) {
         // Point / spot light (point.cpp:36-41, spot.cpp:47-67): colour * scale
         // / d^2 (times the spot falloff); pdf -pmf marks the delta light.
-        delta_L(L, it.pos, w, ls.L);
+        delta_L(sc, L, it.pos, w, ls.L);
         ls.pdf = -pmf_l;
         ls.p = V3{L.pos[0], L.pos[1], L.pos[2]};
         return ls;

@@ -66,7 +66,7 @@ assert INTEGRATOR.itemsize == 48 and ENV.itemsize == 160
 DIFFUSE, BLACK_BODY, METAL, GLASS, PRINCIPLED, SUBSTRATE, MIX = range(7)
 FLAG_DISPERSIVE, FLAG_REMAP, FLAG_CONST_FRESNEL, FLAG_PLASTIC, FLAG_ADD, FLAG_TEXTURE, FLAG_F82 = 1, 2, 4, 8, 16, 32, 64
 EMIT_RGB, EMIT_BLACKBODY = 0, 1
-LIGHT_AREA, LIGHT_POINT, LIGHT_SPOT = 0, 1, 2
+LIGHT_AREA, LIGHT_POINT, LIGHT_SPOT, LIGHT_PROJECTOR = 0, 1, 2, 3
 FILTERS = {'box': 0, 'triangle': 1, 'gaussian': 2, 'mitchell': 3, 'sinc': 4}
 TONE_MAPPERS = ('linear', 'aces', 'reinhard')
 
@@ -987,6 +987,73 @@ class _Builder:
                                                                                        falloff)))))
         self.lights.append(L)
 
+    def projector(self, p):
+        """Projector (projector.cpp:30-126): a delta-position light at the
+        origin of o2w projecting its colour slot (an image, an image times a
+        constant, or a constant colour) through a pinhole along +z; its
+        16-float SPD-table block holds the world-to-light rows, the tangents
+        of the half-angles and the texture id's bits."""
+        L = np.zeros(1, LIGHT)[0]
+        L['inst'] = L['first_prim'] = L['prim_count'] = INVALID
+        L['shape'] = LIGHT_PROJECTOR
+        n = _node(p.get('color'))
+        img, factor = None, [F(1.0)] * 3
+        if _node_type(n) == 'image':
+            img = n
+        elif _node_type(n) == 'multiply':
+            q = n.get('param', {}) or {}
+            lhs, rhs = _node(q.get('lhs')), _node(q.get('rhs'))
+            li, ri = _node_type(lhs) == 'image', _node_type(rhs) == 'image'
+            if li == ri:
+                raise Unsupported('multiply node other than an image times a constant')
+            img = lhs if li else rhs
+            factor = _slot_rgb(q.get('rhs') if li else q.get('lhs'), 1.0)
+        tid = INVALID
+        if img is not None:
+            tid = self.texture(img)
+            scale = F(p['scale']) if isinstance(p.get('scale'), (int, float)) else F(1.0)
+            avg = (self.tex_avg[tid] * np.array(factor, np.float32)).astype(np.float32)
+            L['kind'] = EMIT_RGB
+            L['scale'] = scale
+            L['coef'] = [factor[0], factor[1], factor[2], 0.0]
+            L['rgb_avg'][:3] = (avg * scale).astype(np.float32)
+        else:
+            self.emitter(p, L)
+        o2w = transform(p.get('o2w'))
+        L['pos'][:3] = o2w[:3, 3]
+        L['dir'][:3] = _normalize(o2w[:3, 2])
+        inv = np.linalg.inv(o2w[:3, :3].astype(np.float64))
+        w2o = np.zeros((3, 4))
+        w2o[:, :3] = inv
+        w2o[:, 3] = -inv @ o2w[:3, 3].astype(np.float64)
+        ratio = F(p.get('ratio', 1.0))
+        if ratio == 0.0:
+            W, H = self.textures[tid][1:3] if tid != INVALID else (1, 1)
+            ratio = F(F(W) / F(H))
+        angle = F(F(min(max(F(p.get('angle', 45.0)), F(1.0)), F(89.0))) * F(PI / F(180.0)))
+        tan_y = F(math.tan(angle))
+        block = np.zeros(16, np.float32)
+        block[:12] = w2o.astype(np.float32).ravel()
+        block[12], block[13] = F(ratio * tan_y), tan_y
+        block[14] = np.array([tid], np.uint32).view(np.float32)[0]
+        L['alias_offset'] = self.spd_len
+        self.spd.append(block)
+        self.spd_len += 16
+        # Projector::power (projector.cpp:60-90).
+        y = F(math.sqrt(F(F(1.0) / F(F(ratio * ratio) + F(1.0)))))
+        x = F(ratio * y)
+        z = F(math.sqrt(F(F(x * x) + F(y * y))))
+        p0, p1, p2 = (np.array(v, np.float64) for v in ((x, y, z), (x, -y, z), (-x, -y, z)))
+        crosses = []
+        for a, b in ((p0, p1), (p1, p2), (p2, p0)):
+            c = np.cross(a, b)
+            crosses.append(c / np.linalg.norm(c) if np.dot(c, c) > 0 else c)
+        c01, c12, c20 = crosses
+        solid = abs(math.acos(np.clip(np.dot(c01, -c12), -1, 1)) + math.acos(np.clip(np.dot(c12, -c20), -1, 1)) +
+                    math.acos(np.clip(np.dot(c20, -c01), -1, 1)) - math.pi)
+        L['lum_power'] = luminance(L['rgb_avg'][:3] * F(F(2.0 * solid) / F(4.0 * PI)))
+        self.lights.append(L)
+
     def sky(self, p):
         """The procedural `sky` node: a lat-long image (row 0 at the zenith)
         with a horizon-to-zenith gradient (sqrt of the elevation fraction),
@@ -1139,6 +1206,8 @@ class _Builder:
             lt = l.get('type', 'area')
             if lt in ('point', 'spot'):
                 self.point_light(lt, l.get('param', {}))
+            elif lt == 'projector':
+                self.projector(l.get('param', {}))
             elif lt == 'spherical':
                 if self.env is not None:
                     raise Unsupported('two environment lights')

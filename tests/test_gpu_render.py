@@ -231,6 +231,44 @@ def test_matched_seed_parity_textures(vb, gpu_ctx, tmp_path, spectrum):
     assert all(_match(f, films[0], 1e-3) >= 0.99 for f in films[1:])
 
 
+@pytest.mark.parametrize('light_sampler, spectrum', [('uniform', 'hero'), ('power', 'hero'), ('power', 'srgb')])
+def test_matched_seed_parity_projector(vb, gpu_ctx, tmp_path, light_sampler, spectrum):
+    # Projector lights (projector.cpp:112-125): an image projected through a
+    # frustum of the image's aspect and a constant colour through a wide
+    # one, with the room's area light; delta lights in next-event estimation
+    # (MIS weight 1), power-sampler weights from the reference's formula.
+    from helpers import mean_z, path_sums, pixel_z, write_room_textures
+    write_room_textures(str(tmp_path))
+
+    def doc(w, h, **kw):
+        d = scenes.projector_room(w, h, light_sampler=light_sampler, area_light=True, **kw)
+        if spectrum == 'srgb':
+            d['spectrum'] = {'type': 'srgb'}
+        return d
+    s = vb.Scene(gpu_ctx, doc(64, 64, max_depth=2), base_dir=str(tmp_path)).build_accel()
+    o = oracle.OracleScene(s)
+    s.render(0, 16)
+    g, c = s.film(), o.render(0, 16)
+    assert np.all(np.isfinite(g)) and c[..., :3].max() > 0
+    assert _match(g, c, 1e-3) >= 0.99
+    s = vb.Scene(gpu_ctx, doc(48, 48), base_dir=str(tmp_path)).build_accel()
+    o = oracle.OracleScene.from_json(doc(48, 48), str(tmp_path))
+    s.render(0, 32, fp64=True)
+    gs, gq = s.film(vb.FILM_SUM64)[..., :3], s.film(vb.FILM_SUMSQ64)[..., :3]
+    cs, cq = path_sums(o.paths(np.arange(48 * 48, dtype=np.uint32), 0, 32))
+    cs, cq = cs.reshape(48, 48, 3), cq.reshape(48, 48, 3)
+    z = pixel_z(gs, gq, 32, cs, cq, 32)
+    assert (np.abs(z) > 4.0).mean() <= 0.005
+    assert abs(mean_z(gs, gq, 32, cs, cq, 32)) < 4.0
+    films = []
+    for schedule in ('wavefront', 'grid', 'persistent'):
+        t = vb.Scene(gpu_ctx, doc(32, 32), base_dir=str(tmp_path)).build_accel()
+        t.set_schedule(schedule)
+        t.render(0, 4)
+        films.append(t.film())
+    assert all(np.array_equal(f, films[0]) for f in films[1:])
+
+
 def test_matched_seed_parity_plastic(vb, gpu_ctx):
     # PlasticLobe: Lambert (1 - F) plus Schlick-weighted GGX reflection.
     s = vb.Scene(gpu_ctx, scenes.plastic_room(64, 64, max_depth=2)).build_accel()

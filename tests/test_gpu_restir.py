@@ -33,7 +33,7 @@ def _run(vb, ctx, sc, cams, w, h, base_dir='.'):
 
 
 @pytest.mark.parametrize('materials', ['diffuse', 'metal', 'two_bsdf_candidates', 'substrate_mirror', 'srgb',
-                                       'plastic', 'point_spot', 'environment', 'textured'])
+                                       'plastic', 'point_spot', 'environment', 'textured', 'projector'])
 def test_restir_frames_match_oracle(vb, gpu_ctx, tmp_path, materials):
     # 'diffuse': diffuse walls and emitters (the kernels compiled for those
     # materials alone); 'metal': a gold box as well (the general kernels);
@@ -80,6 +80,13 @@ def test_restir_frames_match_oracle(vb, gpu_ctx, tmp_path, materials):
                 m.update({'type': 'substrate', 'param': {'color': [0.6, 0.5, 0.4], 'roughness': 0.2,
                                                          'remapping_roughness': False}})
     base_dir = '.'
+    if materials == 'projector':
+        # Projectors among the candidates: delta lights whose radiance is an
+        # image lookup (or a constant) inside a frustum.
+        from helpers import write_room_textures
+        write_room_textures(str(tmp_path))
+        base_dir = str(tmp_path)
+        sc['light_sampler']['param']['lights'] += scenes.projector_room()['light_sampler']['param']['lights']
     if materials == 'textured':
         from helpers import write_room_textures
         write_room_textures(str(tmp_path))

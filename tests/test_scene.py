@@ -179,7 +179,7 @@ def test_golden_alias_tables(vb, host_ctx):
 
 def test_unsupported_light_in_light_sampler(vb, host_ctx):
     sc = scenes.box_room(width=4, height=4)
-    sc['light_sampler']['param']['lights'] = [{'type': 'projector', 'param': {}}]
+    sc['light_sampler']['param']['lights'] = [{'type': 'photometric', 'param': {}}]
     with pytest.raises(vb.UnsupportedError):
         vb.Scene(host_ctx, sc)
 

@@ -212,3 +212,43 @@ def test_image_node_outside_colour_slots_is_unsupported(vb, host_ctx, tmp_path):
 def test_missing_image_file_is_an_error(vb, host_ctx, tmp_path):
     with pytest.raises(vb.VisionError, match='cannot open'):
         _texels(vb, host_ctx, tmp_path, 'nope.png')
+
+
+def test_projector_records(vb, host_ctx, tmp_path):
+    # Projector (projector.cpp:30-126): a delta-position light (shape 3) at
+    # o2w's origin; its SPD-table block holds the world-to-light rows, the
+    # half-angle tangents and the texture id; ratio 0 takes the image's
+    # aspect; the power follows the reference's frustum formula.
+    from oracle import scene as oscene
+    write_room_textures(str(tmp_path))
+    doc = scenes.projector_room(16, 16)
+    s = vb.Scene(host_ctx, doc, base_dir=str(tmp_path))
+    lights = s.export('lights', oscene.LIGHT)
+    spd = s.export('spd', np.float32)
+    assert [int(L['shape']) for L in lights] == [3, 3]
+    img, warm = lights
+    np.testing.assert_allclose(img['pos'][:3], [0.1, 0.55, 1.2], rtol=1e-6)
+    b = spd[img['alias_offset']:img['alias_offset'] + 16]
+    w2o = np.eye(4)
+    w2o[:3] = b[:12].reshape(3, 4)
+    # The light's +z axis points at the target; the origin maps to the position.
+    tgt = w2o @ np.array([0.0, 0.5, -0.5, 1.0])
+    assert tgt[2] > 0 and abs(tgt[0]) < 1e-5 and abs(tgt[1]) < 1e-5
+    np.testing.assert_allclose(w2o @ np.array([0.1, 0.55, 1.2, 1.0]), [0, 0, 0, 1], atol=1e-6)
+    tan_y = np.tan(np.float32(14.0) * np.float32(np.pi / 180.0))
+    np.testing.assert_allclose(b[13], tan_y, rtol=1e-6)
+    np.testing.assert_allclose(b[12], tan_y * 64.0 / 48.0, rtol=1e-6)  # checker.png is 64 x 48
+    tex = s.export('textures', np.uint32).reshape(-1, 4)
+    assert b[14:15].view(np.uint32)[0] < tex.shape[0]
+    wb = spd[warm['alias_offset']:warm['alias_offset'] + 16]
+    assert wb[14:15].view(np.uint32)[0] == 0xffffffff
+    np.testing.assert_allclose(wb[12] / wb[13], 1.5, rtol=1e-6)
+    # The oracle's own ingestion agrees (records, block and power).
+    arr, _ = oscene.build(doc, str(tmp_path))
+    o = arr['lights']
+    for f in ('shape', 'kind', 'alias_offset'):
+        np.testing.assert_array_equal(lights[f], o[f])
+    for f in ('pos', 'dir', 'coef', 'rgb_avg', 'scale', 'lum_power'):
+        np.testing.assert_allclose(lights[f], o[f], rtol=2e-5, atol=1e-6)
+    np.testing.assert_allclose(spd, arr['spd'], rtol=2e-6, atol=1e-6)
+    np.testing.assert_array_equal(s.export('light_pmf', np.float32) > 0, arr['light_pmf'] > 0)

@@ -329,7 +329,7 @@ __device__ __forceinline__ PointEval eval_light_point(const DeviceScene &s, f3 p
     AreaLight L = s.lights[light];
     if (L.shape != kLightArea) {
         const f3 lpos = make3(L.pos[0], L.pos[1], L.pos[2]);
-        e.L = delta_light_L<RN>(L, p_ref, wl);
+        e.L = delta_light_L<RN>(s, L, p_ref, wl);
         e.pdf = -1.0f * pmf;
         e.p_light = lpos;
         e.lp.pos = lpos;

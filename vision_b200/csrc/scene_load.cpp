@@ -1281,6 +1281,78 @@ struct Loader {
         s.lights.push_back(L);
     }
 
+    // Projector (projector.cpp:30-126): a delta-position light at the origin
+    // of `o2w` that projects its colour slot (an image node, alone or times a
+    // constant, or a constant colour) through a pinhole looking along +z,
+    // vertical half-angle `angle` (degrees, clamped to [1, 89]), width over
+    // height `ratio` (0: the image's aspect).
+    void add_projector(const Json &p) {
+        AreaLight L{};
+        L.inst = L.first_prim = L.prim_count = kInvalid;
+        L.shape = kLightProjector;
+        uint32_t tex = kInvalid;
+        f3 factor = make3(1.0f);
+        if (texture_slot(p["color"], tex, factor)) {
+            // The texel times the factor is decoded per lookup as an
+            // illumination (decode_to_illumination); an image is not
+            // normalised (Light::Light applies NumberNode::normalize only).
+            const float scale = p["scale"].is_number() ? p["scale"].as_float() : 1.0f;
+            const f3 avg = {tex_avg[tex].x * factor.x, tex_avg[tex].y * factor.y, tex_avg[tex].z * factor.z};
+            L.kind = kEmitRGB;
+            L.scale = scale;
+            L.coef[0] = factor.x;
+            L.coef[1] = factor.y;
+            L.coef[2] = factor.z;
+            L.coef[3] = 0.0f;
+            L.rgb_avg[0] = avg.x * scale;
+            L.rgb_avg[1] = avg.y * scale;
+            L.rgb_avg[2] = avg.z * scale;
+            s.light_rgb.push_back(avg);
+        } else {
+            emitter_colour(p, L);
+        }
+        const m4 o2w = parse_transform(p["o2w"]);
+        const m4 w2o = invert_affine(o2w);
+        L.pos[0] = o2w.m[3][0];
+        L.pos[1] = o2w.m[3][1];
+        L.pos[2] = o2w.m[3][2];
+        const f3 d = normalize(make3(o2w.m[2][0], o2w.m[2][1], o2w.m[2][2]));
+        L.dir[0] = d.x;
+        L.dir[1] = d.y;
+        L.dir[2] = d.z;
+        float ratio = p["ratio"].as_float(1.0f);
+        if (ratio == 0.0f)
+            ratio = tex != kInvalid ? static_cast<float>(s.textures[tex].width) / static_cast<float>(s.textures[tex].height)
+                                    : 1.0f;
+        const float angle = clampf(p["angle"].as_float(45.0f), 1.0f, 89.0f) * (kPi / 180.0f);
+        const float tan_y = std::tan(angle);
+        float block[kProjectorBlock] = {};
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) block[4 * r + c] = w2o.m[c][r];
+        block[12] = ratio * tan_y;
+        block[13] = tan_y;
+        block[14] = bits_float(tex);
+        L.alias_offset = static_cast<uint32_t>(s.spd.size());
+        s.spd.insert(s.spd.end(), block, block + kProjectorBlock);
+        // Projector::power (projector.cpp:60-90): the solid angle of a
+        // frustum with 45-degree corners (the reference's formula, which does
+        // not depend on `angle`) over 4 pi, times two, times the average.
+        const float y = std::sqrt(1.0f / (ratio * ratio + 1.0f));
+        const float x = ratio * y;
+        const float z = std::sqrt(x * x + y * y);
+        const f3 p0 = {x, y, z}, p1 = {x, -y, z}, p2 = {-x, -y, z};
+        f3 c01 = cross(p0, p1), c12 = cross(p1, p2), c20 = cross(p2, p0);
+        if (length_sq(c01) > 0.0f) c01 = normalize(c01);
+        if (length_sq(c12) > 0.0f) c12 = normalize(c12);
+        if (length_sq(c20) > 0.0f) c20 = normalize(c20);
+        const float solid = std::fabs(std::acos(clampf(dot(c01, -c12), -1.0f, 1.0f)) +
+                                      std::acos(clampf(dot(c12, -c20), -1.0f, 1.0f)) +
+                                      std::acos(clampf(dot(c20, -c01), -1.0f, 1.0f)) - kPi);
+        const f3 avg = make3(L.rgb_avg[0], L.rgb_avg[1], L.rgb_avg[2]);
+        L.lum_power = linear_srgb_to_y(avg * ((2.0f * solid) / (4.0f * kPi)));
+        s.lights.push_back(L);
+    }
+
     // Light::Light (light.cpp:10-17): the colour slot (RGB illumination or the
     // blackbody emitter) and the scale, with RGB colours normalised so that
     // the largest channel is folded into the scale; also the average colour.
@@ -1675,6 +1747,10 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
         std::string lt = l["type"].as_string("area");
         if (lt == "point" || lt == "spot") {
             ld.add_point_light(lt, l["param"]);
+            continue;
+        }
+        if (lt == "projector") {
+            ld.add_projector(l["param"]);
             continue;
         }
         if (lt != "spherical") throw unsupported("light type '" + lt + "' in light_sampler");

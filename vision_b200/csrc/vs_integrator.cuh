@@ -122,10 +122,45 @@ __device__ __forceinline__ float spot_falloff(const AreaLight &L, float cos_thet
     return f2 * f2;
 }
 
-// PointLight::Le / SpotLight::Le seen from p_ref: colour * scale / distance^2,
-// times the spot's falloff.
+// Projector::Le (projector.cpp:112-125): the reference point in the light's
+// frame, its squared distance there, and the colour slot at the projected uv
+// when it falls inside the frustum (zero outside and behind).
 template <int N>
-__device__ __forceinline__ Spec<N> delta_light_L(const AreaLight &L, f3 p_ref, const Wavelengths<N> &wl) {
+__device__ __forceinline__ Spec<N> projector_L(const DeviceScene &s, const AreaLight &L, f3 p_ref,
+                                               const Wavelengths<N> &wl) {
+    const float *b = s.spd + L.alias_offset;
+    const f3 p = {b[0] * p_ref.x + b[1] * p_ref.y + b[2] * p_ref.z + b[3],
+                  b[4] * p_ref.x + b[5] * p_ref.y + b[6] * p_ref.z + b[7],
+                  b[8] * p_ref.x + b[9] * p_ref.y + b[10] * p_ref.z + b[11]};
+    const float d2 = length_sq(p);
+    const float u = (p.x / p.z + b[12]) / (2.0f * b[12]);
+    const float v = (p.y / p.z + b[13]) / (2.0f * b[13]);
+    Spec<N> r = Spec<N>::fill(0.0f);
+    if (!(p.z > 0.0f && u >= 0.0f && u <= 1.0f && v >= 0.0f && v <= 1.0f)) return r;
+    const uint32_t tex = __float_as_uint(b[14]);
+    if (tex == kInvalid) return emitter_spectrum<N>(L, wl) * (1.0f / d2);
+    const f3 t = texture_rgb(s, tex, make2(u, v));
+    const f3 rgb = {t.x * L.coef[0], t.y * L.coef[1], t.z * L.coef[2]};
+    if (is_rgb(wl)) {
+        const float ch[3] = {rgb.x, rgb.y, rgb.z};
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.v[i] = ch[i < 3 ? i : 2] * L.scale / d2;
+        return r;
+    }
+    float c[4];
+    rgb2spec_unbound(s.rgb2spec, rgb, c);
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        r.v[i] = sigmoid_poly(c[0], c[1], c[2], wl.lambda[i]) * c[3] * cie_spd(c_spec.d65, wl.lambda[i]) * L.scale / d2;
+    return r;
+}
+
+// Radiance of a delta-position light at p_ref (PointLight::Le, point.cpp:36-41;
+// SpotLight::Le, spot.cpp:47-67; Projector::Le).
+template <int N>
+__device__ __forceinline__ Spec<N> delta_light_L(const DeviceScene &s, const AreaLight &L, f3 p_ref,
+                                                 const Wavelengths<N> &wl) {
+    if (L.shape == kLightProjector) return projector_L<N>(s, L, p_ref, wl);
     const f3 lp = make3(L.pos[0], L.pos[1], L.pos[2]);
     const f3 w_un = p_ref - lp;
     float g = 1.0f / length_sq(w_un);
@@ -159,7 +194,7 @@ __device__ VS_OUTLINE LightSample<N> sample_light(const DeviceScene &s, const In
         // SpotLight::Le: colour * scale / distance^2, times the spot's
         // falloff.  A negative pdf marks the delta light (direct_lighting,
         // integrator.cpp:29-31: MIS weight 1, pdf = the light's pmf).
-        ls.L = delta_light_L<N>(L, it.pos, wl);
+        ls.L = delta_light_L<N>(s, L, it.pos, wl);
         ls.pdf = -pmf_light;
         ls.p_light = make3(L.pos[0], L.pos[1], L.pos[2]);
         return ls;

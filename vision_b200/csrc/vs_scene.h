@@ -54,7 +54,11 @@ enum EmitterKind : uint32_t {
 
 // Shape of a light record: an emissive instance, or one of the delta
 // lights of the light sampler's list (IPointLight, light.h:220-249).
-enum LightShape : uint32_t { kLightArea = 0, kLightPoint = 1, kLightSpot = 2 };
+// A projector keeps, at `alias_offset` in the SPD table, a 16-float block:
+// world-to-light rows (3 x 4), tan of the horizontal and vertical
+// half-angles, the texture id (bits; kInvalid for a constant colour) and 0.
+enum LightShape : uint32_t { kLightArea = 0, kLightPoint = 1, kLightSpot = 2, kLightProjector = 3 };
+constexpr uint32_t kProjectorBlock = 16;
 
 // 112 bytes.  Point and spot lights leave the instance fields unused.
 struct alignas(16) AreaLight {

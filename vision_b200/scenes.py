@@ -208,6 +208,26 @@ def textured_room(width=64, height=64, dimension=4, sampler="independent", max_d
     return sc
 
 
+def projector_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8, light_sampler="uniform",
+                   area_light=False):
+    """The box room lit by two projectors (Projector): one casts the RGB
+    image of textured_room's files (checker.png, its aspect ratio) onto the
+    back wall, the other a constant warm colour onto the floor through a
+    wide 1.5 : 1 frustum; with or without the room's area light."""
+    sc = box_room(width=width, height=height, dimension=dimension, sampler=sampler, max_depth=max_depth)
+    if not area_light:
+        sc["shapes"] = [s for s in sc["shapes"] if s["name"] != "light"]
+    look = lambda pos, target: {"type": "look_at", "param": {"position": pos, "target_pos": target, "up": [0, 1, 0]}}
+    image = {"type": "projector", "param": {
+        "color": {"channels": "xyz", "node": {"fn": "checker.png", "color_space": "srgb"}},
+        "angle": 14.0, "ratio": 0, "scale": 3.0, "o2w": look([0.1, 0.55, 1.2], [0.0, 0.5, -0.5])}}
+    warm = {"type": "projector", "param": {
+        "color": {"channels": "xyz", "node": [1.0, 0.7, 0.4]}, "angle": 25.0, "ratio": 1.5, "scale": 0.6,
+        "o2w": look([0.0, 0.95, 0.3], [0.05, 0.0, 0.1])}}
+    sc["light_sampler"] = {"type": light_sampler, "param": {"lights": [image, warm]}}
+    return sc
+
+
 def point_light_room(width=64, height=64, dimension=4, sampler="independent", max_depth=8, light_sampler="uniform",
                      area_light=True):
     """The box room lit by a white point light near the ceiling and a warm
