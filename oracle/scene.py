@@ -590,6 +590,7 @@ def load_texels(node, base_dir):
     replicated to RGB, alpha dropped.  Decoded by OpenCV: PNG and Radiance
     HDR exactly as the library does; baseline JPEG to within a few levels of
     8 bits (libjpeg's integer IDCT against the library's float IDCT)."""
+    os.environ.setdefault('OPENCV_IO_ENABLE_OPENEXR', '1')
     import cv2
     p = _node_param(node)
     fn = p.get('fn', '')
@@ -597,9 +598,9 @@ def load_texels(node, base_dir):
         raise ValueError('image node without fn')
     path = fn if os.path.isabs(fn) or not base_dir else os.path.join(base_dir, fn)
     ext = fn.rsplit('.', 1)[-1].lower() if '.' in fn else ''
-    if ext not in ('png', 'jpg', 'jpeg', 'hdr'):
+    if ext not in ('png', 'jpg', 'jpeg', 'hdr', 'exr'):
         raise Unsupported('image file format ' + ext)
-    cs = p.get('color_space') or ('linear' if ext == 'hdr' else 'srgb')
+    cs = p.get('color_space') or ('linear' if ext in ('hdr', 'exr') else 'srgb')
     if cs not in ('srgb', 'linear'):
         raise Unsupported('image colour space ' + cs)
     im = cv2.imread(path, cv2.IMREAD_UNCHANGED)

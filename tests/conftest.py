@@ -1,6 +1,9 @@
 import os
 import sys
 
+# OpenCV reads OpenEXR files (the image decoders' reference) only when asked.
+os.environ.setdefault('OPENCV_IO_ENABLE_OPENEXR', '1')
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

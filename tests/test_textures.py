@@ -188,7 +188,7 @@ def test_environment_map_from_an_image_file(vb, host_ctx, tmp_path):
 
 
 @pytest.mark.parametrize('node, what', [
-    ({'type': 'image', 'param': {'fn': 'a.exr'}}, 'exr'),
+    ({'type': 'image', 'param': {'fn': 'a.tga'}}, 'tga'),
     ({'type': 'multiply', 'param': {'lhs': {'type': 'image', 'param': {'fn': 'checker.png'}},
                                     'rhs': {'type': 'image', 'param': {'fn': 'gradient.png'}}}}, 'multiply'),
     ({'type': 'image', 'param': {'fn': 'checker.png', 'color_space': 'aces'}}, 'colour space'),
@@ -252,3 +252,56 @@ def test_projector_records(vb, host_ctx, tmp_path):
         np.testing.assert_allclose(lights[f], o[f], rtol=2e-5, atol=1e-6)
     np.testing.assert_allclose(spd, arr['spd'], rtol=2e-6, atol=1e-6)
     np.testing.assert_array_equal(s.export('light_pmf', np.float32) > 0, arr['light_pmf'] > 0)
+
+
+@pytest.mark.parametrize('compression', [0, 1, 2, 3])
+@pytest.mark.parametrize('half', [True, False])
+def test_openexr_decoder_matches_opencv(vb, host_ctx, tmp_path, compression, half):
+    # OpenEXR scanline files written by OpenEXR through OpenCV: NONE, RLE,
+    # ZIPS and ZIP, HALF and FLOAT channels; a ragged last ZIP block (37
+    # lines), grey (a Y channel) and RGBA; linear by default.
+    rng = np.random.default_rng(compression + 10 * half)
+    img = (rng.random((37, 29, 3)) * np.array([0.5, 8.0, 300.0])).astype(np.float32)
+    img[5:9] = 1.25  # runs for RLE
+    params = [cv2.IMWRITE_EXR_COMPRESSION, compression,
+              cv2.IMWRITE_EXR_TYPE, cv2.IMWRITE_EXR_TYPE_HALF if half else cv2.IMWRITE_EXR_TYPE_FLOAT]
+    cv2.imwrite(str(tmp_path / 'a.exr'), img[..., ::-1], params)
+    ref = cv2.imread(str(tmp_path / 'a.exr'), cv2.IMREAD_UNCHANGED)[..., ::-1]
+    t = _texels(vb, host_ctx, tmp_path, 'a.exr')
+    np.testing.assert_array_equal(t[..., :3], ref)
+    if half:
+        np.testing.assert_allclose(t[..., :3], img, rtol=1e-3)
+    else:
+        np.testing.assert_array_equal(t[..., :3], img)
+    grey = img[..., 1].copy()
+    cv2.imwrite(str(tmp_path / 'g.exr'), grey, params)
+    tg = _texels(vb, host_ctx, tmp_path, 'g.exr')
+    ref_g = cv2.imread(str(tmp_path / 'g.exr'), cv2.IMREAD_UNCHANGED)
+    np.testing.assert_array_equal(tg[..., :3], np.repeat(ref_g[..., None], 3, 2))
+    rgba = np.concatenate([img, np.full(img.shape[:2] + (1,), 0.5, np.float32)], -1)
+    cv2.imwrite(str(tmp_path / 'c.exr'), rgba[..., [2, 1, 0, 3]], params)
+    tc = _texels(vb, host_ctx, tmp_path, 'c.exr')
+    np.testing.assert_array_equal(tc[..., :3], cv2.imread(str(tmp_path / 'c.exr'), cv2.IMREAD_UNCHANGED)[..., 2::-1])
+
+
+def test_openexr_piz_is_unsupported(vb, host_ctx, tmp_path):
+    img = np.ones((8, 8, 3), np.float32)
+    cv2.imwrite(str(tmp_path / 'p.exr'), img, [cv2.IMWRITE_EXR_COMPRESSION, 4])
+    with pytest.raises(vb.UnsupportedError, match='PIZ'):
+        _texels(vb, host_ctx, tmp_path, 'p.exr')
+
+
+REF_SKY = '/root/reference/res/render_scene/cbox/textures/sky.exr'
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SKY), reason='reference assets absent')
+def test_reference_sky_exr_as_environment(vb, host_ctx, tmp_path):
+    # The reference's own ZIP / HALF / ABGR map (cbox/textures/sky.exr) as a
+    # spherical light: its texels equal OpenEXR's decode.
+    sc = scenes.box_room(width=8, height=8)
+    sc['light_sampler']['param']['lights'] = [{'type': 'spherical', 'param': {
+        'color': {'fn': REF_SKY, 'color_space': 'linear'}, 'scale': 1.0}}]
+    s = vb.Scene(host_ctx, sc, base_dir=str(tmp_path))
+    env = s.export('env_tex', np.float32).reshape(256, 512, 4)
+    ref = cv2.imread(REF_SKY, cv2.IMREAD_UNCHANGED)
+    np.testing.assert_array_equal(env[..., :3], ref[..., 2::-1])

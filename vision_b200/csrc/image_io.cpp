@@ -5,6 +5,7 @@
 // HDR (RGBE).  Output: linear RGB as float, row 0 the top of the image.
 #include "vs_image.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -21,6 +22,8 @@ std::vector<uint8_t> read_file(const std::string &path) {
 }
 
 [[noreturn]] void bad(const std::string &what) { throw std::runtime_error("image: " + what); }
+// A valid file using a feature these decoders do not implement.
+[[noreturn]] void not_supported(const std::string &what) { throw std::runtime_error("unsupported: image: " + what); }
 
 // ---- DEFLATE (RFC 1951) ------------------------------------------------------
 
@@ -205,7 +208,7 @@ Image decode_png(const std::vector<uint8_t> &f) {
         p += 12 + len;
     }
     if (w == 0 || h == 0 || w > 65536 || h > 65536) bad("PNG size");
-    if (interlace) bad("interlaced PNG is not supported");
+    if (interlace) not_supported("interlaced PNG");
     int channels = 0;
     switch (ctype) {
         case 0: channels = 1; break;
@@ -451,7 +454,7 @@ Image decode_jpeg(const std::vector<uint8_t> &f) {
             }
             frame = true;
         } else if (m >= 0xc2 && m <= 0xcf && m != 0xc4 && m != 0xc8 && m != 0xcc) {
-            bad("progressive, lossless or arithmetic-coded JPEG is not supported");
+            not_supported("progressive, lossless or arithmetic-coded JPEG");
         } else if (m == 0xdd) {
             restart = (d[0] << 8) | d[1];
         } else if (m == 0xda) {
@@ -630,6 +633,208 @@ Image decode_hdr(const std::vector<uint8_t> &f) {
     return out;
 }
 
+// ---- OpenEXR -------------------------------------------------------------------
+// Single-part scanline files as the OpenEXR file layout defines them: magic
+// 20000630, version 2, header attributes (name, type, size, value) up to an
+// empty name, a table of chunk offsets, and chunks of {first line, packed
+// size, data}.  Channels HALF, FLOAT or UINT at full resolution, stored per
+// line in the channel list's (alphabetical) order.  Compression NONE, RLE
+// (runs), ZIPS (one line) or ZIP (16 lines): a zlib stream, after which the
+// byte-delta predictor and the split into two halves of the byte stream are
+// undone.  PIZ, PXR24, B44 and DWA files, tiled, deep and multi-part files
+// are refused.
+
+uint32_t le32(const uint8_t *p) {
+    return p[0] | (static_cast<uint32_t>(p[1]) << 8) | (static_cast<uint32_t>(p[2]) << 16) |
+           (static_cast<uint32_t>(p[3]) << 24);
+}
+
+// IEEE 754 binary16 to binary32 (exact).
+float half_bits_to_float(uint16_t h) {
+    const uint32_t sign = static_cast<uint32_t>(h >> 15) << 31;
+    const uint32_t e = (h >> 10) & 31u, m = h & 1023u;
+    uint32_t bits;
+    if (e == 0) {
+        const float v = std::ldexp(static_cast<float>(m), -24);
+        return sign ? -v : v;
+    }
+    bits = e == 31 ? (sign | 0x7f800000u | (m << 13)) : (sign | ((e + 112u) << 23) | (m << 13));
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+}
+
+// Undo ZIP / RLE preprocessing: deltas of successive bytes (biased by 128),
+// then the first and second halves of the stream interleaved back.
+void exr_unpredict(std::vector<uint8_t> &t) {
+    for (size_t i = 1; i < t.size(); ++i) t[i] = static_cast<uint8_t>(t[i - 1] + t[i] - 128);
+    std::vector<uint8_t> out(t.size());
+    const size_t half = (t.size() + 1) / 2;
+    for (size_t i = 0; i < t.size(); ++i) out[i] = (i & 1) ? t[half + i / 2] : t[i / 2];
+    t.swap(out);
+}
+
+std::vector<uint8_t> exr_unrle(const uint8_t *d, size_t n, size_t expect) {
+    std::vector<uint8_t> out;
+    out.reserve(expect);
+    size_t p = 0;
+    while (p < n) {
+        const int8_t c = static_cast<int8_t>(d[p++]);
+        if (c < 0) {
+            const size_t k = static_cast<size_t>(-c);
+            if (p + k > n) bad("EXR RLE run truncated");
+            out.insert(out.end(), d + p, d + p + k);
+            p += k;
+        } else {
+            if (p >= n) bad("EXR RLE run truncated");
+            out.insert(out.end(), static_cast<size_t>(c) + 1, d[p++]);
+        }
+        if (out.size() > expect) bad("EXR RLE data too long");
+    }
+    return out;
+}
+
+Image decode_exr(const std::vector<uint8_t> &f) {
+    if (f.size() < 8 || le32(f.data()) != 20000630u) bad("not an OpenEXR file");
+    const uint32_t version = le32(f.data() + 4);
+    if ((version & 0xffu) != 2u) bad("EXR version");
+    if (version & 0x200u) not_supported("tiled EXR");
+    if (version & 0x1800u) not_supported("deep or multi-part EXR");
+    size_t p = 8;
+    auto cstr = [&]() {
+        const size_t start = p;
+        while (p < f.size() && f[p] != 0) ++p;
+        if (p >= f.size() || p - start > 255) bad("EXR header truncated");
+        return std::string(reinterpret_cast<const char *>(&f[start]), (p++) - start);
+    };
+    struct Chan {
+        std::string name;
+        uint32_t type;
+        int32_t xs, ys;
+    };
+    std::vector<Chan> chans;
+    int compression = -1;
+    int32_t dw[4] = {0, 0, -1, -1};
+    bool have_dw = false;
+    for (;;) {
+        const std::string name = cstr();
+        if (name.empty()) break;
+        cstr();  // attribute type
+        if (p + 4 > f.size()) bad("EXR header truncated");
+        const uint32_t size = le32(&f[p]);
+        p += 4;
+        if (size > f.size() - p) bad("EXR header truncated");
+        const uint8_t *v = &f[p];
+        if (name == "channels") {
+            size_t q = 0;
+            while (q < size && v[q] != 0) {
+                size_t e = q;
+                while (e < size && v[e] != 0) ++e;
+                if (e + 17 > size) bad("EXR channel list truncated");
+                Chan c{std::string(reinterpret_cast<const char *>(v + q), e - q), le32(v + e + 1),
+                       static_cast<int32_t>(le32(v + e + 9)), static_cast<int32_t>(le32(v + e + 13))};
+                chans.push_back(c);
+                q = e + 17;
+            }
+        } else if (name == "compression") {
+            if (size < 1) bad("EXR compression attribute");
+            compression = v[0];
+        } else if (name == "dataWindow") {
+            if (size < 16) bad("EXR dataWindow attribute");
+            for (int k = 0; k < 4; ++k) dw[k] = static_cast<int32_t>(le32(v + 4 * k));
+            have_dw = true;
+        }
+        p += size;
+    }
+    if (!have_dw || chans.empty() || compression < 0) bad("EXR header lacks channels, compression or dataWindow");
+    const int64_t w64 = static_cast<int64_t>(dw[2]) - dw[0] + 1, h64 = static_cast<int64_t>(dw[3]) - dw[1] + 1;
+    if (w64 <= 0 || h64 <= 0 || w64 > 65536 || h64 > 65536) bad("EXR size");
+    const uint32_t w = static_cast<uint32_t>(w64), h = static_cast<uint32_t>(h64);
+    static const char *kNames[10] = {"NONE", "RLE", "ZIPS", "ZIP", "PIZ", "PXR24", "B44", "B44A", "DWAA", "DWAB"};
+    uint32_t lines = 0;
+    if (compression == 0 || compression == 1 || compression == 2) lines = 1;
+    else if (compression == 3) lines = 16;
+    else not_supported(std::string("EXR compression ") + (compression < 10 ? kNames[compression] : "unknown"));
+    size_t pixel_bytes = 0;
+    int rgb[3] = {-1, -1, -1}, grey = -1;
+    for (size_t c = 0; c < chans.size(); ++c) {
+        if (chans[c].type > 2) bad("EXR channel type");
+        if (chans[c].xs != 1 || chans[c].ys != 1) not_supported("sub-sampled EXR channels");
+        pixel_bytes += chans[c].type == 1 ? 2 : 4;
+        const std::string &n = chans[c].name;
+        if (n == "R") rgb[0] = static_cast<int>(c);
+        else if (n == "G") rgb[1] = static_cast<int>(c);
+        else if (n == "B") rgb[2] = static_cast<int>(c);
+        else if (n == "Y") grey = static_cast<int>(c);
+    }
+    const bool colour = rgb[0] >= 0 && rgb[1] >= 0 && rgb[2] >= 0;
+    if (!colour && grey < 0) not_supported("EXR without R, G, B or Y channels");
+    Image out;
+    out.width = w;
+    out.height = h;
+    out.channels = colour ? 3 : 1;
+    out.data.assign(static_cast<size_t>(w) * h * out.channels, 0.0f);
+    const size_t line_bytes = pixel_bytes * w;
+    const uint32_t chunks = (h + lines - 1) / lines;
+    if (p + 8ull * chunks > f.size()) bad("EXR offset table truncated");
+    std::vector<bool> seen(chunks, false);
+    for (uint32_t k = 0; k < chunks; ++k) {
+        uint64_t off = 0;
+        for (int b = 7; b >= 0; --b) off = (off << 8) | f[p + 8 * k + b];
+        if (off + 8 > f.size()) bad("EXR chunk offset");
+        const int64_t y0 = static_cast<int64_t>(static_cast<int32_t>(le32(&f[off]))) - dw[1];
+        const uint32_t packed = le32(&f[off + 4]);
+        if (y0 < 0 || y0 >= h64 || y0 % lines != 0 || packed > f.size() - off - 8) bad("EXR chunk header");
+        const uint32_t ci = static_cast<uint32_t>(y0 / lines);
+        if (seen[ci]) bad("EXR chunk repeated");
+        seen[ci] = true;
+        const uint32_t n_lines = std::min<uint32_t>(lines, h - static_cast<uint32_t>(y0));
+        const size_t expect = line_bytes * n_lines;
+        const uint8_t *d = &f[off + 8];
+        std::vector<uint8_t> raw;
+        if (compression == 0 || packed == expect) {
+            if (packed != expect) bad("EXR chunk size");
+            raw.assign(d, d + packed);
+        } else {
+            if (compression == 1) {
+                raw = exr_unrle(d, packed, expect);
+            } else {
+                if (packed < 2) bad("EXR zlib stream");
+                raw = inflate(d + 2, packed - 2, expect);
+            }
+            if (raw.size() != expect) bad("EXR chunk decodes to the wrong size");
+            exr_unpredict(raw);
+        }
+        for (uint32_t l = 0; l < n_lines; ++l) {
+            const uint8_t *row = raw.data() + l * line_bytes;
+            float *dst = out.data.data() + (static_cast<size_t>(y0) + l) * w * out.channels;
+            size_t at = 0;
+            for (size_t c = 0; c < chans.size(); ++c) {
+                const uint32_t t = chans[c].type;
+                const int slot = colour ? (static_cast<int>(c) == rgb[0] ? 0 : static_cast<int>(c) == rgb[1] ? 1
+                                                                          : static_cast<int>(c) == rgb[2] ? 2 : -1)
+                                        : (static_cast<int>(c) == grey ? 0 : -1);
+                for (uint32_t x = 0; x < w; ++x) {
+                    float v;
+                    if (t == 1) {
+                        v = half_bits_to_float(static_cast<uint16_t>(row[at] | (row[at + 1] << 8)));
+                        at += 2;
+                    } else if (t == 2) {
+                        const uint32_t b = le32(row + at);
+                        std::memcpy(&v, &b, 4);
+                        at += 4;
+                    } else {
+                        v = static_cast<float>(le32(row + at));
+                        at += 4;
+                    }
+                    if (slot >= 0) dst[x * out.channels + slot] = v;
+                }
+            }
+        }
+    }
+    return out;
+}
+
 std::string lower_ext(const std::string &path) {
     const size_t dot = path.find_last_of('.');
     std::string e = dot == std::string::npos ? "" : path.substr(dot + 1);
@@ -645,7 +850,8 @@ Image load_image(const std::string &path) {
     if (e == "png") return decode_png(f);
     if (e == "jpg" || e == "jpeg") return decode_jpeg(f);
     if (e == "hdr") return decode_hdr(f);
-    throw std::runtime_error("image: format of '" + path + "' is not supported (PNG, JPEG, Radiance HDR)");
+    if (e == "exr") return decode_exr(f);
+    throw std::runtime_error("unsupported: image: format of '" + path + "' (PNG, JPEG, Radiance HDR, OpenEXR)");
 }
 
 float srgb_to_linear(float c) {

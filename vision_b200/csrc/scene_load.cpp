@@ -341,10 +341,10 @@ std::vector<float> load_texture_texels(const Json &node, const std::string &base
     const size_t dot = path.find_last_of('.');
     std::string ext = dot == std::string::npos ? "" : path.substr(dot + 1);
     for (char &c : ext) c = static_cast<char>(std::tolower(static_cast<unsigned char>(c)));
-    if (ext != "png" && ext != "jpg" && ext != "jpeg" && ext != "hdr")
+    if (ext != "png" && ext != "jpg" && ext != "jpeg" && ext != "hdr" && ext != "exr")
         throw unsupported("image file format '" + ext + "' (" + fn + ")");
     std::string cs = p["color_space"].as_string("");
-    if (cs.empty()) cs = ext == "hdr" ? "linear" : "srgb";
+    if (cs.empty()) cs = ext == "hdr" || ext == "exr" ? "linear" : "srgb";
     if (cs != "srgb" && cs != "linear") throw unsupported("image colour space '" + cs + "'");
     const Image im = load_image(path);
     w = im.width;

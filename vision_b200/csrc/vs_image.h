@@ -15,8 +15,10 @@ struct Image {
     std::vector<float> data;
 };
 
-// PNG, baseline JPEG or Radiance HDR, by file extension; throws
-// std::runtime_error with the reason otherwise.
+// PNG, baseline JPEG, Radiance HDR or OpenEXR (scanline; NONE, RLE, ZIPS or
+// ZIP compression), by file extension; throws std::runtime_error with the
+// reason otherwise ("unsupported: ..." for a valid file using a feature that
+// is not implemented).
 Image load_image(const std::string &path);
 
 // The sRGB transfer function's inverse (IEC 61966-2-1).
