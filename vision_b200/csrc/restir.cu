@@ -773,6 +773,11 @@ __global__ void k_rt_reset(uint32_t npix, const __grid_constant__ RtBuffers b) {
 #ifndef VS_RT_MIN_BLOCKS
 #define VS_RT_MIN_BLOCKS 3
 #endif
+// The light-candidate pass waits on dependent loads (light table, primitive
+// table, vertices) at a quarter occupancy; its own register budget.
+#ifndef VS_RT_LIGHTS_MIN_BLOCKS
+#define VS_RT_LIGHTS_MIN_BLOCKS VS_RT_MIN_BLOCKS
+#endif
 
 // ReSTIRDI shader0 (direct.cpp:519-557).
 __global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
@@ -920,7 +925,7 @@ __global__ void __launch_bounds__(128) k_di_primary(const __grid_constant__ Devi
 }
 
 // Stage 2: the light candidates and the BSDF candidate's ray.
-__global__ void __launch_bounds__(128, VS_RT_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, VS_RT_LIGHTS_MIN_BLOCKS)
     k_di_lights(const __grid_constant__ DeviceScene s, const __grid_constant__ RtParams p,
                 const __grid_constant__ RtBuffers b) {
     const uint32_t n = *b.di_count;
