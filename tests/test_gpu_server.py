@@ -34,6 +34,24 @@ def test_server_job_equals_render(vb, gpu_ctx, served):
     srv.close()
 
 
+def test_server_mix_material_scene(vb, gpu_ctx, served):
+    # Mix and add materials in a served scene: their hits take the mix
+    # shading class of the batch graphs, as in the wavefront schedule.
+    box, _ = served
+    mixed = vb.Scene(gpu_ctx, scenes.mix_room(40, 32, sampler='pcg', max_depth=6)).build_accel()
+    srv = vb.Server(gpu_ctx, hbm_budget=4 << 30, max_jobs=8, paths_per_batch=1 << 15)
+    ids = [srv.add_scene(mixed), srv.add_scene(box)]
+    jobs = [srv.submit(ids[0], 40, 32, 5, frame_begin=0), srv.submit(ids[1], 64, 48, 3, frame_begin=2)]
+    got = srv.result(jobs[0], timeout=120)
+    srv.result(jobs[1], timeout=120)
+    mixed.render(0, 5)
+    ref = mixed.film()
+    assert np.isfinite(got).all() and ref[..., :3].max() > 0
+    close = np.abs(got - ref) <= 1e-5 + 1e-5 * np.abs(ref)
+    assert close.all(-1).mean() >= 0.999, close.all(-1).mean()
+    srv.close()
+
+
 def test_server_same_alone_and_in_mix(vb, gpu_ctx, served):
     box, big = served
     srv = vb.Server(gpu_ctx, hbm_budget=4 << 30, max_jobs=16, paths_per_batch=1 << 15)

@@ -1468,7 +1468,6 @@ int vs_server_add_scene(vs_server *s, vs_scene *scene, uint32_t *scene_id) {
     {
         std::lock_guard<std::mutex> lock(scene->mu);
         if (!scene->uploaded) return s->fail(VS_E_STATE, "vs_scene_build_accel must precede vs_server_add_scene");
-        if (has_mix(scene->host)) return s->fail(VS_E_UNSUPPORTED, "mix / add materials in served scenes");
         if (scene->ctx->device != s->ctx->device) return s->fail(VS_E_INVALID, "scene on another device");
         rt = scene->host.rt;
         if (rt) {

@@ -329,6 +329,8 @@ public:
     // (Re)captures both batch graphs with `depth` bounce iterations per wave.
     // No batch may be in flight.
     cudaError_t capture(uint32_t depth) {
+        // One k_sv_shade<C> per shading class, in the graph and here.
+        static_assert(kWfClasses == 8, "k_sv_shade launches cover classes 0..7");
         int sms = 0, per_ext = 0, per_shadow = 0, per_gen = 0, per_shade[kWfClasses] = {};
         cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_gen, k_sv_generate, 128, 0);
@@ -340,6 +342,7 @@ public:
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[4], k_sv_shade<4>, 128, 0);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[5], k_sv_shade<5>, 128, 0);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[6], k_sv_shade<6>, 128, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shade[7], k_sv_shade<7>, 128, 0);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_shadow, k_sv_shadow, 128, 0);
         if (e != cudaSuccess) return e;
         auto grid_of = [&](int per) { return static_cast<unsigned>(std::max(1, sms * std::max(per, 1))); };
@@ -371,6 +374,7 @@ public:
                     k_sv_shade<4><<<g_shade[4], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
                     k_sv_shade<5><<<g_shade[5], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
                     k_sv_shade<6><<<g_shade[6], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
+                    k_sv_shade<7><<<g_shade[7], 128, 0, stream>>>(d_scenes, wfb[k], cur, base, d_rad[k]);
                     k_sv_shadow<<<g_shadow, 128, 0, stream>>>(d_scenes, wfb[k], base, d_rad[k]);
                 }
             }
