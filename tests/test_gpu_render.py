@@ -420,6 +420,20 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
         assert np.all(films[schedule][1][..., 3] == 9.0)
 
 
+def test_bvh_collapse_gives_the_same_film(vb, gpu_ctx):
+    # The SAH-optimal and the greedy BVH8 collapse give different trees but
+    # the same closest hits, so the same film bit for bit.
+    films = []
+    for collapse in ('greedy', 'sah'):
+        sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
+        sc['render_setting']['bvh_collapse'] = collapse
+        s = vb.Scene(gpu_ctx, sc).build_accel()
+        s.render(0, 4)
+        films.append((s.film(), s.info()['bvh_node_count']))
+    assert films[0][1] != films[1][1]
+    assert np.array_equal(films[0][0], films[1][0])
+
+
 def test_schedule_rejects_unknown(vb, gpu_ctx):
     s = vb.Scene(gpu_ctx, scenes.box_room(width=8, height=8)).build_accel()
     assert vb.lib.vs_render_schedule_set(s.handle, 7) == vb.VS_E_INVALID

@@ -216,6 +216,23 @@ def test_large_scene_counts(vb, host_ctx):
     assert set(types.tolist()) == {2, 3, 4}
 
 
+def test_bvh_collapse_setting(vb, host_ctx):
+    # render_setting.bvh_collapse: "greedy" (default) or "sah" (the
+    # SAH-optimal choice of each wide node's children: fuller nodes).
+    counts = {}
+    for collapse in ('greedy', 'sah'):
+        sc = scenes.large_scene(width=8, height=8, subdivisions=4, grid=100, tiles=2, sky_width=64, sky_height=32)
+        sc['render_setting']['bvh_collapse'] = collapse
+        s = vb.Scene(host_ctx, sc).build_accel()
+        counts[collapse] = s.info()['bvh_node_count']
+        assert s.export('prim_inst').size > 0
+    assert counts['sah'] < counts['greedy']
+    sc = scenes.box_room(width=4, height=4)
+    sc['render_setting']['bvh_collapse'] = 'binned'
+    with pytest.raises(vb.UnsupportedError, match='bvh_collapse'):
+        vb.Scene(host_ctx, sc)
+
+
 @pytest.mark.parametrize('kind, ok', [('linear', True), ('aces', True), ('reinhard', True), ('filmic', False)])
 def test_tone_mapper_parse(vb, host_ctx, kind, ok):
     sc = scenes.box_room(width=4, height=4)

@@ -3,12 +3,15 @@
 // The reference hands its triangles to OptiX (Geometry::build_accel,
 // src/base/mgr/geometry.cpp:36-52); B200 has no RT-core path here, so the
 // acceleration structure is built on the host: a binned-SAH binary BVH with
-// leaves of at most three triangles is collapsed into 8-wide nodes whose child
-// boxes are quantised to 8 bits per plane against a per-node power-of-two grid
-// (80-byte nodes, after Ylitie, Karras and Laine, "Efficient Incoherent Ray
-// Traversal on GPUs Through Compressed Wide BVHs", HPG 2017).  Child slots are
-// ordered by direction so that traversal visits children roughly front to back
-// by flipping slot bits with the ray octant.
+// leaves of at most three triangles is collapsed into 8-wide nodes whose
+// child boxes are quantised to 8 bits per plane against a per-node
+// power-of-two grid (80-byte nodes, after Ylitie, Karras and Laine,
+// "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs",
+// HPG 2017).  Each wide node's children are chosen greedily (open the largest
+// internal child until there are eight) or, per scene, by that paper's
+// SAH-optimal dynamic programme.  Child slots are ordered by direction so
+// that traversal visits children roughly front to back by flipping slot bits
+// with the ray octant.
 #include "vs_host.h"
 
 #include <algorithm>
@@ -210,14 +213,99 @@ struct Collapse {
         }
     }
 
-    bool is_leaf_child(uint32_t id) const { return n2[id].leaf || subtree_count[id] <= kMaxLeaf; }
+    // SAH-optimal collapse (Ylitie, Karras and Laine 2017, section 3.1):
+    // cost[n][i - 1] is the least SAH cost of binary subtree n spread over at
+    // most i child slots of a wide node: n itself as one child (a leaf of at
+    // most kMaxLeaf triangles, or a wide node whose 8 slots are shared by
+    // n's two subtrees), or i slots shared by its two subtrees.  split[n][i - 1]
+    // is the left subtree's share (0: n as one child); as_leaf[n] says which
+    // one-child form won; split8[n] shares the 8 slots of n as a wide node.
+    static constexpr float kCostNode = 1.0f, kCostPrim = 0.3f;
+    std::vector<std::array<float, 8>> cost;
+    std::vector<std::array<uint8_t, 8>> split;
+    std::vector<uint8_t> as_leaf, split8;
+
+    void optimise() {
+        const size_t m = n2.size();
+        cost.assign(m, {});
+        split.assign(m, {});
+        as_leaf.assign(m, 0);
+        split8.assign(m, 0);
+        // Children get larger ids than their parent (ids are handed out on
+        // entry to the binary build), so a reverse sweep sees them first.
+        for (size_t id = m; id-- > 0;) {
+            const Node2 &n = n2[id];
+            const float area = n.box.area();
+            const uint32_t cnt = subtree_count[id];
+            const float c_leaf = cnt <= kMaxLeaf ? area * kCostPrim * static_cast<float>(cnt) : FLT_MAX;
+            if (n.leaf) {
+                as_leaf[id] = 1;
+                for (int i = 0; i < 8; ++i) cost[id][i] = c_leaf;
+                continue;
+            }
+            const std::array<float, 8> &L = cost[n.left], &R = cost[n.right];
+            // The best sharing of i slots between the two subtrees.
+            auto share = [&](int i, int &best_k) {
+                float best = FLT_MAX;
+                best_k = 0;
+                for (int k = 1; k < i; ++k) {
+                    const float c = L[k - 1] + R[i - k - 1];
+                    if (c < best) {
+                        best = c;
+                        best_k = k;
+                    }
+                }
+                return best;
+            };
+            int k8 = 0;
+            const float s8 = share(8, k8);
+            split8[id] = static_cast<uint8_t>(k8);
+            const float c_node = s8 < FLT_MAX ? area * kCostNode + s8 : FLT_MAX;
+            as_leaf[id] = c_leaf <= c_node ? 1 : 0;
+            const float c_one = std::min(c_leaf, c_node);
+            cost[id][0] = c_one;
+            split[id][0] = 0;
+            for (int i = 2; i <= 8; ++i) {
+                int k = 0;
+                const float c = share(i, k);
+                if (c < c_one) {
+                    cost[id][i - 1] = c;
+                    split[id][i - 1] = static_cast<uint8_t>(k);
+                } else {
+                    cost[id][i - 1] = c_one;
+                    split[id][i - 1] = 0;
+                }
+            }
+        }
+    }
+
+    // The children (binary node ids) that subtree n contributes to a wide
+    // node when given at most i slots.
+    void collect(uint32_t id, int i, std::vector<uint32_t> &ch) const {
+        const int k = split[id][i - 1];
+        if (k == 0) {
+            ch.push_back(id);
+            return;
+        }
+        collect(n2[id].left, k, ch);
+        collect(n2[id].right, i - k, ch);
+    }
+
+    bool optimal = false;  // SAH-optimal children instead of the greedy expansion
+    bool is_leaf_child(uint32_t id) const {
+        return optimal ? as_leaf[id] != 0 : (n2[id].leaf || subtree_count[id] <= kMaxLeaf);
+    }
 
     // Writes node `slot_index` of `out` for binary node `id` and recurses.
     void build(uint32_t id, uint32_t out_index, uint32_t depth) {
         max_depth = std::max(max_depth, depth);
         std::vector<uint32_t> ch;
         if (is_leaf_child(id)) {
-            ch.push_back(id);
+            ch.push_back(id);  // a tree of at most kMaxLeaf primitives: one leaf child
+        } else if (optimal) {
+            const int k = split8[id];
+            collect(n2[id].left, k, ch);
+            collect(n2[id].right, 8 - k, ch);
         } else {
             ch.push_back(n2[id].left);
             ch.push_back(n2[id].right);
@@ -348,7 +436,7 @@ namespace {
 // Binned-SAH binary tree over `n` primitive boxes, collapsed into BVH8 nodes
 // appended to `out` (root at the returned index); leaf entries written by
 // `emit` (see Collapse).  Returns the depth of the collapsed tree.
-uint32_t build_tree(const std::vector<Box> &boxes, std::vector<Bvh8Node> &out, uint32_t &root,
+uint32_t build_tree(bool optimal, const std::vector<Box> &boxes, std::vector<Bvh8Node> &out, uint32_t &root,
                     const std::function<void(uint32_t)> &emit, const std::function<uint32_t()> &leaf_base) {
     const uint32_t n = static_cast<uint32_t>(boxes.size());
     std::vector<f3> cent(n);
@@ -361,6 +449,8 @@ uint32_t build_tree(const std::vector<Box> &boxes, std::vector<Bvh8Node> &out, u
     b2.nodes.resize(b2.next.load());
     Collapse col{b2.nodes, order, emit, leaf_base, out, std::vector<uint32_t>(b2.nodes.size(), 0)};
     col.count_tris(0);
+    col.optimal = optimal;
+    if (optimal) col.optimise();
     root = static_cast<uint32_t>(out.size());
     out.resize(out.size() + 1);
     col.build(0, root, 1);
@@ -421,7 +511,7 @@ void build_bvh8(HostScene &s) {
             }
         };
         uint32_t root = 0;
-        s.bvh_depth = build_tree(boxes, s.nodes, root, emit, [&] { return static_cast<uint32_t>(s.tri_v.size() / 12); });
+        s.bvh_depth = build_tree(s.bvh_sah_collapse, boxes, s.nodes, root, emit, [&] { return static_cast<uint32_t>(s.tri_v.size() / 12); });
         if (s.tri_v.size() != static_cast<size_t>(n) * 12) throw std::runtime_error("bvh8: primitive count mismatch");
         s.tlas_root = 0;
         return;
@@ -447,7 +537,7 @@ void build_bvh8(HostScene &s) {
             }
         };
         uint32_t root = 0;
-        depth = std::max(depth, build_tree(boxes, s.nodes, root, emit,
+        depth = std::max(depth, build_tree(s.bvh_sah_collapse, boxes, s.nodes, root, emit,
                                            [&] { return static_cast<uint32_t>(s.tri_v.size() / 12); }));
         s.blas_root.push_back(root);
     }
@@ -464,7 +554,7 @@ void build_bvh8(HostScene &s) {
     std::vector<Bvh8Node> top;
     uint32_t troot = 0;
     auto emit_inst = [&](uint32_t inst) { s.tlas_inst.push_back(inst); };
-    depth = std::max(depth, build_tree(iboxes, top, troot, emit_inst,
+    depth = std::max(depth, build_tree(s.bvh_sah_collapse, iboxes, top, troot, emit_inst,
                                        [&] { return static_cast<uint32_t>(s.tlas_inst.size()); }));
     // Append the top level after the meshes, its root at node 0: child
     // indices of the top level move by the offset of its other nodes.

@@ -1732,6 +1732,11 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
     {
         const Json &inst = root["render_setting"]["instancing"];
         s.instancing = inst.is_bool() ? (inst.as_bool() ? 2 : 0) : (inst.as_string("auto") == "auto" ? 1 : 0);
+        // How the BVH8 picks each wide node's children (an extension key of
+        // this library: the reference hands its triangles to OptiX).
+        const std::string collapse = root["render_setting"]["bvh_collapse"].as_string("greedy");
+        if (collapse != "greedy" && collapse != "sah") throw unsupported("bvh_collapse '" + collapse + "'");
+        s.bvh_sah_collapse = collapse == "sah";
     }
     // Materials, then shapes (which reference materials by name).
     for (const Json &m : root["materials"].elements()) ld.load_material(m);

@@ -91,6 +91,7 @@ struct HostScene {
     std::vector<uint32_t> inst_mesh;  // per instance
     std::vector<m4> inst_w2o;         // per instance
     int instancing = 1;  // 0: one world-space BVH8; 1: auto; 2: two levels when any mesh is shared
+    bool bvh_sah_collapse = false;  // wide-node children: SAH-optimal (true) or greedy (false)
     bool two_level = false;
     uint32_t tlas_root = 0;
     std::vector<uint32_t> tlas_inst;  // top-level leaf entries: instance ids
