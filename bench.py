@@ -75,14 +75,14 @@ DEFAULT_STEPS = {'box_room': 100, 'large_scene': 5, 'many_lights': 64, 'serving'
 NCU_TRAFFIC_PER_PATH = {('large_scene', 'persistent'): 383.6e6 / 2097152,
                         ('box_room', 'persistent'): 7.42e6 / 1048576,
                         # all wavefront kernels of one render (2,097,152 and 1,048,576 paths)
-                        ('large_scene', 'wavefront'): 3017.6e6 / 2097152,
+                        ('large_scene', 'wavefront'): 3059.95e6 / 2097152,
                         ('box_room', 'wavefront'): 1990.0e6 / 1048576}
 
 # Issue-slot utilisation and active threads per instruction of the dominant
 # traversal kernel, from the committed one-kernel ncu capture of the same
 # workload's 2-spp case (the binding measure of the L1/L2-resident traversal).
 NCU_ISSUE = {('large_scene', 'wavefront'): {
-    'issue_active': 0.715, 'threads_per_inst': 10.3,
+    'issue_active': 0.652, 'threads_per_inst': 12.95,
     'issue_source': 'ncu sm__inst_issued / smsp__thread_inst_executed_per_inst_executed of k_wf_extend '
                     '(profiles/k_wf_extend_large_scene.md)'}}
 

@@ -421,17 +421,19 @@ def test_schedules_give_the_same_film(vb, gpu_ctx, case):
 
 
 def test_bvh_collapse_gives_the_same_film(vb, gpu_ctx):
-    # The SAH-optimal and the greedy BVH8 collapse give different trees but
-    # the same closest hits, so the same film bit for bit.
+    # The SAH-optimal and the greedy BVH8 collapse, with leaves of one or
+    # three triangles, give different trees but the same closest hits, so
+    # the same film bit for bit.
     films = []
-    for collapse in ('greedy', 'sah'):
+    for collapse, leaf in (('sah', 1), ('greedy', 1), ('sah', 3), ('greedy', 3)):
         sc = scenes.large_scene(width=40, height=33, subdivisions=3, grid=40, tiles=4, sky_width=256, sky_height=128)
         sc['render_setting']['bvh_collapse'] = collapse
+        sc['render_setting']['bvh_leaf_size'] = leaf
         s = vb.Scene(gpu_ctx, sc).build_accel()
         s.render(0, 4)
         films.append((s.film(), s.info()['bvh_node_count']))
-    assert films[0][1] != films[1][1]
-    assert np.array_equal(films[0][0], films[1][0])
+    assert len({n for _, n in films}) == 4
+    assert all(np.array_equal(films[0][0], f) for f, _ in films[1:])
 
 
 def test_schedule_rejects_unknown(vb, gpu_ctx):

@@ -49,13 +49,14 @@ def test_box_room_closest_hit_bit_exact(vb, gpu_ctx):
     assert 0.0 < miss_rate < 0.9
 
 
-@pytest.mark.parametrize('collapse', ['greedy', 'sah'])
-def test_triangle_soup_closest_hit_bit_exact(vb, gpu_ctx, collapse):
-    # Both ways of choosing each wide node's children: the BVH changes, the
-    # hits do not.
+@pytest.mark.parametrize('collapse, leaf', [('sah', 1), ('sah', 3), ('greedy', 1), ('greedy', 3)])
+def test_triangle_soup_closest_hit_bit_exact(vb, gpu_ctx, collapse, leaf):
+    # Both ways of choosing each wide node's children, and leaves of one and
+    # of three triangles: the BVH changes, the hits do not.
     P, I = _soup(20000, 5)
     sc = scenes.box_room(width=4, height=4)
     sc['render_setting']['bvh_collapse'] = collapse
+    sc['render_setting']['bvh_leaf_size'] = leaf
     sc['shapes'].append({'type': 'mesh', 'name': 'soup', 'param': {'positions': P, 'indices': I,
                                                                   'material': 'Floor'}})
     s = vb.Scene(gpu_ctx, sc).build_accel()

@@ -217,20 +217,34 @@ def test_large_scene_counts(vb, host_ctx):
 
 
 def test_bvh_collapse_setting(vb, host_ctx):
-    # render_setting.bvh_collapse: "greedy" (default) or "sah" (the
-    # SAH-optimal choice of each wide node's children: fuller nodes).
+    # render_setting.bvh_collapse: "sah" (default: the SAH-optimal choice of
+    # each wide node's children, fuller nodes) or "greedy";
+    # render_setting.bvh_leaf_size: 1 to 3 triangles per leaf, or "auto"
+    # (default: 1 for trees of 4096 primitives or more, else 3).
     counts = {}
     for collapse in ('greedy', 'sah'):
-        sc = scenes.large_scene(width=8, height=8, subdivisions=4, grid=100, tiles=2, sky_width=64, sky_height=32)
-        sc['render_setting']['bvh_collapse'] = collapse
-        s = vb.Scene(host_ctx, sc).build_accel()
-        counts[collapse] = s.info()['bvh_node_count']
-        assert s.export('prim_inst').size > 0
-    assert counts['sah'] < counts['greedy']
-    sc = scenes.box_room(width=4, height=4)
-    sc['render_setting']['bvh_collapse'] = 'binned'
-    with pytest.raises(vb.UnsupportedError, match='bvh_collapse'):
-        vb.Scene(host_ctx, sc)
+        for leaf in (1, 3):
+            sc = scenes.large_scene(width=8, height=8, subdivisions=4, grid=100, tiles=2, sky_width=64, sky_height=32)
+            sc['render_setting']['bvh_collapse'] = collapse
+            sc['render_setting']['bvh_leaf_size'] = leaf
+            s = vb.Scene(host_ctx, sc).build_accel()
+            counts[collapse, leaf] = s.info()['bvh_node_count']
+    assert counts['sah', 1] < counts['greedy', 1] and counts['sah', 3] < counts['greedy', 3]
+    assert counts['sah', 3] < counts['sah', 1]
+    sc = scenes.large_scene(width=8, height=8, subdivisions=4, grid=100, tiles=2, sky_width=64, sky_height=32)
+    assert vb.Scene(host_ctx, sc).build_accel().info()['bvh_node_count'] == counts['sah', 1]
+    small = {}
+    for leaf in ('auto', 3):
+        sc = scenes.box_room(width=4, height=4)
+        sc['render_setting']['bvh_leaf_size'] = leaf
+        small[leaf] = vb.Scene(host_ctx, sc).build_accel().info()['bvh_node_count']
+    assert small['auto'] == small[3]
+    for key, value in (('bvh_collapse', 'binned'), ('bvh_leaf_size', 4), ('bvh_leaf_size', 0),
+                       ('bvh_leaf_size', 'large')):
+        sc = scenes.box_room(width=4, height=4)
+        sc['render_setting'][key] = value
+        with pytest.raises(vb.UnsupportedError, match=key):
+            vb.Scene(host_ctx, sc)
 
 
 @pytest.mark.parametrize('kind, ok', [('linear', True), ('aces', True), ('reinhard', True), ('filmic', False)])

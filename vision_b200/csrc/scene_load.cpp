@@ -1734,9 +1734,19 @@ void load_scene_json(const std::string &text, const std::string &base_dir, const
         s.instancing = inst.is_bool() ? (inst.as_bool() ? 2 : 0) : (inst.as_string("auto") == "auto" ? 1 : 0);
         // How the BVH8 picks each wide node's children (an extension key of
         // this library: the reference hands its triangles to OptiX).
-        const std::string collapse = root["render_setting"]["bvh_collapse"].as_string("greedy");
+        const std::string collapse = root["render_setting"]["bvh_collapse"].as_string("sah");
         if (collapse != "greedy" && collapse != "sah") throw unsupported("bvh_collapse '" + collapse + "'");
         s.bvh_sah_collapse = collapse == "sah";
+        const Json &lj = root["render_setting"]["bvh_leaf_size"];
+        if (lj.is_number()) {
+            const uint32_t leaf = lj.as_uint(1u);
+            if (leaf < 1u || leaf > 3u) throw unsupported("bvh_leaf_size " + std::to_string(leaf) + " (1 to 3)");
+            s.bvh_leaf_size = leaf;
+        } else if (lj.as_string("auto") != "auto") {
+            throw unsupported("bvh_leaf_size '" + lj.as_string() + "' (1 to 3 or \"auto\")");
+        } else {
+            s.bvh_leaf_size = 0;
+        }
     }
     // Materials, then shapes (which reference materials by name).
     for (const Json &m : root["materials"].elements()) ld.load_material(m);

@@ -399,6 +399,21 @@ constexpr int kStackSize = 32;
 // with respect to the float triangle test.
 constexpr float kBoxSlack = 1.000001f;
 
+// A bound on the float triangle test's error in t for a hit on the triangle
+// (a, b, c): 2^-16 of the vertices' largest coordinate distance from the ray
+// origin, in units of t (over the ray's dominant direction component).  The
+// test's error is absolute, of the order of the vertices' distances, so a
+// relative slack alone does not cover hits at tiny t.  Closest-hit culling
+// compares boxes against best_t plus this bound, so a box entered within the
+// error of the best hit (another triangle at the same t, as on an edge shared
+// next to the origin) is still opened.
+__device__ __forceinline__ float tri_t_error(const RayPre &r, const float4 &a, const float4 &b, const float4 &c) {
+    const float m = fmaxf(fmaxf(fmaxf(fabsf(a.x - r.o.x), fabsf(a.y - r.o.y)), fmaxf(fabsf(a.z - r.o.z), fabsf(b.x - r.o.x))),
+                          fmaxf(fmaxf(fabsf(b.y - r.o.y), fabsf(b.z - r.o.z)),
+                                fmaxf(fmaxf(fabsf(c.x - r.o.x), fabsf(c.y - r.o.y)), fabsf(c.z - r.o.z))));
+    return m * fabsf(r.sz) * (1.0f / 65536.0f);
+}
+
 struct NodeHits {
     uint32_t internal_hits;  // bits 24..31: internal children in traversal order
     uint32_t tri_hits;       // bits 0..23: triangles of the leaf children that were hit
@@ -486,8 +501,8 @@ __device__ __forceinline__ f3 xf_vector(const float4 &r0, const float4 &r1, cons
 
 // The closest hit inside instance `inst` with t below the current best.
 static __device__ __noinline__ void instance_closest(const DeviceScene &s, const RayPre &rw, uint32_t inst,
-                                                      float tmax, float &best_t, uint32_t &best_prim, float &best_u,
-                                                      float &best_v, uint32_t &visits) {
+                                                      float tmax, float &best_t, float &best_err, uint32_t &best_prim,
+                                                      float &best_u, float &best_v, uint32_t &visits) {
     const float4 *x = s.inst_xf + 4u * inst;
     const float4 r0 = __ldg(x), r1 = __ldg(x + 1), r2 = __ldg(x + 2), meta = __ldg(x + 3);
     const uint32_t first = __float_as_uint(meta.y);
@@ -503,7 +518,7 @@ static __device__ __noinline__ void instance_closest(const DeviceScene &s, const
             uint32_t slot = (bit - 24u) ^ r.oct;
             uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
             if ((ng.y & 0xff000000u) != 0u && sp < kStackSize) stack[sp++] = ng;
-            intersect_children(s.nodes, child, r, best_t * kBoxSlack, ng, tg);
+            intersect_children(s.nodes, child, r, (best_t + best_err) * kBoxSlack, ng, tg);
             ++visits;
         }
         while (tg.y & 0x00ffffffu) {
@@ -517,6 +532,7 @@ static __device__ __noinline__ void instance_closest(const DeviceScene &s, const
                 uint32_t prim = first + __float_as_uint(a.w);
                 if (t < best_t || (t == best_t && prim < best_prim)) {
                     best_t = t; best_prim = prim; best_u = u; best_v = v;
+                    best_err = tri_t_error(r, a, b, c);
                 }
             }
         }
@@ -568,7 +584,7 @@ static __device__ __noinline__ bool trace_closest(const DeviceScene &s, const Ra
     uint2 stack[kStackSize];
     int sp = 0;
     uint32_t nodes_visited = 0, tris_tested = 0;
-    float best_t = tmax;
+    float best_t = tmax, best_err = 0.0f;
     uint32_t best_prim = kInvalid;
     float best_u = 0.0f, best_v = 0.0f;
     // Root as the only internal child (slot 0) of a virtual parent at index 0.
@@ -582,15 +598,15 @@ static __device__ __noinline__ bool trace_closest(const DeviceScene &s, const Ra
             uint32_t slot = (bit - 24u) ^ r.oct;
             uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
             if ((ng.y & 0xff000000u) != 0u && sp < kStackSize) stack[sp++] = ng;
-            intersect_children(s.nodes, child, r, best_t * kBoxSlack, ng, tg);
+            intersect_children(s.nodes, child, r, (best_t + best_err) * kBoxSlack, ng, tg);
             ++nodes_visited;
         }
         if (s.two_level) {
             while (tg.y & 0x00ffffffu) {
                 uint32_t bit = __ffs(tg.y & 0x00ffffffu) - 1u;
                 tg.y &= ~(1u << bit);
-                instance_closest(s, r, __ldg(s.tlas_inst + tg.x + bit), tmax, best_t, best_prim, best_u, best_v,
-                                 nodes_visited);
+                instance_closest(s, r, __ldg(s.tlas_inst + tg.x + bit), tmax, best_t, best_err, best_prim, best_u,
+                                 best_v, nodes_visited);
             }
         }
         while (tg.y & 0x00ffffffu) {
@@ -606,6 +622,7 @@ static __device__ __noinline__ bool trace_closest(const DeviceScene &s, const Ra
                 uint32_t prim = __float_as_uint(a.w);
                 if (t < best_t || (t == best_t && prim < best_prim)) {
                     best_t = t; best_prim = prim; best_u = u; best_v = v;
+                    best_err = tri_t_error(r, a, b, c);
                 }
             }
         }
@@ -684,6 +701,7 @@ struct TravState {
     int sp;
     float tmax;
     float best_t;
+    float best_err;  // tri_t_error of the best hit
     uint32_t best_prim;
     float best_u, best_v;
 };
@@ -694,6 +712,7 @@ __device__ __forceinline__ void trav_init(TravState &t, const RayPre &r, float t
     t.sp = 0;
     t.tmax = tmax;
     t.best_t = tmax;
+    t.best_err = 0.0f;
     t.best_prim = kInvalid;
     t.best_u = 0.0f;
     t.best_v = 0.0f;
@@ -716,15 +735,15 @@ __device__ __forceinline__ bool closest_step(const DeviceScene &s, const RayPre 
         uint32_t slot = (bit - 24u) ^ r.oct;
         uint32_t child = t.ng.x + __popc(t.ng.y & 0xffu & ((1u << slot) - 1u));
         if ((t.ng.y & 0xff000000u) != 0u && t.sp < kStackSize) stack[t.sp++] = t.ng;
-        intersect_children(s.nodes, child, r, t.best_t * kBoxSlack, t.ng, t.tg);
+        intersect_children(s.nodes, child, r, (t.best_t + t.best_err) * kBoxSlack, t.ng, t.tg);
     }
     if (Levels == kLevelsTwo || (Levels == kLevelsAny && s.two_level)) {
         uint32_t visits = 0;
         while (t.tg.y & 0x00ffffffu) {
             uint32_t bit = __ffs(t.tg.y & 0x00ffffffu) - 1u;
             t.tg.y &= ~(1u << bit);
-            instance_closest(s, r, __ldg(s.tlas_inst + t.tg.x + bit), t.tmax, t.best_t, t.best_prim, t.best_u,
-                             t.best_v, visits);
+            instance_closest(s, r, __ldg(s.tlas_inst + t.tg.x + bit), t.tmax, t.best_t, t.best_err, t.best_prim,
+                             t.best_u, t.best_v, visits);
         }
     }
     while (t.tg.y & 0x00ffffffu) {
@@ -739,6 +758,7 @@ __device__ __forceinline__ bool closest_step(const DeviceScene &s, const RayPre 
             uint32_t prim = __float_as_uint(a.w);
             if (th < t.best_t || (th == t.best_t && prim < t.best_prim)) {
                 t.best_t = th;
+                t.best_err = tri_t_error(r, a, b, c);
                 t.best_prim = prim;
                 t.best_u = u;
                 t.best_v = v;

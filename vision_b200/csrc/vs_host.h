@@ -91,7 +91,8 @@ struct HostScene {
     std::vector<uint32_t> inst_mesh;  // per instance
     std::vector<m4> inst_w2o;         // per instance
     int instancing = 1;  // 0: one world-space BVH8; 1: auto; 2: two levels when any mesh is shared
-    bool bvh_sah_collapse = false;  // wide-node children: SAH-optimal (true) or greedy (false)
+    bool bvh_sah_collapse = true;  // wide-node children: SAH-optimal (true) or greedy (false)
+    uint32_t bvh_leaf_size = 0;    // most triangles (or instances) per leaf child, 1..3; 0: by tree size
     bool two_level = false;
     uint32_t tlas_root = 0;
     std::vector<uint32_t> tlas_inst;  // top-level leaf entries: instance ids
