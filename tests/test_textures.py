@@ -305,3 +305,42 @@ def test_reference_sky_exr_as_environment(vb, host_ctx, tmp_path):
     env = s.export('env_tex', np.float32).reshape(256, 512, 4)
     ref = cv2.imread(REF_SKY, cv2.IMREAD_UNCHANGED)
     np.testing.assert_array_equal(env[..., :3], ref[..., 2::-1])
+
+
+@pytest.mark.parametrize('ext', ['png', 'jpg', 'hdr', 'exr'])
+def test_corrupt_image_files_fail_cleanly(vb, host_ctx, tmp_path, ext):
+    # Truncated and byte-damaged files either decode or raise an error
+    # through the C ABI; the decoders check every length, table id, code
+    # length and size they read (a damaged JPEG once indexed past its Huffman
+    # tables).
+    rng = np.random.default_rng(17)
+    img = (rng.random((19, 27, 3)) * 255).astype(np.uint8)
+    src = tmp_path / ('src.' + ext)
+    if ext == 'hdr':
+        cv2.imwrite(str(src), img.astype(np.float32) / 7)
+    elif ext == 'exr':
+        cv2.imwrite(str(src), img.astype(np.float32) / 9, [cv2.IMWRITE_EXR_COMPRESSION, 3])
+    elif ext == 'jpg':
+        cv2.imwrite(str(src), img, [cv2.IMWRITE_JPEG_RST_INTERVAL, 2])
+    else:
+        cv2.imwrite(str(src), img)
+    raw = src.read_bytes()
+    outcomes = set()
+    for trial in range(240):
+        b = bytearray(raw)
+        kind = trial % 3
+        if kind == 0:
+            b = b[:int(rng.integers(0, len(b)))]
+        elif kind == 1:
+            for _ in range(int(rng.integers(1, 8))):
+                b[int(rng.integers(0, len(b)))] = int(rng.integers(0, 256))
+        else:
+            i = int(rng.integers(0, len(b)))
+            b[i:i + 4] = bytes(rng.integers(0, 256, 4).astype(np.uint8))
+        (tmp_path / ('bad.' + ext)).write_bytes(bytes(b))
+        try:
+            _texels(vb, host_ctx, tmp_path, 'bad.' + ext, color_space='linear')
+            outcomes.add('decoded')
+        except vb.VisionError:
+            outcomes.add('error')
+    assert 'error' in outcomes

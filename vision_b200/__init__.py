@@ -268,7 +268,7 @@ class Context:
 
     def check(self, rc, what):
         if rc != VS_OK:
-            msg = '%s: %s' % (what, lib.vs_last_error(self.handle).decode())
+            msg = '%s: %s' % (what, lib.vs_last_error(self.handle).decode('utf-8', 'replace'))
             raise (UnsupportedError if rc == VS_E_UNSUPPORTED else VisionError)(rc, msg)
 
     def rgb_to_spectrum(self, rgb, mode=0):

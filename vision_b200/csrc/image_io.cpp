@@ -22,6 +22,13 @@ std::vector<uint8_t> read_file(const std::string &path) {
 }
 
 [[noreturn]] void bad(const std::string &what) { throw std::runtime_error("image: " + what); }
+// Text taken from a file, for an error message: printable ASCII only.
+std::string printable(const std::string &s) {
+    std::string r = s.substr(0, 64);
+    for (char &c : r)
+        if (c < 0x20 || c > 0x7e) c = '?';
+    return r;
+}
 // A valid file using a feature these decoders do not implement.
 [[noreturn]] void not_supported(const std::string &what) { throw std::runtime_error("unsupported: image: " + what); }
 
@@ -218,7 +225,9 @@ Image decode_png(const std::vector<uint8_t> &f) {
         case 6: channels = 4; break;
         default: bad("PNG colour type");
     }
-    if (!(depth == 8 || depth == 16 || (depth < 8 && (ctype == 0 || ctype == 3)))) bad("PNG bit depth");
+    const bool low = depth == 1 || depth == 2 || depth == 4;
+    if (!(depth == 8 || (depth == 16 && ctype != 3) || (low && (ctype == 0 || ctype == 3)))) bad("PNG bit depth");
+    if (static_cast<uint64_t>(w) * h > (1ull << 28)) bad("PNG size");
     if (idat.size() < 2) bad("PNG without image data");
     const size_t bits_px = static_cast<size_t>(channels) * depth;
     const size_t stride = (bits_px * w + 7) / 8;
@@ -296,7 +305,8 @@ struct JpegHuff {
     // symbol from the counts per length.
     uint8_t counts[17] = {};
     std::vector<uint8_t> symbols;
-    int maxcode[18], valptr[17], mincode[17];
+    int maxcode[18] = {}, valptr[17] = {}, mincode[17] = {};
+    bool defined = false;
     void build() {
         int code = 0, k = 0;
         for (int l = 1; l <= 16; ++l) {
@@ -304,10 +314,13 @@ struct JpegHuff {
             mincode[l] = code;
             code += counts[l];
             k += counts[l];
+            // More codes of this length than the code space holds.
+            if (code > (1 << l)) bad("JPEG Huffman table over-subscribed");
             maxcode[l] = counts[l] ? code - 1 : -1;
             code <<= 1;
         }
         maxcode[17] = 0x7fffffff;
+        defined = true;
     }
 };
 
@@ -345,6 +358,7 @@ struct JpegBits {
         return v;
     }
     int decode(const JpegHuff &h) {
+        if (!h.defined) bad("JPEG scan uses an undefined Huffman table");
         int code = bit();
         for (int l = 1; l <= 16; ++l) {
             if (h.maxcode[l] >= 0 && code <= h.maxcode[l] && code >= h.mincode[l])
@@ -410,14 +424,15 @@ Image decode_jpeg(const std::vector<uint8_t> &f) {
         if (m == 0xd8 || (m >= 0xd0 && m <= 0xd7) || m == 0x01) continue;
         if (m == 0xd9) break;
         const size_t len = (static_cast<size_t>(f[p]) << 8) | f[p + 1];
-        if (p + len > f.size()) bad("JPEG segment truncated");
+        if (len < 2 || p + len > f.size()) bad("JPEG segment truncated");
         const uint8_t *d = &f[p + 2];
         const size_t dl = len - 2;
         if (m == 0xdb) {
             for (size_t i = 0; i < dl;) {
                 const int pq = d[i] >> 4, tq = d[i] & 15;
                 ++i;
-                if (tq > 3) bad("JPEG quantisation table id");
+                if (tq > 3 || pq > 1) bad("JPEG quantisation table id");
+                if (i + (pq ? 128u : 64u) > dl) bad("JPEG quantisation table truncated");
                 for (int k = 0; k < 64; ++k) {
                     qt[tq][k] = pq ? static_cast<uint16_t>((d[i] << 8) | d[i + 1]) : d[i];
                     i += pq ? 2 : 1;
@@ -427,20 +442,26 @@ Image decode_jpeg(const std::vector<uint8_t> &f) {
             for (size_t i = 0; i < dl;) {
                 const int tc = d[i] >> 4, th = d[i] & 15;
                 ++i;
-                if (th > 3) bad("JPEG Huffman table id");
+                if (th > 3 || tc > 1) bad("JPEG Huffman table id");
+                if (i + 16 > dl) bad("JPEG Huffman table truncated");
                 JpegHuff &t = tc ? hac[th] : hdc[th];
                 int total = 0;
                 for (int l = 1; l <= 16; ++l) total += (t.counts[l] = d[i++]);
+                if (i + static_cast<size_t>(total) > dl) bad("JPEG Huffman table truncated");
                 t.symbols.assign(d + i, d + i + total);
                 i += total;
                 t.build();
             }
         } else if (m == 0xc0 || m == 0xc1) {
+            if (frame) bad("JPEG with two frames");
+            if (dl < 6) bad("JPEG frame header truncated");
             if (d[0] != 8) bad("JPEG sample precision other than 8 bits");
             height = (d[1] << 8) | d[2];
             width = (d[3] << 8) | d[4];
+            if (static_cast<uint64_t>(width) * height > (1ull << 28)) bad("JPEG size");
             const int nc = d[5];
             if (nc != 1 && nc != 3) bad("JPEG component count");
+            if (dl < 6u + 3u * nc) bad("JPEG frame header truncated");
             for (int c = 0; c < nc; ++c) {
                 Comp k;
                 k.id = d[6 + 3 * c];
@@ -456,13 +477,17 @@ Image decode_jpeg(const std::vector<uint8_t> &f) {
         } else if (m >= 0xc2 && m <= 0xcf && m != 0xc4 && m != 0xc8 && m != 0xcc) {
             not_supported("progressive, lossless or arithmetic-coded JPEG");
         } else if (m == 0xdd) {
+            if (dl < 2) bad("JPEG restart interval truncated");
             restart = (d[0] << 8) | d[1];
         } else if (m == 0xda) {
             if (!frame || width == 0 || height == 0) bad("JPEG scan before its frame");
+            if (dl < 1) bad("JPEG scan header truncated");
             const int ns = d[0];
+            if (dl < 1u + 2u * ns) bad("JPEG scan header truncated");
             std::vector<int> order;
             for (int s = 0; s < ns; ++s) {
                 const int id = d[1 + 2 * s], t = d[2 + 2 * s];
+                if ((t >> 4) > 3 || (t & 15) > 3) bad("JPEG Huffman table id");
                 for (size_t c = 0; c < comps.size(); ++c)
                     if (comps[c].id == id) {
                         comps[c].td = t >> 4;
@@ -495,12 +520,15 @@ Image decode_jpeg(const std::vector<uint8_t> &f) {
                                 // T.81 F.2.2: DC difference, then AC run / size pairs.
                                 std::memset(coef, 0, sizeof(coef));
                                 const int t = br.decode(hdc[k.td]);
+                                // 8-bit baseline: DC categories up to 11, AC sizes up to 10.
+                                if (t > 11) bad("JPEG DC difference category");
                                 const int diff = t ? JpegBits::extend(br.bits(t), t) : 0;
                                 k.pred += diff;
                                 coef[0] = static_cast<float>(k.pred * qt[k.tq][0]);
                                 for (int i = 1; i < 64;) {
                                     const int rs = br.decode(hac[k.ta]);
                                     const int r = rs >> 4, sz = rs & 15;
+                                    if (sz > 10) bad("JPEG AC coefficient size");
                                     if (sz == 0) {
                                         if (r == 15) {
                                             i += 16;
@@ -582,14 +610,14 @@ Image decode_hdr(const std::vector<uint8_t> &f) {
         if (p >= f.size()) bad("HDR header truncated");
         const std::string s = line();
         if (s.empty()) break;
-        if (s.rfind("FORMAT=", 0) == 0 && s != "FORMAT=32-bit_rle_rgbe") bad("HDR format " + s);
+        if (s.rfind("FORMAT=", 0) == 0 && s != "FORMAT=32-bit_rle_rgbe") bad("HDR format " + printable(s));
     }
     const std::string res = line();
     int w = 0, h = 0;
     char ys[3] = {}, xs[3] = {};
     if (std::sscanf(res.c_str(), "%2s %d %2s %d", ys, &h, xs, &w) != 4 || std::string(ys) != "-Y" ||
         std::string(xs) != "+X" || w <= 0 || h <= 0)
-        bad("HDR resolution line '" + res + "' (only -Y H +X W)");
+        bad("HDR resolution line '" + printable(res) + "' (only -Y H +X W)");
     std::vector<uint8_t> rgbe(static_cast<size_t>(w) * h * 4);
     for (int y = 0; y < h; ++y) {
         uint8_t *row = &rgbe[static_cast<size_t>(y) * w * 4];
